@@ -1,0 +1,306 @@
+#!/usr/bin/env python
+"""Benchmark of the time step on the single large case (4096x2048 lattice,
+NACA 0012 of chord 512 lu with 1024 markers, heave 0.5c + pitch 30 deg at
+St 0.3, Re 1000, FP32 population storage).
+
+One step = one pass of the hot path: the immersed-boundary kernels and the
+fused stream/collide/boundary lattice kernel over the whole lattice. The
+lattice (2 x 302 MB of FP32 populations) is larger than the 126 MB L2, so no
+flush is needed between steps.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun as N independent replicas (the step does not shard:
+every GPU owns whole cases); `value` is the lattice updates of all ranks over
+the slowest rank's device time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MLUPS & %HBM roofline; batched cases/hr + p99 vs plain FP32 at 1% C_L/C_D"
+UNIT = "MLUPS"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", default="fp32")
+    ap.add_argument("--nx", type=int, default=4096)
+    ap.add_argument("--ny", type=int, default=2048)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def large_case(args, n_steps, precision=None):
+    from fortran_loadfile_mitiwing_b200 import cases
+    if (args.nx, args.ny) == (4096, 2048):
+        return cases.heave_pitch_case(n_steps=n_steps, precision=precision or args.precision)
+    chord = args.ny // 4
+    return cases.heave_pitch_case(nx=args.nx, ny=args.ny, chord=chord, pivot=(2 * chord + 1, args.ny // 2 + 1),
+                                  markers=2 * chord, n_steps=n_steps, precision=precision or args.precision)
+
+
+def workload(args):
+    return {
+        "workload": f"heave+pitch NACA 0012, {args.nx}x{args.ny} D2Q9 MRT lattice, chord {args.ny // 4} lu, "
+                    f"{args.ny // 2} markers, Re 1000, St 0.3, U0 0.05, 4-point delta",
+        "nx": args.nx, "ny": args.ny, "markers": args.ny // 2, "storage": args.precision,
+        "l2": "inputs larger than L2 (two population buffers of 9*nx*ny elements)",
+        "parallelism": "replicas",
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        d = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def kf_traffic():
+    """DRAM bytes per lattice-kernel launch from the committed ncu summary, or None."""
+    try:
+        d = json.load(open(os.path.join(ROOT, "profiles", "kf_traffic.json")))
+        return d
+    except Exception:
+        return None
+
+
+def cpu_oracle_rate(case, max_seconds=20.0, threads=None):
+    """Oracle (the CPU restatement, FP64) on the same case: MLUPS over a bounded
+    number of steps; returns (mlups, steps, cores)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    cores = threads or os.cpu_count()
+    pyoracle.set_threads(cores)
+    o = pyoracle.Oracle.from_case(case)
+    o.evolution()                       # first step outside the sample (impulsive start)
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        o.evolution()
+        steps += 1
+        el = time.perf_counter() - t0
+        if el > max_seconds or steps >= 1000:
+            break
+    o.close()
+    nn = case.params.nx * case.params.ny
+    return nn * steps / el / 1e6, steps, cores, el
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    case = large_case(args, n_steps=args.steps + args.warmup + 10)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    cores = os.cpu_count()
+    pyoracle.set_threads(cores)
+    o = pyoracle.Oracle.from_case(case)
+    t_first = time.perf_counter()
+    for _ in range(max(1, min(args.warmup, 2))):
+        o.evolution()
+    per = (time.perf_counter() - t_first) / max(1, min(args.warmup, 2))
+    k = max(1, min(args.steps, int(150.0 / max(per, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(k):
+        o.evolution()
+    el = time.perf_counter() - t0
+    nn = args.nx * args.ny
+    v = nn * k / el / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": k,
+        "warmup": max(1, min(args.warmup, 2)), "ms_per_step": el / k * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload(args),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{k} full time steps of the {args.nx}x{args.ny} case (reference Fortran "
+                                   f"has no compiler here; CPU FP64 restatement, OpenMP on {cores} threads)"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import ctypes as C
+    import numpy as np
+    import torch
+    from fortran_loadfile_mitiwing_b200 import Lbm, build, cases
+    from fortran_loadfile_mitiwing_b200 import _abi
+    build.build()
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(0)
+    lib = _abi.load_library()
+    k, w = args.steps, args.warmup
+    case = large_case(args, n_steps=k + w + 8)
+    s = Lbm.from_case(case, lib)
+    s.run(w, keep_rows=False)
+    lib.lbm_set_timing(s.h, 1)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    rows = s.run(k)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    step_ms, ib_ms, kf_ms, nt = C.c_double(), C.c_double(), C.c_double(), C.c_int()
+    lib.lbm_get_timing(s.h, C.byref(step_ms), C.byref(ib_ms), C.byref(kf_ms), C.byref(nt))
+    assert nt.value == k and rows.shape[0] == k, (nt.value, rows.shape)
+    assert np.all(np.isfinite(rows))
+    t = torch.tensor([step_ms.value], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    tmax_ms = float(t.item())
+    nn = args.nx * args.ny
+    value = nn * k * world / (tmax_ms / 1e3) / 1e6
+    elem = {"fp32": 4, "fp64": 8, "fp16": 2, "bf16": 2}[args.precision]
+    bpl = 18 * elem
+    kf_avg_s = kf_ms.value / k / 1e3
+    achieved = bpl * nn / kf_avg_s / 1e9
+    peak, peak_kind = measured_peak()
+    tr = kf_traffic()
+    traffic = None
+    if tr and tr.get("nx") and tr.get("bytes_per_launch"):
+        traffic = tr["bytes_per_launch"] * nn / (tr["nx"] * tr["ny"])
+    s.close()
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": k, "warmup": w,
+        "ms_per_step": tmax_ms / k, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": {"fp32": "f32", "fp64": "f64", "fp16": "f16-storage/f32", "bf16": "bf16-storage/f32"}[args.precision],
+        "data": "synthetic (generated NACA 0012 contour and motion table, seeded 1e-4 initial perturbation)",
+        "config": workload(args),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic, "peak_source": peak_kind, "bytes_per_update": bpl,
+                     "kernel": "kf_kernel (fused stream/collide/boundary)",
+                     "kernel_ms": kf_ms.value / k, "ib_ms": ib_ms.value / k},
+        "gpu_launches": 6 * k,
+        "clocks": clocks,
+    }
+    if world > 1:
+        torch.distributed.barrier()
+    if rank == 0 and world == 1 and not args.no_e2e:
+        line["e2e"] = run_e2e(args, lib)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        mlups, steps, cores, el = cpu_oracle_rate(large_case(args, n_steps=200, precision="fp64"))
+        line["cpu_baseline"] = {"value": mlups, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": f"{steps} time steps of the same {args.nx}x{args.ny} case "
+                                          f"({el:.1f} s, CPU FP64 restatement, OpenMP)"}
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_e2e(args, lib):
+    """The same metric through the public API with host buffers: set-up from
+    host arrays (boundary, motion table, initial perturbation), K lbm_step
+    calls each returning its force row to the host, and the final fields."""
+    import numpy as np
+    from fortran_loadfile_mitiwing_b200 import Lbm
+    k = args.steps
+    case = large_case(args, n_steps=k + 8)
+    nn = args.nx * args.ny
+    t0 = time.perf_counter()
+    s = Lbm(case.params, lib)
+    for wi, (x, y) in enumerate(case.contours, start=1):
+        s.set_boundary(wi, x, y)
+    s.set_motion_table(case.table)
+    s.init(case.du, case.dv)
+    for _ in range(k):
+        row = s.evolution()
+    rho, u, v = s.fields()
+    el = time.perf_counter() - t0
+    assert np.all(np.isfinite(row))
+    s.close()
+    h2d = (case.table.nbytes + 2 * nn * 8 + 9 * nn * 8 + sum(x.nbytes + y.nbytes for x, y in case.contours)) / k
+    d2h = s.row_len * 8 + 3 * nn * 8 / k
+    return {"value": nn * k / el / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "note": "wall clock around synchronous C-ABI calls; set-up upload amortised over the steps"}
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+    run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,112 @@
+"""ctypes view of include/lbm_b200.h, shared by the product library and the
+CPU oracle (which takes the same lbm_params struct)."""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "liblbmb200.so")
+
+LBM_OK = 0
+LBM_DONE = 1
+LBM_ERR_ARG = -1
+LBM_ERR_CUDA = -2
+LBM_ERR_STATE = -3
+LBM_ERR_IO = -4
+LBM_ERR_SOLVER = -5
+LBM_ERR_NONFINITE = -6
+LBM_ERR_RANGE = -7
+
+LBM_PREC_FP32 = 0
+LBM_PREC_FP64 = 1
+LBM_PREC_FP16 = 2
+LBM_PREC_BF16 = 3
+PRECISIONS = {"fp32": LBM_PREC_FP32, "fp64": LBM_PREC_FP64, "fp16": LBM_PREC_FP16, "bf16": LBM_PREC_BF16}
+
+LBM_DELTA_PESKIN4 = 0
+LBM_DELTA_SMOOTH = 1
+
+STATUS_NAMES = {0: "LBM_OK", 1: "LBM_DONE", -1: "LBM_ERR_ARG", -2: "LBM_ERR_CUDA", -3: "LBM_ERR_STATE",
+                -4: "LBM_ERR_IO", -5: "LBM_ERR_SOLVER", -6: "LBM_ERR_NONFINITE", -7: "LBM_ERR_RANGE"}
+
+
+class LbmParams(C.Structure):
+    """struct lbm_params (include/lbm_b200.h)."""
+    _fields_ = [
+        ("nx", C.c_int32), ("ny", C.c_int32),
+        ("wing_count", C.c_int32), ("points_per_wing", C.c_int32),
+        ("delta_kernel", C.c_int32), ("precision", C.c_int32),
+        ("flags", C.c_int32), ("reserved", C.c_int32),
+        ("scale", C.c_double), ("ox", C.c_double), ("oy", C.c_double),
+        ("uu", C.c_double), ("re", C.c_double),
+        ("s", C.c_double * 9),
+        ("xc", C.c_double), ("yc", C.c_double), ("xp", C.c_double), ("yp", C.c_double),
+        ("mesh_max_scale", C.c_double),
+    ]
+
+
+# every entry point declared in include/lbm_b200.h: name -> (restype, argtypes)
+_P = C.c_void_p
+_D = C.POINTER(C.c_double)
+ABI = {
+    "lbm_default_params": (C.c_int, [C.POINTER(LbmParams)]),
+    "lbm_create": (C.c_int, [C.POINTER(LbmParams), C.POINTER(_P)]),
+    "lbm_destroy": (C.c_int, [_P]),
+    "lbm_set_boundary": (C.c_int, [_P, C.c_int, _D, _D, C.c_int]),
+    "lbm_read_boundary": (C.c_int, [_P, C.c_char_p]),
+    "lbm_set_motion_table": (C.c_int, [_P, _D, C.c_int, C.c_int]),
+    "lbm_load_motion_table": (C.c_int, [_P, C.c_char_p]),
+    "lbm_parse_boundary_file": (C.c_int, [C.c_char_p, C.c_int, _D, _D]),
+    "lbm_parse_motion_file": (C.c_int, [C.c_char_p, C.c_int, _D, C.c_int, C.POINTER(C.c_int)]),
+    "lbm_init": (C.c_int, [_P, _D, _D]),
+    "lbm_step": (C.c_int, [_P, _D]),
+    "lbm_run": (C.c_int, [_P, C.c_int, _D, C.POINTER(C.c_int)]),
+    "lbm_force_row_length": (C.c_int, [_P]),
+    "lbm_get_fields": (C.c_int, [_P, _D, _D, _D]),
+    "lbm_get_populations": (C.c_int, [_P, _D]),
+    "lbm_set_populations": (C.c_int, [_P, _D]),
+    "lbm_residual": (C.c_int, [_P, _D]),
+    "lbm_get_markers": (C.c_int, [_P, _D, _D, _D]),
+    "lbm_set_timing": (C.c_int, [_P, C.c_int]),
+    "lbm_get_timing": (C.c_int, [_P, _D, _D, _D, C.POINTER(C.c_int)]),
+    "lbm_step_index": (C.c_int, [_P]),
+    "lbm_last_error": (C.c_char_p, [_P]),
+}
+
+
+def header_declarations(header_path=None):
+    """Names of the functions include/lbm_b200.h declares (parsed from the text)."""
+    import re
+    if header_path is None:
+        header_path = os.path.join(os.path.dirname(HERE), "include", "lbm_b200.h")
+    txt = open(header_path).read()
+    return sorted(set(re.findall(r"LBM_API\s+(?:const\s+char\s*\*|int)\s*(lbm_\w+)\s*\(", txt)))
+
+
+_lib = None
+
+
+def load_library(path=None):
+    """Loads liblbmb200.so (built in-tree) and binds the ABI. Raises if absent:
+    there is no fallback implementation."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise RuntimeError(f"CUDA library {p} is missing; build it with "
+                           "python -m fortran_loadfile_mitiwing_b200.build")
+    lib = C.CDLL(p)
+    for name, (res, args) in ABI.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def dptr(a):
+    """double* of a contiguous float64 numpy array (or None)."""
+    if a is None:
+        return None
+    return a.ctypes.data_as(_D)

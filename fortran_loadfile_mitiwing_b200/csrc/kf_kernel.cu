@@ -1,0 +1,317 @@
+// kf_kernel.cu -- the fused lattice update: pull streaming, moments, immersed
+// boundary correction, MRT collision with forcing, and the outer boundary
+// condition, in one pass over the lattice.
+//
+// Reference path folded into this kernel (one time step):
+//   streaming           solution.f90:428-454   f0(i,j,k) = f(i-ex, j-ey, k)
+//   physical_variables  solution.f90:471-542   rho, u, v of f0
+//   IB velocity/force   boundary_condition.f90:1645-1659 (u = u* + du, g = 2 rho du)
+//   colission           solution.f90:573-643   MRT relaxation with forcing
+//   boundary_condition1 boundary_condition.f90:288-858 (left/right
+//                       characteristic + extrapolation, top/bottom rows)
+// Interior nodes read 9 populations and write 9: 72 B per update in FP32.
+// Edge nodes recompute the moments of the one or two interior neighbours
+// their formula needs (O(perimeter) extra reads) so that no second launch and
+// no side buffer is needed for the boundary condition.
+#include "lbm_internal.h"
+
+namespace {
+
+template <typename T, typename C>
+__device__ __forceinline__ void pull(const T *__restrict__ fin, long long plane, int pitch, int i, int j, C g[9])
+{
+#pragma unroll
+    for (int k = 0; k < 9; ++k)
+        g[k] = (C)Store<T>::ld(fin + (long long)k * plane + (long long)(j - lbm_ey(k)) * pitch + (i - lbm_ex(k)));
+}
+
+template <typename C>
+__device__ __forceinline__ void moments(const C g[9], C &drho, C &u, C &v)
+{
+    drho = ((g[0] + g[1]) + (g[2] + g[3])) + ((g[4] + g[5]) + (g[6] + g[7])) + g[8];
+    const C jx = (g[1] - g[3]) + (g[5] - g[6]) + (g[8] - g[7]);
+    const C jy = (g[2] - g[4]) + (g[5] + g[6]) - (g[7] + g[8]);
+    const C rho = C(1) + drho;
+    u = jx / rho;
+    v = jy / rho;
+}
+
+// characteristic update of a left (side=0) or right (side=1) column node
+// (boundary_condition.f90:418-438 and :500-520). Returns the updated
+// (drho, u, v) at the edge node and the streamed populations + moments of its
+// first interior neighbour.
+template <typename T, typename C>
+__device__ __forceinline__ void side_bc(const KFArgs<C> &a, const T *__restrict__ fin, int side, int j, C &dr1,
+                                        C &u1, C &v1, C g0n[9], C &drn, C &un, C &vn)
+{
+    const C *col = side == 0 ? a.col_l : a.col_r;
+    const C drs = col[3 * j], us = col[3 * j + 1], vs = col[3 * j + 2];
+    const int in1 = side == 0 ? 1 : a.nx - 2, in2 = side == 0 ? 2 : a.nx - 3;
+    C g2[9], dr2, u2, v2;
+    pull<T, C>(fin, a.plane, a.pitch, in1, j, g0n);
+    moments(g0n, drn, un, vn);
+    pull<T, C>(fin, a.plane, a.pitch, in2, j, g2);
+    moments(g2, dr2, u2, v2);
+    const C cs = a.cs, rhos = C(1) + drs;
+    if (side == 0) {
+        const C rhox = (C(-3) * drs + C(4) * drn - dr2) * C(0.5);
+        const C ux = (C(-3) * us + C(4) * un - u2) * C(0.5);
+        const C vx = (C(-3) * vs + C(4) * vn - v2) * C(0.5);
+        const C lx1 = (us - cs) * (cs * cs * rhox - cs * rhos * ux);
+        const C lx2 = us < C(0) ? us * vx : C(0);
+        dr1 = drs - lx1 * C(1.5);
+        u1 = us + lx1 / (C(2) * cs * (C(1) + dr1));
+        v1 = vs - lx2;
+    } else {
+        const C rhox = (C(3) * drs - C(4) * drn + dr2) * C(0.5);
+        const C ux = (C(3) * us - C(4) * un + u2) * C(0.5);
+        const C vx = (C(3) * vs - C(4) * vn + v2) * C(0.5);
+        const C lx2 = us >= C(0) ? us * vx : C(0);
+        const C lx3 = (us + cs) * (cs * cs * rhox + cs * rhos * ux);
+        dr1 = drs - lx3 * C(1.5);
+        u1 = us + (C(0) - lx3) / (C(2) * cs * (C(1) + dr1));
+        v1 = vs - lx2;
+    }
+}
+
+template <typename T, typename C, bool FIELDS>
+__global__ void __launch_bounds__(256) kf_kernel(const KFArgs<C> a)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= a.nx) return;
+    const T *__restrict__ fin = (const T *)a.fin;
+    T *__restrict__ fout = (T *)a.fout;
+    const long long o = (long long)j * a.pitch + i;
+    C gout[9];
+    C frho, fu, fv;
+    const bool edge = (i == 0) | (i == a.nx - 1) | (j == 0) | (j == a.ny - 1);
+    if (!edge) {
+        C g[9], drho, u, v;
+        pull<T, C>(fin, a.plane, a.pitch, i, j, g);
+        moments(g, drho, u, v);
+        const C rho = C(1) + drho;
+        C gx = C(0), gy = C(0);
+        const PatchInfo pi = *a.pinfo;
+        const unsigned pii = (unsigned)(i - pi.i0), pjj = (unsigned)(j - pi.j0);
+        if (pii < (unsigned)pi.w && pjj < (unsigned)pi.h) {
+            const long long pq = 2ll * ((long long)pjj * pi.w + pii);
+            const C du = a.patch[pq], dv = a.patch[pq + 1];
+            u = u + du;                       // boundary_condition.f90:1650-1651
+            v = v + dv;
+            gx = C(2) * rho * du;             // :1652-1656
+            gy = C(2) * rho * dv;
+        }
+        C m[9];
+        mrt_forward(g, m);
+        const C jx = rho * u, jy = rho * v;
+        const C jj = jx * jx + jy * jy;
+        C e[9];
+        e[0] = C(-1);                          // temp(1)=0 minus (M w)_1
+        e[1] = C(-2) * drho + C(3) * jj;       // solution.f90:605 minus (M w)_2
+        e[2] = drho - C(3) * jj;               // :606
+        e[3] = C(0);
+        e[4] = -jx;
+        e[5] = C(0);
+        e[6] = -jy;
+        e[7] = jx * jx - jy * jy;
+        e[8] = jx * jy;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) m[k] = m[k] + (e[k] - m[k]) * a.s[k];
+        if (gx != C(0) || gy != C(0)) {        // :614-626
+            const C ug = u * gx + v * gy;
+            m[1] += C(6) * (C(1) - C(0.5) * a.s[1]) * ug;
+            m[2] += C(-6) * (C(1) - C(0.5) * a.s[2]) * ug;
+            m[3] += gx;
+            m[4] += -(C(1) - C(0.5) * a.s[4]) * gx;
+            m[5] += gy;
+            m[6] += -(C(1) - C(0.5) * a.s[6]) * gy;
+            m[7] += C(2) * (C(1) - C(0.5) * a.s[7]) * (u * gx - v * gy);
+            m[8] += (C(1) - C(0.5) * a.s[8]) * (u * gy + v * gx);
+        }
+        mrt_inverse(m, gout);
+        frho = rho; fu = u; fv = v;
+    } else {
+        C g0n[9], drn, un, vn;
+        if (j == 0 || j == a.ny - 1) {
+            // top/bottom row: rho from the adjacent row, u = v = 0
+            // (boundary_condition.f90:658-716, 785-843)
+            const int jn = j == 0 ? 1 : a.ny - 2;
+            if (i == 0 || i == a.nx - 1) {
+                const int side = i == 0 ? 0 : 1;
+                C d2[9], dr2, u2, v2;
+                side_bc<T, C>(a, fin, side, jn, drn, un, vn, d2, dr2, u2, v2);
+                const C *c = a.corner + 9 * (2 * side + (j == 0 ? 0 : 1));
+#pragma unroll
+                for (int k = 0; k < 9; ++k) g0n[k] = c[k];   // edge f0, never rewritten
+            } else {
+                pull<T, C>(fin, a.plane, a.pitch, i, jn, g0n);
+                moments(g0n, drn, un, vn);
+            }
+            extrapolate_dev<C>(a.s, drn, C(0), C(0), drn, un, vn, g0n, gout);
+            frho = C(1) + drn; fu = C(0); fv = C(0);
+        } else {
+            // left/right column (boundary_condition.f90:413-483, 495-567)
+            const int side = i == 0 ? 0 : 1;
+            C dr1, u1, v1;
+            side_bc<T, C>(a, fin, side, j, dr1, u1, v1, g0n, drn, un, vn);
+            extrapolate_dev<C>(a.s, dr1, u1, v1, drn, un, vn, g0n, gout);
+            frho = C(1) + dr1; fu = u1; fv = v1;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 9; ++k) Store<T>::st(fout + (long long)k * a.plane + o, gout[k]);
+    if (FIELDS) {
+        const long long q = (long long)j * a.nx + i;
+        a.rho_out[q] = frho;
+        a.u_out[q] = fu;
+        a.v_out[q] = fv;
+    }
+}
+
+template <typename T, typename C>
+int launch_kf_t(lbm_handle *h, const void *fin, void *fout, void *fields)
+{
+    KFArgs<C> a;
+    a.fin = fin;
+    a.fout = fout;
+    a.nx = h->nx;
+    a.ny = h->ny;
+    a.pitch = h->pitch;
+    a.plane = h->plane;
+    for (int k = 0; k < 9; ++k) a.s[k] = (C)h->s[k];
+    a.cs = (C)((double)sqrtf(3.0f) / 3.0);   // boundary_condition.f90:304
+    const C *ec = (const C *)h->edge_c;
+    a.col_l = ec;
+    a.col_r = ec + 3 * h->ny;
+    a.corner = ec + 6 * h->ny;
+    a.pinfo = h->d_pinfo;
+    a.patch = (const C *)h->d_patch;
+    if (fields) {
+        C *fc = (C *)fields;
+        const long long nn = (long long)h->nx * h->ny;
+        a.rho_out = fc;
+        a.u_out = fc + nn;
+        a.v_out = fc + 2 * nn;
+    } else {
+        a.rho_out = a.u_out = a.v_out = nullptr;
+    }
+    dim3 block(256, 1), grid((h->nx + 255) / 256, h->ny);
+    if (fields)
+        kf_kernel<T, C, true><<<grid, block, 0, h->stream>>>(a);
+    else
+        kf_kernel<T, C, false><<<grid, block, 0, h->stream>>>(a);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+// ---- conversions between the host FP64 f(nx,ny,9) and device storage ----
+
+__device__ __forceinline__ double wref(int k) { return k == 0 ? 4.0 / 9.0 : (k < 5 ? 1.0 / 9.0 : 1.0 / 36.0); }
+
+template <typename T>
+__global__ void unpack_kernel(const T *__restrict__ src, double *__restrict__ dst, int nx, int ny, int pitch,
+                              long long plane)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i >= nx) return;
+    dst[(long long)k * nx * ny + (long long)j * nx + i] =
+        (double)Store<T>::ld(src + k * plane + (long long)j * pitch + i) + wref(k);
+}
+
+template <typename T>
+__global__ void pack_kernel(const double *__restrict__ src, T *__restrict__ dst, int nx, int ny, int pitch,
+                            long long plane)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, k = blockIdx.z;
+    if (i >= nx) return;
+    const double g = src[(long long)k * nx * ny + (long long)j * nx + i] - wref(k);
+    Store<T>::st(dst + k * plane + (long long)j * pitch + i, (typename CType<T>::type)g);
+}
+
+// interior sums of erranalysis (solution.f90:102-108), FP64, fields in compute precision
+template <typename C>
+__global__ void residual_kernel(const C *__restrict__ fa, const C *__restrict__ fb, int nx, int ny,
+                                double *__restrict__ out)
+{
+    const long long nn = (long long)nx * ny;
+    double s1 = 0, s2 = 0;
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < nn;
+         q += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(q % nx), j = (int)(q / nx);
+        if (i < 1 || i > nx - 2 || j < 1 || j > ny - 2) continue;
+        const double u = (double)fa[nn + q], v = (double)fa[2 * nn + q];
+        const double u0 = (double)fb[nn + q], v0 = (double)fb[2 * nn + q];
+        s1 += (u - u0) * (u - u0) + (v - v0) * (v - v0);
+        s2 += u * u + v * v;
+    }
+    for (int off = 16; off; off >>= 1) {
+        s1 += __shfl_down_sync(0xffffffffu, s1, off);
+        s2 += __shfl_down_sync(0xffffffffu, s2, off);
+    }
+    __shared__ double r1[32], r2[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) { r1[wid] = s1; r2[wid] = s2; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t1 = 0, t2 = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) { t1 += r1[w]; t2 += r2[w]; }
+        out[2 * blockIdx.x] = t1;
+        out[2 * blockIdx.x + 1] = t2;
+    }
+}
+
+}  // namespace
+
+int launch_kf(lbm_handle *h, const void *fin, void *fout, void *fields)
+{
+    switch (h->prec) {
+    case LBM_PREC_FP32: return launch_kf_t<float, float>(h, fin, fout, fields);
+    case LBM_PREC_FP64: return launch_kf_t<double, double>(h, fin, fout, fields);
+    case LBM_PREC_FP16: return launch_kf_t<__half, float>(h, fin, fout, fields);
+    case LBM_PREC_BF16: return launch_kf_t<__nv_bfloat16, float>(h, fin, fout, fields);
+    }
+    return -1;
+}
+
+int launch_unpack(lbm_handle *h, const void *fsrc, double *dst)
+{
+    dim3 block(256), grid((h->nx + 255) / 256, h->ny, 9);
+    switch (h->prec) {
+    case LBM_PREC_FP32: unpack_kernel<float><<<grid, block, 0, h->stream>>>((const float *)fsrc, dst, h->nx, h->ny, h->pitch, h->plane); break;
+    case LBM_PREC_FP64: unpack_kernel<double><<<grid, block, 0, h->stream>>>((const double *)fsrc, dst, h->nx, h->ny, h->pitch, h->plane); break;
+    case LBM_PREC_FP16: unpack_kernel<__half><<<grid, block, 0, h->stream>>>((const __half *)fsrc, dst, h->nx, h->ny, h->pitch, h->plane); break;
+    case LBM_PREC_BF16: unpack_kernel<__nv_bfloat16><<<grid, block, 0, h->stream>>>((const __nv_bfloat16 *)fsrc, dst, h->nx, h->ny, h->pitch, h->plane); break;
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int launch_pack(lbm_handle *h, const double *src, void *fdst)
+{
+    dim3 block(256), grid((h->nx + 255) / 256, h->ny, 9);
+    switch (h->prec) {
+    case LBM_PREC_FP32: pack_kernel<float><<<grid, block, 0, h->stream>>>(src, (float *)fdst, h->nx, h->ny, h->pitch, h->plane); break;
+    case LBM_PREC_FP64: pack_kernel<double><<<grid, block, 0, h->stream>>>(src, (double *)fdst, h->nx, h->ny, h->pitch, h->plane); break;
+    case LBM_PREC_FP16: pack_kernel<__half><<<grid, block, 0, h->stream>>>(src, (__half *)fdst, h->nx, h->ny, h->pitch, h->plane); break;
+    case LBM_PREC_BF16: pack_kernel<__nv_bfloat16><<<grid, block, 0, h->stream>>>(src, (__nv_bfloat16 *)fdst, h->nx, h->ny, h->pitch, h->plane); break;
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int launch_residual(lbm_handle *h, const void *fa, const void *fb, double *out2)
+{
+    const int blocks = 296, threads = 256;
+    if (h->prec == LBM_PREC_FP64)
+        residual_kernel<double><<<blocks, threads, 0, h->stream>>>((const double *)fa, (const double *)fb, h->nx, h->ny, h->d_red);
+    else
+        residual_kernel<float><<<blocks, threads, 0, h->stream>>>((const float *)fa, (const float *)fb, h->nx, h->ny, h->d_red);
+    if (cudaGetLastError() != cudaSuccess) return -1;
+    std::vector<double> part(2 * blocks);
+    if (cudaMemcpyAsync(part.data(), h->d_red, sizeof(double) * 2 * blocks, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess)
+        return -1;
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return -1;
+    double t1 = 0, t2 = 0;
+    for (int b = 0; b < blocks; ++b) { t1 += part[2 * b]; t2 += part[2 * b + 1]; }
+    out2[0] = t1;
+    out2[1] = t2;
+    return 0;
+}

@@ -1,0 +1,640 @@
+// lbm_capi.cu -- the extern "C" boundary (include/lbm_b200.h): handle
+// lifetime, device memory, initial state, and the per-step launch sequence.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <vector>
+
+#include "lbm_internal.h"
+
+namespace {
+
+const double kWref[9] = {4.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0,
+                         1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0};
+const int kEx[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
+const int kEy[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
+const int kRing = 2048;   // force rows kept on the device between host copies
+
+int set_err(lbm_handle *h, int code, const char *msg)
+{
+    if (h) h->err = msg;
+    return code;
+}
+
+int cuda_err(lbm_handle *h, cudaError_t e, const char *where)
+{
+    char buf[256];
+    snprintf(buf, sizeof buf, "%s: %s", where, cudaGetErrorString(e));
+    return set_err(h, LBM_ERR_CUDA, buf);
+}
+
+#define CK(call, where)                                   \
+    do {                                                  \
+        cudaError_t e_ = (call);                          \
+        if (e_ != cudaSuccess) return cuda_err(h, e_, where); \
+    } while (0)
+
+size_t compute_size(int prec) { return prec == LBM_PREC_FP64 ? sizeof(double) : sizeof(float); }
+
+size_t storage_size(int prec)
+{
+    switch (prec) {
+    case LBM_PREC_FP64: return 8;
+    case LBM_PREC_FP32: return 4;
+    default: return 2;
+    }
+}
+
+// single-precision lattice weights of D2Q9model (D2Q9model.f90:24-32)
+double wsingle(int k) { return k == 0 ? (double)(4.0f / 9.0f) : (k < 5 ? (double)(1.0f / 9.0f) : (double)(1.0f / 36.0f)); }
+
+// D2Q9feq (D2Q9model.f90:35-46), host FP64
+double feq(double rh, double u1, double v1, int k)
+{
+    const double eu = (double)kEx[k] * u1 + (double)kEy[k] * v1;
+    const double utwo = u1 * u1 + v1 * v1;
+    return wsingle(k) * rh * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * utwo);
+}
+
+void free_dev(void *&p)
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+template <typename P> void free_devp(P *&p)
+{
+    void *q = (void *)p;
+    free_dev(q);
+    p = nullptr;
+}
+
+// rows of the motion step table (mode.f90:176-269), host FP64
+void lookup_row(const std::vector<double> &tab, int rows, int cols, double t, int &idx, double *row)
+{
+    auto T = [&](int r, int c) { return tab[(size_t)c * rows + r]; };
+    if (t <= T(0, 0)) {
+        idx = 0;
+        for (int c = 0; c < cols; ++c) row[c] = T(0, c);
+        row[0] = t;
+        return;
+    }
+    if (t >= T(rows - 1, 0)) {
+        idx = std::max(rows - 2, 0);
+        for (int c = 0; c < cols; ++c) row[c] = T(rows - 1, c);
+        row[0] = t;
+        return;
+    }
+    int mi = std::max(0, std::min(idx, rows - 2));
+    while (mi > 0 && t < T(mi, 0)) mi--;
+    while (mi < rows - 2 && t > T(mi + 1, 0)) mi++;
+    idx = mi;
+    if (fabs(t - T(mi, 0)) <= 1.0e-12) {
+        for (int c = 0; c < cols; ++c) row[c] = T(mi, c);
+        row[0] = t;
+        return;
+    }
+    if (fabs(t - T(mi + 1, 0)) <= 1.0e-12) {
+        for (int c = 0; c < cols; ++c) row[c] = T(mi + 1, c);
+        row[0] = t;
+        return;
+    }
+    const double t1 = T(mi, 0), t2 = T(mi + 1, 0);
+    if (fabs(t2 - t1) <= 1.0e-14) {
+        for (int c = 0; c < cols; ++c) row[c] = T(mi, c);
+        row[0] = t;
+        return;
+    }
+    const double weight = (t - t1) / (t2 - t1);
+    for (int c = 0; c < cols; ++c) row[c] = (1.0 - weight) * T(mi, c) + weight * T(mi + 1, c);
+    row[0] = t;
+}
+
+// Allocates the immersed-boundary scratch once geometry and motion are known:
+// the correction patch is sized by the largest per-step rectangle of the
+// bodies' bounding discs over the whole motion table.
+int ensure_ib(lbm_handle *h)
+{
+    if (h->ib_ready) return LBM_OK;
+    int wmax = 0, hmax = 0;
+    if (h->nseg > 0) {
+        std::vector<double> R(h->nwing, 0.0);
+        for (int w = 0; w < h->nwing; ++w)
+            for (int p = 0; p < h->ppw; ++p) {
+                const double x = h->hx0[w * h->ppw + p], y = h->hy0[w * h->ppw + p];
+                R[w] = std::max(R[w], sqrt(x * x + y * y));
+            }
+        for (int s = 0; s < h->msteps; ++s) {
+            double xlo = 1e300, xhi = -1e300, ylo = 1e300, yhi = -1e300;
+            for (int w = 0; w < h->nwing; ++w) {
+                const double sa = h->mstep_host[(size_t)s * h->mcols + 4 + 9 * w];
+                const double sb = h->mstep_host[(size_t)s * h->mcols + 7 + 9 * w];
+                const double cx = (sa + h->p.xc - h->p.ox) / h->p.scale, cy = (sb + h->p.yc - h->p.oy) / h->p.scale;
+                const double r = R[w] / h->p.scale + 4.0;
+                xlo = std::min(xlo, cx - r); xhi = std::max(xhi, cx + r);
+                ylo = std::min(ylo, cy - r); yhi = std::max(yhi, cy + r);
+            }
+            wmax = std::max(wmax, (int)ceil(xhi - xlo) + 2);
+            hmax = std::max(hmax, (int)ceil(yhi - ylo) + 2);
+        }
+        wmax = std::min(wmax, h->nx);
+        hmax = std::min(hmax, h->ny);
+    }
+    h->patch_wmax = wmax;
+    h->patch_hmax = hmax;
+    h->patch_cap = std::max(1, wmax * hmax);
+    const size_t cs = compute_size(h->prec);
+    CK(cudaMalloc(&h->d_patch, 2 * cs * (size_t)h->patch_cap), "alloc patch");
+    CK(cudaMemsetAsync(h->d_patch, 0, 2 * cs * (size_t)h->patch_cap, h->stream), "clear patch");
+    const int ns = std::max(1, h->nseg);
+    CK(cudaMalloc(&h->d_mk, sizeof(Marker) * ns), "alloc markers");
+    CK(cudaMalloc(&h->d_rhs, sizeof(double) * 2 * ns), "alloc rhs");
+    CK(cudaMalloc(&h->d_y, sizeof(double) * 2 * ns), "alloc y");
+    CK(cudaMalloc(&h->d_B, sizeof(double) * (size_t)ns * ns), "alloc B");
+    const int nblk = h->patch_gx() * h->patch_gy();
+    CK(cudaMalloc(&h->d_partial, sizeof(double) * 3 * LBM_MAXW * (size_t)nblk), "alloc partials");
+    if (ib_configure(h) != 0) return set_err(h, LBM_ERR_CUDA, "ib_configure failed");
+    h->ib_ready = 1;
+    return LBM_OK;
+}
+
+int check_status(lbm_handle *h)
+{
+    unsigned st = 0;
+    CK(cudaMemcpyAsync(&st, h->d_status, sizeof st, cudaMemcpyDeviceToHost, h->stream), "read status");
+    CK(cudaStreamSynchronize(h->stream), "step sync");
+    if (!st) return LBM_OK;
+    CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream), "clear status");
+    if (st & LBM_ST_RANGE)
+        return set_err(h, LBM_ERR_RANGE, "move_boundary: a marker support box reaches the three outermost node layers");
+    if (st & LBM_ST_OVERFLOW) return set_err(h, LBM_ERR_RANGE, "immersed boundary: correction patch overflow");
+    if (st & LBM_ST_SOLVER) return set_err(h, LBM_ERR_SOLVER, "immersed boundary: D D^T not positive definite");
+    if (st & LBM_ST_NONFINITE) return set_err(h, LBM_ERR_NONFINITE, "non-finite force");
+    return set_err(h, LBM_ERR_CUDA, "unknown device status");
+}
+
+// sums the event intervals of `count` step slots after the stream is idle:
+// step time is the span from the first step's start to the last step's end
+// (gaps between launches included), IB and lattice times are per-kernel sums
+int collect_timing(lbm_handle *h, int count)
+{
+    if (count < 1) return LBM_OK;
+    for (int s = 0; s < count; ++s) {
+        float a = 0, b = 0;
+        CK(cudaEventElapsedTime(&a, h->ev[3 * s], h->ev[3 * s + 1]), "event time");
+        CK(cudaEventElapsedTime(&b, h->ev[3 * s + 1], h->ev[3 * s + 2]), "event time");
+        h->t_ib += a;
+        h->t_kf += b;
+        h->t_steps++;
+    }
+    float span = 0;
+    CK(cudaEventElapsedTime(&span, h->ev[0], h->ev[3 * (count - 1) + 2]), "event time");
+    h->t_step += span;
+    return LBM_OK;
+}
+
+// The per-step sequence: IB chain, then the fused lattice update.
+int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool fields_every)
+{
+    if (!h->inited) return set_err(h, LBM_ERR_STATE, "step: lbm_init not called");
+    for (int w = 0; w < h->nwing; ++w)
+        if (!h->have_wing[w]) return set_err(h, LBM_ERR_STATE, "step: boundary of a wing not set");
+    int rc = ensure_ib(h);
+    if (rc) return rc;
+    int done = 0, pending = 0;
+    rc = LBM_OK;
+    for (int s = 0; s < nsteps; ++s) {
+        const double time = (double)(h->n - 1) * (h->p.scale * h->p.uu);   // main.f90:352
+        if (time > h->mend + 1.0e-12) { rc = LBM_DONE; break; }
+        const int slot = pending;
+        const void *fin = h->fbuf[h->cur];
+        void *fout = h->fbuf[h->cur ^ 1];
+        if (h->timing) CK(cudaEventRecord(h->ev[3 * slot], h->stream), "event");
+        if (launch_ib(h, fin, h->n, slot)) return cuda_err(h, cudaGetLastError(), "launch ib");
+        if (h->timing) CK(cudaEventRecord(h->ev[3 * slot + 1], h->stream), "event");
+        void *fields = nullptr;
+        const bool want = fields_every || s >= nsteps - 2;
+        if (want) {
+            const int fs = h->fields_slot ^ 1;
+            fields = h->d_fields[fs];
+            h->fields_slot = fs;
+            h->fields_step[fs] = h->n;
+        }
+        if (launch_kf(h, fin, fout, fields)) return cuda_err(h, cudaGetLastError(), "launch kf");
+        if (h->timing) CK(cudaEventRecord(h->ev[3 * slot + 2], h->stream), "event");
+        h->cur ^= 1;
+        h->n++;
+        h->steps_done++;
+        done++;
+        pending++;
+        if (pending == h->ring_cap || s == nsteps - 1) {
+            if (rows_out)
+                CK(cudaMemcpyAsync(rows_out + (size_t)(done - pending) * h->row_len, h->d_ring,
+                                   sizeof(double) * h->row_len * pending, cudaMemcpyDeviceToHost, h->stream),
+                   "copy force rows");
+            int st = check_status(h);
+            if (st) return st;
+            if (h->timing && (st = collect_timing(h, pending))) return st;
+            pending = 0;
+        }
+    }
+    if (pending) {
+        if (rows_out)
+            CK(cudaMemcpyAsync(rows_out + (size_t)(done - pending) * h->row_len, h->d_ring,
+                               sizeof(double) * h->row_len * pending, cudaMemcpyDeviceToHost, h->stream),
+               "copy force rows");
+        int st = check_status(h);
+        if (st) return st;
+        if (h->timing && (st = collect_timing(h, pending))) return st;
+    }
+    if (done_out) *done_out = done;
+    return rc;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_default_params(lbm_params *p)
+{
+    if (!p) return LBM_ERR_ARG;
+    memset(p, 0, sizeof *p);
+    p->nx = 4001;                 // nint(40/0.01)+1 (ini_mesh.f90:22)
+    p->ny = 2001;                 // nint(20/0.01)+1 (ini_mesh.f90:23)
+    p->wing_count = 2;            // main.f90:18
+    p->points_per_wing = 205;     // main.f90:21
+    p->delta_kernel = LBM_DELTA_SMOOTH;   // boundary_condition.f90:1530
+    p->precision = LBM_PREC_FP32;
+    p->scale = 0.01;              // mesh_max_scale (main.f90:32)
+    p->ox = -20.0;                // -0.5*width (ini_mesh.f90:36)
+    p->oy = -10.0;
+    p->uu = 0.01;                 // main.f90:12
+    p->re = 500.0;                // main.f90:84
+    const double s[9] = {0.0, 1.1, 1.05, 0.0, 1.2, 0.0, 1.2, 0.0, 0.0};   // ini_mesh.f90:59-67
+    memcpy(p->s, s, sizeof s);
+    p->mesh_max_scale = 0.01;
+    return LBM_OK;
+}
+
+int lbm_create(const lbm_params *p, lbm_t **out)
+{
+    if (!p || !out) return LBM_ERR_ARG;
+    *out = nullptr;
+    if (p->nx < 16 || p->ny < 16 || p->wing_count < 0 || p->wing_count > LBM_MAXW ||
+        (p->wing_count > 0 && p->points_per_wing < 3) || !(p->scale > 0) || !(p->uu > 0) || !(p->re > 0) ||
+        p->precision < 0 || p->precision > 3 || p->delta_kernel < 0 || p->delta_kernel > 1 || p->flags != 0)
+        return LBM_ERR_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return LBM_ERR_CUDA;
+    lbm_handle *h = new lbm_handle();
+    h->p = *p;
+    cudaGetDevice(&h->dev);
+    h->nx = p->nx;
+    h->ny = p->ny;
+    h->pitch = (p->nx + 63) / 64 * 64;
+    h->plane = (long long)h->pitch * p->ny;
+    h->nwing = p->wing_count;
+    h->ppw = h->nwing > 0 ? p->points_per_wing : 0;
+    h->spw = h->ppw > 0 ? h->ppw - 1 : 0;
+    h->npts = h->nwing * h->ppw;
+    h->nseg = h->nwing * h->spw;
+    h->niu = p->uu * (1.0 / p->scale) / p->re;   // ini_mesh.f90:30
+    h->tau = 3.0 * h->niu + 0.5;                  // ini_mesh.f90:31
+    for (int k = 0; k < 9; ++k) h->s[k] = p->s[k];
+    if (p->s[7] <= 0) h->s[7] = 1.0 / h->tau;
+    if (p->s[8] <= 0) h->s[8] = 1.0 / h->tau;
+    h->prec = p->precision;
+    h->elem = storage_size(h->prec);
+    h->hx0.assign(std::max(1, h->npts), 0.0);
+    h->hy0.assign(std::max(1, h->npts), 0.0);
+    h->harc.assign(std::max(1, h->nseg), 0.0);
+    h->have_wing.assign(LBM_MAXW, 0);
+    h->row_len = 1 + 3 * h->nwing + 3 + 9 * h->nwing;
+    h->ring_cap = kRing;
+    auto fail = [&](cudaError_t e, const char *w) {
+        lbm_destroy(h);
+        (void)e; (void)w;
+        return LBM_ERR_CUDA;
+    };
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
+    const size_t fbytes = h->elem * 9 * (size_t)h->plane;
+    for (int b = 0; b < 2; ++b) {
+        if ((e = cudaMalloc(&h->fbuf[b], fbytes)) != cudaSuccess) return fail(e, "alloc f");
+        if ((e = cudaMemset(h->fbuf[b], 0, fbytes)) != cudaSuccess) return fail(e, "clear f");
+    }
+    const size_t cs = compute_size(h->prec);
+    const size_t nn = (size_t)h->nx * h->ny;
+    for (int b = 0; b < 2; ++b)
+        if ((e = cudaMalloc(&h->d_fields[b], 3 * cs * nn)) != cudaSuccess) return fail(e, "alloc fields");
+    if ((e = cudaMalloc(&h->edge_c, cs * (6 * (size_t)h->ny + 36))) != cudaSuccess) return fail(e, "alloc edge");
+    if ((e = cudaMalloc(&h->d_status, sizeof(unsigned))) != cudaSuccess) return fail(e, "alloc status");
+    if ((e = cudaMalloc(&h->d_counter, sizeof(unsigned))) != cudaSuccess) return fail(e, "alloc counter");
+    if ((e = cudaMalloc(&h->d_pinfo, sizeof(PatchInfo))) != cudaSuccess) return fail(e, "alloc pinfo");
+    if ((e = cudaMalloc(&h->d_red, sizeof(double) * 2 * 296)) != cudaSuccess) return fail(e, "alloc red");
+    if ((e = cudaMalloc(&h->d_solve_res, sizeof(double))) != cudaSuccess) return fail(e, "alloc res");
+    if ((e = cudaMalloc(&h->d_ring, sizeof(double) * h->row_len * (size_t)h->ring_cap)) != cudaSuccess)
+        return fail(e, "alloc ring");
+    cudaMemset(h->d_status, 0, sizeof(unsigned));
+    cudaMemset(h->d_counter, 0, sizeof(unsigned));
+    cudaMemset(h->d_pinfo, 0, sizeof(PatchInfo));
+    cudaMemset(h->d_solve_res, 0, sizeof(double));
+    if (h->npts > 0) {
+        if ((e = cudaMalloc(&h->d_xb0, sizeof(double) * h->npts)) != cudaSuccess) return fail(e, "alloc xb0");
+        if ((e = cudaMalloc(&h->d_yb0, sizeof(double) * h->npts)) != cudaSuccess) return fail(e, "alloc yb0");
+        if ((e = cudaMalloc(&h->d_arc, sizeof(double) * h->nseg)) != cudaSuccess) return fail(e, "alloc arc");
+    }
+    if ((e = cudaDeviceSynchronize()) != cudaSuccess) return fail(e, "sync");
+    *out = h;
+    return LBM_OK;
+}
+
+int lbm_destroy(lbm_t *h)
+{
+    if (!h) return LBM_ERR_ARG;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (int b = 0; b < 2; ++b) { free_dev(h->fbuf[b]); free_dev(h->d_fields[b]); }
+    free_dev(h->edge_c);
+    free_devp(h->d_xb0); free_devp(h->d_yb0); free_devp(h->d_arc); free_devp(h->d_mstep);
+    free_devp(h->d_mk); free_devp(h->d_rhs); free_devp(h->d_B); free_devp(h->d_y);
+    free_devp(h->d_pinfo); free_dev(h->d_patch); free_devp(h->d_partial); free_devp(h->d_counter);
+    free_devp(h->d_ring); free_devp(h->d_status); free_devp(h->d_solve_res); free_devp(h->d_red);
+    free_devp(h->d_stage);
+    for (auto &e : h->ev) cudaEventDestroy(e);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return LBM_OK;
+}
+
+int lbm_set_boundary(lbm_t *h, int wing, const double *x, const double *y, int npts)
+{
+    if (!h) return LBM_ERR_ARG;
+    if (wing < 1 || wing > h->nwing || !x || !y || npts != h->ppw)
+        return set_err(h, LBM_ERR_ARG, "set_boundary: bad wing index or point count");
+    const int ps = (wing - 1) * h->ppw, ss = (wing - 1) * h->spw;
+    for (int i = 0; i < npts; ++i) {
+        if (!std::isfinite(x[i]) || !std::isfinite(y[i])) return set_err(h, LBM_ERR_ARG, "set_boundary: non-finite point");
+        h->hx0[ps + i] = x[i];
+        h->hy0[ps + i] = y[i];
+    }
+    for (int i0 = 0; i0 < h->spw; ++i0) {                 // airfoil.f90:235-238
+        const double dx = h->hx0[ps + i0 + 1] - h->hx0[ps + i0];
+        const double dy = h->hy0[ps + i0 + 1] - h->hy0[ps + i0];
+        h->harc[ss + i0] = sqrt(dx * dx + dy * dy) / h->p.scale;
+    }
+    for (int i = 0; i < npts; ++i) {                      // airfoil.f90:240-241
+        h->hx0[ps + i] = h->hx0[ps + i] + (h->p.xc - h->p.xp);
+        h->hy0[ps + i] = h->hy0[ps + i] + (h->p.yc - h->p.yp);
+    }
+    CK(cudaMemcpyAsync(h->d_xb0 + ps, h->hx0.data() + ps, sizeof(double) * npts, cudaMemcpyHostToDevice, h->stream), "copy xb0");
+    CK(cudaMemcpyAsync(h->d_yb0 + ps, h->hy0.data() + ps, sizeof(double) * npts, cudaMemcpyHostToDevice, h->stream), "copy yb0");
+    CK(cudaMemcpyAsync(h->d_arc + ss, h->harc.data() + ss, sizeof(double) * h->spw, cudaMemcpyHostToDevice, h->stream), "copy arc");
+    CK(cudaStreamSynchronize(h->stream), "sync boundary");
+    h->have_wing[wing - 1] = 1;
+    h->ib_ready = 0;
+    free_dev(h->d_patch);
+    free_devp(h->d_mk); free_devp(h->d_rhs); free_devp(h->d_B); free_devp(h->d_y); free_devp(h->d_partial);
+    return LBM_OK;
+}
+
+int lbm_set_motion_table(lbm_t *h, const double *table, int rows, int cols)
+{
+    if (!h) return LBM_ERR_ARG;
+    if (!table) return set_err(h, LBM_ERR_ARG, "motion table: null");
+    if (cols != 1 + 9 * h->nwing) return set_err(h, LBM_ERR_IO, "motion table: column count must be 1+9*wing_count");
+    if (rows < 1) return set_err(h, LBM_ERR_IO, "motion table: empty");          // mode.f90:101-104
+    for (int r = 1; r < rows; ++r)                                                 // mode.f90:130-135
+        if (table[r] < table[r - 1]) return set_err(h, LBM_ERR_IO, "motion table: time column must be non-decreasing");
+    for (size_t q = 0; q < (size_t)rows * cols; ++q)
+        if (!std::isfinite(table[q])) return set_err(h, LBM_ERR_IO, "motion table: non-finite value");
+    h->mtab.assign(table, table + (size_t)rows * cols);
+    h->mrows = rows;
+    h->mcols = cols;
+    h->mend = table[rows - 1];                                                     // mode.f90:127
+    h->mdt = h->p.scale * h->p.uu;                                                 // main.f90:255
+    h->msteps = (int)((h->mend + 1.0e-12) / h->mdt) + 1;                           // mode.f90:258
+    h->mstep_host.assign((size_t)h->msteps * cols, 0.0);
+    int idx = 0;
+    std::vector<double> row(cols);
+    for (int i = 1; i <= h->msteps; ++i) {                                         // mode.f90:263-268
+        lookup_row(h->mtab, rows, cols, (double)(i - 1) * h->mdt, idx, row.data());
+        std::copy(row.begin(), row.end(), h->mstep_host.begin() + (size_t)(i - 1) * cols);
+    }
+    free_devp(h->d_mstep);
+    CK(cudaMalloc(&h->d_mstep, sizeof(double) * h->mstep_host.size()), "alloc step table");
+    CK(cudaMemcpyAsync(h->d_mstep, h->mstep_host.data(), sizeof(double) * h->mstep_host.size(),
+                       cudaMemcpyHostToDevice, h->stream), "copy step table");
+    CK(cudaStreamSynchronize(h->stream), "sync motion");
+    h->ib_ready = 0;
+    free_dev(h->d_patch);
+    free_devp(h->d_mk); free_devp(h->d_rhs); free_devp(h->d_B); free_devp(h->d_y); free_devp(h->d_partial);
+    return LBM_OK;
+}
+
+int lbm_init(lbm_t *h, const double *du, const double *dv)
+{
+    if (!h) return LBM_ERR_ARG;
+    if (h->mstep_host.empty()) return set_err(h, LBM_ERR_STATE, "init: motion table not loaded (mode.f90:275-276)");
+    const int nx = h->nx, ny = h->ny;
+    const size_t nn = (size_t)nx * ny;
+    // initial f = feq(rho=1, u=UU(+du), v=0(+dv)) with single-precision weights
+    // (solution.f90:33-59), kept as FP64 deviations f - w
+    std::vector<double> g(nn * 9);
+    std::vector<double> fu(nn), fv(nn);
+    for (size_t q = 0; q < nn; ++q) {
+        double u = h->p.uu, v = 0.0;
+        if (du) u = u + du[q];
+        if (dv) v = v + dv[q];
+        fu[q] = u;
+        fv[q] = v;
+        for (int k = 0; k < 9; ++k) g[(size_t)k * nn + q] = feq(1.0, u, v, k) - kWref[k];
+    }
+    // edge constants: moments of the edge f0 (physical_variables on the
+    // edge, solution.f90:516-520) and the corner-column f0 populations
+    const size_t cs = compute_size(h->prec);
+    std::vector<double> ec(6 * (size_t)ny + 36);
+    for (int side = 0; side < 2; ++side) {
+        const int i = side == 0 ? 0 : nx - 1;
+        for (int j = 0; j < ny; ++j) {
+            const size_t q = (size_t)j * nx + i;
+            double temprho = 0.0, tempu = 0.0, tempv = 0.0;
+            for (int k = 0; k < 9; ++k) {
+                const double f = feq(1.0, fu[q], fv[q], k);
+                temprho = temprho + f;
+                tempu = tempu + (double)kEx[k] * f;
+                tempv = tempv + (double)kEy[k] * f;
+            }
+            double *o = ec.data() + (size_t)side * 3 * ny + 3 * (size_t)j;
+            o[0] = temprho - 1.0;
+            o[1] = tempu / temprho;
+            o[2] = tempv / temprho;
+        }
+    }
+    const int ci[4] = {0, 0, nx - 1, nx - 1}, cj[4] = {1, ny - 2, 1, ny - 2};
+    for (int c = 0; c < 4; ++c)
+        for (int k = 0; k < 9; ++k) ec[6 * (size_t)ny + 9 * c + k] = g[(size_t)k * nn + (size_t)cj[c] * nx + ci[c]];
+    if (cs == sizeof(double)) {
+        CK(cudaMemcpyAsync(h->edge_c, ec.data(), sizeof(double) * ec.size(), cudaMemcpyHostToDevice, h->stream), "copy edge");
+    } else {
+        std::vector<float> ef(ec.begin(), ec.end());
+        CK(cudaMemcpyAsync(h->edge_c, ef.data(), sizeof(float) * ef.size(), cudaMemcpyHostToDevice, h->stream), "copy edge");
+    }
+    // populations
+    if (!h->d_stage) CK(cudaMalloc(&h->d_stage, sizeof(double) * nn * 9), "alloc stage");
+    for (size_t q = 0; q < nn * 9; ++q) g[q] += kWref[q / nn];   // back to f for the pack kernel
+    CK(cudaMemcpyAsync(h->d_stage, g.data(), sizeof(double) * nn * 9, cudaMemcpyHostToDevice, h->stream), "copy f");
+    if (launch_pack(h, h->d_stage, h->fbuf[0])) return cuda_err(h, cudaGetLastError(), "pack");
+    h->cur = 0;
+    // initial fields (rho = 1, u, v) in slot 0: u0 of the first step
+    {
+        std::vector<double> fl(3 * nn);
+        for (size_t q = 0; q < nn; ++q) { fl[q] = 1.0; fl[nn + q] = fu[q]; fl[2 * nn + q] = fv[q]; }
+        if (cs == sizeof(double)) {
+            CK(cudaMemcpyAsync(h->d_fields[0], fl.data(), sizeof(double) * 3 * nn, cudaMemcpyHostToDevice, h->stream), "copy fields");
+        } else {
+            std::vector<float> ff(fl.begin(), fl.end());
+            CK(cudaMemcpyAsync(h->d_fields[0], ff.data(), sizeof(float) * 3 * nn, cudaMemcpyHostToDevice, h->stream), "copy fields");
+            CK(cudaStreamSynchronize(h->stream), "sync fields");
+        }
+    }
+    h->fields_slot = 0;
+    h->fields_step[0] = 0;
+    h->fields_step[1] = -1;
+    CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream), "clear status");
+    CK(cudaMemsetAsync(h->d_pinfo, 0, sizeof(PatchInfo), h->stream), "clear pinfo");
+    CK(cudaStreamSynchronize(h->stream), "sync init");
+    h->n = 1;
+    h->steps_done = 0;
+    h->inited = 1;
+    return LBM_OK;
+}
+
+int lbm_step(lbm_t *h, double *force_row)
+{
+    if (!h) return LBM_ERR_ARG;
+    return run_steps(h, 1, force_row, nullptr, true);
+}
+
+int lbm_run(lbm_t *h, int nsteps, double *force_rows, int *done_steps)
+{
+    if (!h) return LBM_ERR_ARG;
+    if (done_steps) *done_steps = 0;
+    if (nsteps < 0) return set_err(h, LBM_ERR_ARG, "run: negative step count");
+    if (nsteps == 0) return LBM_OK;
+    return run_steps(h, nsteps, force_rows, done_steps, false);
+}
+
+int lbm_force_row_length(const lbm_t *h) { return h ? h->row_len : LBM_ERR_ARG; }
+
+int lbm_get_fields(lbm_t *h, double *rho, double *u, double *v)
+{
+    if (!h) return LBM_ERR_ARG;
+    if (!h->inited) return set_err(h, LBM_ERR_STATE, "get_fields: not initialised");
+    const int slot = h->fields_slot;
+    if (h->fields_step[slot] != h->steps_done)
+        return set_err(h, LBM_ERR_STATE, "get_fields: the last step did not keep its fields");
+    const size_t nn = (size_t)h->nx * h->ny;
+    double *dst[3] = {rho, u, v};
+    if (h->prec == LBM_PREC_FP64) {
+        for (int c = 0; c < 3; ++c)
+            if (dst[c])
+                CK(cudaMemcpyAsync(dst[c], (const double *)h->d_fields[slot] + c * nn, sizeof(double) * nn,
+                                   cudaMemcpyDeviceToHost, h->stream), "copy fields");
+        CK(cudaStreamSynchronize(h->stream), "sync fields");
+    } else {
+        std::vector<float> tmp(nn);
+        for (int c = 0; c < 3; ++c) {
+            if (!dst[c]) continue;
+            CK(cudaMemcpyAsync(tmp.data(), (const float *)h->d_fields[slot] + c * nn, sizeof(float) * nn,
+                               cudaMemcpyDeviceToHost, h->stream), "copy fields");
+            CK(cudaStreamSynchronize(h->stream), "sync fields");
+            for (size_t q = 0; q < nn; ++q) dst[c][q] = tmp[q];
+        }
+    }
+    return LBM_OK;
+}
+
+int lbm_get_populations(lbm_t *h, double *f)
+{
+    if (!h || !f) return LBM_ERR_ARG;
+    if (!h->inited) return set_err(h, LBM_ERR_STATE, "get_populations: not initialised");
+    const size_t nn = (size_t)h->nx * h->ny;
+    if (!h->d_stage) CK(cudaMalloc(&h->d_stage, sizeof(double) * nn * 9), "alloc stage");
+    if (launch_unpack(h, h->fbuf[h->cur], h->d_stage)) return cuda_err(h, cudaGetLastError(), "unpack");
+    CK(cudaMemcpyAsync(f, h->d_stage, sizeof(double) * nn * 9, cudaMemcpyDeviceToHost, h->stream), "copy f");
+    CK(cudaStreamSynchronize(h->stream), "sync f");
+    return LBM_OK;
+}
+
+int lbm_set_populations(lbm_t *h, const double *f)
+{
+    if (!h || !f) return LBM_ERR_ARG;
+    if (!h->inited) return set_err(h, LBM_ERR_STATE, "set_populations: not initialised");
+    const size_t nn = (size_t)h->nx * h->ny;
+    if (!h->d_stage) CK(cudaMalloc(&h->d_stage, sizeof(double) * nn * 9), "alloc stage");
+    CK(cudaMemcpyAsync(h->d_stage, f, sizeof(double) * nn * 9, cudaMemcpyHostToDevice, h->stream), "copy f");
+    if (launch_pack(h, h->d_stage, h->fbuf[h->cur])) return cuda_err(h, cudaGetLastError(), "pack");
+    CK(cudaStreamSynchronize(h->stream), "sync f");
+    h->fields_step[0] = h->fields_step[1] = -1;
+    return LBM_OK;
+}
+
+int lbm_residual(lbm_t *h, double *err)
+{
+    if (!h || !err) return LBM_ERR_ARG;
+    const int a = h->fields_slot, b = a ^ 1;
+    if (h->steps_done < 1 || h->fields_step[a] != h->steps_done || h->fields_step[b] != h->steps_done - 1)
+        return set_err(h, LBM_ERR_STATE, "residual: fields of the last two states were not kept");
+    double s[2];
+    if (launch_residual(h, h->d_fields[a], h->d_fields[b], s)) return cuda_err(h, cudaGetLastError(), "residual");
+    *err = sqrt(s[0]) / (sqrt(s[1]) + 1e-30);   // solution.f90:120-122
+    return LBM_OK;
+}
+
+int lbm_get_markers(lbm_t *h, double *xb2, double *yb2, double *solve_residual)
+{
+    if (!h) return LBM_ERR_ARG;
+    if (!h->ib_ready || h->nseg == 0) return set_err(h, LBM_ERR_STATE, "get_markers: no immersed boundary step run");
+    std::vector<Marker> mk(h->nseg);
+    CK(cudaMemcpyAsync(mk.data(), h->d_mk, sizeof(Marker) * h->nseg, cudaMemcpyDeviceToHost, h->stream), "copy markers");
+    double res = 0;
+    CK(cudaMemcpyAsync(&res, h->d_solve_res, sizeof(double), cudaMemcpyDeviceToHost, h->stream), "copy res");
+    CK(cudaStreamSynchronize(h->stream), "sync markers");
+    for (int k = 0; k < h->nseg; ++k) {
+        if (xb2) xb2[k] = mk[k].xm;
+        if (yb2) yb2[k] = mk[k].ym;
+    }
+    if (solve_residual) *solve_residual = res;
+    return LBM_OK;
+}
+
+int lbm_set_timing(lbm_t *h, int enable)
+{
+    if (!h) return LBM_ERR_ARG;
+    if (enable && h->ev.empty()) {
+        h->ev.resize(3 * (size_t)h->ring_cap);
+        for (auto &e : h->ev) CK(cudaEventCreate(&e), "event create");
+    }
+    h->timing = enable ? 1 : 0;
+    h->t_step = h->t_ib = h->t_kf = 0;
+    h->t_steps = 0;
+    return LBM_OK;
+}
+
+int lbm_get_timing(lbm_t *h, double *step_ms, double *ib_ms, double *lattice_ms, int *steps)
+{
+    if (!h) return LBM_ERR_ARG;
+    if (step_ms) *step_ms = h->t_step;
+    if (ib_ms) *ib_ms = h->t_ib;
+    if (lattice_ms) *lattice_ms = h->t_kf;
+    if (steps) *steps = h->t_steps;
+    return LBM_OK;
+}
+
+int lbm_step_index(const lbm_t *h) { return h ? h->n : LBM_ERR_ARG; }
+
+const char *lbm_last_error(const lbm_t *h) { return h ? h->err.c_str() : "lbm_create failed (bad parameters or no CUDA device)"; }
+
+}  // extern "C"

@@ -1,0 +1,131 @@
+// lbm_internal.h -- handle layout and kernel launchers (not part of the ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include <vector>
+
+#include "../../include/lbm_b200.h"
+#include "lbm_common.cuh"
+
+// constants of the left/right columns that never change after init: the
+// moments of the edge f0 that streaming never rewrites (solution.f90:440-447,
+// 516-520), and the edge f0 populations the top/bottom extrapolation reads at
+// the corner columns (boundary_condition.f90:705, 832).
+struct EdgeConst {
+    double *col_l;   // [3*ny]: drho, u, v of column 1 (1-based)
+    double *col_r;   // [3*ny]: column Nx
+    double *corner;  // [4*9] deviation f0 at (1,2), (1,Ny-1), (Nx,2), (Nx,Ny-1)
+};
+
+// arguments of the fused stream+collide+boundary kernel
+template <typename C>
+struct KFArgs {
+    const void *fin;
+    void *fout;
+    int nx, ny, pitch;
+    long long plane;
+    C s[9];
+    C cs;
+    const C *col_l, *col_r, *corner;   // edge constants in compute precision
+    const PatchInfo *pinfo;
+    const C *patch;                    // interleaved (du, dv) per patch node
+    C *rho_out, *u_out, *v_out;        // fields, when requested (else null)
+};
+
+// arguments of the immersed-boundary kernels
+struct IBArgs {
+    const void *fin;    // populations the step streams from
+    int prec;           // LBM_PREC_*
+    int nx, ny, pitch;
+    long long plane;
+    int nwing, ppw, spw, nseg;
+    int smooth;
+    double scale, ox, oy, uu, xc, yc, mesh_max_scale;
+    const double *xb0, *yb0, *arc;
+    const double *mstep;  // step table, row-major [msteps][mcols]
+    int msteps, mcols;
+    double mdt;
+    Marker *mk;
+    double *rhs;        // [2*nseg]
+    double *B;          // [nseg*nseg], row-major
+    double *y;          // [2*nseg]
+    PatchInfo *pinfo;
+    void *patch;        // compute-precision (du, dv) pairs
+    int patch_cap;      // nodes
+    int patch_wmax, patch_hmax;  // rectangle the spread grid covers
+    double *partial;    // per-block force partials
+    unsigned *counter;  // last-block counter
+    double *force_ring; // [ring_cap][row_len]
+    int row_len;
+    unsigned *status;
+    double *solve_res;  // relative residual of the last solve
+};
+
+struct lbm_handle {
+    lbm_params p;
+    int nx = 0, ny = 0, pitch = 0;
+    long long plane = 0;
+    int nwing = 0, ppw = 0, spw = 0, npts = 0, nseg = 0;
+    double niu = 0, tau = 0, s[9] = {0};
+    int prec = 0;
+    size_t elem = 4;
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    void *fbuf[2] = {nullptr, nullptr};
+    int cur = 0;
+    // edge constants (FP64 master + compute-precision copy)
+    EdgeConst edge{};
+    void *edge_c = nullptr;  // compute precision: col_l, col_r, corner packed
+    // geometry and motion
+    std::vector<double> hx0, hy0, harc;
+    std::vector<int> have_wing;
+    double *d_xb0 = nullptr, *d_yb0 = nullptr, *d_arc = nullptr;
+    std::vector<double> mtab;  // column-major rows x cols, as given
+    int mrows = 0, mcols = 0;
+    double mend = 0, mdt = 0;
+    int msteps = 0;
+    std::vector<double> mstep_host;  // step table, row-major [msteps][mcols]
+    double *d_mstep = nullptr;
+    // immersed boundary scratch
+    Marker *d_mk = nullptr;
+    double *d_rhs = nullptr, *d_B = nullptr, *d_y = nullptr;
+    PatchInfo *d_pinfo = nullptr;
+    void *d_patch = nullptr;
+    int patch_cap = 0;               // nodes
+    int patch_wmax = 0, patch_hmax = 0;
+    int patch_gx() const { return patch_wmax > 0 ? (patch_wmax + 15) / 16 : 1; }
+    int patch_gy() const { return patch_hmax > 0 ? (patch_hmax + 15) / 16 : 1; }
+    int ib_ready = 0;
+    double *d_partial = nullptr;
+    unsigned *d_counter = nullptr;
+    double *d_ring = nullptr;
+    int ring_cap = 0;
+    int row_len = 0;
+    unsigned *d_status = nullptr;
+    double *d_solve_res = nullptr;
+    // fields of the last field-writing steps (compute precision), two slots
+    void *d_fields[2] = {nullptr, nullptr};
+    int fields_slot = 0;           // slot written by the last field step
+    int fields_step[2] = {-1, -1}; // step index written into each slot
+    double *d_red = nullptr;       // residual reduction scratch
+    double *d_stage = nullptr;     // FP64 (nx,ny,9) staging for get/set of populations
+    // device timing (lbm_set_timing): three events per step slot of the ring
+    int timing = 0;
+    std::vector<cudaEvent_t> ev;
+    double t_step = 0, t_ib = 0, t_kf = 0;
+    int t_steps = 0;
+    // driver state
+    int n = 1;
+    int inited = 0;
+    int steps_done = 0;
+    std::string err;
+};
+
+// kernel launchers (kf_kernel.cu, ib_kernels.cu)
+int ib_configure(lbm_handle *h);
+int launch_kf(lbm_handle *h, const void *fin, void *fout, void *fields);
+int launch_ib(lbm_handle *h, const void *fin, int step_index, int ring_slot);
+int launch_residual(lbm_handle *h, const void *fa, const void *fb, double *out2);
+int launch_unpack(lbm_handle *h, const void *fsrc, double *dst);   // deviation -> f (FP64)
+int launch_pack(lbm_handle *h, const double *src, void *fdst);     // f (FP64) -> deviation
+int launch_fields_to_double(lbm_handle *h, const void *fields, double *rho, double *u, double *v);

@@ -1,0 +1,134 @@
+"""Python host side of the B200 time step, mirroring the reference's
+subroutine interface (ini_mesh, read_boundary, load_motion_table, init,
+evolution, erranalysis, output/saveflowfield) over the C ABI of
+include/lbm_b200.h. All compute runs in liblbmb200.so; this module only moves
+host arrays across the boundary."""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import _abi
+from ._abi import dptr
+
+
+class LbmError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{_abi.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class Lbm:
+    """One case on the GPU (lbm_create ... lbm_destroy)."""
+
+    def __init__(self, params, lib=None):
+        self.lib = lib or _abi.load_library()
+        self.params = params
+        h = C.c_void_p()
+        rc = self.lib.lbm_create(C.byref(params), C.byref(h))
+        if rc != 0:
+            raise LbmError(rc, self.lib.lbm_last_error(None).decode())
+        self.h = h
+        self.nx, self.ny = params.nx, params.ny
+        self.row_len = self.lib.lbm_force_row_length(self.h)
+
+    # -- error handling --------------------------------------------------
+    def _ck(self, rc, ok=(0,)):
+        if rc not in ok:
+            raise LbmError(rc, self.lib.lbm_last_error(self.h).decode())
+        return rc
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.lbm_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- set-up (ini_mesh / read_boundary / load_motion_table / init) ----
+    def set_boundary(self, wing, x, y):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.ascontiguousarray(y, dtype=np.float64)
+        self._ck(self.lib.lbm_set_boundary(self.h, wing, dptr(x), dptr(y), len(x)))
+
+    def read_boundary(self, directory=""):
+        self._ck(self.lib.lbm_read_boundary(self.h, os.fsencode(directory)))
+
+    def set_motion_table(self, table):
+        t = np.asfortranarray(table, dtype=np.float64)
+        rows, cols = t.shape
+        flat = np.ascontiguousarray(t.reshape(-1, order="F"))
+        self._ck(self.lib.lbm_set_motion_table(self.h, dptr(flat), rows, cols))
+
+    def load_motion_table(self, path="motion_params.dat"):
+        self._ck(self.lib.lbm_load_motion_table(self.h, os.fsencode(path)))
+
+    def init(self, du=None, dv=None):
+        du = None if du is None else np.ascontiguousarray(du, dtype=np.float64)
+        dv = None if dv is None else np.ascontiguousarray(dv, dtype=np.float64)
+        self._ck(self.lib.lbm_init(self.h, dptr(du), dptr(dv)))
+
+    @classmethod
+    def from_case(cls, case, lib=None):
+        s = cls(case.params, lib)
+        for w, (x, y) in enumerate(case.contours, start=1):
+            s.set_boundary(w, x, y)
+        s.set_motion_table(case.table)
+        s.init(case.du, case.dv)
+        return s
+
+    # -- the time step (evolution) ----------------------------------------
+    def evolution(self):
+        """One step; returns its force.dat row, or None past motion_end_time."""
+        row = np.zeros(self.row_len)
+        rc = self._ck(self.lib.lbm_step(self.h, dptr(row)), ok=(0, 1))
+        return None if rc == 1 else row
+
+    def run(self, nsteps, keep_rows=True):
+        rows = np.zeros((max(nsteps, 1), self.row_len)) if keep_rows else None
+        done = C.c_int(0)
+        self._ck(self.lib.lbm_run(self.h, nsteps, dptr(rows), C.byref(done)), ok=(0, 1))
+        return rows[: done.value] if keep_rows else done.value
+
+    # -- observation --------------------------------------------------------
+    def fields(self):
+        """(rho, u, v) as (ny, nx) arrays (row j, column i)."""
+        n = self.nx * self.ny
+        rho, u, v = np.zeros(n), np.zeros(n), np.zeros(n)
+        self._ck(self.lib.lbm_get_fields(self.h, dptr(rho), dptr(u), dptr(v)))
+        return tuple(a.reshape(self.ny, self.nx) for a in (rho, u, v))
+
+    def populations(self):
+        """f as (9, ny, nx)."""
+        f = np.zeros(9 * self.nx * self.ny)
+        self._ck(self.lib.lbm_get_populations(self.h, dptr(f)))
+        return f.reshape(9, self.ny, self.nx)
+
+    def set_populations(self, f):
+        f = np.ascontiguousarray(f, dtype=np.float64).reshape(-1)
+        self._ck(self.lib.lbm_set_populations(self.h, dptr(f)))
+
+    def erranalysis(self):
+        e = C.c_double()
+        self._ck(self.lib.lbm_residual(self.h, C.byref(e)))
+        return e.value
+
+    def markers(self):
+        n = self.params.wing_count * (self.params.points_per_wing - 1)
+        x, y, r = np.zeros(n), np.zeros(n), C.c_double()
+        self._ck(self.lib.lbm_get_markers(self.h, dptr(x), dptr(y), C.byref(r)))
+        return x, y, r.value
+
+    @property
+    def step_index(self):
+        return self.lib.lbm_step_index(self.h)

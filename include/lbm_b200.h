@@ -1,0 +1,202 @@
+/*
+ * lbm_b200.h -- C ABI of the B200 time step of the D2Q9 MRT lattice-Boltzmann
+ * flapping-airfoil solver (immersed boundary, implicit velocity correction).
+ *
+ * Every entry point replaces one Fortran subroutine (or one block of the
+ * driver loop) of the reference R-IFFERY/Fortran_loadFile_mitiwing; the
+ * citation next to each declaration names it (file:line in that project).
+ *
+ * Conventions
+ *   - Every function returns an int status (LBM_OK == 0). No exception or
+ *     longjmp crosses this boundary. lbm_last_error() gives the message of the
+ *     last failing call on a handle.
+ *   - Host arrays are Fortran order, x fastest, 1-based node (i,j) at
+ *     index (i-1) + (j-1)*nx; populations (nx,ny,9) add (k-1)*nx*ny. Motion
+ *     tables are (rows, cols) column-major, exactly as the Fortran driver
+ *     holds motion_table(count, motion_column_count).
+ *   - A handle owns all of its device memory and one CUDA stream. Host
+ *     pointers are borrowed for the duration of a call only. Calls on one
+ *     handle must be serialised by the caller; different handles may be
+ *     driven from different host threads.
+ *   - Device pointers never cross this ABI.
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define LBM_API __attribute__((visibility("default")))
+#else
+#define LBM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_ABI_VERSION 1
+
+/* status codes */
+#define LBM_OK               0
+#define LBM_DONE             1   /* time passed motion_end_time (main.f90:352-353) */
+#define LBM_ERR_ARG         -1   /* bad argument / size */
+#define LBM_ERR_CUDA        -2   /* CUDA runtime error, or no usable device */
+#define LBM_ERR_STATE       -3   /* call out of order (e.g. step before init) */
+#define LBM_ERR_IO          -4   /* file missing or malformed (mode.f90:82-135, airfoil.f90:224-234) */
+#define LBM_ERR_SOLVER      -5   /* immersed-boundary system not positive definite / singular */
+#define LBM_ERR_NONFINITE   -6   /* NaN/Inf seen in forces or in the mass check */
+#define LBM_ERR_RANGE       -7   /* a marker's support box reaches the three outermost node layers */
+
+/* storage precision of the populations (all collision arithmetic is FP32,
+ * or FP64 for LBM_PREC_FP64; immersed-boundary solve and force sums are FP64) */
+#define LBM_PREC_FP32  0
+#define LBM_PREC_FP64  1
+#define LBM_PREC_FP16  2
+#define LBM_PREC_BF16  3
+
+/* discrete delta kernel (boundary_condition.f90:1530, 1563-1600) */
+#define LBM_DELTA_PESKIN4  0   /* smooth=0: 4-point Peskin, support |r|<2   */
+#define LBM_DELTA_SMOOTH   1   /* smooth=1: smoothed kernel, support |r|<=2.5 */
+
+/* Run parameters. In the reference these are compile-time PARAMETERs of
+ * module com_date (main.f90:4-137) and values set by ini_mesh
+ * (ini_mesh.f90:15-67); here they are runtime values. */
+typedef struct lbm_params {
+    int32_t nx, ny;            /* mesh%Nx, mesh%Ny (ini_mesh.f90:22-23) */
+    int32_t wing_count;        /* wing_count (main.f90:18) */
+    int32_t points_per_wing;   /* boundary_points_per_wing (main.f90:21); closed contour */
+    int32_t delta_kernel;      /* LBM_DELTA_*; the reference hard-codes smooth=1 */
+    int32_t precision;         /* LBM_PREC_* */
+    int32_t flags;             /* reserved, must be 0 */
+    int32_t reserved;
+    double scale;              /* mesh%scale: lattice spacing in chords (1/chord_lu) */
+    double ox, oy;             /* mesh%ox, mesh%oy: physical position of node (1,1) */
+    double uu;                 /* UU: lattice free-stream speed (main.f90:12) */
+    double re;                 /* Re (main.f90:84); nu = uu/scale/re, tau = 3 nu + 0.5 */
+    double s[9];               /* MRT rates mesh%s (ini_mesh.f90:59-67);
+                                  s[7] or s[8] <= 0 means 1/tau_f */
+    double xc, yc;             /* body reference point xc, yc (main.f90:85) */
+    double xp, yp;             /* pivot xp, yp (main.f90:86) */
+    double mesh_max_scale;     /* mesh_max_scale (main.f90:32), only scales movenum */
+} lbm_params;
+
+typedef struct lbm_handle lbm_t;
+
+/* ---- set-up ------------------------------------------------------------ */
+
+/* Fills p with the reference's own PARAMETER values (main.f90:7-137,
+ * ini_mesh.f90:15-67): 4001x2001, scale 0.01, UU 0.01, Re 500, two wings of
+ * 205 points, s=(0,1.1,1.05,0,1.2,0,1.2,1/tau,1/tau), smooth=1, FP32 storage. */
+LBM_API int lbm_default_params(lbm_params *p);
+
+/* ini_mesh (ini_mesh.f90:1-81): validates the parameters and allocates the
+ * device state (two population buffers, IB scratch, step table). */
+LBM_API int lbm_create(const lbm_params *p, lbm_t **out);
+
+/* frees everything the handle owns (the reference frees nothing) */
+LBM_API int lbm_destroy(lbm_t *h);
+
+/* read_boundary (airfoil.f90:207-242) for one wing from memory: npts
+ * (= points_per_wing) points of a closed contour in chords, body frame.
+ * Computes arc_l = |segment| / scale and applies the (xc-xp, yc-yp) shift
+ * (airfoil.f90:235-241). wing is 1-based. */
+LBM_API int lbm_set_boundary(lbm_t *h, int wing, const double *x, const double *y, int npts);
+
+/* read_boundary from files: boundary.dat for wing 1 and boundary<w-1>.dat for
+ * wing w (airfoil.f90:191-205), format (2f14.8), in directory dir ("" = cwd). */
+LBM_API int lbm_read_boundary(lbm_t *h, const char *dir);
+
+/* load_motion_table + build_motion_step_table(scale*UU) (mode.f90:68-142,
+ * 245-269) from memory: table is (rows, cols) column-major with
+ * cols = 1 + 9*wing_count (time, then per wing angle, omega, omgac, sa, sau,
+ * saac, sb, sbv, sbac). Rejects an empty table and a decreasing time column. */
+LBM_API int lbm_set_motion_table(lbm_t *h, const double *table, int rows, int cols);
+
+/* load_motion_table from a motion_params.dat file (mode.f90:68-142). */
+LBM_API int lbm_load_motion_table(lbm_t *h, const char *path);
+
+/* Host-only parsers behind lbm_read_boundary / lbm_load_motion_table; they
+ * need no device. The boundary parser reads npts (2f14.8) records of one file
+ * (airfoil.f90:229). The motion parser reads the non-blank rows of a
+ * list-directed motion_params.dat (mode.f90:88-123) into table (column-major,
+ * max_rows x cols); *rows receives the row count (also when table is NULL,
+ * which only counts). */
+LBM_API int lbm_parse_boundary_file(const char *path, int npts, double *x, double *y);
+LBM_API int lbm_parse_motion_file(const char *path, int cols, double *table, int max_rows, int *rows);
+
+/* init (solution.f90:1-72) plus the driver's state reset (main.f90:294-328):
+ * rho=1, u=UU, v=0, f=f0=feq with single-precision lattice weights.
+ * du, dv (nx*ny each, nullable) are added to u and v before feq is taken;
+ * they carry a seeded initial perturbation, which the reference does not
+ * have (zero arrays reproduce it exactly). */
+LBM_API int lbm_init(lbm_t *h, const double *du, const double *dv);
+
+/* ---- the time step ---------------------------------------------------- */
+
+/* One pass of the driver loop body (main.f90:352-359): time=(n-1)*scale*UU,
+ * stop if time > motion_end_time+1e-12 (returns LBM_DONE), else
+ * evolution (solution.f90:269-410): mode, move_boundary, streaming,
+ * physical_variables, immersed_boundary_Wu, colission, force normalisation,
+ * boundary_condition1. force_row (nullable, lbm_force_row_length doubles)
+ * receives the force.dat row of this step (solution.f90:349-377). */
+LBM_API int lbm_step(lbm_t *h, double *force_row);
+
+/* nsteps passes of lbm_step, enqueued back to back on the device with no host
+ * synchronisation in between (the main.f90:351-418 loop without output).
+ * force_rows (nullable) receives nsteps rows, row-major, row length
+ * lbm_force_row_length. *done_steps (nullable) = steps actually run; the run
+ * stops early with LBM_DONE at motion_end_time. */
+LBM_API int lbm_run(lbm_t *h, int nsteps, double *force_rows, int *done_steps);
+
+/* length of one force.dat row: 1 + 3*wing_count + 3 + 9*wing_count
+ * (solution.f90:350-375) */
+LBM_API int lbm_force_row_length(const lbm_t *h);
+
+/* ---- observation / checkpoint ---------------------------------------- */
+
+/* the !$acc update host of rho, u, v (main.f90:408) as FP64 (nx,ny) arrays,
+ * values after the boundary condition of the last step. Any pointer may be
+ * NULL. */
+LBM_API int lbm_get_fields(lbm_t *h, double *rho, double *u, double *v);
+
+/* populations f(nx,ny,9) as FP64, after the last step (mesh%f). */
+LBM_API int lbm_get_populations(lbm_t *h, double *f);
+
+/* restores f(nx,ny,9) (readflowfield, solution.f90:1709-1839, the f part);
+ * the edge f0 copies are kept from lbm_init. */
+LBM_API int lbm_set_populations(lbm_t *h, const double *f);
+
+/* erranalysis (solution.f90:74-127): ||u-u0|| / (||u|| + 1e-30) over the
+ * interior, u from the last step and u0 from the state before it (the
+ * initial field after one step). Needs one step run since init (else
+ * LBM_ERR_STATE). */
+LBM_API int lbm_residual(lbm_t *h, double *err);
+
+/* immersed-boundary diagnostics of the last step: marker midpoints xb2,yb2
+ * (n = wing_count*(points_per_wing-1) each, nullable) and the relative
+ * residual ||A x - rhs|| / ||rhs|| of the solve (nullable). */
+LBM_API int lbm_get_markers(lbm_t *h, double *xb2, double *yb2, double *solve_residual);
+
+/* Device timing of the step loop, the CUDA-event analogue of the driver's
+ * per-phase cpu_time totals (main.f90:355-369, 420-433). With timing on,
+ * lbm_step/lbm_run record CUDA events on the handle's stream around the
+ * immersed-boundary kernels and around the lattice kernel of every step.
+ * lbm_get_timing returns, since the last lbm_set_timing, the summed device
+ * milliseconds of the whole steps, of the immersed-boundary kernels and of
+ * the lattice kernel, and the number of steps timed (any pointer nullable). */
+LBM_API int lbm_set_timing(lbm_t *h, int enable);
+LBM_API int lbm_get_timing(lbm_t *h, double *step_ms, double *ib_ms, double *lattice_ms, int *steps);
+
+/* current step counter n of the driver loop (1 before the first step). */
+LBM_API int lbm_step_index(const lbm_t *h);
+
+/* message of the last failing call on h ("" if none); h may be NULL for
+ * errors of lbm_create. The string stays valid until the next call on h. */
+LBM_API const char *lbm_last_error(const lbm_t *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LBM_B200_H */

@@ -1,0 +1,159 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Tolerances:
+  FP64 storage: max |f_gpu - f_oracle| <= 1e-11 (f ~ 0.03..0.44), fields
+    likewise, force coefficients within 1e-8 relative (summation order only).
+  FP32 storage, 400x200 plunge case, first 1000 steps (the low-Re parity
+    window): populations, velocity field and per-step C_D/C_L within 1e-5
+    relative; populations as max|df|/max|f|, velocity as ||du||/||u||, forces
+    per step against max(|C|, rms C over the window) so that zero crossings of
+    C_L are not divided by ~0.
+"""
+import numpy as np
+import pytest
+
+from fortran_loadfile_mitiwing_b200 import Lbm, LbmError, cases, io_formats
+from fortran_loadfile_mitiwing_b200 import _abi
+
+pytestmark = pytest.mark.gpu
+
+
+def run_both(case, nsteps, gpu_lib, oracle_mod, use_run=False):
+    g = Lbm.from_case(case, gpu_lib)
+    o = oracle_mod.Oracle.from_case(case)
+    if use_run:
+        rg = g.run(nsteps)
+    else:
+        rg = np.array([g.evolution() for _ in range(nsteps)])
+    ro = o.run(nsteps)
+    return g, o, rg, ro
+
+
+def rel_series(a, b):
+    floor = np.sqrt(np.mean(b * b, axis=0, keepdims=True))
+    return np.max(np.abs(a - b) / np.maximum(np.abs(b), floor))
+
+
+def test_fp64_parity_small_case(gpu_lib, oracle_mod):
+    case = cases.small_case(precision="fp64", n_steps=200, pitch_deg=10.0)
+    g, o, rg, ro = run_both(case, 100, gpu_lib, oracle_mod)
+    assert np.abs(g.populations() - o.populations()).max() < 1e-11
+    for a, b in zip(g.fields(), o.fields()):
+        assert np.abs(a - b).max() < 1e-11
+    np.testing.assert_array_equal(rg[:, 0], ro[:, 0])          # time column
+    np.testing.assert_array_equal(rg[:, 7:], ro[:, 7:])        # motion columns
+    assert rel_series(rg[:, 1:7], ro[:, 1:7]) < 1e-8
+    xg, yg, res = g.markers()
+    xo, yo, _ = o.markers()
+    np.testing.assert_array_equal(xg, xo)
+    np.testing.assert_array_equal(yg, yo)
+
+
+def test_fp64_parity_two_wings_smooth_kernel(gpu_lib, oracle_mod):
+    case = cases.small_case(nx=128, wings=2, delta=_abi.LBM_DELTA_SMOOTH, precision="fp64", n_steps=60)
+    g, o, rg, ro = run_both(case, 40, gpu_lib, oracle_mod, use_run=True)
+    assert np.abs(g.populations() - o.populations()).max() < 1e-11
+    assert rel_series(rg[:, 1:10], ro[:, 1:10]) < 1e-8
+
+
+def test_fp64_parity_without_body(gpu_lib, oracle_mod):
+    case = cases.small_case(wings=0, precision="fp64", n_steps=40)
+    g, o, rg, ro = run_both(case, 30, gpu_lib, oracle_mod)
+    assert np.abs(g.populations() - o.populations()).max() < 1e-12
+    for a, b in zip(g.fields(), o.fields()):
+        assert np.abs(a - b).max() < 1e-12
+
+
+def test_fp32_parity_plunge_400x200_first_1000_steps(gpu_lib, oracle_mod):
+    case = cases.plunge_case(precision="fp32", n_steps=4000)
+    g, o, rg, ro = run_both(case, 1000, gpu_lib, oracle_mod, use_run=True)
+    fg, fo = g.populations(), o.populations()
+    assert np.abs(fg - fo).max() / np.abs(fo).max() < 1e-5
+    _, ug, vg = g.fields()
+    _, uo, vo = o.fields()
+    vel = np.sqrt(np.sum((ug - uo) ** 2 + (vg - vo) ** 2) / np.sum(uo ** 2 + vo ** 2))
+    assert vel < 1e-5
+    assert rel_series(rg[:, 1:3], ro[:, 1:3]) < 1e-5
+
+
+def test_step_and_run_agree_bitwise(gpu_lib):
+    case = cases.small_case(precision="fp32", n_steps=100)
+    a = Lbm.from_case(case, gpu_lib)
+    b = Lbm.from_case(case, gpu_lib)
+    ra = np.array([a.evolution() for _ in range(25)])
+    rb = b.run(25)
+    np.testing.assert_array_equal(a.populations(), b.populations())
+    np.testing.assert_array_equal(ra, rb)
+
+
+def test_residual_matches_oracle(gpu_lib, oracle_mod):
+    case = cases.small_case(precision="fp64", n_steps=100)
+    g = Lbm.from_case(case, gpu_lib)
+    o = oracle_mod.Oracle.from_case(case)
+    g.evolution()
+    o.evolution()
+    assert abs(g.erranalysis() - o.erranalysis()) < 1e-10
+    g.run(10)
+    o.run(10)
+    assert abs(g.erranalysis() - o.erranalysis()) < 1e-10 * max(1.0, o.erranalysis())
+
+
+def test_range_error_is_reported(gpu_lib):
+    case = cases.small_case(pivot=(8, 33), precision="fp32")
+    g = Lbm.from_case(case, gpu_lib)
+    with pytest.raises(LbmError) as ei:
+        g.evolution()
+    assert ei.value.status == _abi.LBM_ERR_RANGE
+
+
+def test_run_stops_at_motion_end(gpu_lib):
+    case = cases.small_case(n_steps=7)
+    g = Lbm.from_case(case, gpu_lib)
+    rows = g.run(20)
+    assert rows.shape[0] == 7
+    assert g.evolution() is None
+    assert g.step_index == 8
+
+
+def test_step_before_init_is_refused(gpu_lib):
+    case = cases.small_case()
+    g = Lbm(case.params, gpu_lib)
+    with pytest.raises(LbmError) as ei:
+        g.evolution()
+    assert ei.value.status == _abi.LBM_ERR_STATE
+
+
+def test_file_inputs_match_memory_inputs(gpu_lib, tmp_path):
+    case = cases.small_case(precision="fp64", n_steps=30)
+    io_formats.write_boundary(tmp_path / "boundary.dat", *case.contours[0])
+    io_formats.write_motion(tmp_path / "motion_params.dat", case.table)
+    a = Lbm.from_case(case, gpu_lib)
+    b = Lbm(case.params, gpu_lib)
+    b.read_boundary(str(tmp_path))
+    b.load_motion_table(str(tmp_path / "motion_params.dat"))
+    b.init(case.du, case.dv)
+    ra, rb = a.run(20), b.run(20)
+    np.testing.assert_array_equal(ra, rb)
+    np.testing.assert_array_equal(a.populations(), b.populations())
+
+
+def test_populations_round_trip(gpu_lib):
+    case = cases.small_case(precision="fp64", n_steps=30)
+    g = Lbm.from_case(case, gpu_lib)
+    g.run(5)
+    f = g.populations()
+    g.set_populations(f)
+    np.testing.assert_array_equal(g.populations(), f)
+
+
+def test_checkpoint_restart_continues_identically(gpu_lib):
+    case = cases.small_case(precision="fp32", n_steps=60)
+    a = Lbm.from_case(case, gpu_lib)
+    a.run(20)
+    f = a.populations()
+    ra = a.run(10)
+    b = Lbm.from_case(case, gpu_lib)
+    b.run(20)
+    b.set_populations(f)
+    rb = b.run(10)
+    np.testing.assert_array_equal(ra, rb)

@@ -1,0 +1,224 @@
+"""Property tests that pin the CPU oracle (no GPU). The reference ships no
+tests or golden vectors, so these properties are what the oracle is checked
+against before it checks the CUDA path."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from fortran_loadfile_mitiwing_b200 import cases
+
+
+def test_mrt_matrix_inverse(oracle_mod):
+    m, mi = oracle_mod.mrt_matrices()
+    assert np.abs(m @ mi - np.eye(9)).max() < 1e-15
+    # rows of M are orthogonal: M^-1 = M^T diag(1/|row|^2)
+    exact = m.T / (m * m).sum(axis=1)
+    assert np.abs(mi - exact).max() < 1e-16
+
+
+def test_lattice_order_and_single_precision_weights(oracle_mod):
+    e, w = oracle_mod.lattice()
+    assert e.tolist() == [[0, 0], [1, 0], [0, 1], [-1, 0], [0, -1], [1, 1], [-1, 1], [-1, -1], [1, -1]]
+    assert w[0] == float(np.float32(4.0) / np.float32(9.0))
+    assert w[1] == float(np.float32(1.0) / np.float32(9.0))
+    assert w[5] == float(np.float32(1.0) / np.float32(36.0))
+    assert w[0] != 4.0 / 9.0   # the REAL*4 quotient, not the FP64 one
+
+
+@pytest.mark.parametrize("smooth,support", [(0, 2.0), (1, 2.5)])
+def test_delta_kernel_partition_of_unity_and_symmetry(oracle_mod, smooth, support):
+    rng = np.random.default_rng(1)
+    for r0 in rng.uniform(0.0, 1.0, 50):
+        vals = [oracle_mod.delta(r0 + i, smooth) for i in range(-4, 5)]
+        assert abs(sum(vals) - 1.0) < 1e-14
+        first = sum((r0 + i) * v for i, v in zip(range(-4, 5), vals))
+        assert abs(first) < 1e-14
+    for r in rng.uniform(0.0, 3.0, 50):
+        assert oracle_mod.delta(r, smooth) == oracle_mod.delta(-r, smooth)
+    assert oracle_mod.delta(support + 1e-9, smooth) == 0.0
+    assert oracle_mod.delta(support + 0.3, smooth) == 0.0
+
+
+def test_peskin_kernel_values(oracle_mod):
+    # phi(0) = 1/2, phi(1) = 1/4, phi(0.5) = (3-1+sqrt(2))/8
+    assert abs(oracle_mod.delta(0.0, 0) - 0.5) < 1e-16
+    assert abs(oracle_mod.delta(1.0, 0) - 0.25) < 1e-16
+    assert abs(oracle_mod.delta(0.5, 0) - (2.0 + math.sqrt(2.0)) / 8.0) < 1e-16
+
+
+def test_motion_lookup_rows_and_interpolation(oracle_mod):
+    t = np.array([0.0, 0.1, 0.2, 0.4])
+    table = np.stack([t, 10 * t, t * t], axis=1)
+    np.testing.assert_array_equal(oracle_mod.motion_lookup(table, 0.1), table[1])
+    r = oracle_mod.motion_lookup(table, 0.3)
+    assert abs(r[1] - 3.0) < 1e-12 and abs(r[2] - 0.1) < 1e-12   # linear between rows
+    np.testing.assert_array_equal(oracle_mod.motion_lookup(table, -1.0), [-1.0, table[0, 1], table[0, 2]])
+    np.testing.assert_array_equal(oracle_mod.motion_lookup(table, 9.0), [9.0, table[3, 1], table[3, 2]])
+
+
+def _small(oracle_mod, **kw):
+    c = cases.small_case(**kw)
+    return c, oracle_mod.Oracle.from_case(c)
+
+
+def test_motion_table_rejects_decreasing_time(oracle_mod):
+    c = cases.small_case()
+    o = oracle_mod.Oracle(c.params)
+    bad = c.table.copy()
+    bad[5, 0] = bad[3, 0]
+    with pytest.raises(oracle_mod.OracleError):
+        o.set_motion_table(bad)
+    with pytest.raises(oracle_mod.OracleError):
+        o.set_motion_table(c.table[:, :5])
+
+
+def test_streaming_is_a_pull_permutation(oracle_mod):
+    c, o = _small(oracle_mod)
+    f_prev = o.populations().copy()
+    o.evolution()
+    f0 = o.streamed()
+    e, _ = oracle_mod.lattice()
+    for k in range(9):
+        ex, ey = e[k]
+        src = f_prev[k, 1 - ey:c.params.ny - 1 - ey, 1 - ex:c.params.nx - 1 - ex]
+        np.testing.assert_array_equal(f0[k, 1:-1, 1:-1], src)
+
+
+def test_collision_conserves_mass_and_momentum_off_body(oracle_mod):
+    c, o = _small(oracle_mod)
+    o.evolution()
+    f0, f = o.streamed(), o.populations()
+    gx, gy = o.gforce()
+    e, _ = oracle_mod.lattice()
+    free = (gx == 0) & (gy == 0)
+    free[0, :] = free[-1, :] = False
+    free[:, 0] = free[:, -1] = False
+    assert free.sum() > 0.9 * free.size * 0.8
+    for comp in (np.ones(9), e[:, 0], e[:, 1]):
+        a = np.tensordot(comp, f0, axes=(0, 0))[free]
+        b = np.tensordot(comp, f, axes=(0, 0))[free]
+        assert np.abs(a - b).max() < 5e-15
+
+
+def test_ib_interpolated_velocity_equals_body_velocity(oracle_mod):
+    """Defining property of the implicit scheme: after the correction the
+    delta-interpolated velocity at each marker is the marker velocity."""
+    c, o = _small(oracle_mod, pitch_deg=10.0)
+    for _ in range(3):
+        row = o.evolution()
+    p = c.params
+    rho, u, v = o.fields()
+    xm, ym, res = o.markers()
+    assert res < 1e-12
+    wing_row = row
+    sa, sau, saac, sb, sbv, sbac, angle, omega, omgac = wing_row[7:16]
+    x0, y0 = c.contours[0]
+    xbar = 0.5 * (x0[1:] + x0[:-1])
+    ybar = 0.5 * (y0[1:] + y0[:-1])
+    ub = p.uu * (-omega * math.sin(angle) * xbar + omega * math.cos(angle) * ybar + sau)
+    vb = p.uu * (-omega * math.cos(angle) * xbar - omega * math.sin(angle) * ybar + sbv)
+    for k in range(len(xm)):
+        ic = (xm[k] - p.ox) / p.scale
+        jc = (ym[k] - p.oy) / p.scale
+        su = sv = 0.0
+        for i in range(int(ic) - 3, int(ic) + 4):
+            for j in range(int(jc) - 3, int(jc) + 4):
+                wgt = oracle_mod.delta(i - ic, p.delta_kernel) * oracle_mod.delta(j - jc, p.delta_kernel)
+                su += wgt * u[j, i]
+                sv += wgt * v[j, i]
+        assert abs(su - ub[k]) < 1e-11 * p.uu * 100
+        assert abs(sv - vb[k]) < 1e-11 * p.uu * 100
+
+
+def test_force_row_is_normalised_sum_of_force_density(oracle_mod):
+    c, o = _small(oracle_mod)
+    for _ in range(4):
+        row = o.evolution()
+    p = c.params
+    gx, gy = o.gforce()
+    chord = 1.0 / p.scale
+    cx = 2.0 * (-gx.sum()) / (p.uu * p.uu * chord)
+    cy = 2.0 * (-gy.sum()) / (p.uu * p.uu * chord)
+    assert abs(cx - row[1]) < 1e-9 * max(1.0, abs(cx))
+    assert abs(cy - row[2]) < 1e-9 * max(1.0, abs(cy))
+    # moment about the moving pivot (boundary_condition.f90:1672-1674)
+    jj, ii = np.nonzero((gx != 0) | (gy != 0))
+    sa, sb = row[7], row[10]
+    x0 = (p.ox + p.scale * ii - (p.xc + sa)) / p.scale
+    y0 = (p.oy + p.scale * jj - (p.yc + sb)) / p.scale
+    mom = np.sum(-x0 * gy[jj, ii] + y0 * gx[jj, ii])
+    cm = -2.0 * mom / (p.uu * p.uu * chord * chord)
+    assert abs(cm - row[3]) < 1e-9 * max(1.0, abs(cm))
+    # totals equal the single wing
+    np.testing.assert_allclose(row[4:7], row[1:4], rtol=0, atol=1e-12)
+
+
+def test_erranalysis_matches_definition(oracle_mod):
+    c, o = _small(oracle_mod)
+    o.evolution()
+    _, u1, v1 = [a.copy() for a in o.fields()]
+    o.evolution()
+    _, u2, v2 = o.fields()
+    s = (slice(1, -1), slice(1, -1))
+    t1 = np.sum((u2[s] - u1[s]) ** 2 + (v2[s] - v1[s]) ** 2)
+    t2 = np.sum(u2[s] ** 2 + v2[s] ** 2)
+    assert abs(o.erranalysis() - math.sqrt(t1) / (math.sqrt(t2) + 1e-30)) < 1e-14
+
+
+def test_top_bottom_rows_and_stale_edge_f0(oracle_mod):
+    c, o = _small(oracle_mod)
+    f_init = o.populations().copy()
+    for _ in range(3):
+        o.evolution()
+    rho, u, v = o.fields()
+    for row, nbr in ((0, 1), (-1, -2)):
+        assert np.all(u[row] == 0.0) and np.all(v[row] == 0.0)
+        np.testing.assert_array_equal(rho[row], rho[nbr])
+    f0 = o.streamed()
+    # streaming never rewrites the edge f0 (solution.f90:440-447)
+    np.testing.assert_array_equal(f0[:, 0, :], f_init[:, 0, :])
+    np.testing.assert_array_equal(f0[:, :, -1], f_init[:, :, -1])
+
+
+def test_range_error_when_body_reaches_edge(oracle_mod):
+    c = cases.small_case(pivot=(8, 33))
+    o = oracle_mod.Oracle.from_case(c)
+    with pytest.raises(oracle_mod.OracleError, match="-7"):
+        o.evolution()
+
+
+def test_run_stops_at_motion_end(oracle_mod):
+    c = cases.small_case(n_steps=5)
+    o = oracle_mod.Oracle.from_case(c)
+    rows = o.run(10)
+    assert rows.shape[0] == 5
+    assert o.evolution() is None
+
+
+def test_two_wings_and_smooth_kernel_step(oracle_mod):
+    c, o = _small(oracle_mod, nx=128, wings=2, delta=1)
+    rows = o.run(5)
+    assert rows.shape == (5, 1 + 6 + 3 + 18)
+    assert np.all(np.isfinite(rows))
+    np.testing.assert_allclose(rows[:, 7], rows[:, 1] + rows[:, 4], rtol=1e-13, atol=1e-13)
+
+
+def test_no_body_runs(oracle_mod):
+    c = cases.small_case(wings=0)
+    o = oracle_mod.Oracle.from_case(c)
+    rows = o.run(3)
+    assert rows.shape == (3, 4)
+    assert np.all(rows[:, 1:] == 0.0)
+
+
+def test_geometry_generator_reproduces_reference_boundary_file():
+    """naca0012(204) is the layout of the reference's own boundary.dat."""
+    ref = "/root/reference/boundary.dat"
+    if not os.path.exists(ref):
+        pytest.skip("reference tree not present")
+    d = np.loadtxt(ref)
+    x, y = cases.naca0012(204)
+    assert np.abs(x - d[:, 0]).max() < 1.5e-8
+    assert np.abs(y - d[:, 1]).max() < 1.5e-8
