@@ -22,6 +22,8 @@ LBM_PREC_FP16 = 2
 LBM_PREC_BF16 = 3
 PRECISIONS = {"fp32": LBM_PREC_FP32, "fp64": LBM_PREC_FP64, "fp16": LBM_PREC_FP16, "bf16": LBM_PREC_BF16}
 
+LBM_FLAG_DENSE_SOLVE = 1
+
 LBM_DELTA_PESKIN4 = 0
 LBM_DELTA_SMOOTH = 1
 
@@ -65,7 +67,7 @@ ABI = {
     "lbm_get_populations": (C.c_int, [_P, _D]),
     "lbm_set_populations": (C.c_int, [_P, _D]),
     "lbm_residual": (C.c_int, [_P, _D]),
-    "lbm_get_markers": (C.c_int, [_P, _D, _D, _D]),
+    "lbm_get_markers": (C.c_int, [_P, _D, _D, _D, C.POINTER(C.c_int)]),
     "lbm_set_timing": (C.c_int, [_P, C.c_int]),
     "lbm_get_timing": (C.c_int, [_P, _D, _D, _D, C.POINTER(C.c_int)]),
     "lbm_step_index": (C.c_int, [_P]),

@@ -7,24 +7,31 @@
 // solves A x = U_b - X1 u* by LU (cusolverDnDgetrf/getrs) and spreads
 // du = X2 x. With D = X1, A = (D D^T) W, so y = W x solves the symmetric
 // positive definite system (D D^T) y = U_b - D u* and du = D^T y: the same
-// correction, with arc_l dropping out. The kernels below
-//   ib_prepare  marker positions, velocities, support boxes, one-axis kernel
-//               values, the bounding rectangle of all boxes (one CTA);
-//   ib_interp   b = D u*, one warp per marker, warp-shuffle sum over its box;
-//   ib_assemble B = D D^T; the delta is separable, so each entry is
-//               (sum_i phx_k phx_l)(sum_j phy_k phy_l) over the box overlap;
-//   ib_solve    Cholesky of B and two triangular solves (one CTA);
+// correction, with arc_l dropping out. Three launches:
+//   ib_markers  one warp per marker: position, boundary velocity, support box
+//               and one-axis kernel values (move_boundary, :1540-1606), then
+//               b = D u* over the box with a warp-shuffle sum (:1609-1629);
+//   ib_solve    one CTA: correction-patch rectangle and force-row header;
+//               markers sorted along the longer axis of the marker cloud,
+//               where D D^T is banded (delta supports overlap only for
+//               markers less than 6 lu apart); the band is cut into 16x16
+//               blocks and solved by block cyclic reduction (FP64, log2 of the
+//               block count levels); a dense Cholesky is the fallback when a
+//               coupling reaches past the neighbouring block;
 //   ib_spread   du = D^T y per node, gathered in marker order over the
 //               markers whose box covers the node (no atomics), written to the
 //               correction patch the lattice kernel reads; force and moment
-//               sums in FP64 with a deterministic two-level reduction.
+//               sums in FP64 with a deterministic two-level reduction
+//               (:1645-1675, solution.f90:327-336).
 #include <math.h>
 
 #include "lbm_internal.h"
 
 namespace {
 
-const size_t kSolveSmem = 220 * 1024;   // dynamic shared memory cap of ib_solve
+constexpr int BS = 16;                 // cyclic-reduction block size
+constexpr int NSORT_MAX = 4096;        // largest marker count (sort in shared memory)
+constexpr int SOLVE_THREADS = 1024;
 
 // one-axis kernel value (boundary_condition.f90:1563-1600), disr = |r|
 __device__ __forceinline__ double delta1(double disr, int smooth)
@@ -76,104 +83,80 @@ __device__ __forceinline__ const double *motion_row(const IBArgs &a, int step_in
     return a.mstep + (long long)(idx - 1) * a.mcols;
 }
 
-__global__ void __launch_bounds__(1024) ib_prepare(const IBArgs a, int step_index, int ring_slot)
+// marker geometry of segment k (airfoil.f90:255-335, boundary_condition.f90:1540-1606)
+__device__ Marker make_marker(const IBArgs &a, const double *row, int k)
 {
-    __shared__ int bb[4];
-    if (threadIdx.x == 0) { bb[0] = 1 << 30; bb[1] = 1 << 30; bb[2] = -1; bb[3] = -1; }
-    __syncthreads();
-    double time;
-    const double *row = motion_row(a, step_index, &time);
     const double scale = a.scale, ox = a.ox, oy = a.oy;
-    for (int k = threadIdx.x; k < a.nseg; k += blockDim.x) {
-        const int w = k / a.spw;
-        const int p0 = w * a.ppw + (k - w * a.spw);
-        const double angle = row[1 + 9 * w], omega = row[2 + 9 * w];
-        const double sa = row[4 + 9 * w], sau = row[5 + 9 * w];
-        const double sb = row[7 + 9 * w], sbv = row[8 + 9 * w];
-        const double ca = cos(angle), sn = sin(angle);
-        // airfoil.f90:261-263 (body_extra_s and movenum are zero: no dynamics)
-        const double xa = ca * a.xb0[p0] + sn * a.yb0[p0] + sa + a.xc;
-        const double xb = ca * a.xb0[p0 + 1] + sn * a.yb0[p0 + 1] + sa + a.xc;
-        const double ya = -sn * a.xb0[p0] + ca * a.yb0[p0] + sb + a.yc;
-        const double yb = -sn * a.xb0[p0 + 1] + ca * a.yb0[p0 + 1] + sb + a.yc;
-        Marker m;
-        m.xm = 0.5 * (xb + xa);                                           // :267-270
-        m.ym = 0.5 * (yb + ya);
-        // boundary_condition.f90:1547-1550 (body_extra_v is zero)
-        m.ub = a.uu * (-omega * sn * 0.5 * (a.xb0[p0 + 1] + a.xb0[p0]) +
-                       omega * ca * 0.5 * (a.yb0[p0 + 1] + a.yb0[p0]) + sau);
-        m.vb = a.uu * (-omega * ca * 0.5 * (a.xb0[p0 + 1] + a.xb0[p0]) -
-                       omega * sn * 0.5 * (a.yb0[p0 + 1] + a.yb0[p0]) + sbv);
-        // support box, 1-based scans of airfoil.f90:290-321; a marker off the
-        // lattice (or not finite) is a range error before any scan runs
-        const double fx = (m.xm - ox) / scale + 1.0, fy = (m.ym - oy) / scale + 1.0;
-        if (!(fx > 3.0 && fx < (double)(a.nx - 2) && fy > 3.0 && fy < (double)(a.ny - 2))) {
-            atomicOr(a.status, LBM_ST_RANGE);
-            for (int t = 0; t < LBM_BOX; ++t) m.phx[t] = m.phy[t] = 0.0;
-            m.i1 = 3; m.i2 = 2; m.j1 = 3; m.j2 = 2;   // empty box
-            m.wing = w;
-            m.pad = 0;
-            a.mk[k] = m;
-            continue;
-        }
-        int i1 = (int)((m.xm - ox) / scale + 1.0);
-        for (int i = i1; i >= 1; --i)
-            if (fabs((ox + (double)(i - 1) * scale - m.xm) / scale) > 2.5) { i1 = i + 1; break; }
-        int i2 = (int)((m.xm - ox) / scale + 1.0);
-        for (int i = i2; i <= a.nx; ++i)
-            if (fabs((ox + (double)(i - 1) * scale - m.xm) / scale) > 2.5) { i2 = i - 1; break; }
-        int j2 = (int)((m.ym - oy) / scale + 1.0);
-        for (int i = j2; i <= a.ny; ++i)
-            if (fabs((oy + (double)(i - 1) * scale - m.ym) / scale) > 2.5) { j2 = i - 1; break; }
-        int j1 = (int)((m.ym - oy) / scale + 1.0);
-        for (int i = j1; i >= 1; --i)
-            if (fabs((oy + (double)(i - 1) * scale - m.ym) / scale) > 2.5) { j1 = i + 1; break; }
-        if (i1 < 4 || j1 < 4 || i2 > a.nx - 3 || j2 > a.ny - 3 || i2 - i1 >= LBM_BOX || j2 - j1 >= LBM_BOX) {
-            atomicOr(a.status, LBM_ST_RANGE);
-            i1 = 4; i2 = 3; j1 = 4; j2 = 3;   // empty box
-        }
-        for (int t = 0; t < LBM_BOX; ++t) {
-            const int ii = i1 + t, jj = j1 + t;
-            m.phx[t] = ii <= i2 ? delta1(fabs((ox + scale * (double)(ii - 1) - m.xm) / scale), a.smooth) : 0.0;
-            m.phy[t] = jj <= j2 ? delta1(fabs((oy + scale * (double)(jj - 1) - m.ym) / scale), a.smooth) : 0.0;
-        }
-        m.i1 = i1 - 1; m.i2 = i2 - 1; m.j1 = j1 - 1; m.j2 = j2 - 1;
-        m.wing = w;
-        m.pad = 0;
-        a.mk[k] = m;
-        if (i2 >= i1 && j2 >= j1) {
-            atomicMin(&bb[0], i1 - 1); atomicMin(&bb[1], j1 - 1);
-            atomicMax(&bb[2], i2 - 1); atomicMax(&bb[3], j2 - 1);
-        }
+    const int w = k / a.spw;
+    const int p0 = w * a.ppw + (k - w * a.spw);
+    const double angle = row[1 + 9 * w], omega = row[2 + 9 * w];
+    const double sa = row[4 + 9 * w], sau = row[5 + 9 * w];
+    const double sb = row[7 + 9 * w], sbv = row[8 + 9 * w];
+    const double ca = cos(angle), sn = sin(angle);
+    // airfoil.f90:261-263 (body_extra_s and movenum are zero: no dynamics)
+    const double xa = ca * a.xb0[p0] + sn * a.yb0[p0] + sa + a.xc;
+    const double xb = ca * a.xb0[p0 + 1] + sn * a.yb0[p0 + 1] + sa + a.xc;
+    const double ya = -sn * a.xb0[p0] + ca * a.yb0[p0] + sb + a.yc;
+    const double yb = -sn * a.xb0[p0 + 1] + ca * a.yb0[p0 + 1] + sb + a.yc;
+    Marker m;
+    m.xm = 0.5 * (xb + xa);                                           // :267-270
+    m.ym = 0.5 * (yb + ya);
+    // boundary_condition.f90:1547-1550 (body_extra_v is zero)
+    m.ub = a.uu * (-omega * sn * 0.5 * (a.xb0[p0 + 1] + a.xb0[p0]) +
+                   omega * ca * 0.5 * (a.yb0[p0 + 1] + a.yb0[p0]) + sau);
+    m.vb = a.uu * (-omega * ca * 0.5 * (a.xb0[p0 + 1] + a.xb0[p0]) -
+                   omega * sn * 0.5 * (a.yb0[p0 + 1] + a.yb0[p0]) + sbv);
+    m.wing = w;
+    m.pad = 0;
+    for (int t = 0; t < LBM_BOX; ++t) m.phx[t] = m.phy[t] = 0.0;
+    m.i1 = 3; m.i2 = 2; m.j1 = 3; m.j2 = 2;   // empty box unless set below
+    // a marker off the lattice (or not finite) is a range error before any scan
+    const double fx = (m.xm - ox) / scale + 1.0, fy = (m.ym - oy) / scale + 1.0;
+    if (!(fx > 3.0 && fx < (double)(a.nx - 2) && fy > 3.0 && fy < (double)(a.ny - 2))) {
+        atomicOr(a.status, LBM_ST_RANGE);
+        return m;
     }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        PatchInfo pi{0, 0, 0, 0};
-        if (bb[2] >= bb[0]) {
-            pi.i0 = bb[0]; pi.j0 = bb[1]; pi.w = bb[2] - bb[0] + 1; pi.h = bb[3] - bb[1] + 1;
-            if ((long long)pi.w * pi.h > a.patch_cap || pi.w > a.patch_wmax || pi.h > a.patch_hmax) { atomicOr(a.status, LBM_ST_OVERFLOW); pi = PatchInfo{0, 0, 0, 0}; }
-        }
-        *a.pinfo = pi;
-        // force.dat row: time and the motion columns (solution.f90:350-375)
-        double *fr = a.force_ring + (long long)ring_slot * a.row_len;
-        fr[0] = time;
-        const int mc = 1 + 3 * a.nwing + 3;
-        for (int w = 0; w < a.nwing; ++w) {
-            const double *r = row + 1 + 9 * w;   // angle omega omgac sa sau saac sb sbv sbac
-            double *o = fr + mc + 9 * w;
-            o[0] = r[3]; o[1] = r[4]; o[2] = r[5]; o[3] = r[6]; o[4] = r[7]; o[5] = r[8];
-            o[6] = r[0]; o[7] = r[1]; o[8] = r[2];
-        }
+    // support box, 1-based scans of airfoil.f90:290-321
+    int i1 = (int)((m.xm - ox) / scale + 1.0);
+    for (int i = i1; i >= 1; --i)
+        if (fabs((ox + (double)(i - 1) * scale - m.xm) / scale) > 2.5) { i1 = i + 1; break; }
+    int i2 = (int)((m.xm - ox) / scale + 1.0);
+    for (int i = i2; i <= a.nx; ++i)
+        if (fabs((ox + (double)(i - 1) * scale - m.xm) / scale) > 2.5) { i2 = i - 1; break; }
+    int j2 = (int)((m.ym - oy) / scale + 1.0);
+    for (int i = j2; i <= a.ny; ++i)
+        if (fabs((oy + (double)(i - 1) * scale - m.ym) / scale) > 2.5) { j2 = i - 1; break; }
+    int j1 = (int)((m.ym - oy) / scale + 1.0);
+    for (int i = j1; i >= 1; --i)
+        if (fabs((oy + (double)(i - 1) * scale - m.ym) / scale) > 2.5) { j1 = i + 1; break; }
+    if (i1 < 4 || j1 < 4 || i2 > a.nx - 3 || j2 > a.ny - 3 || i2 - i1 >= LBM_BOX || j2 - j1 >= LBM_BOX) {
+        atomicOr(a.status, LBM_ST_RANGE);
+        return m;
     }
+    for (int t = 0; t < LBM_BOX; ++t) {
+        const int ii = i1 + t, jj = j1 + t;
+        m.phx[t] = ii <= i2 ? delta1(fabs((ox + scale * (double)(ii - 1) - m.xm) / scale), a.smooth) : 0.0;
+        m.phy[t] = jj <= j2 ? delta1(fabs((oy + scale * (double)(jj - 1) - m.ym) / scale), a.smooth) : 0.0;
+    }
+    m.i1 = i1 - 1; m.i2 = i2 - 1; m.j1 = j1 - 1; m.j2 = j2 - 1;
+    return m;
 }
 
+// one warp per marker: geometry, then b = D u* and rhs = U_b - b
 template <typename T>
-__global__ void __launch_bounds__(256) ib_interp(const IBArgs a)
+__global__ void __launch_bounds__(256) ib_markers(const IBArgs a, int step_index)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int k = blockIdx.x * 8 + warp;
     if (k >= a.nseg) return;
-    const Marker &m = a.mk[k];
+    const double *row = motion_row(a, step_index, nullptr);
+    Marker m;
+    if (lane == 0) m = make_marker(a, row, k);
+    // broadcast the marker to the warp through shared memory
+    __shared__ Marker sm[8];
+    if (lane == 0) { sm[warp] = m; a.mk[k] = m; }
+    __syncwarp();
+    m = sm[warp];
     const int nbx = m.i2 - m.i1 + 1, nby = m.j2 - m.j1 + 1;
     const int nn = nbx > 0 && nby > 0 ? nbx * nby : 0;
     double su = 0.0, sv = 0.0;
@@ -196,74 +179,118 @@ __global__ void __launch_bounds__(256) ib_interp(const IBArgs a)
     }
 }
 
-__global__ void __launch_bounds__(128) ib_assemble(const IBArgs a)
+// (D D^T)(k,l): the delta is separable, so the node sum over the box overlap
+// is (sum_i phx_k phx_l)(sum_j phy_k phy_l)
+__device__ __forceinline__ double bval(const Marker &mk, const Marker &ml)
 {
-    const int k = blockIdx.x;
-    const Marker mk = a.mk[k];
-    for (int l = threadIdx.x; l < a.nseg; l += blockDim.x) {
-        const Marker &ml = a.mk[l];
-        const int ia = max(mk.i1, ml.i1), ib = min(mk.i2, ml.i2);
-        const int ja = max(mk.j1, ml.j1), jb = min(mk.j2, ml.j2);
-        double b = 0.0;
-        if (ia <= ib && ja <= jb) {
-            double sx = 0.0, sy = 0.0;
-            for (int i = ia; i <= ib; ++i) sx += mk.phx[i - mk.i1] * ml.phx[i - ml.i1];
-            for (int j = ja; j <= jb; ++j) sy += mk.phy[j - mk.j1] * ml.phy[j - ml.j1];
-            b = sx * sy;
+    const int ia = max(mk.i1, ml.i1), ib = min(mk.i2, ml.i2);
+    const int ja = max(mk.j1, ml.j1), jb = min(mk.j2, ml.j2);
+    if (ia > ib || ja > jb) return 0.0;
+    double sx = 0.0, sy = 0.0;
+    for (int i = ia; i <= ib; ++i) sx += mk.phx[i - mk.i1] * ml.phx[i - ml.i1];
+    for (int j = ja; j <= jb; ++j) sy += mk.phy[j - mk.j1] * ml.phy[j - ml.j1];
+    return sx * sy;
+}
+
+__device__ __forceinline__ bool boxes_overlap(const Marker &mk, const Marker &ml)
+{
+    return max(mk.i1, ml.i1) <= min(mk.i2, ml.i2) && max(mk.j1, ml.j1) <= min(mk.j2, ml.j2);
+}
+
+// Cholesky of one BS x BS block by one warp, in shared memory (lower
+// triangle, row-major); returns false if not positive definite
+__device__ bool warp_chol(double *G)
+{
+    const int lane = threadIdx.x & 31;
+    bool ok = true;
+    for (int k = 0; k < BS; ++k) {
+        const double d = G[k * BS + k];
+        const bool good = d > 0.0 && isfinite(d);
+        ok = ok && good;
+        const double dk = good ? sqrt(d) : 1.0;
+        __syncwarp();
+        if (lane == 0) G[k * BS + k] = dk;
+        for (int i = k + 1 + lane; i < BS; i += 32) G[i * BS + k] /= dk;
+        __syncwarp();
+        for (int q = lane; q < BS * BS; q += 32) {
+            const int i = q / BS, j = q % BS;
+            if (j > k && j <= i) G[i * BS + j] -= G[i * BS + k] * G[j * BS + k];
         }
-        a.B[(long long)k * a.nseg + l] = b;
+        __syncwarp();
+    }
+    return ok;
+}
+
+// X <- (G G^T)^-1 X for a row-major BS x ncol matrix X in global memory
+// (lane per column)
+__device__ void warp_chol_solve(const double *G, double *X, int ncol)
+{
+    const int lane = threadIdx.x & 31;
+    for (int c = lane; c < ncol; c += 32) {
+        for (int r = 0; r < BS; ++r) {
+            double s = X[r * ncol + c];
+            for (int q = 0; q < r; ++q) s -= G[r * BS + q] * X[q * ncol + c];
+            X[r * ncol + c] = s / G[r * BS + r];
+        }
+        for (int r = BS - 1; r >= 0; --r) {
+            double s = X[r * ncol + c];
+            for (int q = r + 1; q < BS; ++q) s -= G[q * BS + r] * X[q * ncol + c];
+            X[r * ncol + c] = s / G[r * BS + r];
+        }
+    }
+    __syncwarp();
+}
+
+__device__ void write_header(const IBArgs &a, const double *row, double time, int ring_slot)
+{
+    double *fr = a.force_ring + (long long)ring_slot * a.row_len;
+    fr[0] = time;
+    const int mc = 1 + 3 * a.nwing + 3;
+    for (int w = 0; w < a.nwing; ++w) {
+        const double *r = row + 1 + 9 * w;   // angle omega omgac sa sau saac sb sbv sbac
+        double *o = fr + mc + 9 * w;         // solution.f90:363-374 order
+        o[0] = r[3]; o[1] = r[4]; o[2] = r[5]; o[3] = r[6]; o[4] = r[7]; o[5] = r[8];
+        o[6] = r[0]; o[7] = r[1]; o[8] = r[2];
     }
 }
 
-// Cholesky B = L L^T (lower triangle, in place) with the forward solve fused
-// into the factorisation (column k of L is staged in shared memory, so the
-// trailing update reads rows contiguously), then the backward solve L^T y = z
-// by rows. One CTA. B lives in shared memory when it fits, else in global
-// memory (L2). Dynamic shared memory: colk[n], y[2n], then L[n*n] if resident.
-__global__ void __launch_bounds__(1024) ib_solve(const IBArgs a, int use_smem)
+// dense fallback: Cholesky of the full B (global memory) and two solves, whole CTA
+__device__ void dense_solve(const IBArgs &a, const Marker *mk, double *yv, int *bad)
 {
-    extern __shared__ double sm[];
-    const int n = a.nseg;
-    double *colk = sm, *yv = sm + n;
-    double *L = use_smem ? sm + 3 * n : a.B;
-    const int tid = threadIdx.x, nt = blockDim.x;
+    const int n = a.nseg, tid = threadIdx.x, nt = blockDim.x;
     const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
-    if (use_smem)
-        for (long long q = tid; q < (long long)n * n; q += nt) L[q] = a.B[q];
+    double *L = a.B;
+    for (long long q = tid; q < (long long)n * n; q += nt) {
+        const int k = (int)(q / n), l = (int)(q % n);
+        L[q] = bval(mk[k], mk[l]);
+    }
     for (int q = tid; q < 2 * n; q += nt) yv[q] = a.rhs[q];
-    __shared__ int bad;
-    if (tid == 0) bad = 0;
     __syncthreads();
     for (int k = 0; k < n; ++k) {
         if (tid == 0) {
             const double d = L[(long long)k * n + k];
             double dk = 1.0;
-            if (!(d > 0.0) || !isfinite(d)) bad = 1;
+            if (!(d > 0.0) || !isfinite(d)) *bad = 1;
             else dk = sqrt(d);
             L[(long long)k * n + k] = dk;
-            colk[k] = dk;
         }
         __syncthreads();
-        const double dk = colk[k];
-        for (int i = k + 1 + tid; i < n; i += nt) {
-            const double v = L[(long long)i * n + k] / dk;
-            L[(long long)i * n + k] = v;
-            colk[i] = v;
-        }
-        if (tid < 2) yv[tid * n + k] /= dk;                    // z_k
+        const double dk = L[(long long)k * n + k];
+        for (int i = k + 1 + tid; i < n; i += nt) L[(long long)i * n + k] /= dk;
+        if (tid < 2) yv[tid * n + k] /= dk;
         __syncthreads();
         for (int i = k + 1 + warp; i < n; i += nw) {
-            const double lik = colk[i];
-            for (int j = k + 1 + lane; j <= i; j += 32) L[(long long)i * n + j] -= lik * colk[j];
+            const double lik = L[(long long)i * n + k];
+            for (int j = k + 1 + lane; j <= i; j += 32) L[(long long)i * n + j] -= lik * L[(long long)j * n + k];
         }
         const double z0 = yv[k], z1 = yv[n + k];
         for (int i = k + 1 + tid; i < n; i += nt) {
-            yv[i] -= colk[i] * z0;
-            yv[n + i] -= colk[i] * z1;
+            const double lik = L[(long long)i * n + k];
+            yv[i] -= lik * z0;
+            yv[n + i] -= lik * z1;
         }
         __syncthreads();
     }
-    // backward: L^T y = z; row j of L is column j of L^T
     for (int j = n - 1; j >= 0; --j) {
         if (tid < 2) yv[tid * n + j] /= L[(long long)j * n + j];
         __syncthreads();
@@ -273,8 +300,289 @@ __global__ void __launch_bounds__(1024) ib_solve(const IBArgs a, int use_smem)
         }
         __syncthreads();
     }
-    for (int q = tid; q < 2 * n; q += nt) a.y[q] = yv[q];
-    if (tid == 0 && bad) atomicOr(a.status, LBM_ST_SOLVER);
+}
+
+// relative residual ||B y - rhs|| / ||rhs|| of both right-hand sides over the
+// sorted band (couplings exist only within `reach`), written with the
+// half-bandwidth; a residual above 1e-6 or a failed factorisation flags the
+// step as a solver failure
+__device__ void solve_residual(const IBArgs &a, const double *key, const int *idx, double reach, int wmax, int bad)
+{
+    const int n = a.nseg, tid = threadIdx.x, nt = blockDim.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    __shared__ double wr[32][2];
+    double num = 0.0, den = 0.0;
+    for (int s = tid; s < n; s += nt) {
+        const int k = idx[s];
+        double b0 = 0.0, b1 = 0.0;
+        int t = s;
+        while (t > 0 && key[s] - key[t - 1] <= reach) --t;
+        for (; t < n && key[t] - key[s] <= reach; ++t) {
+            const int l = idx[t];
+            const double b = bval(a.mk[k], a.mk[l]);
+            b0 += b * a.y[l];
+            b1 += b * a.y[n + l];
+        }
+        const double r0 = b0 - a.rhs[k], r1 = b1 - a.rhs[n + k];
+        num += r0 * r0 + r1 * r1;
+        den += a.rhs[k] * a.rhs[k] + a.rhs[n + k] * a.rhs[n + k];
+    }
+    for (int off = 16; off; off >>= 1) {
+        num += __shfl_xor_sync(0xffffffffu, num, off);
+        den += __shfl_xor_sync(0xffffffffu, den, off);
+    }
+    if (lane == 0) { wr[warp][0] = num; wr[warp][1] = den; }
+    __syncthreads();
+    if (tid == 0) {
+        double sn = 0.0, sd = 0.0;
+        for (int w = 0; w < (nt >> 5); ++w) { sn += wr[w][0]; sd += wr[w][1]; }
+        const double res = sqrt(sn) / (sqrt(sd) + 1e-300);
+        a.solve_res[0] = res;
+        a.solve_res[1] = (double)wmax;
+        if (bad || !(res < 1e-6)) atomicOr(a.status, LBM_ST_SOLVER);
+    }
+}
+
+// The linear solve of one step, one CTA of SOLVE_THREADS threads.
+// Dynamic shared memory: key[ns] (double), idx[ns] (int, then ns ints of
+// padding), G[32][BS*BS] (double), ns = n rounded up to a power of two.
+__global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int step_index, int ring_slot)
+{
+    extern __shared__ double smem[];
+    const int n = a.nseg, tid = threadIdx.x, nt = blockDim.x;
+    const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
+    int ns = 1;
+    while (ns < n) ns <<= 1;
+    double *key = smem;
+    int *idx = (int *)(key + ns);
+    double *G = (double *)(idx + 2 * ns) + warp * BS * BS;
+    __shared__ int bb[4];
+    __shared__ double ext[4];
+    __shared__ int wmax, bad;
+    const Marker *mk = a.mk;
+    if (tid == 0) {
+        bb[0] = 1 << 30; bb[1] = 1 << 30; bb[2] = -1; bb[3] = -1;
+        ext[0] = 1e300; ext[1] = -1e300; ext[2] = 1e300; ext[3] = -1e300;
+        wmax = 0; bad = 0;
+    }
+    __syncthreads();
+    // patch rectangle and marker-cloud extent
+    double lx0 = 1e300, lx1 = -1e300, ly0 = 1e300, ly1 = -1e300;
+    int b0 = 1 << 30, b1 = 1 << 30, b2 = -1, b3 = -1;
+    for (int k = tid; k < n; k += nt) {
+        const Marker &m = mk[k];
+        lx0 = fmin(lx0, m.xm); lx1 = fmax(lx1, m.xm); ly0 = fmin(ly0, m.ym); ly1 = fmax(ly1, m.ym);
+        if (m.i2 >= m.i1 && m.j2 >= m.j1) {
+            b0 = min(b0, m.i1); b1 = min(b1, m.j1); b2 = max(b2, m.i2); b3 = max(b3, m.j2);
+        }
+    }
+    for (int off = 16; off; off >>= 1) {
+        lx0 = fmin(lx0, __shfl_xor_sync(0xffffffffu, lx0, off));
+        lx1 = fmax(lx1, __shfl_xor_sync(0xffffffffu, lx1, off));
+        ly0 = fmin(ly0, __shfl_xor_sync(0xffffffffu, ly0, off));
+        ly1 = fmax(ly1, __shfl_xor_sync(0xffffffffu, ly1, off));
+        b0 = min(b0, __shfl_xor_sync(0xffffffffu, b0, off));
+        b1 = min(b1, __shfl_xor_sync(0xffffffffu, b1, off));
+        b2 = max(b2, __shfl_xor_sync(0xffffffffu, b2, off));
+        b3 = max(b3, __shfl_xor_sync(0xffffffffu, b3, off));
+    }
+    __shared__ double wext[32][4];
+    if (lane == 0) {
+        atomicMin(&bb[0], b0); atomicMin(&bb[1], b1); atomicMax(&bb[2], b2); atomicMax(&bb[3], b3);
+        wext[warp][0] = lx0; wext[warp][1] = lx1; wext[warp][2] = ly0; wext[warp][3] = ly1;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        for (int w = 0; w < nw; ++w) {
+            ext[0] = fmin(ext[0], wext[w][0]); ext[1] = fmax(ext[1], wext[w][1]);
+            ext[2] = fmin(ext[2], wext[w][2]); ext[3] = fmax(ext[3], wext[w][3]);
+        }
+        double time;
+        const double *row = motion_row(a, step_index, &time);
+        write_header(a, row, time, ring_slot);
+        PatchInfo pi{0, 0, 0, 0};
+        if (bb[2] >= bb[0]) {
+            pi.i0 = bb[0]; pi.j0 = bb[1]; pi.w = bb[2] - bb[0] + 1; pi.h = bb[3] - bb[1] + 1;
+            if ((long long)pi.w * pi.h > a.patch_cap || pi.w > a.patch_wmax || pi.h > a.patch_hmax) {
+                atomicOr(a.status, LBM_ST_OVERFLOW);
+                pi = PatchInfo{0, 0, 0, 0};
+            }
+        }
+        *a.pinfo = pi;
+    }
+    __syncthreads();
+    if (n == 0) return;
+    // sort markers along the longer axis (stable: ties by index)
+    const bool by_x = (ext[1] - ext[0]) >= (ext[3] - ext[2]);
+    for (int s = tid; s < ns; s += nt) {
+        key[s] = s < n ? (by_x ? mk[s].xm : mk[s].ym) : 1e300;
+        idx[s] = s;
+    }
+    __syncthreads();
+    for (int size = 2; size <= ns; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int s = tid; s < ns; s += nt) {
+                const int t = s ^ stride;
+                if (t > s) {
+                    const bool up = (s & size) == 0;
+                    const bool gt = key[s] > key[t] || (key[s] == key[t] && idx[s] > idx[t]);
+                    if (gt == up) {
+                        const double kk = key[s]; key[s] = key[t]; key[t] = kk;
+                        const int ii = idx[s]; idx[s] = idx[t]; idx[t] = ii;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    // half-bandwidth of D D^T in the sorted order: boxes (<= 6 nodes wide)
+    // can overlap only for markers less than 6 lattice units apart
+    const double reach = 6.0 * a.scale;
+    for (int s = tid; s < n; s += nt) {
+        int wl = 0;
+        for (int t = s + 1; t < n && key[t] - key[s] <= reach; ++t)
+            if (boxes_overlap(mk[idx[s]], mk[idx[t]])) wl = t - s;
+        if (wl) atomicMax(&wmax, wl);
+    }
+    __syncthreads();
+    double *yv = a.bX + 2 * (long long)BS * ((n + BS - 1) / BS);   // 2n scratch after the block rhs
+    if (wmax > BS || a.force_dense) {
+        dense_solve(a, mk, yv, &bad);
+        for (int q = tid; q < 2 * n; q += nt) a.y[q] = yv[q];
+        __syncthreads();
+        solve_residual(a, key, idx, reach, wmax, bad);
+        return;
+    }
+    // block tridiagonal form: D_i (BS x BS), L_i couples block i to block i-1,
+    // X_i holds the two right-hand sides (BS x 2), padded with identity rows
+    const int nb = (n + BS - 1) / BS;
+    double *Db = a.bD, *Lb = a.bL, *Fb = a.bF, *Xb = a.bX;
+    const int FC = 2 * BS + 2;   // columns of F: [D^-1 L | D^-1 U | D^-1 r]
+    for (long long q = tid; q < (long long)nb * BS * BS; q += nt) {
+        const int blk = (int)(q / (BS * BS)), r = (int)(q % (BS * BS)) / BS, c = (int)(q % BS);
+        const int sr = blk * BS + r, sc = blk * BS + c, sp = (blk - 1) * BS + c;
+        double d;
+        if (sr < n && sc < n) d = bval(mk[idx[sr]], mk[idx[sc]]);
+        else d = (r == c) ? 1.0 : 0.0;
+        Db[q] = d;
+        Lb[q] = (blk > 0 && sr < n) ? bval(mk[idx[sr]], mk[idx[sp]]) : 0.0;
+    }
+    for (int q = tid; q < nb * BS; q += nt) {
+        Xb[2 * q] = q < n ? a.rhs[idx[q]] : 0.0;
+        Xb[2 * q + 1] = q < n ? a.rhs[n + idx[q]] : 0.0;
+    }
+    __syncthreads();
+    // cyclic reduction: at stride st the active blocks are multiples of st;
+    // odd multiples are eliminated into their even neighbours
+    int levels = 0;
+    for (int st = 1; st < nb; st <<= 1, ++levels) {
+        const int nodd = (nb - st + 2 * st - 1) / (2 * st);
+        for (int m = warp; m < nodd; m += nw) {
+            const int o = st * (2 * m + 1), q2 = o + st;
+            double *F = Fb + (long long)o * BS * FC;
+            for (int e = lane; e < BS * BS; e += 32) G[e] = Db[(long long)o * BS * BS + e];
+            for (int e = lane; e < BS * FC; e += 32) {
+                const int r = e / FC, c = e % FC;
+                double v;
+                if (c < BS) v = Lb[(long long)o * BS * BS + r * BS + c];                          // L_o
+                else if (c < 2 * BS) v = q2 < nb ? Lb[(long long)q2 * BS * BS + (c - BS) * BS + r] : 0.0;  // U_o = L_q^T
+                else v = Xb[2 * ((long long)o * BS + r) + (c - 2 * BS)];                          // r_o
+                F[e] = v;
+            }
+            __syncwarp();
+            if (!warp_chol(G) && lane == 0) bad = 1;
+            warp_chol_solve(G, F, FC);
+        }
+        __syncthreads();
+        const int neven = (nb + 2 * st - 1) / (2 * st);
+        for (int m = warp; m < neven; m += nw) {
+            const int e = 2 * st * m, o1 = e - st, o2 = e + st;
+            double *De = Db + (long long)e * BS * BS, *Le = Lb + (long long)e * BS * BS;
+            double *Xe = Xb + 2 * (long long)e * BS;
+            // right neighbour o2 (e is its previous block): D_e -= L_o2^T FL_o2, r_e -= L_o2^T Fr_o2
+            if (o2 < nb) {
+                const double *Lo = Lb + (long long)o2 * BS * BS;
+                const double *F = Fb + (long long)o2 * BS * FC;
+                for (int q = lane; q < BS * BS + 2 * BS; q += 32) {
+                    double s = 0.0;
+                    if (q < BS * BS) {
+                        const int r = q / BS, c = q % BS;
+                        for (int t = 0; t < BS; ++t) s += Lo[t * BS + r] * F[t * FC + c];
+                        De[q] -= s;
+                    } else {
+                        const int r = (q - BS * BS) / 2, c = (q - BS * BS) % 2;
+                        for (int t = 0; t < BS; ++t) s += Lo[t * BS + r] * F[t * FC + 2 * BS + c];
+                        Xe[2 * r + c] -= s;
+                    }
+                }
+            }
+            __syncwarp();
+            // left neighbour o1 (e is its next block): D_e -= L_e FU_o1,
+            // r_e -= L_e Fr_o1, new L_e = -L_e FL_o1
+            if (m > 0) {
+                const double *F = Fb + (long long)o1 * BS * FC;
+                double nl[(BS * BS + 31) / 32];
+                double dd[(BS * BS + 31) / 32];
+                double xr[(2 * BS + 31) / 32];
+                int cnt = 0;
+                for (int q = lane; q < BS * BS; q += 32, ++cnt) {
+                    const int r = q / BS, c = q % BS;
+                    double s1 = 0.0, s2 = 0.0;
+                    for (int t = 0; t < BS; ++t) {
+                        const double l = Le[r * BS + t];
+                        s1 += l * F[t * FC + BS + c];
+                        s2 += l * F[t * FC + c];
+                    }
+                    dd[cnt] = s1;
+                    nl[cnt] = -s2;
+                }
+                cnt = 0;
+                for (int q = lane; q < 2 * BS; q += 32, ++cnt) {
+                    const int r = q / 2, c = q % 2;
+                    double s = 0.0;
+                    for (int t = 0; t < BS; ++t) s += Le[r * BS + t] * F[t * FC + 2 * BS + c];
+                    xr[cnt] = s;
+                }
+                __syncwarp();
+                cnt = 0;
+                for (int q = lane; q < BS * BS; q += 32, ++cnt) { De[q] -= dd[cnt]; Le[q] = nl[cnt]; }
+                cnt = 0;
+                for (int q = lane; q < 2 * BS; q += 32, ++cnt) Xe[q] -= xr[cnt];
+            }
+        }
+        __syncthreads();
+    }
+    // the last active block (block 0)
+    if (warp == 0) {
+        for (int e = lane; e < BS * BS; e += 32) G[e] = Db[e];
+        __syncwarp();
+        if (!warp_chol(G) && lane == 0) bad = 1;
+        warp_chol_solve(G, Xb, 2);
+    }
+    __syncthreads();
+    // back substitution: x_o = Fr_o - FL_o x_p - FU_o x_q, coarsest level first
+    for (int lv = levels - 1; lv >= 0; --lv) {
+        const int st = 1 << lv;
+        const int nodd = (nb - st + 2 * st - 1) / (2 * st);
+        for (int m = warp; m < nodd; m += nw) {
+            const int o = st * (2 * m + 1), p = o - st, q2 = o + st;
+            const double *F = Fb + (long long)o * BS * FC;
+            for (int q = lane; q < 2 * BS; q += 32) {
+                const int r = q / 2, c = q % 2;
+                double s = F[r * FC + 2 * BS + c];
+                for (int t = 0; t < BS; ++t) s -= F[r * FC + t] * Xb[2 * ((long long)p * BS + t) + c];
+                if (q2 < nb)
+                    for (int t = 0; t < BS; ++t) s -= F[r * FC + BS + t] * Xb[2 * ((long long)q2 * BS + t) + c];
+                Xb[2 * ((long long)o * BS + r) + c] = s;
+            }
+        }
+        __syncthreads();
+    }
+    for (int s = tid; s < n; s += nt) {
+        a.y[idx[s]] = Xb[2 * s];
+        a.y[n + idx[s]] = Xb[2 * s + 1];
+    }
+    __syncthreads();
+    solve_residual(a, key, idx, reach, wmax, bad);
 }
 
 // du = D^T y over the current patch, 16x16 nodes per CTA, plus FP64 force and
@@ -341,9 +649,8 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
     // force and moment of this node
     double fx = 0, fy = 0, mz = 0;
     const bool in_support = active && wing < (1 << 20);
-    double time;
-    const double *row = motion_row(a, step_index, &time);
     if (in_support) {
+        const double *row = motion_row(a, step_index, nullptr);
         double rho, u, v;
         node_moments<T>(a, gi, gj, rho, u, v);
         const double temp1 = 2.0 * rho * du, temp2 = 2.0 * rho * dv;
@@ -405,6 +712,13 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
     }
 }
 
+size_t solve_smem(int n)
+{
+    int ns = 1;
+    while (ns < n) ns <<= 1;
+    return sizeof(double) * ns + sizeof(int) * 2 * ns + sizeof(double) * 32 * BS * BS;
+}
+
 IBArgs make_args(lbm_handle *h, const void *fin)
 {
     IBArgs a;
@@ -413,11 +727,13 @@ IBArgs make_args(lbm_handle *h, const void *fin)
     a.nx = h->nx; a.ny = h->ny; a.pitch = h->pitch; a.plane = h->plane;
     a.nwing = h->nwing; a.ppw = h->ppw; a.spw = h->spw; a.nseg = h->nseg;
     a.smooth = h->p.delta_kernel;
+    a.force_dense = (h->p.flags & LBM_FLAG_DENSE_SOLVE) != 0;
     a.scale = h->p.scale; a.ox = h->p.ox; a.oy = h->p.oy; a.uu = h->p.uu;
     a.xc = h->p.xc; a.yc = h->p.yc; a.mesh_max_scale = h->p.mesh_max_scale;
     a.xb0 = h->d_xb0; a.yb0 = h->d_yb0; a.arc = h->d_arc;
     a.mstep = h->d_mstep; a.msteps = h->msteps; a.mcols = h->mcols; a.mdt = h->mdt;
     a.mk = h->d_mk; a.rhs = h->d_rhs; a.B = h->d_B; a.y = h->d_y;
+    a.bD = h->d_bD; a.bL = h->d_bL; a.bF = h->d_bF; a.bX = h->d_bX;
     a.pinfo = h->d_pinfo; a.patch = h->d_patch; a.patch_cap = h->patch_cap;
     a.patch_wmax = h->patch_wmax; a.patch_hmax = h->patch_hmax;
     a.partial = h->d_partial; a.counter = h->d_counter;
@@ -431,16 +747,8 @@ int launch_ib_t(lbm_handle *h, const void *fin, int step_index, int ring_slot)
 {
     IBArgs a = make_args(h, fin);
     cudaStream_t st = h->stream;
-    ib_prepare<<<1, 1024, 0, st>>>(a, step_index, ring_slot);
-    if (h->nseg > 0) {
-        ib_interp<T><<<(h->nseg + 7) / 8, 256, 0, st>>>(a);
-        ib_assemble<<<h->nseg, 128, 0, st>>>(a);
-        const size_t base = sizeof(double) * 3 * (size_t)h->nseg;
-        const size_t full = base + sizeof(double) * (size_t)h->nseg * h->nseg;
-        const int use_smem = full <= kSolveSmem;
-        if (base > kSolveSmem) return -1;
-        ib_solve<<<1, 1024, use_smem ? full : base, st>>>(a, use_smem);
-    }
+    if (h->nseg > 0) ib_markers<T><<<(h->nseg + 7) / 8, 256, 0, st>>>(a, step_index);
+    ib_solve<<<1, SOLVE_THREADS, solve_smem(h->nseg), st>>>(a, step_index, ring_slot);
     dim3 grid(h->patch_gx(), h->patch_gy());
     ib_spread<T, C><<<grid, 256, 0, st>>>(a, step_index, ring_slot);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
@@ -448,10 +756,23 @@ int launch_ib_t(lbm_handle *h, const void *fin, int step_index, int ring_slot)
 
 }  // namespace
 
+// scratch sizes of the block cyclic reduction (doubles)
+size_t ib_block_scratch(int nseg, size_t *d, size_t *l, size_t *f, size_t *x)
+{
+    const size_t nb = (size_t)(nseg + BS - 1) / BS;
+    *d = nb * BS * BS;
+    *l = nb * BS * BS;
+    *f = nb * BS * (2 * BS + 2);
+    *x = 2 * nb * BS + 2 * (size_t)nseg;
+    return *d + *l + *f + *x;
+}
+
+int ib_max_markers() { return NSORT_MAX; }
+
 int ib_configure(lbm_handle *h)
 {
-    // ib_solve may need up to kSolveSmem of dynamic shared memory
-    if (cudaFuncSetAttribute(ib_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSolveSmem) != cudaSuccess)
+    if (cudaFuncSetAttribute(ib_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem(NSORT_MAX)) !=
+        cudaSuccess)
         return -1;
     return 0;
 }

@@ -116,20 +116,26 @@ __global__ void __launch_bounds__(256) kf_kernel(const KFArgs<C> a)
         e[6] = -jy;
         e[7] = jx * jx - jy * jy;
         e[8] = jx * jy;
+        // m' = m + s(meq - m) + fp (solution.f90:632-634); the new populations
+        // are taken as g + M^-1 (m' - m), which equals M^-1 m' exactly but
+        // rounds relative to the small non-equilibrium update, not to g
+        C d[9];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) m[k] = m[k] + (e[k] - m[k]) * a.s[k];
+        for (int k = 0; k < 9; ++k) d[k] = (e[k] - m[k]) * a.s[k];
         if (gx != C(0) || gy != C(0)) {        // :614-626
             const C ug = u * gx + v * gy;
-            m[1] += C(6) * (C(1) - C(0.5) * a.s[1]) * ug;
-            m[2] += C(-6) * (C(1) - C(0.5) * a.s[2]) * ug;
-            m[3] += gx;
-            m[4] += -(C(1) - C(0.5) * a.s[4]) * gx;
-            m[5] += gy;
-            m[6] += -(C(1) - C(0.5) * a.s[6]) * gy;
-            m[7] += C(2) * (C(1) - C(0.5) * a.s[7]) * (u * gx - v * gy);
-            m[8] += (C(1) - C(0.5) * a.s[8]) * (u * gy + v * gx);
+            d[1] += C(6) * (C(1) - C(0.5) * a.s[1]) * ug;
+            d[2] += C(-6) * (C(1) - C(0.5) * a.s[2]) * ug;
+            d[3] += gx;
+            d[4] += -(C(1) - C(0.5) * a.s[4]) * gx;
+            d[5] += gy;
+            d[6] += -(C(1) - C(0.5) * a.s[6]) * gy;
+            d[7] += C(2) * (C(1) - C(0.5) * a.s[7]) * (u * gx - v * gy);
+            d[8] += (C(1) - C(0.5) * a.s[8]) * (u * gy + v * gx);
         }
-        mrt_inverse(m, gout);
+        mrt_inverse(d, gout);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) gout[k] += g[k];
         frho = rho; fu = u; fv = v;
     } else {
         C g0n[9], drn, un, vn;

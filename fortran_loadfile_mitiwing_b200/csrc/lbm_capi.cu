@@ -112,6 +112,15 @@ void lookup_row(const std::vector<double> &tab, int rows, int cols, double t, in
     row[0] = t;
 }
 
+// releases the immersed-boundary scratch (sizes depend on geometry and motion)
+void free_ib(lbm_handle *h)
+{
+    h->ib_ready = 0;
+    free_dev(h->d_patch);
+    free_devp(h->d_mk); free_devp(h->d_rhs); free_devp(h->d_B); free_devp(h->d_y); free_devp(h->d_partial);
+    free_devp(h->d_bD); free_devp(h->d_bL); free_devp(h->d_bF); free_devp(h->d_bX);
+}
+
 // Allocates the immersed-boundary scratch once geometry and motion are known:
 // the correction patch is sized by the largest per-step rectangle of the
 // bodies' bounding discs over the whole motion table.
@@ -153,6 +162,12 @@ int ensure_ib(lbm_handle *h)
     CK(cudaMalloc(&h->d_rhs, sizeof(double) * 2 * ns), "alloc rhs");
     CK(cudaMalloc(&h->d_y, sizeof(double) * 2 * ns), "alloc y");
     CK(cudaMalloc(&h->d_B, sizeof(double) * (size_t)ns * ns), "alloc B");
+    size_t sd, sl, sf, sx;
+    ib_block_scratch(ns, &sd, &sl, &sf, &sx);
+    CK(cudaMalloc(&h->d_bD, sizeof(double) * sd), "alloc block D");
+    CK(cudaMalloc(&h->d_bL, sizeof(double) * sl), "alloc block L");
+    CK(cudaMalloc(&h->d_bF, sizeof(double) * sf), "alloc block F");
+    CK(cudaMalloc(&h->d_bX, sizeof(double) * sx), "alloc block X");
     const int nblk = h->patch_gx() * h->patch_gy();
     CK(cudaMalloc(&h->d_partial, sizeof(double) * 3 * LBM_MAXW * (size_t)nblk), "alloc partials");
     if (ib_configure(h) != 0) return set_err(h, LBM_ERR_CUDA, "ib_configure failed");
@@ -284,7 +299,8 @@ int lbm_create(const lbm_params *p, lbm_t **out)
     *out = nullptr;
     if (p->nx < 16 || p->ny < 16 || p->wing_count < 0 || p->wing_count > LBM_MAXW ||
         (p->wing_count > 0 && p->points_per_wing < 3) || !(p->scale > 0) || !(p->uu > 0) || !(p->re > 0) ||
-        p->precision < 0 || p->precision > 3 || p->delta_kernel < 0 || p->delta_kernel > 1 || p->flags != 0)
+        p->precision < 0 || p->precision > 3 || p->delta_kernel < 0 || p->delta_kernel > 1 || (p->flags & ~LBM_FLAG_DENSE_SOLVE) != 0 ||
+        (long long)p->wing_count * (p->points_per_wing - 1) > ib_max_markers())
         return LBM_ERR_ARG;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return LBM_ERR_CUDA;
@@ -334,13 +350,13 @@ int lbm_create(const lbm_params *p, lbm_t **out)
     if ((e = cudaMalloc(&h->d_counter, sizeof(unsigned))) != cudaSuccess) return fail(e, "alloc counter");
     if ((e = cudaMalloc(&h->d_pinfo, sizeof(PatchInfo))) != cudaSuccess) return fail(e, "alloc pinfo");
     if ((e = cudaMalloc(&h->d_red, sizeof(double) * 2 * 296)) != cudaSuccess) return fail(e, "alloc red");
-    if ((e = cudaMalloc(&h->d_solve_res, sizeof(double))) != cudaSuccess) return fail(e, "alloc res");
+    if ((e = cudaMalloc(&h->d_solve_res, 2 * sizeof(double))) != cudaSuccess) return fail(e, "alloc res");
     if ((e = cudaMalloc(&h->d_ring, sizeof(double) * h->row_len * (size_t)h->ring_cap)) != cudaSuccess)
         return fail(e, "alloc ring");
     cudaMemset(h->d_status, 0, sizeof(unsigned));
     cudaMemset(h->d_counter, 0, sizeof(unsigned));
     cudaMemset(h->d_pinfo, 0, sizeof(PatchInfo));
-    cudaMemset(h->d_solve_res, 0, sizeof(double));
+    cudaMemset(h->d_solve_res, 0, 2 * sizeof(double));
     if (h->npts > 0) {
         if ((e = cudaMalloc(&h->d_xb0, sizeof(double) * h->npts)) != cudaSuccess) return fail(e, "alloc xb0");
         if ((e = cudaMalloc(&h->d_yb0, sizeof(double) * h->npts)) != cudaSuccess) return fail(e, "alloc yb0");
@@ -358,8 +374,8 @@ int lbm_destroy(lbm_t *h)
     for (int b = 0; b < 2; ++b) { free_dev(h->fbuf[b]); free_dev(h->d_fields[b]); }
     free_dev(h->edge_c);
     free_devp(h->d_xb0); free_devp(h->d_yb0); free_devp(h->d_arc); free_devp(h->d_mstep);
-    free_devp(h->d_mk); free_devp(h->d_rhs); free_devp(h->d_B); free_devp(h->d_y);
-    free_devp(h->d_pinfo); free_dev(h->d_patch); free_devp(h->d_partial); free_devp(h->d_counter);
+    free_ib(h);
+    free_devp(h->d_pinfo); free_devp(h->d_counter);
     free_devp(h->d_ring); free_devp(h->d_status); free_devp(h->d_solve_res); free_devp(h->d_red);
     free_devp(h->d_stage);
     for (auto &e : h->ev) cudaEventDestroy(e);
@@ -393,9 +409,7 @@ int lbm_set_boundary(lbm_t *h, int wing, const double *x, const double *y, int n
     CK(cudaMemcpyAsync(h->d_arc + ss, h->harc.data() + ss, sizeof(double) * h->spw, cudaMemcpyHostToDevice, h->stream), "copy arc");
     CK(cudaStreamSynchronize(h->stream), "sync boundary");
     h->have_wing[wing - 1] = 1;
-    h->ib_ready = 0;
-    free_dev(h->d_patch);
-    free_devp(h->d_mk); free_devp(h->d_rhs); free_devp(h->d_B); free_devp(h->d_y); free_devp(h->d_partial);
+    free_ib(h);
     return LBM_OK;
 }
 
@@ -427,9 +441,7 @@ int lbm_set_motion_table(lbm_t *h, const double *table, int rows, int cols)
     CK(cudaMemcpyAsync(h->d_mstep, h->mstep_host.data(), sizeof(double) * h->mstep_host.size(),
                        cudaMemcpyHostToDevice, h->stream), "copy step table");
     CK(cudaStreamSynchronize(h->stream), "sync motion");
-    h->ib_ready = 0;
-    free_dev(h->d_patch);
-    free_devp(h->d_mk); free_devp(h->d_rhs); free_devp(h->d_B); free_devp(h->d_y); free_devp(h->d_partial);
+    free_ib(h);
     return LBM_OK;
 }
 
@@ -593,20 +605,21 @@ int lbm_residual(lbm_t *h, double *err)
     return LBM_OK;
 }
 
-int lbm_get_markers(lbm_t *h, double *xb2, double *yb2, double *solve_residual)
+int lbm_get_markers(lbm_t *h, double *xb2, double *yb2, double *solve_residual, int *half_bandwidth)
 {
     if (!h) return LBM_ERR_ARG;
     if (!h->ib_ready || h->nseg == 0) return set_err(h, LBM_ERR_STATE, "get_markers: no immersed boundary step run");
     std::vector<Marker> mk(h->nseg);
     CK(cudaMemcpyAsync(mk.data(), h->d_mk, sizeof(Marker) * h->nseg, cudaMemcpyDeviceToHost, h->stream), "copy markers");
-    double res = 0;
-    CK(cudaMemcpyAsync(&res, h->d_solve_res, sizeof(double), cudaMemcpyDeviceToHost, h->stream), "copy res");
+    double res[2] = {0, 0};
+    CK(cudaMemcpyAsync(res, h->d_solve_res, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "copy res");
     CK(cudaStreamSynchronize(h->stream), "sync markers");
     for (int k = 0; k < h->nseg; ++k) {
         if (xb2) xb2[k] = mk[k].xm;
         if (yb2) yb2[k] = mk[k].ym;
     }
-    if (solve_residual) *solve_residual = res;
+    if (solve_residual) *solve_residual = res[0];
+    if (half_bandwidth) *half_bandwidth = (int)res[1];
     return LBM_OK;
 }
 

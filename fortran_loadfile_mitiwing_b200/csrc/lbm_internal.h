@@ -40,6 +40,7 @@ struct IBArgs {
     long long plane;
     int nwing, ppw, spw, nseg;
     int smooth;
+    int force_dense;    // LBM_FLAG_DENSE_SOLVE
     double scale, ox, oy, uu, xc, yc, mesh_max_scale;
     const double *xb0, *yb0, *arc;
     const double *mstep;  // step table, row-major [msteps][mcols]
@@ -49,6 +50,8 @@ struct IBArgs {
     double *rhs;        // [2*nseg]
     double *B;          // [nseg*nseg], row-major
     double *y;          // [2*nseg]
+    double *bD, *bL, *bF, *bX;  // block cyclic reduction scratch (diagonal, lower,
+                                // eliminated-block factors, right-hand sides)
     PatchInfo *pinfo;
     void *patch;        // compute-precision (du, dv) pairs
     int patch_cap;      // nodes
@@ -89,6 +92,7 @@ struct lbm_handle {
     // immersed boundary scratch
     Marker *d_mk = nullptr;
     double *d_rhs = nullptr, *d_B = nullptr, *d_y = nullptr;
+    double *d_bD = nullptr, *d_bL = nullptr, *d_bF = nullptr, *d_bX = nullptr;
     PatchInfo *d_pinfo = nullptr;
     void *d_patch = nullptr;
     int patch_cap = 0;               // nodes
@@ -123,6 +127,8 @@ struct lbm_handle {
 
 // kernel launchers (kf_kernel.cu, ib_kernels.cu)
 int ib_configure(lbm_handle *h);
+int ib_max_markers();
+size_t ib_block_scratch(int nseg, size_t *d, size_t *l, size_t *f, size_t *x);
 int launch_kf(lbm_handle *h, const void *fin, void *fout, void *fields);
 int launch_ib(lbm_handle *h, const void *fin, int step_index, int ring_slot);
 int launch_residual(lbm_handle *h, const void *fa, const void *fb, double *out2);

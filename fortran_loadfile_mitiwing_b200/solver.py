@@ -124,10 +124,16 @@ class Lbm:
         return e.value
 
     def markers(self):
+        """(xb2, yb2, solve residual) of the last step."""
+        x, y, r, _ = self.solver_info()
+        return x, y, r
+
+    def solver_info(self):
+        """(xb2, yb2, solve residual, half-bandwidth of the marker system)."""
         n = self.params.wing_count * (self.params.points_per_wing - 1)
-        x, y, r = np.zeros(n), np.zeros(n), C.c_double()
-        self._ck(self.lib.lbm_get_markers(self.h, dptr(x), dptr(y), C.byref(r)))
-        return x, y, r.value
+        x, y, r, w = np.zeros(n), np.zeros(n), C.c_double(), C.c_int()
+        self._ck(self.lib.lbm_get_markers(self.h, dptr(x), dptr(y), C.byref(r), C.byref(w)))
+        return x, y, r.value, w.value
 
     @property
     def step_index(self):

@@ -55,6 +55,11 @@ extern "C" {
 #define LBM_PREC_FP16  2
 #define LBM_PREC_BF16  3
 
+/* flags: solve the marker system with the dense Cholesky even when it is
+ * banded (the path the solver otherwise takes only for couplings that reach
+ * past the neighbouring 16-marker block); for verification */
+#define LBM_FLAG_DENSE_SOLVE 1
+
 /* discrete delta kernel (boundary_condition.f90:1530, 1563-1600) */
 #define LBM_DELTA_PESKIN4  0   /* smooth=0: 4-point Peskin, support |r|<2   */
 #define LBM_DELTA_SMOOTH   1   /* smooth=1: smoothed kernel, support |r|<=2.5 */
@@ -68,7 +73,7 @@ typedef struct lbm_params {
     int32_t points_per_wing;   /* boundary_points_per_wing (main.f90:21); closed contour */
     int32_t delta_kernel;      /* LBM_DELTA_*; the reference hard-codes smooth=1 */
     int32_t precision;         /* LBM_PREC_* */
-    int32_t flags;             /* reserved, must be 0 */
+    int32_t flags;             /* LBM_FLAG_* bits, else 0 */
     int32_t reserved;
     double scale;              /* mesh%scale: lattice spacing in chords (1/chord_lu) */
     double ox, oy;             /* mesh%ox, mesh%oy: physical position of node (1,1) */
@@ -174,9 +179,11 @@ LBM_API int lbm_set_populations(lbm_t *h, const double *f);
 LBM_API int lbm_residual(lbm_t *h, double *err);
 
 /* immersed-boundary diagnostics of the last step: marker midpoints xb2,yb2
- * (n = wing_count*(points_per_wing-1) each, nullable) and the relative
- * residual ||A x - rhs|| / ||rhs|| of the solve (nullable). */
-LBM_API int lbm_get_markers(lbm_t *h, double *xb2, double *yb2, double *solve_residual);
+ * (airfoil.f90:267-270; n = wing_count*(points_per_wing-1) each), the
+ * relative residual ||B y - rhs|| / ||rhs|| of the marker system solve, and
+ * the half-bandwidth of B in the marker order the solver used (above 16 the
+ * banded solver hands over to a dense Cholesky). Every pointer is nullable. */
+LBM_API int lbm_get_markers(lbm_t *h, double *xb2, double *yb2, double *solve_residual, int *half_bandwidth);
 
 /* Device timing of the step loop, the CUDA-event analogue of the driver's
  * per-phase cpu_time totals (main.f90:355-369, 420-433). With timing on,
