@@ -52,6 +52,18 @@ def dist_setup(args):
     return world, rank, local
 
 
+def replica_value(local_ms, nodes, steps, world, device="cuda"):
+    """Whole-job MLUPS of `world` independent replicas: every rank updated
+    nodes*steps lattice nodes; the job time is the slowest rank's device time
+    (max over ranks). Returns (value, max_ms). The max is the only collective."""
+    import torch
+    t = torch.tensor([float(local_ms)], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    tmax = float(t.item())
+    return nodes * steps * world / (tmax / 1e3) / 1e6, tmax
+
+
 def large_case(args, n_steps, precision=None):
     from fortran_loadfile_mitiwing_b200 import cases
     if (args.nx, args.ny) == (4096, 2048):
@@ -222,12 +234,8 @@ def run_ours(args, world, rank, local):
     lib.lbm_get_timing(s.h, C.byref(step_ms), C.byref(ib_ms), C.byref(kf_ms), C.byref(nt))
     assert nt.value == k and rows.shape[0] == k, (nt.value, rows.shape)
     assert np.all(np.isfinite(rows))
-    t = torch.tensor([step_ms.value], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    tmax_ms = float(t.item())
     nn = args.nx * args.ny
-    value = nn * k * world / (tmax_ms / 1e3) / 1e6
+    value, tmax_ms = replica_value(step_ms.value, nn, k, world)
     elem = {"fp32": 4, "fp64": 8, "fp16": 2, "bf16": 2}[args.precision]
     bpl = 18 * elem
     kf_avg_s = kf_ms.value / k / 1e3

@@ -32,6 +32,9 @@ namespace {
 constexpr int BS = 16;                 // cyclic-reduction block size
 constexpr int NSORT_MAX = 4096;        // largest marker count (sort in shared memory)
 constexpr int SOLVE_THREADS = 1024;
+constexpr int BOPS_WARPS = 16;             // warps running block operations
+constexpr int FC = 2 * BS + 2;             // columns of F: [D^-1 L | D^-1 U | D^-1 r]
+constexpr int WS = BS * BS + BS * FC + BS * BS + 2 * BS;   // workspace per warp (doubles)
 
 // one-axis kernel value (boundary_condition.f90:1563-1600), disr = |r|
 __device__ __forceinline__ double delta1(double disr, int smooth)
@@ -302,31 +305,12 @@ __device__ void dense_solve(const IBArgs &a, const Marker *mk, double *yv, int *
     }
 }
 
-// relative residual ||B y - rhs|| / ||rhs|| of both right-hand sides over the
-// sorted band (couplings exist only within `reach`), written with the
-// half-bandwidth; a residual above 1e-6 or a failed factorisation flags the
-// step as a solver failure
-__device__ void solve_residual(const IBArgs &a, const double *key, const int *idx, double reach, int wmax, int bad)
+// block reduction of the residual sums; writes the relative residual and the
+// half-bandwidth, and flags a failed factorisation or a residual above 1e-6
+__device__ void finish_residual(const IBArgs &a, double num, double den, int wmax, int bad)
 {
-    const int n = a.nseg, tid = threadIdx.x, nt = blockDim.x;
-    const int lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     __shared__ double wr[32][2];
-    double num = 0.0, den = 0.0;
-    for (int s = tid; s < n; s += nt) {
-        const int k = idx[s];
-        double b0 = 0.0, b1 = 0.0;
-        int t = s;
-        while (t > 0 && key[s] - key[t - 1] <= reach) --t;
-        for (; t < n && key[t] - key[s] <= reach; ++t) {
-            const int l = idx[t];
-            const double b = bval(a.mk[k], a.mk[l]);
-            b0 += b * a.y[l];
-            b1 += b * a.y[n + l];
-        }
-        const double r0 = b0 - a.rhs[k], r1 = b1 - a.rhs[n + k];
-        num += r0 * r0 + r1 * r1;
-        den += a.rhs[k] * a.rhs[k] + a.rhs[n + k] * a.rhs[n + k];
-    }
     for (int off = 16; off; off >>= 1) {
         num += __shfl_xor_sync(0xffffffffu, num, off);
         den += __shfl_xor_sync(0xffffffffu, den, off);
@@ -343,9 +327,36 @@ __device__ void solve_residual(const IBArgs &a, const double *key, const int *id
     }
 }
 
+// relative residual ||B y - rhs|| / ||rhs|| of both right-hand sides over the
+// sorted band (couplings exist only within `reach`), written with the
+// half-bandwidth; a residual above 1e-6 or a failed factorisation flags the
+// step as a solver failure
+__device__ void solve_residual(const IBArgs &a, const double *key, const int *idx, double reach, int wmax, int bad)
+{
+    const int n = a.nseg, tid = threadIdx.x, nt = blockDim.x;
+    double num = 0.0, den = 0.0;
+    for (int s = tid; s < n; s += nt) {
+        const int k = idx[s];
+        double b0 = 0.0, b1 = 0.0;
+        int t = s;
+        while (t > 0 && key[s] - key[t - 1] <= reach) --t;
+        for (; t < n && key[t] - key[s] <= reach; ++t) {
+            const int l = idx[t];
+            const double b = bval(a.mk[k], a.mk[l]);
+            b0 += b * a.y[l];
+            b1 += b * a.y[n + l];
+        }
+        const double r0 = b0 - a.rhs[k], r1 = b1 - a.rhs[n + k];
+        num += r0 * r0 + r1 * r1;
+        den += a.rhs[k] * a.rhs[k] + a.rhs[n + k] * a.rhs[n + k];
+    }
+    finish_residual(a, num, den, wmax, bad);
+}
+
 // The linear solve of one step, one CTA of SOLVE_THREADS threads.
 // Dynamic shared memory: key[ns] (double), idx[ns] (int, then ns ints of
-// padding), G[32][BS*BS] (double), ns = n rounded up to a power of two.
+// padding), then one block-operation workspace of WS doubles for each of the
+// first BOPS_WARPS warps; ns = n rounded up to a power of two.
 __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int step_index, int ring_slot)
 {
     extern __shared__ double smem[];
@@ -355,7 +366,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
     while (ns < n) ns <<= 1;
     double *key = smem;
     int *idx = (int *)(key + ns);
-    double *G = (double *)(idx + 2 * ns) + warp * BS * BS;
+    double *Wbase = (double *)(idx + 2 * ns);
     __shared__ int bb[4];
     __shared__ double ext[4];
     __shared__ int wmax, bad;
@@ -453,18 +464,22 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
         return;
     }
     // block tridiagonal form: D_i (BS x BS), L_i couples block i to block i-1,
-    // X_i holds the two right-hand sides (BS x 2), padded with identity rows
+    // X_i holds the two right-hand sides (BS x 2), padded with identity rows;
+    // D0/L0 keep the assembled blocks for the residual
     const int nb = (n + BS - 1) / BS;
     double *Db = a.bD, *Lb = a.bL, *Fb = a.bF, *Xb = a.bX;
-    const int FC = 2 * BS + 2;   // columns of F: [D^-1 L | D^-1 U | D^-1 r]
+    double *D0 = a.bD + (long long)nb * BS * BS, *L0 = a.bL + (long long)nb * BS * BS;
     for (long long q = tid; q < (long long)nb * BS * BS; q += nt) {
         const int blk = (int)(q / (BS * BS)), r = (int)(q % (BS * BS)) / BS, c = (int)(q % BS);
         const int sr = blk * BS + r, sc = blk * BS + c, sp = (blk - 1) * BS + c;
         double d;
         if (sr < n && sc < n) d = bval(mk[idx[sr]], mk[idx[sc]]);
         else d = (r == c) ? 1.0 : 0.0;
+        const double l = (blk > 0 && sr < n) ? bval(mk[idx[sr]], mk[idx[sp]]) : 0.0;
         Db[q] = d;
-        Lb[q] = (blk > 0 && sr < n) ? bval(mk[idx[sr]], mk[idx[sp]]) : 0.0;
+        D0[q] = d;
+        Lb[q] = l;
+        L0[q] = l;
     }
     for (int q = tid; q < nb * BS; q += nt) {
         Xb[2 * q] = q < n ? a.rhs[idx[q]] : 0.0;
@@ -472,91 +487,107 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
     }
     __syncthreads();
     // cyclic reduction: at stride st the active blocks are multiples of st;
-    // odd multiples are eliminated into their even neighbours
+    // odd multiples are eliminated into their even neighbours. Each block
+    // operation runs on one warp in its shared-memory workspace W.
+    double *W = Wbase + (long long)warp * WS;
+    const bool bw = warp < BOPS_WARPS;
     int levels = 0;
     for (int st = 1; st < nb; st <<= 1, ++levels) {
         const int nodd = (nb - st + 2 * st - 1) / (2 * st);
-        for (int m = warp; m < nodd; m += nw) {
-            const int o = st * (2 * m + 1), q2 = o + st;
-            double *F = Fb + (long long)o * BS * FC;
-            for (int e = lane; e < BS * BS; e += 32) G[e] = Db[(long long)o * BS * BS + e];
-            for (int e = lane; e < BS * FC; e += 32) {
-                const int r = e / FC, c = e % FC;
-                double v;
-                if (c < BS) v = Lb[(long long)o * BS * BS + r * BS + c];                          // L_o
-                else if (c < 2 * BS) v = q2 < nb ? Lb[(long long)q2 * BS * BS + (c - BS) * BS + r] : 0.0;  // U_o = L_q^T
-                else v = Xb[2 * ((long long)o * BS + r) + (c - 2 * BS)];                          // r_o
-                F[e] = v;
-            }
-            __syncwarp();
-            if (!warp_chol(G) && lane == 0) bad = 1;
-            warp_chol_solve(G, F, FC);
-        }
-        __syncthreads();
-        const int neven = (nb + 2 * st - 1) / (2 * st);
-        for (int m = warp; m < neven; m += nw) {
-            const int e = 2 * st * m, o1 = e - st, o2 = e + st;
-            double *De = Db + (long long)e * BS * BS, *Le = Lb + (long long)e * BS * BS;
-            double *Xe = Xb + 2 * (long long)e * BS;
-            // right neighbour o2 (e is its previous block): D_e -= L_o2^T FL_o2, r_e -= L_o2^T Fr_o2
-            if (o2 < nb) {
-                const double *Lo = Lb + (long long)o2 * BS * BS;
-                const double *F = Fb + (long long)o2 * BS * FC;
-                for (int q = lane; q < BS * BS + 2 * BS; q += 32) {
-                    double s = 0.0;
-                    if (q < BS * BS) {
-                        const int r = q / BS, c = q % BS;
-                        for (int t = 0; t < BS; ++t) s += Lo[t * BS + r] * F[t * FC + c];
-                        De[q] -= s;
-                    } else {
-                        const int r = (q - BS * BS) / 2, c = (q - BS * BS) % 2;
-                        for (int t = 0; t < BS; ++t) s += Lo[t * BS + r] * F[t * FC + 2 * BS + c];
-                        Xe[2 * r + c] -= s;
-                    }
-                }
-            }
-            __syncwarp();
-            // left neighbour o1 (e is its next block): D_e -= L_e FU_o1,
-            // r_e -= L_e Fr_o1, new L_e = -L_e FL_o1
-            if (m > 0) {
-                const double *F = Fb + (long long)o1 * BS * FC;
-                double nl[(BS * BS + 31) / 32];
-                double dd[(BS * BS + 31) / 32];
-                double xr[(2 * BS + 31) / 32];
-                int cnt = 0;
-                for (int q = lane; q < BS * BS; q += 32, ++cnt) {
-                    const int r = q / BS, c = q % BS;
-                    double s1 = 0.0, s2 = 0.0;
-                    for (int t = 0; t < BS; ++t) {
-                        const double l = Le[r * BS + t];
-                        s1 += l * F[t * FC + BS + c];
-                        s2 += l * F[t * FC + c];
-                    }
-                    dd[cnt] = s1;
-                    nl[cnt] = -s2;
-                }
-                cnt = 0;
-                for (int q = lane; q < 2 * BS; q += 32, ++cnt) {
-                    const int r = q / 2, c = q % 2;
-                    double s = 0.0;
-                    for (int t = 0; t < BS; ++t) s += Le[r * BS + t] * F[t * FC + 2 * BS + c];
-                    xr[cnt] = s;
+        if (bw)
+            for (int m = warp; m < nodd; m += BOPS_WARPS) {
+                const int o = st * (2 * m + 1), q2 = o + st;
+                double *Gs = W, *Fs = W + BS * BS;
+                for (int e = lane; e < BS * BS; e += 32) Gs[e] = Db[(long long)o * BS * BS + e];
+                for (int e = lane; e < BS * FC; e += 32) {
+                    const int r = e / FC, c = e % FC;
+                    double v;
+                    if (c < BS) v = Lb[(long long)o * BS * BS + r * BS + c];                      // L_o
+                    else if (c < 2 * BS) v = q2 < nb ? Lb[(long long)q2 * BS * BS + (c - BS) * BS + r] : 0.0;  // U_o = L_q^T
+                    else v = Xb[2 * ((long long)o * BS + r) + (c - 2 * BS)];                      // r_o
+                    Fs[e] = v;
                 }
                 __syncwarp();
-                cnt = 0;
-                for (int q = lane; q < BS * BS; q += 32, ++cnt) { De[q] -= dd[cnt]; Le[q] = nl[cnt]; }
-                cnt = 0;
-                for (int q = lane; q < 2 * BS; q += 32, ++cnt) Xe[q] -= xr[cnt];
+                if (!warp_chol(Gs) && lane == 0) bad = 1;
+                warp_chol_solve(Gs, Fs, FC);
+                double *F = Fb + (long long)o * BS * FC;
+                for (int e = lane; e < BS * FC; e += 32) F[e] = Fs[e];
+                __syncwarp();
             }
-        }
+        __syncthreads();
+        const int neven = (nb + 2 * st - 1) / (2 * st);
+        if (bw)
+            for (int m = warp; m < neven; m += BOPS_WARPS) {
+                const int e = 2 * st * m, o1 = e - st, o2 = e + st;
+                double *As = W, *Fs = W + BS * BS, *Ds = Fs + BS * FC, *Xs = Ds + BS * BS;
+                double *De = Db + (long long)e * BS * BS, *Le = Lb + (long long)e * BS * BS;
+                double *Xe = Xb + 2 * (long long)e * BS;
+                for (int q = lane; q < BS * BS; q += 32) Ds[q] = De[q];
+                for (int q = lane; q < 2 * BS; q += 32) Xs[q] = Xe[q];
+                // right neighbour o2 (e is its previous block):
+                // D_e -= L_o2^T FL_o2, r_e -= L_o2^T Fr_o2
+                if (o2 < nb) {
+                    const double *Lo = Lb + (long long)o2 * BS * BS;
+                    const double *F = Fb + (long long)o2 * BS * FC;
+                    for (int q = lane; q < BS * BS; q += 32) As[q] = Lo[q];
+                    for (int q = lane; q < BS * FC; q += 32) Fs[q] = F[q];
+                    __syncwarp();
+                    for (int q = lane; q < BS * BS + 2 * BS; q += 32) {
+                        double sum = 0.0;
+                        if (q < BS * BS) {
+                            const int r = q / BS, c = q % BS;
+                            for (int t = 0; t < BS; ++t) sum += As[t * BS + r] * Fs[t * FC + c];
+                            Ds[q] -= sum;
+                        } else {
+                            const int r = (q - BS * BS) / 2, c = (q - BS * BS) % 2;
+                            for (int t = 0; t < BS; ++t) sum += As[t * BS + r] * Fs[t * FC + 2 * BS + c];
+                            Xs[2 * r + c] -= sum;
+                        }
+                    }
+                    __syncwarp();
+                }
+                // left neighbour o1 (e is its next block): D_e -= L_e FU_o1,
+                // r_e -= L_e Fr_o1, new L_e = -L_e FL_o1
+                if (m > 0) {
+                    const double *F = Fb + (long long)o1 * BS * FC;
+                    for (int q = lane; q < BS * BS; q += 32) As[q] = Le[q];
+                    for (int q = lane; q < BS * FC; q += 32) Fs[q] = F[q];
+                    __syncwarp();
+                    for (int q = lane; q < BS * BS + 2 * BS; q += 32) {
+                        if (q < BS * BS) {
+                            const int r = q / BS, c = q % BS;
+                            double s1 = 0.0, s2 = 0.0;
+                            for (int t = 0; t < BS; ++t) {
+                                const double l = As[r * BS + t];
+                                s1 += l * Fs[t * FC + BS + c];
+                                s2 += l * Fs[t * FC + c];
+                            }
+                            Ds[q] -= s1;
+                            Le[q] = -s2;
+                        } else {
+                            const int r = (q - BS * BS) / 2, c = (q - BS * BS) % 2;
+                            double sum = 0.0;
+                            for (int t = 0; t < BS; ++t) sum += As[r * BS + t] * Fs[t * FC + 2 * BS + c];
+                            Xs[2 * r + c] -= sum;
+                        }
+                    }
+                    __syncwarp();
+                }
+                for (int q = lane; q < BS * BS; q += 32) De[q] = Ds[q];
+                for (int q = lane; q < 2 * BS; q += 32) Xe[q] = Xs[q];
+                __syncwarp();
+            }
         __syncthreads();
     }
     // the last active block (block 0)
     if (warp == 0) {
-        for (int e = lane; e < BS * BS; e += 32) G[e] = Db[e];
+        double *Gs = W, *Fs = W + BS * BS;
+        for (int e = lane; e < BS * BS; e += 32) Gs[e] = Db[e];
+        for (int e = lane; e < 2 * BS; e += 32) Fs[e] = Xb[e];
         __syncwarp();
-        if (!warp_chol(G) && lane == 0) bad = 1;
-        warp_chol_solve(G, Xb, 2);
+        if (!warp_chol(Gs) && lane == 0) bad = 1;
+        warp_chol_solve(Gs, Fs, 2);
+        for (int e = lane; e < 2 * BS; e += 32) Xb[e] = Fs[e];
     }
     __syncthreads();
     // back substitution: x_o = Fr_o - FL_o x_p - FU_o x_q, coarsest level first
@@ -568,11 +599,11 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
             const double *F = Fb + (long long)o * BS * FC;
             for (int q = lane; q < 2 * BS; q += 32) {
                 const int r = q / 2, c = q % 2;
-                double s = F[r * FC + 2 * BS + c];
-                for (int t = 0; t < BS; ++t) s -= F[r * FC + t] * Xb[2 * ((long long)p * BS + t) + c];
+                double sum = F[r * FC + 2 * BS + c];
+                for (int t = 0; t < BS; ++t) sum -= F[r * FC + t] * Xb[2 * ((long long)p * BS + t) + c];
                 if (q2 < nb)
-                    for (int t = 0; t < BS; ++t) s -= F[r * FC + BS + t] * Xb[2 * ((long long)q2 * BS + t) + c];
-                Xb[2 * ((long long)o * BS + r) + c] = s;
+                    for (int t = 0; t < BS; ++t) sum -= F[r * FC + BS + t] * Xb[2 * ((long long)q2 * BS + t) + c];
+                Xb[2 * ((long long)o * BS + r) + c] = sum;
             }
         }
         __syncthreads();
@@ -581,8 +612,25 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
         a.y[idx[s]] = Xb[2 * s];
         a.y[n + idx[s]] = Xb[2 * s + 1];
     }
-    __syncthreads();
-    solve_residual(a, key, idx, reach, wmax, bad);
+    // residual ||B y - rhs|| / ||rhs|| with the assembled blocks
+    double num = 0.0, den = 0.0;
+    for (int s = tid; s < n; s += nt) {
+        const int i = s / BS, r = s % BS;
+        double acc[2];
+        for (int c = 0; c < 2; ++c) {
+            double sum = 0.0;
+            for (int t = 0; t < BS; ++t) sum += D0[((long long)i * BS + r) * BS + t] * Xb[2 * ((long long)i * BS + t) + c];
+            if (i > 0)
+                for (int t = 0; t < BS; ++t) sum += L0[((long long)i * BS + r) * BS + t] * Xb[2 * ((long long)(i - 1) * BS + t) + c];
+            if (i + 1 < nb)
+                for (int t = 0; t < BS; ++t) sum += L0[((long long)(i + 1) * BS + t) * BS + r] * Xb[2 * ((long long)(i + 1) * BS + t) + c];
+            acc[c] = sum;
+        }
+        const double b0 = a.rhs[idx[s]], b1 = a.rhs[n + idx[s]];
+        num += (acc[0] - b0) * (acc[0] - b0) + (acc[1] - b1) * (acc[1] - b1);
+        den += b0 * b0 + b1 * b1;
+    }
+    finish_residual(a, num, den, wmax, bad);
 }
 
 // du = D^T y over the current patch, 16x16 nodes per CTA, plus FP64 force and
@@ -687,16 +735,30 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
     __syncthreads();
     if (!amlast) return;
     __threadfence();
+    // last block: every thread sums a fixed strided subset of the block
+    // partials, then a fixed warp/block tree (deterministic order)
+    for (int w = 0; w < a.nwing; ++w) {
+        double s0 = 0, s1 = 0, s2 = 0;
+        for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+            const double *p = a.partial + (long long)b * 3 * LBM_MAXW + 3 * w;
+            s0 += __ldcg(p); s1 += __ldcg(p + 1); s2 += __ldcg(p + 2);
+        }
+#pragma unroll
+        for (int off = 16; off; off >>= 1) {
+            s0 += __shfl_down_sync(0xffffffffu, s0, off);
+            s1 += __shfl_down_sync(0xffffffffu, s1, off);
+            s2 += __shfl_down_sync(0xffffffffu, s2, off);
+        }
+        if (lane == 0) { red[warp][3 * w] = s0; red[warp][3 * w + 1] = s1; red[warp][3 * w + 2] = s2; }
+    }
+    __syncthreads();
     if (threadIdx.x == 0) {
         double *fr = a.force_ring + (long long)ring_slot * a.row_len;
         double tot[3] = {0, 0, 0};
         const double uu = a.uu, scale = a.scale;
         for (int w = 0; w < a.nwing; ++w) {
             double s0 = 0, s1 = 0, s2 = 0;
-            for (int b = 0; b < nblk; ++b) {
-                const double *p = a.partial + (long long)b * 3 * LBM_MAXW + 3 * w;
-                s0 += __ldcg(p); s1 += __ldcg(p + 1); s2 += __ldcg(p + 2);
-            }
+            for (int w8 = 0; w8 < 8; ++w8) { s0 += red[w8][3 * w]; s1 += red[w8][3 * w + 1]; s2 += red[w8][3 * w + 2]; }
             // solution.f90:327-330
             const double cx = 2.0 * s0 / (uu * uu * (1.0 / scale));
             const double cy = 2.0 * s1 / (uu * uu * (1.0 / scale));
@@ -716,7 +778,7 @@ size_t solve_smem(int n)
 {
     int ns = 1;
     while (ns < n) ns <<= 1;
-    return sizeof(double) * ns + sizeof(int) * 2 * ns + sizeof(double) * 32 * BS * BS;
+    return sizeof(double) * ns + sizeof(int) * 2 * ns + sizeof(double) * BOPS_WARPS * WS;
 }
 
 IBArgs make_args(lbm_handle *h, const void *fin)
@@ -760,8 +822,8 @@ int launch_ib_t(lbm_handle *h, const void *fin, int step_index, int ring_slot)
 size_t ib_block_scratch(int nseg, size_t *d, size_t *l, size_t *f, size_t *x)
 {
     const size_t nb = (size_t)(nseg + BS - 1) / BS;
-    *d = nb * BS * BS;
-    *l = nb * BS * BS;
+    *d = 2 * nb * BS * BS;   // working blocks, then the assembled copy
+    *l = 2 * nb * BS * BS;
     *f = nb * BS * (2 * BS + 2);
     *x = 2 * nb * BS + 2 * (size_t)nseg;
     return *d + *l + *f + *x;

@@ -74,97 +74,114 @@ __device__ __forceinline__ void side_bc(const KFArgs<C> &a, const T *__restrict_
     }
 }
 
-template <typename T, typename C, bool FIELDS>
-__global__ void __launch_bounds__(256) kf_kernel(const KFArgs<C> a)
+// interior node: moments of the streamed populations g, immersed-boundary
+// correction from the patch, MRT collision with forcing
+template <typename C>
+__device__ __forceinline__ void collide_interior(const KFArgs<C> &a, const PatchInfo &pi, const C g[9], int i, int j,
+                                                 C gout[9], C &frho, C &fu, C &fv)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
-    if (i >= a.nx) return;
-    const T *__restrict__ fin = (const T *)a.fin;
-    T *__restrict__ fout = (T *)a.fout;
-    const long long o = (long long)j * a.pitch + i;
-    C gout[9];
-    C frho, fu, fv;
-    const bool edge = (i == 0) | (i == a.nx - 1) | (j == 0) | (j == a.ny - 1);
-    if (!edge) {
-        C g[9], drho, u, v;
-        pull<T, C>(fin, a.plane, a.pitch, i, j, g);
-        moments(g, drho, u, v);
-        const C rho = C(1) + drho;
-        C gx = C(0), gy = C(0);
-        const PatchInfo pi = *a.pinfo;
-        const unsigned pii = (unsigned)(i - pi.i0), pjj = (unsigned)(j - pi.j0);
-        if (pii < (unsigned)pi.w && pjj < (unsigned)pi.h) {
-            const long long pq = 2ll * ((long long)pjj * pi.w + pii);
-            const C du = a.patch[pq], dv = a.patch[pq + 1];
-            u = u + du;                       // boundary_condition.f90:1650-1651
-            v = v + dv;
-            gx = C(2) * rho * du;             // :1652-1656
-            gy = C(2) * rho * dv;
-        }
-        C m[9];
-        mrt_forward(g, m);
-        const C jx = rho * u, jy = rho * v;
-        const C jj = jx * jx + jy * jy;
-        C e[9];
-        e[0] = C(-1);                          // temp(1)=0 minus (M w)_1
-        e[1] = C(-2) * drho + C(3) * jj;       // solution.f90:605 minus (M w)_2
-        e[2] = drho - C(3) * jj;               // :606
-        e[3] = C(0);
-        e[4] = -jx;
-        e[5] = C(0);
-        e[6] = -jy;
-        e[7] = jx * jx - jy * jy;
-        e[8] = jx * jy;
-        // m' = m + s(meq - m) + fp (solution.f90:632-634); the new populations
-        // are taken as g + M^-1 (m' - m), which equals M^-1 m' exactly but
-        // rounds relative to the small non-equilibrium update, not to g
-        C d[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) d[k] = (e[k] - m[k]) * a.s[k];
-        if (gx != C(0) || gy != C(0)) {        // :614-626
-            const C ug = u * gx + v * gy;
-            d[1] += C(6) * (C(1) - C(0.5) * a.s[1]) * ug;
-            d[2] += C(-6) * (C(1) - C(0.5) * a.s[2]) * ug;
-            d[3] += gx;
-            d[4] += -(C(1) - C(0.5) * a.s[4]) * gx;
-            d[5] += gy;
-            d[6] += -(C(1) - C(0.5) * a.s[6]) * gy;
-            d[7] += C(2) * (C(1) - C(0.5) * a.s[7]) * (u * gx - v * gy);
-            d[8] += (C(1) - C(0.5) * a.s[8]) * (u * gy + v * gx);
-        }
-        mrt_inverse(d, gout);
-#pragma unroll
-        for (int k = 0; k < 9; ++k) gout[k] += g[k];
-        frho = rho; fu = u; fv = v;
-    } else {
-        C g0n[9], drn, un, vn;
-        if (j == 0 || j == a.ny - 1) {
-            // top/bottom row: rho from the adjacent row, u = v = 0
-            // (boundary_condition.f90:658-716, 785-843)
-            const int jn = j == 0 ? 1 : a.ny - 2;
-            if (i == 0 || i == a.nx - 1) {
-                const int side = i == 0 ? 0 : 1;
-                C d2[9], dr2, u2, v2;
-                side_bc<T, C>(a, fin, side, jn, drn, un, vn, d2, dr2, u2, v2);
-                const C *c = a.corner + 9 * (2 * side + (j == 0 ? 0 : 1));
-#pragma unroll
-                for (int k = 0; k < 9; ++k) g0n[k] = c[k];   // edge f0, never rewritten
-            } else {
-                pull<T, C>(fin, a.plane, a.pitch, i, jn, g0n);
-                moments(g0n, drn, un, vn);
-            }
-            extrapolate_dev<C>(a.s, drn, C(0), C(0), drn, un, vn, g0n, gout);
-            frho = C(1) + drn; fu = C(0); fv = C(0);
-        } else {
-            // left/right column (boundary_condition.f90:413-483, 495-567)
-            const int side = i == 0 ? 0 : 1;
-            C dr1, u1, v1;
-            side_bc<T, C>(a, fin, side, j, dr1, u1, v1, g0n, drn, un, vn);
-            extrapolate_dev<C>(a.s, dr1, u1, v1, drn, un, vn, g0n, gout);
-            frho = C(1) + dr1; fu = u1; fv = v1;
-        }
+    C drho, u, v;
+    moments(g, drho, u, v);
+    const C rho = C(1) + drho;
+    C gx = C(0), gy = C(0);
+    const unsigned pii = (unsigned)(i - pi.i0), pjj = (unsigned)(j - pi.j0);
+    if (pii < (unsigned)pi.w && pjj < (unsigned)pi.h) {
+        const int pq = 2 * ((int)pjj * pi.w + (int)pii);
+        const C du = a.patch[pq], dv = a.patch[pq + 1];
+        u = u + du;                       // boundary_condition.f90:1650-1651
+        v = v + dv;
+        gx = C(2) * rho * du;             // :1652-1656
+        gy = C(2) * rho * dv;
     }
+    C m[9];
+    mrt_forward(g, m);
+    const C jx = rho * u, jy = rho * v;
+    const C jj = jx * jx + jy * jy;
+    C e[9];
+    e[0] = C(-1);                          // temp(1)=0 minus (M w)_1
+    e[1] = C(-2) * drho + C(3) * jj;       // solution.f90:605 minus (M w)_2
+    e[2] = drho - C(3) * jj;               // :606
+    e[3] = C(0);
+    e[4] = -jx;
+    e[5] = C(0);
+    e[6] = -jy;
+    e[7] = jx * jx - jy * jy;
+    e[8] = jx * jy;
+    // m' = m + s(meq - m) + fp (solution.f90:632-634); the new populations
+    // are taken as g + M^-1 (m' - m), which equals M^-1 m' exactly but
+    // rounds relative to the small non-equilibrium update, not to g
+    C d[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) d[k] = (e[k] - m[k]) * a.s[k];
+    if (gx != C(0) || gy != C(0)) {        // :614-626
+        const C ug = u * gx + v * gy;
+        d[1] += C(6) * (C(1) - C(0.5) * a.s[1]) * ug;
+        d[2] += C(-6) * (C(1) - C(0.5) * a.s[2]) * ug;
+        d[3] += gx;
+        d[4] += -(C(1) - C(0.5) * a.s[4]) * gx;
+        d[5] += gy;
+        d[6] += -(C(1) - C(0.5) * a.s[6]) * gy;
+        d[7] += C(2) * (C(1) - C(0.5) * a.s[7]) * (u * gx - v * gy);
+        d[8] += (C(1) - C(0.5) * a.s[8]) * (u * gy + v * gx);
+    }
+    mrt_inverse(d, gout);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) gout[k] += g[k];
+    frho = rho; fu = u; fv = v;
+}
+
+// edge node: boundary_condition1 (boundary_condition.f90:413-853)
+template <typename T, typename C>
+__device__ __forceinline__ void edge_update(const KFArgs<C> &a, const T *__restrict__ fin, int i, int j, C gout[9],
+                                            C &frho, C &fu, C &fv)
+{
+    C g0n[9], drn, un, vn;
+    if (j == 0 || j == a.ny - 1) {
+        // top/bottom row: rho from the adjacent row, u = v = 0
+        // (boundary_condition.f90:658-716, 785-843)
+        const int jn = j == 0 ? 1 : a.ny - 2;
+        if (i == 0 || i == a.nx - 1) {
+            const int side = i == 0 ? 0 : 1;
+            C d2[9], dr2, u2, v2;
+            side_bc<T, C>(a, fin, side, jn, drn, un, vn, d2, dr2, u2, v2);
+            const C *c = a.corner + 9 * (2 * side + (j == 0 ? 0 : 1));
+#pragma unroll
+            for (int k = 0; k < 9; ++k) g0n[k] = c[k];   // edge f0, never rewritten
+        } else {
+            pull<T, C>(fin, a.plane, a.pitch, i, jn, g0n);
+            moments(g0n, drn, un, vn);
+        }
+        extrapolate_dev<C>(a.s, drn, C(0), C(0), drn, un, vn, g0n, gout);
+        frho = C(1) + drn; fu = C(0); fv = C(0);
+    } else {
+        // left/right column (boundary_condition.f90:413-483, 495-567)
+        const int side = i == 0 ? 0 : 1;
+        C dr1, u1, v1;
+        side_bc<T, C>(a, fin, side, j, dr1, u1, v1, g0n, drn, un, vn);
+        extrapolate_dev<C>(a.s, dr1, u1, v1, drn, un, vn, g0n, gout);
+        frho = C(1) + dr1; fu = u1; fv = v1;
+    }
+}
+
+// any node with scalar loads
+template <typename T, typename C>
+__device__ __forceinline__ void node_update(const KFArgs<C> &a, const PatchInfo &pi, const T *__restrict__ fin, int i,
+                                            int j, C gout[9], C &frho, C &fu, C &fv)
+{
+    if (i == 0 || i == a.nx - 1 || j == 0 || j == a.ny - 1) {
+        edge_update<T, C>(a, fin, i, j, gout, frho, fu, fv);
+    } else {
+        C g[9];
+        pull<T, C>(fin, a.plane, a.pitch, i, j, g);
+        collide_interior<C>(a, pi, g, i, j, gout, frho, fu, fv);
+    }
+}
+
+template <typename T, typename C, bool FIELDS>
+__device__ __forceinline__ void store_node(const KFArgs<C> &a, T *__restrict__ fout, int i, int j, const C gout[9],
+                                           C frho, C fu, C fv)
+{
+    const long long o = (long long)j * a.pitch + i;
 #pragma unroll
     for (int k = 0; k < 9; ++k) Store<T>::st(fout + (long long)k * a.plane + o, gout[k]);
     if (FIELDS) {
@@ -173,6 +190,125 @@ __global__ void __launch_bounds__(256) kf_kernel(const KFArgs<C> a)
         a.u_out[q] = fu;
         a.v_out[q] = fv;
     }
+}
+
+// one node per thread, scalar loads (any lattice size)
+template <typename T, typename C, bool FIELDS>
+__global__ void __launch_bounds__(256) kf_kernel(const KFArgs<C> a)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y;
+    if (i >= a.nx) return;
+    const T *__restrict__ fin = (const T *)a.fin;
+    T *__restrict__ fout = (T *)a.fout;
+    const PatchInfo pi = *a.pinfo;
+    C gout[9], frho, fu, fv;
+    node_update<T, C>(a, pi, fin, i, j, gout, frho, fu, fv);
+    store_node<T, C, FIELDS>(a, fout, i, j, gout, frho, fu, fv);
+}
+
+template <typename T, int VEC> struct alignas(sizeof(T) * VEC) VecT {
+    T v[VEC];
+};
+
+// VEC consecutive nodes of one row per thread: the 9 planes are read with
+// aligned VEC-wide loads at rows j - e_y; the x-shifted planes take their
+// missing neighbour element from the adjacent lane (warp shuffle), or from
+// memory at the warp's ends. 32-bit offsets (9 planes < 2^31 elements).
+template <typename T, typename C, bool FIELDS, int VEC>
+__global__ void __launch_bounds__(128) kf_vec(const KFArgs<C> a)
+{
+    const int lane = threadIdx.x & 31;
+    const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * VEC;
+    const int j = blockIdx.y;
+    const T *__restrict__ fin = (const T *)a.fin;
+    T *__restrict__ fout = (T *)a.fout;
+    const int pitch = a.pitch, plane = (int)a.plane;
+    const PatchInfo pi = *a.pinfo;
+    if (j == 0 || j == a.ny - 1) {             // warp-uniform: edge rows
+        for (int e = 0; e < VEC; ++e) {
+            const int i = i0 + e;
+            if (i >= a.nx) break;
+            C gout[9], frho, fu, fv;
+            edge_update<T, C>(a, fin, i, j, gout, frho, fu, fv);
+            store_node<T, C, FIELDS>(a, fout, i, j, gout, frho, fu, fv);
+        }
+        return;
+    }
+    const bool inrow = i0 < pitch;
+    T v[9][VEC];
+    T xl[9], xr[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        const T *p = fin + k * plane + (j - lbm_ey(k)) * pitch + i0;
+        if (inrow) {
+            const VecT<T, VEC> w = *reinterpret_cast<const VecT<T, VEC> *>(p);
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) v[k][e] = w.v[e];
+        } else {
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) v[k][e] = T(0.0f);
+        }
+        if (lbm_ex(k) == 1) {
+            xl[k] = __shfl_up_sync(0xffffffffu, v[k][VEC - 1], 1);
+            if (lane == 0) xl[k] = (i0 >= 1 && i0 - 1 < pitch) ? p[-1] : T(0.0f);
+        } else if (lbm_ex(k) == -1) {
+            xr[k] = __shfl_down_sync(0xffffffffu, v[k][0], 1);
+            if (lane == 31) xr[k] = (i0 + VEC < a.nx) ? p[VEC] : T(0.0f);
+        }
+    }
+    if (i0 >= a.nx) return;
+    if (i0 >= 1 && i0 + VEC - 1 <= a.nx - 2) {
+        T out[9][VEC];
+#pragma unroll
+        for (int e = 0; e < VEC; ++e) {
+            C g[9];
+#pragma unroll
+            for (int k = 0; k < 9; ++k) {
+                T t;
+                if (lbm_ex(k) == 0) t = v[k][e];
+                else if (lbm_ex(k) == 1) t = e == 0 ? xl[k] : v[k][e - 1];
+                else t = e == VEC - 1 ? xr[k] : v[k][e + 1];
+                g[k] = (C)Store<T>::cvt(t);
+            }
+            C gout[9], frho, fu, fv;
+            collide_interior<C>(a, pi, g, i0 + e, j, gout, frho, fu, fv);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) out[k][e] = Store<T>::pack(gout[k]);
+            if (FIELDS) {
+                const int q = j * a.nx + i0 + e;
+                a.rho_out[q] = frho;
+                a.u_out[q] = fu;
+                a.v_out[q] = fv;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            VecT<T, VEC> w;
+#pragma unroll
+            for (int e = 0; e < VEC; ++e) w.v[e] = out[k][e];
+            *reinterpret_cast<VecT<T, VEC> *>(fout + k * plane + j * pitch + i0) = w;
+        }
+    } else {
+        for (int e = 0; e < VEC; ++e) {
+            const int i = i0 + e;
+            if (i >= a.nx) break;
+            C gout[9], frho, fu, fv;
+            node_update<T, C>(a, pi, fin, i, j, gout, frho, fu, fv);
+            store_node<T, C, FIELDS>(a, fout, i, j, gout, frho, fu, fv);
+        }
+    }
+}
+
+template <typename T, typename C, int VEC>
+void launch_vec(const KFArgs<C> &a, bool fields, int nx, int ny, cudaStream_t st)
+{
+    const int per_block = 128 * VEC;
+    dim3 block(128, 1), grid((nx + per_block - 1) / per_block, ny);
+    if (fields)
+        kf_vec<T, C, true, VEC><<<grid, block, 0, st>>>(a);
+    else
+        kf_vec<T, C, false, VEC><<<grid, block, 0, st>>>(a);
 }
 
 template <typename T, typename C>
@@ -202,11 +338,19 @@ int launch_kf_t(lbm_handle *h, const void *fin, void *fout, void *fields)
     } else {
         a.rho_out = a.u_out = a.v_out = nullptr;
     }
-    dim3 block(256, 1), grid((h->nx + 255) / 256, h->ny);
-    if (fields)
-        kf_kernel<T, C, true><<<grid, block, 0, h->stream>>>(a);
-    else
-        kf_kernel<T, C, false><<<grid, block, 0, h->stream>>>(a);
+    const bool small_index = 9ll * h->plane < (1ll << 31) && (long long)h->nx * h->ny < (1ll << 31);
+    const int vec = small_index ? h->kf_vec : 1;
+    if (vec == 4 && h->pitch % 4 == 0) {
+        launch_vec<T, C, 4>(a, fields != nullptr, h->nx, h->ny, h->stream);
+    } else if (vec == 2 && h->pitch % 2 == 0) {
+        launch_vec<T, C, 2>(a, fields != nullptr, h->nx, h->ny, h->stream);
+    } else {
+        dim3 block(256, 1), grid((h->nx + 255) / 256, h->ny);
+        if (fields)
+            kf_kernel<T, C, true><<<grid, block, 0, h->stream>>>(a);
+        else
+            kf_kernel<T, C, false><<<grid, block, 0, h->stream>>>(a);
+    }
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

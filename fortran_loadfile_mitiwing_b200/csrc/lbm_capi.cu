@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <vector>
 
 #include "lbm_internal.h"
@@ -323,6 +324,13 @@ int lbm_create(const lbm_params *p, lbm_t **out)
     if (p->s[8] <= 0) h->s[8] = 1.0 / h->tau;
     h->prec = p->precision;
     h->elem = storage_size(h->prec);
+    // nodes per thread of the lattice kernel; LBM_KF_VEC (1, 2 or 4) overrides
+    // the default for tuning
+    h->kf_vec = 2;
+    if (const char *ev = getenv("LBM_KF_VEC")) {
+        const int v = atoi(ev);
+        if (v == 1 || v == 2 || v == 4) h->kf_vec = v;
+    }
     h->hx0.assign(std::max(1, h->npts), 0.0);
     h->hy0.assign(std::max(1, h->npts), 0.0);
     h->harc.assign(std::max(1, h->nseg), 0.0);

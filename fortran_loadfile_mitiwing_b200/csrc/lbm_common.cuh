@@ -57,23 +57,31 @@ template <> struct CType<double> { using type = double; };
 
 // storage conversions
 template <typename T> struct Store;
+// ld/st: one element from/to memory in compute precision; cvt/pack: convert
+// an element already in registers
 template <> struct Store<float> {
     static __device__ __forceinline__ float ld(const float *p) { return __ldg(p); }
-    static __device__ __forceinline__ float to(float x) { return x; }
     static __device__ __forceinline__ void st(float *p, float x) { *p = x; }
+    static __device__ __forceinline__ float cvt(float x) { return x; }
+    static __device__ __forceinline__ float pack(float x) { return x; }
 };
 template <> struct Store<double> {
     static __device__ __forceinline__ double ld(const double *p) { return __ldg(p); }
-    static __device__ __forceinline__ double to(double x) { return x; }
     static __device__ __forceinline__ void st(double *p, double x) { *p = x; }
+    static __device__ __forceinline__ double cvt(double x) { return x; }
+    static __device__ __forceinline__ double pack(double x) { return x; }
 };
 template <> struct Store<__half> {
     static __device__ __forceinline__ float ld(const __half *p) { return __half2float(__ldg(p)); }
     static __device__ __forceinline__ void st(__half *p, float x) { *p = __float2half_rn(x); }
+    static __device__ __forceinline__ float cvt(__half x) { return __half2float(x); }
+    static __device__ __forceinline__ __half pack(float x) { return __float2half_rn(x); }
 };
 template <> struct Store<__nv_bfloat16> {
     static __device__ __forceinline__ float ld(const __nv_bfloat16 *p) { return __bfloat162float(__ldg(p)); }
     static __device__ __forceinline__ void st(__nv_bfloat16 *p, float x) { *p = __float2bfloat16_rn(x); }
+    static __device__ __forceinline__ float cvt(__nv_bfloat16 x) { return __bfloat162float(x); }
+    static __device__ __forceinline__ __nv_bfloat16 pack(float x) { return __float2bfloat16_rn(x); }
 };
 
 // m = M g for the MRT matrix of solution.f90:17-25 (rows: rho, e, eps, jx, qx,

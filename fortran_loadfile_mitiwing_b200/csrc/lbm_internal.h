@@ -72,6 +72,7 @@ struct lbm_handle {
     double niu = 0, tau = 0, s[9] = {0};
     int prec = 0;
     size_t elem = 4;
+    int kf_vec = 4;   // nodes per thread of the lattice kernel (1, 2 or 4)
     int dev = 0;
     cudaStream_t stream = nullptr;
     void *fbuf[2] = {nullptr, nullptr};
