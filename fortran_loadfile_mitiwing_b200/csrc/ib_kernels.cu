@@ -805,10 +805,9 @@ IBArgs make_args(lbm_handle *h, const void *fin)
 }
 
 template <typename T, typename C>
-int launch_ib_t(lbm_handle *h, const void *fin, int step_index, int ring_slot)
+int launch_ib_t(lbm_handle *h, const void *fin, int step_index, int ring_slot, cudaStream_t st)
 {
     IBArgs a = make_args(h, fin);
-    cudaStream_t st = h->stream;
     if (h->nseg > 0) ib_markers<T><<<(h->nseg + 7) / 8, 256, 0, st>>>(a, step_index);
     ib_solve<<<1, SOLVE_THREADS, solve_smem(h->nseg), st>>>(a, step_index, ring_slot);
     dim3 grid(h->patch_gx(), h->patch_gy());
@@ -839,13 +838,14 @@ int ib_configure(lbm_handle *h)
     return 0;
 }
 
-int launch_ib(lbm_handle *h, const void *fin, int step_index, int ring_slot)
+int launch_ib(lbm_handle *h, const void *fin, int step_index, int ring_slot, cudaStream_t st)
 {
+    if (!st) st = h->stream;
     switch (h->prec) {
-    case LBM_PREC_FP32: return launch_ib_t<float, float>(h, fin, step_index, ring_slot);
-    case LBM_PREC_FP64: return launch_ib_t<double, double>(h, fin, step_index, ring_slot);
-    case LBM_PREC_FP16: return launch_ib_t<__half, float>(h, fin, step_index, ring_slot);
-    case LBM_PREC_BF16: return launch_ib_t<__nv_bfloat16, float>(h, fin, step_index, ring_slot);
+    case LBM_PREC_FP32: return launch_ib_t<float, float>(h, fin, step_index, ring_slot, st);
+    case LBM_PREC_FP64: return launch_ib_t<double, double>(h, fin, step_index, ring_slot, st);
+    case LBM_PREC_FP16: return launch_ib_t<__half, float>(h, fin, step_index, ring_slot, st);
+    case LBM_PREC_BF16: return launch_ib_t<__nv_bfloat16, float>(h, fin, step_index, ring_slot, st);
     }
     return -1;
 }

@@ -196,12 +196,21 @@ __device__ __forceinline__ void store_node(const KFArgs<C> &a, T *__restrict__ f
 template <typename T, typename C, bool FIELDS>
 __global__ void __launch_bounds__(256) kf_kernel(const KFArgs<C> a)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    int j = blockIdx.y;
+    if (a.mode == KF_INNER) {
+        if (i >= a.rw) return;
+        i += a.rx0;
+        j += a.ry0;
+    } else if (a.mode == KF_OUTER && (unsigned)(i - a.rx0) < (unsigned)a.rw && (unsigned)(j - a.ry0) < (unsigned)a.rh) {
+        return;
+    }
     if (i >= a.nx) return;
     const T *__restrict__ fin = (const T *)a.fin;
     T *__restrict__ fout = (T *)a.fout;
-    const PatchInfo pi = *a.pinfo;
+    // the outer part runs while the IB kernels rewrite the patch: it reads
+    // neither (no outer node lies in any patch)
+    const PatchInfo pi = a.mode == KF_OUTER ? PatchInfo{0, 0, 0, 0} : *a.pinfo;
     C gout[9], frho, fu, fv;
     node_update<T, C>(a, pi, fin, i, j, gout, frho, fu, fv);
     store_node<T, C, FIELDS>(a, fout, i, j, gout, frho, fu, fv);
@@ -219,12 +228,20 @@ template <typename T, typename C, bool FIELDS, int VEC>
 __global__ void __launch_bounds__(128) kf_vec(const KFArgs<C> a)
 {
     const int lane = threadIdx.x & 31;
-    const int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * VEC;
-    const int j = blockIdx.y;
+    int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * VEC;
+    int j = blockIdx.y;
+    int iend = a.nx;                           // first column this launch does not own
+    if (a.mode == KF_INNER) {
+        i0 += a.rx0;
+        j += a.ry0;
+        iend = a.rx0 + a.rw;
+    }
     const T *__restrict__ fin = (const T *)a.fin;
     T *__restrict__ fout = (T *)a.fout;
     const int pitch = a.pitch, plane = (int)a.plane;
-    const PatchInfo pi = *a.pinfo;
+    // the outer part runs while the IB kernels rewrite the patch: it reads
+    // neither (no outer node lies in any patch)
+    const PatchInfo pi = a.mode == KF_OUTER ? PatchInfo{0, 0, 0, 0} : *a.pinfo;
     if (j == 0 || j == a.ny - 1) {             // warp-uniform: edge rows
         for (int e = 0; e < VEC; ++e) {
             const int i = i0 + e;
@@ -257,7 +274,11 @@ __global__ void __launch_bounds__(128) kf_vec(const KFArgs<C> a)
             if (lane == 31) xr[k] = (i0 + VEC < a.nx) ? p[VEC] : T(0.0f);
         }
     }
-    if (i0 >= a.nx) return;
+    if (i0 >= iend) return;
+    // the split rectangle's x bounds are multiples of VEC, so a thread's nodes
+    // are all inside or all outside it
+    if (a.mode == KF_OUTER && (unsigned)(i0 - a.rx0) < (unsigned)a.rw && (unsigned)(j - a.ry0) < (unsigned)a.rh)
+        return;
     if (i0 >= 1 && i0 + VEC - 1 <= a.nx - 2) {
         T out[9][VEC];
 #pragma unroll
@@ -300,11 +321,163 @@ __global__ void __launch_bounds__(128) kf_vec(const KFArgs<C> a)
     }
 }
 
+// ---- bulk-copy staged lattice kernel ----------------------------------
+// A CTA owns a strip of TW columns and sweeps rows_per_cta interior rows.
+// For every output row j one elected thread issues nine 1-D bulk copies
+// (cp.async.bulk, completion on an mbarrier) of the plane rows j - e_y with a
+// 16-byte halo on both sides into a KS-stage shared-memory ring; the threads
+// then read the shifted populations from shared memory. The copies keep
+// KS x 9 row segments in flight per CTA without holding them in registers.
+// Rows 0 and ny-1 are handled by one extra CTA row of the grid, and columns
+// 0 and nx-1 by the scalar edge path.
+
+constexpr int TW = 256;        // strip width (threads per CTA)
+constexpr int KS = 4;          // pipeline stages
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+template <typename T> __host__ __device__ constexpr int tma_halo() { return 16 / (int)sizeof(T); }
+template <typename T> __host__ __device__ constexpr int tma_seg() { return TW + 2 * tma_halo<T>(); }
+template <typename T> constexpr size_t tma_smem() { return sizeof(T) * KS * 9 * tma_seg<T>() + 8 * KS; }
+
+template <typename T, typename C, bool FIELDS>
+__global__ void __launch_bounds__(TW) kf_tma(const KFArgs<C> a)
+{
+    constexpr int H = tma_halo<T>(), SEG = tma_seg<T>();
+    extern __shared__ __align__(128) unsigned char smraw[];
+    T *buf = reinterpret_cast<T *>(smraw);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + sizeof(T) * KS * 9 * SEG);
+    const int tid = threadIdx.x;
+    const int x0 = blockIdx.x * TW;
+    const int i = x0 + tid;
+    const T *__restrict__ fin = (const T *)a.fin;
+    T *__restrict__ fout = (T *)a.fout;
+    const PatchInfo pi = a.mode == KF_OUTER ? PatchInfo{0, 0, 0, 0} : *a.pinfo;
+    if (blockIdx.y == gridDim.y - 1) {         // the two edge rows of this strip
+        if (i < a.nx)
+            for (int j = 0; j < a.ny; j += a.ny - 1) {
+                C gout[9], frho, fu, fv;
+                edge_update<T, C>(a, fin, i, j, gout, frho, fu, fv);
+                store_node<T, C, FIELDS>(a, fout, i, j, gout, frho, fu, fv);
+            }
+        return;
+    }
+    const int j0 = 1 + blockIdx.y * a.rows_per_cta;
+    const int nrows = min(a.rows_per_cta, a.ny - 1 - j0);
+    if (nrows <= 0) return;
+    const int width = min(TW, a.nx - x0);
+    const uint32_t bytes = (uint32_t)((((width + 2 * H) * (int)sizeof(T)) + 15) / 16 * 16);
+    if (tid == 0) {
+        for (int s = 0; s < KS; ++s) mbar_init(&bar[s], 1);
+        mbar_init_fence();
+    }
+    __syncthreads();
+    auto issue = [&](int r) {
+        const int s = r % KS, j = j0 + r;
+        mbar_expect_tx(&bar[s], 9u * bytes);
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+            bulk_g2s(buf + (s * 9 + k) * SEG,
+                     fin + (long long)k * a.plane + (long long)(j - lbm_ey(k)) * a.pitch + (x0 - H), bytes, &bar[s]);
+    };
+    if (tid == 0)
+        for (int r = 0; r < KS && r < nrows; ++r) issue(r);
+    for (int r = 0; r < nrows; ++r) {
+        const int s = r % KS, j = j0 + r;
+        const uint32_t parity = (uint32_t)((r / KS) & 1);
+        // bounded wait: a copy that never lands is reported, not waited on forever
+        int spins = 0;
+        while (!mbar_try_wait(&bar[s], parity)) {
+            if (++spins > (1 << 22)) {
+                if (tid == 0) atomicOr(a.status, LBM_ST_TIMEOUT);
+                return;
+            }
+        }
+        const bool skip = a.mode == KF_OUTER && (unsigned)(i - a.rx0) < (unsigned)a.rw && (unsigned)(j - a.ry0) < (unsigned)a.rh;
+        if (i < a.nx && !skip) {
+            C gout[9], frho, fu, fv;
+            if (i == 0 || i == a.nx - 1) {
+                edge_update<T, C>(a, fin, i, j, gout, frho, fu, fv);
+            } else {
+                C g[9];
+                const T *row = buf + s * 9 * SEG + H + tid;
+#pragma unroll
+                for (int k = 0; k < 9; ++k) g[k] = (C)Store<T>::cvt(row[k * SEG - lbm_ex(k)]);
+                collide_interior<C>(a, pi, g, i, j, gout, frho, fu, fv);
+            }
+            store_node<T, C, FIELDS>(a, fout, i, j, gout, frho, fu, fv);
+        }
+        __syncthreads();                       // stage s fully read
+        if (tid == 0 && r + KS < nrows) {
+            fence_proxy_async();
+            issue(r + KS);
+        }
+    }
+}
+
+template <typename T, typename C>
+void launch_tma(const KFArgs<C> &a, bool fields, int nx, int ny, cudaStream_t st)
+{
+    dim3 block(TW, 1), grid((nx + TW - 1) / TW, (ny - 2 + a.rows_per_cta - 1) / a.rows_per_cta + 1);
+    const size_t smem = tma_smem<T>();
+    if (fields)
+        kf_tma<T, C, true><<<grid, block, smem, st>>>(a);
+    else
+        kf_tma<T, C, false><<<grid, block, smem, st>>>(a);
+}
+
+template <typename T, typename C>
+int configure_tma()
+{
+    const int smem = (int)tma_smem<T>();
+    if (cudaFuncSetAttribute(kf_tma<T, C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+        return -1;
+    if (cudaFuncSetAttribute(kf_tma<T, C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+        return -1;
+    return 0;
+}
+
 template <typename T, typename C, int VEC>
 void launch_vec(const KFArgs<C> &a, bool fields, int nx, int ny, cudaStream_t st)
 {
     const int per_block = 128 * VEC;
-    dim3 block(128, 1), grid((nx + per_block - 1) / per_block, ny);
+    const int wx = a.mode == KF_INNER ? a.rw : nx, wy = a.mode == KF_INNER ? a.rh : ny;
+    dim3 block(128, 1), grid((wx + per_block - 1) / per_block, wy);
     if (fields)
         kf_vec<T, C, true, VEC><<<grid, block, 0, st>>>(a);
     else
@@ -312,9 +485,14 @@ void launch_vec(const KFArgs<C> &a, bool fields, int nx, int ny, cudaStream_t st
 }
 
 template <typename T, typename C>
-int launch_kf_t(lbm_handle *h, const void *fin, void *fout, void *fields)
+int launch_kf_t(lbm_handle *h, const void *fin, void *fout, void *fields, int mode, cudaStream_t st)
 {
     KFArgs<C> a;
+    a.mode = mode;
+    a.rx0 = h->env_x0;
+    a.ry0 = h->env_y0;
+    a.rw = h->env_w;
+    a.rh = h->env_h;
     a.fin = fin;
     a.fout = fout;
     a.nx = h->nx;
@@ -340,16 +518,28 @@ int launch_kf_t(lbm_handle *h, const void *fin, void *fout, void *fields)
     }
     const bool small_index = 9ll * h->plane < (1ll << 31) && (long long)h->nx * h->ny < (1ll << 31);
     const int vec = small_index ? h->kf_vec : 1;
-    if (vec == 4 && h->pitch % 4 == 0) {
-        launch_vec<T, C, 4>(a, fields != nullptr, h->nx, h->ny, h->stream);
+    a.rows_per_cta = h->kf_rows;
+    a.status = h->d_status;
+    if (mode != KF_ALL && (a.rw <= 0 || a.rh <= 0)) return mode == KF_INNER ? 0 : -1;
+    if (!st) st = h->stream;
+    if (h->kf_tma && mode != KF_INNER && h->ny >= 3) {
+        static bool configured = false;   // per process; the attribute is per function
+        if (!configured) {
+            if (configure_tma<T, C>()) return -1;
+            configured = true;
+        }
+        launch_tma<T, C>(a, fields != nullptr, h->nx, h->ny, st);
+    } else if (vec == 4 && h->pitch % 4 == 0) {
+        launch_vec<T, C, 4>(a, fields != nullptr, h->nx, h->ny, st);
     } else if (vec == 2 && h->pitch % 2 == 0) {
-        launch_vec<T, C, 2>(a, fields != nullptr, h->nx, h->ny, h->stream);
+        launch_vec<T, C, 2>(a, fields != nullptr, h->nx, h->ny, st);
     } else {
-        dim3 block(256, 1), grid((h->nx + 255) / 256, h->ny);
+        const int wx = mode == KF_INNER ? a.rw : h->nx, wy = mode == KF_INNER ? a.rh : h->ny;
+        dim3 block(256, 1), grid((wx + 255) / 256, wy);
         if (fields)
-            kf_kernel<T, C, true><<<grid, block, 0, h->stream>>>(a);
+            kf_kernel<T, C, true><<<grid, block, 0, st>>>(a);
         else
-            kf_kernel<T, C, false><<<grid, block, 0, h->stream>>>(a);
+            kf_kernel<T, C, false><<<grid, block, 0, st>>>(a);
     }
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
@@ -412,13 +602,13 @@ __global__ void residual_kernel(const C *__restrict__ fa, const C *__restrict__ 
 
 }  // namespace
 
-int launch_kf(lbm_handle *h, const void *fin, void *fout, void *fields)
+int launch_kf(lbm_handle *h, const void *fin, void *fout, void *fields, int mode, cudaStream_t st)
 {
     switch (h->prec) {
-    case LBM_PREC_FP32: return launch_kf_t<float, float>(h, fin, fout, fields);
-    case LBM_PREC_FP64: return launch_kf_t<double, double>(h, fin, fout, fields);
-    case LBM_PREC_FP16: return launch_kf_t<__half, float>(h, fin, fout, fields);
-    case LBM_PREC_BF16: return launch_kf_t<__nv_bfloat16, float>(h, fin, fout, fields);
+    case LBM_PREC_FP32: return launch_kf_t<float, float>(h, fin, fout, fields, mode, st);
+    case LBM_PREC_FP64: return launch_kf_t<double, double>(h, fin, fout, fields, mode, st);
+    case LBM_PREC_FP16: return launch_kf_t<__half, float>(h, fin, fout, fields, mode, st);
+    case LBM_PREC_BF16: return launch_kf_t<__nv_bfloat16, float>(h, fin, fout, fields, mode, st);
     }
     return -1;
 }

@@ -116,6 +116,8 @@ void lookup_row(const std::vector<double> &tab, int rows, int cols, double t, in
 // releases the immersed-boundary scratch (sizes depend on geometry and motion)
 void free_ib(lbm_handle *h)
 {
+    if (h->side) cudaStreamSynchronize(h->side);
+    if (h->stream) cudaStreamSynchronize(h->stream);
     h->ib_ready = 0;
     free_dev(h->d_patch);
     free_devp(h->d_mk); free_devp(h->d_rhs); free_devp(h->d_B); free_devp(h->d_y); free_devp(h->d_partial);
@@ -129,6 +131,7 @@ int ensure_ib(lbm_handle *h)
 {
     if (h->ib_ready) return LBM_OK;
     int wmax = 0, hmax = 0;
+    double gx0 = 1e300, gx1 = -1e300, gy0 = 1e300, gy1 = -1e300;   // motion envelope (lattice units)
     if (h->nseg > 0) {
         std::vector<double> R(h->nwing, 0.0);
         for (int w = 0; w < h->nwing; ++w)
@@ -148,12 +151,23 @@ int ensure_ib(lbm_handle *h)
             }
             wmax = std::max(wmax, (int)ceil(xhi - xlo) + 2);
             hmax = std::max(hmax, (int)ceil(yhi - ylo) + 2);
+            gx0 = std::min(gx0, xlo); gx1 = std::max(gx1, xhi);
+            gy0 = std::min(gy0, ylo); gy1 = std::max(gy1, yhi);
         }
         wmax = std::min(wmax, h->nx);
         hmax = std::min(hmax, h->ny);
     }
     h->patch_wmax = wmax;
     h->patch_hmax = hmax;
+    // split rectangle: every support node of every step lies inside it (the
+    // disc of radius R+4 lu around each pivot covers the marker boxes); x
+    // bounds rounded out to multiples of 4, clipped to the interior
+    h->env_x0 = h->env_y0 = h->env_w = h->env_h = 0;
+    if (h->nseg > 0) {
+        int x0 = std::max(4, ((int)floor(gx0) - 1) / 4 * 4), x1 = std::min(h->nx - 4, ((int)ceil(gx1) + 2 + 3) / 4 * 4);
+        int y0 = std::max(1, (int)floor(gy0) - 1), y1 = std::min(h->ny - 1, (int)ceil(gy1) + 2);
+        if (x1 > x0 && y1 > y0) { h->env_x0 = x0; h->env_y0 = y0; h->env_w = x1 - x0; h->env_h = y1 - y0; }
+    }
     h->patch_cap = std::max(1, wmax * hmax);
     const size_t cs = compute_size(h->prec);
     CK(cudaMalloc(&h->d_patch, 2 * cs * (size_t)h->patch_cap), "alloc patch");
@@ -191,27 +205,38 @@ int check_status(lbm_handle *h)
     return set_err(h, LBM_ERR_CUDA, "unknown device status");
 }
 
-// sums the event intervals of `count` step slots after the stream is idle:
+// sums the event intervals of `count` step slots after the streams are idle:
 // step time is the span from the first step's start to the last step's end
-// (gaps between launches included), IB and lattice times are per-kernel sums
-int collect_timing(lbm_handle *h, int count)
+// (gaps between launches included); the lattice time is the sum of the
+// lattice kernels' intervals; the IB time is measured on the stream it ran on
+int collect_timing(lbm_handle *h, int count, bool split)
 {
     if (count < 1) return LBM_OK;
     for (int s = 0; s < count; ++s) {
-        float a = 0, b = 0;
-        CK(cudaEventElapsedTime(&a, h->ev[3 * s], h->ev[3 * s + 1]), "event time");
-        CK(cudaEventElapsedTime(&b, h->ev[3 * s + 1], h->ev[3 * s + 2]), "event time");
-        h->t_ib += a;
-        h->t_kf += b;
+        float a = 0, b = 0, c = 0;
+        CK(cudaEventElapsedTime(&a, h->ev[4 * s], h->ev[4 * s + 1]), "event time");
+        CK(cudaEventElapsedTime(&b, h->ev[4 * s + 2], h->ev[4 * s + 3]), "event time");
+        if (split) {
+            CK(cudaEventElapsedTime(&c, h->ev_side[2 * s], h->ev_side[2 * s + 1]), "event time");
+            h->t_kf += a + b;
+            h->t_ib += c;
+        } else {
+            h->t_ib += a;
+            h->t_kf += b;
+        }
         h->t_steps++;
     }
     float span = 0;
-    CK(cudaEventElapsedTime(&span, h->ev[0], h->ev[3 * (count - 1) + 2]), "event time");
+    CK(cudaEventElapsedTime(&span, h->ev[0], h->ev[4 * (count - 1) + 3]), "event time");
     h->t_step += span;
     return LBM_OK;
 }
 
-// The per-step sequence: IB chain, then the fused lattice update.
+// The per-step sequence. Without a body, or with the split off: IB chain,
+// then the fused lattice update, on the main stream. With the split: the IB
+// chain runs on the side stream (after the previous step's inner update)
+// while the main stream updates the lattice outside the motion envelope;
+// the main stream then waits for the IB chain and updates the envelope.
 int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool fields_every)
 {
     if (!h->inited) return set_err(h, LBM_ERR_STATE, "step: lbm_init not called");
@@ -219,6 +244,8 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
         if (!h->have_wing[w]) return set_err(h, LBM_ERR_STATE, "step: boundary of a wing not set");
     int rc = ensure_ib(h);
     if (rc) return rc;
+    const bool split = h->overlap && h->nseg > 0 && h->env_w > 0 && h->env_h > 0;
+    if (split) CK(cudaEventRecord(h->ev_inner, h->stream), "event");
     int done = 0, pending = 0;
     rc = LBM_OK;
     for (int s = 0; s < nsteps; ++s) {
@@ -227,9 +254,6 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
         const int slot = pending;
         const void *fin = h->fbuf[h->cur];
         void *fout = h->fbuf[h->cur ^ 1];
-        if (h->timing) CK(cudaEventRecord(h->ev[3 * slot], h->stream), "event");
-        if (launch_ib(h, fin, h->n, slot)) return cuda_err(h, cudaGetLastError(), "launch ib");
-        if (h->timing) CK(cudaEventRecord(h->ev[3 * slot + 1], h->stream), "event");
         void *fields = nullptr;
         const bool want = fields_every || s >= nsteps - 2;
         if (want) {
@@ -238,8 +262,31 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             h->fields_slot = fs;
             h->fields_step[fs] = h->n;
         }
-        if (launch_kf(h, fin, fout, fields)) return cuda_err(h, cudaGetLastError(), "launch kf");
-        if (h->timing) CK(cudaEventRecord(h->ev[3 * slot + 2], h->stream), "event");
+        cudaEvent_t *e = h->timing ? &h->ev[4 * slot] : nullptr;
+        if (split) {
+            CK(cudaStreamWaitEvent(h->side, h->ev_inner, 0), "wait");
+            if (e) CK(cudaEventRecord(h->ev_side[2 * slot], h->side), "event");
+            if (launch_ib(h, fin, h->n, slot, h->side)) return cuda_err(h, cudaGetLastError(), "launch ib");
+            if (e) CK(cudaEventRecord(h->ev_side[2 * slot + 1], h->side), "event");
+            CK(cudaEventRecord(h->ev_ib, h->side), "event");
+            if (e) CK(cudaEventRecord(e[0], h->stream), "event");
+            if (launch_kf(h, fin, fout, fields, KF_OUTER)) return cuda_err(h, cudaGetLastError(), "launch kf");
+            if (e) CK(cudaEventRecord(e[1], h->stream), "event");
+            CK(cudaStreamWaitEvent(h->stream, h->ev_ib, 0), "wait");
+            if (e) CK(cudaEventRecord(e[2], h->stream), "event");
+            if (launch_kf(h, fin, fout, fields, KF_INNER)) return cuda_err(h, cudaGetLastError(), "launch kf");
+            if (e) CK(cudaEventRecord(e[3], h->stream), "event");
+            CK(cudaEventRecord(h->ev_inner, h->stream), "event");
+        } else {
+            if (e) CK(cudaEventRecord(e[0], h->stream), "event");
+            if (launch_ib(h, fin, h->n, slot)) return cuda_err(h, cudaGetLastError(), "launch ib");
+            if (e) {
+                CK(cudaEventRecord(e[1], h->stream), "event");
+                CK(cudaEventRecord(e[2], h->stream), "event");
+            }
+            if (launch_kf(h, fin, fout, fields)) return cuda_err(h, cudaGetLastError(), "launch kf");
+            if (e) CK(cudaEventRecord(e[3], h->stream), "event");
+        }
         h->cur ^= 1;
         h->n++;
         h->steps_done++;
@@ -252,7 +299,7 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
                    "copy force rows");
             int st = check_status(h);
             if (st) return st;
-            if (h->timing && (st = collect_timing(h, pending))) return st;
+            if (h->timing && (st = collect_timing(h, pending, split))) return st;
             pending = 0;
         }
     }
@@ -263,7 +310,7 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
                "copy force rows");
         int st = check_status(h);
         if (st) return st;
-        if (h->timing && (st = collect_timing(h, pending))) return st;
+        if (h->timing && (st = collect_timing(h, pending, split))) return st;
     }
     if (done_out) *done_out = done;
     return rc;
@@ -326,10 +373,15 @@ int lbm_create(const lbm_params *p, lbm_t **out)
     h->elem = storage_size(h->prec);
     // nodes per thread of the lattice kernel; LBM_KF_VEC (1, 2 or 4) overrides
     // the default for tuning
-    h->kf_vec = 2;
+    h->kf_vec = 1;
     if (const char *ev = getenv("LBM_KF_VEC")) {
         const int v = atoi(ev);
         if (v == 1 || v == 2 || v == 4) h->kf_vec = v;
+    }
+    if (const char *ev = getenv("LBM_KF_TMA")) h->kf_tma = atoi(ev) != 0;
+    if (const char *ev = getenv("LBM_KF_ROWS")) {
+        const int v = atoi(ev);
+        if (v >= 1 && v <= 4096) h->kf_rows = v;
     }
     h->hx0.assign(std::max(1, h->npts), 0.0);
     h->hy0.assign(std::max(1, h->npts), 0.0);
@@ -344,10 +396,18 @@ int lbm_create(const lbm_params *p, lbm_t **out)
     };
     cudaError_t e;
     if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
-    const size_t fbytes = h->elem * 9 * (size_t)h->plane;
+    if ((e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "side stream");
+    if ((e = cudaEventCreateWithFlags(&h->ev_ib, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+    if ((e = cudaEventCreateWithFlags(&h->ev_inner, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+    if (const char *ov = getenv("LBM_OVERLAP")) h->overlap = atoi(ov) != 0;
+    // population buffers carry LBM_FPAD elements of padding before and after
+    // the 9 planes, so the bulk row copies of the lattice kernel (which read a
+    // 16-byte halo left and right of every row segment) stay in bounds
+    const size_t fbytes = h->elem * (9 * (size_t)h->plane + 2 * LBM_FPAD);
     for (int b = 0; b < 2; ++b) {
-        if ((e = cudaMalloc(&h->fbuf[b], fbytes)) != cudaSuccess) return fail(e, "alloc f");
-        if ((e = cudaMemset(h->fbuf[b], 0, fbytes)) != cudaSuccess) return fail(e, "clear f");
+        if ((e = cudaMalloc(&h->falloc[b], fbytes)) != cudaSuccess) return fail(e, "alloc f");
+        if ((e = cudaMemset(h->falloc[b], 0, fbytes)) != cudaSuccess) return fail(e, "clear f");
+        h->fbuf[b] = (char *)h->falloc[b] + h->elem * LBM_FPAD;
     }
     const size_t cs = compute_size(h->prec);
     const size_t nn = (size_t)h->nx * h->ny;
@@ -379,14 +439,19 @@ int lbm_destroy(lbm_t *h)
 {
     if (!h) return LBM_ERR_ARG;
     if (h->stream) cudaStreamSynchronize(h->stream);
-    for (int b = 0; b < 2; ++b) { free_dev(h->fbuf[b]); free_dev(h->d_fields[b]); }
+    for (int b = 0; b < 2; ++b) { free_dev(h->falloc[b]); h->fbuf[b] = nullptr; free_dev(h->d_fields[b]); }
     free_dev(h->edge_c);
     free_devp(h->d_xb0); free_devp(h->d_yb0); free_devp(h->d_arc); free_devp(h->d_mstep);
     free_ib(h);
     free_devp(h->d_pinfo); free_devp(h->d_counter);
     free_devp(h->d_ring); free_devp(h->d_status); free_devp(h->d_solve_res); free_devp(h->d_red);
     free_devp(h->d_stage);
+    if (h->side) cudaStreamSynchronize(h->side);
     for (auto &e : h->ev) cudaEventDestroy(e);
+    for (auto &e : h->ev_side) cudaEventDestroy(e);
+    if (h->ev_ib) cudaEventDestroy(h->ev_ib);
+    if (h->ev_inner) cudaEventDestroy(h->ev_inner);
+    if (h->side) cudaStreamDestroy(h->side);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return LBM_OK;
@@ -635,8 +700,10 @@ int lbm_set_timing(lbm_t *h, int enable)
 {
     if (!h) return LBM_ERR_ARG;
     if (enable && h->ev.empty()) {
-        h->ev.resize(3 * (size_t)h->ring_cap);
+        h->ev.resize(4 * (size_t)h->ring_cap);
+        h->ev_side.resize(2 * (size_t)h->ring_cap);
         for (auto &e : h->ev) CK(cudaEventCreate(&e), "event create");
+        for (auto &e : h->ev_side) CK(cudaEventCreate(&e), "event create");
     }
     h->timing = enable ? 1 : 0;
     h->t_step = h->t_ib = h->t_kf = 0;

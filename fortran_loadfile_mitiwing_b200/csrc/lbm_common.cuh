@@ -33,6 +33,7 @@ __host__ __device__ constexpr int lbm_ey(int k)
 #define LBM_ST_SOLVER 2u     // IB matrix not positive definite
 #define LBM_ST_NONFINITE 4u  // NaN/Inf in forces
 #define LBM_ST_OVERFLOW 8u   // patch larger than its allocation
+#define LBM_ST_TIMEOUT 16u   // a bounded wait on a shared-memory barrier gave up
 
 // current immersed-boundary correction patch (0-based node rectangle)
 struct PatchInfo {

@@ -30,7 +30,17 @@ struct KFArgs {
     const PatchInfo *pinfo;
     const C *patch;                    // interleaved (du, dv) per patch node
     C *rho_out, *u_out, *v_out;        // fields, when requested (else null)
+    int mode;                          // KF_ALL, KF_OUTER (skip rect), KF_INNER (rect only)
+    int rows_per_cta;                  // row sweep length of the staged kernel
+    unsigned *status;                  // device status word (bounded-wait timeouts)
+    int rx0, ry0, rw, rh;              // split rectangle (0-based origin, extent)
 };
+
+#define LBM_FPAD 64   // elements of padding before and after the population planes
+
+#define KF_ALL 0
+#define KF_OUTER 1
+#define KF_INNER 2
 
 // arguments of the immersed-boundary kernels
 struct IBArgs {
@@ -72,10 +82,13 @@ struct lbm_handle {
     double niu = 0, tau = 0, s[9] = {0};
     int prec = 0;
     size_t elem = 4;
-    int kf_vec = 4;   // nodes per thread of the lattice kernel (1, 2 or 4)
+    int kf_vec = 1;   // nodes per thread of the register-loading lattice kernel (1, 2 or 4)
+    int kf_tma = 1;   // bulk-copy staged lattice kernel (the default)
+    int kf_rows = 16; // rows swept by one CTA of the staged kernel
     int dev = 0;
     cudaStream_t stream = nullptr;
-    void *fbuf[2] = {nullptr, nullptr};
+    void *fbuf[2] = {nullptr, nullptr};     // first element of plane 0
+    void *falloc[2] = {nullptr, nullptr};   // allocations (fbuf - LBM_FPAD elements)
     int cur = 0;
     // edge constants (FP64 master + compute-precision copy)
     EdgeConst edge{};
@@ -101,6 +114,14 @@ struct lbm_handle {
     int patch_gx() const { return patch_wmax > 0 ? (patch_wmax + 15) / 16 : 1; }
     int patch_gy() const { return patch_hmax > 0 ? (patch_hmax + 15) / 16 : 1; }
     int ib_ready = 0;
+    // split of the lattice update around the bodies' motion envelope: the
+    // outer part runs concurrently with the immersed-boundary kernels on the
+    // side stream, the inner part after them (0-based rectangle, x origin and
+    // width multiples of 4)
+    int overlap = 1;
+    int env_x0 = 0, env_y0 = 0, env_w = 0, env_h = 0;
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_ib = nullptr, ev_inner = nullptr;
     double *d_partial = nullptr;
     unsigned *d_counter = nullptr;
     double *d_ring = nullptr;
@@ -114,9 +135,11 @@ struct lbm_handle {
     int fields_step[2] = {-1, -1}; // step index written into each slot
     double *d_red = nullptr;       // residual reduction scratch
     double *d_stage = nullptr;     // FP64 (nx,ny,9) staging for get/set of populations
-    // device timing (lbm_set_timing): three events per step slot of the ring
+    // device timing (lbm_set_timing): per step slot of the ring, four events on
+    // the main stream (start, lattice part 1 done, lattice part 2 start, end)
+    // and two on the side stream (IB start, IB end)
     int timing = 0;
-    std::vector<cudaEvent_t> ev;
+    std::vector<cudaEvent_t> ev, ev_side;
     double t_step = 0, t_ib = 0, t_kf = 0;
     int t_steps = 0;
     // driver state
@@ -130,8 +153,8 @@ struct lbm_handle {
 int ib_configure(lbm_handle *h);
 int ib_max_markers();
 size_t ib_block_scratch(int nseg, size_t *d, size_t *l, size_t *f, size_t *x);
-int launch_kf(lbm_handle *h, const void *fin, void *fout, void *fields);
-int launch_ib(lbm_handle *h, const void *fin, int step_index, int ring_slot);
+int launch_kf(lbm_handle *h, const void *fin, void *fout, void *fields, int mode = KF_ALL, cudaStream_t st = nullptr);
+int launch_ib(lbm_handle *h, const void *fin, int step_index, int ring_slot, cudaStream_t st = nullptr);
 int launch_residual(lbm_handle *h, const void *fa, const void *fb, double *out2);
 int launch_unpack(lbm_handle *h, const void *fsrc, double *dst);   // deviation -> f (FP64)
 int launch_pack(lbm_handle *h, const double *src, void *fdst);     // f (FP64) -> deviation
