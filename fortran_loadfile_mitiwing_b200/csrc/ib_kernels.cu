@@ -30,7 +30,7 @@
 namespace {
 
 constexpr int BS = 16;                 // cyclic-reduction block size
-constexpr int NSORT_MAX = 4096;        // largest marker count (sort in shared memory)
+constexpr int NSORT_MAX = 2048;        // largest marker count (sort in shared memory)
 constexpr int SOLVE_THREADS = 1024;
 constexpr int BOPS_WARPS = 16;             // warps running block operations
 constexpr int FC = 2 * BS + 2;             // columns of F: [D^-1 L | D^-1 U | D^-1 r]
@@ -195,55 +195,57 @@ __device__ __forceinline__ double bval(const Marker &mk, const Marker &ml)
     return sx * sy;
 }
 
-__device__ __forceinline__ bool boxes_overlap(const Marker &mk, const Marker &ml)
-{
-    return max(mk.i1, ml.i1) <= min(mk.i2, ml.i2) && max(mk.j1, ml.j1) <= min(mk.j2, ml.j2);
-}
 
-// Cholesky of one BS x BS block by one warp, in shared memory (lower
-// triangle, row-major); returns false if not positive definite
-__device__ bool warp_chol(double *G)
+// In-place inverse of one symmetric positive definite BS x BS block by one
+// warp (Gauss-Jordan without pivoting, stable for SPD), row-major in shared
+// memory; each of the BS steps is one parallel rank-1 update. Returns false
+// if a pivot is not positive.
+__device__ bool warp_inv(double *G)
 {
     const int lane = threadIdx.x & 31;
     bool ok = true;
     for (int k = 0; k < BS; ++k) {
-        const double d = G[k * BS + k];
-        const bool good = d > 0.0 && isfinite(d);
+        const double p = G[k * BS + k];
+        const bool good = p > 0.0 && isfinite(p);
         ok = ok && good;
-        const double dk = good ? sqrt(d) : 1.0;
+        const double piv = good ? 1.0 / p : 1.0;
         __syncwarp();
-        if (lane == 0) G[k * BS + k] = dk;
-        for (int i = k + 1 + lane; i < BS; i += 32) G[i * BS + k] /= dk;
+        if (lane < BS && lane != k) G[k * BS + lane] *= piv;            // row k
         __syncwarp();
-        for (int q = lane; q < BS * BS; q += 32) {
+#pragma unroll
+        for (int q = lane; q < BS * BS; q += 32) {                       // other rows
             const int i = q / BS, j = q % BS;
-            if (j > k && j <= i) G[i * BS + j] -= G[i * BS + k] * G[j * BS + k];
+            if (i != k && j != k) G[q] -= G[i * BS + k] * G[k * BS + j];
         }
+        __syncwarp();
+        if (lane < BS && lane != k) G[lane * BS + k] *= -piv;           // column k
+        if (lane == 0) G[k * BS + k] = piv;
         __syncwarp();
     }
     return ok;
 }
 
-// X <- (G G^T)^-1 X for a row-major BS x ncol matrix X in global memory
-// (lane per column)
-__device__ void warp_chol_solve(const double *G, double *X, int ncol)
+// C = A B for a BS x BS matrix A and BS x ncol matrices B, C (row-major,
+// leading dimension ncol), one warp, independent dot products per lane
+__device__ void warp_mm(const double *A, const double *B, double *C, int ncol)
 {
     const int lane = threadIdx.x & 31;
-    for (int c = lane; c < ncol; c += 32) {
-        for (int r = 0; r < BS; ++r) {
-            double s = X[r * ncol + c];
-            for (int q = 0; q < r; ++q) s -= G[r * BS + q] * X[q * ncol + c];
-            X[r * ncol + c] = s / G[r * BS + r];
-        }
-        for (int r = BS - 1; r >= 0; --r) {
-            double s = X[r * ncol + c];
-            for (int q = r + 1; q < BS; ++q) s -= G[q * BS + r] * X[q * ncol + c];
-            X[r * ncol + c] = s / G[r * BS + r];
-        }
+    for (int q = lane; q < BS * ncol; q += 32) {
+        const int r = q / ncol, c = q % ncol;
+        double s = 0.0;
+#pragma unroll
+        for (int t = 0; t < BS; ++t) s += A[r * BS + t] * B[t * ncol + c];
+        C[q] = s;
     }
     __syncwarp();
 }
 
+__device__ __forceinline__ bool box_overlap(int4 p, int4 q)
+{
+    return max(p.x, q.x) <= min(p.y, q.y) && max(p.z, q.z) <= min(p.w, q.w);
+}
+
+// time and motion columns of this step's force.dat row (solution.f90:350-375)
 __device__ void write_header(const IBArgs &a, const double *row, double time, int ring_slot)
 {
     double *fr = a.force_ring + (long long)ring_slot * a.row_len;
@@ -354,9 +356,10 @@ __device__ void solve_residual(const IBArgs &a, const double *key, const int *id
 }
 
 // The linear solve of one step, one CTA of SOLVE_THREADS threads.
-// Dynamic shared memory: key[ns] (double), idx[ns] (int, then ns ints of
-// padding), then one block-operation workspace of WS doubles for each of the
-// first BOPS_WARPS warps; ns = n rounded up to a power of two.
+// Dynamic shared memory: key[ns] (double), box[ns] (int4, marker support box
+// i1,i2,j1,j2), idx[ns] (int, then ns ints of padding), then one
+// block-operation workspace of WS doubles for each of the first BOPS_WARPS
+// warps; ns = n rounded up to a power of two.
 __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int step_index, int ring_slot)
 {
     extern __shared__ double smem[];
@@ -365,10 +368,12 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
     int ns = 1;
     while (ns < n) ns <<= 1;
     double *key = smem;
-    int *idx = (int *)(key + ns);
+    int4 *box = (int4 *)(key + ns);
+    int *idx = (int *)(box + ns);
     double *Wbase = (double *)(idx + 2 * ns);
     __shared__ int bb[4];
     __shared__ double ext[4];
+    __shared__ double wext[32][4];
     __shared__ int wmax, bad;
     const Marker *mk = a.mk;
     if (tid == 0) {
@@ -377,15 +382,15 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
         wmax = 0; bad = 0;
     }
     __syncthreads();
-    // patch rectangle and marker-cloud extent
+    // support boxes to shared memory; patch rectangle and marker-cloud extent
     double lx0 = 1e300, lx1 = -1e300, ly0 = 1e300, ly1 = -1e300;
     int b0 = 1 << 30, b1 = 1 << 30, b2 = -1, b3 = -1;
     for (int k = tid; k < n; k += nt) {
-        const Marker &m = mk[k];
-        lx0 = fmin(lx0, m.xm); lx1 = fmax(lx1, m.xm); ly0 = fmin(ly0, m.ym); ly1 = fmax(ly1, m.ym);
-        if (m.i2 >= m.i1 && m.j2 >= m.j1) {
-            b0 = min(b0, m.i1); b1 = min(b1, m.j1); b2 = max(b2, m.i2); b3 = max(b3, m.j2);
-        }
+        const double xm = mk[k].xm, ym = mk[k].ym;
+        const int4 q = make_int4(mk[k].i1, mk[k].i2, mk[k].j1, mk[k].j2);
+        box[k] = q;
+        lx0 = fmin(lx0, xm); lx1 = fmax(lx1, xm); ly0 = fmin(ly0, ym); ly1 = fmax(ly1, ym);
+        if (q.y >= q.x && q.w >= q.z) { b0 = min(b0, q.x); b1 = min(b1, q.z); b2 = max(b2, q.y); b3 = max(b3, q.w); }
     }
     for (int off = 16; off; off >>= 1) {
         lx0 = fmin(lx0, __shfl_xor_sync(0xffffffffu, lx0, off));
@@ -397,7 +402,6 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
         b2 = max(b2, __shfl_xor_sync(0xffffffffu, b2, off));
         b3 = max(b3, __shfl_xor_sync(0xffffffffu, b3, off));
     }
-    __shared__ double wext[32][4];
     if (lane == 0) {
         atomicMin(&bb[0], b0); atomicMin(&bb[1], b1); atomicMax(&bb[2], b2); atomicMax(&bb[3], b3);
         wext[warp][0] = lx0; wext[warp][1] = lx1; wext[warp][2] = ly0; wext[warp][3] = ly1;
@@ -450,8 +454,9 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
     const double reach = 6.0 * a.scale;
     for (int s = tid; s < n; s += nt) {
         int wl = 0;
+        const int4 ps = box[idx[s]];
         for (int t = s + 1; t < n && key[t] - key[s] <= reach; ++t)
-            if (boxes_overlap(mk[idx[s]], mk[idx[t]])) wl = t - s;
+            if (box_overlap(ps, box[idx[t]])) wl = t - s;
         if (wl) atomicMax(&wmax, wl);
     }
     __syncthreads();
@@ -465,54 +470,89 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
     }
     // block tridiagonal form: D_i (BS x BS), L_i couples block i to block i-1,
     // X_i holds the two right-hand sides (BS x 2), padded with identity rows;
-    // D0/L0 keep the assembled blocks for the residual
+    // D0/L0 keep the assembled blocks for the residual. One warp per block,
+    // with the block's and the previous block's markers staged in W.
     const int nb = (n + BS - 1) / BS;
     double *Db = a.bD, *Lb = a.bL, *Fb = a.bF, *Xb = a.bX;
     double *D0 = a.bD + (long long)nb * BS * BS, *L0 = a.bL + (long long)nb * BS * BS;
-    for (long long q = tid; q < (long long)nb * BS * BS; q += nt) {
-        const int blk = (int)(q / (BS * BS)), r = (int)(q % (BS * BS)) / BS, c = (int)(q % BS);
-        const int sr = blk * BS + r, sc = blk * BS + c, sp = (blk - 1) * BS + c;
-        double d;
-        if (sr < n && sc < n) d = bval(mk[idx[sr]], mk[idx[sc]]);
-        else d = (r == c) ? 1.0 : 0.0;
-        const double l = (blk > 0 && sr < n) ? bval(mk[idx[sr]], mk[idx[sp]]) : 0.0;
-        Db[q] = d;
-        D0[q] = d;
-        Lb[q] = l;
-        L0[q] = l;
-    }
+    double *W = Wbase + (long long)warp * WS;
+    const bool bw = warp < BOPS_WARPS;
+    if (bw)
+        for (int blk = warp; blk < nb; blk += BOPS_WARPS) {
+            // staged markers: 2*BS entries of (phx[6], phy[6]) and boxes
+            double *ph = W;                                  // [2*BS][12]
+            int4 *bxw = (int4 *)(W + 2 * BS * 12);           // [2*BS]
+            for (int q = lane; q < 2 * BS * 12; q += 32) {
+                const int m = q / 12, c = q % 12;
+                const int srt = (blk - 1) * BS + m;          // m < BS: previous block
+                double v = 0.0;
+                if (srt >= 0 && srt < n) {
+                    const Marker &mm = mk[idx[srt]];
+                    v = c < 6 ? mm.phx[c] : mm.phy[c - 6];
+                }
+                ph[q] = v;
+            }
+            for (int m = lane; m < 2 * BS; m += 32) {
+                const int srt = (blk - 1) * BS + m;
+                bxw[m] = (srt >= 0 && srt < n) ? box[idx[srt]] : make_int4(1, 0, 1, 0);
+            }
+            __syncwarp();
+            for (int q = lane; q < 2 * BS * BS; q += 32) {
+                const int r = (q % (BS * BS)) / BS, c = q % BS;
+                const bool lower = q >= BS * BS;             // coupling to the previous block
+                const int mr = BS + r, mc = lower ? c : BS + c;
+                const int sr = blk * BS + r;
+                double v;
+                const int4 p = bxw[mr], o = bxw[mc];
+                if (sr >= n) {
+                    v = (!lower && r == c) ? 1.0 : 0.0;
+                } else if (!lower && blk * BS + c >= n) {
+                    v = 0.0;
+                } else if (lower && blk == 0) {
+                    v = 0.0;
+                } else {
+                    const int ia = max(p.x, o.x), ib = min(p.y, o.y), ja = max(p.z, o.z), jb = min(p.w, o.w);
+                    v = 0.0;
+                    if (ia <= ib && ja <= jb) {
+                        double sx = 0.0, sy = 0.0;
+                        for (int i = ia; i <= ib; ++i) sx += ph[mr * 12 + i - p.x] * ph[mc * 12 + i - o.x];
+                        for (int j = ja; j <= jb; ++j) sy += ph[mr * 12 + 6 + j - p.z] * ph[mc * 12 + 6 + j - o.z];
+                        v = sx * sy;
+                    }
+                }
+                const long long g = (long long)blk * BS * BS + r * BS + c;
+                if (lower) { Lb[g] = v; L0[g] = v; }
+                else { Db[g] = v; D0[g] = v; }
+            }
+            __syncwarp();
+        }
     for (int q = tid; q < nb * BS; q += nt) {
         Xb[2 * q] = q < n ? a.rhs[idx[q]] : 0.0;
         Xb[2 * q + 1] = q < n ? a.rhs[n + idx[q]] : 0.0;
     }
     __syncthreads();
     // cyclic reduction: at stride st the active blocks are multiples of st;
-    // odd multiples are eliminated into their even neighbours. Each block
-    // operation runs on one warp in its shared-memory workspace W.
-    double *W = Wbase + (long long)warp * WS;
-    const bool bw = warp < BOPS_WARPS;
+    // odd multiples are eliminated into their even neighbours
     int levels = 0;
     for (int st = 1; st < nb; st <<= 1, ++levels) {
         const int nodd = (nb - st + 2 * st - 1) / (2 * st);
         if (bw)
             for (int m = warp; m < nodd; m += BOPS_WARPS) {
+                // F_o = D_o^-1 [L_o | L_q^T | r_o]
                 const int o = st * (2 * m + 1), q2 = o + st;
-                double *Gs = W, *Fs = W + BS * BS;
+                double *Gs = W, *Rs = W + BS * BS;
                 for (int e = lane; e < BS * BS; e += 32) Gs[e] = Db[(long long)o * BS * BS + e];
                 for (int e = lane; e < BS * FC; e += 32) {
                     const int r = e / FC, c = e % FC;
                     double v;
-                    if (c < BS) v = Lb[(long long)o * BS * BS + r * BS + c];                      // L_o
-                    else if (c < 2 * BS) v = q2 < nb ? Lb[(long long)q2 * BS * BS + (c - BS) * BS + r] : 0.0;  // U_o = L_q^T
-                    else v = Xb[2 * ((long long)o * BS + r) + (c - 2 * BS)];                      // r_o
-                    Fs[e] = v;
+                    if (c < BS) v = Lb[(long long)o * BS * BS + r * BS + c];
+                    else if (c < 2 * BS) v = q2 < nb ? Lb[(long long)q2 * BS * BS + (c - BS) * BS + r] : 0.0;
+                    else v = Xb[2 * ((long long)o * BS + r) + (c - 2 * BS)];
+                    Rs[e] = v;
                 }
                 __syncwarp();
-                if (!warp_chol(Gs) && lane == 0) bad = 1;
-                warp_chol_solve(Gs, Fs, FC);
-                double *F = Fb + (long long)o * BS * FC;
-                for (int e = lane; e < BS * FC; e += 32) F[e] = Fs[e];
-                __syncwarp();
+                if (!warp_inv(Gs) && lane == 0) bad = 1;
+                warp_mm(Gs, Rs, Fb + (long long)o * BS * FC, FC);
             }
         __syncthreads();
         const int neven = (nb + 2 * st - 1) / (2 * st);
@@ -536,10 +576,12 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
                         double sum = 0.0;
                         if (q < BS * BS) {
                             const int r = q / BS, c = q % BS;
+#pragma unroll
                             for (int t = 0; t < BS; ++t) sum += As[t * BS + r] * Fs[t * FC + c];
                             Ds[q] -= sum;
                         } else {
                             const int r = (q - BS * BS) / 2, c = (q - BS * BS) % 2;
+#pragma unroll
                             for (int t = 0; t < BS; ++t) sum += As[t * BS + r] * Fs[t * FC + 2 * BS + c];
                             Xs[2 * r + c] -= sum;
                         }
@@ -557,6 +599,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
                         if (q < BS * BS) {
                             const int r = q / BS, c = q % BS;
                             double s1 = 0.0, s2 = 0.0;
+#pragma unroll
                             for (int t = 0; t < BS; ++t) {
                                 const double l = As[r * BS + t];
                                 s1 += l * Fs[t * FC + BS + c];
@@ -567,6 +610,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
                         } else {
                             const int r = (q - BS * BS) / 2, c = (q - BS * BS) % 2;
                             double sum = 0.0;
+#pragma unroll
                             for (int t = 0; t < BS; ++t) sum += As[r * BS + t] * Fs[t * FC + 2 * BS + c];
                             Xs[2 * r + c] -= sum;
                         }
@@ -581,12 +625,12 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
     }
     // the last active block (block 0)
     if (warp == 0) {
-        double *Gs = W, *Fs = W + BS * BS;
+        double *Gs = W, *Rs = W + BS * BS, *Fs = Rs + 2 * BS;
         for (int e = lane; e < BS * BS; e += 32) Gs[e] = Db[e];
-        for (int e = lane; e < 2 * BS; e += 32) Fs[e] = Xb[e];
+        for (int e = lane; e < 2 * BS; e += 32) Rs[e] = Xb[e];
         __syncwarp();
-        if (!warp_chol(Gs) && lane == 0) bad = 1;
-        warp_chol_solve(Gs, Fs, 2);
+        if (!warp_inv(Gs) && lane == 0) bad = 1;
+        warp_mm(Gs, Rs, Fs, 2);
         for (int e = lane; e < 2 * BS; e += 32) Xb[e] = Fs[e];
     }
     __syncthreads();
@@ -599,11 +643,14 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
             const double *F = Fb + (long long)o * BS * FC;
             for (int q = lane; q < 2 * BS; q += 32) {
                 const int r = q / 2, c = q % 2;
-                double sum = F[r * FC + 2 * BS + c];
-                for (int t = 0; t < BS; ++t) sum -= F[r * FC + t] * Xb[2 * ((long long)p * BS + t) + c];
-                if (q2 < nb)
-                    for (int t = 0; t < BS; ++t) sum -= F[r * FC + BS + t] * Xb[2 * ((long long)q2 * BS + t) + c];
-                Xb[2 * ((long long)o * BS + r) + c] = sum;
+                double s1 = F[r * FC + 2 * BS + c], s2 = 0.0;
+#pragma unroll
+                for (int t = 0; t < BS; ++t) s1 -= F[r * FC + t] * Xb[2 * ((long long)p * BS + t) + c];
+                if (q2 < nb) {
+#pragma unroll
+                    for (int t = 0; t < BS; ++t) s2 += F[r * FC + BS + t] * Xb[2 * ((long long)q2 * BS + t) + c];
+                }
+                Xb[2 * ((long long)o * BS + r) + c] = s1 - s2;
             }
         }
         __syncthreads();
@@ -616,18 +663,26 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
     double num = 0.0, den = 0.0;
     for (int s = tid; s < n; s += nt) {
         const int i = s / BS, r = s % BS;
-        double acc[2];
-        for (int c = 0; c < 2; ++c) {
-            double sum = 0.0;
-            for (int t = 0; t < BS; ++t) sum += D0[((long long)i * BS + r) * BS + t] * Xb[2 * ((long long)i * BS + t) + c];
-            if (i > 0)
-                for (int t = 0; t < BS; ++t) sum += L0[((long long)i * BS + r) * BS + t] * Xb[2 * ((long long)(i - 1) * BS + t) + c];
-            if (i + 1 < nb)
-                for (int t = 0; t < BS; ++t) sum += L0[((long long)(i + 1) * BS + t) * BS + r] * Xb[2 * ((long long)(i + 1) * BS + t) + c];
-            acc[c] = sum;
+        double a0 = 0.0, a1 = 0.0, c0 = 0.0, c1 = 0.0, e0 = 0.0, e1 = 0.0;
+        const double *dr = D0 + ((long long)i * BS + r) * BS;
+        const double *xi = Xb + 2 * (long long)i * BS;
+#pragma unroll
+        for (int t = 0; t < BS; ++t) { a0 += dr[t] * xi[2 * t]; a1 += dr[t] * xi[2 * t + 1]; }
+        if (i > 0) {
+            const double *lr = L0 + ((long long)i * BS + r) * BS;
+            const double *xp = Xb + 2 * (long long)(i - 1) * BS;
+#pragma unroll
+            for (int t = 0; t < BS; ++t) { c0 += lr[t] * xp[2 * t]; c1 += lr[t] * xp[2 * t + 1]; }
+        }
+        if (i + 1 < nb) {
+            const double *ln = L0 + (long long)(i + 1) * BS * BS + r;
+            const double *xq = Xb + 2 * (long long)(i + 1) * BS;
+#pragma unroll
+            for (int t = 0; t < BS; ++t) { e0 += ln[t * BS] * xq[2 * t]; e1 += ln[t * BS] * xq[2 * t + 1]; }
         }
         const double b0 = a.rhs[idx[s]], b1 = a.rhs[n + idx[s]];
-        num += (acc[0] - b0) * (acc[0] - b0) + (acc[1] - b1) * (acc[1] - b1);
+        const double r0 = a0 + c0 + e0 - b0, r1 = a1 + c1 + e1 - b1;
+        num += r0 * r0 + r1 * r1;
         den += b0 * b0 + b1 * b1;
     }
     finish_residual(a, num, den, wmax, bad);
@@ -778,7 +833,7 @@ size_t solve_smem(int n)
 {
     int ns = 1;
     while (ns < n) ns <<= 1;
-    return sizeof(double) * ns + sizeof(int) * 2 * ns + sizeof(double) * BOPS_WARPS * WS;
+    return sizeof(double) * ns + sizeof(int4) * ns + sizeof(int) * 2 * ns + sizeof(double) * BOPS_WARPS * WS;
 }
 
 IBArgs make_args(lbm_handle *h, const void *fin)
