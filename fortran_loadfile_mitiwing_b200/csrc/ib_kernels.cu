@@ -1,5 +1,5 @@
 // ib_kernels.cu -- immersed boundary of one time step (FP64), ahead of the
-// fused lattice update.
+// lattice update of the correction patch.
 //
 // Reference: move_boundary (airfoil.f90:244-338) and immersed_boundary_Wu
 // (boundary_condition.f90:1512-1736). The reference builds dense X1 (nseg x
@@ -7,34 +7,43 @@
 // solves A x = U_b - X1 u* by LU (cusolverDnDgetrf/getrs) and spreads
 // du = X2 x. With D = X1, A = (D D^T) W, so y = W x solves the symmetric
 // positive definite system (D D^T) y = U_b - D u* and du = D^T y: the same
-// correction, with arc_l dropping out. Three launches:
+// correction, with arc_l dropping out. The launches of one step:
 //   ib_markers  one warp per marker: position, boundary velocity, support box
 //               and one-axis kernel values (move_boundary, :1540-1606), then
 //               b = D u* over the box with a warp-shuffle sum (:1609-1629);
-//   ib_solve    one CTA: correction-patch rectangle and force-row header;
-//               markers sorted along the longer axis of the marker cloud,
-//               where D D^T is banded (delta supports overlap only for
-//               markers less than 6 lu apart); the band is cut into 16x16
-//               blocks and solved by block cyclic reduction (FP64, log2 of the
-//               block count levels); a dense Cholesky is the fallback when a
-//               coupling reaches past the neighbouring block;
+//   ib_order    (several bodies only) one CTA sorts the markers along the
+//               longer axis of the marker cloud. A single rigid body keeps one
+//               order for the whole run: its markers sorted by body-frame
+//               chordwise position, computed once on the host;
+//   ib_assemble one CTA per 16-marker block of that order: D D^T is banded in
+//               it (delta supports overlap only for markers less than 5 lu
+//               apart per axis), so the CTA builds its diagonal block and the
+//               block coupling it to the previous one, and checks that no
+//               coupling reaches further;
+//   ib_solve    one CTA: correction-patch rectangle, force-row header, block
+//               cyclic reduction of the block tridiagonal system (log2 of the
+//               block count levels of Gauss-Jordan block inverses and block
+//               products, FP64), back substitution; a dense Cholesky replaces
+//               it when a coupling reaches past the neighbouring block;
 //   ib_spread   du = D^T y per node, gathered in marker order over the
 //               markers whose box covers the node (no atomics), written to the
 //               correction patch the lattice kernel reads; force and moment
-//               sums in FP64 with a deterministic two-level reduction
-//               (:1645-1675, solution.f90:327-336).
+//               sums (:1645-1675, solution.f90:327-336) and the solve
+//               residual in FP64 with a deterministic two-level reduction.
 #include <math.h>
 
 #include "lbm_internal.h"
 
 namespace {
 
-constexpr int BS = 16;                 // cyclic-reduction block size
-constexpr int NSORT_MAX = 2048;        // largest marker count (sort in shared memory)
-constexpr int SOLVE_THREADS = 1024;
-constexpr int BOPS_WARPS = 16;             // warps running block operations
-constexpr int FC = 2 * BS + 2;             // columns of F: [D^-1 L | D^-1 U | D^-1 r]
-constexpr int WS = BS * BS + BS * FC + BS * BS + 2 * BS;   // workspace per warp (doubles)
+constexpr int BS = 16;                 // block size of the cyclic reduction
+constexpr int NMARK_MAX = 2048;        // largest marker count
+constexpr int SOLVE_THREADS = 512;
+constexpr int BOPS_WARPS = 16;         // warps running block operations
+constexpr int FC = 2 * BS + 2;         // columns of F: [D^-1 L | D^-1 U | D^-1 r]
+constexpr int GP = BS + 1;             // padded row stride of square blocks in shared memory
+constexpr int WS = BS * GP + BS * FC + BS * GP + 2 * BS;   // workspace per warp (doubles)
+constexpr int NPART = 3 * LBM_MAXW + 3;                     // per-CTA partials of ib_spread
 
 // one-axis kernel value (boundary_condition.f90:1563-1600), disr = |r|
 __device__ __forceinline__ double delta1(double disr, int smooth)
@@ -195,55 +204,12 @@ __device__ __forceinline__ double bval(const Marker &mk, const Marker &ml)
     return sx * sy;
 }
 
-
-// In-place inverse of one symmetric positive definite BS x BS block by one
-// warp (Gauss-Jordan without pivoting, stable for SPD), row-major in shared
-// memory; each of the BS steps is one parallel rank-1 update. Returns false
-// if a pivot is not positive.
-__device__ bool warp_inv(double *G)
-{
-    const int lane = threadIdx.x & 31;
-    bool ok = true;
-    for (int k = 0; k < BS; ++k) {
-        const double p = G[k * BS + k];
-        const bool good = p > 0.0 && isfinite(p);
-        ok = ok && good;
-        const double piv = good ? 1.0 / p : 1.0;
-        __syncwarp();
-        if (lane < BS && lane != k) G[k * BS + lane] *= piv;            // row k
-        __syncwarp();
-#pragma unroll
-        for (int q = lane; q < BS * BS; q += 32) {                       // other rows
-            const int i = q / BS, j = q % BS;
-            if (i != k && j != k) G[q] -= G[i * BS + k] * G[k * BS + j];
-        }
-        __syncwarp();
-        if (lane < BS && lane != k) G[lane * BS + k] *= -piv;           // column k
-        if (lane == 0) G[k * BS + k] = piv;
-        __syncwarp();
-    }
-    return ok;
-}
-
-// C = A B for a BS x BS matrix A and BS x ncol matrices B, C (row-major,
-// leading dimension ncol), one warp, independent dot products per lane
-__device__ void warp_mm(const double *A, const double *B, double *C, int ncol)
-{
-    const int lane = threadIdx.x & 31;
-    for (int q = lane; q < BS * ncol; q += 32) {
-        const int r = q / ncol, c = q % ncol;
-        double s = 0.0;
-#pragma unroll
-        for (int t = 0; t < BS; ++t) s += A[r * BS + t] * B[t * ncol + c];
-        C[q] = s;
-    }
-    __syncwarp();
-}
-
 __device__ __forceinline__ bool box_overlap(int4 p, int4 q)
 {
     return max(p.x, q.x) <= min(p.y, q.y) && max(p.z, q.z) <= min(p.w, q.w);
 }
+
+__device__ __forceinline__ int4 mbox(const Marker &m) { return make_int4(m.i1, m.i2, m.j1, m.j2); }
 
 // time and motion columns of this step's force.dat row (solution.f90:350-375)
 __device__ void write_header(const IBArgs &a, const double *row, double time, int ring_slot)
@@ -259,17 +225,207 @@ __device__ void write_header(const IBArgs &a, const double *row, double time, in
     }
 }
 
+// Several bodies: sort the markers along the longer axis of the marker cloud
+// (stable, ties by index) into perm/key, with reach = 6 lattice units along
+// that axis. One CTA; dynamic shared memory key[ns] (double) + idx[ns] (int).
+__global__ void __launch_bounds__(1024) ib_order(const IBArgs a)
+{
+    extern __shared__ double osm[];
+    const int n = a.nseg, tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
+    int ns = 1;
+    while (ns < n) ns <<= 1;
+    double *key = osm;
+    int *idx = (int *)(key + ns);
+    __shared__ double wext[32][4];
+    __shared__ bool by_x;
+    double lx0 = 1e300, lx1 = -1e300, ly0 = 1e300, ly1 = -1e300;
+    for (int k = tid; k < n; k += nt) {
+        const double xm = a.mk[k].xm, ym = a.mk[k].ym;
+        lx0 = fmin(lx0, xm); lx1 = fmax(lx1, xm); ly0 = fmin(ly0, ym); ly1 = fmax(ly1, ym);
+    }
+    for (int off = 16; off; off >>= 1) {
+        lx0 = fmin(lx0, __shfl_xor_sync(0xffffffffu, lx0, off));
+        lx1 = fmax(lx1, __shfl_xor_sync(0xffffffffu, lx1, off));
+        ly0 = fmin(ly0, __shfl_xor_sync(0xffffffffu, ly0, off));
+        ly1 = fmax(ly1, __shfl_xor_sync(0xffffffffu, ly1, off));
+    }
+    if (lane == 0) { wext[warp][0] = lx0; wext[warp][1] = lx1; wext[warp][2] = ly0; wext[warp][3] = ly1; }
+    __syncthreads();
+    if (tid == 0) {
+        double e0 = 1e300, e1 = -1e300, e2 = 1e300, e3 = -1e300;
+        for (int w = 0; w < (nt >> 5); ++w) {
+            e0 = fmin(e0, wext[w][0]); e1 = fmax(e1, wext[w][1]);
+            e2 = fmin(e2, wext[w][2]); e3 = fmax(e3, wext[w][3]);
+        }
+        by_x = (e1 - e0) >= (e3 - e2);
+        *a.reach = 6.0 * a.scale;
+    }
+    __syncthreads();
+    for (int s2 = tid; s2 < ns; s2 += nt) {
+        key[s2] = s2 < n ? (by_x ? a.mk[s2].xm : a.mk[s2].ym) : 1e300;
+        idx[s2] = s2;
+    }
+    __syncthreads();
+    for (int size = 2; size <= ns; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int s2 = tid; s2 < ns; s2 += nt) {
+                const int t = s2 ^ stride;
+                if (t > s2) {
+                    const bool up = (s2 & size) == 0;
+                    const bool gt = key[s2] > key[t] || (key[s2] == key[t] && idx[s2] > idx[t]);
+                    if (gt == up) {
+                        const double kk = key[s2]; key[s2] = key[t]; key[t] = kk;
+                        const int ii = idx[s2]; idx[s2] = idx[t]; idx[t] = ii;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (int s2 = tid; s2 < n; s2 += nt) {
+        a.perm[s2] = idx[s2];
+        a.key[s2] = key[s2];
+    }
+}
+
+// One CTA per block of BS markers in the solve order: the diagonal block D_b
+// and the coupling L_b to block b-1 (kept twice: working copy and assembled
+// copy for the residual), the block's right-hand sides, and the longest
+// coupling in the order (half-bandwidth).
+__global__ void __launch_bounds__(256) ib_assemble(const IBArgs a)
+{
+    const int n = a.nseg, blk = blockIdx.x, tid = threadIdx.x;
+    __shared__ double ph[2 * BS][12];
+    __shared__ int4 bx[2 * BS];
+    __shared__ int wl;
+    if (tid == 0) wl = 0;
+    for (int q = tid; q < 2 * BS * 12; q += blockDim.x) {
+        const int m = q / 12, c = q % 12, srt = (blk - 1) * BS + m;
+        double v = 0.0;
+        if (srt >= 0 && srt < n) {
+            const Marker &mm = a.mk[a.perm[srt]];
+            v = c < 6 ? mm.phx[c] : mm.phy[c - 6];
+        }
+        ph[m][c] = v;
+    }
+    for (int m = tid; m < 2 * BS; m += blockDim.x) {
+        const int srt = (blk - 1) * BS + m;
+        bx[m] = (srt >= 0 && srt < n) ? mbox(a.mk[a.perm[srt]]) : make_int4(1, 0, 1, 0);
+    }
+    __syncthreads();
+    const int nb = (n + BS - 1) / BS;
+    double *D0 = a.bD + (long long)nb * BS * BS, *L0 = a.bL + (long long)nb * BS * BS;
+    for (int q = tid; q < 2 * BS * BS; q += blockDim.x) {
+        const bool lower = q >= BS * BS;
+        const int r = (q % (BS * BS)) / BS, c = q % BS;
+        const int mr = BS + r, mc = lower ? c : BS + c, sr = blk * BS + r;
+        double v = 0.0;
+        if (sr >= n) {
+            v = (!lower && r == c) ? 1.0 : 0.0;
+        } else if ((!lower && blk * BS + c < n) || (lower && blk > 0)) {
+            const int4 p = bx[mr], o = bx[mc];
+            const int ia = max(p.x, o.x), ib = min(p.y, o.y), ja = max(p.z, o.z), jb = min(p.w, o.w);
+            if (ia <= ib && ja <= jb) {
+                double sx = 0.0, sy = 0.0;
+                for (int i = ia; i <= ib; ++i) sx += ph[mr][i - p.x] * ph[mc][i - o.x];
+                for (int j = ja; j <= jb; ++j) sy += ph[mr][6 + j - p.z] * ph[mc][6 + j - o.z];
+                v = sx * sy;
+            }
+        }
+        const long long g = (long long)blk * BS * BS + r * BS + c;
+        if (lower) { a.bL[g] = v; L0[g] = v; }
+        else { a.bD[g] = v; D0[g] = v; }
+    }
+    if (tid < 2 * BS) {
+        const int r = tid / 2, c = tid % 2, srt = blk * BS + r;
+        a.bX[2 * srt + c] = srt < n ? a.rhs[c * n + a.perm[srt]] : 0.0;
+    }
+    // half-bandwidth: boxes (<= 6 nodes wide) overlap only for markers closer
+    // than `reach` along the order's key
+    if (tid < BS) {
+        const int srt = blk * BS + tid;
+        if (srt < n) {
+            const double reach = *a.reach;
+            const int4 p = bx[BS + tid];
+            const double ks = a.key[srt];
+            int w = 0;
+            for (int t = srt + 1; t < n && a.key[t] - ks <= reach; ++t)
+                if (box_overlap(p, mbox(a.mk[a.perm[t]]))) w = t - srt;
+            if (w) atomicMax(&wl, w);
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && wl) atomicMax(a.wmax, wl);
+}
+
+// In-place inverse of one symmetric positive definite BS x BS block by one
+// warp (Gauss-Jordan without pivoting, stable for SPD), row stride GP in
+// shared memory; each of the BS steps is one parallel rank-1 update.
+// Returns false if a pivot is not positive.
+__device__ bool warp_inv(double *G)
+{
+    const int lane = threadIdx.x & 31;
+    bool ok = true;
+    for (int k = 0; k < BS; ++k) {
+        const double p = G[k * GP + k];
+        const bool good = p > 0.0 && isfinite(p);
+        ok = ok && good;
+        const double piv = good ? 1.0 / p : 1.0;
+        __syncwarp();
+        if (lane < BS && lane != k) G[k * GP + lane] *= piv;            // row k
+        __syncwarp();
+#pragma unroll
+        for (int e = 0; e < BS * BS / 32; ++e) {                         // other rows
+            const int q = lane + 32 * e, i = q / BS, j = q % BS;
+            if (i != k && j != k) G[i * GP + j] -= G[i * GP + k] * G[k * GP + j];
+        }
+        __syncwarp();
+        if (lane < BS && lane != k) G[lane * GP + k] *= -piv;           // column k
+        if (lane == 0) G[k * GP + k] = piv;
+        __syncwarp();
+    }
+    return ok;
+}
+
+// C = A B, A (BS x BS, row stride GP), B (BS x NCOL), C (BS x NCOL) row-major;
+// one warp, each lane accumulates its entries in registers over t
+template <int NCOL>
+__device__ void warp_mm(const double *A, const double *B, double *C)
+{
+    constexpr int PER = (BS * NCOL + 31) / 32;
+    const int lane = threadIdx.x & 31;
+    double acc[PER];
+#pragma unroll
+    for (int e = 0; e < PER; ++e) acc[e] = 0.0;
+#pragma unroll
+    for (int t = 0; t < BS; ++t) {
+#pragma unroll
+        for (int e = 0; e < PER; ++e) {
+            const int q = lane + 32 * e;
+            if (q < BS * NCOL) acc[e] += A[(q / NCOL) * GP + t] * B[t * NCOL + q % NCOL];
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < PER; ++e) {
+        const int q = lane + 32 * e;
+        if (q < BS * NCOL) C[q] = acc[e];
+    }
+    __syncwarp();
+}
+
 // dense fallback: Cholesky of the full B (global memory) and two solves, whole CTA
-__device__ void dense_solve(const IBArgs &a, const Marker *mk, double *yv, int *bad)
+__device__ void dense_solve(const IBArgs &a, double *yv, int *bad)
 {
     const int n = a.nseg, tid = threadIdx.x, nt = blockDim.x;
     const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
     double *L = a.B;
     for (long long q = tid; q < (long long)n * n; q += nt) {
         const int k = (int)(q / n), l = (int)(q % n);
-        L[q] = bval(mk[k], mk[l]);
+        L[q] = bval(a.mk[a.perm[k]], a.mk[a.perm[l]]);
     }
-    for (int q = tid; q < 2 * n; q += nt) yv[q] = a.rhs[q];
+    for (int q = tid; q < n; q += nt) {
+        yv[q] = a.rhs[a.perm[q]];
+        yv[n + q] = a.rhs[n + a.perm[q]];
+    }
     __syncthreads();
     for (int k = 0; k < n; ++k) {
         if (tid == 0) {
@@ -307,111 +463,33 @@ __device__ void dense_solve(const IBArgs &a, const Marker *mk, double *yv, int *
     }
 }
 
-// block reduction of the residual sums; writes the relative residual and the
-// half-bandwidth, and flags a failed factorisation or a residual above 1e-6
-__device__ void finish_residual(const IBArgs &a, double num, double den, int wmax, int bad)
-{
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
-    __shared__ double wr[32][2];
-    for (int off = 16; off; off >>= 1) {
-        num += __shfl_xor_sync(0xffffffffu, num, off);
-        den += __shfl_xor_sync(0xffffffffu, den, off);
-    }
-    if (lane == 0) { wr[warp][0] = num; wr[warp][1] = den; }
-    __syncthreads();
-    if (tid == 0) {
-        double sn = 0.0, sd = 0.0;
-        for (int w = 0; w < (nt >> 5); ++w) { sn += wr[w][0]; sd += wr[w][1]; }
-        const double res = sqrt(sn) / (sqrt(sd) + 1e-300);
-        a.solve_res[0] = res;
-        a.solve_res[1] = (double)wmax;
-        if (bad || !(res < 1e-6)) atomicOr(a.status, LBM_ST_SOLVER);
-    }
-}
-
-// relative residual ||B y - rhs|| / ||rhs|| of both right-hand sides over the
-// sorted band (couplings exist only within `reach`), written with the
-// half-bandwidth; a residual above 1e-6 or a failed factorisation flags the
-// step as a solver failure
-__device__ void solve_residual(const IBArgs &a, const double *key, const int *idx, double reach, int wmax, int bad)
-{
-    const int n = a.nseg, tid = threadIdx.x, nt = blockDim.x;
-    double num = 0.0, den = 0.0;
-    for (int s = tid; s < n; s += nt) {
-        const int k = idx[s];
-        double b0 = 0.0, b1 = 0.0;
-        int t = s;
-        while (t > 0 && key[s] - key[t - 1] <= reach) --t;
-        for (; t < n && key[t] - key[s] <= reach; ++t) {
-            const int l = idx[t];
-            const double b = bval(a.mk[k], a.mk[l]);
-            b0 += b * a.y[l];
-            b1 += b * a.y[n + l];
-        }
-        const double r0 = b0 - a.rhs[k], r1 = b1 - a.rhs[n + k];
-        num += r0 * r0 + r1 * r1;
-        den += a.rhs[k] * a.rhs[k] + a.rhs[n + k] * a.rhs[n + k];
-    }
-    finish_residual(a, num, den, wmax, bad);
-}
-
-// The linear solve of one step, one CTA of SOLVE_THREADS threads.
-// Dynamic shared memory: key[ns] (double), box[ns] (int4, marker support box
-// i1,i2,j1,j2), idx[ns] (int, then ns ints of padding), then one
-// block-operation workspace of WS doubles for each of the first BOPS_WARPS
-// warps; ns = n rounded up to a power of two.
+// The linear solve of one step, one CTA of SOLVE_THREADS threads; dynamic
+// shared memory: one block-operation workspace of WS doubles per warp of the
+// first BOPS_WARPS warps.
 __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int step_index, int ring_slot)
 {
-    extern __shared__ double smem[];
+    extern __shared__ double Wbase[];
     const int n = a.nseg, tid = threadIdx.x, nt = blockDim.x;
     const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
-    int ns = 1;
-    while (ns < n) ns <<= 1;
-    double *key = smem;
-    int4 *box = (int4 *)(key + ns);
-    int *idx = (int *)(box + ns);
-    double *Wbase = (double *)(idx + 2 * ns);
     __shared__ int bb[4];
-    __shared__ double ext[4];
-    __shared__ double wext[32][4];
-    __shared__ int wmax, bad;
-    const Marker *mk = a.mk;
-    if (tid == 0) {
-        bb[0] = 1 << 30; bb[1] = 1 << 30; bb[2] = -1; bb[3] = -1;
-        ext[0] = 1e300; ext[1] = -1e300; ext[2] = 1e300; ext[3] = -1e300;
-        wmax = 0; bad = 0;
-    }
+    __shared__ int bad, wmax;
+    if (tid == 0) { bb[0] = 1 << 30; bb[1] = 1 << 30; bb[2] = -1; bb[3] = -1; bad = 0; wmax = *a.wmax; }
     __syncthreads();
-    // support boxes to shared memory; patch rectangle and marker-cloud extent
-    double lx0 = 1e300, lx1 = -1e300, ly0 = 1e300, ly1 = -1e300;
+    // patch rectangle: bounding box of all support boxes
     int b0 = 1 << 30, b1 = 1 << 30, b2 = -1, b3 = -1;
     for (int k = tid; k < n; k += nt) {
-        const double xm = mk[k].xm, ym = mk[k].ym;
-        const int4 q = make_int4(mk[k].i1, mk[k].i2, mk[k].j1, mk[k].j2);
-        box[k] = q;
-        lx0 = fmin(lx0, xm); lx1 = fmax(lx1, xm); ly0 = fmin(ly0, ym); ly1 = fmax(ly1, ym);
+        const int4 q = mbox(a.mk[k]);
         if (q.y >= q.x && q.w >= q.z) { b0 = min(b0, q.x); b1 = min(b1, q.z); b2 = max(b2, q.y); b3 = max(b3, q.w); }
     }
     for (int off = 16; off; off >>= 1) {
-        lx0 = fmin(lx0, __shfl_xor_sync(0xffffffffu, lx0, off));
-        lx1 = fmax(lx1, __shfl_xor_sync(0xffffffffu, lx1, off));
-        ly0 = fmin(ly0, __shfl_xor_sync(0xffffffffu, ly0, off));
-        ly1 = fmax(ly1, __shfl_xor_sync(0xffffffffu, ly1, off));
         b0 = min(b0, __shfl_xor_sync(0xffffffffu, b0, off));
         b1 = min(b1, __shfl_xor_sync(0xffffffffu, b1, off));
         b2 = max(b2, __shfl_xor_sync(0xffffffffu, b2, off));
         b3 = max(b3, __shfl_xor_sync(0xffffffffu, b3, off));
     }
-    if (lane == 0) {
-        atomicMin(&bb[0], b0); atomicMin(&bb[1], b1); atomicMax(&bb[2], b2); atomicMax(&bb[3], b3);
-        wext[warp][0] = lx0; wext[warp][1] = lx1; wext[warp][2] = ly0; wext[warp][3] = ly1;
-    }
+    if (lane == 0) { atomicMin(&bb[0], b0); atomicMin(&bb[1], b1); atomicMax(&bb[2], b2); atomicMax(&bb[3], b3); }
     __syncthreads();
     if (tid == 0) {
-        for (int w = 0; w < nw; ++w) {
-            ext[0] = fmin(ext[0], wext[w][0]); ext[1] = fmax(ext[1], wext[w][1]);
-            ext[2] = fmin(ext[2], wext[w][2]); ext[3] = fmax(ext[3], wext[w][3]);
-        }
         double time;
         const double *row = motion_row(a, step_index, &time);
         write_header(a, row, time, ring_slot);
@@ -424,115 +502,27 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
             }
         }
         *a.pinfo = pi;
+        a.solve_res[1] = (double)wmax;
+        *a.wmax = 0;   // for the next step's assembly
     }
-    __syncthreads();
     if (n == 0) return;
-    // sort markers along the longer axis (stable: ties by index)
-    const bool by_x = (ext[1] - ext[0]) >= (ext[3] - ext[2]);
-    for (int s = tid; s < ns; s += nt) {
-        key[s] = s < n ? (by_x ? mk[s].xm : mk[s].ym) : 1e300;
-        idx[s] = s;
-    }
-    __syncthreads();
-    for (int size = 2; size <= ns; size <<= 1)
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int s = tid; s < ns; s += nt) {
-                const int t = s ^ stride;
-                if (t > s) {
-                    const bool up = (s & size) == 0;
-                    const bool gt = key[s] > key[t] || (key[s] == key[t] && idx[s] > idx[t]);
-                    if (gt == up) {
-                        const double kk = key[s]; key[s] = key[t]; key[t] = kk;
-                        const int ii = idx[s]; idx[s] = idx[t]; idx[t] = ii;
-                    }
-                }
-            }
-            __syncthreads();
-        }
-    // half-bandwidth of D D^T in the sorted order: boxes (<= 6 nodes wide)
-    // can overlap only for markers less than 6 lattice units apart
-    const double reach = 6.0 * a.scale;
-    for (int s = tid; s < n; s += nt) {
-        int wl = 0;
-        const int4 ps = box[idx[s]];
-        for (int t = s + 1; t < n && key[t] - key[s] <= reach; ++t)
-            if (box_overlap(ps, box[idx[t]])) wl = t - s;
-        if (wl) atomicMax(&wmax, wl);
-    }
-    __syncthreads();
-    double *yv = a.bX + 2 * (long long)BS * ((n + BS - 1) / BS);   // 2n scratch after the block rhs
-    if (wmax > BS || a.force_dense) {
-        dense_solve(a, mk, yv, &bad);
-        for (int q = tid; q < 2 * n; q += nt) a.y[q] = yv[q];
-        __syncthreads();
-        solve_residual(a, key, idx, reach, wmax, bad);
-        return;
-    }
-    // block tridiagonal form: D_i (BS x BS), L_i couples block i to block i-1,
-    // X_i holds the two right-hand sides (BS x 2), padded with identity rows;
-    // D0/L0 keep the assembled blocks for the residual. One warp per block,
-    // with the block's and the previous block's markers staged in W.
     const int nb = (n + BS - 1) / BS;
     double *Db = a.bD, *Lb = a.bL, *Fb = a.bF, *Xb = a.bX;
-    double *D0 = a.bD + (long long)nb * BS * BS, *L0 = a.bL + (long long)nb * BS * BS;
+    if (wmax > BS || a.force_dense) {
+        double *yv = Xb + 2 * (long long)BS * nb;   // 2n scratch after the block rhs
+        dense_solve(a, yv, &bad);
+        for (int q = tid; q < n; q += nt) {
+            a.y[a.perm[q]] = yv[q];
+            a.y[n + a.perm[q]] = yv[n + q];
+        }
+        if (tid == 0 && bad) atomicOr(a.status, LBM_ST_SOLVER);
+        return;
+    }
+    // cyclic reduction: at stride st the active blocks are multiples of st;
+    // odd multiples are eliminated into their even neighbours. Each block
+    // operation runs on one warp in its shared-memory workspace W.
     double *W = Wbase + (long long)warp * WS;
     const bool bw = warp < BOPS_WARPS;
-    if (bw)
-        for (int blk = warp; blk < nb; blk += BOPS_WARPS) {
-            // staged markers: 2*BS entries of (phx[6], phy[6]) and boxes
-            double *ph = W;                                  // [2*BS][12]
-            int4 *bxw = (int4 *)(W + 2 * BS * 12);           // [2*BS]
-            for (int q = lane; q < 2 * BS * 12; q += 32) {
-                const int m = q / 12, c = q % 12;
-                const int srt = (blk - 1) * BS + m;          // m < BS: previous block
-                double v = 0.0;
-                if (srt >= 0 && srt < n) {
-                    const Marker &mm = mk[idx[srt]];
-                    v = c < 6 ? mm.phx[c] : mm.phy[c - 6];
-                }
-                ph[q] = v;
-            }
-            for (int m = lane; m < 2 * BS; m += 32) {
-                const int srt = (blk - 1) * BS + m;
-                bxw[m] = (srt >= 0 && srt < n) ? box[idx[srt]] : make_int4(1, 0, 1, 0);
-            }
-            __syncwarp();
-            for (int q = lane; q < 2 * BS * BS; q += 32) {
-                const int r = (q % (BS * BS)) / BS, c = q % BS;
-                const bool lower = q >= BS * BS;             // coupling to the previous block
-                const int mr = BS + r, mc = lower ? c : BS + c;
-                const int sr = blk * BS + r;
-                double v;
-                const int4 p = bxw[mr], o = bxw[mc];
-                if (sr >= n) {
-                    v = (!lower && r == c) ? 1.0 : 0.0;
-                } else if (!lower && blk * BS + c >= n) {
-                    v = 0.0;
-                } else if (lower && blk == 0) {
-                    v = 0.0;
-                } else {
-                    const int ia = max(p.x, o.x), ib = min(p.y, o.y), ja = max(p.z, o.z), jb = min(p.w, o.w);
-                    v = 0.0;
-                    if (ia <= ib && ja <= jb) {
-                        double sx = 0.0, sy = 0.0;
-                        for (int i = ia; i <= ib; ++i) sx += ph[mr * 12 + i - p.x] * ph[mc * 12 + i - o.x];
-                        for (int j = ja; j <= jb; ++j) sy += ph[mr * 12 + 6 + j - p.z] * ph[mc * 12 + 6 + j - o.z];
-                        v = sx * sy;
-                    }
-                }
-                const long long g = (long long)blk * BS * BS + r * BS + c;
-                if (lower) { Lb[g] = v; L0[g] = v; }
-                else { Db[g] = v; D0[g] = v; }
-            }
-            __syncwarp();
-        }
-    for (int q = tid; q < nb * BS; q += nt) {
-        Xb[2 * q] = q < n ? a.rhs[idx[q]] : 0.0;
-        Xb[2 * q + 1] = q < n ? a.rhs[n + idx[q]] : 0.0;
-    }
-    __syncthreads();
-    // cyclic reduction: at stride st the active blocks are multiples of st;
-    // odd multiples are eliminated into their even neighbours
     int levels = 0;
     for (int st = 1; st < nb; st <<= 1, ++levels) {
         const int nodd = (nb - st + 2 * st - 1) / (2 * st);
@@ -540,8 +530,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
             for (int m = warp; m < nodd; m += BOPS_WARPS) {
                 // F_o = D_o^-1 [L_o | L_q^T | r_o]
                 const int o = st * (2 * m + 1), q2 = o + st;
-                double *Gs = W, *Rs = W + BS * BS;
-                for (int e = lane; e < BS * BS; e += 32) Gs[e] = Db[(long long)o * BS * BS + e];
+                double *Gs = W, *Rs = W + BS * GP;
+                for (int e = lane; e < BS * BS; e += 32) Gs[(e / BS) * GP + e % BS] = Db[(long long)o * BS * BS + e];
                 for (int e = lane; e < BS * FC; e += 32) {
                     const int r = e / FC, c = e % FC;
                     double v;
@@ -552,39 +542,45 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
                 }
                 __syncwarp();
                 if (!warp_inv(Gs) && lane == 0) bad = 1;
-                warp_mm(Gs, Rs, Fb + (long long)o * BS * FC, FC);
+                warp_mm<FC>(Gs, Rs, Fb + (long long)o * BS * FC);
             }
         __syncthreads();
         const int neven = (nb + 2 * st - 1) / (2 * st);
         if (bw)
             for (int m = warp; m < neven; m += BOPS_WARPS) {
                 const int e = 2 * st * m, o1 = e - st, o2 = e + st;
-                double *As = W, *Fs = W + BS * BS, *Ds = Fs + BS * FC, *Xs = Ds + BS * BS;
+                double *As = W, *Fs = W + BS * GP, *Ds = Fs + BS * FC, *Xs = Ds + BS * GP;
                 double *De = Db + (long long)e * BS * BS, *Le = Lb + (long long)e * BS * BS;
                 double *Xe = Xb + 2 * (long long)e * BS;
-                for (int q = lane; q < BS * BS; q += 32) Ds[q] = De[q];
+                for (int q = lane; q < BS * BS; q += 32) Ds[(q / BS) * GP + q % BS] = De[q];
                 for (int q = lane; q < 2 * BS; q += 32) Xs[q] = Xe[q];
                 // right neighbour o2 (e is its previous block):
                 // D_e -= L_o2^T FL_o2, r_e -= L_o2^T Fr_o2
                 if (o2 < nb) {
                     const double *Lo = Lb + (long long)o2 * BS * BS;
                     const double *F = Fb + (long long)o2 * BS * FC;
-                    for (int q = lane; q < BS * BS; q += 32) As[q] = Lo[q];
+                    for (int q = lane; q < BS * BS; q += 32) As[(q / BS) * GP + q % BS] = Lo[q];
                     for (int q = lane; q < BS * FC; q += 32) Fs[q] = F[q];
                     __syncwarp();
-                    for (int q = lane; q < BS * BS + 2 * BS; q += 32) {
-                        double sum = 0.0;
-                        if (q < BS * BS) {
-                            const int r = q / BS, c = q % BS;
+                    constexpr int PER = (BS * BS + 2 * BS + 31) / 32;
+                    double acc[PER];
 #pragma unroll
-                            for (int t = 0; t < BS; ++t) sum += As[t * BS + r] * Fs[t * FC + c];
-                            Ds[q] -= sum;
-                        } else {
-                            const int r = (q - BS * BS) / 2, c = (q - BS * BS) % 2;
+                    for (int k = 0; k < PER; ++k) acc[k] = 0.0;
 #pragma unroll
-                            for (int t = 0; t < BS; ++t) sum += As[t * BS + r] * Fs[t * FC + 2 * BS + c];
-                            Xs[2 * r + c] -= sum;
+                    for (int t = 0; t < BS; ++t) {
+#pragma unroll
+                        for (int k = 0; k < PER; ++k) {
+                            const int q = lane + 32 * k;
+                            if (q < BS * BS) acc[k] += As[t * GP + q / BS] * Fs[t * FC + q % BS];
+                            else if (q < BS * BS + 2 * BS)
+                                acc[k] += As[t * GP + (q - BS * BS) / 2] * Fs[t * FC + 2 * BS + (q - BS * BS) % 2];
                         }
+                    }
+#pragma unroll
+                    for (int k = 0; k < PER; ++k) {
+                        const int q = lane + 32 * k;
+                        if (q < BS * BS) Ds[(q / BS) * GP + q % BS] -= acc[k];
+                        else if (q < BS * BS + 2 * BS) Xs[q - BS * BS] -= acc[k];
                     }
                     __syncwarp();
                 }
@@ -592,32 +588,36 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
                 // r_e -= L_e Fr_o1, new L_e = -L_e FL_o1
                 if (m > 0) {
                     const double *F = Fb + (long long)o1 * BS * FC;
-                    for (int q = lane; q < BS * BS; q += 32) As[q] = Le[q];
+                    for (int q = lane; q < BS * BS; q += 32) As[(q / BS) * GP + q % BS] = Le[q];
                     for (int q = lane; q < BS * FC; q += 32) Fs[q] = F[q];
                     __syncwarp();
-                    for (int q = lane; q < BS * BS + 2 * BS; q += 32) {
-                        if (q < BS * BS) {
-                            const int r = q / BS, c = q % BS;
-                            double s1 = 0.0, s2 = 0.0;
+                    // entries: [0, BS*BS) D update, [BS*BS, 2*BS*BS) new L, then 2*BS rhs
+                    constexpr int NE = 2 * BS * BS + 2 * BS, PER = (NE + 31) / 32;
+                    double acc[PER];
 #pragma unroll
-                            for (int t = 0; t < BS; ++t) {
-                                const double l = As[r * BS + t];
-                                s1 += l * Fs[t * FC + BS + c];
-                                s2 += l * Fs[t * FC + c];
-                            }
-                            Ds[q] -= s1;
-                            Le[q] = -s2;
-                        } else {
-                            const int r = (q - BS * BS) / 2, c = (q - BS * BS) % 2;
-                            double sum = 0.0;
+                    for (int k = 0; k < PER; ++k) acc[k] = 0.0;
 #pragma unroll
-                            for (int t = 0; t < BS; ++t) sum += As[r * BS + t] * Fs[t * FC + 2 * BS + c];
-                            Xs[2 * r + c] -= sum;
+                    for (int t = 0; t < BS; ++t) {
+#pragma unroll
+                        for (int k = 0; k < PER; ++k) {
+                            const int q = lane + 32 * k;
+                            if (q < BS * BS) acc[k] += As[(q / BS) * GP + t] * Fs[t * FC + BS + q % BS];
+                            else if (q < 2 * BS * BS)
+                                acc[k] += As[((q - BS * BS) / BS) * GP + t] * Fs[t * FC + (q - BS * BS) % BS];
+                            else if (q < NE)
+                                acc[k] += As[((q - 2 * BS * BS) / 2) * GP + t] * Fs[t * FC + 2 * BS + (q - 2 * BS * BS) % 2];
                         }
+                    }
+#pragma unroll
+                    for (int k = 0; k < PER; ++k) {
+                        const int q = lane + 32 * k;
+                        if (q < BS * BS) Ds[(q / BS) * GP + q % BS] -= acc[k];
+                        else if (q < 2 * BS * BS) Le[q - BS * BS] = -acc[k];
+                        else if (q < NE) Xs[q - 2 * BS * BS] -= acc[k];
                     }
                     __syncwarp();
                 }
-                for (int q = lane; q < BS * BS; q += 32) De[q] = Ds[q];
+                for (int q = lane; q < BS * BS; q += 32) De[q] = Ds[(q / BS) * GP + q % BS];
                 for (int q = lane; q < 2 * BS; q += 32) Xe[q] = Xs[q];
                 __syncwarp();
             }
@@ -625,13 +625,12 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
     }
     // the last active block (block 0)
     if (warp == 0) {
-        double *Gs = W, *Rs = W + BS * BS, *Fs = Rs + 2 * BS;
-        for (int e = lane; e < BS * BS; e += 32) Gs[e] = Db[e];
+        double *Gs = W, *Rs = W + BS * GP;
+        for (int e = lane; e < BS * BS; e += 32) Gs[(e / BS) * GP + e % BS] = Db[e];
         for (int e = lane; e < 2 * BS; e += 32) Rs[e] = Xb[e];
         __syncwarp();
         if (!warp_inv(Gs) && lane == 0) bad = 1;
-        warp_mm(Gs, Rs, Fs, 2);
-        for (int e = lane; e < 2 * BS; e += 32) Xb[e] = Fs[e];
+        warp_mm<2>(Gs, Rs, Xb);
     }
     __syncthreads();
     // back substitution: x_o = Fr_o - FL_o x_p - FU_o x_q, coarsest level first
@@ -641,51 +640,23 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
         for (int m = warp; m < nodd; m += nw) {
             const int o = st * (2 * m + 1), p = o - st, q2 = o + st;
             const double *F = Fb + (long long)o * BS * FC;
-            for (int q = lane; q < 2 * BS; q += 32) {
-                const int r = q / 2, c = q % 2;
-                double s1 = F[r * FC + 2 * BS + c], s2 = 0.0;
+            const int r = lane / 2, c = lane % 2;
+            double s1 = F[r * FC + 2 * BS + c], s2 = 0.0, s3 = 0.0;
 #pragma unroll
-                for (int t = 0; t < BS; ++t) s1 -= F[r * FC + t] * Xb[2 * ((long long)p * BS + t) + c];
-                if (q2 < nb) {
+            for (int t = 0; t < BS; ++t) s2 += F[r * FC + t] * Xb[2 * ((long long)p * BS + t) + c];
+            if (q2 < nb) {
 #pragma unroll
-                    for (int t = 0; t < BS; ++t) s2 += F[r * FC + BS + t] * Xb[2 * ((long long)q2 * BS + t) + c];
-                }
-                Xb[2 * ((long long)o * BS + r) + c] = s1 - s2;
+                for (int t = 0; t < BS; ++t) s3 += F[r * FC + BS + t] * Xb[2 * ((long long)q2 * BS + t) + c];
             }
+            Xb[2 * ((long long)o * BS + r) + c] = s1 - s2 - s3;
         }
         __syncthreads();
     }
-    for (int s = tid; s < n; s += nt) {
-        a.y[idx[s]] = Xb[2 * s];
-        a.y[n + idx[s]] = Xb[2 * s + 1];
+    for (int s2 = tid; s2 < n; s2 += nt) {
+        a.y[a.perm[s2]] = Xb[2 * s2];
+        a.y[n + a.perm[s2]] = Xb[2 * s2 + 1];
     }
-    // residual ||B y - rhs|| / ||rhs|| with the assembled blocks
-    double num = 0.0, den = 0.0;
-    for (int s = tid; s < n; s += nt) {
-        const int i = s / BS, r = s % BS;
-        double a0 = 0.0, a1 = 0.0, c0 = 0.0, c1 = 0.0, e0 = 0.0, e1 = 0.0;
-        const double *dr = D0 + ((long long)i * BS + r) * BS;
-        const double *xi = Xb + 2 * (long long)i * BS;
-#pragma unroll
-        for (int t = 0; t < BS; ++t) { a0 += dr[t] * xi[2 * t]; a1 += dr[t] * xi[2 * t + 1]; }
-        if (i > 0) {
-            const double *lr = L0 + ((long long)i * BS + r) * BS;
-            const double *xp = Xb + 2 * (long long)(i - 1) * BS;
-#pragma unroll
-            for (int t = 0; t < BS; ++t) { c0 += lr[t] * xp[2 * t]; c1 += lr[t] * xp[2 * t + 1]; }
-        }
-        if (i + 1 < nb) {
-            const double *ln = L0 + (long long)(i + 1) * BS * BS + r;
-            const double *xq = Xb + 2 * (long long)(i + 1) * BS;
-#pragma unroll
-            for (int t = 0; t < BS; ++t) { e0 += ln[t * BS] * xq[2 * t]; e1 += ln[t * BS] * xq[2 * t + 1]; }
-        }
-        const double b0 = a.rhs[idx[s]], b1 = a.rhs[n + idx[s]];
-        const double r0 = a0 + c0 + e0 - b0, r1 = a1 + c1 + e1 - b1;
-        num += r0 * r0 + r1 * r1;
-        den += b0 * b0 + b1 * b1;
-    }
-    finish_residual(a, num, den, wmax, bad);
+    if (tid == 0 && bad) atomicOr(a.status, LBM_ST_SOLVER);
 }
 
 // du = D^T y over the current patch, 16x16 nodes per CTA, plus FP64 force and
@@ -696,7 +667,7 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
     __shared__ int list[256];
     __shared__ int wsum[8];
     __shared__ int nlist;
-    __shared__ double red[8][3 * LBM_MAXW];
+    __shared__ double red[8][NPART];
     __shared__ bool amlast;
     const PatchInfo pi = *a.pinfo;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -764,7 +735,36 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
         const double y0 = (a.oy + a.scale * (double)gj - (a.yc + sb)) / a.scale;
         mz = -x0 * temp2 + y0 * temp1;
     }
+    // residual rows of the marker system, (B y - rhs)_s over the band
+    double rnum = 0.0, rden = 0.0;
+    {
+        const int nblk0 = gridDim.x * gridDim.y, bid0 = blockIdx.y * gridDim.x + blockIdx.x;
+        const int n = a.nseg;
+        const double reach = n > 0 ? *a.reach : 0.0;
+        for (int s = bid0 * blockDim.x + threadIdx.x; s < n; s += nblk0 * blockDim.x) {
+            const Marker &ms = a.mk[a.perm[s]];
+            const double ks = a.key[s];
+            int t = s;
+            while (t > 0 && ks - a.key[t - 1] <= reach) --t;
+            double b0 = 0.0, b1 = 0.0;
+            for (; t < n && a.key[t] - ks <= reach; ++t) {
+                const int l = a.perm[t];
+                const double b = bval(ms, a.mk[l]);
+                b0 += b * a.y[l];
+                b1 += b * a.y[n + l];
+            }
+            const double q0 = a.rhs[a.perm[s]], q1 = a.rhs[n + a.perm[s]];
+            rnum += (b0 - q0) * (b0 - q0) + (b1 - q1) * (b1 - q1);
+            rden += q0 * q0 + q1 * q1;
+        }
+#pragma unroll
+        for (int off = 16; off; off >>= 1) {
+            rnum += __shfl_down_sync(0xffffffffu, rnum, off);
+            rden += __shfl_down_sync(0xffffffffu, rden, off);
+        }
+    }
     // deterministic block reduction per wing
+    if (lane == 0) { red[warp][3 * LBM_MAXW] = rnum; red[warp][3 * LBM_MAXW + 1] = rden; }
     for (int w = 0; w < a.nwing; ++w) {
         double v0 = (in_support && wing == w) ? fx : 0.0;
         double v1 = (in_support && wing == w) ? fy : 0.0;
@@ -779,10 +779,10 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
     }
     __syncthreads();
     const int nblk = gridDim.x * gridDim.y, bid = blockIdx.y * gridDim.x + blockIdx.x;
-    if (threadIdx.x < 3 * a.nwing) {
+    if (threadIdx.x < 3 * a.nwing || threadIdx.x == 3 * LBM_MAXW || threadIdx.x == 3 * LBM_MAXW + 1) {
         double s = 0.0;
         for (int w8 = 0; w8 < 8; ++w8) s += red[w8][threadIdx.x];
-        a.partial[(long long)bid * 3 * LBM_MAXW + threadIdx.x] = s;
+        a.partial[(long long)bid * NPART + threadIdx.x] = s;
     }
     __threadfence();
     __syncthreads();
@@ -792,11 +792,14 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
     __threadfence();
     // last block: every thread sums a fixed strided subset of the block
     // partials, then a fixed warp/block tree (deterministic order)
-    for (int w = 0; w < a.nwing; ++w) {
+    for (int w = 0; w <= a.nwing; ++w) {
+        // w < nwing: force and moment of wing w; w == nwing: residual sums
+        const int off0 = w < a.nwing ? 3 * w : 3 * LBM_MAXW;
         double s0 = 0, s1 = 0, s2 = 0;
         for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
-            const double *p = a.partial + (long long)b * 3 * LBM_MAXW + 3 * w;
-            s0 += __ldcg(p); s1 += __ldcg(p + 1); s2 += __ldcg(p + 2);
+            const double *p = a.partial + (long long)b * NPART + off0;
+            s0 += __ldcg(p); s1 += __ldcg(p + 1);
+            if (w < a.nwing) s2 += __ldcg(p + 2);
         }
 #pragma unroll
         for (int off = 16; off; off >>= 1) {
@@ -825,16 +828,24 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
         fr[1 + 3 * a.nwing] = tot[0];
         fr[2 + 3 * a.nwing] = tot[1];
         fr[3 + 3 * a.nwing] = tot[2];
+        // solve residual ||B y - rhs|| / ||rhs|| (FP64 solve: ~1e-14)
+        double sn = 0, sd = 0;
+        for (int w8 = 0; w8 < 8; ++w8) { sn += red[w8][3 * a.nwing]; sd += red[w8][3 * a.nwing + 1]; }
+        const double res = sqrt(sn) / (sqrt(sd) + 1e-300);
+        a.solve_res[0] = res;
+        if (a.nseg > 0 && !(res < 1e-6)) atomicOr(a.status, LBM_ST_SOLVER);
         *a.counter = 0u;
     }
 }
 
-size_t solve_smem(int n)
+size_t order_smem(int n)
 {
     int ns = 1;
     while (ns < n) ns <<= 1;
-    return sizeof(double) * ns + sizeof(int4) * ns + sizeof(int) * 2 * ns + sizeof(double) * BOPS_WARPS * WS;
+    return (sizeof(double) + sizeof(int)) * ns;
 }
+
+constexpr size_t kSolveSmem = sizeof(double) * BOPS_WARPS * WS;
 
 IBArgs make_args(lbm_handle *h, const void *fin)
 {
@@ -851,6 +862,7 @@ IBArgs make_args(lbm_handle *h, const void *fin)
     a.mstep = h->d_mstep; a.msteps = h->msteps; a.mcols = h->mcols; a.mdt = h->mdt;
     a.mk = h->d_mk; a.rhs = h->d_rhs; a.B = h->d_B; a.y = h->d_y;
     a.bD = h->d_bD; a.bL = h->d_bL; a.bF = h->d_bF; a.bX = h->d_bX;
+    a.perm = h->d_perm; a.key = h->d_key; a.reach = h->d_reach; a.wmax = h->d_wmax;
     a.pinfo = h->d_pinfo; a.patch = h->d_patch; a.patch_cap = h->patch_cap;
     a.patch_wmax = h->patch_wmax; a.patch_hmax = h->patch_hmax;
     a.partial = h->d_partial; a.counter = h->d_counter;
@@ -863,14 +875,21 @@ template <typename T, typename C>
 int launch_ib_t(lbm_handle *h, const void *fin, int step_index, int ring_slot, cudaStream_t st)
 {
     IBArgs a = make_args(h, fin);
-    if (h->nseg > 0) ib_markers<T><<<(h->nseg + 7) / 8, 256, 0, st>>>(a, step_index);
-    ib_solve<<<1, SOLVE_THREADS, solve_smem(h->nseg), st>>>(a, step_index, ring_slot);
+    if (h->nseg > 0) {
+        ib_markers<T><<<(h->nseg + 7) / 8, 256, 0, st>>>(a, step_index);
+        if (!h->static_order) ib_order<<<1, 1024, order_smem(h->nseg), st>>>(a);
+        ib_assemble<<<(h->nseg + BS - 1) / BS, 256, 0, st>>>(a);
+    }
+    ib_solve<<<1, SOLVE_THREADS, kSolveSmem, st>>>(a, step_index, ring_slot);
     dim3 grid(h->patch_gx(), h->patch_gy());
     ib_spread<T, C><<<grid, 256, 0, st>>>(a, step_index, ring_slot);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 }  // namespace
+
+// per-CTA partials of ib_spread (doubles)
+int ib_partials_per_block() { return NPART; }
 
 // scratch sizes of the block cyclic reduction (doubles)
 size_t ib_block_scratch(int nseg, size_t *d, size_t *l, size_t *f, size_t *x)
@@ -883,11 +902,13 @@ size_t ib_block_scratch(int nseg, size_t *d, size_t *l, size_t *f, size_t *x)
     return *d + *l + *f + *x;
 }
 
-int ib_max_markers() { return NSORT_MAX; }
+int ib_max_markers() { return NMARK_MAX; }
 
 int ib_configure(lbm_handle *h)
 {
-    if (cudaFuncSetAttribute(ib_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)solve_smem(NSORT_MAX)) !=
+    if (cudaFuncSetAttribute(ib_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSolveSmem) != cudaSuccess)
+        return -1;
+    if (cudaFuncSetAttribute(ib_order, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)order_smem(NMARK_MAX)) !=
         cudaSuccess)
         return -1;
     return 0;

@@ -122,6 +122,7 @@ void free_ib(lbm_handle *h)
     free_dev(h->d_patch);
     free_devp(h->d_mk); free_devp(h->d_rhs); free_devp(h->d_B); free_devp(h->d_y); free_devp(h->d_partial);
     free_devp(h->d_bD); free_devp(h->d_bL); free_devp(h->d_bF); free_devp(h->d_bX);
+    free_devp(h->d_perm); free_devp(h->d_key); free_devp(h->d_reach); free_devp(h->d_wmax);
 }
 
 // Allocates the immersed-boundary scratch once geometry and motion are known:
@@ -184,7 +185,32 @@ int ensure_ib(lbm_handle *h)
     CK(cudaMalloc(&h->d_bF, sizeof(double) * sf), "alloc block F");
     CK(cudaMalloc(&h->d_bX, sizeof(double) * sx), "alloc block X");
     const int nblk = h->patch_gx() * h->patch_gy();
-    CK(cudaMalloc(&h->d_partial, sizeof(double) * 3 * LBM_MAXW * (size_t)nblk), "alloc partials");
+    CK(cudaMalloc(&h->d_partial, sizeof(double) * ib_partials_per_block() * (size_t)nblk), "alloc partials");
+    // solve order of the markers: one rigid body keeps its markers sorted by
+    // body-frame chordwise position for the whole run (two markers whose
+    // support boxes overlap are less than 5*sqrt(2) lattice units apart in any
+    // orientation); several bodies are sorted on the device every step
+    CK(cudaMalloc(&h->d_perm, sizeof(int) * ns), "alloc perm");
+    CK(cudaMalloc(&h->d_key, sizeof(double) * ns), "alloc key");
+    CK(cudaMalloc(&h->d_reach, sizeof(double)), "alloc reach");
+    CK(cudaMalloc(&h->d_wmax, sizeof(int)), "alloc wmax");
+    CK(cudaMemsetAsync(h->d_wmax, 0, sizeof(int), h->stream), "clear wmax");
+    h->static_order = h->nwing == 1;
+    if (h->static_order) {
+        std::vector<int> perm(h->nseg);
+        std::vector<double> xk(h->nseg), key(h->nseg);
+        for (int k = 0; k < h->nseg; ++k) {
+            perm[k] = k;
+            xk[k] = 0.5 * (h->hx0[k] + h->hx0[k + 1]);
+        }
+        std::stable_sort(perm.begin(), perm.end(), [&](int p1, int p2) { return xk[p1] < xk[p2]; });
+        for (int q = 0; q < h->nseg; ++q) key[q] = xk[perm[q]];
+        const double reach = 7.1 * h->p.scale;
+        CK(cudaMemcpyAsync(h->d_perm, perm.data(), sizeof(int) * h->nseg, cudaMemcpyHostToDevice, h->stream), "copy perm");
+        CK(cudaMemcpyAsync(h->d_key, key.data(), sizeof(double) * h->nseg, cudaMemcpyHostToDevice, h->stream), "copy key");
+        CK(cudaMemcpyAsync(h->d_reach, &reach, sizeof(double), cudaMemcpyHostToDevice, h->stream), "copy reach");
+        CK(cudaStreamSynchronize(h->stream), "sync order");
+    }
     if (ib_configure(h) != 0) return set_err(h, LBM_ERR_CUDA, "ib_configure failed");
     h->ib_ready = 1;
     return LBM_OK;

@@ -62,6 +62,10 @@ struct IBArgs {
     double *y;          // [2*nseg]
     double *bD, *bL, *bF, *bX;  // block cyclic reduction scratch (diagonal, lower,
                                 // eliminated-block factors, right-hand sides)
+    int *perm;                  // solve order: sorted position -> marker
+    double *key;                // sort key of each sorted position
+    double *reach;              // key distance beyond which boxes cannot overlap
+    int *wmax;                  // half-bandwidth found by the assembly
     PatchInfo *pinfo;
     void *patch;        // compute-precision (du, dv) pairs
     int patch_cap;      // nodes
@@ -107,6 +111,9 @@ struct lbm_handle {
     Marker *d_mk = nullptr;
     double *d_rhs = nullptr, *d_B = nullptr, *d_y = nullptr;
     double *d_bD = nullptr, *d_bL = nullptr, *d_bF = nullptr, *d_bX = nullptr;
+    int *d_perm = nullptr, *d_wmax = nullptr;
+    double *d_key = nullptr, *d_reach = nullptr;
+    int static_order = 0;   // one rigid body: fixed body-frame marker order
     PatchInfo *d_pinfo = nullptr;
     void *d_patch = nullptr;
     int patch_cap = 0;               // nodes
@@ -152,6 +159,7 @@ struct lbm_handle {
 // kernel launchers (kf_kernel.cu, ib_kernels.cu)
 int ib_configure(lbm_handle *h);
 int ib_max_markers();
+int ib_partials_per_block();
 size_t ib_block_scratch(int nseg, size_t *d, size_t *l, size_t *f, size_t *x);
 int launch_kf(lbm_handle *h, const void *fin, void *fout, void *fields, int mode = KF_ALL, cudaStream_t st = nullptr);
 int launch_ib(lbm_handle *h, const void *fin, int step_index, int ring_slot, cudaStream_t st = nullptr);
