@@ -364,23 +364,33 @@ __global__ void __launch_bounds__(256) ib_assemble(const IBArgs a)
 __device__ bool warp_inv(double *G)
 {
     const int lane = threadIdx.x & 31;
+    const int j = lane % BS, ih = lane / BS;    // this lane's column, and row parity
     bool ok = true;
     for (int k = 0; k < BS; ++k) {
         const double p = G[k * GP + k];
         const bool good = p > 0.0 && isfinite(p);
         ok = ok && good;
         const double piv = good ? 1.0 / p : 1.0;
-        __syncwarp();
-        if (lane < BS && lane != k) G[k * GP + lane] *= piv;            // row k
-        __syncwarp();
+        // all reads of the step first (no store of the step can alias them),
+        // then the stores
+        const double rowk = G[k * GP + j] * piv;                         // scaled row k
+        double cik[BS / 2], gij[BS / 2];
 #pragma unroll
-        for (int e = 0; e < BS * BS / 32; ++e) {                         // other rows
-            const int q = lane + 32 * e, i = q / BS, j = q % BS;
-            if (i != k && j != k) G[i * GP + j] -= G[i * GP + k] * G[k * GP + j];
+        for (int e = 0; e < BS / 2; ++e) {
+            const int i = 2 * e + ih;
+            cik[e] = G[i * GP + k];
+            gij[e] = G[i * GP + j];
         }
         __syncwarp();
-        if (lane < BS && lane != k) G[lane * GP + k] *= -piv;           // column k
-        if (lane == 0) G[k * GP + k] = piv;
+#pragma unroll
+        for (int e = 0; e < BS / 2; ++e) {
+            const int i = 2 * e + ih;
+            double v;
+            if (i == k) v = (j == k) ? piv : rowk;                       // row k
+            else if (j == k) v = -cik[e] * piv;                          // column k
+            else v = gij[e] - cik[e] * rowk;                             // rank-1 update
+            G[i * GP + j] = v;
+        }
         __syncwarp();
     }
     return ok;
@@ -664,11 +674,15 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
 template <typename T, typename C>
 __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index, int ring_slot)
 {
-    __shared__ int list[256];
     __shared__ int wsum[8];
     __shared__ int nlist;
     __shared__ double red[8][NPART];
     __shared__ bool amlast;
+    // markers whose support box meets this tile, staged in marker order
+    __shared__ int4 sbox[256];
+    __shared__ double sph[256][12];
+    __shared__ double sy[256][2];
+    __shared__ int swing[256];
     const PatchInfo pi = *a.pinfo;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const int ti0 = blockIdx.x * 16, tj0 = blockIdx.y * 16;
@@ -684,30 +698,39 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
         for (int c0 = 0; c0 < a.nseg; c0 += 256) {
             const int k = c0 + threadIdx.x;
             bool hit = false;
+            int4 q = make_int4(1, 0, 1, 0);
             if (k < a.nseg) {
-                const Marker &m = a.mk[k];
-                hit = m.i1 <= tb && m.i2 >= ta && m.j1 <= sb_ && m.j2 >= sa_ && m.i2 >= m.i1;
+                q = mbox(a.mk[k]);
+                hit = q.x <= tb && q.y >= ta && q.z <= sb_ && q.w >= sa_ && q.y >= q.x;
             }
             const unsigned bal = __ballot_sync(0xffffffffu, hit);
             if (lane == 0) wsum[warp] = __popc(bal);
             __syncthreads();
             if (threadIdx.x == 0) {
-                int s = 0;
-                for (int w = 0; w < 8; ++w) { const int t = wsum[w]; wsum[w] = s; s += t; }
-                nlist = s;
+                int acc = 0;
+                for (int w = 0; w < 8; ++w) { const int t = wsum[w]; wsum[w] = acc; acc += t; }
+                nlist = acc;
             }
             __syncthreads();
-            if (hit) list[wsum[warp] + __popc(bal & ((1u << lane) - 1u))] = k;
+            if (hit) {
+                const int slot = wsum[warp] + __popc(bal & ((1u << lane) - 1u));
+                const Marker &m = a.mk[k];
+                sbox[slot] = q;
+#pragma unroll
+                for (int c = 0; c < 6; ++c) { sph[slot][c] = m.phx[c]; sph[slot][6 + c] = m.phy[c]; }
+                sy[slot][0] = a.y[k];
+                sy[slot][1] = a.y[a.nseg + k];
+                swing[slot] = m.wing;
+            }
             __syncthreads();
             if (active) {
-                for (int q = 0; q < nlist; ++q) {
-                    const Marker &m = a.mk[list[q]];
-                    if (gi >= m.i1 && gi <= m.i2 && gj >= m.j1 && gj <= m.j2) {
-                        const double wgt = m.phx[gi - m.i1] * m.phy[gj - m.j1];
-                        const int kk = list[q];
-                        du += wgt * a.y[kk];
-                        dv += wgt * a.y[a.nseg + kk];
-                        wing = min(wing, m.wing);
+                for (int t = 0; t < nlist; ++t) {
+                    const int4 b = sbox[t];
+                    if (gi >= b.x && gi <= b.y && gj >= b.z && gj <= b.w) {
+                        const double wgt = sph[t][gi - b.x] * sph[t][6 + gj - b.z];
+                        du += wgt * sy[t][0];
+                        dv += wgt * sy[t][1];
+                        wing = min(wing, swing[t]);
                     }
                 }
             }
@@ -735,32 +758,34 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
         const double y0 = (a.oy + a.scale * (double)gj - (a.yc + sb)) / a.scale;
         mz = -x0 * temp2 + y0 * temp1;
     }
-    // residual rows of the marker system, (B y - rhs)_s over the band
+    // residual rows of the marker system, (B y - rhs)_s: one warp per row,
+    // lanes over the couplings within the half-bandwidth of this step
     double rnum = 0.0, rden = 0.0;
     {
         const int nblk0 = gridDim.x * gridDim.y, bid0 = blockIdx.y * gridDim.x + blockIdx.x;
         const int n = a.nseg;
-        const double reach = n > 0 ? *a.reach : 0.0;
-        for (int s = bid0 * blockDim.x + threadIdx.x; s < n; s += nblk0 * blockDim.x) {
-            const Marker &ms = a.mk[a.perm[s]];
-            const double ks = a.key[s];
-            int t = s;
-            while (t > 0 && ks - a.key[t - 1] <= reach) --t;
+        const int hw = n > 0 ? (int)a.solve_res[1] : 0;
+        for (int s = bid0 * 8 + warp; s < n; s += nblk0 * 8) {
+            const int ks = a.perm[s];
+            const Marker &ms = a.mk[ks];
             double b0 = 0.0, b1 = 0.0;
-            for (; t < n && a.key[t] - ks <= reach; ++t) {
+            for (int t = s - hw + lane; t <= s + hw; t += 32) {
+                if (t < 0 || t >= n) continue;
                 const int l = a.perm[t];
                 const double b = bval(ms, a.mk[l]);
                 b0 += b * a.y[l];
                 b1 += b * a.y[n + l];
             }
-            const double q0 = a.rhs[a.perm[s]], q1 = a.rhs[n + a.perm[s]];
-            rnum += (b0 - q0) * (b0 - q0) + (b1 - q1) * (b1 - q1);
-            rden += q0 * q0 + q1 * q1;
-        }
 #pragma unroll
-        for (int off = 16; off; off >>= 1) {
-            rnum += __shfl_down_sync(0xffffffffu, rnum, off);
-            rden += __shfl_down_sync(0xffffffffu, rden, off);
+            for (int off = 16; off; off >>= 1) {
+                b0 += __shfl_xor_sync(0xffffffffu, b0, off);
+                b1 += __shfl_xor_sync(0xffffffffu, b1, off);
+            }
+            if (lane == 0) {
+                const double q0 = a.rhs[ks], q1 = a.rhs[n + ks];
+                rnum += (b0 - q0) * (b0 - q0) + (b1 - q1) * (b1 - q1);
+                rden += q0 * q0 + q1 * q1;
+            }
         }
     }
     // deterministic block reduction per wing
