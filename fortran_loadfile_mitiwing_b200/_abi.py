@@ -70,6 +70,7 @@ ABI = {
     "lbm_get_markers": (C.c_int, [_P, _D, _D, _D, C.POINTER(C.c_int)]),
     "lbm_set_timing": (C.c_int, [_P, C.c_int]),
     "lbm_get_timing": (C.c_int, [_P, _D, _D, _D, C.POINTER(C.c_int)]),
+    "lbm_get_launch_count": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
     "lbm_step_index": (C.c_int, [_P]),
     "lbm_last_error": (C.c_char_p, [_P]),
 }

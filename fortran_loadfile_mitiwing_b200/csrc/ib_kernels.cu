@@ -357,42 +357,54 @@ __global__ void __launch_bounds__(256) ib_assemble(const IBArgs a)
     if (tid == 0 && wl) atomicMax(a.wmax, wl);
 }
 
+// Reciprocal of a positive FP64 value by the Newton-Raphson iteration for
+// 1/p: the FP32 reciprocal is the seed, and each step r <- r (2 - p r)
+// doubles the correct digits (~2^-23 -> 2^-46 -> below FP64 rounding).
+// Values outside the FP32 normal range take the IEEE divide.
+__device__ __forceinline__ double recip64(double p)
+{
+    if (!(p > 1e-30 && p < 1e30)) return 1.0 / p;
+    double r = (double)__frcp_rn((float)p);
+    r = r * (2.0 - p * r);
+    r = r * (2.0 - p * r);
+    return r;
+}
+
 // In-place inverse of one symmetric positive definite BS x BS block by one
 // warp (Gauss-Jordan without pivoting, stable for SPD), row stride GP in
-// shared memory; each of the BS steps is one parallel rank-1 update.
-// Returns false if a pivot is not positive.
+// shared memory. The block is held in registers during the BS elimination
+// steps: lane (j, h) owns column j of rows 2e+h; the pivot row and column are
+// broadcast by warp shuffles. Returns false if a pivot is not positive.
 __device__ bool warp_inv(double *G)
 {
     const int lane = threadIdx.x & 31;
-    const int j = lane % BS, ih = lane / BS;    // this lane's column, and row parity
+    const int j = lane % BS, ih = lane / BS;
+    double g[BS / 2];
+#pragma unroll
+    for (int e = 0; e < BS / 2; ++e) g[e] = G[(2 * e + ih) * GP + j];
     bool ok = true;
+#pragma unroll
     for (int k = 0; k < BS; ++k) {
-        const double p = G[k * GP + k];
+        const int kh = k & 1, ke = k >> 1;            // owner half and register of row k
+        const double p = __shfl_sync(0xffffffffu, g[ke], kh * BS + k);
         const bool good = p > 0.0 && isfinite(p);
         ok = ok && good;
-        const double piv = good ? 1.0 / p : 1.0;
-        // all reads of the step first (no store of the step can alias them),
-        // then the stores
-        const double rowk = G[k * GP + j] * piv;                         // scaled row k
-        double cik[BS / 2], gij[BS / 2];
+        const double piv = good ? recip64(p) : 1.0;
+        const double rowk = __shfl_sync(0xffffffffu, g[ke], kh * BS + j) * piv;   // scaled G[k][j]
+        double cik[BS / 2];
+#pragma unroll
+        for (int e = 0; e < BS / 2; ++e) cik[e] = __shfl_sync(0xffffffffu, g[e], ih * BS + k);   // G[2e+ih][k]
 #pragma unroll
         for (int e = 0; e < BS / 2; ++e) {
             const int i = 2 * e + ih;
-            cik[e] = G[i * GP + k];
-            gij[e] = G[i * GP + j];
+            if (i == k) g[e] = (j == k) ? piv : rowk;         // row k
+            else if (j == k) g[e] = -cik[e] * piv;            // column k
+            else g[e] = g[e] - cik[e] * rowk;                 // rank-1 update
         }
-        __syncwarp();
-#pragma unroll
-        for (int e = 0; e < BS / 2; ++e) {
-            const int i = 2 * e + ih;
-            double v;
-            if (i == k) v = (j == k) ? piv : rowk;                       // row k
-            else if (j == k) v = -cik[e] * piv;                          // column k
-            else v = gij[e] - cik[e] * rowk;                             // rank-1 update
-            G[i * GP + j] = v;
-        }
-        __syncwarp();
     }
+#pragma unroll
+    for (int e = 0; e < BS / 2; ++e) G[(2 * e + ih) * GP + j] = g[e];
+    __syncwarp();
     return ok;
 }
 
@@ -904,10 +916,12 @@ int launch_ib_t(lbm_handle *h, const void *fin, int step_index, int ring_slot, c
         ib_markers<T><<<(h->nseg + 7) / 8, 256, 0, st>>>(a, step_index);
         if (!h->static_order) ib_order<<<1, 1024, order_smem(h->nseg), st>>>(a);
         ib_assemble<<<(h->nseg + BS - 1) / BS, 256, 0, st>>>(a);
+        h->launches += h->static_order ? 2 : 3;
     }
     ib_solve<<<1, SOLVE_THREADS, kSolveSmem, st>>>(a, step_index, ring_slot);
     dim3 grid(h->patch_gx(), h->patch_gy());
     ib_spread<T, C><<<grid, 256, 0, st>>>(a, step_index, ring_slot);
+    h->launches += 2;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

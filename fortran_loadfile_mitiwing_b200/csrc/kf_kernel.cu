@@ -541,6 +541,7 @@ int launch_kf_t(lbm_handle *h, const void *fin, void *fout, void *fields, int mo
         else
             kf_kernel<T, C, false><<<grid, block, 0, st>>>(a);
     }
+    h->launches += 1;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -622,6 +623,7 @@ int launch_unpack(lbm_handle *h, const void *fsrc, double *dst)
     case LBM_PREC_FP16: unpack_kernel<__half><<<grid, block, 0, h->stream>>>((const __half *)fsrc, dst, h->nx, h->ny, h->pitch, h->plane); break;
     case LBM_PREC_BF16: unpack_kernel<__nv_bfloat16><<<grid, block, 0, h->stream>>>((const __nv_bfloat16 *)fsrc, dst, h->nx, h->ny, h->pitch, h->plane); break;
     }
+    h->launches += 1;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -634,6 +636,7 @@ int launch_pack(lbm_handle *h, const double *src, void *fdst)
     case LBM_PREC_FP16: pack_kernel<__half><<<grid, block, 0, h->stream>>>(src, (__half *)fdst, h->nx, h->ny, h->pitch, h->plane); break;
     case LBM_PREC_BF16: pack_kernel<__nv_bfloat16><<<grid, block, 0, h->stream>>>(src, (__nv_bfloat16 *)fdst, h->nx, h->ny, h->pitch, h->plane); break;
     }
+    h->launches += 1;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -644,6 +647,7 @@ int launch_residual(lbm_handle *h, const void *fa, const void *fb, double *out2)
         residual_kernel<double><<<blocks, threads, 0, h->stream>>>((const double *)fa, (const double *)fb, h->nx, h->ny, h->d_red);
     else
         residual_kernel<float><<<blocks, threads, 0, h->stream>>>((const float *)fa, (const float *)fb, h->nx, h->ny, h->d_red);
+    h->launches += 1;
     if (cudaGetLastError() != cudaSuccess) return -1;
     std::vector<double> part(2 * blocks);
     if (cudaMemcpyAsync(part.data(), h->d_red, sizeof(double) * 2 * blocks, cudaMemcpyDeviceToHost, h->stream) != cudaSuccess)

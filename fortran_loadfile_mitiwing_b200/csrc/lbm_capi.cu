@@ -747,6 +747,13 @@ int lbm_get_timing(lbm_t *h, double *step_ms, double *ib_ms, double *lattice_ms,
     return LBM_OK;
 }
 
+int lbm_get_launch_count(const lbm_t *h, long long *count)
+{
+    if (!h || !count) return LBM_ERR_ARG;
+    *count = h->launches;
+    return LBM_OK;
+}
+
 int lbm_step_index(const lbm_t *h) { return h ? h->n : LBM_ERR_ARG; }
 
 const char *lbm_last_error(const lbm_t *h) { return h ? h->err.c_str() : "lbm_create failed (bad parameters or no CUDA device)"; }

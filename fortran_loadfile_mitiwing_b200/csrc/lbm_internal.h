@@ -88,7 +88,7 @@ struct lbm_handle {
     size_t elem = 4;
     int kf_vec = 1;   // nodes per thread of the register-loading lattice kernel (1, 2 or 4)
     int kf_tma = 1;   // bulk-copy staged lattice kernel (the default)
-    int kf_rows = 16; // rows swept by one CTA of the staged kernel
+    int kf_rows = 8;  // rows swept by one CTA of the staged kernel
     int dev = 0;
     cudaStream_t stream = nullptr;
     void *fbuf[2] = {nullptr, nullptr};     // first element of plane 0
@@ -149,6 +149,7 @@ struct lbm_handle {
     std::vector<cudaEvent_t> ev, ev_side;
     double t_step = 0, t_ib = 0, t_kf = 0;
     int t_steps = 0;
+    long long launches = 0;   // kernels launched by this handle (lbm_get_launch_count)
     // driver state
     int n = 1;
     int inited = 0;

@@ -195,6 +195,11 @@ LBM_API int lbm_get_markers(lbm_t *h, double *xb2, double *yb2, double *solve_re
 LBM_API int lbm_set_timing(lbm_t *h, int enable);
 LBM_API int lbm_get_timing(lbm_t *h, double *step_ms, double *ib_ms, double *lattice_ms, int *steps);
 
+/* number of CUDA kernels this handle has launched since lbm_create (all
+ * entry points: steps, population transfers, residuals). No counterpart in
+ * the reference, which has no device code. */
+LBM_API int lbm_get_launch_count(const lbm_t *h, long long *count);
+
 /* current step counter n of the driver loop (1 before the first step). */
 LBM_API int lbm_step_index(const lbm_t *h);
 
