@@ -15,6 +15,8 @@ LBM_ERR_IO = -4
 LBM_ERR_SOLVER = -5
 LBM_ERR_NONFINITE = -6
 LBM_ERR_RANGE = -7
+LBM_ERR_SIZE = -8
+LBM_RESIDUAL_MAX_ROWS = 16384
 
 LBM_PREC_FP32 = 0
 LBM_PREC_FP64 = 1
@@ -70,6 +72,7 @@ ABI = {
     "lbm_get_markers": (C.c_int, [_P, _D, _D, _D, C.POINTER(C.c_int)]),
     "lbm_set_timing": (C.c_int, [_P, C.c_int]),
     "lbm_get_timing": (C.c_int, [_P, _D, _D, _D, C.POINTER(C.c_int)]),
+    "lbm_residual_device": (C.c_int, [_P, _P, _P, _P, C.c_int, C.c_int, C.c_int, _P, _D]),
     "lbm_get_launch_count": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
     "lbm_step_index": (C.c_int, [_P]),
     "lbm_last_error": (C.c_char_p, [_P]),

@@ -18,7 +18,8 @@
  *     pointers are borrowed for the duration of a call only. Calls on one
  *     handle must be serialised by the caller; different handles may be
  *     driven from different host threads.
- *   - Device pointers never cross this ABI.
+ *   - Device pointers never cross this ABI, except the velocity fields given
+ *     to lbm_residual_device.
  */
 #ifndef LBM_B200_H
 #define LBM_B200_H
@@ -47,6 +48,7 @@ extern "C" {
 #define LBM_ERR_SOLVER      -5   /* immersed-boundary system not positive definite / singular */
 #define LBM_ERR_NONFINITE   -6   /* NaN/Inf seen in forces or in the mass check */
 #define LBM_ERR_RANGE       -7   /* a marker's support box reaches the three outermost node layers */
+#define LBM_ERR_SIZE        -8   /* size beyond a fixed maximum (lbm_residual_device) */
 
 /* storage precision of the populations (all collision arithmetic is FP32,
  * or FP64 for LBM_PREC_FP64; immersed-boundary solve and force sums are FP64) */
@@ -194,6 +196,29 @@ LBM_API int lbm_get_markers(lbm_t *h, double *xb2, double *yb2, double *solve_re
  * the lattice kernel, and the number of steps timed (any pointer nullable). */
 LBM_API int lbm_set_timing(lbm_t *h, int enable);
 LBM_API int lbm_get_timing(lbm_t *h, double *step_ms, double *ib_ms, double *lattice_ms, int *steps);
+
+/* Residual of erranalysis (solution.f90:74-122) on velocity fields held in
+ * the CALLER's device memory, for drivers that keep u, v on the GPU
+ * themselves (OpenACC or CUDA Fortran arrays, as the reference's own
+ * erranalysis uses) and cannot let the library allocate: their arrays may
+ * fill the device's memory, and an allocation or free per call would
+ * synchronise the device. This entry point has no counterpart in the
+ * reference. It needs no handle and allocates nothing: its scratch is one
+ * fixed array in device memory per device, sized for at most
+ * LBM_RESIDUAL_MAX_ROWS interior rows (ny - 2); a larger ny returns
+ * LBM_ERR_SIZE and launches nothing.
+ *   u, v, u0, v0: device arrays of nx*ny values (x fastest), FP64 or FP32
+ *     as `precision` says (LBM_PREC_FP64 / LBM_PREC_FP32), on the current
+ *     device; interior nodes only enter the sums, as in the reference.
+ *   stream: a cudaStream_t, or NULL for the legacy default stream; the call
+ *     synchronises it and writes *err = ||u - u0|| / (||u|| + 1e-30).
+ * The first call on each device (with that device current) looks up the
+ * scratch's address; make that first call before any stream capture. Calls
+ * whose work overlaps on the GPU (other streams, other host threads on the
+ * same device) share the scratch and race: serialise them. */
+#define LBM_RESIDUAL_MAX_ROWS 16384
+LBM_API int lbm_residual_device(const void *u, const void *v, const void *u0, const void *v0,
+                                int nx, int ny, int precision, void *stream, double *err);
 
 /* number of CUDA kernels this handle has launched since lbm_create (all
  * entry points: steps, population transfers, residuals). No counterpart in
