@@ -34,7 +34,7 @@ UNIT = "MLUPS"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--precision", default="fp32")
@@ -94,6 +94,13 @@ class ClockSampler:
         self.gpu = gpu_index
         self.proc = None
         self.path = None
+        self.skip = 0
+
+    def _lines(self):
+        try:
+            return [ln for ln in open(self.path) if ln.strip()]
+        except OSError:
+            return []
 
     def start(self):
         try:
@@ -104,6 +111,12 @@ class ClockSampler:
                  "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return
+        # wait for the sampler's first line, then keep only later samples
+        t0 = time.perf_counter()
+        while not self._lines() and time.perf_counter() - t0 < 5.0 and self.proc.poll() is None:
+            time.sleep(0.02)
+        self.skip = len(self._lines())
 
     def stop(self):
         if not self.proc:
@@ -115,7 +128,9 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
+        lines = self._lines()
+        lines = lines[self.skip:] or lines
+        for line in lines:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -141,10 +156,15 @@ def measured_peak():
 
 
 def kf_traffic():
-    """DRAM bytes per lattice-kernel launch from the committed ncu summary, or None."""
+    """DRAM bytes per lattice-kernel launch from the committed ncu summary
+    (the `key: value` lines of profiles/kf_tma_traffic.txt), or None."""
     try:
-        d = json.load(open(os.path.join(ROOT, "profiles", "kf_traffic.json")))
-        return d
+        d = {}
+        for line in open(os.path.join(ROOT, "profiles", "kf_tma_traffic.txt")):
+            k, sep, v = line.partition(":")
+            if sep and k.strip() in ("nx", "ny", "bytes_per_launch"):
+                d[k.strip()] = float(v.split()[0])
+        return d or None
     except Exception:
         return None
 
@@ -258,7 +278,7 @@ def run_ours(args, world, rank, local):
         "config": workload(args),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "peak_source": peak_kind, "bytes_per_update": bpl,
-                     "kernel": "kf_kernel (fused stream/collide/boundary)",
+                     "kernel": "kf_tma (fused stream/collide/boundary; with the split, kf_tma outside the body envelope + kf_vec inside)",
                      "kernel_ms": kf_ms.value / k, "ib_ms": ib_ms.value / k},
         "gpu_launches": int(n1.value - n0.value),
         "clocks": clocks,
