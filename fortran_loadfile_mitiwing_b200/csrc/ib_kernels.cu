@@ -7,10 +7,15 @@
 // solves A x = U_b - X1 u* by LU (cusolverDnDgetrf/getrs) and spreads
 // du = X2 x. With D = X1, A = (D D^T) W, so y = W x solves the symmetric
 // positive definite system (D D^T) y = U_b - D u* and du = D^T y: the same
-// correction, with arc_l dropping out. The launches of one step:
-//   ib_markers  one warp per marker: position, boundary velocity, support box
-//               and one-axis kernel values (move_boundary, :1540-1606), then
-//               b = D u* over the box with a warp-shuffle sum (:1609-1629);
+// correction, with arc_l dropping out.
+//
+// The marker positions follow the prescribed motion, so D D^T and its
+// factorization depend on the step index only, not on the flow. The
+// launches are therefore two chains. The factorization chain of a step
+// (which the host runs one step ahead, concurrently with the previous step,
+// into one of two buffer slots):
+//   ib_geometry one thread per marker: position, boundary velocity, support
+//               box and one-axis kernel values (move_boundary, :1540-1606);
 //   ib_order    (several bodies only) one CTA sorts the markers along the
 //               longer axis of the marker cloud. A single rigid body keeps one
 //               order for the whole run: its markers sorted by body-frame
@@ -20,16 +25,24 @@
 //               apart per axis), so the CTA builds its diagonal block and the
 //               block coupling it to the previous one, and checks that no
 //               coupling reaches further;
-//   ib_solve    one CTA: correction-patch rectangle, force-row header, block
-//               cyclic reduction of the block tridiagonal system (log2 of the
-//               block count levels of Gauss-Jordan block inverses and block
-//               products, FP64), back substitution; a dense Cholesky replaces
-//               it when a coupling reaches past the neighbouring block;
+//   ib_factor   one CTA: block cyclic reduction of the block tridiagonal
+//               matrix (log2 of the block count levels of Gauss-Jordan block
+//               inverses and block products, FP64), keeping per eliminated
+//               block D^-1 and the two coupling factors; a dense Cholesky
+//               replaces it when a coupling reaches past the neighbouring block.
+// The flow chain of the step:
+//   ib_interp   one warp per marker: b = D u* over the support box and
+//               rhs = U_b - b (:1609-1629);
+//   ib_solve    one CTA: correction-patch rectangle, force-row header, the
+//               forward and backward sweeps of the reduction over the two
+//               right-hand sides (or the two triangular solves of the dense
+//               factor);
 //   ib_spread   du = D^T y per node, gathered in marker order over the
 //               markers whose box covers the node (no atomics), written to the
 //               correction patch the lattice kernel reads; force and moment
 //               sums (:1645-1675, solution.f90:327-336) and the solve
 //               residual in FP64 with a deterministic two-level reduction.
+
 #include <math.h>
 
 #include "lbm_internal.h"
@@ -38,12 +51,14 @@ namespace {
 
 constexpr int BS = 16;                 // block size of the cyclic reduction
 constexpr int NMARK_MAX = 2048;        // largest marker count
+constexpr int FACTOR_THREADS = 512;
+constexpr int BOPS_WARPS = FACTOR_THREADS / 32;   // warps running block operations
 constexpr int SOLVE_THREADS = 512;
-constexpr int BOPS_WARPS = 16;         // warps running block operations
-constexpr int FC = 2 * BS + 2;         // columns of F: [D^-1 L | D^-1 U | D^-1 r]
+constexpr int FL = 2 * BS;             // columns of a coupling panel [L_o | L_q^T]
+constexpr int GW = 3 * BS;             // row width of a stored factor block [D^-1 | F_L | F_U]
 constexpr int GP = BS + 1;             // padded row stride of square blocks in shared memory
-constexpr int WS = BS * GP + BS * FC + BS * GP + 2 * BS;   // workspace per warp (doubles)
-constexpr int NPART = 3 * LBM_MAXW + 3;                     // per-CTA partials of ib_spread
+constexpr int WS = BS * GP + BS * FL + BS * GP;   // workspace per warp (doubles)
+constexpr int NPART = 3 * LBM_MAXW + 3;           // per-CTA partials of ib_spread
 
 // one-axis kernel value (boundary_condition.f90:1563-1600), disr = |r|
 __device__ __forceinline__ double delta1(double disr, int smooth)
@@ -155,21 +170,24 @@ __device__ Marker make_marker(const IBArgs &a, const double *row, int k)
     return m;
 }
 
-// one warp per marker: geometry, then b = D u* and rhs = U_b - b
+
+// one thread per marker: geometry of this step (errors go to the slot's status)
+__global__ void __launch_bounds__(128) ib_geometry(const IBArgs a, int step_index)
+{
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.nseg) return;
+    const double *row = motion_row(a, step_index, nullptr);
+    a.mk[k] = make_marker(a, row, k);
+}
+
+// one warp per marker: b = D u* over the support box, rhs = U_b - b
 template <typename T>
-__global__ void __launch_bounds__(256) ib_markers(const IBArgs a, int step_index)
+__global__ void __launch_bounds__(256) ib_interp(const IBArgs a)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int k = blockIdx.x * 8 + warp;
     if (k >= a.nseg) return;
-    const double *row = motion_row(a, step_index, nullptr);
-    Marker m;
-    if (lane == 0) m = make_marker(a, row, k);
-    // broadcast the marker to the warp through shared memory
-    __shared__ Marker sm[8];
-    if (lane == 0) { sm[warp] = m; a.mk[k] = m; }
-    __syncwarp();
-    m = sm[warp];
+    const Marker m = a.mk[k];
     const int nbx = m.i2 - m.i1 + 1, nby = m.j2 - m.j1 + 1;
     const int nn = nbx > 0 && nby > 0 ? nbx * nby : 0;
     double su = 0.0, sv = 0.0;
@@ -225,6 +243,7 @@ __device__ void write_header(const IBArgs &a, const double *row, double time, in
         o[6] = r[0]; o[7] = r[1]; o[8] = r[2];
     }
 }
+
 
 // Several bodies: sort the markers along the longer axis of the marker cloud
 // (stable, ties by index) into perm/key, with reach = 6 lattice units along
@@ -288,10 +307,10 @@ __global__ void __launch_bounds__(1024) ib_order(const IBArgs a)
     }
 }
 
-// One CTA per block of BS markers in the solve order: the diagonal block D_b
-// and the coupling L_b to block b-1 (kept twice: working copy and assembled
-// copy for the residual), the block's right-hand sides, and the longest
-// coupling in the order (half-bandwidth).
+
+// One CTA per block of BS markers in the solve order: the diagonal block D_b,
+// the coupling L_b to block b-1, and the longest coupling in the order
+// (half-bandwidth).
 __global__ void __launch_bounds__(256) ib_assemble(const IBArgs a)
 {
     const int n = a.nseg, blk = blockIdx.x, tid = threadIdx.x;
@@ -313,8 +332,6 @@ __global__ void __launch_bounds__(256) ib_assemble(const IBArgs a)
         bx[m] = (srt >= 0 && srt < n) ? mbox(a.mk[a.perm[srt]]) : make_int4(1, 0, 1, 0);
     }
     __syncthreads();
-    const int nb = (n + BS - 1) / BS;
-    double *D0 = a.bD + (long long)nb * BS * BS, *L0 = a.bL + (long long)nb * BS * BS;
     for (int q = tid; q < 2 * BS * BS; q += blockDim.x) {
         const bool lower = q >= BS * BS;
         const int r = (q % (BS * BS)) / BS, c = q % BS;
@@ -333,12 +350,8 @@ __global__ void __launch_bounds__(256) ib_assemble(const IBArgs a)
             }
         }
         const long long g = (long long)blk * BS * BS + r * BS + c;
-        if (lower) { a.bL[g] = v; L0[g] = v; }
-        else { a.bD[g] = v; D0[g] = v; }
-    }
-    if (tid < 2 * BS) {
-        const int r = tid / 2, c = tid % 2, srt = blk * BS + r;
-        a.bX[2 * srt + c] = srt < n ? a.rhs[c * n + a.perm[srt]] : 0.0;
+        if (lower) a.bL[g] = v;
+        else a.bD[g] = v;
     }
     // half-bandwidth: boxes (<= 6 nodes wide) overlap only for markers closer
     // than `reach` along the order's key
@@ -396,12 +409,6 @@ __device__ bool warp_inv(double *G)
     return ok;
 }
 
-// Block products of the cyclic reduction. Lane 2r+h of a warp owns output
-// row r (0..BS-1) and half h of the columns; B rows are read as 16-byte pairs
-// that the two lanes of a row share, so one product of a BS x BS block with a
-// BS x FC panel costs BS x (1 + BS/4 + 1) shared loads per lane, not one
-// per multiply-add.
-
 // n doubles (a multiple of 32) from global to shared memory, all loads in flight
 template <int N>
 __device__ __forceinline__ void stage(double *dst, const double *__restrict__ src)
@@ -428,51 +435,35 @@ __device__ __forceinline__ void stage_sq(double *dst, const double *__restrict__
     }
 }
 
-// acc[c] = sum_t A(r,t) B[t][h*BS + c] (c < BS) and acc[BS] = sum_t A(r,t) B[t][2 BS + h];
-// A(r,t) is A[r][t] (padded layout), or A[t][r] when TA; B is BS x FC
-template <bool TA>
-__device__ __forceinline__ void rowmm_full(const double *A, const double *B, double acc[BS + 1])
+
+// Block products of the cyclic reduction. Lane 2r+h of a warp owns output
+// row r (0..BS-1) and half h of the columns; B rows are read as 16-byte pairs
+// that the two lanes of a row share, so a product costs BS x (1 + NH/2)
+// shared loads per lane instead of two per multiply-add.
+// acc[c] = sum_t A(r,t) B[t*ldb + h*NH + c], c < NH; A(r,t) is A[r][t] in the
+// padded (GP) layout, or A[t][r] when TA.
+template <int NH, bool TA>
+__device__ __forceinline__ void rowmm(const double *A, const double *B, int ldb, double acc[NH])
 {
     const int lane = threadIdx.x & 31, r = lane >> 1, h = lane & 1;
 #pragma unroll
-    for (int c = 0; c <= BS; ++c) acc[c] = 0.0;
+    for (int c = 0; c < NH; ++c) acc[c] = 0.0;
 #pragma unroll
     for (int t = 0; t < BS; ++t) {
         const double a = TA ? A[t * GP + r] : A[r * GP + t];
-        const double2 *b = reinterpret_cast<const double2 *>(B + t * FC + h * BS);
+        const double2 *b = reinterpret_cast<const double2 *>(B + t * ldb + h * NH);
 #pragma unroll
-        for (int c = 0; c < BS / 2; ++c) {
+        for (int c = 0; c < NH / 2; ++c) {
             const double2 bb = b[c];
             acc[2 * c] += a * bb.x;
             acc[2 * c + 1] += a * bb.y;
         }
-        acc[BS] += a * B[t * FC + 2 * BS + h];
     }
 }
 
-// acc[c] = sum_t A(r,t) B[t][h*BS/2 + c] (c < BS/2) and acc[BS/2] = sum_t A(r,t) B[t][2 BS + h]
-template <bool TA>
-__device__ __forceinline__ void rowmm_half(const double *A, const double *B, double acc[BS / 2 + 1])
-{
-    const int lane = threadIdx.x & 31, r = lane >> 1, h = lane & 1;
-#pragma unroll
-    for (int c = 0; c <= BS / 2; ++c) acc[c] = 0.0;
-#pragma unroll
-    for (int t = 0; t < BS; ++t) {
-        const double a = TA ? A[t * GP + r] : A[r * GP + t];
-        const double2 *b = reinterpret_cast<const double2 *>(B + t * FC + h * (BS / 2));
-#pragma unroll
-        for (int c = 0; c < BS / 4; ++c) {
-            const double2 bb = b[c];
-            acc[2 * c] += a * bb.x;
-            acc[2 * c + 1] += a * bb.y;
-        }
-        acc[BS / 2] += a * B[t * FC + 2 * BS + h];
-    }
-}
-
-// dense fallback: Cholesky of the full B (global memory) and two solves, whole CTA
-__device__ void dense_solve(const IBArgs &a, double *yv, int *bad)
+// dense fallback, factor: Cholesky L L^T of the full D D^T in the solve order
+// (row-major, lower triangle, in place), whole CTA
+__device__ void dense_factor(const IBArgs &a, int *bad)
 {
     const int n = a.nseg, tid = threadIdx.x, nt = blockDim.x;
     const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
@@ -480,10 +471,6 @@ __device__ void dense_solve(const IBArgs &a, double *yv, int *bad)
     for (long long q = tid; q < (long long)n * n; q += nt) {
         const int k = (int)(q / n), l = (int)(q % n);
         L[q] = bval(a.mk[a.perm[k]], a.mk[a.perm[l]]);
-    }
-    for (int q = tid; q < n; q += nt) {
-        yv[q] = a.rhs[a.perm[q]];
-        yv[n + q] = a.rhs[n + a.perm[q]];
     }
     __syncthreads();
     for (int k = 0; k < n; ++k) {
@@ -497,13 +484,26 @@ __device__ void dense_solve(const IBArgs &a, double *yv, int *bad)
         __syncthreads();
         const double dk = L[(long long)k * n + k];
         for (int i = k + 1 + tid; i < n; i += nt) L[(long long)i * n + k] /= dk;
-        if (tid < 2) yv[tid * n + k] /= dk;
         __syncthreads();
         for (int i = k + 1 + warp; i < n; i += nw) {
             const double lik = L[(long long)i * n + k];
             for (int j = k + 1 + lane; j <= i; j += 32) L[(long long)i * n + j] -= lik * L[(long long)j * n + k];
         }
-        const double z0 = yv[k], z1 = yv[n + k];
+        __syncthreads();
+    }
+}
+
+// dense fallback, solve: L z = r, then L^T y = z, for the two right-hand
+// sides yv[0..n) and yv[n..2n) (shared memory), whole CTA
+__device__ void dense_tri(const IBArgs &a, double *yv)
+{
+    const int n = a.nseg, tid = threadIdx.x, nt = blockDim.x;
+    const double *L = a.B;
+    for (int k = 0; k < n; ++k) {
+        const double dk = L[(long long)k * n + k];
+        const double z0 = yv[k] / dk, z1 = yv[n + k] / dk;
+        __syncthreads();
+        if (tid == 0) { yv[k] = z0; yv[n + k] = z1; }
         for (int i = k + 1 + tid; i < n; i += nt) {
             const double lik = L[(long long)i * n + k];
             yv[i] -= lik * z0;
@@ -522,17 +522,167 @@ __device__ void dense_solve(const IBArgs &a, double *yv, int *bad)
     }
 }
 
-// The linear solve of one step, one CTA of SOLVE_THREADS threads; dynamic
-// shared memory: one block-operation workspace of WS doubles per warp of the
-// first BOPS_WARPS warps.
-__global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int step_index, int ring_slot)
+
+// Factorization of one step's D D^T, one CTA of FACTOR_THREADS threads;
+// dynamic shared memory: one block-operation workspace of WS doubles per warp.
+// Block cyclic reduction: at stride st the active blocks are the multiples
+// of st, and the odd multiples o are eliminated into their even neighbours.
+// For each eliminated block the factor buffer keeps, row by row, BS x GW
+// values [D_o^-1 | F_L | F_U] with F_L = D_o^-1 L_o (coupling to o - st) and
+// F_U = D_o^-1 L_q^T (coupling to q = o + st); block 0, the last one left,
+// keeps D_0^-1. The even neighbours are updated as
+//   D_e -= L_q^T F_L(q) + L_e F_U(p),   L_e <- -L_e F_L(p)   (p = e - st, q = e + st).
+__global__ void __launch_bounds__(FACTOR_THREADS) ib_factor(const IBArgs a)
 {
     extern __shared__ __align__(16) double Wbase[];
+    const int n = a.nseg, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    __shared__ int bad, dense;
+    if (tid == 0) {
+        const int w = *a.wmax;
+        bad = 0;
+        dense = (w > BS || a.force_dense) ? 1 : 0;
+        a.fmode[0] = dense;
+        a.fmode[1] = w;
+        *a.wmax = 0;   // for the next assembly
+    }
+    __syncthreads();
+    if (n == 0) return;
+    if (dense) {
+        dense_factor(a, &bad);
+        __syncthreads();
+        if (tid == 0 && bad) atomicOr(a.status, LBM_ST_SOLVER);
+        return;
+    }
+    const int nb = (n + BS - 1) / BS;
+    double *Db = a.bD, *Lb = a.bL, *Gf = a.gf;
+    double *W = Wbase + (long long)warp * WS;
+    const int pr = lane >> 1, ph = lane & 1;   // product lane layout: row, column half
+    for (int st = 1; st < nb; st <<= 1) {
+        const int nodd = (nb - st + 2 * st - 1) / (2 * st);
+        for (int m = warp; m < nodd; m += BOPS_WARPS) {
+            const int o = st * (2 * m + 1), q2 = o + st;
+            double *Gs = W, *Rs = W + BS * GP;   // D_o, then [L_o | L_q^T]
+            stage_sq(Gs, Db + (long long)o * BS * BS);
+            {
+                double lv[BS * BS / 32], lq[BS * BS / 32];
+#pragma unroll
+                for (int it = 0; it < BS * BS / 32; ++it) {
+                    lv[it] = Lb[(long long)o * BS * BS + lane + 32 * it];
+                    lq[it] = q2 < nb ? Lb[(long long)q2 * BS * BS + lane + 32 * it] : 0.0;
+                }
+#pragma unroll
+                for (int it = 0; it < BS * BS / 32; ++it) {
+                    const int e = lane + 32 * it, r = e / BS, c = e % BS;
+                    Rs[r * FL + c] = lv[it];
+                    Rs[c * FL + BS + r] = lq[it];
+                }
+            }
+            __syncwarp();
+            if (!warp_inv(Gs) && lane == 0) bad = 1;
+            double *Go = Gf + (long long)o * BS * GW + pr * GW;
+#pragma unroll
+            for (int c = 0; c < BS / 2; ++c) Go[ph * (BS / 2) + c] = Gs[pr * GP + ph * (BS / 2) + c];
+            double acc[BS];
+            rowmm<BS, false>(Gs, Rs, FL, acc);
+            double2 *F2 = reinterpret_cast<double2 *>(Go + BS + ph * BS);
+#pragma unroll
+            for (int c = 0; c < BS / 2; ++c) F2[c] = make_double2(acc[2 * c], acc[2 * c + 1]);
+            __syncwarp();
+        }
+        __syncthreads();
+        const int neven = (nb + 2 * st - 1) / (2 * st);
+        for (int m = warp; m < neven; m += BOPS_WARPS) {
+            const int e = 2 * st * m, o1 = e - st, o2 = e + st;
+            double *As = W, *Fs = W + BS * GP, *Ds = Fs + BS * FL;
+            double *De = Db + (long long)e * BS * BS, *Le = Lb + (long long)e * BS * BS;
+            stage_sq(Ds, De);
+            if (o2 < nb) {   // D_e -= L_q^T F_L(q)
+                stage_sq(As, Lb + (long long)o2 * BS * BS);
+                const double *G = Gf + (long long)o2 * BS * GW + BS;
+                double v[BS * BS / 32];
+#pragma unroll
+                for (int it = 0; it < BS * BS / 32; ++it) {
+                    const int q = lane + 32 * it;
+                    v[it] = G[(q / BS) * GW + q % BS];
+                }
+#pragma unroll
+                for (int it = 0; it < BS * BS / 32; ++it) {
+                    const int q = lane + 32 * it;
+                    Fs[(q / BS) * FL + q % BS] = v[it];
+                }
+                __syncwarp();
+                double acc[BS / 2];
+                rowmm<BS / 2, true>(As, Fs, FL, acc);
+#pragma unroll
+                for (int c = 0; c < BS / 2; ++c) Ds[pr * GP + ph * (BS / 2) + c] -= acc[c];
+                __syncwarp();
+            }
+            if (m > 0) {   // D_e -= L_e F_U(p), L_e <- -L_e F_L(p); lanes h = 0 hold the new L_e row
+                stage_sq(As, Le);
+                const double *G = Gf + (long long)o1 * BS * GW + BS;
+                double v[BS * FL / 32];
+#pragma unroll
+                for (int it = 0; it < BS * FL / 32; ++it) {
+                    const int q = lane + 32 * it;
+                    v[it] = G[(q / FL) * GW + q % FL];
+                }
+#pragma unroll
+                for (int it = 0; it < BS * FL / 32; ++it) Fs[lane + 32 * it] = v[it];
+                __syncwarp();
+                double acc[BS];
+                rowmm<BS, false>(As, Fs, FL, acc);
+                if (ph == 0) {
+                    double2 *L2 = reinterpret_cast<double2 *>(Le + pr * BS);
+#pragma unroll
+                    for (int c = 0; c < BS / 2; ++c) L2[c] = make_double2(-acc[2 * c], -acc[2 * c + 1]);
+                } else {
+#pragma unroll
+                    for (int c = 0; c < BS; ++c) Ds[pr * GP + c] -= acc[c];
+                }
+                __syncwarp();
+            }
+#pragma unroll
+            for (int it = 0; it < BS * BS / 32; ++it) {
+                const int q = lane + 32 * it;
+                De[q] = Ds[(q / BS) * GP + q % BS];
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+    }
+    // block 0: inverted by every warp on its own copy, stored by warp 0 (a
+    // lone warp working while the others wait at the barrier was measured
+    // several times slower)
+    {
+        double *Gs = W;
+        stage_sq(Gs, Db);
+        __syncwarp();
+        const bool ok = warp_inv(Gs);
+        if (warp == 0) {
+            double *Go = Gf + pr * GW;
+#pragma unroll
+            for (int c = 0; c < BS / 2; ++c) Go[ph * (BS / 2) + c] = Gs[pr * GP + ph * (BS / 2) + c];
+            if (!ok && lane == 0) bad = 1;
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && bad) atomicOr(a.status, LBM_ST_SOLVER);
+}
+
+// The flow-dependent solve of one step, one CTA of SOLVE_THREADS threads;
+// dynamic shared memory: the right-hand sides in the solve order, two values
+// per marker, padded to whole blocks.
+//   forward, st = 1, 2, 4, ...:  r_e -= F_L(q)^T r_q + F_U(p)^T r_p  (even e)
+//   block 0:                     x_0 = D_0^-1 r_0
+//   backward, st = ..., 2, 1:    x_o = D_o^-1 r_o - F_L(o) x_p - F_U(o) x_q  (odd o)
+// (F_L(q)^T = L_q^T D_q^-1 and F_U(p)^T = L_e D_p^-1 since D is symmetric.)
+__global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int step_index, int ring_slot)
+{
+    extern __shared__ __align__(16) double X[];
     const int n = a.nseg, tid = threadIdx.x, nt = blockDim.x;
     const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
     __shared__ int bb[4];
-    __shared__ int bad, wmax;
-    if (tid == 0) { bb[0] = 1 << 30; bb[1] = 1 << 30; bb[2] = -1; bb[3] = -1; bad = 0; wmax = *a.wmax; }
+    if (tid == 0) { bb[0] = 1 << 30; bb[1] = 1 << 30; bb[2] = -1; bb[3] = -1; }
     __syncthreads();
     // patch rectangle: bounding box of all support boxes
     int b0 = 1 << 30, b1 = 1 << 30, b2 = -1, b3 = -1;
@@ -552,6 +702,9 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
         double time;
         const double *row = motion_row(a, step_index, &time);
         write_header(a, row, time, ring_slot);
+        // errors of this step's factorization chain
+        const unsigned fs = *a.fstatus;
+        if (fs) { atomicOr(a.status, fs); *a.fstatus = 0u; }
         PatchInfo pi{0, 0, 0, 0};
         if (bb[2] >= bb[0]) {
             pi.i0 = bb[0]; pi.j0 = bb[1]; pi.w = bb[2] - bb[0] + 1; pi.h = bb[3] - bb[1] + 1;
@@ -561,162 +714,86 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
             }
         }
         *a.pinfo = pi;
-        a.solve_res[1] = (double)wmax;
-        *a.wmax = 0;   // for the next step's assembly
+        a.solve_res[1] = (double)a.fmode[1];
     }
     if (n == 0) return;
     const int nb = (n + BS - 1) / BS;
-    double *Db = a.bD, *Lb = a.bL, *Fb = a.bF, *Xb = a.bX;
-    if (wmax > BS || a.force_dense) {
-        double *yv = Xb + 2 * (long long)BS * nb;   // 2n scratch after the block rhs
-        dense_solve(a, yv, &bad);
-        for (int q = tid; q < n; q += nt) {
-            a.y[a.perm[q]] = yv[q];
-            a.y[n + a.perm[q]] = yv[n + q];
+    if (a.fmode[0]) {   // dense factor
+        for (int s = tid; s < n; s += nt) {
+            X[s] = a.rhs[a.perm[s]];
+            X[n + s] = a.rhs[n + a.perm[s]];
         }
-        if (tid == 0 && bad) atomicOr(a.status, LBM_ST_SOLVER);
+        __syncthreads();
+        dense_tri(a, X);
+        for (int s = tid; s < n; s += nt) {
+            a.y[a.perm[s]] = X[s];
+            a.y[n + a.perm[s]] = X[n + s];
+        }
         return;
     }
-    // cyclic reduction: at stride st the active blocks are multiples of st;
-    // odd multiples are eliminated into their even neighbours. Each block
-    // operation runs on one warp in its shared-memory workspace W.
-    double *W = Wbase + (long long)warp * WS;
-    const bool bw = warp < BOPS_WARPS;
-    const int pr = lane >> 1, ph = lane & 1;     // product lane layout: row, column half
-    int levels = 0;
-    for (int st = 1; st < nb; st <<= 1, ++levels) {
-        const int nodd = (nb - st + 2 * st - 1) / (2 * st);
-        if (bw)
-            for (int m = warp; m < nodd; m += BOPS_WARPS) {
-                // F_o = D_o^-1 [L_o | L_q^T | r_o]
-                const int o = st * (2 * m + 1), q2 = o + st;
-                double *Gs = W, *Rs = W + BS * GP;
-                stage_sq(Gs, Db + (long long)o * BS * BS);
-                {
-                    double lv[BS * BS / 32], lq[BS * BS / 32];
-#pragma unroll
-                    for (int it = 0; it < BS * BS / 32; ++it) {
-                        lv[it] = Lb[(long long)o * BS * BS + lane + 32 * it];
-                        lq[it] = q2 < nb ? Lb[(long long)q2 * BS * BS + lane + 32 * it] : 0.0;
-                    }
-                    const double xr = Xb[2 * (long long)o * BS + lane];
-#pragma unroll
-                    for (int it = 0; it < BS * BS / 32; ++it) {
-                        const int e = lane + 32 * it, r = e / BS, c = e % BS;
-                        Rs[r * FC + c] = lv[it];
-                        Rs[c * FC + BS + r] = lq[it];
-                    }
-                    Rs[pr * FC + 2 * BS + ph] = xr;
-                }
-                __syncwarp();
-                if (!warp_inv(Gs) && lane == 0) bad = 1;
-                double acc[BS + 1];
-                rowmm_full<false>(Gs, Rs, acc);
-                double *F = Fb + (long long)o * BS * FC + pr * FC;
-                double2 *F2 = reinterpret_cast<double2 *>(F + ph * BS);
-#pragma unroll
-                for (int c = 0; c < BS / 2; ++c) F2[c] = make_double2(acc[2 * c], acc[2 * c + 1]);
-                F[2 * BS + ph] = acc[BS];
-                __syncwarp();
-            }
-        __syncthreads();
-        const int neven = (nb + 2 * st - 1) / (2 * st);
-        if (bw)
-            for (int m = warp; m < neven; m += BOPS_WARPS) {
-                const int e = 2 * st * m, o1 = e - st, o2 = e + st;
-                double *As = W, *Fs = W + BS * GP, *Ds = Fs + BS * FC, *Xs = Ds + BS * GP;
-                double *De = Db + (long long)e * BS * BS, *Le = Lb + (long long)e * BS * BS;
-                double *Xe = Xb + 2 * (long long)e * BS;
-                stage_sq(Ds, De);
-                Xs[lane] = Xe[lane];
-                // right neighbour o2 (e is its previous block):
-                // D_e -= L_o2^T FL_o2, r_e -= L_o2^T Fr_o2
-                if (o2 < nb) {
-                    stage_sq(As, Lb + (long long)o2 * BS * BS);
-                    stage<BS * FC>(Fs, Fb + (long long)o2 * BS * FC);
-                    __syncwarp();
-                    double acc[BS / 2 + 1];
-                    rowmm_half<true>(As, Fs, acc);
-#pragma unroll
-                    for (int c = 0; c < BS / 2; ++c) Ds[pr * GP + ph * (BS / 2) + c] -= acc[c];
-                    Xs[lane] -= acc[BS / 2];
-                    __syncwarp();
-                }
-                // left neighbour o1 (e is its next block): D_e -= L_e FU_o1,
-                // r_e -= L_e Fr_o1, new L_e = -L_e FL_o1 (lanes h = 0 hold the
-                // new L_e row, lanes h = 1 the D_e update)
-                if (m > 0) {
-                    stage_sq(As, Le);
-                    stage<BS * FC>(Fs, Fb + (long long)o1 * BS * FC);
-                    __syncwarp();
-                    double acc[BS + 1];
-                    rowmm_full<false>(As, Fs, acc);
-                    if (ph == 0) {
-                        double2 *L2 = reinterpret_cast<double2 *>(Le + pr * BS);
-#pragma unroll
-                        for (int c = 0; c < BS / 2; ++c) L2[c] = make_double2(-acc[2 * c], -acc[2 * c + 1]);
-                    } else {
-#pragma unroll
-                        for (int c = 0; c < BS; ++c) Ds[pr * GP + c] -= acc[c];
-                    }
-                    Xs[lane] -= acc[BS];
-                    __syncwarp();
-                }
-#pragma unroll
-                for (int it = 0; it < BS * BS / 32; ++it) {
-                    const int q = lane + 32 * it;
-                    De[q] = Ds[(q / BS) * GP + q % BS];
-                }
-                Xe[lane] = Xs[lane];
-                __syncwarp();
-            }
-        __syncthreads();
-    }
-    // the last active block (block 0), solved by every block-operation warp
-    // on its own copy and stored by warp 0: measured 6x faster than warp 0
-    // alone while the other warps wait at the barrier
-    if (bw) {
-        double *Gs = W, *Rs = W + BS * GP;
-        stage_sq(Gs, Db);
-        Rs[lane] = Xb[lane];
-        __syncwarp();
-        const bool ok = warp_inv(Gs);
-        double x = 0.0;
-#pragma unroll
-        for (int t = 0; t < BS; ++t) x += Gs[pr * GP + t] * Rs[2 * t + ph];
-        __syncthreads();   // every warp has read Xb
-        if (warp == 0) {
-            Xb[lane] = x;
-            if (!ok && lane == 0) bad = 1;
-        }
-    } else {
-        __syncthreads();
+    for (int s = tid; s < nb * BS; s += nt) {
+        X[2 * s] = s < n ? a.rhs[a.perm[s]] : 0.0;
+        X[2 * s + 1] = s < n ? a.rhs[n + a.perm[s]] : 0.0;
     }
     __syncthreads();
-    // back substitution: x_o = Fr_o - FL_o x_p - FU_o x_q, coarsest level first
+    const double *Gf = a.gf;
+    const int i = lane >> 1, c = lane & 1;   // row of the block, right-hand side
+    int levels = 0;
+    for (int st = 1; st < nb; st <<= 1, ++levels) {
+        const int neven = (nb + 2 * st - 1) / (2 * st);
+        for (int m = warp; m < neven; m += nw) {
+            const int e = 2 * st * m, o1 = e - st, o2 = e + st;
+            double acc = 0.0;
+            if (o2 < nb) {
+                const double *F = Gf + (long long)o2 * BS * GW + BS + i;      // F_L(q)[t][i]
+                const double *r = X + 2 * o2 * BS + c;
+#pragma unroll
+                for (int t = 0; t < BS; ++t) acc += F[t * GW] * r[2 * t];
+            }
+            if (m > 0) {
+                const double *F = Gf + (long long)o1 * BS * GW + 2 * BS + i;  // F_U(p)[t][i]
+                const double *r = X + 2 * o1 * BS + c;
+#pragma unroll
+                for (int t = 0; t < BS; ++t) acc += F[t * GW] * r[2 * t];
+            }
+            X[2 * (e * BS + i) + c] -= acc;
+        }
+        __syncthreads();
+    }
+    if (warp == 0) {
+        const double *G = Gf + i * GW;
+        double x = 0.0;
+#pragma unroll
+        for (int t = 0; t < BS; ++t) x += G[t] * X[2 * t + c];
+        __syncwarp();
+        X[lane] = x;
+    }
+    __syncthreads();
     for (int lv = levels - 1; lv >= 0; --lv) {
         const int st = 1 << lv;
         const int nodd = (nb - st + 2 * st - 1) / (2 * st);
         for (int m = warp; m < nodd; m += nw) {
             const int o = st * (2 * m + 1), p = o - st, q2 = o + st;
-            const double *F = Fb + (long long)o * BS * FC;
-            const int r = lane / 2, c = lane % 2;
-            double s1 = F[r * FC + 2 * BS + c], s2 = 0.0, s3 = 0.0;
+            const double *G = Gf + (long long)o * BS * GW + i * GW;
+            double s1 = 0.0, s2 = 0.0, s3 = 0.0;
 #pragma unroll
-            for (int t = 0; t < BS; ++t) s2 += F[r * FC + t] * Xb[2 * ((long long)p * BS + t) + c];
+            for (int t = 0; t < BS; ++t) {
+                s1 += G[t] * X[2 * (o * BS + t) + c];
+                s2 += G[BS + t] * X[2 * (p * BS + t) + c];
+            }
             if (q2 < nb) {
 #pragma unroll
-                for (int t = 0; t < BS; ++t) s3 += F[r * FC + BS + t] * Xb[2 * ((long long)q2 * BS + t) + c];
+                for (int t = 0; t < BS; ++t) s3 += G[2 * BS + t] * X[2 * (q2 * BS + t) + c];
             }
-            Xb[2 * ((long long)o * BS + r) + c] = s1 - s2 - s3;
+            __syncwarp();
+            X[2 * (o * BS + i) + c] = s1 - s2 - s3;
         }
         __syncthreads();
     }
-    for (int s2 = tid; s2 < n; s2 += nt) {
-        a.y[a.perm[s2]] = Xb[2 * s2];
-        a.y[n + a.perm[s2]] = Xb[2 * s2 + 1];
+    for (int s = tid; s < n; s += nt) {
+        a.y[a.perm[s]] = X[2 * s];
+        a.y[n + a.perm[s]] = X[2 * s + 1];
     }
-    if (tid == 0 && bad) atomicOr(a.status, LBM_ST_SOLVER);
 }
 
 // du = D^T y over the current patch, 16x16 nodes per CTA, plus FP64 force and
@@ -913,6 +990,7 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
     }
 }
 
+
 size_t order_smem(int n)
 {
     int ns = 1;
@@ -920,10 +998,14 @@ size_t order_smem(int n)
     return (sizeof(double) + sizeof(int)) * ns;
 }
 
-constexpr size_t kSolveSmem = sizeof(double) * BOPS_WARPS * WS;
+constexpr size_t kFactorSmem = sizeof(double) * BOPS_WARPS * WS;
+constexpr size_t kSolveSmem = sizeof(double) * 2 * ((NMARK_MAX + BS - 1) / BS) * BS;
 
-IBArgs make_args(lbm_handle *h, const void *fin)
+// arguments of the kernels of one buffer slot (the factorization of the
+// step with parity `slot`)
+IBArgs make_args(lbm_handle *h, const void *fin, int slot)
 {
+    const size_t ns = (size_t)(h->nseg > 0 ? h->nseg : 1);
     IBArgs a;
     a.fin = fin;
     a.prec = h->prec;
@@ -935,9 +1017,16 @@ IBArgs make_args(lbm_handle *h, const void *fin)
     a.xc = h->p.xc; a.yc = h->p.yc; a.mesh_max_scale = h->p.mesh_max_scale;
     a.xb0 = h->d_xb0; a.yb0 = h->d_yb0; a.arc = h->d_arc;
     a.mstep = h->d_mstep; a.msteps = h->msteps; a.mcols = h->mcols; a.mdt = h->mdt;
-    a.mk = h->d_mk; a.rhs = h->d_rhs; a.B = h->d_B; a.y = h->d_y;
-    a.bD = h->d_bD; a.bL = h->d_bL; a.bF = h->d_bF; a.bX = h->d_bX;
-    a.perm = h->d_perm; a.key = h->d_key; a.reach = h->d_reach; a.wmax = h->d_wmax;
+    a.mk = h->d_mk + slot * ns;
+    a.perm = h->static_order ? h->d_perm : h->d_perm + slot * ns;
+    a.key = h->static_order ? h->d_key : h->d_key + slot * ns;
+    a.gf = h->d_gf + slot * h->gf_slot;
+    a.B = h->d_B + slot * ns * ns;
+    a.fmode = h->d_fmode + 2 * slot;
+    a.fstatus = h->d_fstatus + slot;
+    a.rhs = h->d_rhs; a.y = h->d_y;
+    a.bD = h->d_bD; a.bL = h->d_bL;
+    a.reach = h->d_reach; a.wmax = h->d_wmax;
     a.pinfo = h->d_pinfo; a.patch = h->d_patch; a.patch_cap = h->patch_cap;
     a.patch_wmax = h->patch_wmax; a.patch_hmax = h->patch_hmax;
     a.partial = h->d_partial; a.counter = h->d_counter;
@@ -947,14 +1036,12 @@ IBArgs make_args(lbm_handle *h, const void *fin)
 }
 
 template <typename T, typename C>
-int launch_ib_t(lbm_handle *h, const void *fin, int step_index, int ring_slot, cudaStream_t st)
+int launch_flow_t(lbm_handle *h, const void *fin, int step_index, int ring_slot, int slot, cudaStream_t st)
 {
-    IBArgs a = make_args(h, fin);
+    IBArgs a = make_args(h, fin, slot);
     if (h->nseg > 0) {
-        ib_markers<T><<<(h->nseg + 7) / 8, 256, 0, st>>>(a, step_index);
-        if (!h->static_order) ib_order<<<1, 1024, order_smem(h->nseg), st>>>(a);
-        ib_assemble<<<(h->nseg + BS - 1) / BS, 256, 0, st>>>(a);
-        h->launches += h->static_order ? 2 : 3;
+        ib_interp<T><<<(h->nseg + 7) / 8, 256, 0, st>>>(a);
+        h->launches += 1;
     }
     ib_solve<<<1, SOLVE_THREADS, kSolveSmem, st>>>(a, step_index, ring_slot);
     dim3 grid(h->patch_gx(), h->patch_gy());
@@ -968,21 +1055,22 @@ int launch_ib_t(lbm_handle *h, const void *fin, int step_index, int ring_slot, c
 // per-CTA partials of ib_spread (doubles)
 int ib_partials_per_block() { return NPART; }
 
-// scratch sizes of the block cyclic reduction (doubles)
-size_t ib_block_scratch(int nseg, size_t *d, size_t *l, size_t *f, size_t *x)
+// scratch of the block cyclic reduction (doubles): working diagonal and
+// coupling blocks (one set), and the factor buffer of one slot
+void ib_factor_scratch(int nseg, size_t *work_blocks, size_t *factor_slot)
 {
     const size_t nb = (size_t)(nseg + BS - 1) / BS;
-    *d = 2 * nb * BS * BS;   // working blocks, then the assembled copy
-    *l = 2 * nb * BS * BS;
-    *f = nb * BS * (2 * BS + 2);
-    *x = 2 * nb * BS + 2 * (size_t)nseg;
-    return *d + *l + *f + *x;
+    *work_blocks = nb * BS * BS;
+    *factor_slot = nb * BS * GW;
 }
 
 int ib_max_markers() { return NMARK_MAX; }
 
 int ib_configure(lbm_handle *h)
 {
+    (void)h;
+    if (cudaFuncSetAttribute(ib_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactorSmem) != cudaSuccess)
+        return -1;
     if (cudaFuncSetAttribute(ib_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSolveSmem) != cudaSuccess)
         return -1;
     if (cudaFuncSetAttribute(ib_order, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)order_smem(NMARK_MAX)) !=
@@ -991,14 +1079,31 @@ int ib_configure(lbm_handle *h)
     return 0;
 }
 
-int launch_ib(lbm_handle *h, const void *fin, int step_index, int ring_slot, cudaStream_t st)
+// factorization chain of step `step_index` into buffer slot `slot`
+int launch_factor(lbm_handle *h, int step_index, int slot, cudaStream_t st)
+{
+    if (!st) st = h->stream;
+    if (h->nseg == 0) return 0;
+    IBArgs a = make_args(h, nullptr, slot);
+    a.status = a.fstatus;   // errors of this chain are reported by the step that uses it
+    ib_geometry<<<(h->nseg + 127) / 128, 128, 0, st>>>(a, step_index);
+    if (!h->static_order) ib_order<<<1, 1024, order_smem(h->nseg), st>>>(a);
+    ib_assemble<<<(h->nseg + BS - 1) / BS, 256, 0, st>>>(a);
+    ib_factor<<<1, FACTOR_THREADS, kFactorSmem, st>>>(a);
+    h->launches += h->static_order ? 3 : 4;
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+// flow chain of step `step_index`: interpolation, solve with the factor of
+// `slot`, spread and forces
+int launch_flow(lbm_handle *h, const void *fin, int step_index, int ring_slot, int slot, cudaStream_t st)
 {
     if (!st) st = h->stream;
     switch (h->prec) {
-    case LBM_PREC_FP32: return launch_ib_t<float, float>(h, fin, step_index, ring_slot, st);
-    case LBM_PREC_FP64: return launch_ib_t<double, double>(h, fin, step_index, ring_slot, st);
-    case LBM_PREC_FP16: return launch_ib_t<__half, float>(h, fin, step_index, ring_slot, st);
-    case LBM_PREC_BF16: return launch_ib_t<__nv_bfloat16, float>(h, fin, step_index, ring_slot, st);
+    case LBM_PREC_FP32: return launch_flow_t<float, float>(h, fin, step_index, ring_slot, slot, st);
+    case LBM_PREC_FP64: return launch_flow_t<double, double>(h, fin, step_index, ring_slot, slot, st);
+    case LBM_PREC_FP16: return launch_flow_t<__half, float>(h, fin, step_index, ring_slot, slot, st);
+    case LBM_PREC_BF16: return launch_flow_t<__nv_bfloat16, float>(h, fin, step_index, ring_slot, slot, st);
     }
     return -1;
 }

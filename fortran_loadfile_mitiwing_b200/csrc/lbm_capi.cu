@@ -116,12 +116,14 @@ void lookup_row(const std::vector<double> &tab, int rows, int cols, double t, in
 // releases the immersed-boundary scratch (sizes depend on geometry and motion)
 void free_ib(lbm_handle *h)
 {
+    if (h->fstream) cudaStreamSynchronize(h->fstream);
     if (h->side) cudaStreamSynchronize(h->side);
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->ib_ready = 0;
+    h->factored[0] = h->factored[1] = -1;
     free_dev(h->d_patch);
     free_devp(h->d_mk); free_devp(h->d_rhs); free_devp(h->d_B); free_devp(h->d_y); free_devp(h->d_partial);
-    free_devp(h->d_bD); free_devp(h->d_bL); free_devp(h->d_bF); free_devp(h->d_bX);
+    free_devp(h->d_bD); free_devp(h->d_bL); free_devp(h->d_gf); free_devp(h->d_fmode); free_devp(h->d_fstatus);
     free_devp(h->d_perm); free_devp(h->d_key); free_devp(h->d_reach); free_devp(h->d_wmax);
 }
 
@@ -174,24 +176,27 @@ int ensure_ib(lbm_handle *h)
     CK(cudaMalloc(&h->d_patch, 2 * cs * (size_t)h->patch_cap), "alloc patch");
     CK(cudaMemsetAsync(h->d_patch, 0, 2 * cs * (size_t)h->patch_cap, h->stream), "clear patch");
     const int ns = std::max(1, h->nseg);
-    CK(cudaMalloc(&h->d_mk, sizeof(Marker) * ns), "alloc markers");
+    CK(cudaMalloc(&h->d_mk, 2 * sizeof(Marker) * ns), "alloc markers");
     CK(cudaMalloc(&h->d_rhs, sizeof(double) * 2 * ns), "alloc rhs");
     CK(cudaMalloc(&h->d_y, sizeof(double) * 2 * ns), "alloc y");
-    CK(cudaMalloc(&h->d_B, sizeof(double) * (size_t)ns * ns), "alloc B");
-    size_t sd, sl, sf, sx;
-    ib_block_scratch(ns, &sd, &sl, &sf, &sx);
-    CK(cudaMalloc(&h->d_bD, sizeof(double) * sd), "alloc block D");
-    CK(cudaMalloc(&h->d_bL, sizeof(double) * sl), "alloc block L");
-    CK(cudaMalloc(&h->d_bF, sizeof(double) * sf), "alloc block F");
-    CK(cudaMalloc(&h->d_bX, sizeof(double) * sx), "alloc block X");
+    CK(cudaMalloc(&h->d_B, 2 * sizeof(double) * (size_t)ns * ns), "alloc B");
+    size_t swork;
+    ib_factor_scratch(ns, &swork, &h->gf_slot);
+    CK(cudaMalloc(&h->d_bD, sizeof(double) * swork), "alloc block D");
+    CK(cudaMalloc(&h->d_bL, sizeof(double) * swork), "alloc block L");
+    CK(cudaMalloc(&h->d_gf, 2 * sizeof(double) * h->gf_slot), "alloc factor blocks");
+    CK(cudaMalloc(&h->d_fmode, 4 * sizeof(int)), "alloc factor mode");
+    CK(cudaMalloc(&h->d_fstatus, 2 * sizeof(unsigned)), "alloc factor status");
+    CK(cudaMemsetAsync(h->d_fmode, 0, 4 * sizeof(int), h->stream), "clear factor mode");
+    CK(cudaMemsetAsync(h->d_fstatus, 0, 2 * sizeof(unsigned), h->stream), "clear factor status");
     const int nblk = h->patch_gx() * h->patch_gy();
     CK(cudaMalloc(&h->d_partial, sizeof(double) * ib_partials_per_block() * (size_t)nblk), "alloc partials");
     // solve order of the markers: one rigid body keeps its markers sorted by
     // body-frame chordwise position for the whole run (two markers whose
     // support boxes overlap are less than 5*sqrt(2) lattice units apart in any
     // orientation); several bodies are sorted on the device every step
-    CK(cudaMalloc(&h->d_perm, sizeof(int) * ns), "alloc perm");
-    CK(cudaMalloc(&h->d_key, sizeof(double) * ns), "alloc key");
+    CK(cudaMalloc(&h->d_perm, 2 * sizeof(int) * ns), "alloc perm");
+    CK(cudaMalloc(&h->d_key, 2 * sizeof(double) * ns), "alloc key");
     CK(cudaMalloc(&h->d_reach, sizeof(double)), "alloc reach");
     CK(cudaMalloc(&h->d_wmax, sizeof(int)), "alloc wmax");
     CK(cudaMemsetAsync(h->d_wmax, 0, sizeof(int), h->stream), "clear wmax");
@@ -272,12 +277,24 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
     if (rc) return rc;
     const bool split = h->overlap && h->nseg > 0 && h->env_w > 0 && h->env_h > 0;
     if (split) CK(cudaEventRecord(h->ev_inner, h->stream), "event");
+    // factorization of step `step` into slot step & 1. With the split it runs
+    // on the factor stream once the slot's previous user (the flow chain two
+    // steps back) is done; otherwise in order on the main stream.
+    auto factor = [&](int step, cudaStream_t st) -> int {
+        const int q = step & 1;
+        if (split) CK(cudaStreamWaitEvent(h->fstream, h->ev_spread[q], 0), "wait");
+        if (launch_factor(h, step, q, split ? h->fstream : st)) return cuda_err(h, cudaGetLastError(), "launch factor");
+        if (split) CK(cudaEventRecord(h->ev_factor[q], h->fstream), "event");
+        h->factored[q] = step;
+        return LBM_OK;
+    };
+    const double dt_time = h->p.scale * h->p.uu;
     int done = 0, pending = 0;
     rc = LBM_OK;
     for (int s = 0; s < nsteps; ++s) {
-        const double time = (double)(h->n - 1) * (h->p.scale * h->p.uu);   // main.f90:352
+        const double time = (double)(h->n - 1) * dt_time;   // main.f90:352
         if (time > h->mend + 1.0e-12) { rc = LBM_DONE; break; }
-        const int slot = pending;
+        const int slot = pending, q = h->n & 1;
         const void *fin = h->fbuf[h->cur];
         void *fout = h->fbuf[h->cur ^ 1];
         void *fields = nullptr;
@@ -290,11 +307,16 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
         }
         cudaEvent_t *e = h->timing ? &h->ev[4 * slot] : nullptr;
         if (split) {
+            if (h->factored[q] != h->n && (rc = factor(h->n, h->stream))) return rc;
             CK(cudaStreamWaitEvent(h->side, h->ev_inner, 0), "wait");
+            CK(cudaStreamWaitEvent(h->side, h->ev_factor[q], 0), "wait");
             if (e) CK(cudaEventRecord(h->ev_side[2 * slot], h->side), "event");
-            if (launch_ib(h, fin, h->n, slot, h->side)) return cuda_err(h, cudaGetLastError(), "launch ib");
+            if (launch_flow(h, fin, h->n, slot, q, h->side)) return cuda_err(h, cudaGetLastError(), "launch ib");
             if (e) CK(cudaEventRecord(h->ev_side[2 * slot + 1], h->side), "event");
             CK(cudaEventRecord(h->ev_ib, h->side), "event");
+            CK(cudaEventRecord(h->ev_spread[q], h->side), "event");
+            // the next step's factorization, overlapping this step
+            if ((double)h->n * dt_time <= h->mend + 1.0e-12 && (rc = factor(h->n + 1, h->stream))) return rc;
             if (e) CK(cudaEventRecord(e[0], h->stream), "event");
             if (launch_kf(h, fin, fout, fields, KF_OUTER)) return cuda_err(h, cudaGetLastError(), "launch kf");
             if (e) CK(cudaEventRecord(e[1], h->stream), "event");
@@ -305,7 +327,8 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             CK(cudaEventRecord(h->ev_inner, h->stream), "event");
         } else {
             if (e) CK(cudaEventRecord(e[0], h->stream), "event");
-            if (launch_ib(h, fin, h->n, slot)) return cuda_err(h, cudaGetLastError(), "launch ib");
+            if (h->nseg > 0 && h->factored[q] != h->n && (rc = factor(h->n, h->stream))) return rc;
+            if (launch_flow(h, fin, h->n, slot, q, h->stream)) return cuda_err(h, cudaGetLastError(), "launch ib");
             if (e) {
                 CK(cudaEventRecord(e[1], h->stream), "event");
                 CK(cudaEventRecord(e[2], h->stream), "event");
@@ -425,6 +448,11 @@ int lbm_create(const lbm_params *p, lbm_t **out)
     if ((e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "side stream");
     if ((e = cudaEventCreateWithFlags(&h->ev_ib, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
     if ((e = cudaEventCreateWithFlags(&h->ev_inner, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+    if ((e = cudaStreamCreateWithFlags(&h->fstream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "factor stream");
+    for (int q = 0; q < 2; ++q) {
+        if ((e = cudaEventCreateWithFlags(&h->ev_factor[q], cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+        if ((e = cudaEventCreateWithFlags(&h->ev_spread[q], cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+    }
     if (const char *ov = getenv("LBM_OVERLAP")) h->overlap = atoi(ov) != 0;
     // population buffers carry LBM_FPAD elements of padding before and after
     // the 9 planes, so the bulk row copies of the lattice kernel (which read a
@@ -473,10 +501,16 @@ int lbm_destroy(lbm_t *h)
     free_devp(h->d_ring); free_devp(h->d_status); free_devp(h->d_solve_res); free_devp(h->d_red);
     free_devp(h->d_stage);
     if (h->side) cudaStreamSynchronize(h->side);
+    if (h->fstream) cudaStreamSynchronize(h->fstream);
     for (auto &e : h->ev) cudaEventDestroy(e);
     for (auto &e : h->ev_side) cudaEventDestroy(e);
     if (h->ev_ib) cudaEventDestroy(h->ev_ib);
     if (h->ev_inner) cudaEventDestroy(h->ev_inner);
+    for (int q = 0; q < 2; ++q) {
+        if (h->ev_factor[q]) cudaEventDestroy(h->ev_factor[q]);
+        if (h->ev_spread[q]) cudaEventDestroy(h->ev_spread[q]);
+    }
+    if (h->fstream) cudaStreamDestroy(h->fstream);
     if (h->side) cudaStreamDestroy(h->side);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -709,7 +743,8 @@ int lbm_get_markers(lbm_t *h, double *xb2, double *yb2, double *solve_residual, 
     if (!h) return LBM_ERR_ARG;
     if (!h->ib_ready || h->nseg == 0) return set_err(h, LBM_ERR_STATE, "get_markers: no immersed boundary step run");
     std::vector<Marker> mk(h->nseg);
-    CK(cudaMemcpyAsync(mk.data(), h->d_mk, sizeof(Marker) * h->nseg, cudaMemcpyDeviceToHost, h->stream), "copy markers");
+    const Marker *last = h->d_mk + (size_t)((h->n - 1) & 1) * h->nseg;   // slot of the last step
+    CK(cudaMemcpyAsync(mk.data(), last, sizeof(Marker) * h->nseg, cudaMemcpyDeviceToHost, h->stream), "copy markers");
     double res[2] = {0, 0};
     CK(cudaMemcpyAsync(res, h->d_solve_res, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "copy res");
     CK(cudaStreamSynchronize(h->stream), "sync markers");

@@ -56,16 +56,20 @@ struct IBArgs {
     const double *mstep;  // step table, row-major [msteps][mcols]
     int msteps, mcols;
     double mdt;
-    Marker *mk;
+    // buffers of one slot (the step whose factorization they hold)
+    Marker *mk;         // [nseg] marker geometry
+    int *perm;          // solve order: sorted position -> marker
+    double *key;        // sort key of each sorted position
+    double *gf;         // factor blocks [D^-1 | F_L | F_U] of the cyclic reduction
+    double *B;          // [nseg*nseg] dense Cholesky factor (fallback), row-major
+    int *fmode;         // [2]: 1 if the dense factor is used, half-bandwidth
+    unsigned *fstatus;  // errors of the factorization chain of the slot's step
+    // per step
     double *rhs;        // [2*nseg]
-    double *B;          // [nseg*nseg], row-major
     double *y;          // [2*nseg]
-    double *bD, *bL, *bF, *bX;  // block cyclic reduction scratch (diagonal, lower,
-                                // eliminated-block factors, right-hand sides)
-    int *perm;                  // solve order: sorted position -> marker
-    double *key;                // sort key of each sorted position
-    double *reach;              // key distance beyond which boxes cannot overlap
-    int *wmax;                  // half-bandwidth found by the assembly
+    double *bD, *bL;    // working diagonal and coupling blocks of the reduction
+    double *reach;      // key distance beyond which boxes cannot overlap
+    int *wmax;          // half-bandwidth found by the assembly
     PatchInfo *pinfo;
     void *patch;        // compute-precision (du, dv) pairs
     int patch_cap;      // nodes
@@ -107,11 +111,20 @@ struct lbm_handle {
     int msteps = 0;
     std::vector<double> mstep_host;  // step table, row-major [msteps][mcols]
     double *d_mstep = nullptr;
-    // immersed boundary scratch
-    Marker *d_mk = nullptr;
-    double *d_rhs = nullptr, *d_B = nullptr, *d_y = nullptr;
-    double *d_bD = nullptr, *d_bL = nullptr, *d_bF = nullptr, *d_bX = nullptr;
-    int *d_perm = nullptr, *d_wmax = nullptr;
+    // immersed boundary scratch. The factorization of a step depends on its
+    // index only (prescribed motion); slot (step & 1) holds it, so that the
+    // factorization of the next step can run while the current step uses
+    // the other slot.
+    Marker *d_mk = nullptr;                         // 2 slots
+    double *d_gf = nullptr;                         // 2 slots of gf_slot doubles
+    size_t gf_slot = 0;
+    double *d_B = nullptr;                          // 2 slots of nseg*nseg
+    int *d_fmode = nullptr;                         // 2 slots of 2
+    unsigned *d_fstatus = nullptr;                  // 2 slots
+    int factored[2] = {-1, -1};                     // step index held by each slot
+    double *d_rhs = nullptr, *d_y = nullptr;
+    double *d_bD = nullptr, *d_bL = nullptr;
+    int *d_perm = nullptr, *d_wmax = nullptr;       // perm/key: 2 slots unless static_order
     double *d_key = nullptr, *d_reach = nullptr;
     int static_order = 0;   // one rigid body: fixed body-frame marker order
     PatchInfo *d_pinfo = nullptr;
@@ -129,6 +142,11 @@ struct lbm_handle {
     int env_x0 = 0, env_y0 = 0, env_w = 0, env_h = 0;
     cudaStream_t side = nullptr;
     cudaEvent_t ev_ib = nullptr, ev_inner = nullptr;
+    // factorization chain one step ahead (with the split): its own stream;
+    // ev_factor[s] marks the slot's factorization done, ev_spread[s] the last
+    // use of the slot by a step's flow chain
+    cudaStream_t fstream = nullptr;
+    cudaEvent_t ev_factor[2] = {nullptr, nullptr}, ev_spread[2] = {nullptr, nullptr};
     double *d_partial = nullptr;
     unsigned *d_counter = nullptr;
     double *d_ring = nullptr;
@@ -161,9 +179,10 @@ struct lbm_handle {
 int ib_configure(lbm_handle *h);
 int ib_max_markers();
 int ib_partials_per_block();
-size_t ib_block_scratch(int nseg, size_t *d, size_t *l, size_t *f, size_t *x);
+void ib_factor_scratch(int nseg, size_t *work_blocks, size_t *factor_slot);
 int launch_kf(lbm_handle *h, const void *fin, void *fout, void *fields, int mode = KF_ALL, cudaStream_t st = nullptr);
-int launch_ib(lbm_handle *h, const void *fin, int step_index, int ring_slot, cudaStream_t st = nullptr);
+int launch_factor(lbm_handle *h, int step_index, int slot, cudaStream_t st);
+int launch_flow(lbm_handle *h, const void *fin, int step_index, int ring_slot, int slot, cudaStream_t st);
 int launch_residual(lbm_handle *h, const void *fa, const void *fb, double *out2);
 int launch_unpack(lbm_handle *h, const void *fsrc, double *dst);   // deviation -> f (FP64)
 int launch_pack(lbm_handle *h, const double *src, void *fdst);     // f (FP64) -> deviation
