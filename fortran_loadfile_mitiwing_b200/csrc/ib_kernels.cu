@@ -25,18 +25,19 @@
 //               apart per axis), so the CTA builds its diagonal block and the
 //               block coupling it to the previous one, and checks that no
 //               coupling reaches further;
-//   ib_factor   one CTA: block cyclic reduction of the block tridiagonal
-//               matrix (log2 of the block count levels of Gauss-Jordan block
-//               inverses and block products, FP64), keeping per eliminated
-//               block D^-1 and the two coupling factors; a dense Cholesky
-//               replaces it when a coupling reaches past the neighbouring block.
+//   ib_factor   one CTA: correction-patch rectangle, then block cyclic
+//               reduction of the block tridiagonal matrix (log2 of the block
+//               count levels of Gauss-Jordan block inverses and block
+//               products, FP64), keeping per eliminated block D^-1 and the two
+//               coupling factors; a dense Cholesky replaces it when a coupling
+//               reaches past the neighbouring block.
 // The flow chain of the step:
 //   ib_interp   one warp per marker: b = D u* over the support box and
 //               rhs = U_b - b (:1609-1629);
-//   ib_solve    one CTA: correction-patch rectangle, force-row header, the
-//               forward and backward sweeps of the reduction over the two
-//               right-hand sides (or the two triangular solves of the dense
-//               factor);
+//   ib_solve    one CTA: the forward and backward sweeps of the reduction
+//               over the two right-hand sides, each level's factor blocks
+//               staged in shared memory by bulk copies (or the two triangular
+//               solves of the dense factor), and the force row's header;
 //   ib_spread   du = D^T y per node, gathered in marker order over the
 //               markers whose box covers the node (no atomics), written to the
 //               correction patch the lattice kernel reads; force and moment
@@ -53,7 +54,8 @@ constexpr int BS = 16;                 // block size of the cyclic reduction
 constexpr int NMARK_MAX = 2048;        // largest marker count
 constexpr int FACTOR_THREADS = 512;
 constexpr int BOPS_WARPS = FACTOR_THREADS / 32;   // warps running block operations
-constexpr int SOLVE_THREADS = 512;
+constexpr int SOLVE_THREADS = 1024;
+constexpr int STAGE_BLOCKS = 32;       // factor blocks of one level staged in shared memory by ib_solve
 constexpr int FL = 2 * BS;             // columns of a coupling panel [L_o | L_q^T]
 constexpr int GW = 3 * BS;             // row width of a stored factor block [D^-1 | F_L | F_U]
 constexpr int GP = BS + 1;             // padded row stride of square blocks in shared memory
@@ -109,6 +111,27 @@ __device__ __forceinline__ const double *motion_row(const IBArgs &a, int step_in
     idx = idx < 1 ? 1 : (idx > a.msteps ? a.msteps : idx);
     if (time_out) *time_out = time;
     return a.mstep + (long long)(idx - 1) * a.mcols;
+}
+
+// Arguments of one member of a batched factorization launch: the step
+// step0 + blockIdx.y, its buffer slot (step modulo the slot count) and the
+// member's working set.
+__device__ __forceinline__ IBArgs member_args(IBArgs a, int step)
+{
+    const int slot = step % a.nslots, mem = blockIdx.y;
+    a.mk += slot * a.st_mk;
+    a.perm += slot * a.st_perm;
+    a.key += slot * a.st_perm;
+    a.B += slot * a.st_B;
+    a.gf += slot * a.wk_gf;
+    a.pinfo += slot;
+    a.fmode += 2 * slot;
+    a.fstatus += slot;
+    a.status = a.fstatus;   // errors of the chain are reported by the step that uses it
+    a.bD += mem * a.wk_blocks;
+    a.bL += mem * a.wk_blocks;
+    a.wmax += mem;
+    return a;
 }
 
 // marker geometry of segment k (airfoil.f90:255-335, boundary_condition.f90:1540-1606)
@@ -172,8 +195,10 @@ __device__ Marker make_marker(const IBArgs &a, const double *row, int k)
 
 
 // one thread per marker: geometry of this step (errors go to the slot's status)
-__global__ void __launch_bounds__(128) ib_geometry(const IBArgs a, int step_index)
+__global__ void __launch_bounds__(128) ib_geometry(const IBArgs base, int step0)
 {
+    const int step_index = step0 + blockIdx.y;
+    const IBArgs a = member_args(base, step_index);
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.nseg) return;
     const double *row = motion_row(a, step_index, nullptr);
@@ -248,8 +273,9 @@ __device__ void write_header(const IBArgs &a, const double *row, double time, in
 // Several bodies: sort the markers along the longer axis of the marker cloud
 // (stable, ties by index) into perm/key, with reach = 6 lattice units along
 // that axis. One CTA; dynamic shared memory key[ns] (double) + idx[ns] (int).
-__global__ void __launch_bounds__(1024) ib_order(const IBArgs a)
+__global__ void __launch_bounds__(1024) ib_order(const IBArgs base, int step0)
 {
+    const IBArgs a = member_args(base, step0 + blockIdx.y);
     extern __shared__ double osm[];
     const int n = a.nseg, tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     int ns = 1;
@@ -311,8 +337,9 @@ __global__ void __launch_bounds__(1024) ib_order(const IBArgs a)
 // One CTA per block of BS markers in the solve order: the diagonal block D_b,
 // the coupling L_b to block b-1, and the longest coupling in the order
 // (half-bandwidth).
-__global__ void __launch_bounds__(256) ib_assemble(const IBArgs a)
+__global__ void __launch_bounds__(256) ib_assemble(const IBArgs base, int step0)
 {
+    const IBArgs a = member_args(base, step0 + blockIdx.y);
     const int n = a.nseg, blk = blockIdx.x, tid = threadIdx.x;
     __shared__ double ph[2 * BS][12];
     __shared__ int4 bx[2 * BS];
@@ -532,12 +559,41 @@ __device__ void dense_tri(const IBArgs &a, double *yv)
 // F_U = D_o^-1 L_q^T (coupling to q = o + st); block 0, the last one left,
 // keeps D_0^-1. The even neighbours are updated as
 //   D_e -= L_q^T F_L(q) + L_e F_U(p),   L_e <- -L_e F_L(p)   (p = e - st, q = e + st).
-__global__ void __launch_bounds__(FACTOR_THREADS) ib_factor(const IBArgs a)
+__global__ void __launch_bounds__(FACTOR_THREADS) ib_factor(const IBArgs base, int step0)
 {
+    const IBArgs a = member_args(base, step0 + blockIdx.y);
     extern __shared__ __align__(16) double Wbase[];
     const int n = a.nseg, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     __shared__ int bad, dense;
+    __shared__ int bb[4];
+    if (tid == 0) { bb[0] = 1 << 30; bb[1] = 1 << 30; bb[2] = -1; bb[3] = -1; }
+    __syncthreads();
+    // patch rectangle of the step: bounding box of all support boxes
+    {
+        int b0 = 1 << 30, b1 = 1 << 30, b2 = -1, b3 = -1;
+        for (int k = tid; k < n; k += blockDim.x) {
+            const int4 q = mbox(a.mk[k]);
+            if (q.y >= q.x && q.w >= q.z) { b0 = min(b0, q.x); b1 = min(b1, q.z); b2 = max(b2, q.y); b3 = max(b3, q.w); }
+        }
+        for (int off = 16; off; off >>= 1) {
+            b0 = min(b0, __shfl_xor_sync(0xffffffffu, b0, off));
+            b1 = min(b1, __shfl_xor_sync(0xffffffffu, b1, off));
+            b2 = max(b2, __shfl_xor_sync(0xffffffffu, b2, off));
+            b3 = max(b3, __shfl_xor_sync(0xffffffffu, b3, off));
+        }
+        if (lane == 0) { atomicMin(&bb[0], b0); atomicMin(&bb[1], b1); atomicMax(&bb[2], b2); atomicMax(&bb[3], b3); }
+    }
+    __syncthreads();
     if (tid == 0) {
+        PatchInfo pi{0, 0, 0, 0};
+        if (bb[2] >= bb[0]) {
+            pi.i0 = bb[0]; pi.j0 = bb[1]; pi.w = bb[2] - bb[0] + 1; pi.h = bb[3] - bb[1] + 1;
+            if ((long long)pi.w * pi.h > a.patch_cap || pi.w > a.patch_wmax || pi.h > a.patch_hmax) {
+                atomicOr(a.status, LBM_ST_OVERFLOW);
+                pi = PatchInfo{0, 0, 0, 0};
+            }
+        }
+        *a.pinfo = pi;
         const int w = *a.wmax;
         bad = 0;
         dense = (w > BS || a.force_dense) ? 1 : 0;
@@ -669,55 +725,43 @@ __global__ void __launch_bounds__(FACTOR_THREADS) ib_factor(const IBArgs a)
     if (tid == 0 && bad) atomicOr(a.status, LBM_ST_SOLVER);
 }
 
-// The flow-dependent solve of one step, one CTA of SOLVE_THREADS threads;
-// dynamic shared memory: the right-hand sides in the solve order, two values
-// per marker, padded to whole blocks.
+// The flow-dependent solve of one step, one CTA of SOLVE_THREADS threads,
+// with the cyclic-reduction factors of the step's slot:
 //   forward, st = 1, 2, 4, ...:  r_e -= F_L(q)^T r_q + F_U(p)^T r_p  (even e)
 //   block 0:                     x_0 = D_0^-1 r_0
 //   backward, st = ..., 2, 1:    x_o = D_o^-1 r_o - F_L(o) x_p - F_U(o) x_q  (odd o)
 // (F_L(q)^T = L_q^T D_q^-1 and F_U(p)^T = L_e D_p^-1 since D is symmetric.)
+// Each level reads the factor blocks of that level's odd blocks; when they
+// fit (at most STAGE_BLOCKS), one thread brings them into shared memory with
+// bulk copies (6 KB per block, completion on an mbarrier) before the level's
+// arithmetic, so that the level costs one memory round trip instead of one
+// per dependent load. Also writes the force row's header and reports the
+// errors of the factorization chain. Dynamic shared memory: the staged
+// blocks, then the right-hand sides in the solve order (two per marker,
+// padded to whole blocks), then the mbarrier.
 __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int step_index, int ring_slot)
 {
-    extern __shared__ __align__(16) double X[];
+    extern __shared__ __align__(128) double smem[];
     const int n = a.nseg, tid = threadIdx.x, nt = blockDim.x;
     const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
-    __shared__ int bb[4];
-    if (tid == 0) { bb[0] = 1 << 30; bb[1] = 1 << 30; bb[2] = -1; bb[3] = -1; }
-    __syncthreads();
-    // patch rectangle: bounding box of all support boxes
-    int b0 = 1 << 30, b1 = 1 << 30, b2 = -1, b3 = -1;
-    for (int k = tid; k < n; k += nt) {
-        const int4 q = mbox(a.mk[k]);
-        if (q.y >= q.x && q.w >= q.z) { b0 = min(b0, q.x); b1 = min(b1, q.z); b2 = max(b2, q.y); b3 = max(b3, q.w); }
-    }
-    for (int off = 16; off; off >>= 1) {
-        b0 = min(b0, __shfl_xor_sync(0xffffffffu, b0, off));
-        b1 = min(b1, __shfl_xor_sync(0xffffffffu, b1, off));
-        b2 = max(b2, __shfl_xor_sync(0xffffffffu, b2, off));
-        b3 = max(b3, __shfl_xor_sync(0xffffffffu, b3, off));
-    }
-    if (lane == 0) { atomicMin(&bb[0], b0); atomicMin(&bb[1], b1); atomicMax(&bb[2], b2); atomicMax(&bb[3], b3); }
-    __syncthreads();
+    const int nb = (n + BS - 1) / BS;
+    double *stage_buf = smem;
+    double *X = smem + STAGE_BLOCKS * BS * GW;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(X + 2 * nb * BS);
+    __shared__ int timed_out;
     if (tid == 0) {
         double time;
         const double *row = motion_row(a, step_index, &time);
         write_header(a, row, time, ring_slot);
-        // errors of this step's factorization chain
         const unsigned fs = *a.fstatus;
         if (fs) { atomicOr(a.status, fs); *a.fstatus = 0u; }
-        PatchInfo pi{0, 0, 0, 0};
-        if (bb[2] >= bb[0]) {
-            pi.i0 = bb[0]; pi.j0 = bb[1]; pi.w = bb[2] - bb[0] + 1; pi.h = bb[3] - bb[1] + 1;
-            if ((long long)pi.w * pi.h > a.patch_cap || pi.w > a.patch_wmax || pi.h > a.patch_hmax) {
-                atomicOr(a.status, LBM_ST_OVERFLOW);
-                pi = PatchInfo{0, 0, 0, 0};
-            }
-        }
-        *a.pinfo = pi;
         a.solve_res[1] = (double)a.fmode[1];
+        timed_out = 0;
+        mbar_init(bar, 1);
+        mbar_init_fence();
     }
+    __syncthreads();
     if (n == 0) return;
-    const int nb = (n + BS - 1) / BS;
     if (a.fmode[0]) {   // dense factor
         for (int s = tid; s < n; s += nt) {
             X[s] = a.rhs[a.perm[s]];
@@ -735,23 +779,51 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
         X[2 * s] = s < n ? a.rhs[a.perm[s]] : 0.0;
         X[2 * s + 1] = s < n ? a.rhs[n + a.perm[s]] : 0.0;
     }
-    __syncthreads();
     const double *Gf = a.gf;
+    uint32_t parity = 0;
+    // factor blocks of the odd blocks of level st: staged (returns the base
+    // of block o at index (o/st - 1)/2), or read from global memory
+    auto stage_level = [&](int st) -> bool {
+        const int nodd = (nb - st + 2 * st - 1) / (2 * st);
+        if (nodd > STAGE_BLOCKS) return false;
+        __syncthreads();   // previous readers of the stage buffer are done
+        if (tid == 0) {
+            fence_proxy_async();
+            constexpr uint32_t kBlockBytes = sizeof(double) * BS * GW;
+            mbar_expect_tx(bar, kBlockBytes * (uint32_t)nodd);
+            for (int m = 0; m < nodd; ++m)
+                bulk_g2s(stage_buf + m * BS * GW, Gf + (long long)st * (2 * m + 1) * BS * GW, kBlockBytes, bar);
+        }
+        // bounded wait: copies that never land are reported, not waited on forever
+        int spins = 0;
+        while (!mbar_try_wait(bar, parity)) {
+            if (++spins > (1 << 22)) { timed_out = 1; break; }
+        }
+        parity ^= 1u;
+        __syncthreads();   // every thread sees the same timed_out
+        return true;
+    };
+    auto fblock = [&](bool staged, int st, int o) -> const double * {
+        return staged ? stage_buf + ((o / st - 1) / 2) * BS * GW : Gf + (long long)o * BS * GW;
+    };
+    __syncthreads();
     const int i = lane >> 1, c = lane & 1;   // row of the block, right-hand side
     int levels = 0;
     for (int st = 1; st < nb; st <<= 1, ++levels) {
+        const bool staged = stage_level(st);
+        if (timed_out) break;
         const int neven = (nb + 2 * st - 1) / (2 * st);
         for (int m = warp; m < neven; m += nw) {
             const int e = 2 * st * m, o1 = e - st, o2 = e + st;
             double acc = 0.0;
             if (o2 < nb) {
-                const double *F = Gf + (long long)o2 * BS * GW + BS + i;      // F_L(q)[t][i]
+                const double *F = fblock(staged, st, o2) + BS + i;      // F_L(q)[t][i]
                 const double *r = X + 2 * o2 * BS + c;
 #pragma unroll
                 for (int t = 0; t < BS; ++t) acc += F[t * GW] * r[2 * t];
             }
             if (m > 0) {
-                const double *F = Gf + (long long)o1 * BS * GW + 2 * BS + i;  // F_U(p)[t][i]
+                const double *F = fblock(staged, st, o1) + 2 * BS + i;  // F_U(p)[t][i]
                 const double *r = X + 2 * o1 * BS + c;
 #pragma unroll
                 for (int t = 0; t < BS; ++t) acc += F[t * GW] * r[2 * t];
@@ -760,35 +832,48 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
         }
         __syncthreads();
     }
-    if (warp == 0) {
-        const double *G = Gf + i * GW;
-        double x = 0.0;
+    if (!timed_out) {
+        if (warp == 0) {
+            const double *G = Gf + i * GW;
+            double x = 0.0;
 #pragma unroll
-        for (int t = 0; t < BS; ++t) x += G[t] * X[2 * t + c];
-        __syncwarp();
-        X[lane] = x;
-    }
-    __syncthreads();
-    for (int lv = levels - 1; lv >= 0; --lv) {
-        const int st = 1 << lv;
-        const int nodd = (nb - st + 2 * st - 1) / (2 * st);
-        for (int m = warp; m < nodd; m += nw) {
-            const int o = st * (2 * m + 1), p = o - st, q2 = o + st;
-            const double *G = Gf + (long long)o * BS * GW + i * GW;
-            double s1 = 0.0, s2 = 0.0, s3 = 0.0;
-#pragma unroll
-            for (int t = 0; t < BS; ++t) {
-                s1 += G[t] * X[2 * (o * BS + t) + c];
-                s2 += G[BS + t] * X[2 * (p * BS + t) + c];
-            }
-            if (q2 < nb) {
-#pragma unroll
-                for (int t = 0; t < BS; ++t) s3 += G[2 * BS + t] * X[2 * (q2 * BS + t) + c];
-            }
+            for (int t = 0; t < BS; ++t) x += G[t] * X[2 * t + c];
             __syncwarp();
-            X[2 * (o * BS + i) + c] = s1 - s2 - s3;
+            X[lane] = x;
         }
         __syncthreads();
+        for (int lv = levels - 1; lv >= 0; --lv) {
+            const int st = 1 << lv;
+            const bool staged = stage_level(st);
+            if (timed_out) break;
+            const int nodd = (nb - st + 2 * st - 1) / (2 * st);
+            for (int m = warp; m < nodd; m += nw) {
+                const int o = st * (2 * m + 1), p = o - st, q2 = o + st;
+                const double *G = fblock(staged, st, o) + i * GW;
+                double s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll
+                for (int t = 0; t < BS; ++t) {
+                    s1 += G[t] * X[2 * (o * BS + t) + c];
+                    s2 += G[BS + t] * X[2 * (p * BS + t) + c];
+                }
+                if (q2 < nb) {
+#pragma unroll
+                    for (int t = 0; t < BS; ++t) s3 += G[2 * BS + t] * X[2 * (q2 * BS + t) + c];
+                }
+                __syncwarp();
+                X[2 * (o * BS + i) + c] = s1 - s2 - s3;
+            }
+            __syncthreads();
+        }
+    }
+    if (timed_out) {
+        // wait (bounded) for copies still in flight before the CTA's shared
+        // memory is released, and report
+        if (tid == 0) atomicOr(a.status, LBM_ST_TIMEOUT);
+        int spins = 0;
+        while (!mbar_try_wait(bar, parity ^ 1u) && ++spins < (1 << 22)) {
+        }
+        return;
     }
     for (int s = tid; s < n; s += nt) {
         a.y[a.perm[s]] = X[2 * s];
@@ -999,10 +1084,16 @@ size_t order_smem(int n)
 }
 
 constexpr size_t kFactorSmem = sizeof(double) * BOPS_WARPS * WS;
-constexpr size_t kSolveSmem = sizeof(double) * 2 * ((NMARK_MAX + BS - 1) / BS) * BS;
+constexpr size_t kSolveSmemMax = sizeof(double) * (STAGE_BLOCKS * BS * GW + 2 * NMARK_MAX) + 16;
+size_t solve_smem(int nseg)
+{
+    const size_t nb = (size_t)(nseg + BS - 1) / BS;
+    return sizeof(double) * (STAGE_BLOCKS * BS * GW + 2 * nb * BS) + 16;
+}
 
-// arguments of the kernels of one buffer slot (the factorization of the
-// step with parity `slot`)
+// arguments of the flow chain of the step held in buffer slot `slot`; for
+// the batched factorization kernels, the arguments of slot 0 and member 0
+// with the strides that member_args applies
 IBArgs make_args(lbm_handle *h, const void *fin, int slot)
 {
     const size_t ns = (size_t)(h->nseg > 0 ? h->nseg : 1);
@@ -1017,17 +1108,24 @@ IBArgs make_args(lbm_handle *h, const void *fin, int slot)
     a.xc = h->p.xc; a.yc = h->p.yc; a.mesh_max_scale = h->p.mesh_max_scale;
     a.xb0 = h->d_xb0; a.yb0 = h->d_yb0; a.arc = h->d_arc;
     a.mstep = h->d_mstep; a.msteps = h->msteps; a.mcols = h->mcols; a.mdt = h->mdt;
+    a.nslots = h->nslots;
+    a.st_mk = (long long)ns;
+    a.st_perm = h->static_order ? 0 : (long long)ns;
+    a.st_B = (long long)(ns * ns);
+    a.wk_blocks = (long long)h->work_blocks;
+    a.wk_gf = (long long)h->gf_slot;
     a.mk = h->d_mk + slot * ns;
-    a.perm = h->static_order ? h->d_perm : h->d_perm + slot * ns;
-    a.key = h->static_order ? h->d_key : h->d_key + slot * ns;
-    a.gf = h->d_gf + slot * h->gf_slot;
+    a.perm = h->d_perm + slot * a.st_perm;
+    a.key = h->d_key + slot * a.st_perm;
     a.B = h->d_B + slot * ns * ns;
     a.fmode = h->d_fmode + 2 * slot;
     a.fstatus = h->d_fstatus + slot;
+    a.pinfo = h->d_pinfo + slot;
+    a.gf = h->d_gf + slot * h->gf_slot;
     a.rhs = h->d_rhs; a.y = h->d_y;
     a.bD = h->d_bD; a.bL = h->d_bL;
     a.reach = h->d_reach; a.wmax = h->d_wmax;
-    a.pinfo = h->d_pinfo; a.patch = h->d_patch; a.patch_cap = h->patch_cap;
+    a.patch = h->d_patch; a.patch_cap = h->patch_cap;
     a.patch_wmax = h->patch_wmax; a.patch_hmax = h->patch_hmax;
     a.partial = h->d_partial; a.counter = h->d_counter;
     a.force_ring = h->d_ring; a.row_len = h->row_len;
@@ -1043,7 +1141,7 @@ int launch_flow_t(lbm_handle *h, const void *fin, int step_index, int ring_slot,
         ib_interp<T><<<(h->nseg + 7) / 8, 256, 0, st>>>(a);
         h->launches += 1;
     }
-    ib_solve<<<1, SOLVE_THREADS, kSolveSmem, st>>>(a, step_index, ring_slot);
+    ib_solve<<<1, SOLVE_THREADS, solve_smem(h->nseg), st>>>(a, step_index, ring_slot);
     dim3 grid(h->patch_gx(), h->patch_gy());
     ib_spread<T, C><<<grid, 256, 0, st>>>(a, step_index, ring_slot);
     h->launches += 2;
@@ -1071,7 +1169,7 @@ int ib_configure(lbm_handle *h)
     (void)h;
     if (cudaFuncSetAttribute(ib_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactorSmem) != cudaSuccess)
         return -1;
-    if (cudaFuncSetAttribute(ib_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSolveSmem) != cudaSuccess)
+    if (cudaFuncSetAttribute(ib_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSolveSmemMax) != cudaSuccess)
         return -1;
     if (cudaFuncSetAttribute(ib_order, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)order_smem(NMARK_MAX)) !=
         cudaSuccess)
@@ -1079,17 +1177,17 @@ int ib_configure(lbm_handle *h)
     return 0;
 }
 
-// factorization chain of step `step_index` into buffer slot `slot`
-int launch_factor(lbm_handle *h, int step_index, int slot, cudaStream_t st)
+// factorization chains of the `count` steps step0, step0+1, ... (each into
+// its slot), one launch per kernel with the steps along grid y
+int launch_factor(lbm_handle *h, int step0, int count, cudaStream_t st)
 {
-    if (!st) st = h->stream;
-    if (h->nseg == 0) return 0;
-    IBArgs a = make_args(h, nullptr, slot);
-    a.status = a.fstatus;   // errors of this chain are reported by the step that uses it
-    ib_geometry<<<(h->nseg + 127) / 128, 128, 0, st>>>(a, step_index);
-    if (!h->static_order) ib_order<<<1, 1024, order_smem(h->nseg), st>>>(a);
-    ib_assemble<<<(h->nseg + BS - 1) / BS, 256, 0, st>>>(a);
-    ib_factor<<<1, FACTOR_THREADS, kFactorSmem, st>>>(a);
+    if (h->nseg == 0 || count <= 0) return 0;
+    const IBArgs a = make_args(h, nullptr, 0);
+    const int nb = (h->nseg + BS - 1) / BS;
+    ib_geometry<<<dim3((h->nseg + 127) / 128, count), 128, 0, st>>>(a, step0);
+    if (!h->static_order) ib_order<<<dim3(1, count), 1024, order_smem(h->nseg), st>>>(a, step0);
+    ib_assemble<<<dim3(nb, count), 256, 0, st>>>(a, step0);
+    ib_factor<<<dim3(1, count), FACTOR_THREADS, kFactorSmem, st>>>(a, step0);
     h->launches += h->static_order ? 3 : 4;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -334,42 +334,7 @@ __global__ void __launch_bounds__(128) kf_vec(const KFArgs<C> a)
 constexpr int TW = 256;        // strip width (threads per CTA)
 constexpr int KS = 4;          // pipeline stages
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
-{
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_u32(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
-                 : "memory");
-}
-
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// mbarrier and bulk-copy helpers: lbm_common.cuh
 
 template <typename T> __host__ __device__ constexpr int tma_halo() { return 16 / (int)sizeof(T); }
 template <typename T> __host__ __device__ constexpr int tma_seg() { return TW + 2 * tma_halo<T>(); }
@@ -505,7 +470,7 @@ int launch_kf_t(lbm_handle *h, const void *fin, void *fout, void *fields, int mo
     a.col_l = ec;
     a.col_r = ec + 3 * h->ny;
     a.corner = ec + 6 * h->ny;
-    a.pinfo = h->d_pinfo;
+    a.pinfo = h->d_pinfo + h->pinfo_slot;
     a.patch = (const C *)h->d_patch;
     if (fields) {
         C *fc = (C *)fields;

@@ -120,7 +120,7 @@ void free_ib(lbm_handle *h)
     if (h->side) cudaStreamSynchronize(h->side);
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->ib_ready = 0;
-    h->factored[0] = h->factored[1] = -1;
+    h->batch_in_half[0] = h->batch_in_half[1] = -1;
     free_dev(h->d_patch);
     free_devp(h->d_mk); free_devp(h->d_rhs); free_devp(h->d_B); free_devp(h->d_y); free_devp(h->d_partial);
     free_devp(h->d_bD); free_devp(h->d_bL); free_devp(h->d_gf); free_devp(h->d_fmode); free_devp(h->d_fstatus);
@@ -176,30 +176,30 @@ int ensure_ib(lbm_handle *h)
     CK(cudaMalloc(&h->d_patch, 2 * cs * (size_t)h->patch_cap), "alloc patch");
     CK(cudaMemsetAsync(h->d_patch, 0, 2 * cs * (size_t)h->patch_cap, h->stream), "clear patch");
     const int ns = std::max(1, h->nseg);
-    CK(cudaMalloc(&h->d_mk, 2 * sizeof(Marker) * ns), "alloc markers");
+    const size_t S = (size_t)h->nslots, K = (size_t)h->fbatch;
+    CK(cudaMalloc(&h->d_mk, S * sizeof(Marker) * ns), "alloc markers");
     CK(cudaMalloc(&h->d_rhs, sizeof(double) * 2 * ns), "alloc rhs");
     CK(cudaMalloc(&h->d_y, sizeof(double) * 2 * ns), "alloc y");
-    CK(cudaMalloc(&h->d_B, 2 * sizeof(double) * (size_t)ns * ns), "alloc B");
-    size_t swork;
-    ib_factor_scratch(ns, &swork, &h->gf_slot);
-    CK(cudaMalloc(&h->d_bD, sizeof(double) * swork), "alloc block D");
-    CK(cudaMalloc(&h->d_bL, sizeof(double) * swork), "alloc block L");
-    CK(cudaMalloc(&h->d_gf, 2 * sizeof(double) * h->gf_slot), "alloc factor blocks");
-    CK(cudaMalloc(&h->d_fmode, 4 * sizeof(int)), "alloc factor mode");
-    CK(cudaMalloc(&h->d_fstatus, 2 * sizeof(unsigned)), "alloc factor status");
-    CK(cudaMemsetAsync(h->d_fmode, 0, 4 * sizeof(int), h->stream), "clear factor mode");
-    CK(cudaMemsetAsync(h->d_fstatus, 0, 2 * sizeof(unsigned), h->stream), "clear factor status");
+    CK(cudaMalloc(&h->d_B, S * sizeof(double) * (size_t)ns * ns), "alloc B");
+    ib_factor_scratch(ns, &h->work_blocks, &h->gf_slot);
+    CK(cudaMalloc(&h->d_bD, K * sizeof(double) * h->work_blocks), "alloc block D");
+    CK(cudaMalloc(&h->d_bL, K * sizeof(double) * h->work_blocks), "alloc block L");
+    CK(cudaMalloc(&h->d_gf, S * sizeof(double) * h->gf_slot), "alloc factor blocks");
+    CK(cudaMalloc(&h->d_fmode, S * 2 * sizeof(int)), "alloc factor mode");
+    CK(cudaMalloc(&h->d_fstatus, S * sizeof(unsigned)), "alloc factor status");
+    CK(cudaMemsetAsync(h->d_fmode, 0, S * 2 * sizeof(int), h->stream), "clear factor mode");
+    CK(cudaMemsetAsync(h->d_fstatus, 0, S * sizeof(unsigned), h->stream), "clear factor status");
     const int nblk = h->patch_gx() * h->patch_gy();
     CK(cudaMalloc(&h->d_partial, sizeof(double) * ib_partials_per_block() * (size_t)nblk), "alloc partials");
     // solve order of the markers: one rigid body keeps its markers sorted by
     // body-frame chordwise position for the whole run (two markers whose
     // support boxes overlap are less than 5*sqrt(2) lattice units apart in any
     // orientation); several bodies are sorted on the device every step
-    CK(cudaMalloc(&h->d_perm, 2 * sizeof(int) * ns), "alloc perm");
-    CK(cudaMalloc(&h->d_key, 2 * sizeof(double) * ns), "alloc key");
+    CK(cudaMalloc(&h->d_perm, S * sizeof(int) * ns), "alloc perm");
+    CK(cudaMalloc(&h->d_key, S * sizeof(double) * ns), "alloc key");
     CK(cudaMalloc(&h->d_reach, sizeof(double)), "alloc reach");
-    CK(cudaMalloc(&h->d_wmax, sizeof(int)), "alloc wmax");
-    CK(cudaMemsetAsync(h->d_wmax, 0, sizeof(int), h->stream), "clear wmax");
+    CK(cudaMalloc(&h->d_wmax, K * sizeof(int)), "alloc wmax");
+    CK(cudaMemsetAsync(h->d_wmax, 0, K * sizeof(int), h->stream), "clear wmax");
     h->static_order = h->nwing == 1;
     if (h->static_order) {
         std::vector<int> perm(h->nseg);
@@ -277,24 +277,33 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
     if (rc) return rc;
     const bool split = h->overlap && h->nseg > 0 && h->env_w > 0 && h->env_h > 0;
     if (split) CK(cudaEventRecord(h->ev_inner, h->stream), "event");
-    // factorization of step `step` into slot step & 1. With the split it runs
-    // on the factor stream once the slot's previous user (the flow chain two
-    // steps back) is done; otherwise in order on the main stream.
-    auto factor = [&](int step, cudaStream_t st) -> int {
-        const int q = step & 1;
-        if (split) CK(cudaStreamWaitEvent(h->fstream, h->ev_spread[q], 0), "wait");
-        if (launch_factor(h, step, q, split ? h->fstream : st)) return cuda_err(h, cudaGetLastError(), "launch factor");
-        if (split) CK(cudaEventRecord(h->ev_factor[q], h->fstream), "event");
-        h->factored[q] = step;
+    // Factorization of batch b (steps b*K .. b*K+K-1 that the motion table
+    // reaches, into slot half b & 1). With the split it runs on the factor
+    // stream once the half's previous user (the batch two back) is done;
+    // otherwise in order on the main stream.
+    const double dt_time = h->p.scale * h->p.uu;
+    const int K = h->fbatch;
+    // last step with time <= mend, plus one against rounding (factorizing a
+    // step that is never run costs nothing but time)
+    const int last_step = (int)std::floor((h->mend + 1.0e-12) / dt_time) + 2;
+    auto factor_batch = [&](int b) -> int {
+        const int half = b & 1;
+        const int s0 = std::max(1, b * K), s1 = std::min(b * K + K - 1, last_step);
+        h->batch_in_half[half] = b;
+        if (h->nseg == 0 || s1 < s0) return LBM_OK;
+        cudaStream_t st = split ? h->fstream : h->stream;
+        if (split) CK(cudaStreamWaitEvent(h->fstream, h->ev_free[half], 0), "wait");
+        if (launch_factor(h, s0, s1 - s0 + 1, st)) return cuda_err(h, cudaGetLastError(), "launch factor");
+        if (split) CK(cudaEventRecord(h->ev_batch[half], h->fstream), "event");
         return LBM_OK;
     };
-    const double dt_time = h->p.scale * h->p.uu;
     int done = 0, pending = 0;
     rc = LBM_OK;
     for (int s = 0; s < nsteps; ++s) {
         const double time = (double)(h->n - 1) * dt_time;   // main.f90:352
         if (time > h->mend + 1.0e-12) { rc = LBM_DONE; break; }
-        const int slot = pending, q = h->n & 1;
+        const int slot = pending, b = h->n / K, half = b & 1, q = h->n % h->nslots;
+        h->pinfo_slot = q;
         const void *fin = h->fbuf[h->cur];
         void *fout = h->fbuf[h->cur ^ 1];
         void *fields = nullptr;
@@ -307,16 +316,16 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
         }
         cudaEvent_t *e = h->timing ? &h->ev[4 * slot] : nullptr;
         if (split) {
-            if (h->factored[q] != h->n && (rc = factor(h->n, h->stream))) return rc;
+            if (h->batch_in_half[half] != b && (rc = factor_batch(b))) return rc;
             CK(cudaStreamWaitEvent(h->side, h->ev_inner, 0), "wait");
-            CK(cudaStreamWaitEvent(h->side, h->ev_factor[q], 0), "wait");
+            CK(cudaStreamWaitEvent(h->side, h->ev_batch[half], 0), "wait");
             if (e) CK(cudaEventRecord(h->ev_side[2 * slot], h->side), "event");
             if (launch_flow(h, fin, h->n, slot, q, h->side)) return cuda_err(h, cudaGetLastError(), "launch ib");
             if (e) CK(cudaEventRecord(h->ev_side[2 * slot + 1], h->side), "event");
             CK(cudaEventRecord(h->ev_ib, h->side), "event");
-            CK(cudaEventRecord(h->ev_spread[q], h->side), "event");
-            // the next step's factorization, overlapping this step
-            if ((double)h->n * dt_time <= h->mend + 1.0e-12 && (rc = factor(h->n + 1, h->stream))) return rc;
+            CK(cudaEventRecord(h->ev_free[half], h->side), "event");
+            // the next batch's factorization, overlapping this batch's steps
+            if ((b + 1) * K <= last_step && h->batch_in_half[half ^ 1] != b + 1 && (rc = factor_batch(b + 1))) return rc;
             if (e) CK(cudaEventRecord(e[0], h->stream), "event");
             if (launch_kf(h, fin, fout, fields, KF_OUTER)) return cuda_err(h, cudaGetLastError(), "launch kf");
             if (e) CK(cudaEventRecord(e[1], h->stream), "event");
@@ -327,7 +336,7 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             CK(cudaEventRecord(h->ev_inner, h->stream), "event");
         } else {
             if (e) CK(cudaEventRecord(e[0], h->stream), "event");
-            if (h->nseg > 0 && h->factored[q] != h->n && (rc = factor(h->n, h->stream))) return rc;
+            if (h->batch_in_half[half] != b && (rc = factor_batch(b))) return rc;
             if (launch_flow(h, fin, h->n, slot, q, h->stream)) return cuda_err(h, cudaGetLastError(), "launch ib");
             if (e) {
                 CK(cudaEventRecord(e[1], h->stream), "event");
@@ -445,15 +454,26 @@ int lbm_create(const lbm_params *p, lbm_t **out)
     };
     cudaError_t e;
     if ((e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
-    if ((e = cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "side stream");
+    // the immersed-boundary flow chain is on the step's critical path: its
+    // stream has the highest priority, so that its CTAs are placed before
+    // queued lattice CTAs as SMs free up
+    int prio_low = 0, prio_high = 0;
+    if ((e = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high)) != cudaSuccess) return fail(e, "priorities");
+    if ((e = cudaStreamCreateWithPriority(&h->side, cudaStreamNonBlocking, prio_high)) != cudaSuccess)
+        return fail(e, "side stream");
     if ((e = cudaEventCreateWithFlags(&h->ev_ib, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
     if ((e = cudaEventCreateWithFlags(&h->ev_inner, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
     if ((e = cudaStreamCreateWithFlags(&h->fstream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "factor stream");
     for (int q = 0; q < 2; ++q) {
-        if ((e = cudaEventCreateWithFlags(&h->ev_factor[q], cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
-        if ((e = cudaEventCreateWithFlags(&h->ev_spread[q], cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+        if ((e = cudaEventCreateWithFlags(&h->ev_batch[q], cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+        if ((e = cudaEventCreateWithFlags(&h->ev_free[q], cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
     }
     if (const char *ov = getenv("LBM_OVERLAP")) h->overlap = atoi(ov) != 0;
+    if (const char *fb = getenv("LBM_IB_BATCH")) {
+        const int v = atoi(fb);
+        if (v >= 1 && 2 * v <= LBM_NSLOT_MAX) h->fbatch = v;
+    }
+    h->nslots = 2 * h->fbatch;
     // population buffers carry LBM_FPAD elements of padding before and after
     // the 9 planes, so the bulk row copies of the lattice kernel (which read a
     // 16-byte halo left and right of every row segment) stay in bounds
@@ -470,14 +490,14 @@ int lbm_create(const lbm_params *p, lbm_t **out)
     if ((e = cudaMalloc(&h->edge_c, cs * (6 * (size_t)h->ny + 36))) != cudaSuccess) return fail(e, "alloc edge");
     if ((e = cudaMalloc(&h->d_status, sizeof(unsigned))) != cudaSuccess) return fail(e, "alloc status");
     if ((e = cudaMalloc(&h->d_counter, sizeof(unsigned))) != cudaSuccess) return fail(e, "alloc counter");
-    if ((e = cudaMalloc(&h->d_pinfo, sizeof(PatchInfo))) != cudaSuccess) return fail(e, "alloc pinfo");
+    if ((e = cudaMalloc(&h->d_pinfo, LBM_NSLOT_MAX * sizeof(PatchInfo))) != cudaSuccess) return fail(e, "alloc pinfo");
     if ((e = cudaMalloc(&h->d_red, sizeof(double) * 2 * 296)) != cudaSuccess) return fail(e, "alloc red");
     if ((e = cudaMalloc(&h->d_solve_res, 2 * sizeof(double))) != cudaSuccess) return fail(e, "alloc res");
     if ((e = cudaMalloc(&h->d_ring, sizeof(double) * h->row_len * (size_t)h->ring_cap)) != cudaSuccess)
         return fail(e, "alloc ring");
     cudaMemset(h->d_status, 0, sizeof(unsigned));
     cudaMemset(h->d_counter, 0, sizeof(unsigned));
-    cudaMemset(h->d_pinfo, 0, sizeof(PatchInfo));
+    cudaMemset(h->d_pinfo, 0, LBM_NSLOT_MAX * sizeof(PatchInfo));
     cudaMemset(h->d_solve_res, 0, 2 * sizeof(double));
     if (h->npts > 0) {
         if ((e = cudaMalloc(&h->d_xb0, sizeof(double) * h->npts)) != cudaSuccess) return fail(e, "alloc xb0");
@@ -507,8 +527,8 @@ int lbm_destroy(lbm_t *h)
     if (h->ev_ib) cudaEventDestroy(h->ev_ib);
     if (h->ev_inner) cudaEventDestroy(h->ev_inner);
     for (int q = 0; q < 2; ++q) {
-        if (h->ev_factor[q]) cudaEventDestroy(h->ev_factor[q]);
-        if (h->ev_spread[q]) cudaEventDestroy(h->ev_spread[q]);
+        if (h->ev_batch[q]) cudaEventDestroy(h->ev_batch[q]);
+        if (h->ev_free[q]) cudaEventDestroy(h->ev_free[q]);
     }
     if (h->fstream) cudaStreamDestroy(h->fstream);
     if (h->side) cudaStreamDestroy(h->side);
@@ -648,7 +668,7 @@ int lbm_init(lbm_t *h, const double *du, const double *dv)
     h->fields_step[0] = 0;
     h->fields_step[1] = -1;
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream), "clear status");
-    CK(cudaMemsetAsync(h->d_pinfo, 0, sizeof(PatchInfo), h->stream), "clear pinfo");
+    CK(cudaMemsetAsync(h->d_pinfo, 0, LBM_NSLOT_MAX * sizeof(PatchInfo), h->stream), "clear pinfo");
     CK(cudaStreamSynchronize(h->stream), "sync init");
     h->n = 1;
     h->steps_done = 0;
@@ -743,7 +763,7 @@ int lbm_get_markers(lbm_t *h, double *xb2, double *yb2, double *solve_residual, 
     if (!h) return LBM_ERR_ARG;
     if (!h->ib_ready || h->nseg == 0) return set_err(h, LBM_ERR_STATE, "get_markers: no immersed boundary step run");
     std::vector<Marker> mk(h->nseg);
-    const Marker *last = h->d_mk + (size_t)((h->n - 1) & 1) * h->nseg;   // slot of the last step
+    const Marker *last = h->d_mk + (size_t)((h->n - 1) % h->nslots) * h->nseg;   // slot of the last step
     CK(cudaMemcpyAsync(mk.data(), last, sizeof(Marker) * h->nseg, cudaMemcpyDeviceToHost, h->stream), "copy markers");
     double res[2] = {0, 0};
     CK(cudaMemcpyAsync(res, h->d_solve_res, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "copy res");

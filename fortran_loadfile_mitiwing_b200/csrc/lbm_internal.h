@@ -36,6 +36,7 @@ struct KFArgs {
     int rx0, ry0, rw, rh;              // split rectangle (0-based origin, extent)
 };
 
+#define LBM_NSLOT_MAX 16   // largest slot count of the factorization batches
 #define LBM_FPAD 64   // elements of padding before and after the population planes
 
 #define KF_ALL 0
@@ -70,6 +71,9 @@ struct IBArgs {
     double *bD, *bL;    // working diagonal and coupling blocks of the reduction
     double *reach;      // key distance beyond which boxes cannot overlap
     int *wmax;          // half-bandwidth found by the assembly
+    // slot and working-set strides of the batched factorization (elements)
+    int nslots;
+    long long st_mk, st_perm, st_B, wk_blocks, wk_gf;
     PatchInfo *pinfo;
     void *patch;        // compute-precision (du, dv) pairs
     int patch_cap;      // nodes
@@ -112,22 +116,25 @@ struct lbm_handle {
     std::vector<double> mstep_host;  // step table, row-major [msteps][mcols]
     double *d_mstep = nullptr;
     // immersed boundary scratch. The factorization of a step depends on its
-    // index only (prescribed motion); slot (step & 1) holds it, so that the
-    // factorization of the next step can run while the current step uses
-    // the other slot.
-    Marker *d_mk = nullptr;                         // 2 slots
-    double *d_gf = nullptr;                         // 2 slots of gf_slot doubles
-    size_t gf_slot = 0;
-    double *d_B = nullptr;                          // 2 slots of nseg*nseg
-    int *d_fmode = nullptr;                         // 2 slots of 2
-    unsigned *d_fstatus = nullptr;                  // 2 slots
-    int factored[2] = {-1, -1};                     // step index held by each slot
+    // index only (prescribed motion). Steps are factorized in batches of
+    // fbatch consecutive steps (batch b: steps b*fbatch .. b*fbatch+fbatch-1),
+    // each step into slot step % nslots (nslots = 2 fbatch): the next batch
+    // is factorized while the steps of the current one run.
+    int fbatch = 4, nslots = 8;
+    int batch_in_half[2] = {-1, -1};                // batch index held by each half of the slots
+    Marker *d_mk = nullptr;                         // nslots x nseg
+    double *d_B = nullptr;                          // nslots x nseg*nseg
+    int *d_fmode = nullptr;                         // nslots x 2
+    unsigned *d_fstatus = nullptr;                  // nslots
+    double *d_gf = nullptr;                         // nslots x gf_slot doubles
+    size_t gf_slot = 0, work_blocks = 0;
     double *d_rhs = nullptr, *d_y = nullptr;
-    double *d_bD = nullptr, *d_bL = nullptr;
-    int *d_perm = nullptr, *d_wmax = nullptr;       // perm/key: 2 slots unless static_order
+    double *d_bD = nullptr, *d_bL = nullptr;        // fbatch working sets of work_blocks doubles
+    int *d_perm = nullptr, *d_wmax = nullptr;       // perm/key: nslots unless static_order; wmax: fbatch
     double *d_key = nullptr, *d_reach = nullptr;
     int static_order = 0;   // one rigid body: fixed body-frame marker order
-    PatchInfo *d_pinfo = nullptr;
+    PatchInfo *d_pinfo = nullptr;   // LBM_NSLOT_MAX slots (patch rectangle of the slot's step)
+    int pinfo_slot = 0;             // slot the next lattice launch reads
     void *d_patch = nullptr;
     int patch_cap = 0;               // nodes
     int patch_wmax = 0, patch_hmax = 0;
@@ -142,11 +149,11 @@ struct lbm_handle {
     int env_x0 = 0, env_y0 = 0, env_w = 0, env_h = 0;
     cudaStream_t side = nullptr;
     cudaEvent_t ev_ib = nullptr, ev_inner = nullptr;
-    // factorization chain one step ahead (with the split): its own stream;
-    // ev_factor[s] marks the slot's factorization done, ev_spread[s] the last
-    // use of the slot by a step's flow chain
+    // factorization batches (with the split): their own stream; ev_batch[h]
+    // marks the batch of slot half h factorized, ev_free[h] the last use of
+    // that half by a step's flow chain
     cudaStream_t fstream = nullptr;
-    cudaEvent_t ev_factor[2] = {nullptr, nullptr}, ev_spread[2] = {nullptr, nullptr};
+    cudaEvent_t ev_batch[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
     double *d_partial = nullptr;
     unsigned *d_counter = nullptr;
     double *d_ring = nullptr;
@@ -181,7 +188,7 @@ int ib_max_markers();
 int ib_partials_per_block();
 void ib_factor_scratch(int nseg, size_t *work_blocks, size_t *factor_slot);
 int launch_kf(lbm_handle *h, const void *fin, void *fout, void *fields, int mode = KF_ALL, cudaStream_t st = nullptr);
-int launch_factor(lbm_handle *h, int step_index, int slot, cudaStream_t st);
+int launch_factor(lbm_handle *h, int step0, int count, cudaStream_t st);
 int launch_flow(lbm_handle *h, const void *fin, int step_index, int ring_slot, int slot, cudaStream_t st);
 int launch_residual(lbm_handle *h, const void *fa, const void *fb, double *out2);
 int launch_unpack(lbm_handle *h, const void *fsrc, double *dst);   // deviation -> f (FP64)
