@@ -61,6 +61,8 @@ constexpr int GW = 3 * BS;             // row width of a stored factor block [D^
 constexpr int GP = BS + 1;             // padded row stride of square blocks in shared memory
 constexpr int WS = BS * GP + BS * FL + BS * GP;   // workspace per warp (doubles)
 constexpr int NPART = 3 * LBM_MAXW + 3;           // per-CTA partials of ib_spread
+constexpr int TILE = 16;                          // correction-patch tile (nodes per side)
+constexpr int TILE_CAP = 256;                     // markers listed per tile
 
 // one-axis kernel value (boundary_condition.f90:1563-1600), disr = |r|
 __device__ __forceinline__ double delta1(double disr, int smooth)
@@ -125,6 +127,7 @@ __device__ __forceinline__ IBArgs member_args(IBArgs a, int step)
     a.B += slot * a.st_B;
     a.gf += slot * a.wk_gf;
     a.pinfo += slot;
+    a.tiles += slot * a.st_tiles;
     a.fmode += 2 * slot;
     a.fstatus += slot;
     a.status = a.fstatus;   // errors of the chain are reported by the step that uses it
@@ -210,6 +213,15 @@ template <typename T>
 __global__ void __launch_bounds__(256) ib_interp(const IBArgs a)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // bring the slot's factor blocks, which the lattice kernels have evicted
+    // since the factorization wrote them, back into L2 for ib_solve: one
+    // 128-byte line per thread
+    {
+        const long long nlines = (a.wk_gf * (long long)sizeof(double) + 127) / 128;
+        const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        for (long long l = t; l < nlines; l += (long long)gridDim.x * blockDim.x)
+            asm volatile("prefetch.global.L2 [%0];" ::"l"(reinterpret_cast<const char *>(a.gf) + 128 * l));
+    }
     const int k = blockIdx.x * 8 + warp;
     if (k >= a.nseg) return;
     const Marker m = a.mk[k];
@@ -881,6 +893,122 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
     }
 }
 
+// Markers whose support box meets each tile of the step's correction patch,
+// in increasing marker index (the order of the spread's sums), one CTA per
+// tile; geometry only, so part of the factorization chain. Layout per tile:
+// count, then up to TILE_CAP marker indices; a larger count tells the
+// spread to scan all markers for that tile.
+__global__ void __launch_bounds__(256) ib_tiles(const IBArgs base, int step0)
+{
+    const IBArgs a = member_args(base, step0 + blockIdx.y);
+    __shared__ int wsum[8];
+    __shared__ int total;
+    const PatchInfo pi = *a.pinfo;
+    const int tx = blockIdx.x % a.tiles_x, ty = blockIdx.x / a.tiles_x;
+    int *list = a.tiles + (long long)blockIdx.x * (TILE_CAP + 1);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (threadIdx.x == 0) total = 0;
+    __syncthreads();
+    const int ti0 = tx * TILE, tj0 = ty * TILE;
+    if (ti0 >= pi.w || tj0 >= pi.h) {
+        if (threadIdx.x == 0) list[0] = 0;
+        return;
+    }
+    const int ta = pi.i0 + ti0, tb = ta + TILE - 1, sa_ = pi.j0 + tj0, sb_ = sa_ + TILE - 1;
+    for (int c0 = 0; c0 < a.nseg; c0 += 256) {
+        const int k = c0 + threadIdx.x;
+        bool hit = false;
+        if (k < a.nseg) {
+            const int4 q = mbox(a.mk[k]);
+            hit = q.x <= tb && q.y >= ta && q.z <= sb_ && q.w >= sa_ && q.y >= q.x;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, hit);
+        if (lane == 0) wsum[warp] = __popc(bal);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int acc = total;
+            for (int w = 0; w < 8; ++w) { const int t = wsum[w]; wsum[w] = acc; acc += t; }
+            total = acc;
+        }
+        __syncthreads();
+        if (hit) {
+            const int slot = wsum[warp] + __popc(bal & ((1u << lane) - 1u));
+            if (slot < TILE_CAP) list[1 + slot] = k;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) list[0] = total;
+}
+
+// Residual of the step's solve, ||B y - rhs|| / ||rhs|| with B = D D^T
+// recomputed from the marker geometry (independent of the factorization):
+// one warp per row of the solve order, lanes over the couplings within the
+// half-bandwidth; deterministic two-level sum (CTA partials, last CTA).
+// Flags LBM_ST_SOLVER unless it is below 1e-6.
+__global__ void __launch_bounds__(256) ib_residual(const IBArgs a)
+{
+    __shared__ double red[8][2];
+    __shared__ bool amlast;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int n = a.nseg, s = blockIdx.x * 8 + warp;
+    const int hw = (int)a.solve_res[1];
+    double rnum = 0.0, rden = 0.0;
+    if (s < n) {
+        const int ks = a.perm[s];
+        const Marker &ms = a.mk[ks];
+        double b0 = 0.0, b1 = 0.0;
+        for (int t = s - hw + lane; t <= s + hw; t += 32) {
+            if (t < 0 || t >= n) continue;
+            const int l = a.perm[t];
+            const double b = bval(ms, a.mk[l]);
+            b0 += b * a.y[l];
+            b1 += b * a.y[n + l];
+        }
+#pragma unroll
+        for (int off = 16; off; off >>= 1) {
+            b0 += __shfl_xor_sync(0xffffffffu, b0, off);
+            b1 += __shfl_xor_sync(0xffffffffu, b1, off);
+        }
+        const double q0 = a.rhs[ks], q1 = a.rhs[n + ks];
+        rnum = (b0 - q0) * (b0 - q0) + (b1 - q1) * (b1 - q1);
+        rden = q0 * q0 + q1 * q1;
+    }
+    if (lane == 0) { red[warp][0] = rnum; red[warp][1] = rden; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t0 = 0, t1 = 0;
+        for (int w = 0; w < 8; ++w) { t0 += red[w][0]; t1 += red[w][1]; }
+        a.partial[2 * blockIdx.x] = t0;
+        a.partial[2 * blockIdx.x + 1] = t1;
+        __threadfence();
+        amlast = atomicAdd(a.counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!amlast) return;
+    __threadfence();
+    double s0 = 0.0, s1 = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+        s0 += __ldcg(a.partial + 2 * b);
+        s1 += __ldcg(a.partial + 2 * b + 1);
+    }
+#pragma unroll
+    for (int off = 16; off; off >>= 1) {
+        s0 += __shfl_down_sync(0xffffffffu, s0, off);
+        s1 += __shfl_down_sync(0xffffffffu, s1, off);
+    }
+    __syncthreads();
+    if (lane == 0) { red[warp][0] = s0; red[warp][1] = s1; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double sn = 0, sd = 0;
+        for (int w = 0; w < 8; ++w) { sn += red[w][0]; sd += red[w][1]; }
+        const double res = sqrt(sn) / (sqrt(sd) + 1e-300);
+        a.solve_res[0] = res;
+        if (!(res < 1e-6)) atomicOr(a.status, LBM_ST_SOLVER);
+        *a.counter = 0u;
+    }
+}
+
 // du = D^T y over the current patch, 16x16 nodes per CTA, plus FP64 force and
 // moment partials (boundary_condition.f90:1645-1675)
 template <typename T, typename C>
@@ -906,7 +1034,34 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
     double du = 0.0, dv = 0.0;
     int wing = 1 << 20;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (tile_active) {
+    const int *tlist = a.tiles + (long long)(blockIdx.y * gridDim.x + blockIdx.x) * (TILE_CAP + 1);
+    const int listed = tile_active ? tlist[0] : 0;
+    if (tile_active && listed <= TILE_CAP) {
+        // markers listed for this tile by the factorization chain
+        if (threadIdx.x == 0) nlist = listed;
+        if ((int)threadIdx.x < listed) {
+            const int k = tlist[1 + threadIdx.x];
+            const Marker &m = a.mk[k];
+            sbox[threadIdx.x] = mbox(m);
+#pragma unroll
+            for (int c = 0; c < 6; ++c) { sph[threadIdx.x][c] = m.phx[c]; sph[threadIdx.x][6 + c] = m.phy[c]; }
+            sy[threadIdx.x][0] = a.y[k];
+            sy[threadIdx.x][1] = a.y[a.nseg + k];
+            swing[threadIdx.x] = m.wing;
+        }
+        __syncthreads();
+        if (active) {
+            for (int t = 0; t < nlist; ++t) {
+                const int4 b = sbox[t];
+                if (gi >= b.x && gi <= b.y && gj >= b.z && gj <= b.w) {
+                    const double wgt = sph[t][gi - b.x] * sph[t][6 + gj - b.z];
+                    du += wgt * sy[t][0];
+                    dv += wgt * sy[t][1];
+                    wing = min(wing, swing[t]);
+                }
+            }
+        }
+    } else if (tile_active) {
         for (int c0 = 0; c0 < a.nseg; c0 += 256) {
             const int k = c0 + threadIdx.x;
             bool hit = false;
@@ -970,38 +1125,7 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
         const double y0 = (a.oy + a.scale * (double)gj - (a.yc + sb)) / a.scale;
         mz = -x0 * temp2 + y0 * temp1;
     }
-    // residual rows of the marker system, (B y - rhs)_s: one warp per row,
-    // lanes over the couplings within the half-bandwidth of this step
-    double rnum = 0.0, rden = 0.0;
-    {
-        const int nblk0 = gridDim.x * gridDim.y, bid0 = blockIdx.y * gridDim.x + blockIdx.x;
-        const int n = a.nseg;
-        const int hw = n > 0 ? (int)a.solve_res[1] : 0;
-        for (int s = bid0 * 8 + warp; s < n; s += nblk0 * 8) {
-            const int ks = a.perm[s];
-            const Marker &ms = a.mk[ks];
-            double b0 = 0.0, b1 = 0.0;
-            for (int t = s - hw + lane; t <= s + hw; t += 32) {
-                if (t < 0 || t >= n) continue;
-                const int l = a.perm[t];
-                const double b = bval(ms, a.mk[l]);
-                b0 += b * a.y[l];
-                b1 += b * a.y[n + l];
-            }
-#pragma unroll
-            for (int off = 16; off; off >>= 1) {
-                b0 += __shfl_xor_sync(0xffffffffu, b0, off);
-                b1 += __shfl_xor_sync(0xffffffffu, b1, off);
-            }
-            if (lane == 0) {
-                const double q0 = a.rhs[ks], q1 = a.rhs[n + ks];
-                rnum += (b0 - q0) * (b0 - q0) + (b1 - q1) * (b1 - q1);
-                rden += q0 * q0 + q1 * q1;
-            }
-        }
-    }
     // deterministic block reduction per wing
-    if (lane == 0) { red[warp][3 * LBM_MAXW] = rnum; red[warp][3 * LBM_MAXW + 1] = rden; }
     for (int w = 0; w < a.nwing; ++w) {
         double v0 = (in_support && wing == w) ? fx : 0.0;
         double v1 = (in_support && wing == w) ? fy : 0.0;
@@ -1016,7 +1140,7 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
     }
     __syncthreads();
     const int nblk = gridDim.x * gridDim.y, bid = blockIdx.y * gridDim.x + blockIdx.x;
-    if (threadIdx.x < 3 * a.nwing || threadIdx.x == 3 * LBM_MAXW || threadIdx.x == 3 * LBM_MAXW + 1) {
+    if (threadIdx.x < 3 * a.nwing) {
         double s = 0.0;
         for (int w8 = 0; w8 < 8; ++w8) s += red[w8][threadIdx.x];
         a.partial[(long long)bid * NPART + threadIdx.x] = s;
@@ -1029,14 +1153,11 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
     __threadfence();
     // last block: every thread sums a fixed strided subset of the block
     // partials, then a fixed warp/block tree (deterministic order)
-    for (int w = 0; w <= a.nwing; ++w) {
-        // w < nwing: force and moment of wing w; w == nwing: residual sums
-        const int off0 = w < a.nwing ? 3 * w : 3 * LBM_MAXW;
+    for (int w = 0; w < a.nwing; ++w) {
         double s0 = 0, s1 = 0, s2 = 0;
         for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
-            const double *p = a.partial + (long long)b * NPART + off0;
-            s0 += __ldcg(p); s1 += __ldcg(p + 1);
-            if (w < a.nwing) s2 += __ldcg(p + 2);
+            const double *p = a.partial + (long long)b * NPART + 3 * w;
+            s0 += __ldcg(p); s1 += __ldcg(p + 1); s2 += __ldcg(p + 2);
         }
 #pragma unroll
         for (int off = 16; off; off >>= 1) {
@@ -1065,12 +1186,6 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
         fr[1 + 3 * a.nwing] = tot[0];
         fr[2 + 3 * a.nwing] = tot[1];
         fr[3 + 3 * a.nwing] = tot[2];
-        // solve residual ||B y - rhs|| / ||rhs|| (FP64 solve: ~1e-14)
-        double sn = 0, sd = 0;
-        for (int w8 = 0; w8 < 8; ++w8) { sn += red[w8][3 * a.nwing]; sd += red[w8][3 * a.nwing + 1]; }
-        const double res = sqrt(sn) / (sqrt(sd) + 1e-300);
-        a.solve_res[0] = res;
-        if (a.nseg > 0 && !(res < 1e-6)) atomicOr(a.status, LBM_ST_SOLVER);
         *a.counter = 0u;
     }
 }
@@ -1121,6 +1236,9 @@ IBArgs make_args(lbm_handle *h, const void *fin, int slot)
     a.fmode = h->d_fmode + 2 * slot;
     a.fstatus = h->d_fstatus + slot;
     a.pinfo = h->d_pinfo + slot;
+    a.tiles_x = h->patch_gx();
+    a.st_tiles = (long long)h->patch_gx() * h->patch_gy() * (TILE_CAP + 1);
+    a.tiles = h->d_tiles + slot * a.st_tiles;
     a.gf = h->d_gf + slot * h->gf_slot;
     a.rhs = h->d_rhs; a.y = h->d_y;
     a.bD = h->d_bD; a.bL = h->d_bL;
@@ -1148,10 +1266,24 @@ int launch_flow_t(lbm_handle *h, const void *fin, int step_index, int ring_slot,
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
+// the residual check of the step's solve (needed by no later kernel of the step)
+template <typename T, typename C>
+int launch_check_t(lbm_handle *h, int slot, cudaStream_t st)
+{
+    if (h->nseg == 0) return 0;
+    IBArgs a = make_args(h, nullptr, slot);
+    ib_residual<<<(h->nseg + 7) / 8, 256, 0, st>>>(a);
+    h->launches += 1;
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
 }  // namespace
 
 // per-CTA partials of ib_spread (doubles)
 int ib_partials_per_block() { return NPART; }
+
+// ints per patch tile of the tile lists (count + TILE_CAP indices)
+int ib_tile_ints() { return TILE_CAP + 1; }
 
 // scratch of the block cyclic reduction (doubles): working diagonal and
 // coupling blocks (one set), and the factor buffer of one slot
@@ -1188,8 +1320,15 @@ int launch_factor(lbm_handle *h, int step0, int count, cudaStream_t st)
     if (!h->static_order) ib_order<<<dim3(1, count), 1024, order_smem(h->nseg), st>>>(a, step0);
     ib_assemble<<<dim3(nb, count), 256, 0, st>>>(a, step0);
     ib_factor<<<dim3(1, count), FACTOR_THREADS, kFactorSmem, st>>>(a, step0);
-    h->launches += h->static_order ? 3 : 4;
+    ib_tiles<<<dim3(h->patch_gx() * h->patch_gy(), count), 256, 0, st>>>(a, step0);
+    h->launches += h->static_order ? 4 : 5;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+// residual check of the step held in `slot`, after its flow chain
+int launch_check(lbm_handle *h, int slot, cudaStream_t st)
+{
+    return launch_check_t<float, float>(h, slot, st ? st : h->stream);
 }
 
 // flow chain of step `step_index`: interpolation, solve with the factor of

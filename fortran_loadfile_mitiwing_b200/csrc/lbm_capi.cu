@@ -123,7 +123,7 @@ void free_ib(lbm_handle *h)
     h->batch_in_half[0] = h->batch_in_half[1] = -1;
     free_dev(h->d_patch);
     free_devp(h->d_mk); free_devp(h->d_rhs); free_devp(h->d_B); free_devp(h->d_y); free_devp(h->d_partial);
-    free_devp(h->d_bD); free_devp(h->d_bL); free_devp(h->d_gf); free_devp(h->d_fmode); free_devp(h->d_fstatus);
+    free_devp(h->d_bD); free_devp(h->d_bL); free_devp(h->d_gf); free_devp(h->d_fmode); free_devp(h->d_fstatus); free_devp(h->d_tiles);
     free_devp(h->d_perm); free_devp(h->d_key); free_devp(h->d_reach); free_devp(h->d_wmax);
 }
 
@@ -190,7 +190,10 @@ int ensure_ib(lbm_handle *h)
     CK(cudaMemsetAsync(h->d_fmode, 0, S * 2 * sizeof(int), h->stream), "clear factor mode");
     CK(cudaMemsetAsync(h->d_fstatus, 0, S * sizeof(unsigned), h->stream), "clear factor status");
     const int nblk = h->patch_gx() * h->patch_gy();
-    CK(cudaMalloc(&h->d_partial, sizeof(double) * ib_partials_per_block() * (size_t)nblk), "alloc partials");
+    // partials of the spread (per patch tile) and of the residual check (per 8 markers)
+    const size_t npart = std::max((size_t)ib_partials_per_block() * nblk, 2 * (size_t)((ns + 7) / 8));
+    CK(cudaMalloc(&h->d_partial, sizeof(double) * npart), "alloc partials");
+    CK(cudaMalloc(&h->d_tiles, S * sizeof(int) * ib_tile_ints() * (size_t)nblk), "alloc tile lists");
     // solve order of the markers: one rigid body keeps its markers sorted by
     // body-frame chordwise position for the whole run (two markers whose
     // support boxes overlap are less than 5*sqrt(2) lattice units apart in any
@@ -323,6 +326,7 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             if (launch_flow(h, fin, h->n, slot, q, h->side)) return cuda_err(h, cudaGetLastError(), "launch ib");
             if (e) CK(cudaEventRecord(h->ev_side[2 * slot + 1], h->side), "event");
             CK(cudaEventRecord(h->ev_ib, h->side), "event");
+            if (launch_check(h, q, h->side)) return cuda_err(h, cudaGetLastError(), "launch check");
             CK(cudaEventRecord(h->ev_free[half], h->side), "event");
             // the next batch's factorization, overlapping this batch's steps
             if ((b + 1) * K <= last_step && h->batch_in_half[half ^ 1] != b + 1 && (rc = factor_batch(b + 1))) return rc;
@@ -338,6 +342,7 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             if (e) CK(cudaEventRecord(e[0], h->stream), "event");
             if (h->batch_in_half[half] != b && (rc = factor_batch(b))) return rc;
             if (launch_flow(h, fin, h->n, slot, q, h->stream)) return cuda_err(h, cudaGetLastError(), "launch ib");
+            if (launch_check(h, q, h->stream)) return cuda_err(h, cudaGetLastError(), "launch check");
             if (e) {
                 CK(cudaEventRecord(e[1], h->stream), "event");
                 CK(cudaEventRecord(e[2], h->stream), "event");
@@ -355,6 +360,10 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
                 CK(cudaMemcpyAsync(rows_out + (size_t)(done - pending) * h->row_len, h->d_ring,
                                    sizeof(double) * h->row_len * pending, cudaMemcpyDeviceToHost, h->stream),
                    "copy force rows");
+            if (split) {   // the residual checks run on the side stream after the spread
+                CK(cudaEventRecord(h->ev_ib, h->side), "event");
+                CK(cudaStreamWaitEvent(h->stream, h->ev_ib, 0), "wait");
+            }
             int st = check_status(h);
             if (st) return st;
             if (h->timing && (st = collect_timing(h, pending, split))) return st;
@@ -366,6 +375,10 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             CK(cudaMemcpyAsync(rows_out + (size_t)(done - pending) * h->row_len, h->d_ring,
                                sizeof(double) * h->row_len * pending, cudaMemcpyDeviceToHost, h->stream),
                "copy force rows");
+        if (split) {
+            CK(cudaEventRecord(h->ev_ib, h->side), "event");
+            CK(cudaStreamWaitEvent(h->stream, h->ev_ib, 0), "wait");
+        }
         int st = check_status(h);
         if (st) return st;
         if (h->timing && (st = collect_timing(h, pending, split))) return st;

@@ -75,6 +75,9 @@ struct IBArgs {
     int nslots;
     long long st_mk, st_perm, st_B, wk_blocks, wk_gf;
     PatchInfo *pinfo;
+    int *tiles;         // per patch tile: marker count, then the listed markers (slot)
+    int tiles_x;        // tiles per patch row
+    long long st_tiles; // ints per slot of the tile lists
     void *patch;        // compute-precision (du, dv) pairs
     int patch_cap;      // nodes
     int patch_wmax, patch_hmax;  // rectangle the spread grid covers
@@ -134,6 +137,7 @@ struct lbm_handle {
     double *d_key = nullptr, *d_reach = nullptr;
     int static_order = 0;   // one rigid body: fixed body-frame marker order
     PatchInfo *d_pinfo = nullptr;   // LBM_NSLOT_MAX slots (patch rectangle of the slot's step)
+    int *d_tiles = nullptr;         // nslots x tile lists of the patch grid
     int pinfo_slot = 0;             // slot the next lattice launch reads
     void *d_patch = nullptr;
     int patch_cap = 0;               // nodes
@@ -190,6 +194,8 @@ void ib_factor_scratch(int nseg, size_t *work_blocks, size_t *factor_slot);
 int launch_kf(lbm_handle *h, const void *fin, void *fout, void *fields, int mode = KF_ALL, cudaStream_t st = nullptr);
 int launch_factor(lbm_handle *h, int step0, int count, cudaStream_t st);
 int launch_flow(lbm_handle *h, const void *fin, int step_index, int ring_slot, int slot, cudaStream_t st);
+int launch_check(lbm_handle *h, int slot, cudaStream_t st);
+int ib_tile_ints();   // ints per patch tile of the tile lists
 int launch_residual(lbm_handle *h, const void *fa, const void *fb, double *out2);
 int launch_unpack(lbm_handle *h, const void *fsrc, double *dst);   // deviation -> f (FP64)
 int launch_pack(lbm_handle *h, const double *src, void *fdst);     // f (FP64) -> deviation
