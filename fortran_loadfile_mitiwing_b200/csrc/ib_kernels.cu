@@ -59,6 +59,15 @@ constexpr int STAGE_BLOCKS = 32;       // factor blocks of one level staged in s
 constexpr int FL = 2 * BS;             // columns of a coupling panel [L_o | L_q^T]
 constexpr int GW = 3 * BS;             // row width of a stored factor block [D^-1 | F_L | F_U]
 constexpr int GP = BS + 1;             // padded row stride of square blocks in shared memory
+constexpr int SOLVE_SMEM_BUDGET = 232192;   // dynamic shared memory of ib_solve (bytes)
+
+// factor blocks ib_solve can stage next to the right-hand sides of nb blocks
+__host__ __device__ constexpr int stage_cap(int nb)
+{
+    return (SOLVE_SMEM_BUDGET - 16 - 2 * nb * BS * (int)sizeof(double)) / (BS * GW * (int)sizeof(double)) < STAGE_BLOCKS
+               ? (SOLVE_SMEM_BUDGET - 16 - 2 * nb * BS * (int)sizeof(double)) / (BS * GW * (int)sizeof(double))
+               : STAGE_BLOCKS;
+}
 constexpr int WS = BS * GP + BS * FL + BS * GP;   // workspace per warp (doubles)
 constexpr int NPART = 3 * LBM_MAXW + 3;           // per-CTA partials of ib_spread
 constexpr int TILE = 16;                          // correction-patch tile (nodes per side)
@@ -744,10 +753,13 @@ __global__ void __launch_bounds__(FACTOR_THREADS) ib_factor(const IBArgs base, i
 //   backward, st = ..., 2, 1:    x_o = D_o^-1 r_o - F_L(o) x_p - F_U(o) x_q  (odd o)
 // (F_L(q)^T = L_q^T D_q^-1 and F_U(p)^T = L_e D_p^-1 since D is symmetric.)
 // Each level reads the factor blocks of that level's odd blocks; when they
-// fit (at most STAGE_BLOCKS), one thread brings them into shared memory with
-// bulk copies (6 KB per block, completion on an mbarrier) before the level's
-// arithmetic, so that the level costs one memory round trip instead of one
-// per dependent load. Also writes the force row's header and reports the
+// fit (at most stage_cap), the lanes of warp 0 bring them into shared memory
+// with bulk copies (one 6-KB block each, completion on an mbarrier) before
+// the level's arithmetic, so that the level costs one memory round trip
+// instead of one per dependent load. Rows of a block are GW = 96 words apart,
+// all on one bank: the backward sweep, which reads one row per lane pair,
+// walks the columns in a rotated order (lane row i starts at column i) so
+// that the 16 rows read in one step fall on distinct banks. Also writes the force row's header and reports the
 // errors of the factorization chain. Dynamic shared memory: the staged
 // blocks, then the right-hand sides in the solve order (two per marker,
 // padded to whole blocks), then the mbarrier.
@@ -758,7 +770,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
     const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
     const int nb = (n + BS - 1) / BS;
     double *stage_buf = smem;
-    double *X = smem + STAGE_BLOCKS * BS * GW;
+    const int scap = stage_cap(nb);
+    double *X = smem + scap * BS * GW;
     uint64_t *bar = reinterpret_cast<uint64_t *>(X + 2 * nb * BS);
     __shared__ int timed_out;
     if (tid == 0) {
@@ -797,13 +810,14 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
     // of block o at index (o/st - 1)/2), or read from global memory
     auto stage_level = [&](int st) -> bool {
         const int nodd = (nb - st + 2 * st - 1) / (2 * st);
-        if (nodd > STAGE_BLOCKS) return false;
+        if (nodd > scap) return false;
         __syncthreads();   // previous readers of the stage buffer are done
-        if (tid == 0) {
-            fence_proxy_async();
+        if (warp == 0) {
             constexpr uint32_t kBlockBytes = sizeof(double) * BS * GW;
-            mbar_expect_tx(bar, kBlockBytes * (uint32_t)nodd);
-            for (int m = 0; m < nodd; ++m)
+            if (lane == 0) mbar_expect_tx(bar, kBlockBytes * (uint32_t)nodd);
+            __syncwarp();
+            fence_proxy_async();
+            for (int m = lane; m < nodd; m += 32)
                 bulk_g2s(stage_buf + m * BS * GW, Gf + (long long)st * (2 * m + 1) * BS * GW, kBlockBytes, bar);
         }
         // bounded wait: copies that never land are reported, not waited on forever
@@ -815,9 +829,6 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
         __syncthreads();   // every thread sees the same timed_out
         return true;
     };
-    auto fblock = [&](bool staged, int st, int o) -> const double * {
-        return staged ? stage_buf + ((o / st - 1) / 2) * BS * GW : Gf + (long long)o * BS * GW;
-    };
     __syncthreads();
     const int i = lane >> 1, c = lane & 1;   // row of the block, right-hand side
     int levels = 0;
@@ -825,22 +836,32 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
         const bool staged = stage_level(st);
         if (timed_out) break;
         const int neven = (nb + 2 * st - 1) / (2 * st);
-        for (int m = warp; m < neven; m += nw) {
-            const int e = 2 * st * m, o1 = e - st, o2 = e + st;
+        // one even block e per warp: F_L(q) and F_U(p) from block bases that
+        // are either staged (shared memory, row stride GW) or global (GW);
+        // the two forms are separate so that staged reads stay shared loads
+        auto fwd = [&](const double *Fq, const double *Fp, int ld, int e, bool has_q, bool has_p) {
             double acc = 0.0;
-            if (o2 < nb) {
-                const double *F = fblock(staged, st, o2) + BS + i;      // F_L(q)[t][i]
-                const double *r = X + 2 * o2 * BS + c;
+            if (has_q) {
+                const double *F = Fq + BS + i;       // F_L(q)[t][i]
+                const double *r = X + 2 * (e + st) * BS + c;
 #pragma unroll
-                for (int t = 0; t < BS; ++t) acc += F[t * GW] * r[2 * t];
+                for (int t = 0; t < BS; ++t) acc += F[t * ld] * r[2 * t];
             }
-            if (m > 0) {
-                const double *F = fblock(staged, st, o1) + 2 * BS + i;  // F_U(p)[t][i]
-                const double *r = X + 2 * o1 * BS + c;
+            if (has_p) {
+                const double *F = Fp + 2 * BS + i;   // F_U(p)[t][i]
+                const double *r = X + 2 * (e - st) * BS + c;
 #pragma unroll
-                for (int t = 0; t < BS; ++t) acc += F[t * GW] * r[2 * t];
+                for (int t = 0; t < BS; ++t) acc += F[t * ld] * r[2 * t];
             }
             X[2 * (e * BS + i) + c] -= acc;
+        };
+        for (int m = warp; m < neven; m += nw) {
+            const int e = 2 * st * m, o1 = e - st, o2 = e + st;
+            const bool has_q = o2 < nb, has_p = m > 0;
+            if (staged)   // odd block st(2k+1) is staged at index k
+                fwd(stage_buf + m * BS * GW, stage_buf + (m - 1) * BS * GW, GW, e, has_q, has_p);
+            else
+                fwd(Gf + (long long)o2 * BS * GW, Gf + (long long)o1 * BS * GW, GW, e, has_q, has_p);
         }
         __syncthreads();
     }
@@ -859,21 +880,31 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
             const bool staged = stage_level(st);
             if (timed_out) break;
             const int nodd = (nb - st + 2 * st - 1) / (2 * st);
-            for (int m = warp; m < nodd; m += nw) {
-                const int o = st * (2 * m + 1), p = o - st, q2 = o + st;
-                const double *G = fblock(staged, st, o) + i * GW;
+            auto bwd = [&](const double *G, int o) {
+                const int p = o - st, q2 = o + st;
                 double s1 = 0.0, s2 = 0.0, s3 = 0.0;
 #pragma unroll
-                for (int t = 0; t < BS; ++t) {
+                for (int t0 = 0; t0 < BS; ++t0) {
+                    const int t = (t0 + i) & (BS - 1);   // rotated column order
                     s1 += G[t] * X[2 * (o * BS + t) + c];
                     s2 += G[BS + t] * X[2 * (p * BS + t) + c];
                 }
                 if (q2 < nb) {
 #pragma unroll
-                    for (int t = 0; t < BS; ++t) s3 += G[2 * BS + t] * X[2 * (q2 * BS + t) + c];
+                    for (int t0 = 0; t0 < BS; ++t0) {
+                        const int t = (t0 + i) & (BS - 1);
+                        s3 += G[2 * BS + t] * X[2 * (q2 * BS + t) + c];
+                    }
                 }
                 __syncwarp();
                 X[2 * (o * BS + i) + c] = s1 - s2 - s3;
+            };
+            for (int m = warp; m < nodd; m += nw) {
+                const int o = st * (2 * m + 1);
+                if (staged)
+                    bwd(stage_buf + (m * BS + i) * GW, o);
+                else
+                    bwd(Gf + ((long long)o * BS + i) * GW, o);
             }
             __syncthreads();
         }
@@ -1199,11 +1230,11 @@ size_t order_smem(int n)
 }
 
 constexpr size_t kFactorSmem = sizeof(double) * BOPS_WARPS * WS;
-constexpr size_t kSolveSmemMax = sizeof(double) * (STAGE_BLOCKS * BS * GW + 2 * NMARK_MAX) + 16;
+constexpr size_t kSolveSmemMax = SOLVE_SMEM_BUDGET;
 size_t solve_smem(int nseg)
 {
-    const size_t nb = (size_t)(nseg + BS - 1) / BS;
-    return sizeof(double) * (STAGE_BLOCKS * BS * GW + 2 * nb * BS) + 16;
+    const int nb = (nseg + BS - 1) / BS;
+    return sizeof(double) * ((size_t)stage_cap(nb) * BS * GW + 2 * (size_t)nb * BS) + 16;
 }
 
 // arguments of the flow chain of the step held in buffer slot `slot`; for
