@@ -198,12 +198,15 @@ __global__ void __launch_bounds__(256) kf_kernel(const KFArgs<C> a)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int j = blockIdx.y;
-    if (a.mode == KF_INNER) {
-        if (i >= a.rw) return;
-        i += a.rx0;
-        j += a.ry0;
-    } else if (a.mode == KF_OUTER && (unsigned)(i - a.rx0) < (unsigned)a.rw && (unsigned)(j - a.ry0) < (unsigned)a.rh) {
-        return;
+    if (a.mode != KF_ALL) {   // split around the step's correction patch
+        const PatchInfo r = *a.pinfo;
+        if (a.mode == KF_INNER) {
+            if (i >= r.w || j >= r.h) return;
+            i += r.i0;
+            j += r.j0;
+        } else if ((unsigned)(i - r.i0) < (unsigned)r.w && (unsigned)(j - r.j0) < (unsigned)r.h) {
+            return;
+        }
     }
     if (i >= a.nx) return;
     const T *__restrict__ fin = (const T *)a.fin;
@@ -230,12 +233,7 @@ __global__ void __launch_bounds__(128) kf_vec(const KFArgs<C> a)
     const int lane = threadIdx.x & 31;
     int i0 = (blockIdx.x * blockDim.x + threadIdx.x) * VEC;
     int j = blockIdx.y;
-    int iend = a.nx;                           // first column this launch does not own
-    if (a.mode == KF_INNER) {
-        i0 += a.rx0;
-        j += a.ry0;
-        iend = a.rx0 + a.rw;
-    }
+    const int iend = a.nx;                     // whole lattice only (KF_ALL)
     const T *__restrict__ fin = (const T *)a.fin;
     T *__restrict__ fout = (T *)a.fout;
     const int pitch = a.pitch, plane = (int)a.plane;
@@ -275,10 +273,6 @@ __global__ void __launch_bounds__(128) kf_vec(const KFArgs<C> a)
         }
     }
     if (i0 >= iend) return;
-    // the split rectangle's x bounds are multiples of VEC, so a thread's nodes
-    // are all inside or all outside it
-    if (a.mode == KF_OUTER && (unsigned)(i0 - a.rx0) < (unsigned)a.rw && (unsigned)(j - a.ry0) < (unsigned)a.rh)
-        return;
     if (i0 >= 1 && i0 + VEC - 1 <= a.nx - 2) {
         T out[9][VEC];
 #pragma unroll
@@ -353,6 +347,7 @@ __global__ void __launch_bounds__(TW) kf_tma(const KFArgs<C> a)
     const T *__restrict__ fin = (const T *)a.fin;
     T *__restrict__ fout = (T *)a.fout;
     const PatchInfo pi = a.mode == KF_OUTER ? PatchInfo{0, 0, 0, 0} : *a.pinfo;
+    const PatchInfo rr = a.mode == KF_OUTER ? *a.pinfo : PatchInfo{0, 0, 0, 0};   // nodes the outer part skips
     if (blockIdx.y == gridDim.y - 1) {         // the two edge rows of this strip
         if (i < a.nx)
             for (int j = 0; j < a.ny; j += a.ny - 1) {
@@ -393,7 +388,7 @@ __global__ void __launch_bounds__(TW) kf_tma(const KFArgs<C> a)
                 return;
             }
         }
-        const bool skip = a.mode == KF_OUTER && (unsigned)(i - a.rx0) < (unsigned)a.rw && (unsigned)(j - a.ry0) < (unsigned)a.rh;
+        const bool skip = (unsigned)(i - rr.i0) < (unsigned)rr.w && (unsigned)(j - rr.j0) < (unsigned)rr.h;
         if (i < a.nx && !skip) {
             C gout[9], frho, fu, fv;
             if (i == 0 || i == a.nx - 1) {
@@ -441,8 +436,7 @@ template <typename T, typename C, int VEC>
 void launch_vec(const KFArgs<C> &a, bool fields, int nx, int ny, cudaStream_t st)
 {
     const int per_block = 128 * VEC;
-    const int wx = a.mode == KF_INNER ? a.rw : nx, wy = a.mode == KF_INNER ? a.rh : ny;
-    dim3 block(128, 1), grid((wx + per_block - 1) / per_block, wy);
+    dim3 block(128, 1), grid((nx + per_block - 1) / per_block, ny);
     if (fields)
         kf_vec<T, C, true, VEC><<<grid, block, 0, st>>>(a);
     else
@@ -454,10 +448,6 @@ int launch_kf_t(lbm_handle *h, const void *fin, void *fout, void *fields, int mo
 {
     KFArgs<C> a;
     a.mode = mode;
-    a.rx0 = h->env_x0;
-    a.ry0 = h->env_y0;
-    a.rw = h->env_w;
-    a.rh = h->env_h;
     a.fin = fin;
     a.fout = fout;
     a.nx = h->nx;
@@ -485,7 +475,6 @@ int launch_kf_t(lbm_handle *h, const void *fin, void *fout, void *fields, int mo
     const int vec = small_index ? h->kf_vec : 1;
     a.rows_per_cta = h->kf_rows;
     a.status = h->d_status;
-    if (mode != KF_ALL && (a.rw <= 0 || a.rh <= 0)) return mode == KF_INNER ? 0 : -1;
     if (!st) st = h->stream;
     if (h->kf_tma && mode != KF_INNER && h->ny >= 3) {
         static bool configured = false;   // per process; the attribute is per function
@@ -494,12 +483,14 @@ int launch_kf_t(lbm_handle *h, const void *fin, void *fout, void *fields, int mo
             configured = true;
         }
         launch_tma<T, C>(a, fields != nullptr, h->nx, h->ny, st);
-    } else if (vec == 4 && h->pitch % 4 == 0) {
+    } else if (mode == KF_ALL && vec == 4 && h->pitch % 4 == 0) {
         launch_vec<T, C, 4>(a, fields != nullptr, h->nx, h->ny, st);
-    } else if (vec == 2 && h->pitch % 2 == 0) {
+    } else if (mode == KF_ALL && vec == 2 && h->pitch % 2 == 0) {
         launch_vec<T, C, 2>(a, fields != nullptr, h->nx, h->ny, st);
     } else {
-        const int wx = mode == KF_INNER ? a.rw : h->nx, wy = mode == KF_INNER ? a.rh : h->ny;
+        // the inner part covers the largest patch rectangle; its threads
+        // outside the step's rectangle return at once
+        const int wx = mode == KF_INNER ? h->patch_wmax : h->nx, wy = mode == KF_INNER ? h->patch_hmax : h->ny;
         dim3 block(256, 1), grid((wx + 255) / 256, wy);
         if (fields)
             kf_kernel<T, C, true><<<grid, block, 0, st>>>(a);

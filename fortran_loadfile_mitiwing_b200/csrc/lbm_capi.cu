@@ -330,6 +330,7 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             CK(cudaEventRecord(h->ev_free[half], h->side), "event");
             // the next batch's factorization, overlapping this batch's steps
             if ((b + 1) * K <= last_step && h->batch_in_half[half ^ 1] != b + 1 && (rc = factor_batch(b + 1))) return rc;
+            CK(cudaStreamWaitEvent(h->stream, h->ev_batch[half], 0), "wait");   // the step's patch rectangle
             if (e) CK(cudaEventRecord(e[0], h->stream), "event");
             if (launch_kf(h, fin, fout, fields, KF_OUTER)) return cuda_err(h, cudaGetLastError(), "launch kf");
             if (e) CK(cudaEventRecord(e[1], h->stream), "event");

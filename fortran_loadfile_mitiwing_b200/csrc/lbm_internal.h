@@ -33,7 +33,8 @@ struct KFArgs {
     int mode;                          // KF_ALL, KF_OUTER (skip rect), KF_INNER (rect only)
     int rows_per_cta;                  // row sweep length of the staged kernel
     unsigned *status;                  // device status word (bounded-wait timeouts)
-    int rx0, ry0, rw, rh;              // split rectangle (0-based origin, extent)
+    // split modes: the outer part skips, and the inner part covers, the
+    // step's correction patch rectangle *pinfo
 };
 
 #define LBM_NSLOT_MAX 16   // largest slot count of the factorization batches
