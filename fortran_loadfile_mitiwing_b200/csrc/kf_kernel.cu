@@ -332,29 +332,38 @@ constexpr int KS = 4;          // pipeline stages
 
 template <typename T> __host__ __device__ constexpr int tma_halo() { return 16 / (int)sizeof(T); }
 template <typename T> __host__ __device__ constexpr int tma_seg() { return TW + 2 * tma_halo<T>(); }
-template <typename T> constexpr size_t tma_smem() { return sizeof(T) * KS * 9 * tma_seg<T>() + 8 * KS; }
+template <typename T> constexpr size_t tma_smem() { return sizeof(T) * KS * 9 * tma_seg<T>() + 2 * 8 * KS; }
 
 template <typename T, typename C, bool FIELDS>
 __global__ void __launch_bounds__(TW) kf_tma(const KFArgs<C> a)
 {
-    constexpr int H = tma_halo<T>(), SEG = tma_seg<T>();
+    constexpr int H = tma_halo<T>(), SEG = tma_seg<T>(), NWARP = TW / 32;
     extern __shared__ __align__(128) unsigned char smraw[];
     T *buf = reinterpret_cast<T *>(smraw);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smraw + sizeof(T) * KS * 9 * SEG);
-    const int tid = threadIdx.x;
+    uint64_t *full = reinterpret_cast<uint64_t *>(smraw + sizeof(T) * KS * 9 * SEG);
+    uint64_t *empty = full + KS;
+    const int tid = threadIdx.x, lane = tid & 31;
     const int x0 = blockIdx.x * TW;
     const int i = x0 + tid;
     const T *__restrict__ fin = (const T *)a.fin;
     T *__restrict__ fout = (T *)a.fout;
     const PatchInfo pi = a.mode == KF_OUTER ? PatchInfo{0, 0, 0, 0} : *a.pinfo;
     const PatchInfo rr = a.mode == KF_OUTER ? *a.pinfo : PatchInfo{0, 0, 0, 0};   // nodes the outer part skips
-    if (blockIdx.y == gridDim.y - 1) {         // the two edge rows of this strip
+    if (blockIdx.y == gridDim.y - 1) {
+        // the edge nodes: rows 0 and ny-1 of this strip, and a share of the
+        // nodes of columns 0 and nx-1 (which the strips' row sweeps skip)
         if (i < a.nx)
             for (int j = 0; j < a.ny; j += a.ny - 1) {
                 C gout[9], frho, fu, fv;
                 edge_update<T, C>(a, fin, i, j, gout, frho, fu, fv);
                 store_node<T, C, FIELDS>(a, fout, i, j, gout, frho, fu, fv);
             }
+        for (int q = blockIdx.x * TW + tid; q < 2 * (a.ny - 2); q += gridDim.x * TW) {
+            const int j = 1 + q / 2, ie = (q & 1) ? a.nx - 1 : 0;
+            C gout[9], frho, fu, fv;
+            edge_update<T, C>(a, fin, ie, j, gout, frho, fu, fv);
+            store_node<T, C, FIELDS>(a, fout, ie, j, gout, frho, fu, fv);
+        }
         return;
     }
     const int j0 = 1 + blockIdx.y * a.rows_per_cta;
@@ -363,49 +372,64 @@ __global__ void __launch_bounds__(TW) kf_tma(const KFArgs<C> a)
     const int width = min(TW, a.nx - x0);
     const uint32_t bytes = (uint32_t)((((width + 2 * H) * (int)sizeof(T)) + 15) / 16 * 16);
     if (tid == 0) {
-        for (int s = 0; s < KS; ++s) mbar_init(&bar[s], 1);
+        for (int s = 0; s < KS; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], NWARP);
+        }
         mbar_init_fence();
     }
     __syncthreads();
     auto issue = [&](int r) {
         const int s = r % KS, j = j0 + r;
-        mbar_expect_tx(&bar[s], 9u * bytes);
+        mbar_expect_tx(&full[s], 9u * bytes);
 #pragma unroll
         for (int k = 0; k < 9; ++k)
             bulk_g2s(buf + (s * 9 + k) * SEG,
-                     fin + (long long)k * a.plane + (long long)(j - lbm_ey(k)) * a.pitch + (x0 - H), bytes, &bar[s]);
+                     fin + (long long)k * a.plane + (long long)(j - lbm_ey(k)) * a.pitch + (x0 - H), bytes, &full[s]);
+    };
+    // bounded wait: a barrier that never completes is reported, not waited on forever
+    auto wait = [&](uint64_t *bar, uint32_t parity) -> bool {
+        int spins = 0;
+        while (!mbar_try_wait(bar, parity))
+            if (++spins > (1 << 22)) return false;
+        return true;
     };
     if (tid == 0)
         for (int r = 0; r < KS && r < nrows; ++r) issue(r);
+    // Stage s holds row r = s (mod KS). A warp waits for the row on full[s],
+    // and when done reading it arrives on empty[s]; thread 0 refills the stage
+    // with row r + KS once all warps have arrived. Only warp 0 waits for the
+    // other warps; they run up to KS - 1 rows ahead.
+    bool ok = true;
     for (int r = 0; r < nrows; ++r) {
         const int s = r % KS, j = j0 + r;
         const uint32_t parity = (uint32_t)((r / KS) & 1);
-        // bounded wait: a copy that never lands is reported, not waited on forever
-        int spins = 0;
-        while (!mbar_try_wait(&bar[s], parity)) {
-            if (++spins > (1 << 22)) {
-                if (tid == 0) atomicOr(a.status, LBM_ST_TIMEOUT);
-                return;
-            }
-        }
+        if (!wait(&full[s], parity)) { ok = false; break; }
         const bool skip = (unsigned)(i - rr.i0) < (unsigned)rr.w && (unsigned)(j - rr.j0) < (unsigned)rr.h;
-        if (i < a.nx && !skip) {
+        if (i > 0 && i < a.nx - 1 && !skip) {
             C gout[9], frho, fu, fv;
-            if (i == 0 || i == a.nx - 1) {
-                edge_update<T, C>(a, fin, i, j, gout, frho, fu, fv);
-            } else {
-                C g[9];
-                const T *row = buf + s * 9 * SEG + H + tid;
+            C g[9];
+            const T *row = buf + s * 9 * SEG + H + tid;
 #pragma unroll
-                for (int k = 0; k < 9; ++k) g[k] = (C)Store<T>::cvt(row[k * SEG - lbm_ex(k)]);
-                collide_interior<C>(a, pi, g, i, j, gout, frho, fu, fv);
-            }
+            for (int k = 0; k < 9; ++k) g[k] = (C)Store<T>::cvt(row[k * SEG - lbm_ex(k)]);
+            collide_interior<C>(a, pi, g, i, j, gout, frho, fu, fv);
             store_node<T, C, FIELDS>(a, fout, i, j, gout, frho, fu, fv);
         }
-        __syncthreads();                       // stage s fully read
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[s]);
         if (tid == 0 && r + KS < nrows) {
+            if (!wait(&empty[s], parity)) { ok = false; break; }
             fence_proxy_async();
             issue(r + KS);
+        }
+    }
+    if (!ok) {
+        // report, then wait (bounded) for this CTA's copies still in flight
+        atomicOr(a.status, LBM_ST_TIMEOUT);
+        for (int s = 0; s < KS; ++s) {
+            int spins = 0;
+            while (!mbar_try_wait(&full[s], 0) && !mbar_try_wait(&full[s], 1) && ++spins < (1 << 20)) {
+            }
         }
     }
 }
