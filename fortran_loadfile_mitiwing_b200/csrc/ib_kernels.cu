@@ -25,6 +25,8 @@
 //               apart per axis), so the CTA builds its diagonal block and the
 //               block coupling it to the previous one, and checks that no
 //               coupling reaches further;
+//   ib_tiles    per 16 x 16 tile of the patch rectangle, the markers whose
+//               support box meets it;
 //   ib_factor   one CTA: correction-patch rectangle, then block cyclic
 //               reduction of the block tridiagonal matrix (log2 of the block
 //               count levels of Gauss-Jordan block inverses and block
@@ -38,15 +40,19 @@
 //               over the two right-hand sides, each level's factor blocks
 //               staged in shared memory by bulk copies (or the two triangular
 //               solves of the dense factor), and the force row's header;
-//   ib_spread   du = D^T y per node, gathered in marker order over the
-//               markers whose box covers the node (no atomics), written to the
-//               correction patch the lattice kernel reads; force and moment
-//               sums (:1645-1675, solution.f90:327-336) and the solve
-//               residual in FP64 with a deterministic two-level reduction.
+//   ib_tile_update  one CTA per correction tile (a 16 x 16 tile of the
+//               patch rectangle that lists a marker): du = D^T y per node,
+//               gathered in marker order (no atomics), the lattice update of
+//               the tile's nodes with that correction, and the force and
+//               moment sums (:1645-1675, solution.f90:327-336) in FP64 with a
+//               deterministic two-level reduction. The lattice kernel skips
+//               these nodes and updates all others;
+//   ib_residual the solve's residual, after the step's update.
 
 #include <math.h>
 
 #include "lbm_internal.h"
+#include "lbm_node.cuh"
 
 namespace {
 
@@ -69,7 +75,7 @@ __host__ __device__ constexpr int stage_cap(int nb)
                : STAGE_BLOCKS;
 }
 constexpr int WS = BS * GP + BS * FL + BS * GP;   // workspace per warp (doubles)
-constexpr int NPART = 3 * LBM_MAXW + 3;           // per-CTA partials of ib_spread
+constexpr int NPART = 3 * LBM_MAXW + 3;           // per-CTA partials of ib_tile_update
 constexpr int TILE = 16;                          // correction-patch tile (nodes per side)
 constexpr int TILE_CAP = 256;                     // markers listed per tile
 
@@ -137,6 +143,7 @@ __device__ __forceinline__ IBArgs member_args(IBArgs a, int step)
     a.gf += slot * a.wk_gf;
     a.pinfo += slot;
     a.tiles += slot * a.st_tiles;
+    a.nsup += slot;
     a.fmode += 2 * slot;
     a.fstatus += slot;
     a.status = a.fstatus;   // errors of the chain are reported by the step that uses it
@@ -609,12 +616,13 @@ __global__ void __launch_bounds__(FACTOR_THREADS) ib_factor(const IBArgs base, i
         PatchInfo pi{0, 0, 0, 0};
         if (bb[2] >= bb[0]) {
             pi.i0 = bb[0]; pi.j0 = bb[1]; pi.w = bb[2] - bb[0] + 1; pi.h = bb[3] - bb[1] + 1;
-            if ((long long)pi.w * pi.h > a.patch_cap || pi.w > a.patch_wmax || pi.h > a.patch_hmax) {
+            if (pi.w > a.patch_wmax || pi.h > a.patch_hmax) {
                 atomicOr(a.status, LBM_ST_OVERFLOW);
                 pi = PatchInfo{0, 0, 0, 0};
             }
         }
         *a.pinfo = pi;
+        *a.nsup = 0;   // counted by ib_tiles
         const int w = *a.wmax;
         bad = 0;
         dense = (w > BS || a.force_dense) ? 1 : 0;
@@ -781,6 +789,10 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
         const unsigned fs = *a.fstatus;
         if (fs) { atomicOr(a.status, fs); *a.fstatus = 0u; }
         a.solve_res[1] = (double)a.fmode[1];
+        if (*a.nsup == 0) {   // no correction tile: nothing writes the forces
+            double *fr = a.force_ring + (long long)ring_slot * a.row_len;
+            for (int c = 1; c <= 3 * a.nwing + 3; ++c) fr[c] = 0.0;
+        }
         timed_out = 0;
         mbar_init(bar, 1);
         mbar_init_fence();
@@ -968,7 +980,10 @@ __global__ void __launch_bounds__(256) ib_tiles(const IBArgs base, int step0)
         }
         __syncthreads();
     }
-    if (threadIdx.x == 0) list[0] = total;
+    if (threadIdx.x == 0) {
+        list[0] = total;
+        if (total > 0) atomicAdd(a.nsup, 1);
+    }
 }
 
 // Residual of the step's solve, ||B y - rhs|| / ||rhs|| with B = D D^T
@@ -1040,10 +1055,16 @@ __global__ void __launch_bounds__(256) ib_residual(const IBArgs a)
     }
 }
 
-// du = D^T y over the current patch, 16x16 nodes per CTA, plus FP64 force and
-// moment partials (boundary_condition.f90:1645-1675)
-template <typename T, typename C>
-__global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index, int ring_slot)
+// The correction tiles of the step (the 16 x 16 tiles of the patch
+// rectangle that list a marker), one CTA per tile: du = D^T y per node,
+// gathered in marker order over the markers whose box covers the node (no
+// atomics); then the lattice update of the tile's nodes with that velocity
+// correction (the node path of the lattice kernels); and each node's FP64
+// force and moment (boundary_condition.f90:1645-1675, solution.f90:327-336).
+// The last CTA sums the per-tile partials in tile order into the step's force
+// row. The lattice kernel updates every other node.
+template <typename T, typename C, bool FIELDS>
+__global__ void __launch_bounds__(256) ib_tile_update(const IBArgs a, const KFArgs<C> kf, int step_index, int ring_slot)
 {
     __shared__ int wsum[8];
     __shared__ int nlist;
@@ -1055,19 +1076,21 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
     __shared__ double sy[256][2];
     __shared__ int swing[256];
     const PatchInfo pi = *a.pinfo;
+    const int ti0 = blockIdx.x * TILE, tj0 = blockIdx.y * TILE;
+    if (ti0 >= pi.w || tj0 >= pi.h) return;
+    const int *tlist = a.tiles + (long long)(blockIdx.y * gridDim.x + blockIdx.x) * (TILE_CAP + 1);
+    const int listed = tlist[0];
+    if (listed == 0) return;   // not a correction tile: the lattice kernel updates it
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    const int ti0 = blockIdx.x * 16, tj0 = blockIdx.y * 16;
     const int li = ti0 + tx, lj = tj0 + ty;                    // patch-relative
     const int gi = pi.i0 + li, gj = pi.j0 + lj;                // 0-based node
     const bool active = li < pi.w && lj < pi.h;
-    const bool tile_active = ti0 < pi.w && tj0 < pi.h;
-    const int ta = pi.i0 + ti0, tb = pi.i0 + ti0 + 15, sa_ = pi.j0 + tj0, sb_ = pi.j0 + tj0 + 15;
+    const bool tile_active = true;
+    const int ta = pi.i0 + ti0, tb = ta + TILE - 1, sa_ = pi.j0 + tj0, sb_ = sa_ + TILE - 1;
     double du = 0.0, dv = 0.0;
     int wing = 1 << 20;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int *tlist = a.tiles + (long long)(blockIdx.y * gridDim.x + blockIdx.x) * (TILE_CAP + 1);
-    const int listed = tile_active ? tlist[0] : 0;
-    if (tile_active && listed <= TILE_CAP) {
+    if (listed <= TILE_CAP) {
         // markers listed for this tile by the factorization chain
         if (threadIdx.x == 0) nlist = listed;
         if ((int)threadIdx.x < listed) {
@@ -1135,26 +1158,30 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
             __syncthreads();
         }
     }
-    if (active) {
-        C *patch = (C *)a.patch;
-        const long long pq = 2ll * ((long long)lj * pi.w + li);
-        patch[pq] = (C)du;
-        patch[pq + 1] = (C)dv;
-    }
-    // force and moment of this node
+    // lattice update of the node with the correction, and its force and moment
     double fx = 0, fy = 0, mz = 0;
     const bool in_support = active && wing < (1 << 20);
-    if (in_support) {
-        const double *row = motion_row(a, step_index, nullptr);
-        double rho, u, v;
-        node_moments<T>(a, gi, gj, rho, u, v);
-        const double temp1 = 2.0 * rho * du, temp2 = 2.0 * rho * dv;
-        const double sa = row[4 + 9 * wing], sb = row[7 + 9 * wing];
-        fx = -temp1;
-        fy = -temp2;
-        const double x0 = (a.ox + a.scale * (double)gi - (a.xc + sa)) / a.scale;
-        const double y0 = (a.oy + a.scale * (double)gj - (a.yc + sb)) / a.scale;
-        mz = -x0 * temp2 + y0 * temp1;
+    if (active) {
+        const T *__restrict__ fin = (const T *)kf.fin;
+        C g[9];
+        lbm_node::pull<T, C>(fin, kf.plane, kf.pitch, gi, gj, g);
+        C gout[9], frho, fu, fv;
+        lbm_node::collide_interior<C>(kf, g, true, (C)du, (C)dv, gout, frho, fu, fv);
+        lbm_node::store_node<T, C, FIELDS>(kf, (T *)kf.fout, gi, gj, gout, frho, fu, fv);
+        if (in_support) {
+            // FP64 density of the same streamed populations
+            const double drho = (((double)g[0] + (double)g[1]) + ((double)g[2] + (double)g[3])) +
+                                (((double)g[4] + (double)g[5]) + ((double)g[6] + (double)g[7])) + (double)g[8];
+            const double rho = 1.0 + drho;
+            const double *row = motion_row(a, step_index, nullptr);
+            const double temp1 = 2.0 * rho * du, temp2 = 2.0 * rho * dv;
+            const double sa = row[4 + 9 * wing], sb = row[7 + 9 * wing];
+            fx = -temp1;
+            fy = -temp2;
+            const double x0 = (a.ox + a.scale * (double)gi - (a.xc + sa)) / a.scale;
+            const double y0 = (a.oy + a.scale * (double)gj - (a.yc + sb)) / a.scale;
+            mz = -x0 * temp2 + y0 * temp1;
+        }
     }
     // deterministic block reduction per wing
     for (int w = 0; w < a.nwing; ++w) {
@@ -1178,7 +1205,7 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
     }
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) amlast = atomicAdd(a.counter, 1u) == (unsigned)(nblk - 1);
+    if (threadIdx.x == 0) amlast = atomicAdd(a.counter, 1u) == (unsigned)(*a.nsup - 1);
     __syncthreads();
     if (!amlast) return;
     __threadfence();
@@ -1187,6 +1214,8 @@ __global__ void __launch_bounds__(256) ib_spread(const IBArgs a, int step_index,
     for (int w = 0; w < a.nwing; ++w) {
         double s0 = 0, s1 = 0, s2 = 0;
         for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
+            const int bx = b % gridDim.x, by = b / gridDim.x;
+            if (bx * TILE >= pi.w || by * TILE >= pi.h || a.tiles[(long long)b * (TILE_CAP + 1)] == 0) continue;
             const double *p = a.partial + (long long)b * NPART + 3 * w;
             s0 += __ldcg(p); s1 += __ldcg(p + 1); s2 += __ldcg(p + 2);
         }
@@ -1274,7 +1303,7 @@ IBArgs make_args(lbm_handle *h, const void *fin, int slot)
     a.rhs = h->d_rhs; a.y = h->d_y;
     a.bD = h->d_bD; a.bL = h->d_bL;
     a.reach = h->d_reach; a.wmax = h->d_wmax;
-    a.patch = h->d_patch; a.patch_cap = h->patch_cap;
+    a.nsup = h->d_nsup + slot;
     a.patch_wmax = h->patch_wmax; a.patch_hmax = h->patch_hmax;
     a.partial = h->d_partial; a.counter = h->d_counter;
     a.force_ring = h->d_ring; a.row_len = h->row_len;
@@ -1283,7 +1312,8 @@ IBArgs make_args(lbm_handle *h, const void *fin, int slot)
 }
 
 template <typename T, typename C>
-int launch_flow_t(lbm_handle *h, const void *fin, int step_index, int ring_slot, int slot, cudaStream_t st)
+int launch_flow_t(lbm_handle *h, const void *fin, void *fout, void *fields, int step_index, int ring_slot, int slot,
+                  cudaStream_t st)
 {
     IBArgs a = make_args(h, fin, slot);
     if (h->nseg > 0) {
@@ -1292,7 +1322,11 @@ int launch_flow_t(lbm_handle *h, const void *fin, int step_index, int ring_slot,
     }
     ib_solve<<<1, SOLVE_THREADS, solve_smem(h->nseg), st>>>(a, step_index, ring_slot);
     dim3 grid(h->patch_gx(), h->patch_gy());
-    ib_spread<T, C><<<grid, 256, 0, st>>>(a, step_index, ring_slot);
+    const KFArgs<C> kf = make_kf_args<C>(h, fin, fout, fields, KF_OUTER);
+    if (fields)
+        ib_tile_update<T, C, true><<<grid, 256, 0, st>>>(a, kf, step_index, ring_slot);
+    else
+        ib_tile_update<T, C, false><<<grid, 256, 0, st>>>(a, kf, step_index, ring_slot);
     h->launches += 2;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
@@ -1310,7 +1344,7 @@ int launch_check_t(lbm_handle *h, int slot, cudaStream_t st)
 
 }  // namespace
 
-// per-CTA partials of ib_spread (doubles)
+// per-CTA partials of ib_tile_update (doubles)
 int ib_partials_per_block() { return NPART; }
 
 // ints per patch tile of the tile lists (count + TILE_CAP indices)
@@ -1364,14 +1398,16 @@ int launch_check(lbm_handle *h, int slot, cudaStream_t st)
 
 // flow chain of step `step_index`: interpolation, solve with the factor of
 // `slot`, spread and forces
-int launch_flow(lbm_handle *h, const void *fin, int step_index, int ring_slot, int slot, cudaStream_t st)
+int launch_flow(lbm_handle *h, const void *fin, void *fout, void *fields, int step_index, int ring_slot, int slot,
+                cudaStream_t st)
 {
     if (!st) st = h->stream;
     switch (h->prec) {
-    case LBM_PREC_FP32: return launch_flow_t<float, float>(h, fin, step_index, ring_slot, slot, st);
-    case LBM_PREC_FP64: return launch_flow_t<double, double>(h, fin, step_index, ring_slot, slot, st);
-    case LBM_PREC_FP16: return launch_flow_t<__half, float>(h, fin, step_index, ring_slot, slot, st);
-    case LBM_PREC_BF16: return launch_flow_t<__nv_bfloat16, float>(h, fin, step_index, ring_slot, slot, st);
+    case LBM_PREC_FP32: return launch_flow_t<float, float>(h, fin, fout, fields, step_index, ring_slot, slot, st);
+    case LBM_PREC_FP64: return launch_flow_t<double, double>(h, fin, fout, fields, step_index, ring_slot, slot, st);
+    case LBM_PREC_FP16: return launch_flow_t<__half, float>(h, fin, fout, fields, step_index, ring_slot, slot, st);
+    case LBM_PREC_BF16:
+        return launch_flow_t<__nv_bfloat16, float>(h, fin, fout, fields, step_index, ring_slot, slot, st);
     }
     return -1;
 }

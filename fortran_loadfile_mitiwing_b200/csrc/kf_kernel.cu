@@ -14,183 +14,24 @@
 // their formula needs (O(perimeter) extra reads) so that no second launch and
 // no side buffer is needed for the boundary condition.
 #include "lbm_internal.h"
+#include "lbm_node.cuh"
 
 namespace {
 
-template <typename T, typename C>
-__device__ __forceinline__ void pull(const T *__restrict__ fin, long long plane, int pitch, int i, int j, C g[9])
-{
-#pragma unroll
-    for (int k = 0; k < 9; ++k)
-        g[k] = (C)Store<T>::ld(fin + (long long)k * plane + (long long)(j - lbm_ey(k)) * pitch + (i - lbm_ex(k)));
-}
+using namespace lbm_node;
 
+// a node of the step's correction tiles: inside the patch rectangle r, in a
+// 16 x 16 tile that lists at least one marker. Those nodes are updated by
+// the immersed-boundary tile kernel; the outer part skips them.
 template <typename C>
-__device__ __forceinline__ void moments(const C g[9], C &drho, C &u, C &v)
+__device__ __forceinline__ bool corr_tile(const KFArgs<C> &a, const PatchInfo &r, int i, int j)
 {
-    drho = ((g[0] + g[1]) + (g[2] + g[3])) + ((g[4] + g[5]) + (g[6] + g[7])) + g[8];
-    const C jx = (g[1] - g[3]) + (g[5] - g[6]) + (g[8] - g[7]);
-    const C jy = (g[2] - g[4]) + (g[5] + g[6]) - (g[7] + g[8]);
-    const C rho = C(1) + drho;
-    u = jx / rho;
-    v = jy / rho;
+    const unsigned li = (unsigned)(i - r.i0), lj = (unsigned)(j - r.j0);
+    if (li >= (unsigned)r.w || lj >= (unsigned)r.h) return false;
+    return a.tiles[(long long)((lj >> 4) * a.tiles_x + (li >> 4)) * a.tile_stride] > 0;
 }
 
-// characteristic update of a left (side=0) or right (side=1) column node
-// (boundary_condition.f90:418-438 and :500-520). Returns the updated
-// (drho, u, v) at the edge node and the streamed populations + moments of its
-// first interior neighbour.
-template <typename T, typename C>
-__device__ __forceinline__ void side_bc(const KFArgs<C> &a, const T *__restrict__ fin, int side, int j, C &dr1,
-                                        C &u1, C &v1, C g0n[9], C &drn, C &un, C &vn)
-{
-    const C *col = side == 0 ? a.col_l : a.col_r;
-    const C drs = col[3 * j], us = col[3 * j + 1], vs = col[3 * j + 2];
-    const int in1 = side == 0 ? 1 : a.nx - 2, in2 = side == 0 ? 2 : a.nx - 3;
-    C g2[9], dr2, u2, v2;
-    pull<T, C>(fin, a.plane, a.pitch, in1, j, g0n);
-    moments(g0n, drn, un, vn);
-    pull<T, C>(fin, a.plane, a.pitch, in2, j, g2);
-    moments(g2, dr2, u2, v2);
-    const C cs = a.cs, rhos = C(1) + drs;
-    if (side == 0) {
-        const C rhox = (C(-3) * drs + C(4) * drn - dr2) * C(0.5);
-        const C ux = (C(-3) * us + C(4) * un - u2) * C(0.5);
-        const C vx = (C(-3) * vs + C(4) * vn - v2) * C(0.5);
-        const C lx1 = (us - cs) * (cs * cs * rhox - cs * rhos * ux);
-        const C lx2 = us < C(0) ? us * vx : C(0);
-        dr1 = drs - lx1 * C(1.5);
-        u1 = us + lx1 / (C(2) * cs * (C(1) + dr1));
-        v1 = vs - lx2;
-    } else {
-        const C rhox = (C(3) * drs - C(4) * drn + dr2) * C(0.5);
-        const C ux = (C(3) * us - C(4) * un + u2) * C(0.5);
-        const C vx = (C(3) * vs - C(4) * vn + v2) * C(0.5);
-        const C lx2 = us >= C(0) ? us * vx : C(0);
-        const C lx3 = (us + cs) * (cs * cs * rhox + cs * rhos * ux);
-        dr1 = drs - lx3 * C(1.5);
-        u1 = us + (C(0) - lx3) / (C(2) * cs * (C(1) + dr1));
-        v1 = vs - lx2;
-    }
-}
-
-// interior node: moments of the streamed populations g, immersed-boundary
-// correction from the patch, MRT collision with forcing
-template <typename C>
-__device__ __forceinline__ void collide_interior(const KFArgs<C> &a, const PatchInfo &pi, const C g[9], int i, int j,
-                                                 C gout[9], C &frho, C &fu, C &fv)
-{
-    C drho, u, v;
-    moments(g, drho, u, v);
-    const C rho = C(1) + drho;
-    C gx = C(0), gy = C(0);
-    const unsigned pii = (unsigned)(i - pi.i0), pjj = (unsigned)(j - pi.j0);
-    if (pii < (unsigned)pi.w && pjj < (unsigned)pi.h) {
-        const int pq = 2 * ((int)pjj * pi.w + (int)pii);
-        const C du = a.patch[pq], dv = a.patch[pq + 1];
-        u = u + du;                       // boundary_condition.f90:1650-1651
-        v = v + dv;
-        gx = C(2) * rho * du;             // :1652-1656
-        gy = C(2) * rho * dv;
-    }
-    C m[9];
-    mrt_forward(g, m);
-    const C jx = rho * u, jy = rho * v;
-    const C jj = jx * jx + jy * jy;
-    C e[9];
-    e[0] = C(-1);                          // temp(1)=0 minus (M w)_1
-    e[1] = C(-2) * drho + C(3) * jj;       // solution.f90:605 minus (M w)_2
-    e[2] = drho - C(3) * jj;               // :606
-    e[3] = C(0);
-    e[4] = -jx;
-    e[5] = C(0);
-    e[6] = -jy;
-    e[7] = jx * jx - jy * jy;
-    e[8] = jx * jy;
-    // m' = m + s(meq - m) + fp (solution.f90:632-634); the new populations
-    // are taken as g + M^-1 (m' - m), which equals M^-1 m' exactly but
-    // rounds relative to the small non-equilibrium update, not to g
-    C d[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) d[k] = (e[k] - m[k]) * a.s[k];
-    if (gx != C(0) || gy != C(0)) {        // :614-626
-        const C ug = u * gx + v * gy;
-        d[1] += C(6) * (C(1) - C(0.5) * a.s[1]) * ug;
-        d[2] += C(-6) * (C(1) - C(0.5) * a.s[2]) * ug;
-        d[3] += gx;
-        d[4] += -(C(1) - C(0.5) * a.s[4]) * gx;
-        d[5] += gy;
-        d[6] += -(C(1) - C(0.5) * a.s[6]) * gy;
-        d[7] += C(2) * (C(1) - C(0.5) * a.s[7]) * (u * gx - v * gy);
-        d[8] += (C(1) - C(0.5) * a.s[8]) * (u * gy + v * gx);
-    }
-    mrt_inverse(d, gout);
-#pragma unroll
-    for (int k = 0; k < 9; ++k) gout[k] += g[k];
-    frho = rho; fu = u; fv = v;
-}
-
-// edge node: boundary_condition1 (boundary_condition.f90:413-853)
-template <typename T, typename C>
-__device__ __forceinline__ void edge_update(const KFArgs<C> &a, const T *__restrict__ fin, int i, int j, C gout[9],
-                                            C &frho, C &fu, C &fv)
-{
-    C g0n[9], drn, un, vn;
-    if (j == 0 || j == a.ny - 1) {
-        // top/bottom row: rho from the adjacent row, u = v = 0
-        // (boundary_condition.f90:658-716, 785-843)
-        const int jn = j == 0 ? 1 : a.ny - 2;
-        if (i == 0 || i == a.nx - 1) {
-            const int side = i == 0 ? 0 : 1;
-            C d2[9], dr2, u2, v2;
-            side_bc<T, C>(a, fin, side, jn, drn, un, vn, d2, dr2, u2, v2);
-            const C *c = a.corner + 9 * (2 * side + (j == 0 ? 0 : 1));
-#pragma unroll
-            for (int k = 0; k < 9; ++k) g0n[k] = c[k];   // edge f0, never rewritten
-        } else {
-            pull<T, C>(fin, a.plane, a.pitch, i, jn, g0n);
-            moments(g0n, drn, un, vn);
-        }
-        extrapolate_dev<C>(a.s, drn, C(0), C(0), drn, un, vn, g0n, gout);
-        frho = C(1) + drn; fu = C(0); fv = C(0);
-    } else {
-        // left/right column (boundary_condition.f90:413-483, 495-567)
-        const int side = i == 0 ? 0 : 1;
-        C dr1, u1, v1;
-        side_bc<T, C>(a, fin, side, j, dr1, u1, v1, g0n, drn, un, vn);
-        extrapolate_dev<C>(a.s, dr1, u1, v1, drn, un, vn, g0n, gout);
-        frho = C(1) + dr1; fu = u1; fv = v1;
-    }
-}
-
-// any node with scalar loads
-template <typename T, typename C>
-__device__ __forceinline__ void node_update(const KFArgs<C> &a, const PatchInfo &pi, const T *__restrict__ fin, int i,
-                                            int j, C gout[9], C &frho, C &fu, C &fv)
-{
-    if (i == 0 || i == a.nx - 1 || j == 0 || j == a.ny - 1) {
-        edge_update<T, C>(a, fin, i, j, gout, frho, fu, fv);
-    } else {
-        C g[9];
-        pull<T, C>(fin, a.plane, a.pitch, i, j, g);
-        collide_interior<C>(a, pi, g, i, j, gout, frho, fu, fv);
-    }
-}
-
-template <typename T, typename C, bool FIELDS>
-__device__ __forceinline__ void store_node(const KFArgs<C> &a, T *__restrict__ fout, int i, int j, const C gout[9],
-                                           C frho, C fu, C fv)
-{
-    const long long o = (long long)j * a.pitch + i;
-#pragma unroll
-    for (int k = 0; k < 9; ++k) Store<T>::st(fout + (long long)k * a.plane + o, gout[k]);
-    if (FIELDS) {
-        const long long q = (long long)j * a.nx + i;
-        a.rho_out[q] = frho;
-        a.u_out[q] = fu;
-        a.v_out[q] = fv;
-    }
-}
+// node-level device functions: lbm_node.cuh
 
 // one node per thread, scalar loads (any lattice size)
 template <typename T, typename C, bool FIELDS>
@@ -198,24 +39,12 @@ __global__ void __launch_bounds__(256) kf_kernel(const KFArgs<C> a)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     int j = blockIdx.y;
-    if (a.mode != KF_ALL) {   // split around the step's correction patch
-        const PatchInfo r = *a.pinfo;
-        if (a.mode == KF_INNER) {
-            if (i >= r.w || j >= r.h) return;
-            i += r.i0;
-            j += r.j0;
-        } else if ((unsigned)(i - r.i0) < (unsigned)r.w && (unsigned)(j - r.j0) < (unsigned)r.h) {
-            return;
-        }
-    }
+    if (a.mode == KF_OUTER && corr_tile(a, *a.pinfo, i, j)) return;
     if (i >= a.nx) return;
     const T *__restrict__ fin = (const T *)a.fin;
     T *__restrict__ fout = (T *)a.fout;
-    // the outer part runs while the IB kernels rewrite the patch: it reads
-    // neither (no outer node lies in any patch)
-    const PatchInfo pi = a.mode == KF_OUTER ? PatchInfo{0, 0, 0, 0} : *a.pinfo;
     C gout[9], frho, fu, fv;
-    node_update<T, C>(a, pi, fin, i, j, gout, frho, fu, fv);
+    node_update<T, C>(a, fin, i, j, gout, frho, fu, fv);
     store_node<T, C, FIELDS>(a, fout, i, j, gout, frho, fu, fv);
 }
 
@@ -239,7 +68,6 @@ __global__ void __launch_bounds__(128) kf_vec(const KFArgs<C> a)
     const int pitch = a.pitch, plane = (int)a.plane;
     // the outer part runs while the IB kernels rewrite the patch: it reads
     // neither (no outer node lies in any patch)
-    const PatchInfo pi = a.mode == KF_OUTER ? PatchInfo{0, 0, 0, 0} : *a.pinfo;
     if (j == 0 || j == a.ny - 1) {             // warp-uniform: edge rows
         for (int e = 0; e < VEC; ++e) {
             const int i = i0 + e;
@@ -287,7 +115,7 @@ __global__ void __launch_bounds__(128) kf_vec(const KFArgs<C> a)
                 g[k] = (C)Store<T>::cvt(t);
             }
             C gout[9], frho, fu, fv;
-            collide_interior<C>(a, pi, g, i0 + e, j, gout, frho, fu, fv);
+            collide_interior<C>(a, g, false, C(0), C(0), gout, frho, fu, fv);
 #pragma unroll
             for (int k = 0; k < 9; ++k) out[k][e] = Store<T>::pack(gout[k]);
             if (FIELDS) {
@@ -309,7 +137,7 @@ __global__ void __launch_bounds__(128) kf_vec(const KFArgs<C> a)
             const int i = i0 + e;
             if (i >= a.nx) break;
             C gout[9], frho, fu, fv;
-            node_update<T, C>(a, pi, fin, i, j, gout, frho, fu, fv);
+            node_update<T, C>(a, fin, i, j, gout, frho, fu, fv);
             store_node<T, C, FIELDS>(a, fout, i, j, gout, frho, fu, fv);
         }
     }
@@ -347,8 +175,7 @@ __global__ void __launch_bounds__(TW) kf_tma(const KFArgs<C> a)
     const int i = x0 + tid;
     const T *__restrict__ fin = (const T *)a.fin;
     T *__restrict__ fout = (T *)a.fout;
-    const PatchInfo pi = a.mode == KF_OUTER ? PatchInfo{0, 0, 0, 0} : *a.pinfo;
-    const PatchInfo rr = a.mode == KF_OUTER ? *a.pinfo : PatchInfo{0, 0, 0, 0};   // nodes the outer part skips
+    const PatchInfo rr = a.mode == KF_OUTER ? *a.pinfo : PatchInfo{0, 0, 0, 0};   // step's patch rectangle
     if (blockIdx.y == gridDim.y - 1) {
         // the edge nodes: rows 0 and ny-1 of this strip, and a share of the
         // nodes of columns 0 and nx-1 (which the strips' row sweeps skip)
@@ -405,14 +232,14 @@ __global__ void __launch_bounds__(TW) kf_tma(const KFArgs<C> a)
         const int s = r % KS, j = j0 + r;
         const uint32_t parity = (uint32_t)((r / KS) & 1);
         if (!wait(&full[s], parity)) { ok = false; break; }
-        const bool skip = (unsigned)(i - rr.i0) < (unsigned)rr.w && (unsigned)(j - rr.j0) < (unsigned)rr.h;
+        const bool skip = a.mode == KF_OUTER && corr_tile(a, rr, i, j);
         if (i > 0 && i < a.nx - 1 && !skip) {
             C gout[9], frho, fu, fv;
             C g[9];
             const T *row = buf + s * 9 * SEG + H + tid;
 #pragma unroll
             for (int k = 0; k < 9; ++k) g[k] = (C)Store<T>::cvt(row[k * SEG - lbm_ex(k)]);
-            collide_interior<C>(a, pi, g, i, j, gout, frho, fu, fv);
+            collide_interior<C>(a, g, false, C(0), C(0), gout, frho, fu, fv);
             store_node<T, C, FIELDS>(a, fout, i, j, gout, frho, fu, fv);
         }
         __syncwarp();
@@ -470,37 +297,11 @@ void launch_vec(const KFArgs<C> &a, bool fields, int nx, int ny, cudaStream_t st
 template <typename T, typename C>
 int launch_kf_t(lbm_handle *h, const void *fin, void *fout, void *fields, int mode, cudaStream_t st)
 {
-    KFArgs<C> a;
-    a.mode = mode;
-    a.fin = fin;
-    a.fout = fout;
-    a.nx = h->nx;
-    a.ny = h->ny;
-    a.pitch = h->pitch;
-    a.plane = h->plane;
-    for (int k = 0; k < 9; ++k) a.s[k] = (C)h->s[k];
-    a.cs = (C)((double)sqrtf(3.0f) / 3.0);   // boundary_condition.f90:304
-    const C *ec = (const C *)h->edge_c;
-    a.col_l = ec;
-    a.col_r = ec + 3 * h->ny;
-    a.corner = ec + 6 * h->ny;
-    a.pinfo = h->d_pinfo + h->pinfo_slot;
-    a.patch = (const C *)h->d_patch;
-    if (fields) {
-        C *fc = (C *)fields;
-        const long long nn = (long long)h->nx * h->ny;
-        a.rho_out = fc;
-        a.u_out = fc + nn;
-        a.v_out = fc + 2 * nn;
-    } else {
-        a.rho_out = a.u_out = a.v_out = nullptr;
-    }
+    KFArgs<C> a = make_kf_args<C>(h, fin, fout, fields, mode);
     const bool small_index = 9ll * h->plane < (1ll << 31) && (long long)h->nx * h->ny < (1ll << 31);
     const int vec = small_index ? h->kf_vec : 1;
-    a.rows_per_cta = h->kf_rows;
-    a.status = h->d_status;
     if (!st) st = h->stream;
-    if (h->kf_tma && mode != KF_INNER && h->ny >= 3) {
+    if (h->kf_tma && h->ny >= 3) {
         static bool configured = false;   // per process; the attribute is per function
         if (!configured) {
             if (configure_tma<T, C>()) return -1;
@@ -512,10 +313,7 @@ int launch_kf_t(lbm_handle *h, const void *fin, void *fout, void *fields, int mo
     } else if (mode == KF_ALL && vec == 2 && h->pitch % 2 == 0) {
         launch_vec<T, C, 2>(a, fields != nullptr, h->nx, h->ny, st);
     } else {
-        // the inner part covers the largest patch rectangle; its threads
-        // outside the step's rectangle return at once
-        const int wx = mode == KF_INNER ? h->patch_wmax : h->nx, wy = mode == KF_INNER ? h->patch_hmax : h->ny;
-        dim3 block(256, 1), grid((wx + 255) / 256, wy);
+        dim3 block(256, 1), grid((h->nx + 255) / 256, h->ny);
         if (fields)
             kf_kernel<T, C, true><<<grid, block, 0, st>>>(a);
         else

@@ -121,9 +121,8 @@ void free_ib(lbm_handle *h)
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->ib_ready = 0;
     h->batch_in_half[0] = h->batch_in_half[1] = -1;
-    free_dev(h->d_patch);
     free_devp(h->d_mk); free_devp(h->d_rhs); free_devp(h->d_B); free_devp(h->d_y); free_devp(h->d_partial);
-    free_devp(h->d_bD); free_devp(h->d_bL); free_devp(h->d_gf); free_devp(h->d_fmode); free_devp(h->d_fstatus); free_devp(h->d_tiles);
+    free_devp(h->d_bD); free_devp(h->d_bL); free_devp(h->d_gf); free_devp(h->d_fmode); free_devp(h->d_fstatus); free_devp(h->d_tiles); free_devp(h->d_nsup);
     free_devp(h->d_perm); free_devp(h->d_key); free_devp(h->d_reach); free_devp(h->d_wmax);
 }
 
@@ -171,10 +170,6 @@ int ensure_ib(lbm_handle *h)
         int y0 = std::max(1, (int)floor(gy0) - 1), y1 = std::min(h->ny - 1, (int)ceil(gy1) + 2);
         if (x1 > x0 && y1 > y0) { h->env_x0 = x0; h->env_y0 = y0; h->env_w = x1 - x0; h->env_h = y1 - y0; }
     }
-    h->patch_cap = std::max(1, wmax * hmax);
-    const size_t cs = compute_size(h->prec);
-    CK(cudaMalloc(&h->d_patch, 2 * cs * (size_t)h->patch_cap), "alloc patch");
-    CK(cudaMemsetAsync(h->d_patch, 0, 2 * cs * (size_t)h->patch_cap, h->stream), "clear patch");
     const int ns = std::max(1, h->nseg);
     const size_t S = (size_t)h->nslots, K = (size_t)h->fbatch;
     CK(cudaMalloc(&h->d_mk, S * sizeof(Marker) * ns), "alloc markers");
@@ -193,7 +188,11 @@ int ensure_ib(lbm_handle *h)
     // partials of the spread (per patch tile) and of the residual check (per 8 markers)
     const size_t npart = std::max((size_t)ib_partials_per_block() * nblk, 2 * (size_t)((ns + 7) / 8));
     CK(cudaMalloc(&h->d_partial, sizeof(double) * npart), "alloc partials");
-    CK(cudaMalloc(&h->d_tiles, S * sizeof(int) * ib_tile_ints() * (size_t)nblk), "alloc tile lists");
+    h->tiles_slot = (size_t)ib_tile_ints() * nblk;
+    CK(cudaMalloc(&h->d_tiles, S * sizeof(int) * h->tiles_slot), "alloc tile lists");
+    CK(cudaMemsetAsync(h->d_tiles, 0, S * sizeof(int) * h->tiles_slot, h->stream), "clear tile lists");
+    CK(cudaMalloc(&h->d_nsup, S * sizeof(int)), "alloc tile counts");
+    CK(cudaMemsetAsync(h->d_nsup, 0, S * sizeof(int), h->stream), "clear tile counts");
     // solve order of the markers: one rigid body keeps its markers sorted by
     // body-frame chordwise position for the whole run (two markers whose
     // support boxes overlap are less than 5*sqrt(2) lattice units apart in any
@@ -319,36 +318,39 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
         }
         cudaEvent_t *e = h->timing ? &h->ev[4 * slot] : nullptr;
         if (split) {
+            // side stream: the immersed-boundary chain and the correction
+            // tiles; main stream: every other node, concurrently
             if (h->batch_in_half[half] != b && (rc = factor_batch(b))) return rc;
             CK(cudaStreamWaitEvent(h->side, h->ev_inner, 0), "wait");
             CK(cudaStreamWaitEvent(h->side, h->ev_batch[half], 0), "wait");
             if (e) CK(cudaEventRecord(h->ev_side[2 * slot], h->side), "event");
-            if (launch_flow(h, fin, h->n, slot, q, h->side)) return cuda_err(h, cudaGetLastError(), "launch ib");
+            if (launch_flow(h, fin, fout, fields, h->n, slot, q, h->side)) return cuda_err(h, cudaGetLastError(), "launch ib");
             if (e) CK(cudaEventRecord(h->ev_side[2 * slot + 1], h->side), "event");
             CK(cudaEventRecord(h->ev_ib, h->side), "event");
             if (launch_check(h, q, h->side)) return cuda_err(h, cudaGetLastError(), "launch check");
             CK(cudaEventRecord(h->ev_free[half], h->side), "event");
             // the next batch's factorization, overlapping this batch's steps
             if ((b + 1) * K <= last_step && h->batch_in_half[half ^ 1] != b + 1 && (rc = factor_batch(b + 1))) return rc;
-            CK(cudaStreamWaitEvent(h->stream, h->ev_batch[half], 0), "wait");   // the step's patch rectangle
+            CK(cudaStreamWaitEvent(h->stream, h->ev_batch[half], 0), "wait");   // the step's correction tiles
             if (e) CK(cudaEventRecord(e[0], h->stream), "event");
             if (launch_kf(h, fin, fout, fields, KF_OUTER)) return cuda_err(h, cudaGetLastError(), "launch kf");
             if (e) CK(cudaEventRecord(e[1], h->stream), "event");
             CK(cudaStreamWaitEvent(h->stream, h->ev_ib, 0), "wait");
-            if (e) CK(cudaEventRecord(e[2], h->stream), "event");
-            if (launch_kf(h, fin, fout, fields, KF_INNER)) return cuda_err(h, cudaGetLastError(), "launch kf");
-            if (e) CK(cudaEventRecord(e[3], h->stream), "event");
-            CK(cudaEventRecord(h->ev_inner, h->stream), "event");
+            if (e) {
+                CK(cudaEventRecord(e[2], h->stream), "event");
+                CK(cudaEventRecord(e[3], h->stream), "event");
+            }
+            CK(cudaEventRecord(h->ev_inner, h->stream), "event");   // the step is complete
         } else {
             if (e) CK(cudaEventRecord(e[0], h->stream), "event");
             if (h->batch_in_half[half] != b && (rc = factor_batch(b))) return rc;
-            if (launch_flow(h, fin, h->n, slot, q, h->stream)) return cuda_err(h, cudaGetLastError(), "launch ib");
+            if (launch_flow(h, fin, fout, fields, h->n, slot, q, h->stream)) return cuda_err(h, cudaGetLastError(), "launch ib");
             if (launch_check(h, q, h->stream)) return cuda_err(h, cudaGetLastError(), "launch check");
             if (e) {
                 CK(cudaEventRecord(e[1], h->stream), "event");
                 CK(cudaEventRecord(e[2], h->stream), "event");
             }
-            if (launch_kf(h, fin, fout, fields)) return cuda_err(h, cudaGetLastError(), "launch kf");
+            if (launch_kf(h, fin, fout, fields, h->nseg > 0 ? KF_OUTER : KF_ALL)) return cuda_err(h, cudaGetLastError(), "launch kf");
             if (e) CK(cudaEventRecord(e[3], h->stream), "event");
         }
         h->cur ^= 1;

@@ -27,14 +27,13 @@ struct KFArgs {
     C s[9];
     C cs;
     const C *col_l, *col_r, *corner;   // edge constants in compute precision
-    const PatchInfo *pinfo;
-    const C *patch;                    // interleaved (du, dv) per patch node
+    const PatchInfo *pinfo;            // the step's patch rectangle (KF_OUTER)
+    const int *tiles;                  // the step's tile lists: count per 16 x 16 tile (KF_OUTER)
+    int tiles_x, tile_stride;          // tiles per rectangle row; ints per tile
     C *rho_out, *u_out, *v_out;        // fields, when requested (else null)
-    int mode;                          // KF_ALL, KF_OUTER (skip rect), KF_INNER (rect only)
+    int mode;                          // KF_ALL, or KF_OUTER (all but the correction tiles)
     int rows_per_cta;                  // row sweep length of the staged kernel
     unsigned *status;                  // device status word (bounded-wait timeouts)
-    // split modes: the outer part skips, and the inner part covers, the
-    // step's correction patch rectangle *pinfo
 };
 
 #define LBM_NSLOT_MAX 16   // largest slot count of the factorization batches
@@ -42,7 +41,6 @@ struct KFArgs {
 
 #define KF_ALL 0
 #define KF_OUTER 1
-#define KF_INNER 2
 
 // arguments of the immersed-boundary kernels
 struct IBArgs {
@@ -79,9 +77,8 @@ struct IBArgs {
     int *tiles;         // per patch tile: marker count, then the listed markers (slot)
     int tiles_x;        // tiles per patch row
     long long st_tiles; // ints per slot of the tile lists
-    void *patch;        // compute-precision (du, dv) pairs
-    int patch_cap;      // nodes
-    int patch_wmax, patch_hmax;  // rectangle the spread grid covers
+    int patch_wmax, patch_hmax;  // largest patch rectangle (the tile grid covers it)
+    int *nsup;          // number of correction tiles (tiles listing a marker) of the slot's step
     double *partial;    // per-block force partials
     unsigned *counter;  // last-block counter
     double *force_ring; // [ring_cap][row_len]
@@ -139,9 +136,9 @@ struct lbm_handle {
     int static_order = 0;   // one rigid body: fixed body-frame marker order
     PatchInfo *d_pinfo = nullptr;   // LBM_NSLOT_MAX slots (patch rectangle of the slot's step)
     int *d_tiles = nullptr;         // nslots x tile lists of the patch grid
+    size_t tiles_slot = 0;          // ints per slot of d_tiles
+    int *d_nsup = nullptr;          // nslots: correction tiles of the slot's step
     int pinfo_slot = 0;             // slot the next lattice launch reads
-    void *d_patch = nullptr;
-    int patch_cap = 0;               // nodes
     int patch_wmax = 0, patch_hmax = 0;
     int patch_gx() const { return patch_wmax > 0 ? (patch_wmax + 15) / 16 : 1; }
     int patch_gy() const { return patch_hmax > 0 ? (patch_hmax + 15) / 16 : 1; }
@@ -194,7 +191,8 @@ int ib_partials_per_block();
 void ib_factor_scratch(int nseg, size_t *work_blocks, size_t *factor_slot);
 int launch_kf(lbm_handle *h, const void *fin, void *fout, void *fields, int mode = KF_ALL, cudaStream_t st = nullptr);
 int launch_factor(lbm_handle *h, int step0, int count, cudaStream_t st);
-int launch_flow(lbm_handle *h, const void *fin, int step_index, int ring_slot, int slot, cudaStream_t st);
+int launch_flow(lbm_handle *h, const void *fin, void *fout, void *fields, int step_index, int ring_slot, int slot,
+                cudaStream_t st);
 int launch_check(lbm_handle *h, int slot, cudaStream_t st);
 int ib_tile_ints();   // ints per patch tile of the tile lists
 int launch_residual(lbm_handle *h, const void *fa, const void *fb, double *out2);
