@@ -25,8 +25,9 @@
 //               apart per axis), so the CTA builds its diagonal block and the
 //               block coupling it to the previous one, and checks that no
 //               coupling reaches further;
-//   ib_tiles    per 16 x 16 tile of the patch rectangle, the markers whose
-//               support box meets it;
+//   ib_tile_scatter, ib_tile_sort  per 16 x 16 tile of the patch
+//               rectangle, the markers whose support box meets it (each
+//               marker appends itself; each tile sorts its list);
 //   ib_factor   one CTA: correction-patch rectangle, then block cyclic
 //               reduction of the block tridiagonal matrix (log2 of the block
 //               count levels of Gauss-Jordan block inverses and block
@@ -611,6 +612,8 @@ __global__ void __launch_bounds__(FACTOR_THREADS) ib_factor(const IBArgs base, i
         }
         if (lane == 0) { atomicMin(&bb[0], b0); atomicMin(&bb[1], b1); atomicMax(&bb[2], b2); atomicMax(&bb[3], b3); }
     }
+    for (long long t = tid; t < a.st_tiles / (TILE_CAP + 1); t += blockDim.x)
+        a.tiles[t * (TILE_CAP + 1)] = 0;   // tile counts, for ib_tile_scatter
     __syncthreads();
     if (tid == 0) {
         PatchInfo pi{0, 0, 0, 0};
@@ -622,7 +625,7 @@ __global__ void __launch_bounds__(FACTOR_THREADS) ib_factor(const IBArgs base, i
             }
         }
         *a.pinfo = pi;
-        *a.nsup = 0;   // counted by ib_tiles
+        *a.nsup = 0;   // counted by ib_tile_sort
         const int w = *a.wmax;
         bad = 0;
         dense = (w > BS || a.force_dense) ? 1 : 0;
@@ -936,54 +939,55 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
     }
 }
 
-// Markers whose support box meets each tile of the step's correction patch,
-// in increasing marker index (the order of the spread's sums), one CTA per
-// tile; geometry only, so part of the factorization chain. Layout per tile:
-// count, then up to TILE_CAP marker indices; a larger count tells the
-// spread to scan all markers for that tile.
-__global__ void __launch_bounds__(256) ib_tiles(const IBArgs base, int step0)
+// Markers whose support box meets each 16 x 16 tile of the step's patch
+// rectangle. Layout per tile: count, then up to TILE_CAP marker indices in
+// increasing order (the order of the tile update's sums); a larger count
+// tells the tile update to scan all markers for that tile. Geometry only, so
+// part of the factorization chain, in two passes: each marker appends itself
+// to the (at most 2 x 2) tiles its box meets, then each tile sorts its list.
+// ib_factor has cleared the counts.
+__global__ void __launch_bounds__(256) ib_tile_scatter(const IBArgs base, int step0)
 {
     const IBArgs a = member_args(base, step0 + blockIdx.y);
-    __shared__ int wsum[8];
-    __shared__ int total;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.nseg) return;
     const PatchInfo pi = *a.pinfo;
-    const int tx = blockIdx.x % a.tiles_x, ty = blockIdx.x / a.tiles_x;
+    const int4 q = mbox(a.mk[k]);
+    if (q.y < q.x || q.w < q.z || pi.w <= 0) return;
+    const int tx0 = (q.x - pi.i0) / TILE, tx1 = (q.y - pi.i0) / TILE;
+    const int ty0 = (q.z - pi.j0) / TILE, ty1 = (q.w - pi.j0) / TILE;
+    for (int ty = ty0; ty <= ty1; ++ty)
+        for (int tx = tx0; tx <= tx1; ++tx) {
+            int *list = a.tiles + (long long)(ty * a.tiles_x + tx) * (TILE_CAP + 1);
+            const int pos = atomicAdd(list, 1);
+            if (pos < TILE_CAP) list[1 + pos] = k;
+        }
+}
+
+__global__ void __launch_bounds__(TILE_CAP) ib_tile_sort(const IBArgs base, int step0)
+{
+    const IBArgs a = member_args(base, step0 + blockIdx.y);
+    __shared__ int key[TILE_CAP];
     int *list = a.tiles + (long long)blockIdx.x * (TILE_CAP + 1);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (threadIdx.x == 0) total = 0;
+    const int count = list[0];
+    if (count == 0) return;
+    if (threadIdx.x == 0) atomicAdd(a.nsup, 1);
+    const int m = min(count, TILE_CAP);
+    const int t = threadIdx.x;
+    key[t] = t < m ? list[1 + t] : 0x7fffffff;
     __syncthreads();
-    const int ti0 = tx * TILE, tj0 = ty * TILE;
-    if (ti0 >= pi.w || tj0 >= pi.h) {
-        if (threadIdx.x == 0) list[0] = 0;
-        return;
-    }
-    const int ta = pi.i0 + ti0, tb = ta + TILE - 1, sa_ = pi.j0 + tj0, sb_ = sa_ + TILE - 1;
-    for (int c0 = 0; c0 < a.nseg; c0 += 256) {
-        const int k = c0 + threadIdx.x;
-        bool hit = false;
-        if (k < a.nseg) {
-            const int4 q = mbox(a.mk[k]);
-            hit = q.x <= tb && q.y >= ta && q.z <= sb_ && q.w >= sa_ && q.y >= q.x;
+    // bitonic sort of TILE_CAP keys, ascending
+    for (int size = 2; size <= TILE_CAP; size <<= 1)
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            const int u = t ^ stride;
+            if (u > t) {
+                const bool up = (t & size) == 0;
+                const int x = key[t], y = key[u];
+                if ((x > y) == up) { key[t] = y; key[u] = x; }
+            }
+            __syncthreads();
         }
-        const unsigned bal = __ballot_sync(0xffffffffu, hit);
-        if (lane == 0) wsum[warp] = __popc(bal);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int acc = total;
-            for (int w = 0; w < 8; ++w) { const int t = wsum[w]; wsum[w] = acc; acc += t; }
-            total = acc;
-        }
-        __syncthreads();
-        if (hit) {
-            const int slot = wsum[warp] + __popc(bal & ((1u << lane) - 1u));
-            if (slot < TILE_CAP) list[1 + slot] = k;
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        list[0] = total;
-        if (total > 0) atomicAdd(a.nsup, 1);
-    }
+    if (t < m) list[1 + t] = key[t];
 }
 
 // Residual of the step's solve, ||B y - rhs|| / ||rhs|| with B = D D^T
@@ -1385,8 +1389,9 @@ int launch_factor(lbm_handle *h, int step0, int count, cudaStream_t st)
     if (!h->static_order) ib_order<<<dim3(1, count), 1024, order_smem(h->nseg), st>>>(a, step0);
     ib_assemble<<<dim3(nb, count), 256, 0, st>>>(a, step0);
     ib_factor<<<dim3(1, count), FACTOR_THREADS, kFactorSmem, st>>>(a, step0);
-    ib_tiles<<<dim3(h->patch_gx() * h->patch_gy(), count), 256, 0, st>>>(a, step0);
-    h->launches += h->static_order ? 4 : 5;
+    ib_tile_scatter<<<dim3((h->nseg + 255) / 256, count), 256, 0, st>>>(a, step0);
+    ib_tile_sort<<<dim3(h->patch_gx() * h->patch_gy(), count), TILE_CAP, 0, st>>>(a, step0);
+    h->launches += h->static_order ? 5 : 6;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

@@ -89,8 +89,8 @@ def test_launch_count_per_step(gpu_lib):
     """Per step of one rigid wing: the flow chain (interpolation, solve,
     spread, residual check) and one or two lattice kernels (two when the
     lattice update is split around the body's envelope); plus, per batch of
-    steps, the four kernels of the batched factorization of the marker system
-    (geometry, band assembly, factorization, patch-tile lists)."""
+    steps, the five kernels of the batched factorization of the marker system
+    (geometry, band assembly, factorization, patch-tile lists in two passes)."""
     import ctypes as C
     case = cases.small_case(precision="fp32", n_steps=100)
     g = Lbm.from_case(case, gpu_lib)
@@ -102,8 +102,8 @@ def test_launch_count_per_step(gpu_lib):
     gpu_lib.lbm_get_launch_count(g.h, C.byref(n1))
     total = n1.value - n0.value
     fits = [kf for kf in (1, 2)
-            if total >= steps * (4 + kf) and (total - steps * (4 + kf)) % 4 == 0
-            and 1 <= (total - steps * (4 + kf)) // 4 <= steps]
+            if total >= steps * (4 + kf) and (total - steps * (4 + kf)) % 5 == 0
+            and 1 <= (total - steps * (4 + kf)) // 5 <= steps]
     assert fits, total
 
 
