@@ -144,6 +144,7 @@ __device__ __forceinline__ IBArgs member_args(IBArgs a, int step)
     a.gf += slot * a.wk_gf;
     a.pinfo += slot;
     a.tiles += slot * a.st_tiles;
+    a.ctile += slot * (a.st_tiles / (TILE_CAP + 1));
     a.nsup += slot;
     a.fmode += 2 * slot;
     a.fstatus += slot;
@@ -625,7 +626,7 @@ __global__ void __launch_bounds__(FACTOR_THREADS) ib_factor(const IBArgs base, i
             }
         }
         *a.pinfo = pi;
-        *a.nsup = 0;   // counted by ib_tile_sort
+        *a.nsup = 0;   // counted by ib_tile_scatter
         const int w = *a.wmax;
         bad = 0;
         dense = (w > BS || a.force_dense) ? 1 : 0;
@@ -958,9 +959,11 @@ __global__ void __launch_bounds__(256) ib_tile_scatter(const IBArgs base, int st
     const int ty0 = (q.z - pi.j0) / TILE, ty1 = (q.w - pi.j0) / TILE;
     for (int ty = ty0; ty <= ty1; ++ty)
         for (int tx = tx0; tx <= tx1; ++tx) {
-            int *list = a.tiles + (long long)(ty * a.tiles_x + tx) * (TILE_CAP + 1);
+            const int tile = ty * a.tiles_x + tx;
+            int *list = a.tiles + (long long)tile * (TILE_CAP + 1);
             const int pos = atomicAdd(list, 1);
             if (pos < TILE_CAP) list[1 + pos] = k;
+            if (pos == 0) a.ctile[atomicAdd(a.nsup, 1)] = tile;   // first marker of the tile
         }
 }
 
@@ -968,26 +971,26 @@ __global__ void __launch_bounds__(TILE_CAP) ib_tile_sort(const IBArgs base, int 
 {
     const IBArgs a = member_args(base, step0 + blockIdx.y);
     __shared__ int key[TILE_CAP];
-    int *list = a.tiles + (long long)blockIdx.x * (TILE_CAP + 1);
-    const int count = list[0];
-    if (count == 0) return;
-    if (threadIdx.x == 0) atomicAdd(a.nsup, 1);
-    const int m = min(count, TILE_CAP);
-    const int t = threadIdx.x;
-    key[t] = t < m ? list[1 + t] : 0x7fffffff;
-    __syncthreads();
-    // bitonic sort of TILE_CAP keys, ascending
-    for (int size = 2; size <= TILE_CAP; size <<= 1)
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            const int u = t ^ stride;
-            if (u > t) {
-                const bool up = (t & size) == 0;
-                const int x = key[t], y = key[u];
-                if ((x > y) == up) { key[t] = y; key[u] = x; }
+    const int ntile = *a.nsup, t = threadIdx.x;
+    for (int c = blockIdx.x; c < ntile; c += gridDim.x) {
+        int *list = a.tiles + (long long)a.ctile[c] * (TILE_CAP + 1);
+        const int m = min(list[0], TILE_CAP);
+        key[t] = t < m ? list[1 + t] : 0x7fffffff;
+        __syncthreads();
+        // bitonic sort of TILE_CAP keys, ascending
+        for (int size = 2; size <= TILE_CAP; size <<= 1)
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                const int u = t ^ stride;
+                if (u > t) {
+                    const bool up = (t & size) == 0;
+                    const int x = key[t], y = key[u];
+                    if ((x > y) == up) { key[t] = y; key[u] = x; }
+                }
+                __syncthreads();
             }
-            __syncthreads();
-        }
-    if (t < m) list[1 + t] = key[t];
+        if (t < m) list[1 + t] = key[t];
+        __syncthreads();
+    }
 }
 
 // Residual of the step's solve, ||B y - rhs|| / ||rhs|| with B = D D^T
@@ -1074,78 +1077,41 @@ __global__ void __launch_bounds__(256) ib_tile_update(const IBArgs a, const KFAr
     __shared__ int nlist;
     __shared__ double red[8][NPART];
     __shared__ bool amlast;
-    // markers whose support box meets this tile, staged in marker order
+    // markers whose support box meets the current tile, staged in marker order
     __shared__ int4 sbox[256];
     __shared__ double sph[256][12];
     __shared__ double sy[256][2];
     __shared__ int swing[256];
+    const int ntile = *a.nsup;
+    if (ntile == 0) return;   // no correction tile (ib_solve wrote the zero forces)
     const PatchInfo pi = *a.pinfo;
-    const int ti0 = blockIdx.x * TILE, tj0 = blockIdx.y * TILE;
-    if (ti0 >= pi.w || tj0 >= pi.h) return;
-    const int *tlist = a.tiles + (long long)(blockIdx.y * gridDim.x + blockIdx.x) * (TILE_CAP + 1);
-    const int listed = tlist[0];
-    if (listed == 0) return;   // not a correction tile: the lattice kernel updates it
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    const int li = ti0 + tx, lj = tj0 + ty;                    // patch-relative
-    const int gi = pi.i0 + li, gj = pi.j0 + lj;                // 0-based node
-    const bool active = li < pi.w && lj < pi.h;
-    const bool tile_active = true;
-    const int ta = pi.i0 + ti0, tb = ta + TILE - 1, sa_ = pi.j0 + tj0, sb_ = sa_ + TILE - 1;
-    double du = 0.0, dv = 0.0;
-    int wing = 1 << 20;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (listed <= TILE_CAP) {
-        // markers listed for this tile by the factorization chain
-        if (threadIdx.x == 0) nlist = listed;
-        if ((int)threadIdx.x < listed) {
-            const int k = tlist[1 + threadIdx.x];
-            const Marker &m = a.mk[k];
-            sbox[threadIdx.x] = mbox(m);
-#pragma unroll
-            for (int c = 0; c < 6; ++c) { sph[threadIdx.x][c] = m.phx[c]; sph[threadIdx.x][6 + c] = m.phy[c]; }
-            sy[threadIdx.x][0] = a.y[k];
-            sy[threadIdx.x][1] = a.y[a.nseg + k];
-            swing[threadIdx.x] = m.wing;
-        }
-        __syncthreads();
-        if (active) {
-            for (int t = 0; t < nlist; ++t) {
-                const int4 b = sbox[t];
-                if (gi >= b.x && gi <= b.y && gj >= b.z && gj <= b.w) {
-                    const double wgt = sph[t][gi - b.x] * sph[t][6 + gj - b.z];
-                    du += wgt * sy[t][0];
-                    dv += wgt * sy[t][1];
-                    wing = min(wing, swing[t]);
-                }
-            }
-        }
-    } else if (tile_active) {
-        for (int c0 = 0; c0 < a.nseg; c0 += 256) {
-            const int k = c0 + threadIdx.x;
-            bool hit = false;
-            int4 q = make_int4(1, 0, 1, 0);
-            if (k < a.nseg) {
-                q = mbox(a.mk[k]);
-                hit = q.x <= tb && q.y >= ta && q.z <= sb_ && q.w >= sa_ && q.y >= q.x;
-            }
-            const unsigned bal = __ballot_sync(0xffffffffu, hit);
-            if (lane == 0) wsum[warp] = __popc(bal);
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                int acc = 0;
-                for (int w = 0; w < 8; ++w) { const int t = wsum[w]; wsum[w] = acc; acc += t; }
-                nlist = acc;
-            }
-            __syncthreads();
-            if (hit) {
-                const int slot = wsum[warp] + __popc(bal & ((1u << lane) - 1u));
+    // the correction tiles, strided over the CTAs (the compact list is in no
+    // particular order; each tile's result depends on the tile only)
+    for (int c = blockIdx.x; c < ntile; c += gridDim.x) {
+        const int tile = a.ctile[c];
+        const int ti0 = (tile % a.tiles_x) * TILE, tj0 = (tile / a.tiles_x) * TILE;
+        const int *tlist = a.tiles + (long long)tile * (TILE_CAP + 1);
+        const int listed = tlist[0];
+        const int li = ti0 + tx, lj = tj0 + ty;                    // patch-relative
+        const int gi = pi.i0 + li, gj = pi.j0 + lj;                // 0-based node
+        const bool active = li < pi.w && lj < pi.h;
+        const int ta = pi.i0 + ti0, tb = ta + TILE - 1, sa_ = pi.j0 + tj0, sb_ = sa_ + TILE - 1;
+        double du = 0.0, dv = 0.0;
+        int wing = 1 << 20;
+        if (listed <= TILE_CAP) {
+            // markers listed for this tile by the factorization chain
+            if (threadIdx.x == 0) nlist = listed;
+            if ((int)threadIdx.x < listed) {
+                const int k = tlist[1 + threadIdx.x];
                 const Marker &m = a.mk[k];
-                sbox[slot] = q;
+                sbox[threadIdx.x] = mbox(m);
 #pragma unroll
-                for (int c = 0; c < 6; ++c) { sph[slot][c] = m.phx[c]; sph[slot][6 + c] = m.phy[c]; }
-                sy[slot][0] = a.y[k];
-                sy[slot][1] = a.y[a.nseg + k];
-                swing[slot] = m.wing;
+                for (int q = 0; q < 6; ++q) { sph[threadIdx.x][q] = m.phx[q]; sph[threadIdx.x][6 + q] = m.phy[q]; }
+                sy[threadIdx.x][0] = a.y[k];
+                sy[threadIdx.x][1] = a.y[a.nseg + k];
+                swing[threadIdx.x] = m.wing;
             }
             __syncthreads();
             if (active) {
@@ -1159,67 +1125,109 @@ __global__ void __launch_bounds__(256) ib_tile_update(const IBArgs a, const KFAr
                     }
                 }
             }
-            __syncthreads();
-        }
-    }
-    // lattice update of the node with the correction, and its force and moment
-    double fx = 0, fy = 0, mz = 0;
-    const bool in_support = active && wing < (1 << 20);
-    if (active) {
-        const T *__restrict__ fin = (const T *)kf.fin;
-        C g[9];
-        lbm_node::pull<T, C>(fin, kf.plane, kf.pitch, gi, gj, g);
-        C gout[9], frho, fu, fv;
-        lbm_node::collide_interior<C>(kf, g, true, (C)du, (C)dv, gout, frho, fu, fv);
-        lbm_node::store_node<T, C, FIELDS>(kf, (T *)kf.fout, gi, gj, gout, frho, fu, fv);
-        if (in_support) {
-            // FP64 density of the same streamed populations
-            const double drho = (((double)g[0] + (double)g[1]) + ((double)g[2] + (double)g[3])) +
-                                (((double)g[4] + (double)g[5]) + ((double)g[6] + (double)g[7])) + (double)g[8];
-            const double rho = 1.0 + drho;
-            const double *row = motion_row(a, step_index, nullptr);
-            const double temp1 = 2.0 * rho * du, temp2 = 2.0 * rho * dv;
-            const double sa = row[4 + 9 * wing], sb = row[7 + 9 * wing];
-            fx = -temp1;
-            fy = -temp2;
-            const double x0 = (a.ox + a.scale * (double)gi - (a.xc + sa)) / a.scale;
-            const double y0 = (a.oy + a.scale * (double)gj - (a.yc + sb)) / a.scale;
-            mz = -x0 * temp2 + y0 * temp1;
-        }
-    }
-    // deterministic block reduction per wing
-    for (int w = 0; w < a.nwing; ++w) {
-        double v0 = (in_support && wing == w) ? fx : 0.0;
-        double v1 = (in_support && wing == w) ? fy : 0.0;
-        double v2 = (in_support && wing == w) ? mz : 0.0;
+        } else {
+            // more markers than a list holds: scan all of them, in order
+            for (int c0 = 0; c0 < a.nseg; c0 += 256) {
+                const int k = c0 + threadIdx.x;
+                bool hit = false;
+                int4 q = make_int4(1, 0, 1, 0);
+                if (k < a.nseg) {
+                    q = mbox(a.mk[k]);
+                    hit = q.x <= tb && q.y >= ta && q.z <= sb_ && q.w >= sa_ && q.y >= q.x;
+                }
+                const unsigned bal = __ballot_sync(0xffffffffu, hit);
+                if (lane == 0) wsum[warp] = __popc(bal);
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    int acc = 0;
+                    for (int w = 0; w < 8; ++w) { const int t = wsum[w]; wsum[w] = acc; acc += t; }
+                    nlist = acc;
+                }
+                __syncthreads();
+                if (hit) {
+                    const int slot = wsum[warp] + __popc(bal & ((1u << lane) - 1u));
+                    const Marker &m = a.mk[k];
+                    sbox[slot] = q;
 #pragma unroll
-        for (int off = 16; off; off >>= 1) {
-            v0 += __shfl_down_sync(0xffffffffu, v0, off);
-            v1 += __shfl_down_sync(0xffffffffu, v1, off);
-            v2 += __shfl_down_sync(0xffffffffu, v2, off);
+                    for (int r = 0; r < 6; ++r) { sph[slot][r] = m.phx[r]; sph[slot][6 + r] = m.phy[r]; }
+                    sy[slot][0] = a.y[k];
+                    sy[slot][1] = a.y[a.nseg + k];
+                    swing[slot] = m.wing;
+                }
+                __syncthreads();
+                if (active) {
+                    for (int t = 0; t < nlist; ++t) {
+                        const int4 b = sbox[t];
+                        if (gi >= b.x && gi <= b.y && gj >= b.z && gj <= b.w) {
+                            const double wgt = sph[t][gi - b.x] * sph[t][6 + gj - b.z];
+                            du += wgt * sy[t][0];
+                            dv += wgt * sy[t][1];
+                            wing = min(wing, swing[t]);
+                        }
+                    }
+                }
+                __syncthreads();
+            }
         }
-        if (lane == 0) { red[warp][3 * w] = v0; red[warp][3 * w + 1] = v1; red[warp][3 * w + 2] = v2; }
-    }
-    __syncthreads();
-    const int nblk = gridDim.x * gridDim.y, bid = blockIdx.y * gridDim.x + blockIdx.x;
-    if (threadIdx.x < 3 * a.nwing) {
-        double s = 0.0;
-        for (int w8 = 0; w8 < 8; ++w8) s += red[w8][threadIdx.x];
-        a.partial[(long long)bid * NPART + threadIdx.x] = s;
+        // lattice update of the node with the correction, and its force and moment
+        double fx = 0, fy = 0, mz = 0;
+        const bool in_support = active && wing < (1 << 20);
+        if (active) {
+            const T *__restrict__ fin = (const T *)kf.fin;
+            C g[9];
+            lbm_node::pull<T, C>(fin, kf.plane, kf.pitch, gi, gj, g);
+            C gout[9], frho, fu, fv;
+            lbm_node::collide_interior<C>(kf, g, true, (C)du, (C)dv, gout, frho, fu, fv);
+            lbm_node::store_node<T, C, FIELDS>(kf, (T *)kf.fout, gi, gj, gout, frho, fu, fv);
+            if (in_support) {
+                // FP64 density of the same streamed populations
+                const double drho = (((double)g[0] + (double)g[1]) + ((double)g[2] + (double)g[3])) +
+                                    (((double)g[4] + (double)g[5]) + ((double)g[6] + (double)g[7])) + (double)g[8];
+                const double rho = 1.0 + drho;
+                const double *row = motion_row(a, step_index, nullptr);
+                const double temp1 = 2.0 * rho * du, temp2 = 2.0 * rho * dv;
+                const double sa = row[4 + 9 * wing], sb = row[7 + 9 * wing];
+                fx = -temp1;
+                fy = -temp2;
+                const double x0 = (a.ox + a.scale * (double)gi - (a.xc + sa)) / a.scale;
+                const double y0 = (a.oy + a.scale * (double)gj - (a.yc + sb)) / a.scale;
+                mz = -x0 * temp2 + y0 * temp1;
+            }
+        }
+        // deterministic tile reduction per wing, into the tile's partials
+        for (int w = 0; w < a.nwing; ++w) {
+            double v0 = (in_support && wing == w) ? fx : 0.0;
+            double v1 = (in_support && wing == w) ? fy : 0.0;
+            double v2 = (in_support && wing == w) ? mz : 0.0;
+#pragma unroll
+            for (int off = 16; off; off >>= 1) {
+                v0 += __shfl_down_sync(0xffffffffu, v0, off);
+                v1 += __shfl_down_sync(0xffffffffu, v1, off);
+                v2 += __shfl_down_sync(0xffffffffu, v2, off);
+            }
+            if (lane == 0) { red[warp][3 * w] = v0; red[warp][3 * w + 1] = v1; red[warp][3 * w + 2] = v2; }
+        }
+        __syncthreads();
+        if (threadIdx.x < 3 * a.nwing) {
+            double sum = 0.0;
+            for (int w8 = 0; w8 < 8; ++w8) sum += red[w8][threadIdx.x];
+            a.partial[(long long)tile * NPART + threadIdx.x] = sum;
+        }
+        __syncthreads();   // shared arrays are reused by the next tile
     }
     __threadfence();
     __syncthreads();
-    if (threadIdx.x == 0) amlast = atomicAdd(a.counter, 1u) == (unsigned)(*a.nsup - 1);
+    if (threadIdx.x == 0) amlast = atomicAdd(a.counter, 1u) == gridDim.x - 1;
     __syncthreads();
     if (!amlast) return;
     __threadfence();
-    // last block: every thread sums a fixed strided subset of the block
-    // partials, then a fixed warp/block tree (deterministic order)
+    // last CTA: every thread sums a fixed strided subset of the tiles'
+    // partials, in tile order, then a fixed warp/block tree
+    const int ntiles_all = (int)(a.st_tiles / (TILE_CAP + 1));
     for (int w = 0; w < a.nwing; ++w) {
         double s0 = 0, s1 = 0, s2 = 0;
-        for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
-            const int bx = b % gridDim.x, by = b / gridDim.x;
-            if (bx * TILE >= pi.w || by * TILE >= pi.h || a.tiles[(long long)b * (TILE_CAP + 1)] == 0) continue;
+        for (int b = threadIdx.x; b < ntiles_all; b += blockDim.x) {
+            if (a.tiles[(long long)b * (TILE_CAP + 1)] == 0) continue;
             const double *p = a.partial + (long long)b * NPART + 3 * w;
             s0 += __ldcg(p); s1 += __ldcg(p + 1); s2 += __ldcg(p + 2);
         }
@@ -1308,6 +1316,7 @@ IBArgs make_args(lbm_handle *h, const void *fin, int slot)
     a.bD = h->d_bD; a.bL = h->d_bL;
     a.reach = h->d_reach; a.wmax = h->d_wmax;
     a.nsup = h->d_nsup + slot;
+    a.ctile = h->d_ctile + slot * (a.st_tiles / (TILE_CAP + 1));
     a.patch_wmax = h->patch_wmax; a.patch_hmax = h->patch_hmax;
     a.partial = h->d_partial; a.counter = h->d_counter;
     a.force_ring = h->d_ring; a.row_len = h->row_len;
@@ -1325,7 +1334,7 @@ int launch_flow_t(lbm_handle *h, const void *fin, void *fout, void *fields, int 
         h->launches += 1;
     }
     ib_solve<<<1, SOLVE_THREADS, solve_smem(h->nseg), st>>>(a, step_index, ring_slot);
-    dim3 grid(h->patch_gx(), h->patch_gy());
+    const int grid = std::min(h->patch_gx() * h->patch_gy(), 2 * 148);   // strided over the correction tiles
     const KFArgs<C> kf = make_kf_args<C>(h, fin, fout, fields, KF_OUTER);
     if (fields)
         ib_tile_update<T, C, true><<<grid, 256, 0, st>>>(a, kf, step_index, ring_slot);
@@ -1390,7 +1399,7 @@ int launch_factor(lbm_handle *h, int step0, int count, cudaStream_t st)
     ib_assemble<<<dim3(nb, count), 256, 0, st>>>(a, step0);
     ib_factor<<<dim3(1, count), FACTOR_THREADS, kFactorSmem, st>>>(a, step0);
     ib_tile_scatter<<<dim3((h->nseg + 255) / 256, count), 256, 0, st>>>(a, step0);
-    ib_tile_sort<<<dim3(h->patch_gx() * h->patch_gy(), count), TILE_CAP, 0, st>>>(a, step0);
+    ib_tile_sort<<<dim3(std::min(h->patch_gx() * h->patch_gy(), 148), count), TILE_CAP, 0, st>>>(a, step0);
     h->launches += h->static_order ? 5 : 6;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -122,7 +122,7 @@ void free_ib(lbm_handle *h)
     h->ib_ready = 0;
     h->batch_in_half[0] = h->batch_in_half[1] = -1;
     free_devp(h->d_mk); free_devp(h->d_rhs); free_devp(h->d_B); free_devp(h->d_y); free_devp(h->d_partial);
-    free_devp(h->d_bD); free_devp(h->d_bL); free_devp(h->d_gf); free_devp(h->d_fmode); free_devp(h->d_fstatus); free_devp(h->d_tiles); free_devp(h->d_nsup);
+    free_devp(h->d_bD); free_devp(h->d_bL); free_devp(h->d_gf); free_devp(h->d_fmode); free_devp(h->d_fstatus); free_devp(h->d_tiles); free_devp(h->d_nsup); free_devp(h->d_ctile);
     free_devp(h->d_perm); free_devp(h->d_key); free_devp(h->d_reach); free_devp(h->d_wmax);
 }
 
@@ -192,6 +192,7 @@ int ensure_ib(lbm_handle *h)
     CK(cudaMalloc(&h->d_tiles, S * sizeof(int) * h->tiles_slot), "alloc tile lists");
     CK(cudaMemsetAsync(h->d_tiles, 0, S * sizeof(int) * h->tiles_slot, h->stream), "clear tile lists");
     CK(cudaMalloc(&h->d_nsup, S * sizeof(int)), "alloc tile counts");
+    CK(cudaMalloc(&h->d_ctile, S * sizeof(int) * (size_t)nblk), "alloc correction tiles");
     CK(cudaMemsetAsync(h->d_nsup, 0, S * sizeof(int), h->stream), "clear tile counts");
     // solve order of the markers: one rigid body keeps its markers sorted by
     // body-frame chordwise position for the whole run (two markers whose

@@ -79,6 +79,7 @@ struct IBArgs {
     long long st_tiles; // ints per slot of the tile lists
     int patch_wmax, patch_hmax;  // largest patch rectangle (the tile grid covers it)
     int *nsup;          // number of correction tiles (tiles listing a marker) of the slot's step
+    int *ctile;         // their tile indices, in no particular order
     double *partial;    // per-block force partials
     unsigned *counter;  // last-block counter
     double *force_ring; // [ring_cap][row_len]
@@ -138,6 +139,7 @@ struct lbm_handle {
     int *d_tiles = nullptr;         // nslots x tile lists of the patch grid
     size_t tiles_slot = 0;          // ints per slot of d_tiles
     int *d_nsup = nullptr;          // nslots: correction tiles of the slot's step
+    int *d_ctile = nullptr;         // nslots x tiles: the correction tiles' indices
     int pinfo_slot = 0;             // slot the next lattice launch reads
     int patch_wmax = 0, patch_hmax = 0;
     int patch_gx() const { return patch_wmax > 0 ? (patch_wmax + 15) / 16 : 1; }
