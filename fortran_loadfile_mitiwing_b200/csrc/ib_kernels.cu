@@ -48,7 +48,8 @@
 //               moment sums (:1645-1675, solution.f90:327-336) in FP64 with a
 //               deterministic two-level reduction. The lattice kernel skips
 //               these nodes and updates all others;
-//   ib_residual the solve's residual, after the step's update.
+//   ib_forces   the force row from the tiles' partials, and
+//   ib_residual the solve's residual, both after the step's update.
 
 #include <math.h>
 
@@ -793,10 +794,6 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
         const unsigned fs = *a.fstatus;
         if (fs) { atomicOr(a.status, fs); *a.fstatus = 0u; }
         a.solve_res[1] = (double)a.fmode[1];
-        if (*a.nsup == 0) {   // no correction tile: nothing writes the forces
-            double *fr = a.force_ring + (long long)ring_slot * a.row_len;
-            for (int c = 1; c <= 3 * a.nwing + 3; ++c) fr[c] = 0.0;
-        }
         timed_out = 0;
         mbar_init(bar, 1);
         mbar_init_fence();
@@ -993,6 +990,52 @@ __global__ void __launch_bounds__(TILE_CAP) ib_tile_sort(const IBArgs base, int 
     }
 }
 
+// The step's force row from the correction tiles' partials, summed in tile
+// order (deterministic), one CTA; no correction tile gives zero forces
+// (solution.f90:327-330 normalisation). Needed by no kernel of the step, so
+// it runs after the step's update.
+__global__ void __launch_bounds__(256) ib_forces(const IBArgs a, int ring_slot)
+{
+    __shared__ double red[8][NPART];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int ntiles_all = (int)(a.st_tiles / (TILE_CAP + 1));
+    for (int w = 0; w < a.nwing; ++w) {
+        double s0 = 0, s1 = 0, s2 = 0;
+        if (a.nseg > 0)
+            for (int b = threadIdx.x; b < ntiles_all; b += blockDim.x) {
+                if (a.tiles[(long long)b * (TILE_CAP + 1)] == 0) continue;
+                const double *p = a.partial + (long long)b * NPART + 3 * w;
+                s0 += p[0]; s1 += p[1]; s2 += p[2];
+            }
+#pragma unroll
+        for (int off = 16; off; off >>= 1) {
+            s0 += __shfl_down_sync(0xffffffffu, s0, off);
+            s1 += __shfl_down_sync(0xffffffffu, s1, off);
+            s2 += __shfl_down_sync(0xffffffffu, s2, off);
+        }
+        if (lane == 0) { red[warp][3 * w] = s0; red[warp][3 * w + 1] = s1; red[warp][3 * w + 2] = s2; }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double *fr = a.force_ring + (long long)ring_slot * a.row_len;
+        double tot[3] = {0, 0, 0};
+        const double uu = a.uu, scale = a.scale;
+        for (int w = 0; w < a.nwing; ++w) {
+            double s0 = 0, s1 = 0, s2 = 0;
+            for (int w8 = 0; w8 < 8; ++w8) { s0 += red[w8][3 * w]; s1 += red[w8][3 * w + 1]; s2 += red[w8][3 * w + 2]; }
+            const double cx = 2.0 * s0 / (uu * uu * (1.0 / scale));
+            const double cy = 2.0 * s1 / (uu * uu * (1.0 / scale));
+            const double cm = -2.0 * s2 / (uu * uu * (1.0 / (scale * scale)));
+            fr[1 + 3 * w] = cx; fr[2 + 3 * w] = cy; fr[3 + 3 * w] = cm;
+            tot[0] += cx; tot[1] += cy; tot[2] += cm;
+            if (!isfinite(cx) || !isfinite(cy) || !isfinite(cm)) atomicOr(a.status, LBM_ST_NONFINITE);
+        }
+        fr[1 + 3 * a.nwing] = tot[0];
+        fr[2 + 3 * a.nwing] = tot[1];
+        fr[3 + 3 * a.nwing] = tot[2];
+    }
+}
+
 // Residual of the step's solve, ||B y - rhs|| / ||rhs|| with B = D D^T
 // recomputed from the marker geometry (independent of the factorization):
 // one warp per row of the solve order, lanes over the couplings within the
@@ -1076,15 +1119,15 @@ __global__ void __launch_bounds__(256) ib_tile_update(const IBArgs a, const KFAr
     __shared__ int wsum[8];
     __shared__ int nlist;
     __shared__ double red[8][NPART];
-    __shared__ bool amlast;
     // markers whose support box meets the current tile, staged in marker order
     __shared__ int4 sbox[256];
     __shared__ double sph[256][12];
     __shared__ double sy[256][2];
     __shared__ int swing[256];
     const int ntile = *a.nsup;
-    if (ntile == 0) return;   // no correction tile (ib_solve wrote the zero forces)
+    if (ntile == 0) return;   // no correction tile
     const PatchInfo pi = *a.pinfo;
+    const T *__restrict__ fin = (const T *)kf.fin;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     // the correction tiles, strided over the CTAs (the compact list is in no
@@ -1098,6 +1141,10 @@ __global__ void __launch_bounds__(256) ib_tile_update(const IBArgs a, const KFAr
         const int gi = pi.i0 + li, gj = pi.j0 + lj;                // 0-based node
         const bool active = li < pi.w && lj < pi.h;
         const int ta = pi.i0 + ti0, tb = ta + TILE - 1, sa_ = pi.j0 + tj0, sb_ = sa_ + TILE - 1;
+        // the node's streamed populations first: their loads overlap the
+        // staging of the markers
+        C g[9];
+        if (active) lbm_node::pull<T, C>(fin, kf.plane, kf.pitch, gi, gj, g);
         double du = 0.0, dv = 0.0;
         int wing = 1 << 20;
         if (listed <= TILE_CAP) {
@@ -1173,9 +1220,6 @@ __global__ void __launch_bounds__(256) ib_tile_update(const IBArgs a, const KFAr
         double fx = 0, fy = 0, mz = 0;
         const bool in_support = active && wing < (1 << 20);
         if (active) {
-            const T *__restrict__ fin = (const T *)kf.fin;
-            C g[9];
-            lbm_node::pull<T, C>(fin, kf.plane, kf.pitch, gi, gj, g);
             C gout[9], frho, fu, fv;
             lbm_node::collide_interior<C>(kf, g, true, (C)du, (C)dv, gout, frho, fu, fv);
             lbm_node::store_node<T, C, FIELDS>(kf, (T *)kf.fout, gi, gj, gout, frho, fu, fv);
@@ -1214,51 +1258,6 @@ __global__ void __launch_bounds__(256) ib_tile_update(const IBArgs a, const KFAr
             a.partial[(long long)tile * NPART + threadIdx.x] = sum;
         }
         __syncthreads();   // shared arrays are reused by the next tile
-    }
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) amlast = atomicAdd(a.counter, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (!amlast) return;
-    __threadfence();
-    // last CTA: every thread sums a fixed strided subset of the tiles'
-    // partials, in tile order, then a fixed warp/block tree
-    const int ntiles_all = (int)(a.st_tiles / (TILE_CAP + 1));
-    for (int w = 0; w < a.nwing; ++w) {
-        double s0 = 0, s1 = 0, s2 = 0;
-        for (int b = threadIdx.x; b < ntiles_all; b += blockDim.x) {
-            if (a.tiles[(long long)b * (TILE_CAP + 1)] == 0) continue;
-            const double *p = a.partial + (long long)b * NPART + 3 * w;
-            s0 += __ldcg(p); s1 += __ldcg(p + 1); s2 += __ldcg(p + 2);
-        }
-#pragma unroll
-        for (int off = 16; off; off >>= 1) {
-            s0 += __shfl_down_sync(0xffffffffu, s0, off);
-            s1 += __shfl_down_sync(0xffffffffu, s1, off);
-            s2 += __shfl_down_sync(0xffffffffu, s2, off);
-        }
-        if (lane == 0) { red[warp][3 * w] = s0; red[warp][3 * w + 1] = s1; red[warp][3 * w + 2] = s2; }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double *fr = a.force_ring + (long long)ring_slot * a.row_len;
-        double tot[3] = {0, 0, 0};
-        const double uu = a.uu, scale = a.scale;
-        for (int w = 0; w < a.nwing; ++w) {
-            double s0 = 0, s1 = 0, s2 = 0;
-            for (int w8 = 0; w8 < 8; ++w8) { s0 += red[w8][3 * w]; s1 += red[w8][3 * w + 1]; s2 += red[w8][3 * w + 2]; }
-            // solution.f90:327-330
-            const double cx = 2.0 * s0 / (uu * uu * (1.0 / scale));
-            const double cy = 2.0 * s1 / (uu * uu * (1.0 / scale));
-            const double cm = -2.0 * s2 / (uu * uu * (1.0 / (scale * scale)));
-            fr[1 + 3 * w] = cx; fr[2 + 3 * w] = cy; fr[3 + 3 * w] = cm;
-            tot[0] += cx; tot[1] += cy; tot[2] += cm;
-            if (!isfinite(cx) || !isfinite(cy) || !isfinite(cm)) atomicOr(a.status, LBM_ST_NONFINITE);
-        }
-        fr[1 + 3 * a.nwing] = tot[0];
-        fr[2 + 3 * a.nwing] = tot[1];
-        fr[3 + 3 * a.nwing] = tot[2];
-        *a.counter = 0u;
     }
 }
 
@@ -1346,10 +1345,12 @@ int launch_flow_t(lbm_handle *h, const void *fin, void *fout, void *fields, int 
 
 // the residual check of the step's solve (needed by no later kernel of the step)
 template <typename T, typename C>
-int launch_check_t(lbm_handle *h, int slot, cudaStream_t st)
+int launch_check_t(lbm_handle *h, int slot, int ring_slot, cudaStream_t st)
 {
-    if (h->nseg == 0) return 0;
     IBArgs a = make_args(h, nullptr, slot);
+    ib_forces<<<1, 256, 0, st>>>(a, ring_slot);
+    h->launches += 1;
+    if (h->nseg == 0) return cudaGetLastError() == cudaSuccess ? 0 : -1;
     ib_residual<<<(h->nseg + 7) / 8, 256, 0, st>>>(a);
     h->launches += 1;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
@@ -1404,10 +1405,10 @@ int launch_factor(lbm_handle *h, int step0, int count, cudaStream_t st)
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
-// residual check of the step held in `slot`, after its flow chain
-int launch_check(lbm_handle *h, int slot, cudaStream_t st)
+// force row and residual check of the step held in `slot`, after its flow chain
+int launch_check(lbm_handle *h, int slot, int ring_slot, cudaStream_t st)
 {
-    return launch_check_t<float, float>(h, slot, st ? st : h->stream);
+    return launch_check_t<float, float>(h, slot, ring_slot, st ? st : h->stream);
 }
 
 // flow chain of step `step_index`: interpolation, solve with the factor of

@@ -328,7 +328,7 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             if (launch_flow(h, fin, fout, fields, h->n, slot, q, h->side)) return cuda_err(h, cudaGetLastError(), "launch ib");
             if (e) CK(cudaEventRecord(h->ev_side[2 * slot + 1], h->side), "event");
             CK(cudaEventRecord(h->ev_ib, h->side), "event");
-            if (launch_check(h, q, h->side)) return cuda_err(h, cudaGetLastError(), "launch check");
+            if (launch_check(h, q, slot, h->side)) return cuda_err(h, cudaGetLastError(), "launch check");
             CK(cudaEventRecord(h->ev_free[half], h->side), "event");
             // the next batch's factorization, overlapping this batch's steps
             if ((b + 1) * K <= last_step && h->batch_in_half[half ^ 1] != b + 1 && (rc = factor_batch(b + 1))) return rc;
@@ -346,7 +346,7 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             if (e) CK(cudaEventRecord(e[0], h->stream), "event");
             if (h->batch_in_half[half] != b && (rc = factor_batch(b))) return rc;
             if (launch_flow(h, fin, fout, fields, h->n, slot, q, h->stream)) return cuda_err(h, cudaGetLastError(), "launch ib");
-            if (launch_check(h, q, h->stream)) return cuda_err(h, cudaGetLastError(), "launch check");
+            if (launch_check(h, q, slot, h->stream)) return cuda_err(h, cudaGetLastError(), "launch check");
             if (e) {
                 CK(cudaEventRecord(e[1], h->stream), "event");
                 CK(cudaEventRecord(e[2], h->stream), "event");
@@ -360,14 +360,14 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
         done++;
         pending++;
         if (pending == h->ring_cap || s == nsteps - 1) {
+            if (split) {   // force rows and residual checks run on the side stream after the update
+                CK(cudaEventRecord(h->ev_ib, h->side), "event");
+                CK(cudaStreamWaitEvent(h->stream, h->ev_ib, 0), "wait");
+            }
             if (rows_out)
                 CK(cudaMemcpyAsync(rows_out + (size_t)(done - pending) * h->row_len, h->d_ring,
                                    sizeof(double) * h->row_len * pending, cudaMemcpyDeviceToHost, h->stream),
                    "copy force rows");
-            if (split) {   // the residual checks run on the side stream after the spread
-                CK(cudaEventRecord(h->ev_ib, h->side), "event");
-                CK(cudaStreamWaitEvent(h->stream, h->ev_ib, 0), "wait");
-            }
             int st = check_status(h);
             if (st) return st;
             if (h->timing && (st = collect_timing(h, pending, split))) return st;
@@ -375,14 +375,14 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
         }
     }
     if (pending) {
-        if (rows_out)
-            CK(cudaMemcpyAsync(rows_out + (size_t)(done - pending) * h->row_len, h->d_ring,
-                               sizeof(double) * h->row_len * pending, cudaMemcpyDeviceToHost, h->stream),
-               "copy force rows");
         if (split) {
             CK(cudaEventRecord(h->ev_ib, h->side), "event");
             CK(cudaStreamWaitEvent(h->stream, h->ev_ib, 0), "wait");
         }
+        if (rows_out)
+            CK(cudaMemcpyAsync(rows_out + (size_t)(done - pending) * h->row_len, h->d_ring,
+                               sizeof(double) * h->row_len * pending, cudaMemcpyDeviceToHost, h->stream),
+               "copy force rows");
         int st = check_status(h);
         if (st) return st;
         if (h->timing && (st = collect_timing(h, pending, split))) return st;

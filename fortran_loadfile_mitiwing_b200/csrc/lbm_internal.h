@@ -195,7 +195,7 @@ int launch_kf(lbm_handle *h, const void *fin, void *fout, void *fields, int mode
 int launch_factor(lbm_handle *h, int step0, int count, cudaStream_t st);
 int launch_flow(lbm_handle *h, const void *fin, void *fout, void *fields, int step_index, int ring_slot, int slot,
                 cudaStream_t st);
-int launch_check(lbm_handle *h, int slot, cudaStream_t st);
+int launch_check(lbm_handle *h, int slot, int ring_slot, cudaStream_t st);
 int ib_tile_ints();   // ints per patch tile of the tile lists
 int launch_residual(lbm_handle *h, const void *fa, const void *fb, double *out2);
 int launch_unpack(lbm_handle *h, const void *fsrc, double *dst);   // deviation -> f (FP64)

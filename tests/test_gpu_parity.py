@@ -86,11 +86,11 @@ def test_step_and_run_agree_bitwise(gpu_lib):
 
 
 def test_launch_count_per_step(gpu_lib):
-    """Per step of one rigid wing: the flow chain (interpolation, solve,
-    spread, residual check) and one or two lattice kernels (two when the
-    lattice update is split around the body's envelope); plus, per batch of
-    steps, the five kernels of the batched factorization of the marker system
-    (geometry, band assembly, factorization, patch-tile lists in two passes)."""
+    """Per step of one rigid wing: the flow chain (interpolation, solve, update
+    of the correction tiles, force row, residual check) and the lattice kernel;
+    plus, per batch of steps, the five kernels of the batched factorization of
+    the marker system (geometry, band assembly, factorization, patch-tile
+    lists in two passes)."""
     import ctypes as C
     case = cases.small_case(precision="fp32", n_steps=100)
     g = Lbm.from_case(case, gpu_lib)
@@ -101,10 +101,9 @@ def test_launch_count_per_step(gpu_lib):
     g.run(steps)
     gpu_lib.lbm_get_launch_count(g.h, C.byref(n1))
     total = n1.value - n0.value
-    fits = [kf for kf in (1, 2)
-            if total >= steps * (4 + kf) and (total - steps * (4 + kf)) % 5 == 0
-            and 1 <= (total - steps * (4 + kf)) // 5 <= steps]
-    assert fits, total
+    per_step = 5 + 1
+    assert total >= steps * per_step and (total - steps * per_step) % 5 == 0, total
+    assert 1 <= (total - steps * per_step) // 5 <= steps, total
 
 
 def test_residual_matches_oracle(gpu_lib, oracle_mod):
