@@ -154,7 +154,17 @@ __global__ void __launch_bounds__(128) kf_vec(const KFArgs<C> a)
 // 0 and nx-1 by the scalar edge path.
 
 constexpr int TW = 256;        // strip width (threads per CTA)
-constexpr int KS = 4;          // pipeline stages
+#ifndef LBM_KF_STAGES
+#define LBM_KF_STAGES 4
+#endif
+#ifndef LBM_KF_MINB
+#define LBM_KF_MINB 3
+#endif
+constexpr int KS = LBM_KF_STAGES;   // pipeline stages
+// Resident CTAs per SM the register budget is sized for. Three leave room on
+// each SM for the immersed-boundary kernels that run beside the lattice
+// update; four make the lattice kernel alone ~2% faster but starve them.
+constexpr int KF_MINB = LBM_KF_MINB;
 
 // mbarrier and bulk-copy helpers: lbm_common.cuh
 
@@ -163,7 +173,7 @@ template <typename T> __host__ __device__ constexpr int tma_seg() { return TW + 
 template <typename T> constexpr size_t tma_smem() { return sizeof(T) * KS * 9 * tma_seg<T>() + 2 * 8 * KS; }
 
 template <typename T, typename C, bool FIELDS>
-__global__ void __launch_bounds__(TW) kf_tma(const KFArgs<C> a)
+__global__ void __launch_bounds__(TW, KF_MINB) kf_tma(const KFArgs<C> a)
 {
     constexpr int H = tma_halo<T>(), SEG = tma_seg<T>(), NWARP = TW / 32;
     extern __shared__ __align__(128) unsigned char smraw[];
