@@ -160,7 +160,9 @@ constexpr int TW = 256;        // strip width (threads per CTA)
 #ifndef LBM_KF_MINB
 #define LBM_KF_MINB 3
 #endif
-constexpr int KS = LBM_KF_STAGES;   // pipeline stages
+// pipeline stages: 2-byte storage halves the bytes of a stage, so it keeps
+// twice the stages to hold the same bytes in flight
+template <typename T> __host__ __device__ constexpr int tma_stages() { return sizeof(T) == 2 ? 2 * LBM_KF_STAGES : LBM_KF_STAGES; }
 // Resident CTAs per SM the register budget is sized for. Three leave room on
 // each SM for the immersed-boundary kernels that run beside the lattice
 // update; four make the lattice kernel alone ~2% faster but starve them.
@@ -170,12 +172,12 @@ constexpr int KF_MINB = LBM_KF_MINB;
 
 template <typename T> __host__ __device__ constexpr int tma_halo() { return 16 / (int)sizeof(T); }
 template <typename T> __host__ __device__ constexpr int tma_seg() { return TW + 2 * tma_halo<T>(); }
-template <typename T> constexpr size_t tma_smem() { return sizeof(T) * KS * 9 * tma_seg<T>() + 2 * 8 * KS; }
+template <typename T> constexpr size_t tma_smem() { return sizeof(T) * tma_stages<T>() * 9 * tma_seg<T>() + 2 * 8 * tma_stages<T>(); }
 
 template <typename T, typename C, bool FIELDS>
 __global__ void __launch_bounds__(TW, KF_MINB) kf_tma(const KFArgs<C> a)
 {
-    constexpr int H = tma_halo<T>(), SEG = tma_seg<T>(), NWARP = TW / 32;
+    constexpr int H = tma_halo<T>(), SEG = tma_seg<T>(), NWARP = TW / 32, KS = tma_stages<T>();
     extern __shared__ __align__(128) unsigned char smraw[];
     T *buf = reinterpret_cast<T *>(smraw);
     uint64_t *full = reinterpret_cast<uint64_t *>(smraw + sizeof(T) * KS * 9 * SEG);

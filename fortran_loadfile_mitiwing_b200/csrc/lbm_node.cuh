@@ -117,19 +117,41 @@ template <typename C>
 __device__ __forceinline__ void collide_interior(const KFArgs<C> &a, const C g[9], bool corr, C du, C dv, C gout[9],
                                                  C &frho, C &fu, C &fv)
 {
-    C drho, u, v;
-    moments(g, drho, u, v);
+    // physical_variables (solution.f90:471-542) on the deviations
+    const C drho = ((g[0] + g[1]) + (g[2] + g[3])) + ((g[4] + g[5]) + (g[6] + g[7])) + g[8];
+    const C jx0 = (g[1] - g[3]) + (g[5] - g[6]) + (g[8] - g[7]);
+    const C jy0 = (g[2] - g[4]) + (g[5] + g[6]) - (g[7] + g[8]);
     const C rho = C(1) + drho;
+    C u = jx0 / rho, v = jy0 / rho;   // needed only for the fields and the correction
+    // j = rho u of the equilibrium: the summed momentum itself when there is
+    // no correction (rho (jx/rho) = jx up to one rounding)
+    C jx = jx0, jy = jy0;
     C gx = C(0), gy = C(0);
     if (corr) {
         u = u + du;                       // boundary_condition.f90:1650-1651
         v = v + dv;
+        jx = rho * u;
+        jy = rho * v;
         gx = C(2) * rho * du;             // :1652-1656
         gy = C(2) * rho * dv;
     }
+    // m = M g (solution.f90:580-600); rows 0, 3, 5 are the moments above
     C m[9];
-    mrt_forward(g, m);
-    const C jx = rho * u, jy = rho * v;
+    {
+        const C as = g[1] + g[2] + g[3] + g[4];
+        const C ds = g[5] + g[6] + g[7] + g[8];
+        const C dx = g[5] - g[6] - g[7] + g[8];
+        const C dy = g[5] + g[6] - g[7] - g[8];
+        m[0] = drho;
+        m[1] = C(-4) * g[0] - as + C(2) * ds;
+        m[2] = C(4) * g[0] - C(2) * as + ds;
+        m[3] = jx0;
+        m[4] = C(-2) * (g[1] - g[3]) + dx;
+        m[5] = jy0;
+        m[6] = C(-2) * (g[2] - g[4]) + dy;
+        m[7] = g[1] - g[2] + g[3] - g[4];
+        m[8] = g[5] - g[6] + g[7] - g[8];
+    }
     const C jj = jx * jx + jy * jy;
     C e[9];
     e[0] = C(-1);                          // temp(1)=0 minus (M w)_1
