@@ -3,7 +3,7 @@ solver (immersed boundary, implicit velocity correction), behind the C ABI of
 include/lbm_b200.h."""
 from ._abi import (LBM_DELTA_PESKIN4, LBM_DELTA_SMOOTH, LBM_PREC_BF16, LBM_PREC_FP16, LBM_PREC_FP32,
                    LBM_PREC_FP64, LbmParams, load_library)
-from .solver import Lbm, LbmError
+from .solver import Batch, Lbm, LbmError
 
-__all__ = ["Lbm", "LbmError", "LbmParams", "load_library", "LBM_PREC_FP32", "LBM_PREC_FP64",
+__all__ = ["Batch", "Lbm", "LbmError", "LbmParams", "load_library", "LBM_PREC_FP32", "LBM_PREC_FP64",
            "LBM_PREC_FP16", "LBM_PREC_BF16", "LBM_DELTA_PESKIN4", "LBM_DELTA_SMOOTH"]

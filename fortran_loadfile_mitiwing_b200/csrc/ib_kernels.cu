@@ -217,8 +217,10 @@ __device__ Marker make_marker(const IBArgs &a, const double *row, int k)
 
 
 // one thread per marker: geometry of this step (errors go to the slot's status)
-__global__ void __launch_bounds__(128) ib_geometry(const IBArgs base, int step0)
+template <bool BATCH>
+__global__ void __launch_bounds__(128) ib_geometry(const IBArgs base0, const IBArgs *batch, int step0)
 {
+    const IBArgs &base = BATCH ? batch[blockIdx.z] : base0;
     const int step_index = step0 + blockIdx.y;
     const IBArgs a = member_args(base, step_index);
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -228,9 +230,10 @@ __global__ void __launch_bounds__(128) ib_geometry(const IBArgs base, int step0)
 }
 
 // one warp per marker: b = D u* over the support box, rhs = U_b - b
-template <typename T>
-__global__ void __launch_bounds__(256) ib_interp(const IBArgs a)
+template <typename T, bool BATCH>
+__global__ void __launch_bounds__(256) ib_interp(const IBArgs a0, const IBArgs *batch)
 {
+    const IBArgs &a = BATCH ? batch[blockIdx.z] : a0;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // bring the slot's factor blocks, which the lattice kernels have evicted
     // since the factorization wrote them, back into L2 for ib_solve: one
@@ -304,9 +307,12 @@ __device__ void write_header(const IBArgs &a, const double *row, double time, in
 // Several bodies: sort the markers along the longer axis of the marker cloud
 // (stable, ties by index) into perm/key, with reach = 6 lattice units along
 // that axis. One CTA; dynamic shared memory key[ns] (double) + idx[ns] (int).
-__global__ void __launch_bounds__(1024) ib_order(const IBArgs base, int step0)
+template <bool BATCH>
+__global__ void __launch_bounds__(1024) ib_order(const IBArgs base0, const IBArgs *batch, int step0)
 {
+    const IBArgs &base = BATCH ? batch[blockIdx.z] : base0;
     const IBArgs a = member_args(base, step0 + blockIdx.y);
+    if (a.static_order) return;   // one rigid body: fixed order (batched launches reach it)
     extern __shared__ double osm[];
     const int n = a.nseg, tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
     int ns = 1;
@@ -368,10 +374,13 @@ __global__ void __launch_bounds__(1024) ib_order(const IBArgs base, int step0)
 // One CTA per block of BS markers in the solve order: the diagonal block D_b,
 // the coupling L_b to block b-1, and the longest coupling in the order
 // (half-bandwidth).
-__global__ void __launch_bounds__(256) ib_assemble(const IBArgs base, int step0)
+template <bool BATCH>
+__global__ void __launch_bounds__(256) ib_assemble(const IBArgs base0, const IBArgs *batch, int step0)
 {
+    const IBArgs &base = BATCH ? batch[blockIdx.z] : base0;
     const IBArgs a = member_args(base, step0 + blockIdx.y);
     const int n = a.nseg, blk = blockIdx.x, tid = threadIdx.x;
+    if (blk >= (n + BS - 1) / BS) return;   // batched launches size the grid for the largest case
     __shared__ double ph[2 * BS][12];
     __shared__ int4 bx[2 * BS];
     __shared__ int wl;
@@ -590,8 +599,10 @@ __device__ void dense_tri(const IBArgs &a, double *yv)
 // F_U = D_o^-1 L_q^T (coupling to q = o + st); block 0, the last one left,
 // keeps D_0^-1. The even neighbours are updated as
 //   D_e -= L_q^T F_L(q) + L_e F_U(p),   L_e <- -L_e F_L(p)   (p = e - st, q = e + st).
-__global__ void __launch_bounds__(FACTOR_THREADS) ib_factor(const IBArgs base, int step0)
+template <bool BATCH>
+__global__ void __launch_bounds__(FACTOR_THREADS) ib_factor(const IBArgs base0, const IBArgs *batch, int step0)
 {
+    const IBArgs &base = BATCH ? batch[blockIdx.z] : base0;
     const IBArgs a = member_args(base, step0 + blockIdx.y);
     extern __shared__ __align__(16) double Wbase[];
     const int n = a.nseg, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -776,8 +787,11 @@ __global__ void __launch_bounds__(FACTOR_THREADS) ib_factor(const IBArgs base, i
 // errors of the factorization chain. Dynamic shared memory: the staged
 // blocks, then the right-hand sides in the solve order (two per marker,
 // padded to whole blocks), then the mbarrier.
-__global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int step_index, int ring_slot)
+template <bool BATCH>
+__global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a0, const IBArgs *batch, int step_index,
+                                                          int ring_slot)
 {
+    const IBArgs &a = BATCH ? batch[blockIdx.z] : a0;
     extern __shared__ __align__(128) double smem[];
     const int n = a.nseg, tid = threadIdx.x, nt = blockDim.x;
     const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
@@ -944,8 +958,10 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a, int st
 // part of the factorization chain, in two passes: each marker appends itself
 // to the (at most 2 x 2) tiles its box meets, then each tile sorts its list.
 // ib_factor has cleared the counts.
-__global__ void __launch_bounds__(256) ib_tile_scatter(const IBArgs base, int step0)
+template <bool BATCH>
+__global__ void __launch_bounds__(256) ib_tile_scatter(const IBArgs base0, const IBArgs *batch, int step0)
 {
+    const IBArgs &base = BATCH ? batch[blockIdx.z] : base0;
     const IBArgs a = member_args(base, step0 + blockIdx.y);
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.nseg) return;
@@ -964,8 +980,10 @@ __global__ void __launch_bounds__(256) ib_tile_scatter(const IBArgs base, int st
         }
 }
 
-__global__ void __launch_bounds__(TILE_CAP) ib_tile_sort(const IBArgs base, int step0)
+template <bool BATCH>
+__global__ void __launch_bounds__(TILE_CAP) ib_tile_sort(const IBArgs base0, const IBArgs *batch, int step0)
 {
+    const IBArgs &base = BATCH ? batch[blockIdx.z] : base0;
     const IBArgs a = member_args(base, step0 + blockIdx.y);
     __shared__ int key[TILE_CAP];
     const int ntile = *a.nsup, t = threadIdx.x;
@@ -994,8 +1012,10 @@ __global__ void __launch_bounds__(TILE_CAP) ib_tile_sort(const IBArgs base, int 
 // order (deterministic), one CTA; no correction tile gives zero forces
 // (solution.f90:327-330 normalisation). Needed by no kernel of the step, so
 // it runs after the step's update.
-__global__ void __launch_bounds__(256) ib_forces(const IBArgs a, int ring_slot)
+template <bool BATCH>
+__global__ void __launch_bounds__(256) ib_forces(const IBArgs a0, const IBArgs *batch, int ring_slot)
 {
+    const IBArgs &a = BATCH ? batch[blockIdx.z] : a0;
     __shared__ double red[8][NPART];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int ntiles_all = (int)(a.st_tiles / (TILE_CAP + 1));
@@ -1041,12 +1061,16 @@ __global__ void __launch_bounds__(256) ib_forces(const IBArgs a, int ring_slot)
 // one warp per row of the solve order, lanes over the couplings within the
 // half-bandwidth; deterministic two-level sum (CTA partials, last CTA).
 // Flags LBM_ST_SOLVER unless it is below 1e-6.
-__global__ void __launch_bounds__(256) ib_residual(const IBArgs a)
+template <bool BATCH>
+__global__ void __launch_bounds__(256) ib_residual(const IBArgs a0, const IBArgs *batch)
 {
+    const IBArgs &a = BATCH ? batch[blockIdx.z] : a0;
     __shared__ double red[8][2];
     __shared__ bool amlast;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int n = a.nseg, s = blockIdx.x * 8 + warp;
+    const int nblk = (n + 7) / 8;
+    if ((int)blockIdx.x >= nblk) return;    // batched launches size the grid for the largest case
     const int hw = (int)a.solve_res[1];
     double rnum = 0.0, rden = 0.0;
     if (s < n) {
@@ -1077,13 +1101,13 @@ __global__ void __launch_bounds__(256) ib_residual(const IBArgs a)
         a.partial[2 * blockIdx.x] = t0;
         a.partial[2 * blockIdx.x + 1] = t1;
         __threadfence();
-        amlast = atomicAdd(a.counter, 1u) == gridDim.x - 1;
+        amlast = atomicAdd(a.counter, 1u) == (unsigned)(nblk - 1);
     }
     __syncthreads();
     if (!amlast) return;
     __threadfence();
     double s0 = 0.0, s1 = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) {
         s0 += __ldcg(a.partial + 2 * b);
         s1 += __ldcg(a.partial + 2 * b + 1);
     }
@@ -1113,9 +1137,12 @@ __global__ void __launch_bounds__(256) ib_residual(const IBArgs a)
 // force and moment (boundary_condition.f90:1645-1675, solution.f90:327-336).
 // The last CTA sums the per-tile partials in tile order into the step's force
 // row. The lattice kernel updates every other node.
-template <typename T, typename C, bool FIELDS>
-__global__ void __launch_bounds__(256) ib_tile_update(const IBArgs a, const KFArgs<C> kf, int step_index, int ring_slot)
+template <typename T, typename C, bool FIELDS, bool BATCH>
+__global__ void __launch_bounds__(256) ib_tile_update(const IBArgs a0, const IBArgs *batch, const KFArgs<C> kf0,
+                                                      const KFArgs<C> *kbatch, int step_index, int ring_slot)
 {
+    const IBArgs &a = BATCH ? batch[blockIdx.z] : a0;
+    const KFArgs<C> &kf = BATCH ? kbatch[blockIdx.z] : kf0;
     __shared__ int wsum[8];
     __shared__ int nlist;
     __shared__ double red[8][NPART];
@@ -1295,6 +1322,7 @@ IBArgs make_args(lbm_handle *h, const void *fin, int slot)
     a.xb0 = h->d_xb0; a.yb0 = h->d_yb0; a.arc = h->d_arc;
     a.mstep = h->d_mstep; a.msteps = h->msteps; a.mcols = h->mcols; a.mdt = h->mdt;
     a.nslots = h->nslots;
+    a.static_order = h->static_order;
     a.st_mk = (long long)ns;
     a.st_perm = h->static_order ? 0 : (long long)ns;
     a.st_B = (long long)(ns * ns);
@@ -1329,16 +1357,16 @@ int launch_flow_t(lbm_handle *h, const void *fin, void *fout, void *fields, int 
 {
     IBArgs a = make_args(h, fin, slot);
     if (h->nseg > 0) {
-        ib_interp<T><<<(h->nseg + 7) / 8, 256, 0, st>>>(a);
+        ib_interp<T, false><<<(h->nseg + 7) / 8, 256, 0, st>>>(a, nullptr);
         h->launches += 1;
     }
-    ib_solve<<<1, SOLVE_THREADS, solve_smem(h->nseg), st>>>(a, step_index, ring_slot);
+    ib_solve<false><<<1, SOLVE_THREADS, solve_smem(h->nseg), st>>>(a, nullptr, step_index, ring_slot);
     const int grid = std::min(h->patch_gx() * h->patch_gy(), 2 * 148);   // strided over the correction tiles
     const KFArgs<C> kf = make_kf_args<C>(h, fin, fout, fields, KF_OUTER);
     if (fields)
-        ib_tile_update<T, C, true><<<grid, 256, 0, st>>>(a, kf, step_index, ring_slot);
+        ib_tile_update<T, C, true, false><<<grid, 256, 0, st>>>(a, nullptr, kf, nullptr, step_index, ring_slot);
     else
-        ib_tile_update<T, C, false><<<grid, 256, 0, st>>>(a, kf, step_index, ring_slot);
+        ib_tile_update<T, C, false, false><<<grid, 256, 0, st>>>(a, nullptr, kf, nullptr, step_index, ring_slot);
     h->launches += 2;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
@@ -1348,10 +1376,10 @@ template <typename T, typename C>
 int launch_check_t(lbm_handle *h, int slot, int ring_slot, cudaStream_t st)
 {
     IBArgs a = make_args(h, nullptr, slot);
-    ib_forces<<<1, 256, 0, st>>>(a, ring_slot);
+    ib_forces<false><<<1, 256, 0, st>>>(a, nullptr, ring_slot);
     h->launches += 1;
     if (h->nseg == 0) return cudaGetLastError() == cudaSuccess ? 0 : -1;
-    ib_residual<<<(h->nseg + 7) / 8, 256, 0, st>>>(a);
+    ib_residual<false><<<(h->nseg + 7) / 8, 256, 0, st>>>(a, nullptr);
     h->launches += 1;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
@@ -1375,17 +1403,25 @@ void ib_factor_scratch(int nseg, size_t *work_blocks, size_t *factor_slot)
 
 int ib_max_markers() { return NMARK_MAX; }
 
+template <bool BATCH>
+int ib_configure_t()
+{
+    if (cudaFuncSetAttribute(ib_factor<BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactorSmem) !=
+        cudaSuccess)
+        return -1;
+    if (cudaFuncSetAttribute(ib_solve<BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSolveSmemMax) !=
+        cudaSuccess)
+        return -1;
+    if (cudaFuncSetAttribute(ib_order<BATCH>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)order_smem(NMARK_MAX)) != cudaSuccess)
+        return -1;
+    return 0;
+}
+
 int ib_configure(lbm_handle *h)
 {
     (void)h;
-    if (cudaFuncSetAttribute(ib_factor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFactorSmem) != cudaSuccess)
-        return -1;
-    if (cudaFuncSetAttribute(ib_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kSolveSmemMax) != cudaSuccess)
-        return -1;
-    if (cudaFuncSetAttribute(ib_order, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)order_smem(NMARK_MAX)) !=
-        cudaSuccess)
-        return -1;
-    return 0;
+    return ib_configure_t<false>() || ib_configure_t<true>() ? -1 : 0;
 }
 
 // factorization chains of the `count` steps step0, step0+1, ... (each into
@@ -1395,12 +1431,13 @@ int launch_factor(lbm_handle *h, int step0, int count, cudaStream_t st)
     if (h->nseg == 0 || count <= 0) return 0;
     const IBArgs a = make_args(h, nullptr, 0);
     const int nb = (h->nseg + BS - 1) / BS;
-    ib_geometry<<<dim3((h->nseg + 127) / 128, count), 128, 0, st>>>(a, step0);
-    if (!h->static_order) ib_order<<<dim3(1, count), 1024, order_smem(h->nseg), st>>>(a, step0);
-    ib_assemble<<<dim3(nb, count), 256, 0, st>>>(a, step0);
-    ib_factor<<<dim3(1, count), FACTOR_THREADS, kFactorSmem, st>>>(a, step0);
-    ib_tile_scatter<<<dim3((h->nseg + 255) / 256, count), 256, 0, st>>>(a, step0);
-    ib_tile_sort<<<dim3(std::min(h->patch_gx() * h->patch_gy(), 148), count), TILE_CAP, 0, st>>>(a, step0);
+    ib_geometry<false><<<dim3((h->nseg + 127) / 128, count), 128, 0, st>>>(a, nullptr, step0);
+    if (!h->static_order) ib_order<false><<<dim3(1, count), 1024, order_smem(h->nseg), st>>>(a, nullptr, step0);
+    ib_assemble<false><<<dim3(nb, count), 256, 0, st>>>(a, nullptr, step0);
+    ib_factor<false><<<dim3(1, count), FACTOR_THREADS, kFactorSmem, st>>>(a, nullptr, step0);
+    ib_tile_scatter<false><<<dim3((h->nseg + 255) / 256, count), 256, 0, st>>>(a, nullptr, step0);
+    ib_tile_sort<false><<<dim3(std::min(h->patch_gx() * h->patch_gy(), 148), count), TILE_CAP, 0, st>>>(a, nullptr,
+                                                                                                        step0);
     h->launches += h->static_order ? 5 : 6;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
@@ -1425,4 +1462,93 @@ int launch_flow(lbm_handle *h, const void *fin, void *fout, void *fields, int st
         return launch_flow_t<__nv_bfloat16, float>(h, fin, fout, fields, step_index, ring_slot, slot, st);
     }
     return -1;
+}
+
+// ---- batches of cases (lbm_batch.cu): arguments from device arrays, one
+// launch per kernel for all cases (grid z = case), grids sized for the
+// largest case
+
+size_t ib_args_size() { return sizeof(IBArgs); }
+
+void ib_args_write(lbm_handle *h, const void *fin, int slot, void *dst) { *(IBArgs *)dst = make_args(h, fin, slot); }
+
+namespace {
+
+int max_seg(lbm_handle *const *hs, int n)
+{
+    int m = 0;
+    for (int c = 0; c < n; ++c) m = std::max(m, hs[c]->nseg);
+    return m;
+}
+
+template <typename T, typename C>
+int launch_flow_batch_t(lbm_handle *const *hs, int ncase, const IBArgs *dargs, const void *dkf, int step_index,
+                        int ring_slot, bool fields, cudaStream_t st)
+{
+    const int ns = max_seg(hs, ncase);
+    ib_interp<T, true><<<dim3((ns + 7) / 8, 1, ncase), 256, 0, st>>>(IBArgs{}, dargs);
+    ib_solve<true><<<dim3(1, 1, ncase), SOLVE_THREADS, solve_smem(ns), st>>>(IBArgs{}, dargs, step_index, ring_slot);
+    int tiles = 1;
+    for (int c = 0; c < ncase; ++c) tiles = std::max(tiles, hs[c]->patch_gx() * hs[c]->patch_gy());
+    const dim3 grid(std::min(tiles, 2 * 148), 1, ncase);
+    const KFArgs<C> *kf = (const KFArgs<C> *)dkf;
+    if (fields)
+        ib_tile_update<T, C, true, true><<<grid, 256, 0, st>>>(IBArgs{}, dargs, KFArgs<C>{}, kf, step_index, ring_slot);
+    else
+        ib_tile_update<T, C, false, true><<<grid, 256, 0, st>>>(IBArgs{}, dargs, KFArgs<C>{}, kf, step_index, ring_slot);
+    for (int c = 0; c < ncase; ++c) hs[c]->launches += 3;
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+}  // namespace
+
+// factorization chains of the steps step0 .. step0+count-1 of every case
+int launch_factor_batch(lbm_handle *const *hs, int ncase, const void *dargs, int step0, int count, cudaStream_t st)
+{
+    if (ncase <= 0 || count <= 0) return 0;
+    const IBArgs *d = (const IBArgs *)dargs;
+    const int ns = max_seg(hs, ncase), nb = (ns + BS - 1) / BS;
+    bool any_order = false;
+    int tiles = 1;
+    for (int c = 0; c < ncase; ++c) {
+        any_order = any_order || !hs[c]->static_order;
+        tiles = std::max(tiles, hs[c]->patch_gx() * hs[c]->patch_gy());
+    }
+    ib_geometry<true><<<dim3((ns + 127) / 128, count, ncase), 128, 0, st>>>(IBArgs{}, d, step0);
+    if (any_order) ib_order<true><<<dim3(1, count, ncase), 1024, order_smem(ns), st>>>(IBArgs{}, d, step0);
+    ib_assemble<true><<<dim3(nb, count, ncase), 256, 0, st>>>(IBArgs{}, d, step0);
+    ib_factor<true><<<dim3(1, count, ncase), FACTOR_THREADS, kFactorSmem, st>>>(IBArgs{}, d, step0);
+    ib_tile_scatter<true><<<dim3((ns + 255) / 256, count, ncase), 256, 0, st>>>(IBArgs{}, d, step0);
+    ib_tile_sort<true><<<dim3(std::min(tiles, 148), count, ncase), TILE_CAP, 0, st>>>(IBArgs{}, d, step0);
+    for (int c = 0; c < ncase; ++c) hs[c]->launches += any_order ? 6 : 5;
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+// flow chains of one step of every case (dargs: the cases' arguments of the
+// step's slot; dkf: their lattice arguments)
+int launch_flow_batch(lbm_handle *const *hs, int ncase, const void *dargs, const void *dkf, int step_index,
+                      int ring_slot, bool fields, cudaStream_t st)
+{
+    if (ncase <= 0) return 0;
+    const IBArgs *d = (const IBArgs *)dargs;
+    switch (hs[0]->prec) {
+    case LBM_PREC_FP32: return launch_flow_batch_t<float, float>(hs, ncase, d, dkf, step_index, ring_slot, fields, st);
+    case LBM_PREC_FP64: return launch_flow_batch_t<double, double>(hs, ncase, d, dkf, step_index, ring_slot, fields, st);
+    case LBM_PREC_FP16: return launch_flow_batch_t<__half, float>(hs, ncase, d, dkf, step_index, ring_slot, fields, st);
+    case LBM_PREC_BF16:
+        return launch_flow_batch_t<__nv_bfloat16, float>(hs, ncase, d, dkf, step_index, ring_slot, fields, st);
+    }
+    return -1;
+}
+
+// force rows and residual checks of one step of every case
+int launch_check_batch(lbm_handle *const *hs, int ncase, const void *dargs, int ring_slot, cudaStream_t st)
+{
+    if (ncase <= 0) return 0;
+    const IBArgs *d = (const IBArgs *)dargs;
+    const int ns = max_seg(hs, ncase);
+    ib_forces<true><<<dim3(1, 1, ncase), 256, 0, st>>>(IBArgs{}, d, ring_slot);
+    ib_residual<true><<<dim3((ns + 7) / 8, 1, ncase), 256, 0, st>>>(IBArgs{}, d);
+    for (int c = 0; c < ncase; ++c) hs[c]->launches += 2;
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

@@ -174,21 +174,22 @@ template <typename T> __host__ __device__ constexpr int tma_halo() { return 16 /
 template <typename T> __host__ __device__ constexpr int tma_seg() { return TW + 2 * tma_halo<T>(); }
 template <typename T> constexpr size_t tma_smem() { return sizeof(T) * tma_stages<T>() * 9 * tma_seg<T>() + 2 * 8 * tma_stages<T>(); }
 
+// One CTA of the staged kernel: strip bx (of gx) and row chunk by (of gy; the
+// last chunk is the edge CTA row) of the lattice described by `a`.
 template <typename T, typename C, bool FIELDS>
-__global__ void __launch_bounds__(TW, KF_MINB) kf_tma(const KFArgs<C> a)
+__device__ __forceinline__ void kf_tma_cta(const KFArgs<C> &a, int bx, int by, int gx, int gy, unsigned char *smraw)
 {
     constexpr int H = tma_halo<T>(), SEG = tma_seg<T>(), NWARP = TW / 32, KS = tma_stages<T>();
-    extern __shared__ __align__(128) unsigned char smraw[];
     T *buf = reinterpret_cast<T *>(smraw);
     uint64_t *full = reinterpret_cast<uint64_t *>(smraw + sizeof(T) * KS * 9 * SEG);
     uint64_t *empty = full + KS;
     const int tid = threadIdx.x, lane = tid & 31;
-    const int x0 = blockIdx.x * TW;
+    const int x0 = bx * TW;
     const int i = x0 + tid;
     const T *__restrict__ fin = (const T *)a.fin;
     T *__restrict__ fout = (T *)a.fout;
     const PatchInfo rr = a.mode == KF_OUTER ? *a.pinfo : PatchInfo{0, 0, 0, 0};   // step's patch rectangle
-    if (blockIdx.y == gridDim.y - 1) {
+    if (by == gy - 1) {
         // the edge nodes: rows 0 and ny-1 of this strip, and a share of the
         // nodes of columns 0 and nx-1 (which the strips' row sweeps skip)
         if (i < a.nx)
@@ -197,7 +198,7 @@ __global__ void __launch_bounds__(TW, KF_MINB) kf_tma(const KFArgs<C> a)
                 edge_update<T, C>(a, fin, i, j, gout, frho, fu, fv);
                 store_node<T, C, FIELDS>(a, fout, i, j, gout, frho, fu, fv);
             }
-        for (int q = blockIdx.x * TW + tid; q < 2 * (a.ny - 2); q += gridDim.x * TW) {
+        for (int q = bx * TW + tid; q < 2 * (a.ny - 2); q += gx * TW) {
             const int j = 1 + q / 2, ie = (q & 1) ? a.nx - 1 : 0;
             C gout[9], frho, fu, fv;
             edge_update<T, C>(a, fin, ie, j, gout, frho, fu, fv);
@@ -205,7 +206,7 @@ __global__ void __launch_bounds__(TW, KF_MINB) kf_tma(const KFArgs<C> a)
         }
         return;
     }
-    const int j0 = 1 + blockIdx.y * a.rows_per_cta;
+    const int j0 = 1 + by * a.rows_per_cta;
     const int nrows = min(a.rows_per_cta, a.ny - 1 - j0);
     if (nrows <= 0) return;
     const int width = min(TW, a.nx - x0);
@@ -273,6 +274,23 @@ __global__ void __launch_bounds__(TW, KF_MINB) kf_tma(const KFArgs<C> a)
     }
 }
 
+template <typename T, typename C, bool FIELDS>
+__global__ void __launch_bounds__(TW, KF_MINB) kf_tma(const KFArgs<C> a)
+{
+    extern __shared__ __align__(128) unsigned char smraw[];
+    kf_tma_cta<T, C, FIELDS>(a, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, smraw);
+}
+
+// Several lattices (a batch of cases) in one launch: CTA b runs entry b of
+// the case table, {case, strip, row chunk, strips | row chunks << 16}.
+template <typename T, typename C, bool FIELDS>
+__global__ void __launch_bounds__(TW, KF_MINB) kf_tma_multi(const KFArgs<C> *cases, const int4 *table)
+{
+    extern __shared__ __align__(128) unsigned char smraw[];
+    const int4 t = table[blockIdx.x];
+    kf_tma_cta<T, C, FIELDS>(cases[t.x], t.y, t.z, t.w & 0xffff, t.w >> 16, smraw);
+}
+
 template <typename T, typename C>
 void launch_tma(const KFArgs<C> &a, bool fields, int nx, int ny, cudaStream_t st)
 {
@@ -292,7 +310,20 @@ int configure_tma()
         return -1;
     if (cudaFuncSetAttribute(kf_tma<T, C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
         return -1;
+    if (cudaFuncSetAttribute(kf_tma_multi<T, C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+        return -1;
+    if (cudaFuncSetAttribute(kf_tma_multi<T, C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+        cudaSuccess)
+        return -1;
     return 0;
+}
+
+// case table entry {case, strip, chunk, gx | gy << 16} of the staged kernel's
+// grid for one lattice
+void tma_grid(int nx, int ny, int rows_per_cta, int *gx, int *gy)
+{
+    *gx = (nx + TW - 1) / TW;
+    *gy = (ny - 2 + rows_per_cta - 1) / rows_per_cta + 1;
 }
 
 template <typename T, typename C, int VEC>
@@ -392,6 +423,48 @@ __global__ void residual_kernel(const C *__restrict__ fa, const C *__restrict__ 
 }
 
 }  // namespace
+
+template <typename T, typename C>
+int launch_kf_multi_t(const void *cases, const int4 *table, int nentries, bool fields, cudaStream_t st)
+{
+    static bool configured = false;   // per process; the attribute is per function
+    if (!configured) {
+        if (configure_tma<T, C>()) return -1;
+        configured = true;
+    }
+    const size_t smem = tma_smem<T>();
+    if (fields)
+        kf_tma_multi<T, C, true><<<nentries, TW, smem, st>>>((const KFArgs<C> *)cases, table);
+    else
+        kf_tma_multi<T, C, false><<<nentries, TW, smem, st>>>((const KFArgs<C> *)cases, table);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+// lattice arguments of one case in the storage precision's compute type
+size_t kf_args_size(int prec) { return prec == LBM_PREC_FP64 ? sizeof(KFArgs<double>) : sizeof(KFArgs<float>); }
+
+void kf_args_write(lbm_handle *h, const void *fin, void *fout, void *fields, int mode, void *dst)
+{
+    if (h->prec == LBM_PREC_FP64)
+        *(KFArgs<double> *)dst = make_kf_args<double>(h, fin, fout, fields, mode);
+    else
+        *(KFArgs<float> *)dst = make_kf_args<float>(h, fin, fout, fields, mode);
+}
+
+void kf_tma_grid(const lbm_handle *h, int *gx, int *gy) { tma_grid(h->nx, h->ny, h->kf_rows, gx, gy); }
+
+// the staged lattice kernel over a batch of cases (device arrays of their
+// arguments and of the case table)
+int launch_kf_multi(int prec, const void *cases, const int4 *table, int nentries, bool fields, cudaStream_t st)
+{
+    switch (prec) {
+    case LBM_PREC_FP32: return launch_kf_multi_t<float, float>(cases, table, nentries, fields, st);
+    case LBM_PREC_FP64: return launch_kf_multi_t<double, double>(cases, table, nentries, fields, st);
+    case LBM_PREC_FP16: return launch_kf_multi_t<__half, float>(cases, table, nentries, fields, st);
+    case LBM_PREC_BF16: return launch_kf_multi_t<__nv_bfloat16, float>(cases, table, nentries, fields, st);
+    }
+    return -1;
+}
 
 int launch_kf(lbm_handle *h, const void *fin, void *fout, void *fields, int mode, cudaStream_t st)
 {

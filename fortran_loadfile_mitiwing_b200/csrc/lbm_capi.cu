@@ -393,6 +393,11 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
 
 }  // namespace
 
+// for lbm_batch.cu
+int handle_prepare_ib(lbm_handle *h) { return ensure_ib(h); }
+int handle_error(lbm_handle *h, int code, const char *msg) { return set_err(h, code, msg); }
+int handle_status(lbm_handle *h) { return check_status(h); }
+
 extern "C" {
 
 int lbm_default_params(lbm_params *p)

@@ -72,6 +72,7 @@ struct IBArgs {
     int *wmax;          // half-bandwidth found by the assembly
     // slot and working-set strides of the batched factorization (elements)
     int nslots;
+    int static_order;   // one rigid body: fixed solve order (ib_order leaves it)
     long long st_mk, st_perm, st_B, wk_blocks, wk_gf;
     PatchInfo *pinfo;
     int *tiles;         // per patch tile: marker count, then the listed markers (slot)
@@ -196,6 +197,20 @@ int launch_factor(lbm_handle *h, int step0, int count, cudaStream_t st);
 int launch_flow(lbm_handle *h, const void *fin, void *fout, void *fields, int step_index, int ring_slot, int slot,
                 cudaStream_t st);
 int launch_check(lbm_handle *h, int slot, int ring_slot, cudaStream_t st);
+// batches of cases stepped together (lbm_batch.cu)
+int handle_prepare_ib(lbm_handle *h);                    // immersed-boundary buffers (once per geometry)
+int handle_error(lbm_handle *h, int code, const char *msg);
+int handle_status(lbm_handle *h);                        // reads and clears the device status
+size_t kf_args_size(int prec);
+void kf_args_write(lbm_handle *h, const void *fin, void *fout, void *fields, int mode, void *dst);
+void kf_tma_grid(const lbm_handle *h, int *gx, int *gy);
+int launch_kf_multi(int prec, const void *cases, const int4 *table, int nentries, bool fields, cudaStream_t st);
+size_t ib_args_size();
+void ib_args_write(lbm_handle *h, const void *fin, int slot, void *dst);
+int launch_factor_batch(lbm_handle *const *hs, int ncase, const void *dargs, int step0, int count, cudaStream_t st);
+int launch_flow_batch(lbm_handle *const *hs, int ncase, const void *dargs, const void *dkf, int step_index,
+                      int ring_slot, bool fields, cudaStream_t st);
+int launch_check_batch(lbm_handle *const *hs, int ncase, const void *dargs, int ring_slot, cudaStream_t st);
 int ib_tile_ints();   // ints per patch tile of the tile lists
 int launch_residual(lbm_handle *h, const void *fa, const void *fb, double *out2);
 int launch_unpack(lbm_handle *h, const void *fsrc, double *dst);   // deviation -> f (FP64)

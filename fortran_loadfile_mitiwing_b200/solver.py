@@ -138,3 +138,75 @@ class Lbm:
     @property
     def step_index(self):
         return self.lib.lbm_step_index(self.h)
+
+
+class Batch:
+    """Several initialised cases stepped together on one GPU
+    (lbm_batch_create ... lbm_batch_destroy): one lattice launch for all of
+    them driven by a case table, one launch per immersed-boundary stage. The
+    cases stay usable as `Lbm` objects; each one's results are those of
+    running it alone."""
+
+    def __init__(self, cases, lib=None):
+        self.cases = list(cases)
+        self.lib = lib or self.cases[0].lib
+        arr = (C.c_void_p * len(self.cases))(*[c.h.value for c in self.cases])
+        b = C.c_void_p()
+        rc = self.lib.lbm_batch_create(arr, len(self.cases), C.byref(b))
+        if rc != 0:
+            msgs = "; ".join(c.lib.lbm_last_error(c.h).decode() for c in self.cases)
+            raise LbmError(rc, msgs)
+        self.b = b
+        self.rows = 0
+
+    def close(self):
+        if getattr(self, "b", None):
+            self.lib.lbm_batch_destroy(self.b)
+            self.b = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_rows(self, rows_per_cta):
+        rc = self.lib.lbm_batch_set_rows(self.b, int(rows_per_cta))
+        if rc != 0:
+            raise LbmError(rc, self.lib.lbm_batch_last_error(self.b).decode())
+        self.rows = int(rows_per_cta)
+
+    def run(self, nsteps, keep_rows=True):
+        """Steps every case up to `nsteps` times; returns each case's force
+        rows (trimmed to the steps it ran) or the step counts."""
+        n = len(self.cases)
+        bufs = [np.zeros((max(nsteps, 1), c.row_len)) for c in self.cases] if keep_rows else None
+        ptrs = (_abi._D * n)(*[dptr(x) for x in bufs]) if keep_rows else None
+        done = (C.c_int * n)()
+        rc = self.lib.lbm_batch_run(self.b, int(nsteps), ptrs, done)
+        if rc not in (0, 1):
+            raise LbmError(rc, self.lib.lbm_batch_last_error(self.b).decode())
+        if not keep_rows:
+            return list(done)
+        return [bufs[c][: done[c]] for c in range(n)]
+
+    def autotune(self, steps_per_trial=20, candidates=(4, 8, 16)):
+        """Picks the lattice kernel's rows per CTA for this batch by timing
+        `steps_per_trial` real steps with each candidate (the steps advance
+        the cases; the results do not depend on the choice). Returns
+        {rows: seconds per step} and keeps the fastest."""
+        import time
+        timing = {}
+        for r in candidates:
+            self.set_rows(r)
+            t0 = time.perf_counter()
+            self.run(steps_per_trial, keep_rows=False)
+            timing[r] = (time.perf_counter() - t0) / steps_per_trial
+        self.set_rows(min(timing, key=timing.get))
+        return timing

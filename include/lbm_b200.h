@@ -232,6 +232,29 @@ LBM_API int lbm_step_index(const lbm_t *h);
  * errors of lbm_create. The string stays valid until the next call on h. */
 LBM_API const char *lbm_last_error(const lbm_t *h);
 
+/* ---- batches: several cases stepped together on one GPU ----------------
+ * The reference runs one case per process (main.f90); flapping-wing studies
+ * are sweeps of many cases. A batch steps initialised handles of different
+ * grid sizes and kinematics in lockstep with one launch per kernel for all of
+ * them: one lattice launch driven by a case table, and each immersed-boundary
+ * stage as one launch over the cases. Each case's results are bit-for-bit
+ * those of running it alone (lbm_run). The batch does not own the handles.
+ *   lbm_batch_create: cases must be initialised, share storage precision,
+ *     device and step index, and have markers.
+ *   lbm_batch_run: runs up to nsteps steps of every case; a case stops when
+ *     its motion table ends (done_steps[c], nullable; LBM_DONE when any case
+ *     stopped early). force_rows[c] (nullable, or an array of nullable
+ *     pointers) receives case c's rows as lbm_run would. Fields are kept for
+ *     the last two steps of the call, as lbm_run.
+ *   lbm_batch_set_rows: rows per CTA of the lattice kernel for the batch
+ *     (0: the cases' own); the batch autotuner of the Python layer sets it. */
+typedef struct lbm_batch lbm_batch_t;
+LBM_API int lbm_batch_create(lbm_t *const *cases, int count, lbm_batch_t **out);
+LBM_API int lbm_batch_destroy(lbm_batch_t *b);
+LBM_API int lbm_batch_set_rows(lbm_batch_t *b, int rows_per_cta);
+LBM_API int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *done_steps);
+LBM_API const char *lbm_batch_last_error(const lbm_batch_t *b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,58 @@
+"""Batches: several cases of different grid sizes and kinematics stepped
+together (one lattice launch driven by a case table, one launch per
+immersed-boundary stage) give each case exactly the results of running it
+alone: force rows and populations bit-for-bit."""
+import numpy as np
+import pytest
+
+from fortran_loadfile_mitiwing_b200 import Batch, Lbm, cases
+
+pytestmark = pytest.mark.gpu
+
+SPECS = [
+    dict(nx=96, ny=64, chord=24, pivot=(33, 33), markers=40, heave=0.25, pitch_deg=10.0, st=0.3, seed=7),
+    dict(nx=160, ny=96, chord=32, pivot=(50, 49), markers=64, heave=0.2, pitch_deg=20.0, st=0.25, seed=11),
+    dict(nx=128, ny=64, chord=20, pivot=(40, 33), markers=36, heave=0.3, pitch_deg=0.0, st=0.35, seed=13),
+]
+
+
+def build(precision, n_steps, specs=SPECS, lib=None):
+    return [Lbm.from_case(cases.small_case(precision=precision, n_steps=n_steps, **sp), lib) for sp in specs]
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_batch_equals_each_case_alone(gpu_lib, precision):
+    steps = 37   # several factorization batches of 4 steps, and a partial one
+    together = build(precision, steps + 20, lib=gpu_lib)
+    alone = build(precision, steps + 20, lib=gpu_lib)
+    with Batch(together) as b:
+        rows_b = b.run(steps)
+    for c, (t, a) in enumerate(zip(together, alone)):
+        rows_a = a.run(steps)
+        np.testing.assert_array_equal(rows_b[c], rows_a, err_msg=f"case {c} force rows")
+        np.testing.assert_array_equal(t.populations(), a.populations(), err_msg=f"case {c} populations")
+
+
+def test_batch_cases_stop_at_their_motion_end(gpu_lib):
+    lens = [30, 50, 40]
+    together = [Lbm.from_case(cases.small_case(precision="fp32", n_steps=n, **sp), gpu_lib) for n, sp in zip(lens, SPECS)]
+    with Batch(together) as b:
+        done = b.run(100, keep_rows=False)
+    # a case runs while (n - 1) dt <= motion end; the table covers n_steps rows
+    alone = [Lbm.from_case(cases.small_case(precision="fp32", n_steps=n, **sp), gpu_lib) for n, sp in zip(lens, SPECS)]
+    for c, a in enumerate(alone):
+        rows_a = a.run(100)
+        assert done[c] == rows_a.shape[0], (c, done[c], rows_a.shape[0])
+        np.testing.assert_array_equal(together[c].populations(), a.populations())
+
+
+def test_autotuned_batch_still_equals_alone(gpu_lib):
+    together = build("fp32", 120, lib=gpu_lib)
+    alone = build("fp32", 120, lib=gpu_lib)
+    with Batch(together) as b:
+        timing = b.autotune(steps_per_trial=5, candidates=(4, 8, 16))
+        assert set(timing) == {4, 8, 16} and b.rows in timing
+        b.run(10, keep_rows=False)
+    for t, a in zip(together, alone):
+        a.run(25)
+        np.testing.assert_array_equal(t.populations(), a.populations())
