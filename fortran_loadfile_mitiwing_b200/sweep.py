@@ -1,0 +1,110 @@
+"""Batched sweep throughput: many flapping-wing cases of different grid sizes
+and kinematics on one GPU, stepped one at a time (each case alone through
+lbm_run) and stepped together (a Batch: one lattice launch over a case
+table, one launch per immersed-boundary stage), in FP32 and FP16 storage.
+
+Cases (seeded): Nx uniform in [512, 2048] (multiples of 64), Ny = Nx/2,
+chord = Ny/4, Re in [100, 2000], heave amplitude in [0.1c, 0.75c], pitch
+amplitude in [0, 45] deg, phase in [0, 180] deg, St in [0.15, 0.45]; NACA
+0012 with 2 markers per lattice unit of chord, pivot at the quarter chord on
+node (2c+1, Ny/2+1), U0 = 0.05, seeded 1e-4 initial perturbation.
+
+Each form runs a fixed sample of steps per case after a warm-up; the report
+gives the aggregate lattice updates per second and the cases per hour that
+rate gives for 5 flapping periods of every case (a case's period is
+c / (f U0) steps, f = St / (2 heave)). Run as
+`python -m fortran_loadfile_mitiwing_b200.sweep [--cases N] [--steps S]`;
+prints one JSON object. Needs a GPU.
+"""
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import cases as cs
+from .solver import Batch, Lbm
+
+U0 = 0.05
+
+
+def sweep_specs(n=64, seed=2026, nx_lo=512, nx_hi=2048):
+    rng = np.random.default_rng(seed)
+    out = []
+    for c in range(n):
+        nx = int(rng.integers(nx_lo // 64, nx_hi // 64 + 1)) * 64
+        ny = nx // 2
+        chord = ny // 4
+        spec = dict(nx=nx, ny=ny, chord=chord, pivot=(2 * chord + 1, ny // 2 + 1), markers=2 * chord,
+                    re=float(rng.uniform(100.0, 2000.0)), heave=float(rng.uniform(0.1, 0.75)),
+                    pitch_deg=float(rng.uniform(0.0, 45.0)), phase_deg=float(rng.uniform(0.0, 180.0)),
+                    st=float(rng.uniform(0.15, 0.45)), seed=seed + c)
+        spec["period_steps"] = chord / (spec["st"] / (2.0 * spec["heave"]) * U0)
+        out.append(spec)
+    return out
+
+
+def make(spec, n_steps, precision, lib=None):
+    kw = {k: spec[k] for k in ("nx", "ny", "chord", "pivot", "markers", "re", "heave", "pitch_deg", "phase_deg",
+                               "st", "seed")}
+    return Lbm.from_case(cs.heave_pitch_case(n_steps=n_steps, precision=precision, uu=U0, **kw), lib)
+
+
+def cases_per_hour(specs, lups_per_s, periods=5):
+    work = sum(s["nx"] * s["ny"] * periods * s["period_steps"] for s in specs)
+    return len(specs) * 3600.0 * lups_per_s / work
+
+
+def run_alone(specs, steps, warmup, precision, lib=None):
+    total, lups = 0.0, 0
+    for sp in specs:
+        s = make(sp, steps + warmup + 8, precision, lib)
+        s.run(warmup, keep_rows=False)
+        t0 = time.perf_counter()
+        s.run(steps, keep_rows=False)
+        total += time.perf_counter() - t0
+        lups += sp["nx"] * sp["ny"] * steps
+        s.close()
+    return lups / total, total
+
+
+def run_batch(specs, steps, warmup, precision, lib=None, tune=True):
+    hs = [make(sp, steps + warmup + 64, precision, lib) for sp in specs]
+    b = Batch(hs)
+    timing = b.autotune(steps_per_trial=max(2, warmup // 3), candidates=(4, 8, 16)) if tune else {}
+    b.run(warmup, keep_rows=False)
+    t0 = time.perf_counter()
+    done = b.run(steps, keep_rows=False)
+    el = time.perf_counter() - t0
+    assert all(d == steps for d in done), done
+    lups = sum(sp["nx"] * sp["ny"] * steps for sp in specs)
+    b.close()
+    for h in hs:
+        h.close()
+    return lups / el, el, timing, b.rows
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--cases", type=int, default=64)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=12)
+    ap.add_argument("--seed", type=int, default=2026)
+    args = ap.parse_args()
+    specs = sweep_specs(args.cases, args.seed)
+    res = {"cases": args.cases, "steps_per_case": args.steps, "seed": args.seed,
+           "grid_nodes_total": sum(s["nx"] * s["ny"] for s in specs)}
+    r, t = run_alone(specs, args.steps, args.warmup, "fp32")
+    res["alone_fp32"] = {"mlups": r / 1e6, "seconds": t, "cases_per_hour_5_periods": cases_per_hour(specs, r)}
+    for prec in ("fp32", "fp16"):
+        r, t, timing, rows = run_batch(specs, args.steps, args.warmup, prec)
+        res["batch_" + prec] = {"mlups": r / 1e6, "seconds": t, "cases_per_hour_5_periods": cases_per_hour(specs, r),
+                                "rows_per_cta": rows, "autotune_s_per_step": timing}
+    base = res["alone_fp32"]["cases_per_hour_5_periods"]
+    for k in ("batch_fp32", "batch_fp16"):
+        res[k]["vs_alone_fp32"] = res[k]["cases_per_hour_5_periods"] / base
+    print(json.dumps(res))
+
+
+if __name__ == "__main__":
+    main()
