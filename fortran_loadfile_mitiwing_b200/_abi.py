@@ -75,9 +75,13 @@ ABI = {
     "lbm_residual_device": (C.c_int, [_P, _P, _P, _P, C.c_int, C.c_int, C.c_int, _P, _D]),
     "lbm_get_launch_count": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
     "lbm_step_index": (C.c_int, [_P]),
+    "lbm_device_bytes": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
     "lbm_last_error": (C.c_char_p, [_P]),
     "lbm_batch_create": (C.c_int, [C.POINTER(_P), C.c_int, C.POINTER(_P)]),
     "lbm_batch_destroy": (C.c_int, [_P]),
+    "lbm_batch_add": (C.c_int, [_P, _P]),
+    "lbm_batch_remove": (C.c_int, [_P, _P]),
+    "lbm_batch_count": (C.c_int, [_P]),
     "lbm_batch_set_rows": (C.c_int, [_P, C.c_int]),
     "lbm_batch_run": (C.c_int, [_P, C.c_int, C.POINTER(_D), C.POINTER(C.c_int)]),
     "lbm_batch_last_error": (C.c_char_p, [_P]),

@@ -132,6 +132,15 @@ __device__ __forceinline__ const double *motion_row(const IBArgs &a, int step_in
     return a.mstep + (long long)(idx - 1) * a.mcols;
 }
 
+// Step of this CTA's member of a factorization launch: step0 + blockIdx.y,
+// or per case in batched launches (the case's own start and count; -1 for
+// the members past its count).
+template <bool BATCH> __device__ __forceinline__ int factor_step(const IBArgs &base, int step0)
+{
+    if (!BATCH) return step0 + (int)blockIdx.y;
+    return (int)blockIdx.y < base.fcount ? base.fstep0 + (int)blockIdx.y : -1;
+}
+
 // Arguments of one member of a batched factorization launch: the step
 // step0 + blockIdx.y, its buffer slot (step modulo the slot count) and the
 // member's working set.
@@ -221,7 +230,8 @@ template <bool BATCH>
 __global__ void __launch_bounds__(128) ib_geometry(const IBArgs base0, const IBArgs *batch, int step0)
 {
     const IBArgs &base = BATCH ? batch[blockIdx.z] : base0;
-    const int step_index = step0 + blockIdx.y;
+    const int step_index = factor_step<BATCH>(base, step0);
+    if (step_index < 0) return;
     const IBArgs a = member_args(base, step_index);
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.nseg) return;
@@ -311,7 +321,9 @@ template <bool BATCH>
 __global__ void __launch_bounds__(1024) ib_order(const IBArgs base0, const IBArgs *batch, int step0)
 {
     const IBArgs &base = BATCH ? batch[blockIdx.z] : base0;
-    const IBArgs a = member_args(base, step0 + blockIdx.y);
+    const int step_index = factor_step<BATCH>(base, step0);
+    if (step_index < 0) return;
+    const IBArgs a = member_args(base, step_index);
     if (a.static_order) return;   // one rigid body: fixed order (batched launches reach it)
     extern __shared__ double osm[];
     const int n = a.nseg, tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, warp = tid >> 5;
@@ -378,7 +390,9 @@ template <bool BATCH>
 __global__ void __launch_bounds__(256) ib_assemble(const IBArgs base0, const IBArgs *batch, int step0)
 {
     const IBArgs &base = BATCH ? batch[blockIdx.z] : base0;
-    const IBArgs a = member_args(base, step0 + blockIdx.y);
+    const int step_index = factor_step<BATCH>(base, step0);
+    if (step_index < 0) return;
+    const IBArgs a = member_args(base, step_index);
     const int n = a.nseg, blk = blockIdx.x, tid = threadIdx.x;
     if (blk >= (n + BS - 1) / BS) return;   // batched launches size the grid for the largest case
     __shared__ double ph[2 * BS][12];
@@ -603,7 +617,9 @@ template <bool BATCH>
 __global__ void __launch_bounds__(FACTOR_THREADS) ib_factor(const IBArgs base0, const IBArgs *batch, int step0)
 {
     const IBArgs &base = BATCH ? batch[blockIdx.z] : base0;
-    const IBArgs a = member_args(base, step0 + blockIdx.y);
+    const int step_index = factor_step<BATCH>(base, step0);
+    if (step_index < 0) return;
+    const IBArgs a = member_args(base, step_index);
     extern __shared__ __align__(16) double Wbase[];
     const int n = a.nseg, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     __shared__ int bad, dense;
@@ -803,7 +819,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a0, const
     __shared__ int timed_out;
     if (tid == 0) {
         double time;
-        const double *row = motion_row(a, step_index, &time);
+        const double *row = motion_row(a, BATCH ? a.cur_step : step_index, &time);
         write_header(a, row, time, ring_slot);
         const unsigned fs = *a.fstatus;
         if (fs) { atomicOr(a.status, fs); *a.fstatus = 0u; }
@@ -962,7 +978,9 @@ template <bool BATCH>
 __global__ void __launch_bounds__(256) ib_tile_scatter(const IBArgs base0, const IBArgs *batch, int step0)
 {
     const IBArgs &base = BATCH ? batch[blockIdx.z] : base0;
-    const IBArgs a = member_args(base, step0 + blockIdx.y);
+    const int step_index = factor_step<BATCH>(base, step0);
+    if (step_index < 0) return;
+    const IBArgs a = member_args(base, step_index);
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.nseg) return;
     const PatchInfo pi = *a.pinfo;
@@ -984,7 +1002,9 @@ template <bool BATCH>
 __global__ void __launch_bounds__(TILE_CAP) ib_tile_sort(const IBArgs base0, const IBArgs *batch, int step0)
 {
     const IBArgs &base = BATCH ? batch[blockIdx.z] : base0;
-    const IBArgs a = member_args(base, step0 + blockIdx.y);
+    const int step_index = factor_step<BATCH>(base, step0);
+    if (step_index < 0) return;
+    const IBArgs a = member_args(base, step_index);
     __shared__ int key[TILE_CAP];
     const int ntile = *a.nsup, t = threadIdx.x;
     for (int c = blockIdx.x; c < ntile; c += gridDim.x) {
@@ -1255,7 +1275,7 @@ __global__ void __launch_bounds__(256) ib_tile_update(const IBArgs a0, const IBA
                 const double drho = (((double)g[0] + (double)g[1]) + ((double)g[2] + (double)g[3])) +
                                     (((double)g[4] + (double)g[5]) + ((double)g[6] + (double)g[7])) + (double)g[8];
                 const double rho = 1.0 + drho;
-                const double *row = motion_row(a, step_index, nullptr);
+                const double *row = motion_row(a, BATCH ? a.cur_step : step_index, nullptr);
                 const double temp1 = 2.0 * rho * du, temp2 = 2.0 * rho * dv;
                 const double sa = row[4 + 9 * wing], sb = row[7 + 9 * wing];
                 fx = -temp1;
@@ -1348,6 +1368,8 @@ IBArgs make_args(lbm_handle *h, const void *fin, int slot)
     a.partial = h->d_partial; a.counter = h->d_counter;
     a.force_ring = h->d_ring; a.row_len = h->row_len;
     a.status = h->d_status; a.solve_res = h->d_solve_res;
+    a.cur_step = h->n;
+    a.fstep0 = 0; a.fcount = 0;
     return a;
 }
 
@@ -1471,6 +1493,14 @@ int launch_flow(lbm_handle *h, const void *fin, void *fout, void *fields, int st
 size_t ib_args_size() { return sizeof(IBArgs); }
 
 void ib_args_write(lbm_handle *h, const void *fin, int slot, void *dst) { *(IBArgs *)dst = make_args(h, fin, slot); }
+
+void ib_factor_args_write(lbm_handle *h, int step0, int count, void *dst)
+{
+    IBArgs a = make_args(h, nullptr, 0);
+    a.fstep0 = step0;
+    a.fcount = count;
+    *(IBArgs *)dst = a;
+}
 
 namespace {
 

@@ -1,40 +1,54 @@
 // lbm_batch.cu -- several cases (handles) stepped together on one GPU.
 //
-// A batch steps its cases in lockstep, with one launch per kernel for all of
-// them: the lattice update of every case is one launch of the staged kernel
-// driven by a case table (CTA -> case, strip, row chunk), and each stage of
-// the immersed boundary (interpolation, solve, correction tiles, forces and
-// residual; and, per batch of steps, the factorization chain) is one launch
-// with the case as grid z, the cases' arguments read from device arrays. The
-// streams and events are the batch's own, with the same structure as one
-// handle's step: factorization one batch of steps ahead, the flow chain on a
-// high-priority stream beside the lattice update.
+// A batch steps its cases with one launch per kernel for all of them: the
+// lattice update of every case is one launch of the staged kernel driven by a
+// case table (CTA -> case, strip, row chunk), and each stage of the immersed
+// boundary (interpolation, solve, correction tiles, forces and residual; and
+// the factorization chain of a batch of steps) is one launch with the case as
+// grid z, the cases' arguments read from device arrays. The streams are the
+// batch's own, with the structure of one handle's step: factorization a batch
+// of steps ahead, the flow chain on a high-priority stream beside the lattice
+// update. Cases may be at different steps (each carries its own step index,
+// slots and factorization state, kept in its handle), and may be added and
+// removed between runs: the base of the serving loop.
 //
 // Every kernel computes each case exactly as the single-case launches do, so
 // a case's results in a batch are bit-for-bit those of running it alone.
 #include <algorithm>
 #include <cmath>
+#include <string>
 #include <vector>
 
 #include "lbm_internal.h"
 
+namespace {
+constexpr int kFactorRing = 8;   // staging buffers of factorization arguments in flight
+// events of the latest factorization launches; a case's halves are at most
+// 2 factorization batches (2K steps, two launches a step) old when used, and
+// a wait on a newer recording of a reused event only waits longer
+constexpr int kGroupRing = 64;
+}
+
 struct lbm_batch {
     std::vector<lbm_handle *> cases;
-    int prec = 0, fbatch = 4, nslots = 8;
+    int prec = -1, fbatch = 4, nslots = 8, dev = 0;
     cudaStream_t main = nullptr, side = nullptr, fstream = nullptr;
-    cudaEvent_t ev_batch[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
-    cudaEvent_t ev_ib = nullptr, ev_done = nullptr;
-    int batch_in_half[2] = {-1, -1};
-    // device argument arrays: factorization (slot 0 base), flow chain (per
-    // step, double-buffered so a step's upload never overwrites arguments a
-    // queued launch still reads), lattice, case table
-    void *d_fargs[2] = {nullptr, nullptr}, *d_sargs[2] = {nullptr, nullptr}, *d_kargs[2] = {nullptr, nullptr};
-    int4 *d_table[2] = {nullptr, nullptr};
-    void *h_fargs[2] = {nullptr, nullptr}, *h_sargs[2] = {nullptr, nullptr}, *h_kargs[2] = {nullptr, nullptr};
-    int4 *h_table[2] = {nullptr, nullptr};
-    cudaEvent_t ev_upload[2] = {nullptr, nullptr}, ev_fupload[2] = {nullptr, nullptr};
+    cudaEvent_t ev_ib = nullptr, ev_done = nullptr, ev_fready = nullptr, ev_side = nullptr;
+    // argument arrays: flow chain and lattice per step (double-buffered so a
+    // step's upload never overwrites arguments a queued launch still reads),
+    // case table, and a ring of factorization argument buffers
+    int cap = 0;         // cases the arrays hold
+    int table_cap = 0;   // case-table entries
+    void *d_sargs[2] = {nullptr, nullptr}, *d_kargs[2] = {nullptr, nullptr};
+    void *h_sargs[2] = {nullptr, nullptr}, *h_kargs[2] = {nullptr, nullptr};
+    int4 *d_table[2] = {nullptr, nullptr}, *h_table[2] = {nullptr, nullptr};
+    cudaEvent_t ev_upload[2] = {nullptr, nullptr};
+    void *d_fargs[kFactorRing] = {}, *h_fargs[kFactorRing] = {};
+    cudaEvent_t ev_fup[kFactorRing] = {};
+    int fring = 0;
+    cudaEvent_t ev_group[kGroupRing] = {};
+    long long gseq = 0;   // factorization launches so far
     size_t ib_sz = 0, kf_sz = 0;
-    int table_cap = 0;
     int rows_per_cta = 0;   // 0: the cases' own setting
     std::string err;
 };
@@ -53,11 +67,15 @@ int berr(lbm_batch *b, int code, const std::string &msg)
         if (e_ != cudaSuccess) return berr(b, LBM_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-void free_batch(lbm_batch *b)
+void sync_streams(lbm_batch *b)
 {
     if (b->main) cudaStreamSynchronize(b->main);
     if (b->side) cudaStreamSynchronize(b->side);
     if (b->fstream) cudaStreamSynchronize(b->fstream);
+}
+
+void free_arrays(lbm_batch *b)
+{
     for (int q = 0; q < 2; ++q) {
         if (b->d_sargs[q]) cudaFree(b->d_sargs[q]);
         if (b->d_kargs[q]) cudaFree(b->d_kargs[q]);
@@ -65,18 +83,109 @@ void free_batch(lbm_batch *b)
         if (b->h_sargs[q]) cudaFreeHost(b->h_sargs[q]);
         if (b->h_kargs[q]) cudaFreeHost(b->h_kargs[q]);
         if (b->h_table[q]) cudaFreeHost(b->h_table[q]);
-        if (b->ev_batch[q]) cudaEventDestroy(b->ev_batch[q]);
-        if (b->ev_free[q]) cudaEventDestroy(b->ev_free[q]);
-        if (b->ev_upload[q]) cudaEventDestroy(b->ev_upload[q]);
-        if (b->ev_fupload[q]) cudaEventDestroy(b->ev_fupload[q]);
-        if (b->d_fargs[q]) cudaFree(b->d_fargs[q]);
-        if (b->h_fargs[q]) cudaFreeHost(b->h_fargs[q]);
+        b->d_sargs[q] = b->d_kargs[q] = b->h_sargs[q] = b->h_kargs[q] = nullptr;
+        b->d_table[q] = b->h_table[q] = nullptr;
     }
-    if (b->ev_ib) cudaEventDestroy(b->ev_ib);
-    if (b->ev_done) cudaEventDestroy(b->ev_done);
+    for (int r = 0; r < kFactorRing; ++r) {
+        if (b->d_fargs[r]) cudaFree(b->d_fargs[r]);
+        if (b->h_fargs[r]) cudaFreeHost(b->h_fargs[r]);
+        b->d_fargs[r] = b->h_fargs[r] = nullptr;
+    }
+    b->cap = b->table_cap = 0;
+}
+
+void free_batch(lbm_batch *b)
+{
+    sync_streams(b);
+    free_arrays(b);
+    for (int q = 0; q < 2; ++q)
+        if (b->ev_upload[q]) cudaEventDestroy(b->ev_upload[q]);
+    for (int r = 0; r < kFactorRing; ++r)
+        if (b->ev_fup[r]) cudaEventDestroy(b->ev_fup[r]);
+    for (int r = 0; r < kGroupRing; ++r)
+        if (b->ev_group[r]) cudaEventDestroy(b->ev_group[r]);
+    for (cudaEvent_t e : {b->ev_ib, b->ev_done, b->ev_fready, b->ev_side})
+        if (e) cudaEventDestroy(e);
     if (b->main) cudaStreamDestroy(b->main);
     if (b->side) cudaStreamDestroy(b->side);
     if (b->fstream) cudaStreamDestroy(b->fstream);
+}
+
+// argument arrays for `ncase` cases and `ntab` case-table entries (grown, never shrunk)
+int reserve(lbm_batch *b, int ncase, int ntab)
+{
+    if (ncase <= b->cap && ntab <= b->table_cap) return LBM_OK;
+    sync_streams(b);
+    const int nc = std::max(ncase, b->cap), nt = std::max(ntab, b->table_cap);
+    free_arrays(b);
+    for (int q = 0; q < 2; ++q) {
+        BCK(cudaMalloc(&b->d_sargs[q], nc * b->ib_sz), "alloc");
+        BCK(cudaMalloc(&b->d_kargs[q], nc * b->kf_sz), "alloc");
+        BCK(cudaMalloc(&b->d_table[q], sizeof(int4) * (size_t)nt), "alloc");
+        BCK(cudaMallocHost(&b->h_sargs[q], nc * b->ib_sz), "alloc");
+        BCK(cudaMallocHost(&b->h_kargs[q], nc * b->kf_sz), "alloc");
+        BCK(cudaMallocHost((void **)&b->h_table[q], sizeof(int4) * (size_t)nt), "alloc");
+    }
+    for (int r = 0; r < kFactorRing; ++r) {
+        BCK(cudaMalloc(&b->d_fargs[r], nc * b->ib_sz), "alloc");
+        BCK(cudaMallocHost(&b->h_fargs[r], nc * b->ib_sz), "alloc");
+    }
+    b->cap = nc;
+    b->table_cap = nt;
+    return LBM_OK;
+}
+
+// case-table entries the case can need (the autotuner may use 4 rows per CTA)
+int table_need(lbm_handle *h)
+{
+    int gx, gy;
+    const int saved = h->kf_rows;
+    h->kf_rows = std::min(h->kf_rows, 4);
+    kf_tma_grid(h, &gx, &gy);
+    h->kf_rows = saved;
+    return gx * gy;
+}
+
+// a case the batch can take: initialised, with markers, matching the batch
+int check_case(lbm_batch *b, lbm_handle *h)
+{
+    if (!h->inited) return handle_error(h, LBM_ERR_STATE, "batch: lbm_init not called");
+    for (int w = 0; w < h->nwing; ++w)
+        if (!h->have_wing[w]) return handle_error(h, LBM_ERR_STATE, "batch: boundary of a wing not set");
+    if (h->nseg < 1) return handle_error(h, LBM_ERR_ARG, "batch: a case without markers");
+    if (h->prec != b->prec || h->fbatch != b->fbatch || h->nslots != b->nslots || h->dev != b->dev)
+        return handle_error(h, LBM_ERR_ARG, "batch: cases must share storage precision, factorization batch and device");
+    for (lbm_handle *o : b->cases)
+        if (o == h) return handle_error(h, LBM_ERR_ARG, "batch: the case is already in the batch");
+    int rc = handle_prepare_ib(h);
+    if (rc) return rc;
+    // the case's own queued work is done before the batch's streams use its buffers
+    if (h->fstream) cudaStreamSynchronize(h->fstream);
+    if (h->side) cudaStreamSynchronize(h->side);
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) return handle_error(h, LBM_ERR_CUDA, "batch: sync");
+    return LBM_OK;
+}
+
+int add_case(lbm_batch *b, lbm_handle *h)
+{
+    if (b->cases.empty() && (b->prec != h->prec || b->fbatch != h->fbatch || b->nslots != h->nslots)) {
+        // an empty batch takes the settings of the case that joins it
+        if (b->prec >= 0) {
+            sync_streams(b);
+            free_arrays(b);
+        }
+        b->prec = h->prec;
+        b->fbatch = h->fbatch;
+        b->nslots = h->nslots;
+        b->kf_sz = kf_args_size(b->prec);
+    }
+    int rc = check_case(b, h);
+    if (rc) return rc;
+    int need = table_need(h);
+    for (lbm_handle *o : b->cases) need += table_need(o);
+    if ((rc = reserve(b, (int)b->cases.size() + 1, need))) return rc;
+    b->cases.push_back(h);
+    return LBM_OK;
 }
 
 }  // namespace
@@ -85,87 +194,66 @@ extern "C" {
 
 int lbm_batch_create(lbm_t *const *cases, int count, lbm_batch_t **out)
 {
-    if (!out || !cases || count < 1) return LBM_ERR_ARG;
+    if (!out || count < 0 || (count > 0 && !cases)) return LBM_ERR_ARG;
     *out = nullptr;
     for (int c = 0; c < count; ++c)
         if (!cases[c]) return LBM_ERR_ARG;
-    lbm_handle *h0 = cases[0];
-    for (int c = 0; c < count; ++c) {
-        lbm_handle *h = cases[c];
-        if (!h->inited) return handle_error(h, LBM_ERR_STATE, "batch: lbm_init not called");
-        for (int w = 0; w < h->nwing; ++w)
-            if (!h->have_wing[w]) return handle_error(h, LBM_ERR_STATE, "batch: boundary of a wing not set");
-        if (h->nseg < 1) return handle_error(h, LBM_ERR_ARG, "batch: a case without markers");
-        if (h->prec != h0->prec || h->fbatch != h0->fbatch || h->nslots != h0->nslots || h->n != h0->n ||
-            h->dev != h0->dev)
-            return handle_error(h, LBM_ERR_ARG,
-                           "batch: cases must share storage precision, factorization batch, device and step index");
-        for (int d = 0; d < c; ++d)
-            if (cases[d] == h) return handle_error(h, LBM_ERR_ARG, "batch: a case appears twice");
-        const int rc = handle_prepare_ib(h);
-        if (rc) return rc;
-    }
     lbm_batch *b = new lbm_batch;
-    b->cases.assign(cases, cases + count);
-    b->prec = h0->prec;
-    b->fbatch = h0->fbatch;
-    b->nslots = h0->nslots;
+    if (count > 0)
+        b->dev = cases[0]->dev;
+    else
+        cudaGetDevice(&b->dev);
     b->ib_sz = ib_args_size();
-    b->kf_sz = kf_args_size(b->prec);
-    auto fail = [&](cudaError_t e, const char *what) {
-        h0->err = std::string("batch: ") + what + ": " + cudaGetErrorString(e);
+    cudaError_t e;
+    int prio_low = 0, prio_high = 0;
+    auto fail = [&](cudaError_t err, const char *what) {
+        if (count > 0) cases[0]->err = std::string("batch: ") + what + ": " + cudaGetErrorString(err);
         free_batch(b);
         delete b;
         return LBM_ERR_CUDA;
     };
-    cudaError_t e;
-    int prio_low = 0, prio_high = 0;
     if ((e = cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high)) != cudaSuccess) return fail(e, "priorities");
     if ((e = cudaStreamCreateWithFlags(&b->main, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
     if ((e = cudaStreamCreateWithPriority(&b->side, cudaStreamNonBlocking, prio_high)) != cudaSuccess)
         return fail(e, "stream");
     if ((e = cudaStreamCreateWithFlags(&b->fstream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
-    for (int q = 0; q < 2; ++q) {
-        if ((e = cudaEventCreateWithFlags(&b->ev_batch[q], cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
-        if ((e = cudaEventCreateWithFlags(&b->ev_free[q], cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
-        if ((e = cudaEventCreateWithFlags(&b->ev_upload[q], cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
-        if ((e = cudaEventCreateWithFlags(&b->ev_fupload[q], cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
-    }
-    if ((e = cudaEventCreateWithFlags(&b->ev_ib, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
-    if ((e = cudaEventCreateWithFlags(&b->ev_done, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
-    // case table capacity: every case's full grid
-    int cap = 0;
-    for (lbm_handle *h : b->cases) {
-        int gx, gy;
-        kf_tma_grid(h, &gx, &gy);
-        // the autotuner may use 4 rows per CTA: twice the chunks of 8
-        cap += gx * (2 * gy + 2);
-    }
-    b->table_cap = cap;
-    const size_t nc = (size_t)count;
-    for (int q = 0; q < 2; ++q) {
-        if ((e = cudaMalloc(&b->d_fargs[q], nc * b->ib_sz)) != cudaSuccess) return fail(e, "alloc");
-        if ((e = cudaMallocHost(&b->h_fargs[q], nc * b->ib_sz)) != cudaSuccess) return fail(e, "alloc");
-        if ((e = cudaMalloc(&b->d_sargs[q], nc * b->ib_sz)) != cudaSuccess) return fail(e, "alloc");
-        if ((e = cudaMalloc(&b->d_kargs[q], nc * b->kf_sz)) != cudaSuccess) return fail(e, "alloc");
-        if ((e = cudaMalloc(&b->d_table[q], sizeof(int4) * (size_t)cap)) != cudaSuccess) return fail(e, "alloc");
-        if ((e = cudaMallocHost(&b->h_sargs[q], nc * b->ib_sz)) != cudaSuccess) return fail(e, "alloc");
-        if ((e = cudaMallocHost(&b->h_kargs[q], nc * b->kf_sz)) != cudaSuccess) return fail(e, "alloc");
-        if ((e = cudaMallocHost((void **)&b->h_table[q], sizeof(int4) * (size_t)cap)) != cudaSuccess)
-            return fail(e, "alloc");
-    }
-    // every case's queued work on its own streams is done before the batch uses it
-    for (lbm_handle *h : b->cases) {
-        if (h->fstream) cudaStreamSynchronize(h->fstream);
-        if (h->side) cudaStreamSynchronize(h->side);
-        if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return fail(e, "sync");
-        // the batch keeps its own factorization slots: the cases' own
-        // lookahead is stale once the batch has stepped them
-        h->batch_in_half[0] = h->batch_in_half[1] = -1;
+    for (cudaEvent_t *ev : {&b->ev_ib, &b->ev_done, &b->ev_fready, &b->ev_side, &b->ev_upload[0], &b->ev_upload[1]})
+        if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+    for (int r = 0; r < kFactorRing; ++r)
+        if ((e = cudaEventCreateWithFlags(&b->ev_fup[r], cudaEventDisableTiming)) != cudaSuccess)
+            return fail(e, "event");
+    for (int r = 0; r < kGroupRing; ++r)
+        if ((e = cudaEventCreateWithFlags(&b->ev_group[r], cudaEventDisableTiming)) != cudaSuccess)
+            return fail(e, "event");
+    for (int c = 0; c < count; ++c) {
+        const int rc = add_case(b, cases[c]);
+        if (rc) {
+            free_batch(b);
+            delete b;
+            return rc;
+        }
     }
     *out = b;
     return LBM_OK;
 }
+
+int lbm_batch_add(lbm_batch_t *b, lbm_t *h)
+{
+    if (!b || !h) return LBM_ERR_ARG;
+    return add_case(b, h);
+}
+
+int lbm_batch_remove(lbm_batch_t *b, lbm_t *h)
+{
+    if (!b || !h) return LBM_ERR_ARG;
+    auto it = std::find(b->cases.begin(), b->cases.end(), h);
+    if (it == b->cases.end()) return berr(b, LBM_ERR_ARG, "batch: the case is not in the batch");
+    sync_streams(b);
+    b->cases.erase(it);
+    return LBM_OK;
+}
+
+int lbm_batch_count(const lbm_batch_t *b) { return b ? (int)b->cases.size() : LBM_ERR_ARG; }
 
 int lbm_batch_destroy(lbm_batch_t *b)
 {
@@ -188,70 +276,134 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
     const int nc = (int)b->cases.size();
     for (int c = 0; c < nc; ++c)
         if (done_steps) done_steps[c] = 0;
-    if (nsteps == 0) return LBM_OK;
+    if (nsteps == 0 || nc == 0) return LBM_OK;
     const int K = b->fbatch;
-    // the lattice kernel's rows per CTA (the autotuner's choice, else the cases')
-    std::vector<int> rows_saved(nc);
+    std::vector<int> rows_saved(nc), last_step(nc), done(nc, 0), start(nc, 0);
     for (int c = 0; c < nc; ++c) {
-        rows_saved[c] = b->cases[c]->kf_rows;
-        if (b->rows_per_cta > 0) b->cases[c]->kf_rows = b->rows_per_cta;
+        lbm_handle *h = b->cases[c];
+        rows_saved[c] = h->kf_rows;
+        if (b->rows_per_cta > 0) h->kf_rows = b->rows_per_cta;
+        const double dt = h->p.scale * h->p.uu;
+        last_step[c] = (int)std::floor((h->mend + 1.0e-12) / dt) + 1;   // last step with time <= mend
     }
     auto restore = [&]() {
         for (int c = 0; c < nc; ++c) b->cases[c]->kf_rows = rows_saved[c];
     };
-    std::vector<int> last_step(nc), done(nc, 0), pending_start(nc, 0);
+    // a case may have been stepped alone or re-initialised since the last
+    // run: its scratch is (re)made, its own queued work finished, and the
+    // case table sized for this run's rows per CTA
+    int need = 0;
     for (int c = 0; c < nc; ++c) {
         lbm_handle *h = b->cases[c];
-        const double dt = h->p.scale * h->p.uu;
-        last_step[c] = (int)std::floor((h->mend + 1.0e-12) / dt) + 1;   // last step with time <= mend
-    }
-    // every case must be at the same step; the batch's factorization slots
-    // are recomputed (a case may have been stepped alone since the last run)
-    for (int c = 1; c < nc; ++c)
-        if (b->cases[c]->n != b->cases[0]->n) {
+        const int rc0 = h->inited ? handle_prepare_ib(h) : handle_error(h, LBM_ERR_STATE, "batch: lbm_init not called");
+        if (rc0) {
             restore();
-            return berr(b, LBM_ERR_STATE, "batch: cases are not at the same step");
+            return berr(b, rc0, std::string("batch: case ") + std::to_string(c) + ": " + h->err);
         }
-    b->batch_in_half[0] = b->batch_in_half[1] = -1;
-    // the factorization of batch bi for every active case, into slot half bi & 1
-    auto factor_batch = [&](int bi, const std::vector<lbm_handle *> &act) -> int {
-        const int half = bi & 1;
-        b->batch_in_half[half] = bi;
-        const int s0 = std::max(1, bi * K);
-        BCK(cudaStreamWaitEvent(b->fstream, b->ev_free[half], 0), "wait");
-        // arguments of the active cases (slot 0 base with the slot strides)
-        BCK(cudaEventSynchronize(b->ev_fupload[half]), "sync upload");
-        for (size_t c = 0; c < act.size(); ++c) ib_args_write(act[c], nullptr, 0, (char *)b->h_fargs[half] + c * b->ib_sz);
-        BCK(cudaMemcpyAsync(b->d_fargs[half], b->h_fargs[half], act.size() * b->ib_sz, cudaMemcpyHostToDevice,
-                            b->fstream),
+        if (h->fstream) cudaStreamSynchronize(h->fstream);
+        if (h->side) cudaStreamSynchronize(h->side);
+        cudaStreamSynchronize(h->stream);
+        int gx, gy;
+        kf_tma_grid(h, &gx, &gy);
+        need += gx * gy;
+    }
+    if (const int rc0 = reserve(b, nc, need)) {
+        restore();
+        return rc0;
+    }
+    // One launch chain factorizes, for every case that needs it, the batch of
+    // steps bi*K .. bi*K+K-1 of that case (each case its own bi) into the
+    // case's slot half bi & 1. It follows the side stream's work so far on
+    // the factor stream (which finished every earlier use of those halves);
+    // the launch's event in the group ring marks it done, and each case
+    // remembers which launch filled each half.
+    const long long seq_start = b->gseq;
+    auto factor_needed = [&](const std::vector<lbm_handle *> &act, const std::vector<int> &idx, bool next) -> int {
+        std::vector<lbm_handle *> grp;
+        std::vector<int> grp_bi;
+        for (size_t c = 0; c < act.size(); ++c) {
+            lbm_handle *h = act[c];
+            const int bi = h->n / K + (next ? 1 : 0);
+            if (h->batch_in_half[bi & 1] == bi) continue;
+            if (next && bi * K > last_step[idx[c]]) continue;
+            grp.push_back(h);
+            grp_bi.push_back(bi);
+        }
+        if (grp.empty()) return LBM_OK;
+        const int r = b->fring;
+        b->fring = (b->fring + 1) % kFactorRing;
+        BCK(cudaStreamWaitEvent(b->fstream, b->ev_side, 0), "wait");
+        BCK(cudaEventSynchronize(b->ev_fup[r]), "sync upload");   // this staging buffer's previous upload
+        for (size_t c = 0; c < grp.size(); ++c) {
+            const int s0 = std::max(1, grp_bi[c] * K);   // steps start at 1
+            ib_factor_args_write(grp[c], s0, grp_bi[c] * K + K - s0, (char *)b->h_fargs[r] + c * b->ib_sz);
+        }
+        BCK(cudaMemcpyAsync(b->d_fargs[r], b->h_fargs[r], grp.size() * b->ib_sz, cudaMemcpyHostToDevice, b->fstream),
             "upload");
-        BCK(cudaEventRecord(b->ev_fupload[half], b->fstream), "event");
-        if (launch_factor_batch(act.data(), (int)act.size(), b->d_fargs[half], s0, K, b->fstream))
+        BCK(cudaEventRecord(b->ev_fup[r], b->fstream), "event");
+        if (launch_factor_batch(grp.data(), (int)grp.size(), b->d_fargs[r], 0, K, b->fstream))
             return berr(b, LBM_ERR_CUDA, "batch: launch factor");
-        BCK(cudaEventRecord(b->ev_batch[half], b->fstream), "event");
+        const long long seq = ++b->gseq;
+        BCK(cudaEventRecord(b->ev_group[seq % kGroupRing], b->fstream), "event");
+        for (size_t c = 0; c < grp.size(); ++c) {
+            const int half = grp_bi[c] & 1;
+            grp[c]->batch_in_half[half] = grp_bi[c];
+            grp[c]->fgroup[half] = seq;
+        }
         return LBM_OK;
     };
-    BCK(cudaEventRecord(b->ev_done, b->main), "event");
     int rc = LBM_OK, pending = 0, step = 0;
+    // copies the force rows of the steps since the last flush (ring rows
+    // 0 .. rows-1, each case its own count) and reads the cases' status
+    auto flush = [&]() -> int {
+        BCK(cudaStreamWaitEvent(b->main, b->ev_side, 0), "wait");
+        for (int c = 0; c < nc; ++c) {
+            lbm_handle *h = b->cases[c];
+            const int rows = done[c] - start[c];
+            if (force_rows && force_rows[c] && rows > 0)
+                BCK(cudaMemcpyAsync(force_rows[c] + (size_t)start[c] * h->row_len, h->d_ring,
+                                    sizeof(double) * h->row_len * rows, cudaMemcpyDeviceToHost, b->main),
+                    "copy force rows");
+        }
+        BCK(cudaStreamSynchronize(b->main), "sync");
+        pending = 0;
+        int st0 = LBM_OK;
+        for (int c = 0; c < nc; ++c) {
+            start[c] = done[c];
+            const int st = handle_status(b->cases[c]);
+            if (st && !st0) {
+                st0 = st;
+                b->err = std::string("batch: case ") + std::to_string(c) + ": " + b->cases[c]->err;
+            }
+        }
+        return st0;
+    };
+    BCK(cudaEventRecord(b->ev_done, b->main), "event");
+    BCK(cudaEventRecord(b->ev_side, b->side), "event");
     std::vector<lbm_handle *> act;
+    std::vector<int> act_idx;
+    std::vector<long long> waited;
     for (; step < nsteps; ++step) {
         act.clear();
-        std::vector<int> act_idx;
+        act_idx.clear();
         for (int c = 0; c < nc; ++c)
             if (b->cases[c]->n <= last_step[c]) {
                 act.push_back(b->cases[c]);
                 act_idx.push_back(c);
             }
         if (act.empty()) break;
-        const int n = act[0]->n;   // lockstep: every active case is at step n
-        const int bi = n / K, half = bi & 1, q = n % b->nslots, buf = step & 1;
-        const bool fields = step >= nsteps - 2;
-        if (b->batch_in_half[half] != bi && (rc = factor_batch(bi, act))) break;
-        // this step's arguments (the upload buffers of two steps back are free)
+        const int buf = step & 1;
+        // fields (rho, u, v) for the last two steps of the call and of every
+        // case that ends within them (all active cases keep them then)
+        bool fields = step >= nsteps - 2;
+        for (size_t c = 0; c < act.size() && !fields; ++c) fields = act[c]->n >= last_step[act_idx[c]] - 1;
+        if ((rc = factor_needed(act, act_idx, false))) break;
+        // this step's arguments (the staging buffers of two steps back are free)
         BCK(cudaEventSynchronize(b->ev_upload[buf]), "sync upload");
         int ntab = 0;
         for (size_t c = 0; c < act.size(); ++c) {
             lbm_handle *h = act[c];
+            const int q = h->n % b->nslots;
             const void *fin = h->fbuf[h->cur];
             void *fout = h->fbuf[h->cur ^ 1];
             void *fd = nullptr;
@@ -266,11 +418,17 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
             kf_args_write(h, fin, fout, fd, KF_OUTER, (char *)b->h_kargs[buf] + c * b->kf_sz);
             int gx, gy;
             kf_tma_grid(h, &gx, &gy);
+            if (ntab + gx * gy > b->table_cap) {
+                rc = berr(b, LBM_ERR_STATE, "batch: case table overflow");
+                break;
+            }
             for (int by = 0; by < gy; ++by)
                 for (int bx = 0; bx < gx; ++bx) b->h_table[buf][ntab++] = make_int4((int)c, bx, by, gx | (gy << 16));
         }
-        if (ntab > b->table_cap) { rc = berr(b, LBM_ERR_STATE, "batch: case table overflow"); break; }
-        // the previous step is complete (and with it every reader of this step's upload buffers)
+        if (rc) break;
+        // side stream: once the previous step is complete (and with it every
+        // reader of this step's upload buffers), the uploads and the flow
+        // chains of all cases
         BCK(cudaStreamWaitEvent(b->side, b->ev_done, 0), "wait");
         BCK(cudaMemcpyAsync(b->d_sargs[buf], b->h_sargs[buf], act.size() * b->ib_sz, cudaMemcpyHostToDevice, b->side),
             "upload");
@@ -279,9 +437,18 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
         BCK(cudaMemcpyAsync(b->d_table[buf], b->h_table[buf], sizeof(int4) * ntab, cudaMemcpyHostToDevice, b->side),
             "upload");
         BCK(cudaEventRecord(b->ev_upload[buf], b->side), "event");
-        // side stream: the flow chains of all cases
-        BCK(cudaStreamWaitEvent(b->side, b->ev_batch[half], 0), "wait");
-        if (launch_flow_batch(act.data(), (int)act.size(), b->d_sargs[buf], b->d_kargs[buf], n, pending, fields,
+        // the factorization launches of this step's halves (those of earlier
+        // runs are complete: every run ends with its streams idle)
+        waited.clear();
+        for (lbm_handle *h : act) {
+            const long long g = h->fgroup[(h->n / K) & 1];
+            if (g > seq_start && std::find(waited.begin(), waited.end(), g) == waited.end()) {
+                BCK(cudaStreamWaitEvent(b->side, b->ev_group[g % kGroupRing], 0), "wait");
+                waited.push_back(g);
+            }
+        }
+        BCK(cudaEventRecord(b->ev_fready, b->side), "event");   // uploads done, factorizations ready
+        if (launch_flow_batch(act.data(), (int)act.size(), b->d_sargs[buf], b->d_kargs[buf], 0, pending, fields,
                               b->side)) {
             rc = berr(b, LBM_ERR_CUDA, "batch: launch flow");
             break;
@@ -291,16 +458,11 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
             rc = berr(b, LBM_ERR_CUDA, "batch: launch check");
             break;
         }
-        BCK(cudaEventRecord(b->ev_free[half], b->side), "event");
-        // the next factorization batch, overlapping this one's steps
-        if (b->batch_in_half[half ^ 1] != bi + 1) {
-            bool any = false;
-            for (size_t c = 0; c < act.size(); ++c) any = any || (bi + 1) * K <= last_step[act_idx[c]];
-            if (any && (rc = factor_batch(bi + 1, act))) break;
-        }
+        BCK(cudaEventRecord(b->ev_side, b->side), "event");
+        // the next factorization batches, overlapping these steps
+        if ((rc = factor_needed(act, act_idx, true))) break;
         // main stream: every case's lattice nodes but its correction tiles
-        BCK(cudaStreamWaitEvent(b->main, b->ev_batch[half], 0), "wait");
-        BCK(cudaStreamWaitEvent(b->main, b->ev_upload[buf], 0), "wait");
+        BCK(cudaStreamWaitEvent(b->main, b->ev_fready, 0), "wait");
         if (launch_kf_multi(b->prec, b->d_kargs[buf], b->d_table[buf], ntab, fields, b->main)) {
             rc = berr(b, LBM_ERR_CUDA, "batch: launch lattice");
             break;
@@ -316,40 +478,20 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
             done[act_idx[c]]++;
         }
         pending++;
-        // force rows to the host every ring's worth of steps and at the end
-        const bool flush = pending == b->cases[0]->ring_cap || step == nsteps - 1;
-        if (flush) {
-            BCK(cudaEventRecord(b->ev_ib, b->side), "event");
-            BCK(cudaStreamWaitEvent(b->main, b->ev_ib, 0), "wait");
-            for (int c = 0; c < nc; ++c) {
-                lbm_handle *h = b->cases[c];
-                const int rows = done[c] - pending_start[c];
-                if (force_rows && force_rows[c] && rows > 0)
-                    BCK(cudaMemcpyAsync(force_rows[c] + (size_t)pending_start[c] * h->row_len, h->d_ring,
-                                        sizeof(double) * h->row_len * rows, cudaMemcpyDeviceToHost, b->main),
-                        "copy force rows");
-            }
-            BCK(cudaStreamSynchronize(b->main), "sync");
-            for (int c = 0; c < nc; ++c) {
-                pending_start[c] = done[c];
-                const int st = handle_status(b->cases[c]);
-                if (st && !rc) {
-                    rc = st;
-                    b->err = std::string("batch: case ") + std::to_string(c) + ": " + b->cases[c]->err;
-                }
-            }
-            pending = 0;
-            if (rc) break;
+        // force rows to the host every ring's worth of steps
+        if (pending == b->cases[0]->ring_cap) {
+            if ((rc = flush())) break;
         }
     }
+    // the rows of the last steps (also when every case ended before nsteps)
+    if (pending > 0 && rc == LBM_OK) rc = flush();
     // leave every stream idle: the cases' own calls follow on their streams
-    cudaStreamSynchronize(b->side);
-    cudaStreamSynchronize(b->fstream);
-    cudaStreamSynchronize(b->main);
+    sync_streams(b);
     restore();
     if (done_steps)
         for (int c = 0; c < nc; ++c) done_steps[c] = done[c];
-    if (rc == LBM_OK && step < nsteps) rc = LBM_DONE;
+    for (int c = 0; c < nc && rc == LBM_OK; ++c)
+        if (done[c] < nsteps) rc = LBM_DONE;
     return rc;
 }
 

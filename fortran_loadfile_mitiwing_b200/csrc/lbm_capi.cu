@@ -7,6 +7,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <mutex>
+#include <unordered_map>
 #include <vector>
 
 #include "lbm_internal.h"
@@ -60,9 +62,35 @@ double feq(double rh, double u1, double v1, int k)
     return wsingle(k) * rh * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * utwo);
 }
 
+// device allocations of the handles, owner and size (lbm_device_bytes)
+std::mutex g_alloc_mu;
+std::unordered_map<void *, std::pair<lbm_handle *, size_t>> g_allocs;
+
+template <typename P> cudaError_t dmalloc(lbm_handle *h, P **p, size_t bytes)
+{
+    void *q = nullptr;
+    const cudaError_t e = cudaMalloc(&q, bytes);
+    if (e != cudaSuccess) return e;
+    *p = (P *)q;
+    std::lock_guard<std::mutex> lock(g_alloc_mu);
+    g_allocs[q] = {h, bytes};
+    h->dev_bytes += (long long)bytes;
+    return e;
+}
+
 void free_dev(void *&p)
 {
-    if (p) cudaFree(p);
+    if (p) {
+        {
+            std::lock_guard<std::mutex> lock(g_alloc_mu);
+            auto it = g_allocs.find(p);
+            if (it != g_allocs.end()) {
+                it->second.first->dev_bytes -= (long long)it->second.second;
+                g_allocs.erase(it);
+            }
+        }
+        cudaFree(p);
+    }
     p = nullptr;
 }
 template <typename P> void free_devp(P *&p)
@@ -172,36 +200,36 @@ int ensure_ib(lbm_handle *h)
     }
     const int ns = std::max(1, h->nseg);
     const size_t S = (size_t)h->nslots, K = (size_t)h->fbatch;
-    CK(cudaMalloc(&h->d_mk, S * sizeof(Marker) * ns), "alloc markers");
-    CK(cudaMalloc(&h->d_rhs, sizeof(double) * 2 * ns), "alloc rhs");
-    CK(cudaMalloc(&h->d_y, sizeof(double) * 2 * ns), "alloc y");
-    CK(cudaMalloc(&h->d_B, S * sizeof(double) * (size_t)ns * ns), "alloc B");
+    CK(dmalloc(h, &h->d_mk, S * sizeof(Marker) * ns), "alloc markers");
+    CK(dmalloc(h, &h->d_rhs, sizeof(double) * 2 * ns), "alloc rhs");
+    CK(dmalloc(h, &h->d_y, sizeof(double) * 2 * ns), "alloc y");
+    CK(dmalloc(h, &h->d_B, S * sizeof(double) * (size_t)ns * ns), "alloc B");
     ib_factor_scratch(ns, &h->work_blocks, &h->gf_slot);
-    CK(cudaMalloc(&h->d_bD, K * sizeof(double) * h->work_blocks), "alloc block D");
-    CK(cudaMalloc(&h->d_bL, K * sizeof(double) * h->work_blocks), "alloc block L");
-    CK(cudaMalloc(&h->d_gf, S * sizeof(double) * h->gf_slot), "alloc factor blocks");
-    CK(cudaMalloc(&h->d_fmode, S * 2 * sizeof(int)), "alloc factor mode");
-    CK(cudaMalloc(&h->d_fstatus, S * sizeof(unsigned)), "alloc factor status");
+    CK(dmalloc(h, &h->d_bD, K * sizeof(double) * h->work_blocks), "alloc block D");
+    CK(dmalloc(h, &h->d_bL, K * sizeof(double) * h->work_blocks), "alloc block L");
+    CK(dmalloc(h, &h->d_gf, S * sizeof(double) * h->gf_slot), "alloc factor blocks");
+    CK(dmalloc(h, &h->d_fmode, S * 2 * sizeof(int)), "alloc factor mode");
+    CK(dmalloc(h, &h->d_fstatus, S * sizeof(unsigned)), "alloc factor status");
     CK(cudaMemsetAsync(h->d_fmode, 0, S * 2 * sizeof(int), h->stream), "clear factor mode");
     CK(cudaMemsetAsync(h->d_fstatus, 0, S * sizeof(unsigned), h->stream), "clear factor status");
     const int nblk = h->patch_gx() * h->patch_gy();
     // partials of the spread (per patch tile) and of the residual check (per 8 markers)
     const size_t npart = std::max((size_t)ib_partials_per_block() * nblk, 2 * (size_t)((ns + 7) / 8));
-    CK(cudaMalloc(&h->d_partial, sizeof(double) * npart), "alloc partials");
+    CK(dmalloc(h, &h->d_partial, sizeof(double) * npart), "alloc partials");
     h->tiles_slot = (size_t)ib_tile_ints() * nblk;
-    CK(cudaMalloc(&h->d_tiles, S * sizeof(int) * h->tiles_slot), "alloc tile lists");
+    CK(dmalloc(h, &h->d_tiles, S * sizeof(int) * h->tiles_slot), "alloc tile lists");
     CK(cudaMemsetAsync(h->d_tiles, 0, S * sizeof(int) * h->tiles_slot, h->stream), "clear tile lists");
-    CK(cudaMalloc(&h->d_nsup, S * sizeof(int)), "alloc tile counts");
-    CK(cudaMalloc(&h->d_ctile, S * sizeof(int) * (size_t)nblk), "alloc correction tiles");
+    CK(dmalloc(h, &h->d_nsup, S * sizeof(int)), "alloc tile counts");
+    CK(dmalloc(h, &h->d_ctile, S * sizeof(int) * (size_t)nblk), "alloc correction tiles");
     CK(cudaMemsetAsync(h->d_nsup, 0, S * sizeof(int), h->stream), "clear tile counts");
     // solve order of the markers: one rigid body keeps its markers sorted by
     // body-frame chordwise position for the whole run (two markers whose
     // support boxes overlap are less than 5*sqrt(2) lattice units apart in any
     // orientation); several bodies are sorted on the device every step
-    CK(cudaMalloc(&h->d_perm, S * sizeof(int) * ns), "alloc perm");
-    CK(cudaMalloc(&h->d_key, S * sizeof(double) * ns), "alloc key");
-    CK(cudaMalloc(&h->d_reach, sizeof(double)), "alloc reach");
-    CK(cudaMalloc(&h->d_wmax, K * sizeof(int)), "alloc wmax");
+    CK(dmalloc(h, &h->d_perm, S * sizeof(int) * ns), "alloc perm");
+    CK(dmalloc(h, &h->d_key, S * sizeof(double) * ns), "alloc key");
+    CK(dmalloc(h, &h->d_reach, sizeof(double)), "alloc reach");
+    CK(dmalloc(h, &h->d_wmax, K * sizeof(int)), "alloc wmax");
     CK(cudaMemsetAsync(h->d_wmax, 0, K * sizeof(int), h->stream), "clear wmax");
     h->static_order = h->nwing == 1;
     if (h->static_order) {
@@ -501,30 +529,30 @@ int lbm_create(const lbm_params *p, lbm_t **out)
     // 16-byte halo left and right of every row segment) stay in bounds
     const size_t fbytes = h->elem * (9 * (size_t)h->plane + 2 * LBM_FPAD);
     for (int b = 0; b < 2; ++b) {
-        if ((e = cudaMalloc(&h->falloc[b], fbytes)) != cudaSuccess) return fail(e, "alloc f");
+        if ((e = dmalloc(h, &h->falloc[b], fbytes)) != cudaSuccess) return fail(e, "alloc f");
         if ((e = cudaMemset(h->falloc[b], 0, fbytes)) != cudaSuccess) return fail(e, "clear f");
         h->fbuf[b] = (char *)h->falloc[b] + h->elem * LBM_FPAD;
     }
     const size_t cs = compute_size(h->prec);
     const size_t nn = (size_t)h->nx * h->ny;
     for (int b = 0; b < 2; ++b)
-        if ((e = cudaMalloc(&h->d_fields[b], 3 * cs * nn)) != cudaSuccess) return fail(e, "alloc fields");
-    if ((e = cudaMalloc(&h->edge_c, cs * (6 * (size_t)h->ny + 36))) != cudaSuccess) return fail(e, "alloc edge");
-    if ((e = cudaMalloc(&h->d_status, sizeof(unsigned))) != cudaSuccess) return fail(e, "alloc status");
-    if ((e = cudaMalloc(&h->d_counter, sizeof(unsigned))) != cudaSuccess) return fail(e, "alloc counter");
-    if ((e = cudaMalloc(&h->d_pinfo, LBM_NSLOT_MAX * sizeof(PatchInfo))) != cudaSuccess) return fail(e, "alloc pinfo");
-    if ((e = cudaMalloc(&h->d_red, sizeof(double) * 2 * 296)) != cudaSuccess) return fail(e, "alloc red");
-    if ((e = cudaMalloc(&h->d_solve_res, 2 * sizeof(double))) != cudaSuccess) return fail(e, "alloc res");
-    if ((e = cudaMalloc(&h->d_ring, sizeof(double) * h->row_len * (size_t)h->ring_cap)) != cudaSuccess)
+        if ((e = dmalloc(h, &h->d_fields[b], 3 * cs * nn)) != cudaSuccess) return fail(e, "alloc fields");
+    if ((e = dmalloc(h, &h->edge_c, cs * (6 * (size_t)h->ny + 36))) != cudaSuccess) return fail(e, "alloc edge");
+    if ((e = dmalloc(h, &h->d_status, sizeof(unsigned))) != cudaSuccess) return fail(e, "alloc status");
+    if ((e = dmalloc(h, &h->d_counter, sizeof(unsigned))) != cudaSuccess) return fail(e, "alloc counter");
+    if ((e = dmalloc(h, &h->d_pinfo, LBM_NSLOT_MAX * sizeof(PatchInfo))) != cudaSuccess) return fail(e, "alloc pinfo");
+    if ((e = dmalloc(h, &h->d_red, sizeof(double) * 2 * 296)) != cudaSuccess) return fail(e, "alloc red");
+    if ((e = dmalloc(h, &h->d_solve_res, 2 * sizeof(double))) != cudaSuccess) return fail(e, "alloc res");
+    if ((e = dmalloc(h, &h->d_ring, sizeof(double) * h->row_len * (size_t)h->ring_cap)) != cudaSuccess)
         return fail(e, "alloc ring");
     cudaMemset(h->d_status, 0, sizeof(unsigned));
     cudaMemset(h->d_counter, 0, sizeof(unsigned));
     cudaMemset(h->d_pinfo, 0, LBM_NSLOT_MAX * sizeof(PatchInfo));
     cudaMemset(h->d_solve_res, 0, 2 * sizeof(double));
     if (h->npts > 0) {
-        if ((e = cudaMalloc(&h->d_xb0, sizeof(double) * h->npts)) != cudaSuccess) return fail(e, "alloc xb0");
-        if ((e = cudaMalloc(&h->d_yb0, sizeof(double) * h->npts)) != cudaSuccess) return fail(e, "alloc yb0");
-        if ((e = cudaMalloc(&h->d_arc, sizeof(double) * h->nseg)) != cudaSuccess) return fail(e, "alloc arc");
+        if ((e = dmalloc(h, &h->d_xb0, sizeof(double) * h->npts)) != cudaSuccess) return fail(e, "alloc xb0");
+        if ((e = dmalloc(h, &h->d_yb0, sizeof(double) * h->npts)) != cudaSuccess) return fail(e, "alloc yb0");
+        if ((e = dmalloc(h, &h->d_arc, sizeof(double) * h->nseg)) != cudaSuccess) return fail(e, "alloc arc");
     }
     if ((e = cudaDeviceSynchronize()) != cudaSuccess) return fail(e, "sync");
     *out = h;
@@ -612,7 +640,7 @@ int lbm_set_motion_table(lbm_t *h, const double *table, int rows, int cols)
         std::copy(row.begin(), row.end(), h->mstep_host.begin() + (size_t)(i - 1) * cols);
     }
     free_devp(h->d_mstep);
-    CK(cudaMalloc(&h->d_mstep, sizeof(double) * h->mstep_host.size()), "alloc step table");
+    CK(dmalloc(h, &h->d_mstep, sizeof(double) * h->mstep_host.size()), "alloc step table");
     CK(cudaMemcpyAsync(h->d_mstep, h->mstep_host.data(), sizeof(double) * h->mstep_host.size(),
                        cudaMemcpyHostToDevice, h->stream), "copy step table");
     CK(cudaStreamSynchronize(h->stream), "sync motion");
@@ -669,7 +697,7 @@ int lbm_init(lbm_t *h, const double *du, const double *dv)
         CK(cudaMemcpyAsync(h->edge_c, ef.data(), sizeof(float) * ef.size(), cudaMemcpyHostToDevice, h->stream), "copy edge");
     }
     // populations
-    if (!h->d_stage) CK(cudaMalloc(&h->d_stage, sizeof(double) * nn * 9), "alloc stage");
+    if (!h->d_stage) CK(dmalloc(h, &h->d_stage, sizeof(double) * nn * 9), "alloc stage");
     for (size_t q = 0; q < nn * 9; ++q) g[q] += kWref[q / nn];   // back to f for the pack kernel
     CK(cudaMemcpyAsync(h->d_stage, g.data(), sizeof(double) * nn * 9, cudaMemcpyHostToDevice, h->stream), "copy f");
     if (launch_pack(h, h->d_stage, h->fbuf[0])) return cuda_err(h, cudaGetLastError(), "pack");
@@ -692,6 +720,7 @@ int lbm_init(lbm_t *h, const double *du, const double *dv)
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream), "clear status");
     CK(cudaMemsetAsync(h->d_pinfo, 0, LBM_NSLOT_MAX * sizeof(PatchInfo), h->stream), "clear pinfo");
     CK(cudaStreamSynchronize(h->stream), "sync init");
+    free_devp(h->d_stage);   // the FP64 staging planes are made for each transfer, not kept
     h->n = 1;
     h->steps_done = 0;
     h->inited = 1;
@@ -748,10 +777,11 @@ int lbm_get_populations(lbm_t *h, double *f)
     if (!h || !f) return LBM_ERR_ARG;
     if (!h->inited) return set_err(h, LBM_ERR_STATE, "get_populations: not initialised");
     const size_t nn = (size_t)h->nx * h->ny;
-    if (!h->d_stage) CK(cudaMalloc(&h->d_stage, sizeof(double) * nn * 9), "alloc stage");
+    if (!h->d_stage) CK(dmalloc(h, &h->d_stage, sizeof(double) * nn * 9), "alloc stage");
     if (launch_unpack(h, h->fbuf[h->cur], h->d_stage)) return cuda_err(h, cudaGetLastError(), "unpack");
     CK(cudaMemcpyAsync(f, h->d_stage, sizeof(double) * nn * 9, cudaMemcpyDeviceToHost, h->stream), "copy f");
     CK(cudaStreamSynchronize(h->stream), "sync f");
+    free_devp(h->d_stage);
     return LBM_OK;
 }
 
@@ -760,10 +790,11 @@ int lbm_set_populations(lbm_t *h, const double *f)
     if (!h || !f) return LBM_ERR_ARG;
     if (!h->inited) return set_err(h, LBM_ERR_STATE, "set_populations: not initialised");
     const size_t nn = (size_t)h->nx * h->ny;
-    if (!h->d_stage) CK(cudaMalloc(&h->d_stage, sizeof(double) * nn * 9), "alloc stage");
+    if (!h->d_stage) CK(dmalloc(h, &h->d_stage, sizeof(double) * nn * 9), "alloc stage");
     CK(cudaMemcpyAsync(h->d_stage, f, sizeof(double) * nn * 9, cudaMemcpyHostToDevice, h->stream), "copy f");
     if (launch_pack(h, h->d_stage, h->fbuf[h->cur])) return cuda_err(h, cudaGetLastError(), "pack");
     CK(cudaStreamSynchronize(h->stream), "sync f");
+    free_devp(h->d_stage);
     h->fields_step[0] = h->fields_step[1] = -1;
     return LBM_OK;
 }
@@ -832,6 +863,13 @@ int lbm_get_launch_count(const lbm_t *h, long long *count)
 }
 
 int lbm_step_index(const lbm_t *h) { return h ? h->n : LBM_ERR_ARG; }
+
+int lbm_device_bytes(const lbm_t *h, long long *bytes)
+{
+    if (!h || !bytes) return LBM_ERR_ARG;
+    *bytes = h->dev_bytes;
+    return LBM_OK;
+}
 
 const char *lbm_last_error(const lbm_t *h) { return h ? h->err.c_str() : "lbm_create failed (bad parameters or no CUDA device)"; }
 

@@ -73,6 +73,8 @@ struct IBArgs {
     // slot and working-set strides of the batched factorization (elements)
     int nslots;
     int static_order;   // one rigid body: fixed solve order (ib_order leaves it)
+    int cur_step;       // step index of the flow chain (batched launches: per case)
+    int fstep0, fcount; // steps of the factorization chain (batched launches: per case)
     long long st_mk, st_perm, st_B, wk_blocks, wk_gf;
     PatchInfo *pinfo;
     int *tiles;         // per patch tile: marker count, then the listed markers (slot)
@@ -180,6 +182,8 @@ struct lbm_handle {
     double t_step = 0, t_ib = 0, t_kf = 0;
     int t_steps = 0;
     long long launches = 0;   // kernels launched by this handle (lbm_get_launch_count)
+    long long dev_bytes = 0;  // device memory the handle holds (lbm_device_bytes)
+    long long fgroup[2] = {-1, -1};   // batch factorization launch that filled each slot half
     // driver state
     int n = 1;
     int inited = 0;
@@ -207,6 +211,7 @@ void kf_tma_grid(const lbm_handle *h, int *gx, int *gy);
 int launch_kf_multi(int prec, const void *cases, const int4 *table, int nentries, bool fields, cudaStream_t st);
 size_t ib_args_size();
 void ib_args_write(lbm_handle *h, const void *fin, int slot, void *dst);
+void ib_factor_args_write(lbm_handle *h, int step0, int count, void *dst);
 int launch_factor_batch(lbm_handle *const *hs, int ncase, const void *dargs, int step0, int count, cudaStream_t st);
 int launch_flow_batch(lbm_handle *const *hs, int ncase, const void *dargs, const void *dkf, int step_index,
                       int ring_slot, bool fields, cudaStream_t st);

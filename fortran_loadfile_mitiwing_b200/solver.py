@@ -139,6 +139,12 @@ class Lbm:
     def step_index(self):
         return self.lib.lbm_step_index(self.h)
 
+    def device_bytes(self):
+        """Device memory the case holds now (lbm_device_bytes)."""
+        v = C.c_longlong()
+        self._ck(self.lib.lbm_device_bytes(self.h, C.byref(v)))
+        return v.value
+
 
 class Batch:
     """Several initialised cases stepped together on one GPU
@@ -147,10 +153,10 @@ class Batch:
     cases stay usable as `Lbm` objects; each one's results are those of
     running it alone."""
 
-    def __init__(self, cases, lib=None):
+    def __init__(self, cases=(), lib=None):
         self.cases = list(cases)
-        self.lib = lib or self.cases[0].lib
-        arr = (C.c_void_p * len(self.cases))(*[c.h.value for c in self.cases])
+        self.lib = lib or (self.cases[0].lib if self.cases else _abi.load_library())
+        arr = (C.c_void_p * max(len(self.cases), 1))(*[c.h.value for c in self.cases])
         b = C.c_void_p()
         rc = self.lib.lbm_batch_create(arr, len(self.cases), C.byref(b))
         if rc != 0:
@@ -158,6 +164,23 @@ class Batch:
             raise LbmError(rc, msgs)
         self.b = b
         self.rows = 0
+
+    def __len__(self):
+        return len(self.cases)
+
+    def add(self, case):
+        """The case joins the batch (at whatever step it is)."""
+        rc = self.lib.lbm_batch_add(self.b, case.h)
+        if rc != 0:
+            raise LbmError(rc, case.lib.lbm_last_error(case.h).decode())
+        self.cases.append(case)
+
+    def remove(self, case):
+        """The case leaves the batch; the others keep their order."""
+        rc = self.lib.lbm_batch_remove(self.b, case.h)
+        if rc != 0:
+            raise LbmError(rc, self.lib.lbm_batch_last_error(self.b).decode())
+        self.cases.remove(case)
 
     def close(self):
         if getattr(self, "b", None):

@@ -44,10 +44,15 @@ def sweep_specs(n=64, seed=2026, nx_lo=512, nx_hi=2048):
     return out
 
 
-def make(spec, n_steps, precision, lib=None):
+def case_of(spec, n_steps, precision, amp=1.0e-4):
+    """The case of a sweep spec (amp=0: without the perturbation arrays)."""
     kw = {k: spec[k] for k in ("nx", "ny", "chord", "pivot", "markers", "re", "heave", "pitch_deg", "phase_deg",
                                "st", "seed")}
-    return Lbm.from_case(cs.heave_pitch_case(n_steps=n_steps, precision=precision, uu=U0, **kw), lib)
+    return cs.heave_pitch_case(n_steps=n_steps, precision=precision, uu=U0, amp=amp, **kw)
+
+
+def make(spec, n_steps, precision, lib=None):
+    return Lbm.from_case(case_of(spec, n_steps, precision), lib)
 
 
 def cases_per_hour(specs, lups_per_s, periods=5):

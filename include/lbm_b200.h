@@ -228,6 +228,13 @@ LBM_API int lbm_get_launch_count(const lbm_t *h, long long *count);
 /* current step counter n of the driver loop (1 before the first step). */
 LBM_API int lbm_step_index(const lbm_t *h);
 
+/* device memory the handle holds now, in bytes: lattice buffers and fields
+ * from lbm_create, immersed-boundary scratch from the first step (FP64
+ * staging for population transfers is made and released within each call).
+ * Serving loops admit cases against an HBM budget with it. No counterpart
+ * in the reference (one case per process there). */
+LBM_API int lbm_device_bytes(const lbm_t *h, long long *bytes);
+
 /* message of the last failing call on h ("" if none); h may be NULL for
  * errors of lbm_create. The string stays valid until the next call on h. */
 LBM_API const char *lbm_last_error(const lbm_t *h);
@@ -235,22 +242,31 @@ LBM_API const char *lbm_last_error(const lbm_t *h);
 /* ---- batches: several cases stepped together on one GPU ----------------
  * The reference runs one case per process (main.f90); flapping-wing studies
  * are sweeps of many cases. A batch steps initialised handles of different
- * grid sizes and kinematics in lockstep with one launch per kernel for all of
- * them: one lattice launch driven by a case table, and each immersed-boundary
- * stage as one launch over the cases. Each case's results are bit-for-bit
- * those of running it alone (lbm_run). The batch does not own the handles.
- *   lbm_batch_create: cases must be initialised, share storage precision,
- *     device and step index, and have markers.
+ * grid sizes and kinematics with one launch per kernel for all of them: one
+ * lattice launch driven by a case table, and each immersed-boundary stage as
+ * one launch over the cases. Cases may be at different steps, and may join
+ * and leave between runs (the serving loop of the Python layer does so).
+ * Each case's results are bit-for-bit those of running it alone (lbm_run).
+ * The batch does not own the handles; between runs a case may also be
+ * stepped alone.
+ *   lbm_batch_create: cases (count >= 0) must be initialised, share storage
+ *     precision, factorization batch and device, and have markers.
+ *   lbm_batch_add / lbm_batch_remove: a case joins (same conditions) or
+ *     leaves the batch; the order of the remaining cases is kept.
+ *   lbm_batch_count: cases in the batch.
  *   lbm_batch_run: runs up to nsteps steps of every case; a case stops when
  *     its motion table ends (done_steps[c], nullable; LBM_DONE when any case
- *     stopped early). force_rows[c] (nullable, or an array of nullable
- *     pointers) receives case c's rows as lbm_run would. Fields are kept for
- *     the last two steps of the call, as lbm_run.
+ *     ran fewer than nsteps). force_rows[c] (nullable, or an array of
+ *     nullable pointers) receives case c's rows as lbm_run would. Fields are
+ *     kept for the last two steps of the call and of each case that ends.
  *   lbm_batch_set_rows: rows per CTA of the lattice kernel for the batch
  *     (0: the cases' own); the batch autotuner of the Python layer sets it. */
 typedef struct lbm_batch lbm_batch_t;
 LBM_API int lbm_batch_create(lbm_t *const *cases, int count, lbm_batch_t **out);
 LBM_API int lbm_batch_destroy(lbm_batch_t *b);
+LBM_API int lbm_batch_add(lbm_batch_t *b, lbm_t *h);
+LBM_API int lbm_batch_remove(lbm_batch_t *b, lbm_t *h);
+LBM_API int lbm_batch_count(const lbm_batch_t *b);
 LBM_API int lbm_batch_set_rows(lbm_batch_t *b, int rows_per_cta);
 LBM_API int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *done_steps);
 LBM_API const char *lbm_batch_last_error(const lbm_batch_t *b);

@@ -56,3 +56,62 @@ def test_autotuned_batch_still_equals_alone(gpu_lib):
     for t, a in zip(together, alone):
         a.run(25)
         np.testing.assert_array_equal(t.populations(), a.populations())
+
+
+def test_cases_join_and_leave_at_different_steps(gpu_lib):
+    """Cases stepped alone before joining, joining a running batch (an empty
+    one included), leaving it and stepped alone afterwards each end bit-for-bit
+    where the same number of steps alone ends."""
+    mixed = build("fp32", 120, lib=gpu_lib)
+    alone = build("fp32", 120, lib=gpu_lib)
+    rows = [[] for _ in mixed]
+
+    def take(b, n):
+        for case, r in zip(b.cases, b.run(n)):
+            rows[mixed.index(case)].append(r)
+
+    rows[0].append(mixed[0].run(6))      # mid-way through a factorization batch of 4 steps
+    rows[2].append(mixed[2].run(13))
+    with Batch([], lib=gpu_lib) as b:
+        b.add(mixed[0])
+        b.add(mixed[1])
+        take(b, 9)
+        b.add(mixed[2])                  # joins at step 14 beside cases at 16 and 10
+        take(b, 10)
+        b.remove(mixed[0])
+        take(b, 5)
+        rows[0].append(mixed[0].run(7))  # alone in between
+        b.add(mixed[0])
+        take(b, 11)
+        assert len(b) == 3
+    for c, (m, a) in enumerate(zip(mixed, alone)):
+        got = np.concatenate(rows[c])
+        ref = a.run(got.shape[0])
+        assert m.step_index == a.step_index
+        np.testing.assert_array_equal(got, ref, err_msg=f"case {c} force rows")
+        np.testing.assert_array_equal(m.populations(), a.populations(), err_msg=f"case {c} populations")
+
+
+def test_rows_of_a_case_ending_alone_in_a_run(gpu_lib):
+    """The only case of a run ends before the run's step count: its last rows
+    still reach the host."""
+    t = Lbm.from_case(cases.small_case(precision="fp32", n_steps=23, **SPECS[0]), gpu_lib)
+    a = Lbm.from_case(cases.small_case(precision="fp32", n_steps=23, **SPECS[0]), gpu_lib)
+    with Batch([t]) as b:
+        r1 = b.run(21)[0]
+        r2 = b.run(7)[0]
+    ref = a.run(100)
+    assert r1.shape[0] + r2.shape[0] == ref.shape[0]
+    np.testing.assert_array_equal(np.concatenate([r1, r2]), ref)
+
+
+def test_batch_refuses_mixed_precision(gpu_lib):
+    from fortran_loadfile_mitiwing_b200 import LbmError
+    a = build("fp32", 20, specs=SPECS[:1], lib=gpu_lib)[0]
+    d = build("fp64", 20, specs=SPECS[1:2], lib=gpu_lib)[0]
+    with Batch([a]) as b:
+        with pytest.raises(LbmError):
+            b.add(d)
+        with pytest.raises(LbmError):
+            b.add(a)                     # already in the batch
+        assert len(b) == 1 and b.lib.lbm_batch_count(b.b) == 1
