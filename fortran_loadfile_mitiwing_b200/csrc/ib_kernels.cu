@@ -1080,7 +1080,8 @@ __global__ void __launch_bounds__(256) ib_forces(const IBArgs a0, const IBArgs *
 // recomputed from the marker geometry (independent of the factorization):
 // one warp per row of the solve order, lanes over the couplings within the
 // half-bandwidth; deterministic two-level sum (CTA partials, last CTA).
-// Flags LBM_ST_SOLVER unless it is below 1e-6.
+// Flags LBM_ST_SOLVER unless it is below 1e-6, or LBM_ST_NONFINITE when the
+// right-hand side itself is not finite (the flow at the markers diverged).
 template <bool BATCH>
 __global__ void __launch_bounds__(256) ib_residual(const IBArgs a0, const IBArgs *batch)
 {
@@ -1144,7 +1145,10 @@ __global__ void __launch_bounds__(256) ib_residual(const IBArgs a0, const IBArgs
         for (int w = 0; w < 8; ++w) { sn += red[w][0]; sd += red[w][1]; }
         const double res = sqrt(sn) / (sqrt(sd) + 1e-300);
         a.solve_res[0] = res;
-        if (!(res < 1e-6)) atomicOr(a.status, LBM_ST_SOLVER);
+        if (!isfinite(sd))
+            atomicOr(a.status, LBM_ST_NONFINITE);
+        else if (!(res < 1e-6))
+            atomicOr(a.status, LBM_ST_SOLVER);
         *a.counter = 0u;
     }
 }

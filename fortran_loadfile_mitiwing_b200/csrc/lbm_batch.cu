@@ -50,6 +50,7 @@ struct lbm_batch {
     long long gseq = 0;   // factorization launches so far
     size_t ib_sz = 0, kf_sz = 0;
     int rows_per_cta = 0;   // 0: the cases' own setting
+    std::vector<int> status;   // each case's status in the last run (lbm_batch_case_status)
     std::string err;
 };
 
@@ -255,6 +256,12 @@ int lbm_batch_remove(lbm_batch_t *b, lbm_t *h)
 
 int lbm_batch_count(const lbm_batch_t *b) { return b ? (int)b->cases.size() : LBM_ERR_ARG; }
 
+int lbm_batch_case_status(const lbm_batch_t *b, int c)
+{
+    if (!b || c < 0 || c >= (int)b->status.size()) return LBM_ERR_ARG;
+    return b->status[c];
+}
+
 int lbm_batch_destroy(lbm_batch_t *b)
 {
     if (!b) return LBM_ERR_ARG;
@@ -276,6 +283,7 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
     const int nc = (int)b->cases.size();
     for (int c = 0; c < nc; ++c)
         if (done_steps) done_steps[c] = 0;
+    b->status.assign(nc, LBM_OK);
     if (nsteps == 0 || nc == 0) return LBM_OK;
     const int K = b->fbatch;
     std::vector<int> rows_saved(nc), last_step(nc), done(nc, 0), start(nc, 0);
@@ -371,6 +379,7 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
         for (int c = 0; c < nc; ++c) {
             start[c] = done[c];
             const int st = handle_status(b->cases[c]);
+            if (st) b->status[c] = st;
             if (st && !st0) {
                 st0 = st;
                 b->err = std::string("batch: case ") + std::to_string(c) + ": " + b->cases[c]->err;

@@ -263,7 +263,8 @@ int check_status(lbm_handle *h)
         return set_err(h, LBM_ERR_RANGE, "move_boundary: a marker support box reaches the three outermost node layers");
     if (st & LBM_ST_OVERFLOW) return set_err(h, LBM_ERR_RANGE, "immersed boundary: correction patch overflow");
     if (st & LBM_ST_SOLVER) return set_err(h, LBM_ERR_SOLVER, "immersed boundary: D D^T not positive definite");
-    if (st & LBM_ST_NONFINITE) return set_err(h, LBM_ERR_NONFINITE, "non-finite force");
+    if (st & LBM_ST_NONFINITE)
+        return set_err(h, LBM_ERR_NONFINITE, "non-finite flow at the markers or force (the flow diverged)");
     return set_err(h, LBM_ERR_CUDA, "unknown device status");
 }
 

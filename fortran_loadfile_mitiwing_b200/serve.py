@@ -123,10 +123,12 @@ class Request:
 
 class Result:
     """A finished solve: its force rows (one per step, as lbm_run gives them)
-    and its times on the server clock."""
+    and its times on the server clock; `error` (code, message) when the case
+    failed (its rows then stop at the failing check)."""
 
-    def __init__(self, rid, rows, arrival, admitted, started, finished, handle=None):
+    def __init__(self, rid, rows, arrival, admitted, started, finished, handle=None, error=None):
         self.rid = rid
+        self.error = error
         self.rows = rows
         self.arrival = arrival
         self.admitted = admitted
@@ -276,26 +278,26 @@ class Server:
         self.peak_cases = max(self.peak_cases, len(self.live))
         if not self.live:
             return []
-        rows = self.batch.run(self.tick_steps)
+        rows, status = self.batch.run(self.tick_steps, errors="return")
         self.ticks += 1
         t = self.clock()
         by_handle = {id(st[0]): rid for rid, st in self.live.items()}
-        finished = []
-        for h, r in zip(list(self.batch.cases), rows):
+        finished = {}
+        for h, r, err in zip(list(self.batch.cases), rows, status):
             rid = by_handle[id(h)]
             st = self.live[rid]
             if r.shape[0]:
                 st[1].append(r)
-            if h.step_index > st[4]:   # the case's motion table ended
-                finished.append(rid)
+            if err is not None or h.step_index > st[4]:   # failed, or the case's motion table ended
+                finished[rid] = err
         out = []
-        for rid in finished:
+        for rid, err in finished.items():
             h, chunks, admitted, started, _ = self.live.pop(rid)
             self.batch.remove(h)
             self.adm.release(rid)
             rows_all = np.concatenate(chunks) if chunks else np.zeros((0, h.row_len))
             req = self.requests.pop(rid)
-            out.append(Result(rid, rows_all, req.arrival, admitted, started, t, h if self.keep_handles else None))
+            out.append(Result(rid, rows_all, req.arrival, admitted, started, t, h if self.keep_handles else None, err))
             if not self.keep_handles:
                 h.close()
         self.done.extend(out)
@@ -313,10 +315,11 @@ def poisson_arrivals(rate, n, seed=0):
 
 
 def serve_stream(specs, rate, periods=3.0, budget_bytes=150e9, precision="fp16", tick_steps=100, seed=1, lib=None,
-                 keep_rows=False):
+                 keep_rows=()):
     """Serves `specs` (sweep.sweep_specs items, `periods` flapping periods
     each) arriving as a Poisson stream of `rate` requests/s in real time;
-    returns the results (rows dropped unless keep_rows) and a summary."""
+    returns the results (force rows kept for the request ids in keep_rows,
+    else only the first and last row) and a summary."""
     from . import sweep
     arrivals = poisson_arrivals(rate, len(specs), seed)
     reqs = []
@@ -339,8 +342,8 @@ def serve_stream(specs, rate, periods=3.0, budget_bytes=150e9, precision="fp16",
                 time.sleep(max(0.0, reqs[nxt].arrival - srv.clock()))
                 continue
             for r in srv.tick(wait_for_ready=True):
-                if not keep_rows:
-                    r.rows = r.rows[:0] if r.rows.shape[0] == 0 else r.rows[[0, -1]]
+                if r.rid not in keep_rows and r.rows.shape[0] > 2:
+                    r.rows = r.rows[[0, -1]]
         res = sorted(srv.done, key=lambda r: r.rid)
     finally:
         srv.close()
@@ -351,6 +354,37 @@ def serve_stream(specs, rate, periods=3.0, budget_bytes=150e9, precision="fp16",
                  "mean_s": float(np.mean(lat)), "makespan_s": span, "cases_per_hour": len(res) * 3600.0 / span,
                  "mlups": lups / span / 1e6, "peak_cases": srv.peak_cases, "peak_bytes": srv.peak_used,
                  "ticks": srv.ticks}
+
+
+COL_CD, COL_CL = 1, 2   # force-row columns of a one-wing case: time, C_x (drag), C_y (lift), ...
+
+
+def period_errors(rows, ref, period_steps, periods):
+    """Per flapping period, |mean(rows) - mean(ref)| of C_D and C_L, each
+    relative to the RMS of `ref`'s coefficient over that period (C_L of a
+    symmetric motion has a mean near zero). Returns the largest of each."""
+    out = {"cd": 0.0, "cl": 0.0}
+    for k in range(int(periods)):
+        a, b = int(round(k * period_steps)), int(round((k + 1) * period_steps))
+        for name, col in (("cd", COL_CD), ("cl", COL_CL)):
+            r = ref[a:b, col]
+            rms = math.sqrt(float(np.mean(r ** 2)))
+            out[name] = max(out[name], abs(float(np.mean(rows[a:b, col]) - np.mean(r))) / rms)
+    return out
+
+
+def fp64_reference_rows(specs, periods=3.0, lib=None):
+    """Force rows of `specs` stored in FP64, run together as one batch to the
+    end of their motion."""
+    from . import sweep
+    hs = [Lbm.from_case(sweep.case_of(sp, int(math.ceil(periods * sp["period_steps"])), "fp64"), lib)
+          for sp in specs]
+    try:
+        with Batch(hs) as b:
+            return b.run(max(int(math.ceil(periods * sp["period_steps"])) for sp in specs) + 2)
+    finally:
+        for h in hs:
+            h.close()
 
 
 def fifo_one_at_a_time(arrivals, service):
@@ -393,6 +427,8 @@ def main():
     ap.add_argument("--tick-steps", type=int, default=100)
     ap.add_argument("--precision", default="fp16")
     ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--check", type=int, default=8,
+                    help="requests of the first stream whose coefficients are checked against FP64 storage")
     args = ap.parse_args()
     specs = sweep.sweep_specs(args.requests, args.seed)
     out = {"requests": args.requests, "periods": args.periods, "budget_gb": args.budget_gb,
@@ -402,8 +438,17 @@ def main():
     service = alone_service_times(specs, args.periods)
     out["fp32_alone_service_s_total"] = float(sum(service))
     for k, rate in enumerate(args.rates):
-        _, summ = serve_stream(specs, rate, args.periods, args.budget_gb * 1e9, args.precision, args.tick_steps,
-                               seed=args.seed + k)
+        keep = set(range(args.check)) if k == 0 else set()
+        res, summ = serve_stream(specs, rate, args.periods, args.budget_gb * 1e9, args.precision, args.tick_steps,
+                                 seed=args.seed + k, keep_rows=keep)
+        if keep:
+            ref = fp64_reference_rows(specs[:args.check], args.periods)
+            errs = [period_errors(res[i].rows, ref[i], specs[i]["period_steps"], args.periods) for i in sorted(keep)]
+            out["coefficients_vs_fp64"] = {
+                "requests": len(keep), "periods": int(args.periods),
+                "max_period_mean_err_cd": max(e["cd"] for e in errs),
+                "max_period_mean_err_cl": max(e["cl"] for e in errs),
+                "note": "per period |mean - mean_fp64| / rms_fp64; served rows vs the same cases in FP64 storage"}
         arr = poisson_arrivals(rate, len(specs), args.seed + k)
         fin = fifo_one_at_a_time(arr, service)
         lat = [f - a for f, a in zip(fin, arr)]

@@ -205,19 +205,29 @@ class Batch:
             raise LbmError(rc, self.lib.lbm_batch_last_error(self.b).decode())
         self.rows = int(rows_per_cta)
 
-    def run(self, nsteps, keep_rows=True):
+    def run(self, nsteps, keep_rows=True, errors="raise"):
         """Steps every case up to `nsteps` times; returns each case's force
-        rows (trimmed to the steps it ran) or the step counts."""
+        rows (trimmed to the steps it ran) or the step counts. A failed case
+        (a diverged flow, say) stops the run: errors="raise" raises LbmError;
+        errors="return" returns (rows or counts, statuses), statuses[c] None
+        for a case that is fine, else (code, message)."""
         n = len(self.cases)
         bufs = [np.zeros((max(nsteps, 1), c.row_len)) for c in self.cases] if keep_rows else None
         ptrs = (_abi._D * n)(*[dptr(x) for x in bufs]) if keep_rows else None
         done = (C.c_int * n)()
         rc = self.lib.lbm_batch_run(self.b, int(nsteps), ptrs, done)
-        if rc not in (0, 1):
+        if rc not in (0, 1) and errors == "raise":
             raise LbmError(rc, self.lib.lbm_batch_last_error(self.b).decode())
-        if not keep_rows:
-            return list(done)
-        return [bufs[c][: done[c]] for c in range(n)]
+        out = [bufs[c][: done[c]] for c in range(n)] if keep_rows else list(done)
+        if errors == "raise":
+            return out
+        status = []
+        for c, case in enumerate(self.cases):
+            st = self.lib.lbm_batch_case_status(self.b, c)
+            status.append(None if st == 0 else (st, case.lib.lbm_last_error(case.h).decode()))
+        if rc not in (0, 1) and all(x is None for x in status):
+            raise LbmError(rc, self.lib.lbm_batch_last_error(self.b).decode())   # not a case's own failure
+        return out, status
 
     def autotune(self, steps_per_trial=20, candidates=(4, 8, 16)):
         """Picks the lattice kernel's rows per CTA for this batch by timing

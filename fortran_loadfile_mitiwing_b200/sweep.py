@@ -7,7 +7,12 @@ Cases (seeded): Nx uniform in [512, 2048] (multiples of 64), Ny = Nx/2,
 chord = Ny/4, Re in [100, 2000], heave amplitude in [0.1c, 0.75c], pitch
 amplitude in [0, 45] deg, phase in [0, 180] deg, St in [0.15, 0.45]; NACA
 0012 with 2 markers per lattice unit of chord, pivot at the quarter chord on
-node (2c+1, Ny/2+1), U0 = 0.05, seeded 1e-4 initial perturbation.
+node (2c+1, Ny/2+1), seeded 1e-4 initial perturbation. U0 = 0.05, lowered
+per case where the body moves fast so that the fluid speed near it stays
+below 0.1 lattice units (`lattice_speed`): with U0 = 0.05 throughout, the
+fastest pitching cases reach 0.15-0.27 lattice units per step (Mach 0.3-0.5)
+and the lattice-Boltzmann flow diverges within a few hundred steps, in any
+storage precision.
 
 Each form runs a fixed sample of steps per case after a warm-up; the report
 gives the aggregate lattice updates per second and the cases per hour that
@@ -18,6 +23,7 @@ prints one JSON object. Needs a GPU.
 """
 import argparse
 import json
+import math
 import time
 
 import numpy as np
@@ -28,7 +34,19 @@ from .solver import Batch, Lbm
 U0 = 0.05
 
 
-def sweep_specs(n=64, seed=2026, nx_lo=512, nx_hi=2048):
+def lattice_speed(spec, uu=U0):
+    """Bound on the fluid speed near the body in lattice units: free stream
+    plus the body surface speed, U0 (1 + pi St (1 + 0.75 theta0 / h)), the
+    heave speed 2 pi f h plus the pitch speed 2 pi f theta0 at the trailing
+    edge (0.75 chord behind the pivot), f = St / (2 h)."""
+    th = math.radians(spec["pitch_deg"])
+    return uu * (1.0 + math.pi * spec["st"] * (1.0 + 0.75 * th / spec["heave"]))
+
+
+def sweep_specs(n=64, seed=2026, nx_lo=512, nx_hi=2048, u_lat=0.1):
+    """Seeded cases; U0 = min(0.05, the U0 that keeps `lattice_speed` at
+    u_lat), so that fast pitching and heaving keep the lattice Mach number
+    below about u_lat / c_s (c_s = 1/sqrt 3). u_lat=None keeps U0 = 0.05."""
     rng = np.random.default_rng(seed)
     out = []
     for c in range(n):
@@ -39,7 +57,9 @@ def sweep_specs(n=64, seed=2026, nx_lo=512, nx_hi=2048):
                     re=float(rng.uniform(100.0, 2000.0)), heave=float(rng.uniform(0.1, 0.75)),
                     pitch_deg=float(rng.uniform(0.0, 45.0)), phase_deg=float(rng.uniform(0.0, 180.0)),
                     st=float(rng.uniform(0.15, 0.45)), seed=seed + c)
-        spec["period_steps"] = chord / (spec["st"] / (2.0 * spec["heave"]) * U0)
+        uu = U0 if u_lat is None else min(U0, u_lat * U0 / lattice_speed(spec))
+        spec["uu"] = uu
+        spec["period_steps"] = chord / (spec["st"] / (2.0 * spec["heave"]) * uu)
         out.append(spec)
     return out
 
@@ -48,7 +68,7 @@ def case_of(spec, n_steps, precision, amp=1.0e-4):
     """The case of a sweep spec (amp=0: without the perturbation arrays)."""
     kw = {k: spec[k] for k in ("nx", "ny", "chord", "pivot", "markers", "re", "heave", "pitch_deg", "phase_deg",
                                "st", "seed")}
-    return cs.heave_pitch_case(n_steps=n_steps, precision=precision, uu=U0, amp=amp, **kw)
+    return cs.heave_pitch_case(n_steps=n_steps, precision=precision, uu=spec.get("uu", U0), amp=amp, **kw)
 
 
 def make(spec, n_steps, precision, lib=None):

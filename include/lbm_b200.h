@@ -46,7 +46,7 @@ extern "C" {
 #define LBM_ERR_STATE       -3   /* call out of order (e.g. step before init) */
 #define LBM_ERR_IO          -4   /* file missing or malformed (mode.f90:82-135, airfoil.f90:224-234) */
 #define LBM_ERR_SOLVER      -5   /* immersed-boundary system not positive definite / singular */
-#define LBM_ERR_NONFINITE   -6   /* NaN/Inf seen in forces or in the mass check */
+#define LBM_ERR_NONFINITE   -6   /* NaN/Inf seen in forces, in the flow at the markers or in the mass check */
 #define LBM_ERR_RANGE       -7   /* a marker's support box reaches the three outermost node layers */
 #define LBM_ERR_SIZE        -8   /* size beyond a fixed maximum (lbm_residual_device) */
 
@@ -254,6 +254,12 @@ LBM_API const char *lbm_last_error(const lbm_t *h);
  *   lbm_batch_add / lbm_batch_remove: a case joins (same conditions) or
  *     leaves the batch; the order of the remaining cases is kept.
  *   lbm_batch_count: cases in the batch.
+ *   lbm_batch_case_status: status of case c (batch order) in the last
+ *     lbm_batch_run: LBM_OK or the error code its checks raised, with the
+ *     message in lbm_last_error of that case. A run stops at the first check
+ *     that finds a failed case (a diverged flow, say); the rows and steps of
+ *     every case up to that check are delivered, and the other cases stay
+ *     valid and may go on in the next run once the failed one is removed.
  *   lbm_batch_run: runs up to nsteps steps of every case; a case stops when
  *     its motion table ends (done_steps[c], nullable; LBM_DONE when any case
  *     ran fewer than nsteps). force_rows[c] (nullable, or an array of
@@ -267,6 +273,7 @@ LBM_API int lbm_batch_destroy(lbm_batch_t *b);
 LBM_API int lbm_batch_add(lbm_batch_t *b, lbm_t *h);
 LBM_API int lbm_batch_remove(lbm_batch_t *b, lbm_t *h);
 LBM_API int lbm_batch_count(const lbm_batch_t *b);
+LBM_API int lbm_batch_case_status(const lbm_batch_t *b, int c);
 LBM_API int lbm_batch_set_rows(lbm_batch_t *b, int rows_per_cta);
 LBM_API int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *done_steps);
 LBM_API const char *lbm_batch_last_error(const lbm_batch_t *b);

@@ -82,6 +82,7 @@ class _FakeCase:
         self.lib = None
         self.rid = spec["rid"]
         self.bytes = spec["bytes"]
+        self.fail_at = spec.get("fail_at")
 
     @classmethod
     def from_case(cls, case, lib=None):
@@ -108,13 +109,17 @@ class _FakeBatch:
     def remove(self, h):
         self.cases.remove(h)
 
-    def run(self, n):
-        out = []
+    def run(self, n, errors="raise"):
+        out, status = [], []
         for h in self.cases:
             k = max(0, min(n, h.last - h.n + 1))
+            fail = h.fail_at is not None and h.n <= h.fail_at < h.n + k
+            if fail:
+                k = h.fail_at - h.n + 1
             out.append(np.array([[h.rid, h.n + i] for i in range(k)], dtype=float).reshape(k, 2))
             h.n += k
-        return out
+            status.append((-6, "diverged") if fail else None)
+        return (out, status) if errors == "return" else out
 
     def close(self):
         pass
@@ -153,3 +158,47 @@ def test_server_joins_and_finishes_cases(monkeypatch, workers):
         assert res[rid].steps == last
     assert sorted(_FakeCase.closed) == [0, 1, 2, 3]
     assert srv.peak_cases == 2
+
+
+def test_period_errors():
+    from fortran_loadfile_mitiwing_b200.serve import period_errors
+    t = np.arange(300)
+    ref = np.zeros((300, 3))
+    ref[:, 1] = 2.0 + np.sin(2 * np.pi * t / 100.0)
+    ref[:, 2] = np.cos(2 * np.pi * t / 100.0)
+    got = ref.copy()
+    got[100:200, 1] += 0.01          # period 2: C_D mean off by 0.01
+    e = period_errors(got, ref, 100.0, 3)
+    rms = math.sqrt(float(np.mean(ref[100:200, 1] ** 2)))
+    assert abs(e["cd"] - 0.01 / rms) < 1e-12 and e["cl"] < 1e-12
+
+
+def test_server_returns_a_failed_case_and_serves_the_rest(monkeypatch):
+    from fortran_loadfile_mitiwing_b200 import serve
+
+    class _Params:
+        scale, uu = 1.0, 1.0
+
+    class _Spec(dict):
+        pass
+
+    def make(rid, last, fail_at=None):
+        c = _Spec(rid=rid, last=last, bytes=10, fail_at=fail_at)
+        c.params = _Params()
+        c.table = np.array([[float(last - 1)]])
+        return lambda: c
+
+    monkeypatch.setattr(serve, "Lbm", _FakeCase)
+    monkeypatch.setattr(serve, "Batch", _FakeBatch)
+    _FakeCase.closed = []
+    with serve.Server(budget_bytes=100, tick_steps=5, workers=0) as srv:
+        srv.submit(serve.Request(0, make(0, 30), estimate=10))
+        srv.submit(serve.Request(1, make(1, 30, fail_at=12), estimate=10))
+        srv.submit(serve.Request(2, make(2, 20), estimate=10))
+        while not srv.idle():
+            srv.tick(wait_for_ready=True)
+        res = {r.rid: r for r in srv.done}
+    assert res[1].error == (-6, "diverged") and res[1].steps == 12
+    assert res[0].error is None and res[0].steps == 30
+    assert res[2].error is None and res[2].steps == 20
+    assert sorted(_FakeCase.closed) == [0, 1, 2]
