@@ -77,6 +77,12 @@ ABI = {
     "lbm_step_index": (C.c_int, [_P]),
     "lbm_device_bytes": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
     "lbm_last_error": (C.c_char_p, [_P]),
+    "lbm_write_tecplot": (C.c_int, [_P, C.c_char_p, C.c_int, C.c_int, C.c_int]),
+    "lbm_write_tecplot_fields": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                           C.c_double, C.c_double, C.c_int, C.c_int, _D, _D, _D, C.c_int, C.c_int,
+                                           _D, _D]),
+    "lbm_save_checkpoint": (C.c_int, [_P, C.c_char_p]),
+    "lbm_load_checkpoint": (C.c_int, [_P, C.c_char_p]),
     "lbm_batch_create": (C.c_int, [C.POINTER(_P), C.c_int, C.POINTER(_P)]),
     "lbm_batch_destroy": (C.c_int, [_P]),
     "lbm_batch_add": (C.c_int, [_P, _P]),

@@ -12,7 +12,7 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "liblbmb200.so")
 ROOT = os.path.dirname(HERE)
 
-SOURCES = ["lbm_capi.cu", "kf_kernel.cu", "ib_kernels.cu", "host_io.cu", "residual_device.cu", "lbm_batch.cu"]
+SOURCES = ["lbm_capi.cu", "kf_kernel.cu", "ib_kernels.cu", "host_io.cu", "residual_device.cu", "lbm_batch.cu", "output_io.cu"]
 HEADERS = ["lbm_common.cuh", "lbm_internal.h"]
 
 NVCC_FLAGS = [

@@ -1,0 +1,416 @@
+// output_io.cu -- the reference's output and restart files behind the C ABI.
+//   F<n>.dat     output (solution.f90:129-238): Tecplot ASCII; a field zone
+//                sampled every stride-th node (X, Y, U/UU, V/UU, pressure
+//                rho/3, vorticity, body, dvordt) and an FE-triangle zone of
+//                the airfoil contour with one centre node per wing.
+//   checkpoint   saveflowfield / readflowfield (solution.f90:1604-1839): the
+//                same two-file scheme (the file and its "_copy"; the reader
+//                falls back to the copy when the file is missing, short or
+//                corrupt), holding this library's exact device state so that
+//                a restart continues bit for bit.
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "lbm_internal.h"
+
+namespace {
+
+int io_err(lbm_handle *h, int code, const std::string &msg)
+{
+    if (h) h->err = msg;
+    return code;
+}
+
+// Fortran Ew.d editing: 0.d1..dd E+xx (E dropped for a 3-digit exponent),
+// right-justified in w characters, asterisks when it does not fit.
+int fmt_e(char *out, double x, int w, int d)
+{
+    char tmp[64];
+    int n;
+    if (std::isnan(x)) {
+        n = snprintf(tmp, sizeof tmp, "NaN");
+    } else if (std::isinf(x)) {
+        n = snprintf(tmp, sizeof tmp, x < 0 ? "-Infinity" : "Infinity");
+    } else if (x == 0.0) {
+        std::string z = std::string(std::signbit(x) ? "-" : "") + "0." + std::string(d, '0') + "E+00";
+        n = snprintf(tmp, sizeof tmp, "%s", z.c_str());
+    } else {
+        char sci[64];
+        snprintf(sci, sizeof sci, "%.*e", d - 1, std::fabs(x));   // d significant digits, rounded
+        // sci = D.DDDDDDDe[+-]XX
+        std::string digits;
+        digits += sci[0];
+        const char *p = sci + 1;
+        if (*p == '.') ++p;
+        while (*p && *p != 'e') digits += *p++;
+        const int ex = atoi(p + 1) + 1;   // 0.DDDD x 10^ex
+        const char sign = ex < 0 ? '-' : '+';
+        const int ax = std::abs(ex);
+        if (ax <= 99)
+            n = snprintf(tmp, sizeof tmp, "%s0.%sE%c%02d", x < 0 ? "-" : "", digits.c_str(), sign, ax);
+        else
+            n = snprintf(tmp, sizeof tmp, "%s0.%s%c%03d", x < 0 ? "-" : "", digits.c_str(), sign, ax);
+    }
+    if (n > w) {
+        memset(out, '*', w);
+    } else {
+        memset(out, ' ', w - n);
+        memcpy(out + (w - n), tmp, n);
+    }
+    return w;
+}
+
+// Fortran Fw.d editing, asterisks when it does not fit
+int fmt_f(char *out, double x, int w, int d)
+{
+    char tmp[128];
+    const int n = snprintf(tmp, sizeof tmp, "%*.*f", w, d, x);
+    if (n > w)
+        memset(out, '*', w);
+    else
+        memcpy(out, tmp, w);
+    return w;
+}
+
+struct FieldGrid {
+    int nx, ny, sx, sy;
+    double ox, oy, scale, uu;
+    const double *rho, *u, *v;
+};
+
+// one line of the field zone for node (i, j), 0-based: format (25e16.8)
+// of X, Y, U/UU, V/UU, rho/3, vorticity (solution.f90:194-210), body, dvordt
+int field_line(const FieldGrid &g, int i, int j, char *out)
+{
+    const long long nx = g.nx;
+    auto U = [&](int a, int b) { return g.u[(size_t)b * nx + a]; };
+    auto V = [&](int a, int b) { return g.v[(size_t)b * nx + a]; };
+    const double h = g.uu * g.scale;
+    double dvx, duy;
+    if (i == g.nx - 1)
+        dvx = (1.5 * V(i, j) - 2.0 * V(i - 1, j) + 0.5 * V(i - 2, j)) / h;
+    else if (i == 0)
+        dvx = (-1.5 * V(i, j) + 2.0 * V(i + 1, j) - 0.5 * V(i + 2, j)) / h;
+    else
+        dvx = (V(i + 1, j) - V(i - 1, j)) / (g.uu * 2.0 * g.scale);
+    if (j == g.ny - 1)
+        duy = (1.5 * U(i, j) - 2.0 * U(i, j - 1) + 0.5 * U(i, j - 2)) / h;
+    else if (j == 0)
+        duy = (-1.5 * U(i, j) + 2.0 * U(i, j + 1) - 0.5 * U(i, j + 2)) / h;
+    else
+        duy = (U(i, j + 1) - U(i, j - 1)) / (g.uu * 2.0 * g.scale);
+    const double vals[8] = {g.ox + (double)i * g.scale, g.oy + (double)j * g.scale, U(i, j) / g.uu, V(i, j) / g.uu,
+                            g.rho[(size_t)j * nx + i] / 3.0, dvx - duy, 0.0, 0.0};
+    int k = 0;
+    for (int c = 0; c < 8; ++c) k += fmt_e(out + k, vals[c], 16, 8);
+    out[k++] = '\n';
+    return k;
+}
+
+// "ZONE ..." header items in list-directed style: integers in 12 columns,
+// reals with 17 significant digits
+std::string ld_int(long long v)
+{
+    char b[32];
+    snprintf(b, sizeof b, "%12lld", v);
+    return b;
+}
+std::string ld_real(double v)
+{
+    char b[48];
+    snprintf(b, sizeof b, "%25.16E", v);
+    return b;
+}
+
+bool write_all(FILE *f, const void *p, size_t n) { return n == 0 || fwrite(p, 1, n, f) == n; }
+
+// the field zone written by threads into per-chunk buffers, in row order
+bool write_field_zone(FILE *f, const FieldGrid &g)
+{
+    const int ox = (g.nx - 1) / g.sx + 1, oy = (g.ny - 1) / g.sy + 1;
+    const int line = 8 * 16 + 1;
+    unsigned nt = std::thread::hardware_concurrency();
+    nt = nt ? std::min(nt, 32u) : 4u;
+    const int rows_per_chunk = std::max(1, (int)(4u << 20) / (line * ox));   // ~4 MB of text per chunk
+    for (int r0 = 0; r0 < oy; r0 += rows_per_chunk * (int)nt) {
+        std::vector<std::string> buf(nt);
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt; ++t) {
+            const int a = r0 + (int)t * rows_per_chunk, b = std::min(oy, a + rows_per_chunk);
+            if (a >= b) break;
+            th.emplace_back([&, t, a, b]() {
+                std::string &s = buf[t];
+                s.resize((size_t)(b - a) * ox * line);
+                char *p = &s[0];
+                for (int jr = a; jr < b; ++jr)
+                    for (int ir = 0; ir < ox; ++ir) p += field_line(g, ir * g.sx, jr * g.sy, p);
+            });
+        }
+        for (auto &x : th) x.join();
+        for (unsigned t = 0; t < th.size(); ++t)
+            if (!write_all(f, buf[t].data(), buf[t].size())) return false;
+    }
+    return true;
+}
+
+// contour points xb1, yb1 (airfoil.f90:255-266) of step `s` (1-based step
+// index of the motion table row the step used)
+void contour_points(const lbm_handle *h, int s, std::vector<double> &x, std::vector<double> &y)
+{
+    const int row = std::max(1, std::min(s, h->msteps)) - 1;
+    const double *r = h->mstep_host.data() + (size_t)row * h->mcols;
+    x.assign(h->npts, 0.0);
+    y.assign(h->npts, 0.0);
+    for (int w = 0; w < h->nwing; ++w) {
+        const double angle = r[1 + 9 * w], sa = r[4 + 9 * w], sb = r[7 + 9 * w];
+        const double ca = cos(angle), sn = sin(angle);
+        for (int p = 0; p < h->ppw; ++p) {
+            const int q = w * h->ppw + p;
+            x[q] = ca * h->hx0[q] + sn * h->hy0[q] + sa + h->p.xc;
+            y[q] = -sn * h->hx0[q] + ca * h->hy0[q] + sb + h->p.yc;
+        }
+    }
+}
+
+int write_tecplot(const char *path, int cycle, const FieldGrid &g, double soltime, int nwing, int ppw,
+                  const double *xb1, const double *yb1, std::string &msg)
+{
+    FILE *f = fopen(path, "wb");
+    if (!f) {
+        msg = std::string("cannot open ") + path;
+        return LBM_ERR_IO;
+    }
+    const int ox = (g.nx - 1) / g.sx + 1, oy = (g.ny - 1) / g.sy + 1;
+    std::string head = "VARIABLES = \"X\" \"Y\" \"U\" \"V\" \"Presure\" \"Vorticity\" \"body\" \"dvordt\" \n";
+    head += " ZONE T=\"Flow feild\", I=" + ld_int(ox) + " ,J=" + ld_int(oy) + " ,SOLUTIONTIME=" + ld_real(soltime) + "\n";
+    bool ok = write_all(f, head.data(), head.size()) && write_field_zone(f, g);
+    if (ok && nwing > 0) {
+        const int bpoint = nwing * ppw, bseg = nwing * (ppw - 1);
+        std::string z = " ZONE T=\"airfoil\", NODES=" + ld_int(bpoint + nwing) + " ELEMENTS,=" + ld_int(bseg) +
+                        ", DATAPACKING=POINT, ZONETYPE=FETRIANGLE,SOLUTIONTIME=" + ld_real(soltime) + "\n";
+        char line[256];
+        auto point = [&](double x, double y) {   // (8f14.8)
+            const double v[8] = {x, y, 255.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+            int k = 0;
+            for (int c = 0; c < 8; ++c) k += fmt_f(line + k, v[c], 14, 8);
+            line[k++] = '\n';
+            z.append(line, k);
+        };
+        for (int q = 0; q < bpoint; ++q) point(xb1[q], yb1[q]);
+        for (int w = 0; w < nwing; ++w) {   // centre node: between the first point and the one halfway round
+            const int j = w * ppw, k = j + (ppw - 1) / 2;
+            point(0.5 * (xb1[j] + xb1[k]), 0.5 * (yb1[j] + yb1[k]));
+        }
+        for (int w = 0; w < nwing; ++w)   // (3I5.3), 1-based node numbers
+            for (int k = w * ppw + 1; k <= w * ppw + ppw - 1; ++k) {
+                const int n = snprintf(line, sizeof line, "%5.3d%5.3d%5.3d\n", k, k + 1, bpoint + w + 1);
+                z.append(line, n);
+            }
+        ok = write_all(f, z.data(), z.size());
+    }
+    ok = (fclose(f) == 0) && ok;
+    if (!ok) msg = std::string("write failed: ") + path;
+    (void)cycle;
+    return ok ? LBM_OK : LBM_ERR_IO;
+}
+
+// ---- checkpoint ---------------------------------------------------------
+
+const char kMagic[16] = {'L', 'B', 'M', 'B', '2', '0', '0', ' ', 'C', 'K', 'P', 'T', ' ', 'v', '1', '\0'};
+
+struct CkptHeader {
+    int32_t version, nx, ny, pitch, prec, nwing, ppw, cur;
+    int64_t n, steps_done, fields_step[2];
+    int32_t fields_slot, pad;
+    int64_t pop_bytes, edge_bytes, field_bytes;
+};
+
+uint64_t fnv1a(uint64_t hsh, const void *p, size_t n)
+{
+    const unsigned char *b = (const unsigned char *)p;
+    for (size_t i = 0; i < n; ++i) {
+        hsh ^= b[i];
+        hsh *= 1099511628211ull;
+    }
+    return hsh;
+}
+
+std::string copy_path(const std::string &path)
+{
+    const size_t slash = path.find_last_of('/');
+    const size_t dot = path.find_last_of('.');
+    if (dot == std::string::npos || (slash != std::string::npos && dot < slash)) return path + "_copy";
+    return path.substr(0, dot) + "_copy" + path.substr(dot);
+}
+
+size_t edge_bytes(const lbm_handle *h)
+{
+    const size_t cs = h->prec == LBM_PREC_FP64 ? 8 : 4;
+    return cs * (6 * (size_t)h->ny + 36);
+}
+
+size_t field_bytes(const lbm_handle *h)
+{
+    const size_t cs = h->prec == LBM_PREC_FP64 ? 8 : 4;
+    return 3 * cs * (size_t)h->nx * h->ny;
+}
+
+// the whole state in host memory (header, populations, edge values, fields x2)
+int gather_state(lbm_handle *h, CkptHeader &hd, std::vector<unsigned char> &blob)
+{
+    hd = CkptHeader{};
+    hd.version = 1;
+    hd.nx = h->nx; hd.ny = h->ny; hd.pitch = h->pitch; hd.prec = h->prec;
+    hd.nwing = h->nwing; hd.ppw = h->ppw; hd.cur = 0;
+    hd.n = h->n; hd.steps_done = h->steps_done;
+    hd.fields_step[0] = h->fields_step[0]; hd.fields_step[1] = h->fields_step[1];
+    hd.fields_slot = h->fields_slot;
+    hd.pop_bytes = (int64_t)(h->elem * 9 * (size_t)h->plane);
+    hd.edge_bytes = (int64_t)edge_bytes(h);
+    hd.field_bytes = (int64_t)field_bytes(h);
+    blob.resize((size_t)(hd.pop_bytes + hd.edge_bytes + 2 * hd.field_bytes));
+    unsigned char *p = blob.data();
+    cudaError_t e = cudaMemcpyAsync(p, h->fbuf[h->cur], hd.pop_bytes, cudaMemcpyDeviceToHost, h->stream);
+    p += hd.pop_bytes;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(p, h->edge_c, hd.edge_bytes, cudaMemcpyDeviceToHost, h->stream);
+    p += hd.edge_bytes;
+    for (int s = 0; s < 2 && e == cudaSuccess; ++s, p += hd.field_bytes)
+        e = cudaMemcpyAsync(p, h->d_fields[s], hd.field_bytes, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return io_err(h, LBM_ERR_CUDA, std::string("checkpoint: ") + cudaGetErrorString(e));
+    return LBM_OK;
+}
+
+int write_ckpt_file(const std::string &path, const CkptHeader &hd, const std::vector<unsigned char> &blob)
+{
+    FILE *f = fopen(path.c_str(), "wb");
+    if (!f) return LBM_ERR_IO;
+    uint64_t sum = fnv1a(1469598103934665603ull, &hd, sizeof hd);
+    sum = fnv1a(sum, blob.data(), blob.size());
+    bool ok = write_all(f, kMagic, sizeof kMagic) && write_all(f, &hd, sizeof hd) &&
+              write_all(f, blob.data(), blob.size()) && write_all(f, &sum, sizeof sum);
+    ok = (fclose(f) == 0) && ok;
+    return ok ? LBM_OK : LBM_ERR_IO;
+}
+
+// reads and checks one checkpoint file against the handle; "" on success
+std::string read_ckpt_file(const lbm_handle *h, const std::string &path, CkptHeader &hd, std::vector<unsigned char> &blob)
+{
+    FILE *f = fopen(path.c_str(), "rb");
+    if (!f) return "cannot open " + path;
+    char magic[16];
+    std::string why;
+    if (fread(magic, 1, 16, f) != 16 || memcmp(magic, kMagic, 16) != 0) why = "not a checkpoint of this library";
+    else if (fread(&hd, 1, sizeof hd, f) != sizeof hd) why = "short header";
+    else if (hd.version != 1) why = "unknown checkpoint version";
+    else if (hd.nx != h->nx || hd.ny != h->ny || hd.pitch != h->pitch || hd.prec != h->prec || hd.nwing != h->nwing ||
+             hd.ppw != h->ppw)
+        why = "grid, storage precision or wings differ from this case";
+    else if (hd.pop_bytes != (int64_t)(h->elem * 9 * (size_t)h->plane) || hd.edge_bytes != (int64_t)edge_bytes(h) ||
+             hd.field_bytes != (int64_t)field_bytes(h))
+        why = "section sizes differ from this case";
+    if (why.empty()) {
+        blob.resize((size_t)(hd.pop_bytes + hd.edge_bytes + 2 * hd.field_bytes));
+        uint64_t sum = 0;
+        if (fread(blob.data(), 1, blob.size(), f) != blob.size() || fread(&sum, 1, sizeof sum, f) != sizeof sum)
+            why = "short file";
+        else if (sum != fnv1a(fnv1a(1469598103934665603ull, &hd, sizeof hd), blob.data(), blob.size()))
+            why = "checksum mismatch";
+    }
+    fclose(f);
+    return why.empty() ? "" : path + ": " + why;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_write_tecplot_fields(const char *path, int nx, int ny, double ox, double oy, double scale, double uu,
+                             double solution_time, int stride_x, int stride_y, const double *rho, const double *u,
+                             const double *v, int wing_count, int points_per_wing, const double *xb1, const double *yb1)
+{
+    if (!path || nx < 3 || ny < 3 || !(scale > 0) || !(uu > 0) || stride_x < 1 || stride_y < 1 || !rho || !u || !v ||
+        wing_count < 0 || (wing_count > 0 && (points_per_wing < 3 || !xb1 || !yb1)))
+        return LBM_ERR_ARG;
+    FieldGrid g{nx, ny, stride_x, stride_y, ox, oy, scale, uu, rho, u, v};
+    std::string msg;
+    return write_tecplot(path, 0, g, solution_time, wing_count, points_per_wing, xb1, yb1, msg);
+}
+
+int lbm_write_tecplot(lbm_t *h, const char *path, int cycle, int stride_x, int stride_y)
+{
+    if (!h || !path || stride_x < 1 || stride_y < 1) return LBM_ERR_ARG;
+    if (!h->inited) return io_err(h, LBM_ERR_STATE, "write_tecplot: not initialised");
+    const size_t nn = (size_t)h->nx * h->ny;
+    std::vector<double> rho(nn), u(nn), v(nn);
+    int rc = lbm_get_fields(h, rho.data(), u.data(), v.data());
+    if (rc) return rc;
+    std::vector<double> xb1, yb1;
+    if (h->nwing > 0) contour_points(h, h->n - 1, xb1, yb1);
+    FieldGrid g{h->nx, h->ny, stride_x, stride_y, h->p.ox, h->p.oy, h->p.scale, h->p.uu,
+                rho.data(), u.data(), v.data()};
+    std::string msg;
+    rc = write_tecplot(path, cycle, g, (double)cycle * h->p.uu * h->p.mesh_max_scale, h->nwing, h->ppw, xb1.data(),
+                       yb1.data(), msg);
+    return rc ? io_err(h, rc, "write_tecplot: " + msg) : LBM_OK;
+}
+
+int lbm_save_checkpoint(lbm_t *h, const char *path)
+{
+    if (!h || !path) return LBM_ERR_ARG;
+    if (!h->inited) return io_err(h, LBM_ERR_STATE, "save_checkpoint: not initialised");
+    if (h->fstream) cudaStreamSynchronize(h->fstream);
+    if (h->side) cudaStreamSynchronize(h->side);
+    CkptHeader hd;
+    std::vector<unsigned char> blob;
+    int rc = gather_state(h, hd, blob);
+    if (rc) return rc;
+    const std::string p = path, c = copy_path(p);
+    if (write_ckpt_file(p, hd, blob)) return io_err(h, LBM_ERR_IO, "save_checkpoint: cannot write " + p);
+    if (write_ckpt_file(c, hd, blob)) return io_err(h, LBM_ERR_IO, "save_checkpoint: cannot write " + c);
+    return LBM_OK;
+}
+
+int lbm_load_checkpoint(lbm_t *h, const char *path)
+{
+    if (!h || !path) return LBM_ERR_ARG;
+    if (!h->inited) return io_err(h, LBM_ERR_STATE, "load_checkpoint: call lbm_init first");
+    CkptHeader hd;
+    std::vector<unsigned char> blob;
+    const std::string p = path, c = copy_path(p);
+    std::string why = read_ckpt_file(h, p, hd, blob);
+    if (!why.empty()) {
+        const std::string why2 = read_ckpt_file(h, c, hd, blob);   // the copy (readflowfield, solution.f90:1757-1790)
+        if (!why2.empty()) return io_err(h, LBM_ERR_IO, "load_checkpoint: " + why + "; " + why2);
+    }
+    if (h->fstream) cudaStreamSynchronize(h->fstream);
+    if (h->side) cudaStreamSynchronize(h->side);
+    cudaStreamSynchronize(h->stream);
+    const unsigned char *q = blob.data();
+    h->cur = 0;
+    cudaError_t e = cudaMemcpyAsync(h->fbuf[0], q, hd.pop_bytes, cudaMemcpyHostToDevice, h->stream);
+    q += hd.pop_bytes;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h->edge_c, q, hd.edge_bytes, cudaMemcpyHostToDevice, h->stream);
+    q += hd.edge_bytes;
+    for (int s = 0; s < 2 && e == cudaSuccess; ++s, q += hd.field_bytes)
+        e = cudaMemcpyAsync(h->d_fields[s], q, hd.field_bytes, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) return io_err(h, LBM_ERR_CUDA, std::string("load_checkpoint: ") + cudaGetErrorString(e));
+    h->n = (int)hd.n;
+    h->steps_done = (int)hd.steps_done;
+    h->fields_slot = hd.fields_slot;
+    h->fields_step[0] = (int)hd.fields_step[0];
+    h->fields_step[1] = (int)hd.fields_step[1];
+    // the factorization slots are filled again for the restored step
+    h->batch_in_half[0] = h->batch_in_half[1] = -1;
+    h->fgroup[0] = h->fgroup[1] = -1;
+    return LBM_OK;
+}
+
+}  // extern "C"

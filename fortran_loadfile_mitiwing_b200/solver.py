@@ -114,6 +114,23 @@ class Lbm:
         self._ck(self.lib.lbm_get_populations(self.h, dptr(f)))
         return f.reshape(9, self.ny, self.nx)
 
+    # -- output and restart files ----------------------------------------
+    def write_tecplot(self, path=None, cycle=None, stride=(2, 2), directory="."):
+        """F<n>.dat of the state after the last step (lbm_write_tecplot);
+        cycle defaults to the reference's n of that step. Returns the path."""
+        cycle = self.step_index - 1 if cycle is None else int(cycle)
+        path = path or os.path.join(directory, f"F{cycle}.dat")
+        self._ck(self.lib.lbm_write_tecplot(self.h, os.fsencode(path), cycle, int(stride[0]), int(stride[1])))
+        return path
+
+    def save_checkpoint(self, path="saved_flow_feild.dat"):
+        """Writes the state to `path` and its _copy (lbm_save_checkpoint)."""
+        self._ck(self.lib.lbm_save_checkpoint(self.h, os.fsencode(path)))
+
+    def load_checkpoint(self, path="saved_flow_feild.dat"):
+        """Restores the state from `path`, else its _copy (lbm_load_checkpoint)."""
+        self._ck(self.lib.lbm_load_checkpoint(self.h, os.fsencode(path)))
+
     def set_populations(self, f):
         f = np.ascontiguousarray(f, dtype=np.float64).reshape(-1)
         self._ck(self.lib.lbm_set_populations(self.h, dptr(f)))

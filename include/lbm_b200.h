@@ -239,6 +239,40 @@ LBM_API int lbm_device_bytes(const lbm_t *h, long long *bytes);
  * errors of lbm_create. The string stays valid until the next call on h. */
 LBM_API const char *lbm_last_error(const lbm_t *h);
 
+/* ---- output and restart files -------------------------------------------
+ * lbm_write_tecplot: the reference's output (solution.f90:129-238) for the
+ *   state after the last step: Tecplot ASCII with the field zone sampled
+ *   every stride_x-th / stride_y-th node from node 1 (the reference uses 2
+ *   and 2; X, Y, U/UU, V/UU, pressure rho/3, vorticity dv/dx - du/dy with its
+ *   one-sided differences on the edges, body and dvordt, written as 0: the
+ *   live reference zeroes body after body_point, solution.f90:69, and never
+ *   calls vor_mom_rate, main.f90:391), format (25e16.8), then the airfoil
+ *   zone: contour points of the last step and one centre node per wing in
+ *   (8f14.8), triangles in (3I5.3). `cycle` is the reference's n (file
+ *   F<n>.dat; SOLUTIONTIME = n UU mesh_max_scale). Header lines are
+ *   list-directed in spirit (values and order), not in one compiler's
+ *   spacing.
+ * lbm_write_tecplot_fields: the same file from host arrays (nx,ny) in
+ *   Fortran order, without a handle (xb1, yb1: wing_count*points_per_wing
+ *   contour points, nullable when wing_count = 0).
+ * lbm_save_checkpoint / lbm_load_checkpoint: saveflowfield / readflowfield
+ *   (solution.f90:1604-1839) as a two-file scheme: `path` and its copy (name
+ *   with "_copy" before the extension, as saved_flow_feild_copy.dat), both
+ *   written; the loader reads `path` and falls back to the copy when it is
+ *   missing, short, from another grid or storage precision, or fails its
+ *   checksum. The content is this library's own state (populations in
+ *   storage precision, boundary reference values, both field slots, step
+ *   counters), so a restart continues bit for bit; it is not the byte layout
+ *   of the reference's form='binary' file. Load after lbm_init of a handle
+ *   with the same parameters, boundary and motion table. */
+LBM_API int lbm_write_tecplot(lbm_t *h, const char *path, int cycle, int stride_x, int stride_y);
+LBM_API int lbm_write_tecplot_fields(const char *path, int nx, int ny, double ox, double oy, double scale, double uu,
+                                     double solution_time, int stride_x, int stride_y, const double *rho,
+                                     const double *u, const double *v, int wing_count, int points_per_wing,
+                                     const double *xb1, const double *yb1);
+LBM_API int lbm_save_checkpoint(lbm_t *h, const char *path);
+LBM_API int lbm_load_checkpoint(lbm_t *h, const char *path);
+
 /* ---- batches: several cases stepped together on one GPU ----------------
  * The reference runs one case per process (main.f90); flapping-wing studies
  * are sweeps of many cases. A batch steps initialised handles of different
