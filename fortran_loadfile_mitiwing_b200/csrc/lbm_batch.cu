@@ -27,6 +27,9 @@ constexpr int kFactorRing = 8;   // staging buffers of factorization arguments i
 // 2 factorization batches (2K steps, two launches a step) old when used, and
 // a wait on a newer recording of a reused event only waits longer
 constexpr int kGroupRing = 64;
+// per-step argument buffers in flight: the host prepares a step's arguments
+// while up to kArgRing - 1 earlier steps are still queued
+constexpr int kArgRing = 8;
 }
 
 struct lbm_batch {
@@ -34,15 +37,17 @@ struct lbm_batch {
     int prec = -1, fbatch = 4, nslots = 8, dev = 0;
     cudaStream_t main = nullptr, side = nullptr, fstream = nullptr;
     cudaEvent_t ev_ib = nullptr, ev_done = nullptr, ev_fready = nullptr, ev_side = nullptr;
-    // argument arrays: flow chain and lattice per step (double-buffered so a
-    // step's upload never overwrites arguments a queued launch still reads),
-    // case table, and a ring of factorization argument buffers
+    // argument arrays: flow chain and lattice per step (a ring of kArgRing,
+    // so a step's upload never overwrites arguments a queued launch still
+    // reads), the case table (two buffers, uploaded again only when the set
+    // of active cases changes), and a ring of factorization argument buffers
     int cap = 0;         // cases the arrays hold
     int table_cap = 0;   // case-table entries
-    void *d_sargs[2] = {nullptr, nullptr}, *d_kargs[2] = {nullptr, nullptr};
-    void *h_sargs[2] = {nullptr, nullptr}, *h_kargs[2] = {nullptr, nullptr};
+    void *d_sargs[kArgRing] = {}, *d_kargs[kArgRing] = {};
+    void *h_sargs[kArgRing] = {}, *h_kargs[kArgRing] = {};
+    cudaEvent_t ev_upload[kArgRing] = {}, ev_kdone[kArgRing] = {};
     int4 *d_table[2] = {nullptr, nullptr}, *h_table[2] = {nullptr, nullptr};
-    cudaEvent_t ev_upload[2] = {nullptr, nullptr};
+    cudaEvent_t ev_tup[2] = {nullptr, nullptr}, ev_tuse[2] = {nullptr, nullptr};
     void *d_fargs[kFactorRing] = {}, *h_fargs[kFactorRing] = {};
     cudaEvent_t ev_fup[kFactorRing] = {};
     int fring = 0;
@@ -77,14 +82,16 @@ void sync_streams(lbm_batch *b)
 
 void free_arrays(lbm_batch *b)
 {
-    for (int q = 0; q < 2; ++q) {
+    for (int q = 0; q < kArgRing; ++q) {
         if (b->d_sargs[q]) cudaFree(b->d_sargs[q]);
         if (b->d_kargs[q]) cudaFree(b->d_kargs[q]);
-        if (b->d_table[q]) cudaFree(b->d_table[q]);
         if (b->h_sargs[q]) cudaFreeHost(b->h_sargs[q]);
         if (b->h_kargs[q]) cudaFreeHost(b->h_kargs[q]);
-        if (b->h_table[q]) cudaFreeHost(b->h_table[q]);
         b->d_sargs[q] = b->d_kargs[q] = b->h_sargs[q] = b->h_kargs[q] = nullptr;
+    }
+    for (int q = 0; q < 2; ++q) {
+        if (b->d_table[q]) cudaFree(b->d_table[q]);
+        if (b->h_table[q]) cudaFreeHost(b->h_table[q]);
         b->d_table[q] = b->h_table[q] = nullptr;
     }
     for (int r = 0; r < kFactorRing; ++r) {
@@ -99,8 +106,14 @@ void free_batch(lbm_batch *b)
 {
     sync_streams(b);
     free_arrays(b);
-    for (int q = 0; q < 2; ++q)
+    for (int q = 0; q < kArgRing; ++q) {
         if (b->ev_upload[q]) cudaEventDestroy(b->ev_upload[q]);
+        if (b->ev_kdone[q]) cudaEventDestroy(b->ev_kdone[q]);
+    }
+    for (int q = 0; q < 2; ++q) {
+        if (b->ev_tup[q]) cudaEventDestroy(b->ev_tup[q]);
+        if (b->ev_tuse[q]) cudaEventDestroy(b->ev_tuse[q]);
+    }
     for (int r = 0; r < kFactorRing; ++r)
         if (b->ev_fup[r]) cudaEventDestroy(b->ev_fup[r]);
     for (int r = 0; r < kGroupRing; ++r)
@@ -119,12 +132,14 @@ int reserve(lbm_batch *b, int ncase, int ntab)
     sync_streams(b);
     const int nc = std::max(ncase, b->cap), nt = std::max(ntab, b->table_cap);
     free_arrays(b);
-    for (int q = 0; q < 2; ++q) {
+    for (int q = 0; q < kArgRing; ++q) {
         BCK(cudaMalloc(&b->d_sargs[q], nc * b->ib_sz), "alloc");
         BCK(cudaMalloc(&b->d_kargs[q], nc * b->kf_sz), "alloc");
-        BCK(cudaMalloc(&b->d_table[q], sizeof(int4) * (size_t)nt), "alloc");
         BCK(cudaMallocHost(&b->h_sargs[q], nc * b->ib_sz), "alloc");
         BCK(cudaMallocHost(&b->h_kargs[q], nc * b->kf_sz), "alloc");
+    }
+    for (int q = 0; q < 2; ++q) {
+        BCK(cudaMalloc(&b->d_table[q], sizeof(int4) * (size_t)nt), "alloc");
         BCK(cudaMallocHost((void **)&b->h_table[q], sizeof(int4) * (size_t)nt), "alloc");
     }
     for (int r = 0; r < kFactorRing; ++r) {
@@ -218,8 +233,12 @@ int lbm_batch_create(lbm_t *const *cases, int count, lbm_batch_t **out)
     if ((e = cudaStreamCreateWithPriority(&b->side, cudaStreamNonBlocking, prio_high)) != cudaSuccess)
         return fail(e, "stream");
     if ((e = cudaStreamCreateWithFlags(&b->fstream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
-    for (cudaEvent_t *ev : {&b->ev_ib, &b->ev_done, &b->ev_fready, &b->ev_side, &b->ev_upload[0], &b->ev_upload[1]})
+    for (cudaEvent_t *ev : {&b->ev_ib, &b->ev_done, &b->ev_fready, &b->ev_side, &b->ev_tup[0], &b->ev_tup[1],
+                            &b->ev_tuse[0], &b->ev_tuse[1]})
         if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+    for (int q = 0; q < kArgRing; ++q)
+        for (cudaEvent_t *ev : {&b->ev_upload[q], &b->ev_kdone[q]})
+            if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
     for (int r = 0; r < kFactorRing; ++r)
         if ((e = cudaEventCreateWithFlags(&b->ev_fup[r], cudaEventDisableTiming)) != cudaSuccess)
             return fail(e, "event");
@@ -392,6 +411,8 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
     std::vector<lbm_handle *> act;
     std::vector<int> act_idx;
     std::vector<long long> waited;
+    std::vector<int> tkey, tkey_now;   // grids of the active cases the current table was built for
+    int tcur = -1, ntab = 0;           // table buffer in use, its entries
     for (; step < nsteps; ++step) {
         act.clear();
         act_idx.clear();
@@ -401,15 +422,16 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
                 act_idx.push_back(c);
             }
         if (act.empty()) break;
-        const int buf = step & 1;
+        const int buf = step % kArgRing;
         // fields (rho, u, v) for the last two steps of the call and of every
         // case that ends within them (all active cases keep them then)
         bool fields = step >= nsteps - 2;
         for (size_t c = 0; c < act.size() && !fields; ++c) fields = act[c]->n >= last_step[act_idx[c]] - 1;
         if ((rc = factor_needed(act, act_idx, false))) break;
-        // this step's arguments (the staging buffers of two steps back are free)
+        // this step's arguments (the staging buffer's previous upload, kArgRing
+        // steps back, is done)
         BCK(cudaEventSynchronize(b->ev_upload[buf]), "sync upload");
-        int ntab = 0;
+        tkey_now.clear();
         for (size_t c = 0; c < act.size(); ++c) {
             lbm_handle *h = act[c];
             const int q = h->n % b->nslots;
@@ -427,25 +449,40 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
             kf_args_write(h, fin, fout, fd, KF_OUTER, (char *)b->h_kargs[buf] + c * b->kf_sz);
             int gx, gy;
             kf_tma_grid(h, &gx, &gy);
-            if (ntab + gx * gy > b->table_cap) {
-                rc = berr(b, LBM_ERR_STATE, "batch: case table overflow");
-                break;
-            }
-            for (int by = 0; by < gy; ++by)
-                for (int bx = 0; bx < gx; ++bx) b->h_table[buf][ntab++] = make_int4((int)c, bx, by, gx | (gy << 16));
+            tkey_now.push_back(gx | (gy << 16));
         }
-        if (rc) break;
-        // side stream: once the previous step is complete (and with it every
-        // reader of this step's upload buffers), the uploads and the flow
-        // chains of all cases
-        BCK(cudaStreamWaitEvent(b->side, b->ev_done, 0), "wait");
+        // the case table, built again only when the active cases change; the
+        // other of its two buffers is reused once its last reader is done
+        if (tcur < 0 || tkey_now != tkey) {
+            const int k = tcur < 0 ? 0 : tcur ^ 1;
+            BCK(cudaEventSynchronize(b->ev_tup[k]), "sync upload");
+            ntab = 0;
+            for (size_t c = 0; c < act.size(); ++c) {
+                const int gx = tkey_now[c] & 0xffff, gy = tkey_now[c] >> 16;
+                if (ntab + gx * gy > b->table_cap) {
+                    rc = berr(b, LBM_ERR_STATE, "batch: case table overflow");
+                    break;
+                }
+                for (int by = 0; by < gy; ++by)
+                    for (int bx = 0; bx < gx; ++bx) b->h_table[k][ntab++] = make_int4((int)c, bx, by, tkey_now[c]);
+            }
+            if (rc) break;
+            BCK(cudaStreamWaitEvent(b->side, b->ev_tuse[k], 0), "wait");
+            BCK(cudaMemcpyAsync(b->d_table[k], b->h_table[k], sizeof(int4) * ntab, cudaMemcpyHostToDevice, b->side),
+                "upload");
+            BCK(cudaEventRecord(b->ev_tup[k], b->side), "event");
+            tcur = k;
+            tkey = tkey_now;
+        }
+        // side stream: the uploads (once the lattice launch that last read this
+        // buffer is done), then, after the previous step, the flow chains
+        BCK(cudaStreamWaitEvent(b->side, b->ev_kdone[buf], 0), "wait");
         BCK(cudaMemcpyAsync(b->d_sargs[buf], b->h_sargs[buf], act.size() * b->ib_sz, cudaMemcpyHostToDevice, b->side),
             "upload");
         BCK(cudaMemcpyAsync(b->d_kargs[buf], b->h_kargs[buf], act.size() * b->kf_sz, cudaMemcpyHostToDevice, b->side),
             "upload");
-        BCK(cudaMemcpyAsync(b->d_table[buf], b->h_table[buf], sizeof(int4) * ntab, cudaMemcpyHostToDevice, b->side),
-            "upload");
         BCK(cudaEventRecord(b->ev_upload[buf], b->side), "event");
+        BCK(cudaStreamWaitEvent(b->side, b->ev_done, 0), "wait");
         // the factorization launches of this step's halves (those of earlier
         // runs are complete: every run ends with its streams idle)
         waited.clear();
@@ -472,10 +509,12 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
         if ((rc = factor_needed(act, act_idx, true))) break;
         // main stream: every case's lattice nodes but its correction tiles
         BCK(cudaStreamWaitEvent(b->main, b->ev_fready, 0), "wait");
-        if (launch_kf_multi(b->prec, b->d_kargs[buf], b->d_table[buf], ntab, fields, b->main)) {
+        if (launch_kf_multi(b->prec, b->d_kargs[buf], b->d_table[tcur], ntab, fields, b->main)) {
             rc = berr(b, LBM_ERR_CUDA, "batch: launch lattice");
             break;
         }
+        BCK(cudaEventRecord(b->ev_kdone[buf], b->main), "event");
+        BCK(cudaEventRecord(b->ev_tuse[tcur], b->main), "event");
         for (lbm_handle *h : act) h->launches += 1;
         BCK(cudaStreamWaitEvent(b->main, b->ev_ib, 0), "wait");
         BCK(cudaEventRecord(b->ev_done, b->main), "event");   // the step is complete
