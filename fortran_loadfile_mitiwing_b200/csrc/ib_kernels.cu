@@ -994,8 +994,40 @@ __global__ void __launch_bounds__(256) ib_tile_scatter(const IBArgs base0, const
             int *list = a.tiles + (long long)tile * (TILE_CAP + 1);
             const int pos = atomicAdd(list, 1);
             if (pos < TILE_CAP) list[1 + pos] = k;
-            if (pos == 0) a.ctile[atomicAdd(a.nsup, 1)] = tile;   // first marker of the tile
         }
+}
+
+// The step's correction tiles (those listing a marker) in ascending tile
+// order, by a block scan of the tile counts: one CTA per member. The order
+// fixes the order of the force sum, so the force rows do not depend on the
+// order the scatter's atomics happened to run in.
+template <bool BATCH>
+__global__ void __launch_bounds__(256) ib_tile_compact(const IBArgs base0, const IBArgs *batch, int step0)
+{
+    const IBArgs &base = BATCH ? batch[blockIdx.z] : base0;
+    const int step_index = factor_step<BATCH>(base, step0);
+    if (step_index < 0) return;
+    const IBArgs a = member_args(base, step_index);
+    __shared__ int wsum[8];
+    const int nt = (int)(a.st_tiles / (TILE_CAP + 1));
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int per = (nt + 255) / 256, b0 = min(nt, t * per), b1 = min(nt, b0 + per);
+    int cnt = 0;
+    for (int b = b0; b < b1; ++b) cnt += a.tiles[(long long)b * (TILE_CAP + 1)] > 0;
+    int x = cnt;   // inclusive scan within the warp
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, off);
+        if (lane >= off) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
+    __syncthreads();
+    int before = 0;
+    for (int w = 0; w < warp; ++w) before += wsum[w];
+    int pos = before + x - cnt;
+    for (int b = b0; b < b1; ++b)
+        if (a.tiles[(long long)b * (TILE_CAP + 1)] > 0) a.ctile[pos++] = b;
+    if (t == 255) *a.nsup = before + x;
 }
 
 template <bool BATCH>
@@ -1011,9 +1043,11 @@ __global__ void __launch_bounds__(TILE_CAP) ib_tile_sort(const IBArgs base0, con
         int *list = a.tiles + (long long)a.ctile[c] * (TILE_CAP + 1);
         const int m = min(list[0], TILE_CAP);
         key[t] = t < m ? list[1 + t] : 0x7fffffff;
+        int np = 2;   // keys sorted: the power of two at or above the count
+        while (np < m) np <<= 1;
         __syncthreads();
-        // bitonic sort of TILE_CAP keys, ascending
-        for (int size = 2; size <= TILE_CAP; size <<= 1)
+        // bitonic sort of np keys, ascending (the padding keys stay at the end)
+        for (int size = 2; size <= np; size <<= 1)
             for (int stride = size >> 1; stride > 0; stride >>= 1) {
                 const int u = t ^ stride;
                 if (u > t) {
@@ -1028,25 +1062,23 @@ __global__ void __launch_bounds__(TILE_CAP) ib_tile_sort(const IBArgs base0, con
     }
 }
 
-// The step's force row from the correction tiles' partials, summed in tile
-// order (deterministic), one CTA; no correction tile gives zero forces
-// (solution.f90:327-330 normalisation). Needed by no kernel of the step, so
-// it runs after the step's update.
+// The step's force row from the correction tiles' partials, summed over the
+// compact tile list in ascending tile order (deterministic), one CTA; no
+// correction tile gives zero forces (solution.f90:327-330 normalisation).
+// Needed by no kernel of the step, so it runs after the step's update.
 template <bool BATCH>
 __global__ void __launch_bounds__(256) ib_forces(const IBArgs a0, const IBArgs *batch, int ring_slot)
 {
     const IBArgs &a = BATCH ? batch[blockIdx.z] : a0;
     __shared__ double red[8][NPART];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int ntiles_all = (int)(a.st_tiles / (TILE_CAP + 1));
+    const int ntile = a.nseg > 0 ? *a.nsup : 0;
     for (int w = 0; w < a.nwing; ++w) {
         double s0 = 0, s1 = 0, s2 = 0;
-        if (a.nseg > 0)
-            for (int b = threadIdx.x; b < ntiles_all; b += blockDim.x) {
-                if (a.tiles[(long long)b * (TILE_CAP + 1)] == 0) continue;
-                const double *p = a.partial + (long long)b * NPART + 3 * w;
-                s0 += p[0]; s1 += p[1]; s2 += p[2];
-            }
+        for (int c = threadIdx.x; c < ntile; c += blockDim.x) {
+            const double *p = a.partial + (long long)a.ctile[c] * NPART + 3 * w;
+            s0 += p[0]; s1 += p[1]; s2 += p[2];
+        }
 #pragma unroll
         for (int off = 16; off; off >>= 1) {
             s0 += __shfl_down_sync(0xffffffffu, s0, off);
@@ -1086,6 +1118,7 @@ template <bool BATCH>
 __global__ void __launch_bounds__(256) ib_residual(const IBArgs a0, const IBArgs *batch)
 {
     const IBArgs &a = BATCH ? batch[blockIdx.z] : a0;
+    if (BATCH && !a.check_res) return;   // this case's step is not checked
     __shared__ double red[8][2];
     __shared__ bool amlast;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1374,6 +1407,7 @@ IBArgs make_args(lbm_handle *h, const void *fin, int slot)
     a.status = h->d_status; a.solve_res = h->d_solve_res;
     a.cur_step = h->n;
     a.fstep0 = 0; a.fcount = 0;
+    a.check_res = 1;
     return a;
 }
 
@@ -1399,12 +1433,12 @@ int launch_flow_t(lbm_handle *h, const void *fin, void *fout, void *fields, int 
 
 // the residual check of the step's solve (needed by no later kernel of the step)
 template <typename T, typename C>
-int launch_check_t(lbm_handle *h, int slot, int ring_slot, cudaStream_t st)
+int launch_check_t(lbm_handle *h, int slot, int ring_slot, bool residual, cudaStream_t st)
 {
     IBArgs a = make_args(h, nullptr, slot);
     ib_forces<false><<<1, 256, 0, st>>>(a, nullptr, ring_slot);
     h->launches += 1;
-    if (h->nseg == 0) return cudaGetLastError() == cudaSuccess ? 0 : -1;
+    if (h->nseg == 0 || !residual) return cudaGetLastError() == cudaSuccess ? 0 : -1;
     ib_residual<false><<<(h->nseg + 7) / 8, 256, 0, st>>>(a, nullptr);
     h->launches += 1;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
@@ -1462,16 +1496,17 @@ int launch_factor(lbm_handle *h, int step0, int count, cudaStream_t st)
     ib_assemble<false><<<dim3(nb, count), 256, 0, st>>>(a, nullptr, step0);
     ib_factor<false><<<dim3(1, count), FACTOR_THREADS, kFactorSmem, st>>>(a, nullptr, step0);
     ib_tile_scatter<false><<<dim3((h->nseg + 255) / 256, count), 256, 0, st>>>(a, nullptr, step0);
+    ib_tile_compact<false><<<dim3(1, count), 256, 0, st>>>(a, nullptr, step0);
     ib_tile_sort<false><<<dim3(std::min(h->patch_gx() * h->patch_gy(), 148), count), TILE_CAP, 0, st>>>(a, nullptr,
                                                                                                         step0);
-    h->launches += h->static_order ? 5 : 6;
+    h->launches += h->static_order ? 6 : 7;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
 // force row and residual check of the step held in `slot`, after its flow chain
-int launch_check(lbm_handle *h, int slot, int ring_slot, cudaStream_t st)
+int launch_check(lbm_handle *h, int slot, int ring_slot, bool residual, cudaStream_t st)
 {
-    return launch_check_t<float, float>(h, slot, ring_slot, st ? st : h->stream);
+    return launch_check_t<float, float>(h, slot, ring_slot, residual, st ? st : h->stream);
 }
 
 // flow chain of step `step_index`: interpolation, solve with the factor of
@@ -1553,8 +1588,9 @@ int launch_factor_batch(lbm_handle *const *hs, int ncase, const void *dargs, int
     ib_assemble<true><<<dim3(nb, count, ncase), 256, 0, st>>>(IBArgs{}, d, step0);
     ib_factor<true><<<dim3(1, count, ncase), FACTOR_THREADS, kFactorSmem, st>>>(IBArgs{}, d, step0);
     ib_tile_scatter<true><<<dim3((ns + 255) / 256, count, ncase), 256, 0, st>>>(IBArgs{}, d, step0);
+    ib_tile_compact<true><<<dim3(1, count, ncase), 256, 0, st>>>(IBArgs{}, d, step0);
     ib_tile_sort<true><<<dim3(std::min(tiles, 148), count, ncase), TILE_CAP, 0, st>>>(IBArgs{}, d, step0);
-    for (int c = 0; c < ncase; ++c) hs[c]->launches += any_order ? 6 : 5;
+    for (int c = 0; c < ncase; ++c) hs[c]->launches += any_order ? 7 : 6;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 

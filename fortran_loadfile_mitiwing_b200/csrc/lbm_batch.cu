@@ -445,7 +445,11 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
                 h->fields_step[fs] = h->n;
             }
             h->pinfo_slot = q;
-            ib_args_write(h, fin, q, (char *)b->h_sargs[buf] + c * b->ib_sz);
+            IBArgs *ia = (IBArgs *)((char *)b->h_sargs[buf] + c * b->ib_sz);
+            ib_args_write(h, fin, q, ia);
+            // the solve-residual check: last step of the case's factorization
+            // batch, of the call, or of the case's motion
+            ia->check_res = (h->n + 1) % K == 0 || step == nsteps - 1 || h->n >= last_step[act_idx[c]];
             kf_args_write(h, fin, fout, fd, KF_OUTER, (char *)b->h_kargs[buf] + c * b->kf_sz);
             int gx, gy;
             kf_tma_grid(h, &gx, &gy);

@@ -347,6 +347,9 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             h->fields_step[fs] = h->n;
         }
         cudaEvent_t *e = h->timing ? &h->ev[4 * slot] : nullptr;
+        // the solve-residual check: on the last step of each factorization
+        // batch and on the last step of the call
+        const bool check_res = (h->n + 1) % K == 0 || s == nsteps - 1;
         if (split) {
             // side stream: the immersed-boundary chain and the correction
             // tiles; main stream: every other node, concurrently
@@ -357,7 +360,7 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             if (launch_flow(h, fin, fout, fields, h->n, slot, q, h->side)) return cuda_err(h, cudaGetLastError(), "launch ib");
             if (e) CK(cudaEventRecord(h->ev_side[2 * slot + 1], h->side), "event");
             CK(cudaEventRecord(h->ev_ib, h->side), "event");
-            if (launch_check(h, q, slot, h->side)) return cuda_err(h, cudaGetLastError(), "launch check");
+            if (launch_check(h, q, slot, check_res, h->side)) return cuda_err(h, cudaGetLastError(), "launch check");
             CK(cudaEventRecord(h->ev_free[half], h->side), "event");
             // the next batch's factorization, overlapping this batch's steps
             if ((b + 1) * K <= last_step && h->batch_in_half[half ^ 1] != b + 1 && (rc = factor_batch(b + 1))) return rc;
@@ -375,7 +378,7 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             if (e) CK(cudaEventRecord(e[0], h->stream), "event");
             if (h->batch_in_half[half] != b && (rc = factor_batch(b))) return rc;
             if (launch_flow(h, fin, fout, fields, h->n, slot, q, h->stream)) return cuda_err(h, cudaGetLastError(), "launch ib");
-            if (launch_check(h, q, slot, h->stream)) return cuda_err(h, cudaGetLastError(), "launch check");
+            if (launch_check(h, q, slot, check_res, h->stream)) return cuda_err(h, cudaGetLastError(), "launch check");
             if (e) {
                 CK(cudaEventRecord(e[1], h->stream), "event");
                 CK(cudaEventRecord(e[2], h->stream), "event");

@@ -75,6 +75,7 @@ struct IBArgs {
     int static_order;   // one rigid body: fixed solve order (ib_order leaves it)
     int cur_step;       // step index of the flow chain (batched launches: per case)
     int fstep0, fcount; // steps of the factorization chain (batched launches: per case)
+    int check_res;      // batched launches: run the solve-residual check for this case's step
     long long st_mk, st_perm, st_B, wk_blocks, wk_gf;
     PatchInfo *pinfo;
     int *tiles;         // per patch tile: marker count, then the listed markers (slot)
@@ -200,7 +201,7 @@ int launch_kf(lbm_handle *h, const void *fin, void *fout, void *fields, int mode
 int launch_factor(lbm_handle *h, int step0, int count, cudaStream_t st);
 int launch_flow(lbm_handle *h, const void *fin, void *fout, void *fields, int step_index, int ring_slot, int slot,
                 cudaStream_t st);
-int launch_check(lbm_handle *h, int slot, int ring_slot, cudaStream_t st);
+int launch_check(lbm_handle *h, int slot, int ring_slot, bool residual, cudaStream_t st);
 // batches of cases stepped together (lbm_batch.cu)
 int handle_prepare_ib(lbm_handle *h);                    // immersed-boundary buffers (once per geometry)
 int handle_error(lbm_handle *h, int code, const char *msg);

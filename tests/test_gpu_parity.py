@@ -87,10 +87,11 @@ def test_step_and_run_agree_bitwise(gpu_lib):
 
 def test_launch_count_per_step(gpu_lib):
     """Per step of one rigid wing: the flow chain (interpolation, solve, update
-    of the correction tiles, force row, residual check) and the lattice kernel;
-    plus, per batch of steps, the five kernels of the batched factorization of
-    the marker system (geometry, band assembly, factorization, patch-tile
-    lists in two passes)."""
+    of the correction tiles, force row) and the lattice kernel; the residual
+    check on the last step of each batch of 4 steps and of the call; per batch
+    of steps, the six kernels of the batched factorization of the marker
+    system (geometry, band assembly, factorization, patch-tile lists in three
+    passes)."""
     import ctypes as C
     case = cases.small_case(precision="fp32", n_steps=100)
     g = Lbm.from_case(case, gpu_lib)
@@ -101,9 +102,12 @@ def test_launch_count_per_step(gpu_lib):
     g.run(steps)
     gpu_lib.lbm_get_launch_count(g.h, C.byref(n1))
     total = n1.value - n0.value
-    per_step = 5 + 1
-    assert total >= steps * per_step and (total - steps * per_step) % 5 == 0, total
-    assert 1 <= (total - steps * per_step) // 5 <= steps, total
+    per_step = 4 + 1
+    # steps n = 2 .. 13: checked where (n + 1) % 4 == 0 (3, 7, 11) and the last (13)
+    checks = sum(1 for n in range(2, 2 + steps) if (n + 1) % 4 == 0 or n == 1 + steps)
+    rest = total - steps * per_step - checks
+    assert rest > 0 and rest % 6 == 0, total
+    assert 1 <= rest // 6 <= steps, total
 
 
 def test_residual_matches_oracle(gpu_lib, oracle_mod):
