@@ -176,7 +176,7 @@ template <typename T> constexpr size_t tma_smem() { return sizeof(T) * tma_stage
 
 // One CTA of the staged kernel: strip bx (of gx) and row chunk by (of gy; the
 // last chunk is the edge CTA row) of the lattice described by `a`.
-template <typename T, typename C, bool FIELDS>
+template <typename T, typename C, bool FIELDS, bool CONS0>
 __device__ __forceinline__ void kf_tma_cta(const KFArgs<C> &a, int bx, int by, int gx, int gy, unsigned char *smraw)
 {
     constexpr int H = tma_halo<T>(), SEG = tma_seg<T>(), NWARP = TW / 32, KS = tma_stages<T>();
@@ -252,7 +252,7 @@ __device__ __forceinline__ void kf_tma_cta(const KFArgs<C> &a, int bx, int by, i
             const T *row = buf + s * 9 * SEG + H + tid;
 #pragma unroll
             for (int k = 0; k < 9; ++k) g[k] = (C)Store<T>::cvt(row[k * SEG - lbm_ex(k)]);
-            collide_interior<C>(a, g, false, C(0), C(0), gout, frho, fu, fv);
+            collide_interior<C, CONS0>(a, g, false, C(0), C(0), gout, frho, fu, fv);
             store_node<T, C, FIELDS>(a, fout, i, j, gout, frho, fu, fv);
         }
         __syncwarp();
@@ -274,21 +274,33 @@ __device__ __forceinline__ void kf_tma_cta(const KFArgs<C> &a, int bx, int by, i
     }
 }
 
-template <typename T, typename C, bool FIELDS>
+template <typename T, typename C, bool FIELDS, bool CONS0>
 __global__ void __launch_bounds__(TW, KF_MINB) kf_tma(const KFArgs<C> a)
 {
     extern __shared__ __align__(128) unsigned char smraw[];
-    kf_tma_cta<T, C, FIELDS>(a, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, smraw);
+    kf_tma_cta<T, C, FIELDS, CONS0>(a, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, smraw);
 }
 
 // Several lattices (a batch of cases) in one launch: CTA b runs entry b of
 // the case table, {case, strip, row chunk, strips | row chunks << 16}.
-template <typename T, typename C, bool FIELDS>
+template <typename T, typename C, bool FIELDS, bool CONS0>
 __global__ void __launch_bounds__(TW, KF_MINB) kf_tma_multi(const KFArgs<C> *cases, const int4 *table)
 {
     extern __shared__ __align__(128) unsigned char smraw[];
     const int4 t = table[blockIdx.x];
-    kf_tma_cta<T, C, FIELDS>(cases[t.x], t.y, t.z, t.w & 0xffff, t.w >> 16, smraw);
+    kf_tma_cta<T, C, FIELDS, CONS0>(cases[t.x], t.y, t.z, t.w & 0xffff, t.w >> 16, smraw);
+}
+
+// the conserved moments' relaxation rates are zero (the reference's setting)
+template <typename C> bool cons0(const KFArgs<C> &a) { return a.s[0] == C(0) && a.s[3] == C(0) && a.s[5] == C(0); }
+
+template <typename T, typename C, bool FIELDS>
+void launch_tma_f(const KFArgs<C> &a, dim3 grid, dim3 block, size_t smem, cudaStream_t st)
+{
+    if (cons0(a))
+        kf_tma<T, C, FIELDS, true><<<grid, block, smem, st>>>(a);
+    else
+        kf_tma<T, C, FIELDS, false><<<grid, block, smem, st>>>(a);
 }
 
 template <typename T, typename C>
@@ -297,23 +309,29 @@ void launch_tma(const KFArgs<C> &a, bool fields, int nx, int ny, cudaStream_t st
     dim3 block(TW, 1), grid((nx + TW - 1) / TW, (ny - 2 + a.rows_per_cta - 1) / a.rows_per_cta + 1);
     const size_t smem = tma_smem<T>();
     if (fields)
-        kf_tma<T, C, true><<<grid, block, smem, st>>>(a);
+        launch_tma_f<T, C, true>(a, grid, block, smem, st);
     else
-        kf_tma<T, C, false><<<grid, block, smem, st>>>(a);
+        launch_tma_f<T, C, false>(a, grid, block, smem, st);
+}
+
+template <typename T, typename C, bool FIELDS, bool CONS0>
+int configure_one(int smem)
+{
+    if (cudaFuncSetAttribute(kf_tma<T, C, FIELDS, CONS0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+        cudaSuccess)
+        return -1;
+    if (cudaFuncSetAttribute(kf_tma_multi<T, C, FIELDS, CONS0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+        cudaSuccess)
+        return -1;
+    return 0;
 }
 
 template <typename T, typename C>
 int configure_tma()
 {
     const int smem = (int)tma_smem<T>();
-    if (cudaFuncSetAttribute(kf_tma<T, C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
-        return -1;
-    if (cudaFuncSetAttribute(kf_tma<T, C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
-        return -1;
-    if (cudaFuncSetAttribute(kf_tma_multi<T, C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
-        return -1;
-    if (cudaFuncSetAttribute(kf_tma_multi<T, C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
-        cudaSuccess)
+    if (configure_one<T, C, true, true>(smem) || configure_one<T, C, true, false>(smem) ||
+        configure_one<T, C, false, true>(smem) || configure_one<T, C, false, false>(smem))
         return -1;
     return 0;
 }
@@ -425,7 +443,7 @@ __global__ void residual_kernel(const C *__restrict__ fa, const C *__restrict__ 
 }  // namespace
 
 template <typename T, typename C>
-int launch_kf_multi_t(const void *cases, const int4 *table, int nentries, bool fields, cudaStream_t st)
+int launch_kf_multi_t(const void *cases, const int4 *table, int nentries, bool fields, bool cons0, cudaStream_t st)
 {
     static bool configured = false;   // per process; the attribute is per function
     if (!configured) {
@@ -433,10 +451,15 @@ int launch_kf_multi_t(const void *cases, const int4 *table, int nentries, bool f
         configured = true;
     }
     const size_t smem = tma_smem<T>();
-    if (fields)
-        kf_tma_multi<T, C, true><<<nentries, TW, smem, st>>>((const KFArgs<C> *)cases, table);
+    const KFArgs<C> *c = (const KFArgs<C> *)cases;
+    if (fields && cons0)
+        kf_tma_multi<T, C, true, true><<<nentries, TW, smem, st>>>(c, table);
+    else if (fields)
+        kf_tma_multi<T, C, true, false><<<nentries, TW, smem, st>>>(c, table);
+    else if (cons0)
+        kf_tma_multi<T, C, false, true><<<nentries, TW, smem, st>>>(c, table);
     else
-        kf_tma_multi<T, C, false><<<nentries, TW, smem, st>>>((const KFArgs<C> *)cases, table);
+        kf_tma_multi<T, C, false, false><<<nentries, TW, smem, st>>>(c, table);
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
 
@@ -455,13 +478,14 @@ void kf_tma_grid(const lbm_handle *h, int *gx, int *gy) { tma_grid(h->nx, h->ny,
 
 // the staged lattice kernel over a batch of cases (device arrays of their
 // arguments and of the case table)
-int launch_kf_multi(int prec, const void *cases, const int4 *table, int nentries, bool fields, cudaStream_t st)
+int launch_kf_multi(int prec, const void *cases, const int4 *table, int nentries, bool fields, bool cons0,
+                    cudaStream_t st)
 {
     switch (prec) {
-    case LBM_PREC_FP32: return launch_kf_multi_t<float, float>(cases, table, nentries, fields, st);
-    case LBM_PREC_FP64: return launch_kf_multi_t<double, double>(cases, table, nentries, fields, st);
-    case LBM_PREC_FP16: return launch_kf_multi_t<__half, float>(cases, table, nentries, fields, st);
-    case LBM_PREC_BF16: return launch_kf_multi_t<__nv_bfloat16, float>(cases, table, nentries, fields, st);
+    case LBM_PREC_FP32: return launch_kf_multi_t<float, float>(cases, table, nentries, fields, cons0, st);
+    case LBM_PREC_FP64: return launch_kf_multi_t<double, double>(cases, table, nentries, fields, cons0, st);
+    case LBM_PREC_FP16: return launch_kf_multi_t<__half, float>(cases, table, nentries, fields, cons0, st);
+    case LBM_PREC_BF16: return launch_kf_multi_t<__nv_bfloat16, float>(cases, table, nentries, fields, cons0, st);
     }
     return -1;
 }

@@ -412,6 +412,8 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
     std::vector<int> act_idx;
     std::vector<long long> waited;
     std::vector<int> tkey, tkey_now;   // grids of the active cases the current table was built for
+    bool cons0 = true;                 // every case's conserved-moment relaxation rates are zero
+    for (lbm_handle *h : b->cases) cons0 = cons0 && h->s[0] == 0.0 && h->s[3] == 0.0 && h->s[5] == 0.0;
     int tcur = -1, ntab = 0;           // table buffer in use, its entries
     for (; step < nsteps; ++step) {
         act.clear();
@@ -513,7 +515,7 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
         if ((rc = factor_needed(act, act_idx, true))) break;
         // main stream: every case's lattice nodes but its correction tiles
         BCK(cudaStreamWaitEvent(b->main, b->ev_fready, 0), "wait");
-        if (launch_kf_multi(b->prec, b->d_kargs[buf], b->d_table[tcur], ntab, fields, b->main)) {
+        if (launch_kf_multi(b->prec, b->d_kargs[buf], b->d_table[tcur], ntab, fields, cons0, b->main)) {
             rc = berr(b, LBM_ERR_CUDA, "batch: launch lattice");
             break;
         }

@@ -113,7 +113,10 @@ __device__ __forceinline__ void side_bc(const KFArgs<C> &a, const T *__restrict_
 // interior node: moments of the streamed populations g, immersed-boundary
 // velocity correction (du, dv) when `corr` (a node of a correction tile),
 // MRT collision with forcing
-template <typename C>
+// CONS0: the relaxation rates of the conserved moments (s[0], s[3], s[5])
+// are zero, as the reference sets them (ini_mesh.f90:59-67); their terms of
+// the update are then left out at compile time.
+template <typename C, bool CONS0 = false>
 __device__ __forceinline__ void collide_interior(const KFArgs<C> &a, const C g[9], bool corr, C du, C dv, C gout[9],
                                                  C &frho, C &fu, C &fv)
 {
@@ -168,7 +171,7 @@ __device__ __forceinline__ void collide_interior(const KFArgs<C> &a, const C g[9
     // rounds relative to the small non-equilibrium update, not to g
     C d[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) d[k] = (e[k] - m[k]) * a.s[k];
+    for (int k = 0; k < 9; ++k) d[k] = (CONS0 && (k == 0 || k == 3 || k == 5)) ? C(0) : (e[k] - m[k]) * a.s[k];
     if (gx != C(0) || gy != C(0)) {        // :614-626
         const C ug = u * gx + v * gy;
         d[1] += C(6) * (C(1) - C(0.5) * a.s[1]) * ug;
