@@ -319,7 +319,9 @@ def run_e2e(args, lib):
     el = time.perf_counter() - t0
     assert rows.shape[0] == k and np.all(np.isfinite(rows))
     s.close()
-    h2d = (case.table.nbytes + 2 * nn * 8 + 9 * nn * 8 + sum(x.nbytes + y.nbytes for x, y in case.contours)) / k
+    # host -> device: motion table, contours and the perturbation du, dv (the
+    # initial populations and fields are built on the device from them)
+    h2d = (case.table.nbytes + 2 * nn * 8 + sum(x.nbytes + y.nbytes for x, y in case.contours)) / k
     d2h = s.row_len * 8 + 3 * nn * 8 / k
     return {"value": nn * k / el / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
             "note": "wall clock around the C-ABI calls (create, boundary, motion table, init, run, fields); "

@@ -408,6 +408,41 @@ __global__ void pack_kernel(const double *__restrict__ src, T *__restrict__ dst,
     Store<T>::st(dst + k * plane + (long long)j * pitch + i, (typename CType<T>::type)g);
 }
 
+// Initial populations and fields (solution.f90:33-59): f = feq(rho = 1,
+// u = UU + du, v = 0 + dv) with the single-precision lattice weights
+// (D2Q9model.f90:24-46), stored as deviations from the reference weights,
+// and the fields (1, u, v). The operations, their order and their rounding
+// are those of the host's FP64 evaluation followed by the pack kernel
+// (feq - w, + w, then - w), with round-to-nearest intrinsics so nothing is
+// contracted into an FMA: the initial state is the same bit for bit.
+template <typename T>
+__global__ void init_kernel(const double *__restrict__ du, const double *__restrict__ dv, double uu,
+                            T *__restrict__ f, typename CType<T>::type *__restrict__ fields, int nx, int ny,
+                            int pitch, long long plane)
+{
+    using C = typename CType<T>::type;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (i >= nx) return;
+    const long long q = (long long)j * nx + i, nn = (long long)nx * ny;
+    double u = uu, v = 0.0;
+    if (du) u = __dadd_rn(u, du[q]);
+    if (dv) v = __dadd_rn(v, dv[q]);
+    const double utwo = __dadd_rn(__dmul_rn(u, u), __dmul_rn(v, v));
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        const double eu = __dadd_rn(__dmul_rn((double)lbm_ex(k), u), __dmul_rn((double)lbm_ey(k), v));
+        const double ws = k == 0 ? (double)(4.0f / 9.0f) : (k < 5 ? (double)(1.0f / 9.0f) : (double)(1.0f / 36.0f));
+        const double poly = __dsub_rn(__dadd_rn(__dadd_rn(1.0, __dmul_rn(3.0, eu)), __dmul_rn(__dmul_rn(4.5, eu), eu)),
+                                      __dmul_rn(1.5, utwo));
+        const double fe = __dmul_rn(__dmul_rn(ws, 1.0), poly);
+        const double fk = __dadd_rn(__dsub_rn(fe, wref(k)), wref(k));
+        Store<T>::st(f + k * plane + (long long)j * pitch + i, (C)__dsub_rn(fk, wref(k)));
+    }
+    fields[q] = C(1);
+    fields[nn + q] = (C)u;
+    fields[2 * nn + q] = (C)v;
+}
+
 // interior sums of erranalysis (solution.f90:102-108), FP64, fields in compute precision
 template <typename C>
 __global__ void residual_kernel(const C *__restrict__ fa, const C *__restrict__ fb, int nx, int ny,
@@ -522,6 +557,33 @@ int launch_pack(lbm_handle *h, const double *src, void *fdst)
     case LBM_PREC_FP64: pack_kernel<double><<<grid, block, 0, h->stream>>>(src, (double *)fdst, h->nx, h->ny, h->pitch, h->plane); break;
     case LBM_PREC_FP16: pack_kernel<__half><<<grid, block, 0, h->stream>>>(src, (__half *)fdst, h->nx, h->ny, h->pitch, h->plane); break;
     case LBM_PREC_BF16: pack_kernel<__nv_bfloat16><<<grid, block, 0, h->stream>>>(src, (__nv_bfloat16 *)fdst, h->nx, h->ny, h->pitch, h->plane); break;
+    }
+    h->launches += 1;
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int launch_init_lattice(lbm_handle *h, const double *du, const double *dv)
+{
+    dim3 block(256), grid((h->nx + 255) / 256, h->ny);
+    const double uu = h->p.uu;
+    switch (h->prec) {
+    case LBM_PREC_FP32:
+        init_kernel<float><<<grid, block, 0, h->stream>>>(du, dv, uu, (float *)h->fbuf[0], (float *)h->d_fields[0],
+                                                          h->nx, h->ny, h->pitch, h->plane);
+        break;
+    case LBM_PREC_FP64:
+        init_kernel<double><<<grid, block, 0, h->stream>>>(du, dv, uu, (double *)h->fbuf[0], (double *)h->d_fields[0],
+                                                           h->nx, h->ny, h->pitch, h->plane);
+        break;
+    case LBM_PREC_FP16:
+        init_kernel<__half><<<grid, block, 0, h->stream>>>(du, dv, uu, (__half *)h->fbuf[0], (float *)h->d_fields[0],
+                                                           h->nx, h->ny, h->pitch, h->plane);
+        break;
+    case LBM_PREC_BF16:
+        init_kernel<__nv_bfloat16><<<grid, block, 0, h->stream>>>(du, dv, uu, (__nv_bfloat16 *)h->fbuf[0],
+                                                                  (float *)h->d_fields[0], h->nx, h->ny, h->pitch,
+                                                                  h->plane);
+        break;
     }
     h->launches += 1;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;

@@ -659,17 +659,14 @@ int lbm_init(lbm_t *h, const double *du, const double *dv)
     const int nx = h->nx, ny = h->ny;
     const size_t nn = (size_t)nx * ny;
     // initial f = feq(rho=1, u=UU(+du), v=0(+dv)) with single-precision weights
-    // (solution.f90:33-59), kept as FP64 deviations f - w
-    std::vector<double> g(nn * 9);
-    std::vector<double> fu(nn), fv(nn);
-    for (size_t q = 0; q < nn; ++q) {
-        double u = h->p.uu, v = 0.0;
+    // (solution.f90:33-59), built on the device from the perturbation
+    // (launch_init_lattice); the host builds only the edge constants
+    auto uv = [&](size_t q, double &u, double &v) {
+        u = h->p.uu;
+        v = 0.0;
         if (du) u = u + du[q];
         if (dv) v = v + dv[q];
-        fu[q] = u;
-        fv[q] = v;
-        for (int k = 0; k < 9; ++k) g[(size_t)k * nn + q] = feq(1.0, u, v, k) - kWref[k];
-    }
+    };
     // edge constants: moments of the edge f0 (physical_variables on the
     // edge, solution.f90:516-520) and the corner-column f0 populations
     const size_t cs = compute_size(h->prec);
@@ -678,9 +675,11 @@ int lbm_init(lbm_t *h, const double *du, const double *dv)
         const int i = side == 0 ? 0 : nx - 1;
         for (int j = 0; j < ny; ++j) {
             const size_t q = (size_t)j * nx + i;
+            double u, v;
+            uv(q, u, v);
             double temprho = 0.0, tempu = 0.0, tempv = 0.0;
             for (int k = 0; k < 9; ++k) {
-                const double f = feq(1.0, fu[q], fv[q], k);
+                const double f = feq(1.0, u, v, k);
                 temprho = temprho + f;
                 tempu = tempu + (double)kEx[k] * f;
                 tempv = tempv + (double)kEy[k] * f;
@@ -692,32 +691,27 @@ int lbm_init(lbm_t *h, const double *du, const double *dv)
         }
     }
     const int ci[4] = {0, 0, nx - 1, nx - 1}, cj[4] = {1, ny - 2, 1, ny - 2};
-    for (int c = 0; c < 4; ++c)
-        for (int k = 0; k < 9; ++k) ec[6 * (size_t)ny + 9 * c + k] = g[(size_t)k * nn + (size_t)cj[c] * nx + ci[c]];
+    for (int c = 0; c < 4; ++c) {
+        double u, v;
+        uv((size_t)cj[c] * nx + ci[c], u, v);
+        for (int k = 0; k < 9; ++k) ec[6 * (size_t)ny + 9 * c + k] = feq(1.0, u, v, k) - kWref[k];
+    }
     if (cs == sizeof(double)) {
         CK(cudaMemcpyAsync(h->edge_c, ec.data(), sizeof(double) * ec.size(), cudaMemcpyHostToDevice, h->stream), "copy edge");
     } else {
         std::vector<float> ef(ec.begin(), ec.end());
         CK(cudaMemcpyAsync(h->edge_c, ef.data(), sizeof(float) * ef.size(), cudaMemcpyHostToDevice, h->stream), "copy edge");
+        CK(cudaStreamSynchronize(h->stream), "sync edge");
     }
-    // populations
-    if (!h->d_stage) CK(dmalloc(h, &h->d_stage, sizeof(double) * nn * 9), "alloc stage");
-    for (size_t q = 0; q < nn * 9; ++q) g[q] += kWref[q / nn];   // back to f for the pack kernel
-    CK(cudaMemcpyAsync(h->d_stage, g.data(), sizeof(double) * nn * 9, cudaMemcpyHostToDevice, h->stream), "copy f");
-    if (launch_pack(h, h->d_stage, h->fbuf[0])) return cuda_err(h, cudaGetLastError(), "pack");
+    // populations and the initial fields (rho = 1, u, v) in slot 0: u0 of the first step
+    double *ddu = nullptr, *ddv = nullptr;
+    if (du || dv) {
+        if (!h->d_stage) CK(dmalloc(h, &h->d_stage, sizeof(double) * nn * 2), "alloc stage");
+        if (du) CK(cudaMemcpyAsync(ddu = h->d_stage, du, sizeof(double) * nn, cudaMemcpyHostToDevice, h->stream), "copy du");
+        if (dv) CK(cudaMemcpyAsync(ddv = h->d_stage + nn, dv, sizeof(double) * nn, cudaMemcpyHostToDevice, h->stream), "copy dv");
+    }
+    if (launch_init_lattice(h, ddu, ddv)) return cuda_err(h, cudaGetLastError(), "init");
     h->cur = 0;
-    // initial fields (rho = 1, u, v) in slot 0: u0 of the first step
-    {
-        std::vector<double> fl(3 * nn);
-        for (size_t q = 0; q < nn; ++q) { fl[q] = 1.0; fl[nn + q] = fu[q]; fl[2 * nn + q] = fv[q]; }
-        if (cs == sizeof(double)) {
-            CK(cudaMemcpyAsync(h->d_fields[0], fl.data(), sizeof(double) * 3 * nn, cudaMemcpyHostToDevice, h->stream), "copy fields");
-        } else {
-            std::vector<float> ff(fl.begin(), fl.end());
-            CK(cudaMemcpyAsync(h->d_fields[0], ff.data(), sizeof(float) * 3 * nn, cudaMemcpyHostToDevice, h->stream), "copy fields");
-            CK(cudaStreamSynchronize(h->stream), "sync fields");
-        }
-    }
     h->fields_slot = 0;
     h->fields_step[0] = 0;
     h->fields_step[1] = -1;

@@ -223,4 +223,7 @@ int ib_tile_ints();   // ints per patch tile of the tile lists
 int launch_residual(lbm_handle *h, const void *fa, const void *fb, double *out2);
 int launch_unpack(lbm_handle *h, const void *fsrc, double *dst);   // deviation -> f (FP64)
 int launch_pack(lbm_handle *h, const double *src, void *fdst);     // f (FP64) -> deviation
+// initial populations and fields (slot 0) of lbm_init from the device copies
+// of the perturbation (nullable)
+int launch_init_lattice(lbm_handle *h, const double *du, const double *dv);
 int launch_fields_to_double(lbm_handle *h, const void *fields, double *rho, double *u, double *v);
