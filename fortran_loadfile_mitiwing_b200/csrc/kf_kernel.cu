@@ -13,6 +13,9 @@
 // Edge nodes recompute the moments of the one or two interior neighbours
 // their formula needs (O(perimeter) extra reads) so that no second launch and
 // no side buffer is needed for the boundary condition.
+#include <cstring>
+#include <vector>
+
 #include "lbm_internal.h"
 #include "lbm_node.cuh"
 
@@ -158,7 +161,7 @@ constexpr int TW = 256;        // strip width (threads per CTA)
 #define LBM_KF_STAGES 4
 #endif
 #ifndef LBM_KF_MINB
-#define LBM_KF_MINB 3
+#define LBM_KF_MINB 4
 #endif
 // pipeline stages: 2-byte storage halves the bytes of a stage, so it keeps
 // twice the stages to hold the same bytes in flight
@@ -167,6 +170,9 @@ template <typename T> __host__ __device__ constexpr int tma_stages() { return si
 // each SM for the immersed-boundary kernels that run beside the lattice
 // update; four make the lattice kernel alone ~2% faster but starve them.
 constexpr int KF_MINB = LBM_KF_MINB;
+// CTAs per SM the staged kernel is compiled for: FP64 storage keeps 3 (its
+// ring alone, ~75 KB a CTA, allows no more), the others LBM_KF_MINB
+template <typename T> constexpr int kf_minb() { return sizeof(T) == 8 ? 3 : KF_MINB; }
 
 // mbarrier and bulk-copy helpers: lbm_common.cuh
 
@@ -274,17 +280,21 @@ __device__ __forceinline__ void kf_tma_cta(const KFArgs<C> &a, int bx, int by, i
     }
 }
 
+// The arguments are read from global memory (the handle's table of argument
+// variants, kf_table_entry): loaded where used rather than held in registers
+// as kernel parameters would be, which keeps the kernel within the 64
+// registers of 4 CTAs per SM.
 template <typename T, typename C, bool FIELDS, bool CONS0>
-__global__ void __launch_bounds__(TW, KF_MINB) kf_tma(const KFArgs<C> a)
+__global__ void __launch_bounds__(TW, kf_minb<T>()) kf_tma(const KFArgs<C> *__restrict__ a)
 {
     extern __shared__ __align__(128) unsigned char smraw[];
-    kf_tma_cta<T, C, FIELDS, CONS0>(a, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, smraw);
+    kf_tma_cta<T, C, FIELDS, CONS0>(*a, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, smraw);
 }
 
 // Several lattices (a batch of cases) in one launch: CTA b runs entry b of
 // the case table, {case, strip, row chunk, strips | row chunks << 16}.
 template <typename T, typename C, bool FIELDS, bool CONS0>
-__global__ void __launch_bounds__(TW, KF_MINB) kf_tma_multi(const KFArgs<C> *cases, const int4 *table)
+__global__ void __launch_bounds__(TW, kf_minb<T>()) kf_tma_multi(const KFArgs<C> *cases, const int4 *table)
 {
     extern __shared__ __align__(128) unsigned char smraw[];
     const int4 t = table[blockIdx.x];
@@ -295,23 +305,71 @@ __global__ void __launch_bounds__(TW, KF_MINB) kf_tma_multi(const KFArgs<C> *cas
 template <typename C> bool cons0(const KFArgs<C> &a) { return a.s[0] == C(0) && a.s[3] == C(0) && a.s[5] == C(0); }
 
 template <typename T, typename C, bool FIELDS>
-void launch_tma_f(const KFArgs<C> &a, dim3 grid, dim3 block, size_t smem, cudaStream_t st)
+void launch_tma_f(const KFArgs<C> &a, const KFArgs<C> *da, dim3 grid, dim3 block, size_t smem, cudaStream_t st)
 {
     if (cons0(a))
-        kf_tma<T, C, FIELDS, true><<<grid, block, smem, st>>>(a);
+        kf_tma<T, C, FIELDS, true><<<grid, block, smem, st>>>(da);
     else
-        kf_tma<T, C, FIELDS, false><<<grid, block, smem, st>>>(a);
+        kf_tma<T, C, FIELDS, false><<<grid, block, smem, st>>>(da);
 }
 
+// a: the launch's arguments on the host; da: the same in device memory
 template <typename T, typename C>
-void launch_tma(const KFArgs<C> &a, bool fields, int nx, int ny, cudaStream_t st)
+void launch_tma(const KFArgs<C> &a, const KFArgs<C> *da, bool fields, int nx, int ny, cudaStream_t st)
 {
     dim3 block(TW, 1), grid((nx + TW - 1) / TW, (ny - 2 + a.rows_per_cta - 1) / a.rows_per_cta + 1);
     const size_t smem = tma_smem<T>();
     if (fields)
-        launch_tma_f<T, C, true>(a, grid, block, smem, st);
+        launch_tma_f<T, C, true>(a, da, grid, block, smem, st);
     else
-        launch_tma_f<T, C, false>(a, grid, block, smem, st);
+        launch_tma_f<T, C, false>(a, da, grid, block, smem, st);
+}
+
+// The handle's table of lattice-argument variants in device memory: the
+// populations' current buffer (2) x the fields written (none, slot 0, slot 1)
+// x the step's slot (patch rectangle and tile lists, LBM_NSLOT_MAX) x the
+// mode (KF_ALL, KF_OUTER), KF_ARGS_STRIDE bytes each. Built when first
+// needed and again after the immersed-boundary scratch or the rows per CTA
+// change.
+template <typename C>
+int kf_table_build(lbm_handle *h)
+{
+    static_assert(sizeof(KFArgs<C>) <= KF_ARGS_STRIDE, "KFArgs larger than its table stride");
+    if (h->fstream) cudaStreamSynchronize(h->fstream);
+    if (h->side) cudaStreamSynchronize(h->side);
+    cudaStreamSynchronize(h->stream);   // no queued launch still reads the table
+    std::vector<unsigned char> host((size_t)KF_TABLE_ENTRIES * KF_ARGS_STRIDE, 0);
+    const int saved = h->pinfo_slot;
+    for (int cur = 0; cur < 2; ++cur)
+        for (int fsel = 0; fsel < 3; ++fsel)
+            for (int q = 0; q < LBM_NSLOT_MAX; ++q)
+                for (int mode = 0; mode < 2; ++mode) {
+                    h->pinfo_slot = q;
+                    const KFArgs<C> a = make_kf_args<C>(h, h->fbuf[cur], h->fbuf[cur ^ 1],
+                                                        fsel ? h->d_fields[fsel - 1] : nullptr, mode);
+                    const size_t e = ((size_t)((cur * 3 + fsel) * LBM_NSLOT_MAX + q) * 2 + mode);
+                    memcpy(host.data() + e * KF_ARGS_STRIDE, &a, sizeof a);
+                }
+    h->pinfo_slot = saved;
+    if (cudaMemcpy(h->d_kftab, host.data(), host.size(), cudaMemcpyHostToDevice) != cudaSuccess) return -1;
+    h->kftab_rows = h->kf_rows;
+    h->kftab_ok = 1;
+    return 0;
+}
+
+// the table entry of a launch; null if the launch is not one of the variants
+template <typename C>
+const KFArgs<C> *kf_table_entry(lbm_handle *h, const void *fin, void *fout, void *fields, int mode)
+{
+    if (!h->d_kftab) return nullptr;
+    if ((!h->kftab_ok || h->kftab_rows != h->kf_rows) && kf_table_build<C>(h)) return nullptr;
+    const int cur = fin == h->fbuf[0] ? 0 : (fin == h->fbuf[1] ? 1 : -1);
+    const int fsel = !fields ? 0 : (fields == h->d_fields[0] ? 1 : (fields == h->d_fields[1] ? 2 : -1));
+    if (cur < 0 || fsel < 0 || fout != h->fbuf[cur ^ 1] || h->pinfo_slot < 0 || h->pinfo_slot >= LBM_NSLOT_MAX ||
+        (mode != KF_ALL && mode != KF_OUTER))
+        return nullptr;
+    const size_t e = ((size_t)((cur * 3 + fsel) * LBM_NSLOT_MAX + h->pinfo_slot) * 2 + mode);
+    return (const KFArgs<C> *)((const unsigned char *)h->d_kftab + e * KF_ARGS_STRIDE);
 }
 
 template <typename T, typename C, bool FIELDS, bool CONS0>
@@ -368,7 +426,9 @@ int launch_kf_t(lbm_handle *h, const void *fin, void *fout, void *fields, int mo
             if (configure_tma<T, C>()) return -1;
             configured = true;
         }
-        launch_tma<T, C>(a, fields != nullptr, h->nx, h->ny, st);
+        const KFArgs<C> *da = kf_table_entry<C>(h, fin, fout, fields, mode);
+        if (!da) return -1;
+        launch_tma<T, C>(a, da, fields != nullptr, h->nx, h->ny, st);
     } else if (mode == KF_ALL && vec == 4 && h->pitch % 4 == 0) {
         launch_vec<T, C, 4>(a, fields != nullptr, h->nx, h->ny, st);
     } else if (mode == KF_ALL && vec == 2 && h->pitch % 2 == 0) {

@@ -148,6 +148,7 @@ void free_ib(lbm_handle *h)
     if (h->side) cudaStreamSynchronize(h->side);
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->ib_ready = 0;
+    h->kftab_ok = 0;   // the lattice arguments point into the scratch
     h->batch_in_half[0] = h->batch_in_half[1] = -1;
     free_devp(h->d_mk); free_devp(h->d_rhs); free_devp(h->d_B); free_devp(h->d_y); free_devp(h->d_partial);
     free_devp(h->d_bD); free_devp(h->d_bL); free_devp(h->d_gf); free_devp(h->d_fmode); free_devp(h->d_fstatus); free_devp(h->d_tiles); free_devp(h->d_nsup); free_devp(h->d_ctile);
@@ -546,6 +547,8 @@ int lbm_create(const lbm_params *p, lbm_t **out)
     if ((e = dmalloc(h, &h->d_counter, sizeof(unsigned))) != cudaSuccess) return fail(e, "alloc counter");
     if ((e = dmalloc(h, &h->d_pinfo, LBM_NSLOT_MAX * sizeof(PatchInfo))) != cudaSuccess) return fail(e, "alloc pinfo");
     if ((e = dmalloc(h, &h->d_red, sizeof(double) * 2 * 296)) != cudaSuccess) return fail(e, "alloc red");
+    if ((e = dmalloc(h, &h->d_kftab, (size_t)KF_TABLE_ENTRIES * KF_ARGS_STRIDE)) != cudaSuccess)
+        return fail(e, "alloc lattice arguments");
     if ((e = dmalloc(h, &h->d_solve_res, 2 * sizeof(double))) != cudaSuccess) return fail(e, "alloc res");
     if ((e = dmalloc(h, &h->d_ring, sizeof(double) * h->row_len * (size_t)h->ring_cap)) != cudaSuccess)
         return fail(e, "alloc ring");
@@ -573,6 +576,7 @@ int lbm_destroy(lbm_t *h)
     free_ib(h);
     free_devp(h->d_pinfo); free_devp(h->d_counter);
     free_devp(h->d_ring); free_devp(h->d_status); free_devp(h->d_solve_res); free_devp(h->d_red);
+    free_dev(h->d_kftab);
     free_devp(h->d_stage);
     if (h->side) cudaStreamSynchronize(h->side);
     if (h->fstream) cudaStreamSynchronize(h->fstream);
