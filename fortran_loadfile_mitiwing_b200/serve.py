@@ -201,10 +201,11 @@ class Server:
     budget_bytes: device memory the cases may hold together; tick_steps: steps
     between admissions; keep_handles: results carry the finished case's handle
     (open; the caller closes it) instead of closing it; workers: threads that
-    prepare admitted cases (0: prepared in `tick`)."""
+    prepare admitted cases (0: prepared in `tick`; 2 measured best: the
+    preparation of cases arriving together keeps pace with the batch)."""
 
     def __init__(self, budget_bytes, tick_steps=100, lib=None, max_cases=256, keep_handles=False,
-                 clock=time.perf_counter, workers=1):
+                 clock=time.perf_counter, workers=2):
         self.adm = Admission(budget_bytes, max_cases)
         self.tick_steps = tick_steps
         self.lib = lib
@@ -316,7 +317,7 @@ def poisson_arrivals(rate, n, seed=0):
 
 
 def serve_stream(specs, rate, periods=3.0, budget_bytes=150e9, precision="fp16", tick_steps=100, seed=1, lib=None,
-                 keep_rows=()):
+                 keep_rows=(), workers=2):
     """Serves `specs` (sweep.sweep_specs items, `periods` flapping periods
     each) arriving as a Poisson stream of `rate` requests/s in real time;
     returns the results (force rows kept for the request ids in keep_rows,
@@ -328,7 +329,7 @@ def serve_stream(specs, rate, periods=3.0, budget_bytes=150e9, precision="fp16",
         n = int(math.ceil(periods * sp["period_steps"]))
         est = estimate_device_bytes(sweep.case_of(sp, n, precision, amp=0.0))
         reqs.append(Request(i, lambda sp=sp, n=n: sweep.case_of(sp, n, precision), float(arrivals[i]), est))
-    srv = Server(budget_bytes, tick_steps=tick_steps, lib=lib)
+    srv = Server(budget_bytes, tick_steps=tick_steps, lib=lib, workers=workers)
     try:
         t0 = srv.clock()
         for r in reqs:
@@ -428,12 +429,13 @@ def main():
     ap.add_argument("--tick-steps", type=int, default=100)
     ap.add_argument("--precision", default="fp16")
     ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--workers", type=int, default=2, help="threads preparing admitted cases")
     ap.add_argument("--check", type=int, default=8,
                     help="requests of the first stream whose coefficients are checked against FP64 storage")
     args = ap.parse_args()
     specs = sweep.sweep_specs(args.requests, args.seed)
     out = {"requests": args.requests, "periods": args.periods, "budget_gb": args.budget_gb,
-           "precision": args.precision, "tick_steps": args.tick_steps,
+           "precision": args.precision, "tick_steps": args.tick_steps, "workers": args.workers,
            "case_distribution": "sweep_specs(seed): Nx in [512, 2048], Ny = Nx/2, chord = Ny/4",
            "served": [], "fp32_one_at_a_time": []}
     service = alone_service_times(specs, args.periods)
@@ -441,7 +443,7 @@ def main():
     for k, rate in enumerate(args.rates):
         keep = set(range(args.check)) if k == 0 else set()
         res, summ = serve_stream(specs, rate, args.periods, args.budget_gb * 1e9, args.precision, args.tick_steps,
-                                 seed=args.seed + k, keep_rows=keep)
+                                 seed=args.seed + k, keep_rows=keep, workers=args.workers)
         if keep:
             ref = fp64_reference_rows(specs[:args.check], args.periods)
             errs = [period_errors(res[i].rows, ref[i], specs[i]["period_steps"], args.periods) for i in sorted(keep)]
