@@ -178,6 +178,14 @@ class Admission:
     def recharge(self, rid, nbytes):
         self.charged[rid] = int(nbytes)
 
+    def withdraw(self, rid):
+        """Takes a waiting request out of the queue; True if it was there."""
+        for k, (r, _) in enumerate(self.queue):
+            if r == rid:
+                del self.queue[k]
+                return True
+        return False
+
     def release(self, rid):
         self.charged.pop(rid, None)
 
@@ -255,6 +263,38 @@ class Server:
 
     def idle(self):
         return not self.live and not self.preparing and not self.adm.queue
+
+    def cancel(self, rid):
+        """Cancels a request wherever it is: waiting (it leaves the queue),
+        being prepared (its case is closed when ready) or running (it leaves
+        the batch between ticks). Its memory is released and a Result with
+        error (LBM_ERR_STATE, "cancelled") and the rows computed so far is
+        returned, or None for an unknown or finished request."""
+        req = self.requests.get(rid)
+        if req is None:
+            return None
+        t = self.clock()
+        if self.adm.withdraw(rid):
+            self.requests.pop(rid)
+            res = Result(rid, np.zeros((0, 0)), req.arrival, None, None, t, None, (-2, "cancelled"))
+        elif rid in self.preparing:
+            fut, admitted = self.preparing.pop(rid)
+            fut.result()[0].close()
+            self.adm.release(rid)
+            self.requests.pop(rid)
+            res = Result(rid, np.zeros((0, 0)), req.arrival, admitted, None, t, None, (-2, "cancelled"))
+        elif rid in self.live:
+            h, chunks, admitted, started, _ = self.live.pop(rid)
+            self.batch.remove(h)
+            self.adm.release(rid)
+            self.requests.pop(rid)
+            rows_all = np.concatenate(chunks) if chunks else np.zeros((0, h.row_len))
+            h.close()
+            res = Result(rid, rows_all, req.arrival, admitted, started, t, None, (-2, "cancelled"))
+        else:
+            return None
+        self.done.append(res)
+        return res
 
     def tick(self, wait_for_ready=False):
         """Admits what fits, joins the prepared cases, steps the batch once;

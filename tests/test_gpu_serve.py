@@ -55,3 +55,25 @@ def test_served_results_equal_alone(gpu_lib, workers):
                 np.testing.assert_array_equal(r.handle.populations(), a.populations(),
                                               err_msg=f"request {r.rid} populations")
             r.handle.close()
+
+
+def test_cancelled_request_leaves_the_others_exact(gpu_lib):
+    lens = [30, 40, 26]
+    reqs = [Request(i, make(i, n)) for i, n in enumerate(lens)]
+    with Server(10 ** 10, tick_steps=6, lib=gpu_lib, keep_handles=True, workers=0) as srv:
+        for r in reqs:
+            srv.submit(r)
+        srv.tick(wait_for_ready=True)
+        srv.tick(wait_for_ready=True)
+        cancelled = srv.cancel(1)                 # running: leaves the batch after 12 steps
+        assert cancelled.error[1] == "cancelled" and cancelled.steps == 12
+        while not srv.idle():
+            srv.tick(wait_for_ready=True)
+        res = {r.rid: r for r in srv.done}
+        for rid in (0, 2):
+            with Lbm.from_case(make(rid, lens[rid])(), gpu_lib) as a:
+                np.testing.assert_array_equal(res[rid].rows, a.run(200))
+                np.testing.assert_array_equal(res[rid].handle.populations(), a.populations())
+            res[rid].handle.close()
+        with Lbm.from_case(make(1, lens[1])(), gpu_lib) as a:
+            np.testing.assert_array_equal(cancelled.rows, a.run(12))

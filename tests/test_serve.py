@@ -202,3 +202,38 @@ def test_server_returns_a_failed_case_and_serves_the_rest(monkeypatch):
     assert res[0].error is None and res[0].steps == 30
     assert res[2].error is None and res[2].steps == 20
     assert sorted(_FakeCase.closed) == [0, 1, 2]
+
+
+def test_cancel_waiting_preparing_and_running(monkeypatch):
+    from fortran_loadfile_mitiwing_b200 import serve
+
+    class _Params:
+        scale, uu = 1.0, 1.0
+
+    class _Spec(dict):
+        pass
+
+    def make(rid, last):
+        c = _Spec(rid=rid, last=last, bytes=40)
+        c.params = _Params()
+        c.table = np.array([[float(last - 1)]])
+        return lambda: c
+
+    monkeypatch.setattr(serve, "Lbm", _FakeCase)
+    monkeypatch.setattr(serve, "Batch", _FakeBatch)
+    _FakeCase.closed = []
+    with serve.Server(budget_bytes=100, tick_steps=4, workers=0) as srv:
+        for rid, last in enumerate([30, 30, 30, 30]):
+            srv.submit(serve.Request(rid, make(rid, last), estimate=45))
+        srv.tick(wait_for_ready=True)          # 0 and 1 run; 2 and 3 wait
+        r3 = srv.cancel(3)                     # waiting
+        assert r3.error == (-2, "cancelled") and 3 not in [q for q, _ in srv.adm.queue]
+        r1 = srv.cancel(1)                     # running: leaves the batch with its rows so far
+        assert r1.error == (-2, "cancelled") and r1.steps == 4 and 1 not in srv.live
+        assert srv.cancel(1) is None and srv.cancel(99) is None
+        while not srv.idle():
+            srv.tick(wait_for_ready=True)
+        res = {r.rid: r for r in srv.done}
+    assert res[0].error is None and res[0].steps == 30
+    assert res[2].error is None and res[2].steps == 30
+    assert sorted(_FakeCase.closed) == [0, 1, 2]
