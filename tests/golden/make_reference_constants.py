@@ -1,0 +1,61 @@
+"""Extracts the constants of the lattice model from the reference's Fortran
+source into reference_constants.json, a fixture the CPU tests compare the
+oracle and the library with (the reference cannot be built here, so its
+source text is the record of these values):
+
+  matm rows        solution.f90:17-25   (the MRT transform M)
+  e(k,:), w(k)     D2Q9model.f90:5-32   (lattice order and weights, as written)
+  mesh%s(1..9)     ini_mesh.f90:59-67   (relaxation rates; 8 and 9 are 1/tau_f)
+
+Run here, where the reference tree is present:
+    python tests/golden/make_reference_constants.py <reference dir>
+"""
+import json
+import os
+import re
+import sys
+
+
+def read(ref, name):
+    with open(os.path.join(ref, name), encoding="utf-8", errors="replace") as fh:
+        return fh.read()
+
+
+def fnum(tok):
+    return float(tok.lower().replace("d", "e"))
+
+
+def main():
+    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    sol = read(ref, "solution.f90")
+    rows = {}
+    for m in re.finditer(r"matm\((\d)\s*,\s*:\s*\)\s*=\s*\(/([^/]*)/\)", sol):
+        rows[int(m.group(1))] = [fnum(t) for t in m.group(2).split(",")]
+    assert sorted(rows) == list(range(1, 10)), rows.keys()
+    d2q9 = read(ref, "D2Q9model.f90")
+    e = {}
+    for m in re.finditer(r"\be\((\d)\s*,\s*(\d)\)\s*=\s*(-?\d+)", d2q9):
+        e.setdefault(int(m.group(1)), [0, 0])[int(m.group(2)) - 1] = int(m.group(3))
+    w = {}
+    for m in re.finditer(r"\bw\((\d)\)\s*=\s*([0-9.]+/[0-9.]+)", d2q9):
+        w[int(m.group(1))] = m.group(2)
+    mesh = read(ref, "ini_mesh.f90")
+    s = {}
+    for m in re.finditer(r"%s\((\d)\)\s*=\s*([^\s!]+)", mesh):
+        k, v = int(m.group(1)), m.group(2)
+        s.setdefault(k, v)
+    out = {
+        "source": {"matm": "solution.f90:17-25", "e_w": "D2Q9model.f90:5-32", "s": "ini_mesh.f90:59-67"},
+        "matm": [rows[k] for k in range(1, 10)],
+        "e": [e[k] for k in range(1, 10)],
+        "w_literal": [w[k] for k in range(1, 10)],
+        "s_literal": [s[k] for k in range(1, 10)],
+    }
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_constants.json")
+    with open(path, "w") as fh:
+        json.dump(out, fh, indent=1)
+    print(path)
+
+
+if __name__ == "__main__":
+    main()

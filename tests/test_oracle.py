@@ -222,3 +222,38 @@ def test_geometry_generator_reproduces_reference_boundary_file():
     x, y = cases.naca0012(204)
     assert np.abs(x - d[:, 0]).max() < 1.5e-8
     assert np.abs(y - d[:, 1]).max() < 1.5e-8
+
+
+def _reference_constants():
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "reference_constants.json")) as fh:
+        return json.load(fh)
+
+
+def test_oracle_model_constants_equal_the_reference_source(oracle_mod):
+    """M, the lattice order and the weights as the reference's source writes
+    them (tests/golden/make_reference_constants.py extracted them)."""
+    ref = _reference_constants()
+    m, _ = oracle_mod.mrt_matrices()
+    np.testing.assert_array_equal(m, np.array(ref["matm"]))
+    e, w = oracle_mod.lattice()
+    assert e.tolist() == ref["e"]
+    for k, lit in enumerate(ref["w_literal"]):
+        # a default-REAL quotient (no d0 exponent): evaluated in single precision
+        num, den = (float(x) for x in lit.split("/"))
+        assert "d" not in lit.lower()
+        assert w[k] == float(np.float32(num) / np.float32(den))
+
+
+def test_default_rates_equal_the_reference_source():
+    """lbm_default_params carries the reference's s(1..7); s(8), s(9) are
+    1/tau_f there and <= 0 here, meaning 'from the viscosity'."""
+    import ctypes as C
+    from fortran_loadfile_mitiwing_b200 import LbmParams, load_library
+    ref = _reference_constants()
+    p = LbmParams()
+    assert load_library().lbm_default_params(C.byref(p)) == 0
+    for k in range(7):
+        assert p.s[k] == float(ref["s_literal"][k].lower().replace("d", "e"))
+    assert all("tau_f" in ref["s_literal"][k] for k in (7, 8)) and p.s[7] <= 0 and p.s[8] <= 0
