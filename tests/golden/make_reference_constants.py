@@ -44,8 +44,43 @@ def main():
     for m in re.finditer(r"%s\((\d)\)\s*=\s*([^\s!]+)", mesh):
         k, v = int(m.group(1)), m.group(2)
         s.setdefault(k, v)
+    # the discrete delta kernels: the x-axis branches of each smooth variant in
+    # the first kernel block of immersed_boundary_Wu, verbatim (condition,
+    # expression)
+    bc = read(ref, "boundary_condition.f90").splitlines()
+    sub = next(i for i, l in enumerate(bc) if re.match(r"(?i)\s*subroutine\s+immersed_boundary_Wu", l))
+    i0 = next(i for i in range(sub, len(bc)) if bc[i].strip().lower().startswith("if(smooth.eq.0)"))
+
+    def block(first):
+        a = next(i for i in range(first, len(bc)) if "disr=abs((x0" in bc[i].replace(" ", ""))
+        b = next(i for i in range(a + 1, len(bc)) if "disr=abs((y0" in bc[i].replace(" ", ""))
+        out, cond = [], None
+        for line in bc[a + 1:b]:
+            t = line.strip()
+            m = re.match(r"(?i)(?:else\s*)?if\s*\((.*)\)\s*then$", t)
+            if m:
+                cond = m.group(1)
+            elif t.lower() == "else":
+                cond = "else"
+            m = re.match(r"kernel1\s*=\s*(.*)$", t)
+            if m:
+                out.append([cond, m.group(1)])
+        return out, b
+
+    kern0, end0 = block(i0)
+    kern1, _ = block(end0 + 1)
+    kern = {0: kern0, 1: kern1}
+    pai = None
+    for name in ("main.f90", "mode.f90", "solution.f90"):
+        m = re.search(r"pai\s*=\s*([0-9.d+-]+)", read(ref, name))
+        if m:
+            pai = m.group(1)
+            break
     out = {
-        "source": {"matm": "solution.f90:17-25", "e_w": "D2Q9model.f90:5-32", "s": "ini_mesh.f90:59-67"},
+        "source": {"matm": "solution.f90:17-25", "e_w": "D2Q9model.f90:5-32", "s": "ini_mesh.f90:59-67",
+                   "kernels": "boundary_condition.f90, first kernel1 block of immersed_boundary_Wu"},
+        "kernel_branches": {"0": kern[0], "1": kern[1]},
+        "pai_literal": pai,
         "matm": [rows[k] for k in range(1, 10)],
         "e": [e[k] for k in range(1, 10)],
         "w_literal": [w[k] for k in range(1, 10)],

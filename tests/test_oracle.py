@@ -257,3 +257,30 @@ def test_default_rates_equal_the_reference_source():
     for k in range(7):
         assert p.s[k] == float(ref["s_literal"][k].lower().replace("d", "e"))
     assert all("tau_f" in ref["s_literal"][k] for k in (7, 8)) and p.s[7] <= 0 and p.s[8] <= 0
+
+
+def _fortran_to_python(expr):
+    import re
+    expr = re.sub(r"(\d+\.\d*)[dD]([+-]?\d+)", r"\1e\2", expr)
+    for a, b in ((".lt.", " < "), (".le.", " <= "), (".gt.", " > "), (".ge.", " >= "), (".and.", " and "),
+                 (".or.", " or ")):
+        expr = expr.replace(a, b).replace(a.upper(), b)
+    return expr
+
+
+@pytest.mark.parametrize("smooth", [0, 1])
+def test_oracle_delta_kernels_equal_the_reference_source(oracle_mod, smooth):
+    """The oracle's one-axis kernels against the reference's branch formulas,
+    evaluated as written (tests/golden/reference_constants.json), over a grid
+    of distances that includes every branch boundary."""
+    ref = _reference_constants()
+    env = {"abs": abs, "sqrt": math.sqrt, "asin": math.asin,
+           "pai": float(_fortran_to_python(ref["pai_literal"]))}
+    branches = [(None if c == "else" else _fortran_to_python(c), _fortran_to_python(e))
+                for c, e in ref["kernel_branches"][str(smooth)]]
+    rs = sorted(set(np.round(np.linspace(0.0, 3.0, 601), 12).tolist() + [0.5, 1.0, 1.5, 2.0, 2.5]))
+    for r in rs:
+        env["disr"] = r
+        want = next(eval(e, env) for c, e in branches if c is None or eval(c, env))
+        got = oracle_mod.delta(r, smooth)
+        assert abs(got - want) <= 1e-15 * max(1.0, abs(want)), (smooth, r, got, want)
