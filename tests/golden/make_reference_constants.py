@@ -6,6 +6,8 @@ source text is the record of these values):
   matm rows        solution.f90:17-25   (the MRT transform M)
   e(k,:), w(k)     D2Q9model.f90:5-32   (lattice order and weights, as written)
   mesh%s(1..9)     ini_mesh.f90:59-67   (relaxation rates; 8 and 9 are 1/tau_f)
+  kernel branches  boundary_condition.f90 (immersed_boundary_Wu's first kernel block)
+  D2Q9feq          D2Q9model.f90:35-46  (the equilibrium)
 
 Run here, where the reference tree is present:
     python tests/golden/make_reference_constants.py <reference dir>
@@ -70,6 +72,13 @@ def main():
     kern0, end0 = block(i0)
     kern1, _ = block(end0 + 1)
     kern = {0: kern0, 1: kern1}
+    # the equilibrium D2Q9feq (D2Q9model.f90:35-46), its three assignments verbatim
+    body = d2q9[d2q9.lower().index("function d2q9feq"):]
+    body = body[:body.lower().index("end function")]
+    feq = {}
+    for name in ("eu", "utwo", "D2Q9feq"):
+        m = re.search(r"(?im)^\s*" + name + r"\s*=\s*(.*)$", body)
+        feq[name] = m.group(1).strip()
     pai = None
     for name in ("main.f90", "mode.f90", "solution.f90"):
         m = re.search(r"pai\s*=\s*([0-9.d+-]+)", read(ref, name))
@@ -80,6 +89,7 @@ def main():
         "source": {"matm": "solution.f90:17-25", "e_w": "D2Q9model.f90:5-32", "s": "ini_mesh.f90:59-67",
                    "kernels": "boundary_condition.f90, first kernel1 block of immersed_boundary_Wu"},
         "kernel_branches": {"0": kern[0], "1": kern[1]},
+        "feq": feq,
         "pai_literal": pai,
         "matm": [rows[k] for k in range(1, 10)],
         "e": [e[k] for k in range(1, 10)],

@@ -284,3 +284,29 @@ def test_oracle_delta_kernels_equal_the_reference_source(oracle_mod, smooth):
         want = next(eval(e, env) for c, e in branches if c is None or eval(c, env))
         got = oracle_mod.delta(r, smooth)
         assert abs(got - want) <= 1e-15 * max(1.0, abs(want)), (smooth, r, got, want)
+
+
+def test_oracle_initial_state_is_the_reference_equilibrium(oracle_mod):
+    """init's populations (solution.f90:33-59) are D2Q9feq(1, UU + du, dv) as
+    the reference source writes it, with its single-precision weights."""
+    from fortran_loadfile_mitiwing_b200 import cases
+    ref = _reference_constants()
+    case = cases.small_case(precision="fp64", n_steps=10)
+    o = oracle_mod.Oracle.from_case(case)
+    f = o.populations()
+    p = case.params
+    ny, nx = f.shape[1:]
+    du, dv = case.du.reshape(ny, nx), case.dv.reshape(ny, nx)
+    e = ref["e"]
+    w = [float(np.float32(float(a)) / np.float32(float(b))) for a, b in (x.split("/") for x in ref["w_literal"])]
+    code = {k: compile(_fortran_to_python(v), k, "eval") for k, v in ref["feq"].items()}
+    for j, i in ((0, 0), (5, 7), (ny // 2, nx // 2), (ny - 1, nx - 1), (13, 41)):
+        # Fortran's 1-based e(k,c) and w(k)
+        env = {"rh": 1.0, "u1": p.uu + du[j, i], "v1": 0.0 + dv[j, i],
+               "e": lambda a, c: e[a - 1][c - 1], "w": lambda a: w[a - 1]}
+        for k in range(9):
+            env["k"] = k + 1
+            env["eu"] = eval(code["eu"], env)
+            env["utwo"] = eval(code["utwo"], env)
+            want = eval(code["D2Q9feq"], env)
+            assert abs(f[k, j, i] - want) <= 2e-16, (k, j, i, f[k, j, i], want)
