@@ -743,41 +743,57 @@ static int immersed_boundary_wu(ora_state *h)
     return rc;
 }
 
+/* one node of colission (solution.f90:592-635): m = M f, the equilibrium
+ * moments (as temp(k) minus M w), the forcing fp(k), m' = m + (meq - m) s +
+ * fp, f' = M^-1 m' */
+static void collide_node(const double matm[Q][Q], const double inv[Q][Q], const double s[Q], const double f[Q], double rt,
+                         double ut, double vt, double gfx, double gfy, double out[Q])
+{
+    double temp[Q], temp1[Q], fp[Q];
+    for (int k = 0; k < Q; ++k) temp[k] = f[k];
+    matmulvoc(temp1, matm, temp);
+    temp[0] = 0.0;
+    temp[1] = -2.0 * rt + 3.0 * (rt * ut * rt * ut + rt * vt * rt * vt);
+    temp[2] = rt - 3.0 * (rt * ut * rt * ut + rt * vt * rt * vt);
+    temp[3] = 0.0;
+    temp[4] = -rt * ut;
+    temp[5] = 0.0;
+    temp[6] = -rt * vt;
+    temp[7] = (rt * ut * rt * ut - rt * vt * rt * vt);
+    temp[8] = (rt * ut * rt * vt);
+    fp[0] = 0.0;                                                   /* mesh%layer == 1 */
+    fp[1] = 6.0 * (1.0 - 0.5 * s[1]) * (ut * gfx + vt * gfy);
+    fp[2] = -6.0 * (1.0 - 0.5 * s[2]) * (ut * gfx + vt * gfy);
+    fp[3] = gfx;
+    fp[4] = -(1.0 - 0.5 * s[4]) * gfx;
+    fp[5] = gfy;
+    fp[6] = -(1.0 - 0.5 * s[6]) * gfy;
+    fp[7] = 2.0 * (1.0 - 0.5 * s[7]) * (ut * gfx - vt * gfy);
+    fp[8] = (1.0 - 0.5 * s[8]) * (ut * gfy + vt * gfx);
+    for (int k = 0; k < Q; ++k) temp[k] = temp1[k] + (temp[k] - temp1[k]) * s[k] + fp[k];
+    matmulvoc(out, inv, temp);
+}
+
+/* the same update for one node's values, for tests against the reference's
+ * source text */
+void ora_collide_node(const ora_state *h, const double f[Q], double rho, double u, double v, double gfx, double gfy,
+                      double out[Q])
+{
+    collide_node(h->matm, h->inv, h->s, f, rho, u, v, gfx, gfy, out);
+}
+
 /* colission (solution.f90:573-643): interior nodes */
 static void colission(ora_state *h)
 {
     const int nx = h->nx, ny = h->ny;
-    const double *s = h->s;
 #pragma omp parallel for schedule(static)
     for (int j = 2; j <= ny - 1; ++j)
         for (int i = 2; i <= nx - 1; ++i) {
             size_t q = IDX(h, i, j);
-            double temp[Q], temp1[Q], fp[Q];
-            for (int k = 1; k <= Q; ++k) temp[k - 1] = FQ(h, h->f, i, j, k);
-            matmulvoc(temp1, h->matm, temp);
-            double ut = h->u[q], vt = h->v[q], rt = h->rho[q];
-            temp[0] = 0.0;
-            temp[1] = -2.0 * rt + 3.0 * (rt * ut * rt * ut + rt * vt * rt * vt);
-            temp[2] = rt - 3.0 * (rt * ut * rt * ut + rt * vt * rt * vt);
-            temp[3] = 0.0;
-            temp[4] = -rt * ut;
-            temp[5] = 0.0;
-            temp[6] = -rt * vt;
-            temp[7] = (rt * ut * rt * ut - rt * vt * rt * vt);
-            temp[8] = (rt * ut * rt * vt);
-            double gfx = h->gfx[q], gfy = h->gfy[q];                   /* mesh%layer == 1 */
-            fp[0] = 0.0;
-            fp[1] = 6.0 * (1.0 - 0.5 * s[1]) * (ut * gfx + vt * gfy);
-            fp[2] = -6.0 * (1.0 - 0.5 * s[2]) * (ut * gfx + vt * gfy);
-            fp[3] = gfx;
-            fp[4] = -(1.0 - 0.5 * s[4]) * gfx;
-            fp[5] = gfy;
-            fp[6] = -(1.0 - 0.5 * s[6]) * gfy;
-            fp[7] = 2.0 * (1.0 - 0.5 * s[7]) * (ut * gfx - vt * gfy);
-            fp[8] = (1.0 - 0.5 * s[8]) * (ut * gfy + vt * gfx);
-            for (int k = 0; k < Q; ++k) temp[k] = temp1[k] + (temp[k] - temp1[k]) * s[k] + fp[k];
-            matmulvoc(temp1, h->inv, temp);
-            for (int k = 1; k <= Q; ++k) FQ(h, h->f, i, j, k) = temp1[k - 1];
+            double f[Q], out[Q];
+            for (int k = 1; k <= Q; ++k) f[k - 1] = FQ(h, h->f, i, j, k);
+            collide_node(h->matm, h->inv, h->s, f, h->rho[q], h->u[q], h->v[q], h->gfx[q], h->gfy[q], out);
+            for (int k = 1; k <= Q; ++k) FQ(h, h->f, i, j, k) = out[k - 1];
         }
 }
 

@@ -44,6 +44,8 @@ const char *ora_last_error(const ora_state *h);
 void ora_mrt_matrices(double *matm, double *inv);          /* 81 each, row-major [row][col] */
 void ora_lattice(int *e, double *w);                         /* e[9][2], w[9] */
 double ora_delta(double r, int smooth);                      /* one-axis kernel value */
+void ora_collide_node(const ora_state *h, const double f[9], double rho, double u, double v, double gfx,
+                      double gfy, double out[9]);   /* one node of colission */
 int ora_motion_row(const ora_state *h, int step_index, double *row); /* step-table row */
 int ora_motion_lookup(const double *table, int rows, int cols, double t, double *row);
 void ora_set_threads(int n);

@@ -50,6 +50,7 @@ def load():
         "ora_mrt_matrices": (None, [_D, _D]),
         "ora_lattice": (None, [C.POINTER(C.c_int), _D]),
         "ora_delta": (C.c_double, [C.c_double, C.c_int]),
+        "ora_collide_node": (None, [P, _D, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, _D]),
         "ora_motion_row": (C.c_int, [P, C.c_int, _D]),
         "ora_motion_lookup": (C.c_int, [_D, C.c_int, C.c_int, C.c_double, _D]),
         "ora_set_threads": (None, [C.c_int]),
@@ -60,6 +61,16 @@ def load():
         fn.argtypes = args
     _lib = lib
     return lib
+
+
+def collide_node(oracle, f, rho, u, v, gfx=0.0, gfy=0.0):
+    """One node of the collision (solution.f90:592-635) with the oracle's
+    rates: post-collision f from f (9), rho, u, v and the force density."""
+    import numpy as np
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    out = np.zeros(9)
+    oracle.lib.ora_collide_node(oracle.h, _dptr(f), rho, u, v, gfx, gfy, _dptr(out))
+    return out
 
 
 class OracleError(RuntimeError):

@@ -8,6 +8,7 @@ source text is the record of these values):
   mesh%s(1..9)     ini_mesh.f90:59-67   (relaxation rates; 8 and 9 are 1/tau_f)
   kernel branches  boundary_condition.f90 (immersed_boundary_Wu's first kernel block)
   D2Q9feq          D2Q9model.f90:35-46  (the equilibrium)
+  colission        solution.f90:605-633 (equilibrium moments, forcing, relaxation)
 
 Run here, where the reference tree is present:
     python tests/golden/make_reference_constants.py <reference dir>
@@ -79,6 +80,16 @@ def main():
     for name in ("eu", "utwo", "D2Q9feq"):
         m = re.search(r"(?im)^\s*" + name + r"\s*=\s*(.*)$", body)
         feq[name] = m.group(1).strip()
+    # colission's per-node equilibrium moments and forcing (solution.f90:605-626), verbatim
+    col = sol[sol.lower().index("subroutine colission"):]
+    col = col[:col.lower().index("end subroutine")]
+    temp = {}
+    for m in re.finditer(r"(?m)^\s*temp\((\d)\)\s*=\s*(.*)$", col):
+        temp.setdefault(int(m.group(1)), m.group(2).strip())
+    fp = {}
+    for m in re.finditer(r"(?m)^\s*fp\((\d)\)\s*=\s*(.*)$", col):
+        fp.setdefault(int(m.group(1)), m.group(2).strip())
+    relax = re.search(r"(?m)^\s*(temp\(k\)\s*=\s*temp1\(k\).*)$", col).group(1).strip()
     pai = None
     for name in ("main.f90", "mode.f90", "solution.f90"):
         m = re.search(r"pai\s*=\s*([0-9.d+-]+)", read(ref, name))
@@ -90,6 +101,8 @@ def main():
                    "kernels": "boundary_condition.f90, first kernel1 block of immersed_boundary_Wu"},
         "kernel_branches": {"0": kern[0], "1": kern[1]},
         "feq": feq,
+        "collision": {"temp": [temp[k] for k in range(1, 10)], "fp": [fp[k] for k in range(1, 10)],
+                      "relax": relax},
         "pai_literal": pai,
         "matm": [rows[k] for k in range(1, 10)],
         "e": [e[k] for k in range(1, 10)],

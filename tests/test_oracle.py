@@ -310,3 +310,48 @@ def test_oracle_initial_state_is_the_reference_equilibrium(oracle_mod):
             env["utwo"] = eval(code["utwo"], env)
             want = eval(code["D2Q9feq"], env)
             assert abs(f[k, j, i] - want) <= 2e-16, (k, j, i, f[k, j, i], want)
+
+
+def test_oracle_collision_is_the_reference_colission(oracle_mod):
+    """One node of colission as the reference source writes it (equilibrium
+    moments temp(k), forcing fp(k), relaxation; solution.f90:592-635),
+    evaluated as written with sequential matrix-vector sums, against the
+    oracle's collision, at random node states with and without force."""
+    from fortran_loadfile_mitiwing_b200 import cases
+    import pyoracle
+    ref = _reference_constants()["collision"]
+    case = cases.small_case(precision="fp64", n_steps=10)
+    o = oracle_mod.Oracle.from_case(case)
+    m, minv = oracle_mod.mrt_matrices()
+    s_rates = [float(x) for x in o.params.s]
+    if s_rates[7] <= 0:   # 1/tau from the viscosity, as the library fills them
+        nu = o.params.uu / (o.params.re * o.params.scale)
+        s_rates[7] = s_rates[8] = 1.0 / (3.0 * nu + 0.5)
+    temp_c = [compile(_fortran_to_python(e.replace("mesh%s(", "s(")), "temp", "eval") for e in ref["temp"]]
+    fp_c = [compile(_fortran_to_python(e.replace("mesh%s(", "s(")), "fp", "eval") for e in ref["fp"]]
+
+    def matmulvoc(a, b):   # boundary_condition.f90:1738-1755: sums in column order
+        out = []
+        for i in range(9):
+            acc = 0.0
+            for j in range(9):
+                acc = acc + a[i][j] * b[j]
+            out.append(acc)
+        return out
+
+    rng = np.random.default_rng(11)
+    e_, w_ = oracle_mod.lattice()
+    for trial in range(20):
+        rt = 1.0 + rng.uniform(-0.02, 0.02)
+        ut, vt = rng.uniform(-0.08, 0.08, 2)
+        gfx, gfy = (0.0, 0.0) if trial % 2 == 0 else rng.uniform(-1e-3, 1e-3, 2)
+        f = w_ * rt * (1.0 + 3.0 * (e_ @ [ut, vt])) + rng.uniform(-1e-3, 1e-3, 9)
+        got = pyoracle.collide_node(o, f, rt, ut, vt, gfx, gfy)
+        env = {"rt": rt, "ut": ut, "vt": vt, "gfx": gfx, "gfy": gfy, "s": lambda k: s_rates[k - 1]}
+        temp1 = matmulvoc(m, f)
+        temp = [eval(c, env) for c in temp_c]
+        fp = [eval(c, env) for c in fp_c]
+        temp = [temp1[k] + (temp[k] - temp1[k]) * s_rates[k] + fp[k] for k in range(9)]
+        want = matmulvoc(minv, temp)
+        np.testing.assert_allclose(got, want, rtol=0, atol=1e-16)
+    assert ref["relax"].replace(" ", "") == "temp(k)=temp1(k)+(temp(k)-temp1(k))*mesh%s(k)+fp(k)"
