@@ -325,7 +325,14 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
         h->batch_in_half[half] = b;
         if (h->nseg == 0 || s1 < s0) return LBM_OK;
         cudaStream_t st = split ? h->fstream : h->stream;
-        if (split) CK(cudaStreamWaitEvent(h->fstream, h->ev_free[half], 0), "wait");
+        // the half's previous users: the side-stream chains of its steps
+        // (ev_free) and the lattice kernels of those steps on the main stream,
+        // which read the slots' patch rectangles and tile counts (ev_inner:
+        // the main stream's last completed step)
+        if (split) {
+            CK(cudaStreamWaitEvent(h->fstream, h->ev_free[half], 0), "wait");
+            CK(cudaStreamWaitEvent(h->fstream, h->ev_inner, 0), "wait");
+        }
         if (launch_factor(h, s0, s1 - s0 + 1, st)) return cuda_err(h, cudaGetLastError(), "launch factor");
         if (split) CK(cudaEventRecord(h->ev_batch[half], h->fstream), "event");
         return LBM_OK;
@@ -569,6 +576,9 @@ int lbm_create(const lbm_params *p, lbm_t **out)
 int lbm_destroy(lbm_t *h)
 {
     if (!h) return LBM_ERR_ARG;
+    // no queued work of the handle may still use what is freed below
+    if (h->fstream) cudaStreamSynchronize(h->fstream);
+    if (h->side) cudaStreamSynchronize(h->side);
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (int b = 0; b < 2; ++b) { free_dev(h->falloc[b]); h->fbuf[b] = nullptr; free_dev(h->d_fields[b]); }
     free_dev(h->edge_c);
