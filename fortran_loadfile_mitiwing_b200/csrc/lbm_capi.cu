@@ -100,6 +100,15 @@ template <typename P> void free_devp(P *&p)
     p = nullptr;
 }
 
+// waits for all of the handle's queued work (lattice, immersed-boundary and
+// factorization streams): before its device buffers are rewritten or freed
+void quiesce(lbm_handle *h)
+{
+    if (h->fstream) cudaStreamSynchronize(h->fstream);
+    if (h->side) cudaStreamSynchronize(h->side);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+}
+
 // rows of the motion step table (mode.f90:176-269), host FP64
 void lookup_row(const std::vector<double> &tab, int rows, int cols, double t, int &idx, double *row)
 {
@@ -608,6 +617,7 @@ int lbm_destroy(lbm_t *h)
 int lbm_set_boundary(lbm_t *h, int wing, const double *x, const double *y, int npts)
 {
     if (!h) return LBM_ERR_ARG;
+    quiesce(h);   // queued work may still read what is rewritten below
     if (wing < 1 || wing > h->nwing || !x || !y || npts != h->ppw)
         return set_err(h, LBM_ERR_ARG, "set_boundary: bad wing index or point count");
     const int ps = (wing - 1) * h->ppw, ss = (wing - 1) * h->spw;
@@ -637,6 +647,7 @@ int lbm_set_boundary(lbm_t *h, int wing, const double *x, const double *y, int n
 int lbm_set_motion_table(lbm_t *h, const double *table, int rows, int cols)
 {
     if (!h) return LBM_ERR_ARG;
+    quiesce(h);   // queued work may still read what is rewritten below
     if (!table) return set_err(h, LBM_ERR_ARG, "motion table: null");
     if (cols != 1 + 9 * h->nwing) return set_err(h, LBM_ERR_IO, "motion table: column count must be 1+9*wing_count");
     if (rows < 1) return set_err(h, LBM_ERR_IO, "motion table: empty");          // mode.f90:101-104
@@ -670,6 +681,7 @@ int lbm_init(lbm_t *h, const double *du, const double *dv)
 {
     if (!h) return LBM_ERR_ARG;
     if (h->mstep_host.empty()) return set_err(h, LBM_ERR_STATE, "init: motion table not loaded (mode.f90:275-276)");
+    quiesce(h);   // queued work may still read what is rewritten below
     const int nx = h->nx, ny = h->ny;
     const size_t nn = (size_t)nx * ny;
     // initial f = feq(rho=1, u=UU(+du), v=0(+dv)) with single-precision weights
@@ -800,6 +812,7 @@ int lbm_get_populations(lbm_t *h, double *f)
 int lbm_set_populations(lbm_t *h, const double *f)
 {
     if (!h || !f) return LBM_ERR_ARG;
+    quiesce(h);   // queued work may still read what is rewritten below
     if (!h->inited) return set_err(h, LBM_ERR_STATE, "set_populations: not initialised");
     const size_t nn = (size_t)h->nx * h->ny;
     if (!h->d_stage) CK(dmalloc(h, &h->d_stage, sizeof(double) * nn * 9), "alloc stage");
