@@ -83,6 +83,12 @@ ABI = {
                                            _D, _D]),
     "lbm_save_checkpoint": (C.c_int, [_P, C.c_char_p]),
     "lbm_load_checkpoint": (C.c_int, [_P, C.c_char_p]),
+    "lbm_save_flow_field": (C.c_int, [_P, C.c_char_p, _D, C.c_int]),
+    "lbm_read_flow_field": (C.c_int, [_P, C.c_char_p, C.POINTER(C.c_int), _D, C.POINTER(C.c_int)]),
+    "lbm_write_flow_field_file": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, _D, C.c_int, _D, _D,
+                                            _D, _D]),
+    "lbm_read_flow_field_file": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), _D,
+                                           C.POINTER(C.c_int), _D, _D, _D, _D]),
     "lbm_batch_create": (C.c_int, [C.POINTER(_P), C.c_int, C.POINTER(_P)]),
     "lbm_batch_destroy": (C.c_int, [_P]),
     "lbm_batch_add": (C.c_int, [_P, _P]),

@@ -447,6 +447,99 @@ int handle_prepare_ib(lbm_handle *h) { return ensure_ib(h); }
 int handle_error(lbm_handle *h, int code, const char *msg) { return set_err(h, code, msg); }
 int handle_status(lbm_handle *h) { return check_status(h); }
 
+// boundary reference values from the edge f0 (FP64, full f; left column,
+// right column, bottom row, top row, 9 per node): the moments
+// physical_variables takes on the edge columns (solution.f90:516-520) and the
+// corner-column f0 populations the top/bottom extrapolation reads
+// (boundary_condition.f90:705, 832)
+int handle_set_edges(lbm_handle *h, const double *ef)
+{
+    const int nx = h->nx, ny = h->ny;
+    std::vector<double> ec(6 * (size_t)ny + 36);
+    for (int side = 0; side < 2; ++side) {
+        for (int j = 0; j < ny; ++j) {
+            const double *f = ef + 9 * ((size_t)side * ny + j);
+            double temprho = 0.0, tempu = 0.0, tempv = 0.0;
+            for (int k = 0; k < 9; ++k) {
+                temprho = temprho + f[k];
+                tempu = tempu + (double)kEx[k] * f[k];
+                tempv = tempv + (double)kEy[k] * f[k];
+            }
+            double *o = ec.data() + (size_t)side * 3 * ny + 3 * (size_t)j;
+            o[0] = temprho - 1.0;
+            o[1] = tempu / temprho;
+            o[2] = tempv / temprho;
+        }
+    }
+    // (1,2), (1,Ny-1), (Nx,2), (Nx,Ny-1) as deviations from the weights
+    const int cside[4] = {0, 0, 1, 1}, cj[4] = {1, ny - 2, 1, ny - 2};
+    for (int c = 0; c < 4; ++c) {
+        const double *f = ef + 9 * ((size_t)cside[c] * ny + cj[c]);
+        for (int k = 0; k < 9; ++k) ec[6 * (size_t)ny + 9 * c + k] = f[k] - kWref[k];
+    }
+    if (compute_size(h->prec) == sizeof(double)) {
+        CK(cudaMemcpyAsync(h->edge_c, ec.data(), sizeof(double) * ec.size(), cudaMemcpyHostToDevice, h->stream), "copy edge");
+        CK(cudaStreamSynchronize(h->stream), "sync edge");
+    } else {
+        std::vector<float> ecf(ec.begin(), ec.end());
+        CK(cudaMemcpyAsync(h->edge_c, ecf.data(), sizeof(float) * ecf.size(), cudaMemcpyHostToDevice, h->stream), "copy edge");
+        CK(cudaStreamSynchronize(h->stream), "sync edge");
+    }
+    h->edge_f0.assign(ef, ef + 9 * (2 * (size_t)ny + 2 * (size_t)nx));
+    return LBM_OK;
+}
+
+// readflowfield (solution.f90:1709-1839) on the device: f is packed into the
+// storage precision, the field slot gets u and v with density 1 (init's
+// rho0; the file has no density), the boundary values come from the edge f0,
+// and the step counter continues after `cycle` (main.f90:321-323: n = cycle1
+// + 1). The factorization slots are filled again for the restored step.
+int handle_restore(lbm_handle *h, const double *f, const double *u, const double *v, const double *edge_f0, int cycle)
+{
+    quiesce(h);
+    const size_t nn = (size_t)h->nx * h->ny;
+    if (!h->d_stage) CK(dmalloc(h, &h->d_stage, sizeof(double) * nn * 9), "alloc stage");
+    CK(cudaMemcpyAsync(h->d_stage, f, sizeof(double) * nn * 9, cudaMemcpyHostToDevice, h->stream), "copy f");
+    if (launch_pack(h, h->d_stage, h->fbuf[0])) return cuda_err(h, cudaGetLastError(), "pack");
+    CK(cudaStreamSynchronize(h->stream), "sync f");
+    free_devp(h->d_stage);
+    h->cur = 0;
+    if (compute_size(h->prec) == sizeof(double)) {
+        std::vector<double> fl(3 * nn);
+        for (size_t q = 0; q < nn; ++q) {
+            fl[q] = 1.0;
+            fl[nn + q] = u[q];
+            fl[2 * nn + q] = v[q];
+        }
+        CK(cudaMemcpyAsync(h->d_fields[0], fl.data(), sizeof(double) * fl.size(), cudaMemcpyHostToDevice, h->stream),
+           "copy fields");
+        CK(cudaStreamSynchronize(h->stream), "sync fields");
+    } else {
+        std::vector<float> fl(3 * nn);
+        for (size_t q = 0; q < nn; ++q) {
+            fl[q] = 1.0f;
+            fl[nn + q] = (float)u[q];
+            fl[2 * nn + q] = (float)v[q];
+        }
+        CK(cudaMemcpyAsync(h->d_fields[0], fl.data(), sizeof(float) * fl.size(), cudaMemcpyHostToDevice, h->stream),
+           "copy fields");
+        CK(cudaStreamSynchronize(h->stream), "sync fields");
+    }
+    const int rc = handle_set_edges(h, edge_f0);
+    if (rc) return rc;
+    CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream), "clear status");
+    CK(cudaMemsetAsync(h->d_pinfo, 0, LBM_NSLOT_MAX * sizeof(PatchInfo), h->stream), "clear pinfo");
+    CK(cudaStreamSynchronize(h->stream), "sync restore");
+    h->n = cycle + 1;
+    h->steps_done = cycle;
+    h->fields_slot = 0;
+    h->fields_step[0] = cycle;
+    h->fields_step[1] = -1;
+    h->batch_in_half[0] = h->batch_in_half[1] = -1;
+    h->fgroup[0] = h->fgroup[1] = -1;
+    return LBM_OK;
+}
+
 extern "C" {
 
 int lbm_default_params(lbm_params *p)
@@ -693,41 +786,25 @@ int lbm_init(lbm_t *h, const double *du, const double *dv)
         if (du) u = u + du[q];
         if (dv) v = v + dv[q];
     };
-    // edge constants: moments of the edge f0 (physical_variables on the
-    // edge, solution.f90:516-520) and the corner-column f0 populations
-    const size_t cs = compute_size(h->prec);
-    std::vector<double> ec(6 * (size_t)ny + 36);
-    for (int side = 0; side < 2; ++side) {
-        const int i = side == 0 ? 0 : nx - 1;
-        for (int j = 0; j < ny; ++j) {
-            const size_t q = (size_t)j * nx + i;
-            double u, v;
-            uv(q, u, v);
-            double temprho = 0.0, tempu = 0.0, tempv = 0.0;
-            for (int k = 0; k < 9; ++k) {
-                const double f = feq(1.0, u, v, k);
-                temprho = temprho + f;
-                tempu = tempu + (double)kEx[k] * f;
-                tempv = tempv + (double)kEy[k] * f;
-            }
-            double *o = ec.data() + (size_t)side * 3 * ny + 3 * (size_t)j;
-            o[0] = temprho - 1.0;
-            o[1] = tempu / temprho;
-            o[2] = tempv / temprho;
-        }
-    }
-    const int ci[4] = {0, 0, nx - 1, nx - 1}, cj[4] = {1, ny - 2, 1, ny - 2};
-    for (int c = 0; c < 4; ++c) {
+    // edge f0 = the initial f on the four edges (streaming never rewrites
+    // them, solution.f90:440-447) and the boundary values taken from them
+    std::vector<double> ef(9 * (2 * (size_t)ny + 2 * (size_t)nx));
+    auto edge_node = [&](size_t at, int i, int j) {
         double u, v;
-        uv((size_t)cj[c] * nx + ci[c], u, v);
-        for (int k = 0; k < 9; ++k) ec[6 * (size_t)ny + 9 * c + k] = feq(1.0, u, v, k) - kWref[k];
+        uv((size_t)j * nx + i, u, v);
+        for (int k = 0; k < 9; ++k) ef[9 * at + k] = feq(1.0, u, v, k);
+    };
+    for (int j = 0; j < ny; ++j) {
+        edge_node((size_t)j, 0, j);
+        edge_node((size_t)ny + j, nx - 1, j);
     }
-    if (cs == sizeof(double)) {
-        CK(cudaMemcpyAsync(h->edge_c, ec.data(), sizeof(double) * ec.size(), cudaMemcpyHostToDevice, h->stream), "copy edge");
-    } else {
-        std::vector<float> ef(ec.begin(), ec.end());
-        CK(cudaMemcpyAsync(h->edge_c, ef.data(), sizeof(float) * ef.size(), cudaMemcpyHostToDevice, h->stream), "copy edge");
-        CK(cudaStreamSynchronize(h->stream), "sync edge");
+    for (int i = 0; i < nx; ++i) {
+        edge_node(2 * (size_t)ny + i, i, 0);
+        edge_node(2 * (size_t)ny + nx + i, i, ny - 1);
+    }
+    {
+        const int rc = handle_set_edges(h, ef.data());
+        if (rc) return rc;
     }
     // populations and the initial fields (rho = 1, u, v) in slot 0: u0 of the first step
     double *ddu = nullptr, *ddv = nullptr;

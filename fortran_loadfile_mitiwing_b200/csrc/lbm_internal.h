@@ -117,6 +117,10 @@ struct lbm_handle {
     // edge constants (FP64 master + compute-precision copy)
     EdgeConst edge{};
     void *edge_c = nullptr;  // compute precision: col_l, col_r, corner packed
+    // the edge f0 populations they come from (FP64, full f, 9 per node): left
+    // column j = 1..Ny, right column j = 1..Ny, bottom row i = 1..Nx, top row
+    // i = 1..Nx (the edge part of the reference's restart file)
+    std::vector<double> edge_f0;
     // geometry and motion
     std::vector<double> hx0, hy0, harc;
     std::vector<int> have_wing;
@@ -212,6 +216,12 @@ int launch_check(lbm_handle *h, int slot, int ring_slot, bool residual, cudaStre
 int handle_prepare_ib(lbm_handle *h);                    // immersed-boundary buffers (once per geometry)
 int handle_error(lbm_handle *h, int code, const char *msg);
 int handle_status(lbm_handle *h);                        // reads and clears the device status
+// boundary reference values from the edge f0 populations (layout of edge_f0)
+int handle_set_edges(lbm_handle *h, const double *edge_f0);
+// state of a restart file in the reference's layout: populations f(nx,ny,9),
+// velocity fields (density 1, as init leaves it), edge f0; next step cycle+1
+int handle_restore(lbm_handle *h, const double *f, const double *u, const double *v, const double *edge_f0,
+                   int cycle);
 size_t kf_args_size(int prec);
 void kf_args_write(lbm_handle *h, const void *fin, void *fout, void *fields, int mode, void *dst);
 void kf_tma_grid(const lbm_handle *h, int *gx, int *gy);

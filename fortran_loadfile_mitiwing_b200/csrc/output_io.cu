@@ -8,6 +8,10 @@
 //                falls back to the copy when the file is missing, short or
 //                corrupt), holding this library's exact device state so that
 //                a restart continues bit for bit.
+//   saved_flow_feild.dat   the same routines in the reference's own byte
+//                layout (nvfortran form='binary'), so that a run can move
+//                between the reference and this library in either direction.
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstdio>
@@ -326,9 +330,212 @@ std::string read_ckpt_file(const lbm_handle *h, const std::string &path, CkptHea
     return why.empty() ? "" : path + ": " + why;
 }
 
+// ---- restart file in the reference's layout ------------------------------
+// saveflowfield (solution.f90:1646-1672) opens the file form='binary':
+// unformatted with no record markers, native byte order, so the file is the
+// items of each WRITE back to back:
+//   int32 cycle1, int32 wing_count,
+//   11 x wing_count float64: body_rel_a, _a_prev, _v, _v_prev, _s, _s_prev,
+//     _pos, _theta_prev, _theta, _temp_theta_prev, _temp_theta,
+//   int32 movenum,
+//   j = 1..Ny, i = 1..Nx: float64 u(i,j), v(i,j), f(i,j,1:9),
+//   j = 2..Ny-1: leftf2(j,:), f0(1,j,:), rightf2(j,:), f0(Nx,j,:),
+//   i = 1..Nx:   upf2(i,:), f0(i,Ny,:), downf2(i,:), f0(i,1,:).
+// leftf2 .. downf2 are copies of the initial edge populations
+// (solution.f90:60-63) that only the multi-block refinement rewrites
+// (solution.f90:1300-1360, not called with one mesh), so they equal the edge
+// f0 and are written from it; the reader does not use them.
+
+const int kBodyArrays = 11;
+
+size_t flow_file_bytes(int nx, int ny, int nwing)
+{
+    return 12 + 8 * (size_t)kBodyArrays * nwing + 88 * (size_t)nx * ny + 8 * 36 * ((size_t)(ny - 2) + (size_t)nx);
+}
+
+int write_flow_file(const char *path, int nx, int ny, int cycle, int nwing, const double *body, int movenum,
+                    const double *u, const double *v, const double *f, const double *ef)
+{
+    FILE *fp = fopen(path, "wb");
+    if (!fp) return LBM_ERR_IO;
+    const size_t nn = (size_t)nx * ny;
+    const int32_t head[2] = {cycle, nwing};
+    std::vector<double> zeros((size_t)kBodyArrays * nwing, 0.0);
+    const int32_t mv = movenum;
+    bool ok = write_all(fp, head, sizeof head) &&
+              write_all(fp, body ? body : zeros.data(), sizeof(double) * kBodyArrays * nwing) &&
+              write_all(fp, &mv, sizeof mv);
+    std::vector<double> row(11 * (size_t)nx);
+    for (int j = 0; j < ny && ok; ++j) {
+        for (int i = 0; i < nx; ++i) {
+            const size_t q = (size_t)j * nx + i;
+            double *o = row.data() + 11 * (size_t)i;
+            o[0] = u[q];
+            o[1] = v[q];
+            for (int k = 0; k < 9; ++k) o[2 + k] = f[k * nn + q];
+        }
+        ok = write_all(fp, row.data(), sizeof(double) * row.size());
+    }
+    const double *L = ef, *R = ef + 9 * (size_t)ny, *B = ef + 18 * (size_t)ny, *T = B + 9 * (size_t)nx;
+    std::vector<double> edge(36 * (size_t)std::max(nx, ny));
+    double *o = edge.data();
+    for (int j = 1; j < ny - 1; ++j)
+        for (const double *src : {L + 9 * (size_t)j, L + 9 * (size_t)j, R + 9 * (size_t)j, R + 9 * (size_t)j}) {
+            memcpy(o, src, 9 * sizeof(double));
+            o += 9;
+        }
+    if (ok) ok = write_all(fp, edge.data(), sizeof(double) * (size_t)(o - edge.data()));
+    o = edge.data();
+    for (int i = 0; i < nx; ++i)
+        for (const double *src : {T + 9 * (size_t)i, T + 9 * (size_t)i, B + 9 * (size_t)i, B + 9 * (size_t)i}) {
+            memcpy(o, src, 9 * sizeof(double));
+            o += 9;
+        }
+    if (ok) ok = write_all(fp, edge.data(), sizeof(double) * (size_t)(o - edge.data()));
+    ok = (fclose(fp) == 0) && ok;
+    return ok ? LBM_OK : LBM_ERR_IO;
+}
+
+// reads one file of the layout above. Returns LBM_OK, LBM_ERR_IO for a file
+// that is missing, short or of another size (the reader of the reference
+// then tries the copy: err=/end= branches, solution.f90:1738-1744), or
+// LBM_ERR_STATE for a wing count other than this case's (the reference
+// stops, solution.f90:1740); `why` says which.
+int read_flow_file(const char *path, int nx, int ny, int nwing, int *cycle, double *body, int *movenum, double *u,
+                   double *v, double *f, double *ef, std::string &why)
+{
+    FILE *fp = fopen(path, "rb");
+    if (!fp) {
+        why = std::string("cannot open ") + path;
+        return LBM_ERR_IO;
+    }
+    auto fail = [&](int code, const std::string &w) {
+        fclose(fp);
+        why = std::string(path) + ": " + w;
+        return code;
+    };
+    int32_t head[2];
+    if (fread(head, sizeof head, 1, fp) != 1) return fail(LBM_ERR_IO, "short file");
+    if (head[1] != nwing) return fail(LBM_ERR_STATE, "wing count " + std::to_string(head[1]) + " in the file, " +
+                                                         std::to_string(nwing) + " in this case");
+    if (fseek(fp, 0, SEEK_END) != 0) return fail(LBM_ERR_IO, "cannot seek");
+    const long long size = ftell(fp);
+    const size_t want = flow_file_bytes(nx, ny, nwing);
+    if (size < 0 || (size_t)size != want)
+        return fail(LBM_ERR_IO, "size " + std::to_string(size) + " bytes, a " + std::to_string(nx) + "x" +
+                                    std::to_string(ny) + " grid with " + std::to_string(nwing) + " wings has " +
+                                    std::to_string(want));
+    if (fseek(fp, 8, SEEK_SET) != 0) return fail(LBM_ERR_IO, "cannot seek");
+    std::vector<double> bs((size_t)kBodyArrays * nwing);
+    int32_t mv = 0;
+    if ((nwing > 0 && fread(bs.data(), sizeof(double), bs.size(), fp) != bs.size()) || fread(&mv, sizeof mv, 1, fp) != 1)
+        return fail(LBM_ERR_IO, "short file");
+    const size_t nn = (size_t)nx * ny;
+    std::vector<double> row(11 * (size_t)nx);
+    for (int j = 0; j < ny; ++j) {
+        if (fread(row.data(), sizeof(double), row.size(), fp) != row.size()) return fail(LBM_ERR_IO, "short file");
+        for (int i = 0; i < nx; ++i) {
+            const size_t q = (size_t)j * nx + i;
+            const double *x = row.data() + 11 * (size_t)i;
+            u[q] = x[0];
+            v[q] = x[1];
+            for (int k = 0; k < 9; ++k) f[k * nn + q] = x[2 + k];
+        }
+    }
+    double *L = ef, *R = ef + 9 * (size_t)ny, *B = ef + 18 * (size_t)ny, *T = B + 9 * (size_t)nx;
+    double rec[36];
+    for (int j = 1; j < ny - 1; ++j) {   // leftf2, f0(1,j), rightf2, f0(Nx,j)
+        if (fread(rec, sizeof(double), 36, fp) != 36) return fail(LBM_ERR_IO, "short file");
+        memcpy(L + 9 * (size_t)j, rec + 9, 9 * sizeof(double));
+        memcpy(R + 9 * (size_t)j, rec + 27, 9 * sizeof(double));
+    }
+    for (int i = 0; i < nx; ++i) {       // upf2, f0(i,Ny), downf2, f0(i,1)
+        if (fread(rec, sizeof(double), 36, fp) != 36) return fail(LBM_ERR_IO, "short file");
+        memcpy(T + 9 * (size_t)i, rec + 9, 9 * sizeof(double));
+        memcpy(B + 9 * (size_t)i, rec + 27, 9 * sizeof(double));
+    }
+    fclose(fp);
+    // the corner nodes of the columns are those of the rows
+    memcpy(L, B, 9 * sizeof(double));
+    memcpy(L + 9 * (size_t)(ny - 1), T, 9 * sizeof(double));
+    memcpy(R, B + 9 * (size_t)(nx - 1), 9 * sizeof(double));
+    memcpy(R + 9 * (size_t)(ny - 1), T + 9 * (size_t)(nx - 1), 9 * sizeof(double));
+    *cycle = head[0];
+    *movenum = mv;
+    if (body) std::copy(bs.begin(), bs.end(), body);
+    return LBM_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int lbm_write_flow_field_file(const char *path, int nx, int ny, int cycle, int wing_count, const double *body_state,
+                              int movenum, const double *u, const double *v, const double *f, const double *edge_f0)
+{
+    if (!path || nx < 3 || ny < 3 || wing_count < 0 || !u || !v || !f || !edge_f0) return LBM_ERR_ARG;
+    return write_flow_file(path, nx, ny, cycle, wing_count, body_state, movenum, u, v, f, edge_f0);
+}
+
+int lbm_read_flow_field_file(const char *path, int nx, int ny, int wing_count, int *cycle, double *body_state,
+                             int *movenum, double *u, double *v, double *f, double *edge_f0)
+{
+    if (!path || nx < 3 || ny < 3 || wing_count < 0 || !cycle || !movenum || !u || !v || !f || !edge_f0)
+        return LBM_ERR_ARG;
+    std::string why;
+    return read_flow_file(path, nx, ny, wing_count, cycle, body_state, movenum, u, v, f, edge_f0, why);
+}
+
+int lbm_save_flow_field(lbm_t *h, const char *path, const double *body_state, int movenum)
+{
+    if (!h || !path) return LBM_ERR_ARG;
+    if (!h->inited) return io_err(h, LBM_ERR_STATE, "save_flow_field: not initialised");
+    const size_t nn = (size_t)h->nx * h->ny;
+    std::vector<double> u(nn), v(nn), f(9 * nn);
+    int rc = lbm_get_fields(h, nullptr, u.data(), v.data());
+    if (rc) return rc;
+    rc = lbm_get_populations(h, f.data());
+    if (rc) return rc;
+    const std::string p = path, c = copy_path(p);
+    for (const std::string &q : {p, c})   // saved_flow_feild.dat and saved_flow_feild_copy.dat
+        if (write_flow_file(q.c_str(), h->nx, h->ny, h->n - 1, h->nwing, body_state, movenum, u.data(), v.data(),
+                            f.data(), h->edge_f0.data()))
+            return io_err(h, LBM_ERR_IO, "save_flow_field: cannot write " + q);
+    return LBM_OK;
+}
+
+int lbm_read_flow_field(lbm_t *h, const char *path, int *cycle, double *body_state, int *movenum)
+{
+    if (!h || !path) return LBM_ERR_ARG;
+    if (!h->inited) return io_err(h, LBM_ERR_STATE, "read_flow_field: call lbm_init first");
+    const size_t nn = (size_t)h->nx * h->ny;
+    std::vector<double> u(nn), v(nn), f(9 * nn), ef(9 * (2 * (size_t)h->ny + 2 * (size_t)h->nx));
+    std::vector<double> body((size_t)kBodyArrays * h->nwing);
+    int cyc = 0, mv = 0;
+    const std::string p = path, c = copy_path(p);
+    std::string why, why2;
+    int rc = read_flow_file(p.c_str(), h->nx, h->ny, h->nwing, &cyc, body.data(), &mv, u.data(), v.data(), f.data(),
+                            ef.data(), why);
+    if (rc == LBM_ERR_STATE) return io_err(h, rc, "read_flow_field: " + why);
+    if (rc) {   // the copy (solution.f90:1768-1802)
+        rc = read_flow_file(c.c_str(), h->nx, h->ny, h->nwing, &cyc, body.data(), &mv, u.data(), v.data(), f.data(),
+                            ef.data(), why2);
+        if (rc) return io_err(h, rc, "read_flow_field: " + why + "; " + why2);
+    }
+    if (cycle) *cycle = cyc;
+    if (movenum) *movenum = mv;
+    if (body_state) std::copy(body.begin(), body.end(), body_state);
+    // free flight (solve_dynamic_equations, main.f90:103) moves the body and
+    // shifts the mesh (move_mesh, main.f90:370-386); the prescribed motion of
+    // this library cannot continue such a state
+    bool moved = mv != 0;
+    for (double b : body) moved = moved || b != 0.0;
+    if (moved)
+        return io_err(h, LBM_ERR_STATE, "read_flow_field: the file holds rigid-body motion state (free flight or a "
+                                        "shifted mesh), which this library does not model");
+    if (cyc < 0) return io_err(h, LBM_ERR_IO, "read_flow_field: negative step number in the file");
+    return handle_restore(h, f.data(), u.data(), v.data(), ef.data(), cyc);
+}
 
 int lbm_write_tecplot_fields(const char *path, int nx, int ny, double ox, double oy, double scale, double uu,
                              double solution_time, int stride_x, int stride_y, const double *rho, const double *u,

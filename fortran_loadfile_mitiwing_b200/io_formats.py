@@ -100,3 +100,43 @@ def write_tecplot_fields(path, rho, u, v, ox, oy, scale, uu, solution_time, stri
                                       _abi.dptr(yb1) if wing_count else None)
     if rc != 0:
         raise IOError(f"lbm_write_tecplot_fields({path}) = {rc}")
+
+
+def edge_count(nx, ny):
+    """Nodes of the edge f0 array: left column, right column, bottom row, top row."""
+    return 2 * ny + 2 * nx
+
+
+def write_flow_field_file(path, cycle, u, v, f, edge_f0, body_state=None, movenum=0, lib=None):
+    """One restart file in the reference's saveflowfield layout from host
+    arrays (lbm_write_flow_field_file): u, v (ny, nx), f (9, ny, nx),
+    edge_f0 (2 ny + 2 nx, 9), body_state (11, wing_count) or None."""
+    lib = lib or _abi.load_library()
+    ny, nx = np.shape(u)
+    a = [np.ascontiguousarray(x, dtype=np.float64).reshape(-1) for x in (u, v, f, edge_f0)]
+    if a[2].size != 9 * nx * ny or a[3].size != 9 * edge_count(nx, ny):
+        raise ValueError("f must hold 9 nx ny values and edge_f0 9 (2 nx + 2 ny)")
+    bs = None if body_state is None else np.ascontiguousarray(body_state, dtype=np.float64).reshape(-1)
+    wing_count = 0 if bs is None else bs.size // 11
+    rc = lib.lbm_write_flow_field_file(os.fsencode(path), nx, ny, int(cycle), wing_count, _abi.dptr(bs),
+                                       int(movenum), *(_abi.dptr(x) for x in a))
+    if rc != 0:
+        raise IOError(f"lbm_write_flow_field_file({path}) = {rc}")
+
+
+def read_flow_field_file(path, nx, ny, wing_count, lib=None):
+    """Reads one restart file of the reference's layout
+    (lbm_read_flow_field_file): dict of cycle, body_state (11, wing_count),
+    movenum, u, v (ny, nx), f (9, ny, nx), edge_f0 (2 ny + 2 nx, 9)."""
+    lib = lib or _abi.load_library()
+    cyc, mv = C.c_int(0), C.c_int(0)
+    bs = np.zeros(11 * wing_count)
+    u, v = np.zeros(nx * ny), np.zeros(nx * ny)
+    f, ef = np.zeros(9 * nx * ny), np.zeros(9 * edge_count(nx, ny))
+    rc = lib.lbm_read_flow_field_file(os.fsencode(path), nx, ny, wing_count, C.byref(cyc), _abi.dptr(bs),
+                                      C.byref(mv), _abi.dptr(u), _abi.dptr(v), _abi.dptr(f), _abi.dptr(ef))
+    if rc != 0:
+        raise IOError(f"lbm_read_flow_field_file({path}) = {_abi.STATUS_NAMES.get(rc, rc)}")
+    return dict(cycle=cyc.value, body_state=bs.reshape(11, wing_count), movenum=mv.value,
+                u=u.reshape(ny, nx), v=v.reshape(ny, nx), f=f.reshape(9, ny, nx),
+                edge_f0=ef.reshape(edge_count(nx, ny), 9))

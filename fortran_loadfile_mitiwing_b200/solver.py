@@ -131,6 +131,23 @@ class Lbm:
         """Restores the state from `path`, else its _copy (lbm_load_checkpoint)."""
         self._ck(self.lib.lbm_load_checkpoint(self.h, os.fsencode(path)))
 
+    def save_flow_field(self, path="saved_flow_feild.dat", body_state=None, movenum=0):
+        """Writes the reference's own restart file (saveflowfield layout) to
+        `path` and its _copy (lbm_save_flow_field)."""
+        bs = None if body_state is None else np.ascontiguousarray(body_state, dtype=np.float64).reshape(-1)
+        if bs is not None and bs.size != 11 * self.params.wing_count:
+            raise ValueError("body_state holds 11 arrays of wing_count values")
+        self._ck(self.lib.lbm_save_flow_field(self.h, os.fsencode(path), dptr(bs), int(movenum)))
+
+    def read_flow_field(self, path="saved_flow_feild.dat"):
+        """Restarts from the reference's restart file `path`, else its _copy
+        (lbm_read_flow_field). Returns (cycle1, body_state (11, wing_count),
+        movenum); the next step is cycle1 + 1."""
+        cyc, mv = C.c_int(0), C.c_int(0)
+        bs = np.zeros(11 * self.params.wing_count)
+        self._ck(self.lib.lbm_read_flow_field(self.h, os.fsencode(path), C.byref(cyc), dptr(bs), C.byref(mv)))
+        return cyc.value, bs.reshape(11, self.params.wing_count), mv.value
+
     def set_populations(self, f):
         f = np.ascontiguousarray(f, dtype=np.float64).reshape(-1)
         self._ck(self.lib.lbm_set_populations(self.h, dptr(f)))

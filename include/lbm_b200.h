@@ -171,7 +171,8 @@ LBM_API int lbm_get_fields(lbm_t *h, double *rho, double *u, double *v);
 LBM_API int lbm_get_populations(lbm_t *h, double *f);
 
 /* restores f(nx,ny,9) (readflowfield, solution.f90:1709-1839, the f part);
- * the edge f0 copies are kept from lbm_init. */
+ * the edge f0 copies are kept from lbm_init (lbm_read_flow_field restores
+ * them from a restart file). */
 LBM_API int lbm_set_populations(lbm_t *h, const double *f);
 
 /* erranalysis (solution.f90:74-127): ||u-u0|| / (||u|| + 1e-30) over the
@@ -272,6 +273,50 @@ LBM_API int lbm_write_tecplot_fields(const char *path, int nx, int ny, double ox
                                      const double *xb1, const double *yb1);
 LBM_API int lbm_save_checkpoint(lbm_t *h, const char *path);
 LBM_API int lbm_load_checkpoint(lbm_t *h, const char *path);
+
+/* ---- restart files in the reference's byte layout -----------------------
+ * saveflowfield / readflowfield (solution.f90:1604-1839) as the reference
+ * writes them: nvfortran form='binary' (no record markers, native byte
+ * order): int32 cycle1, int32 wing_count, 11 x wing_count float64 body-state
+ * arrays (body_rel_a, _a_prev, _v, _v_prev, _s, _s_prev, _pos, _theta_prev,
+ * _theta, _temp_theta_prev, _temp_theta), int32 movenum; per node (j outer,
+ * i inner) float64 u, v, f(1:9); then for j = 2..Ny-1 leftf2, f0(1,j),
+ * rightf2, f0(Nx,j), and for i = 1..Nx upf2, f0(i,Ny), downf2, f0(i,1), 9
+ * float64 each. A file written by the reference restarts this library and the
+ * other way round. A restart continues bit for bit in FP32, FP16 and BF16
+ * storage; FP64 storage keeps f - w, which the file's f holds only to f's
+ * last bit, so an FP64 restart continues within rounding (about 1e-14 in f).
+ * lbm_save_flow_field: the state after the last step into `path` and its copy
+ *   (saved_flow_feild.dat and saved_flow_feild_copy.dat); cycle1 = the last
+ *   step's number (lbm_step_index - 1); u, v of the last step (the step must
+ *   have kept its fields, as for lbm_get_fields); leftf2 .. downf2 written as
+ *   the edge f0 (both are the initial edge populations on the one-mesh path).
+ *   body_state (11*wing_count, nullable = zeros) and movenum are the driver's
+ *   rigid-body values, zero for prescribed motion.
+ * lbm_read_flow_field: after lbm_init of the same case, reads `path`, or its
+ *   copy when `path` is missing, short or of another size (LBM_ERR_IO when
+ *   neither reads); a wing count other than the case's is LBM_ERR_STATE
+ *   without trying the copy (the reference stops). Sets the populations, the
+ *   boundary values from the file's edge f0, the fields (u, v from the file,
+ *   density 1 as after init: the file has none) and the step counter (the
+ *   next step is cycle1 + 1, main.f90:321-323). Returns cycle1, the body
+ *   state and movenum (nullable); a file with non-zero body state or movenum
+ *   (free flight, which this library does not model) is LBM_ERR_STATE and
+ *   leaves the handle unchanged.
+ * lbm_write_flow_field_file / lbm_read_flow_field_file: one file from / into
+ *   host arrays, no handle and no device: u, v (nx,ny) and f (nx,ny,9) in
+ *   Fortran order, edge_f0 = 9 float64 per node for the left column
+ *   (j = 1..Ny), the right column, the bottom row (i = 1..Nx) and the top
+ *   row. The reader returns LBM_ERR_IO (missing, short, other size) or
+ *   LBM_ERR_STATE (other wing count). */
+LBM_API int lbm_save_flow_field(lbm_t *h, const char *path, const double *body_state, int movenum);
+LBM_API int lbm_read_flow_field(lbm_t *h, const char *path, int *cycle, double *body_state, int *movenum);
+LBM_API int lbm_write_flow_field_file(const char *path, int nx, int ny, int cycle, int wing_count,
+                                      const double *body_state, int movenum, const double *u, const double *v,
+                                      const double *f, const double *edge_f0);
+LBM_API int lbm_read_flow_field_file(const char *path, int nx, int ny, int wing_count, int *cycle,
+                                     double *body_state, int *movenum, double *u, double *v, double *f,
+                                     double *edge_f0);
 
 /* ---- batches: several cases stepped together on one GPU ----------------
  * The reference runs one case per process (main.f90); flapping-wing studies
