@@ -14,6 +14,7 @@
 // their formula needs (O(perimeter) extra reads) so that no second launch and
 // no side buffer is needed for the boundary condition.
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "lbm_internal.h"
@@ -154,7 +155,10 @@ __global__ void __launch_bounds__(128) kf_vec(const KFArgs<C> a)
 // then read the shifted populations from shared memory. The copies keep
 // KS x 9 row segments in flight per CTA without holding them in registers.
 // Rows 0 and ny-1 are handled by one extra CTA row of the grid, and columns
-// 0 and nx-1 by the scalar edge path.
+// 0 and nx-1 by the scalar edge path. With FP32 arithmetic (FP32, FP16 and
+// BF16 storage) a thread updates two rows of its column at once with the
+// paired FP32 instructions (collide_pair), which halves the arithmetic
+// instructions of the collision.
 
 constexpr int TW = 256;        // strip width (threads per CTA)
 #ifndef LBM_KF_STAGES
@@ -247,6 +251,59 @@ __device__ __forceinline__ void kf_tma_cta(const KFArgs<C> &a, int bx, int by, i
     // with row r + KS once all warps have arrived. Only warp 0 waits for the
     // other warps; they run up to KS - 1 rows ahead.
     bool ok = true;
+    if constexpr (std::is_same<C, float>::value) {
+        // FP32 arithmetic: rows r and r + 1 of a thread's column as one pair
+        // of the paired instructions (collide_pair); an odd last row is
+        // computed in both halves and stored once
+        const bool interior = i > 0 && i < a.nx - 1;
+        for (int r = 0; r < nrows; r += 2) {
+            const int r1 = min(r + 1, nrows - 1);
+            const int s0 = r % KS, s1 = r1 % KS, j = j0 + r;
+            if (!wait(&full[s0], (uint32_t)((r / KS) & 1)) || !wait(&full[s1], (uint32_t)((r1 / KS) & 1))) {
+                ok = false;
+                break;
+            }
+            const bool st0 = interior && !(a.mode == KF_OUTER && corr_tile(a, rr, i, j));
+            const bool st1 = interior && r1 != r && !(a.mode == KF_OUTER && corr_tile(a, rr, i, j + 1));
+            if (st0 || st1) {
+                float2 g[9], o[9], frho, fu, fv;
+                const T *row0 = buf + s0 * 9 * SEG + H + tid, *row1 = buf + s1 * 9 * SEG + H + tid;
+#pragma unroll
+                for (int k = 0; k < 9; ++k)
+                    g[k] = make_float2(Store<T>::cvt(row0[k * SEG - lbm_ex(k)]), Store<T>::cvt(row1[k * SEG - lbm_ex(k)]));
+                collide_pair<CONS0, FIELDS>(a, g, o, frho, fu, fv);
+                if (st0) {
+                    C go[9];
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) go[k] = o[k].x;
+                    store_node<T, C, FIELDS>(a, fout, i, j, go, frho.x, fu.x, fv.x);
+                }
+                if (st1) {
+                    C go[9];
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) go[k] = o[k].y;
+                    store_node<T, C, FIELDS>(a, fout, i, j + 1, go, frho.y, fu.y, fv.y);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) {
+                mbar_arrive(&empty[s0]);
+                if (r1 != r) mbar_arrive(&empty[s1]);
+            }
+            if (tid == 0) {
+                for (int q = r; q <= r1 && ok; ++q)
+                    if (q + KS < nrows) {
+                        if (!wait(&empty[q % KS], (uint32_t)((q / KS) & 1))) {
+                            ok = false;
+                            break;
+                        }
+                        fence_proxy_async();
+                        issue(q + KS);
+                    }
+                if (!ok) break;
+            }
+        }
+    } else
     for (int r = 0; r < nrows; ++r) {
         const int s = r % KS, j = j0 + r;
         const uint32_t parity = (uint32_t)((r / KS) & 1);

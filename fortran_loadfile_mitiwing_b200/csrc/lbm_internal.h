@@ -25,6 +25,7 @@ struct KFArgs {
     int nx, ny, pitch;
     long long plane;
     C s[9];
+    C sc[9];   // s[k] times row k of the inverse transform's scale, signed for the paired update
     C cs;
     const C *col_l, *col_r, *corner;   // edge constants in compute precision
     const PatchInfo *pinfo;            // the step's patch rectangle (KF_OUTER)
