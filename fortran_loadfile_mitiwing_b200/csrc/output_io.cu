@@ -264,11 +264,15 @@ size_t field_bytes(const lbm_handle *h)
     return 3 * cs * (size_t)h->nx * h->ny;
 }
 
-// the whole state in host memory (header, populations, edge values, fields x2)
+// the FP64 edge f0 the boundary values were built from (lbm_handle::edge_f0)
+size_t ef0_bytes(const lbm_handle *h) { return sizeof(double) * 9 * (2 * (size_t)h->nx + 2 * (size_t)h->ny); }
+
+// the whole state in host memory (header, populations, edge values, fields x2,
+// edge f0)
 int gather_state(lbm_handle *h, CkptHeader &hd, std::vector<unsigned char> &blob)
 {
     hd = CkptHeader{};
-    hd.version = 1;
+    hd.version = 2;
     hd.nx = h->nx; hd.ny = h->ny; hd.pitch = h->pitch; hd.prec = h->prec;
     hd.nwing = h->nwing; hd.ppw = h->ppw; hd.cur = 0;
     hd.n = h->n; hd.steps_done = h->steps_done;
@@ -277,7 +281,7 @@ int gather_state(lbm_handle *h, CkptHeader &hd, std::vector<unsigned char> &blob
     hd.pop_bytes = (int64_t)(h->elem * 9 * (size_t)h->plane);
     hd.edge_bytes = (int64_t)edge_bytes(h);
     hd.field_bytes = (int64_t)field_bytes(h);
-    blob.resize((size_t)(hd.pop_bytes + hd.edge_bytes + 2 * hd.field_bytes));
+    blob.resize((size_t)(hd.pop_bytes + hd.edge_bytes + 2 * hd.field_bytes) + ef0_bytes(h));
     unsigned char *p = blob.data();
     cudaError_t e = cudaMemcpyAsync(p, h->fbuf[h->cur], hd.pop_bytes, cudaMemcpyDeviceToHost, h->stream);
     p += hd.pop_bytes;
@@ -285,6 +289,7 @@ int gather_state(lbm_handle *h, CkptHeader &hd, std::vector<unsigned char> &blob
     p += hd.edge_bytes;
     for (int s = 0; s < 2 && e == cudaSuccess; ++s, p += hd.field_bytes)
         e = cudaMemcpyAsync(p, h->d_fields[s], hd.field_bytes, cudaMemcpyDeviceToHost, h->stream);
+    memcpy(p, h->edge_f0.data(), ef0_bytes(h));
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return io_err(h, LBM_ERR_CUDA, std::string("checkpoint: ") + cudaGetErrorString(e));
     return LBM_OK;
@@ -311,7 +316,7 @@ std::string read_ckpt_file(const lbm_handle *h, const std::string &path, CkptHea
     std::string why;
     if (fread(magic, 1, 16, f) != 16 || memcmp(magic, kMagic, 16) != 0) why = "not a checkpoint of this library";
     else if (fread(&hd, 1, sizeof hd, f) != sizeof hd) why = "short header";
-    else if (hd.version != 1) why = "unknown checkpoint version";
+    else if (hd.version != 2) why = "unknown checkpoint version";
     else if (hd.nx != h->nx || hd.ny != h->ny || hd.pitch != h->pitch || hd.prec != h->prec || hd.nwing != h->nwing ||
              hd.ppw != h->ppw)
         why = "grid, storage precision or wings differ from this case";
@@ -319,7 +324,7 @@ std::string read_ckpt_file(const lbm_handle *h, const std::string &path, CkptHea
              hd.field_bytes != (int64_t)field_bytes(h))
         why = "section sizes differ from this case";
     if (why.empty()) {
-        blob.resize((size_t)(hd.pop_bytes + hd.edge_bytes + 2 * hd.field_bytes));
+        blob.resize((size_t)(hd.pop_bytes + hd.edge_bytes + 2 * hd.field_bytes) + ef0_bytes(h));
         uint64_t sum = 0;
         if (fread(blob.data(), 1, blob.size(), f) != blob.size() || fread(&sum, 1, sizeof sum, f) != sizeof sum)
             why = "short file";
@@ -606,6 +611,8 @@ int lbm_load_checkpoint(lbm_t *h, const char *path)
     q += hd.edge_bytes;
     for (int s = 0; s < 2 && e == cudaSuccess; ++s, q += hd.field_bytes)
         e = cudaMemcpyAsync(h->d_fields[s], q, hd.field_bytes, cudaMemcpyHostToDevice, h->stream);
+    h->edge_f0.resize(ef0_bytes(h) / sizeof(double));
+    memcpy(h->edge_f0.data(), q, ef0_bytes(h));
     if (e == cudaSuccess) e = cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) return io_err(h, LBM_ERR_CUDA, std::string("load_checkpoint: ") + cudaGetErrorString(e));

@@ -262,8 +262,9 @@ LBM_API const char *lbm_last_error(const lbm_t *h);
  *   written; the loader reads `path` and falls back to the copy when it is
  *   missing, short, from another grid or storage precision, or fails its
  *   checksum. The content is this library's own state (populations in
- *   storage precision, boundary reference values, both field slots, step
- *   counters), so a restart continues bit for bit; it is not the byte layout
+ *   storage precision, boundary reference values and the FP64 edge f0 they
+ *   come from, both field slots, step counters), so a restart continues bit
+ *   for bit; it is not the byte layout
  *   of the reference's form='binary' file. Load after lbm_init of a handle
  *   with the same parameters, boundary and motion table. */
 LBM_API int lbm_write_tecplot(lbm_t *h, const char *path, int cycle, int stride_x, int stride_y);

@@ -175,3 +175,18 @@ def test_reference_restart_fallback_and_refusals(gpu_lib, tmp_path):
     with make("fp32", gpu_lib) as d:
         with pytest.raises(LbmError, match="wing count"):
             d.read_flow_field(str(two))
+
+
+def test_checkpoint_carries_the_edge_populations(gpu_lib, tmp_path):
+    """The library's checkpoint keeps the FP64 edge f0, so a handle restored
+    from it (here one initialised with another perturbation) writes the same
+    reference-layout restart file as the handle that saved it."""
+    ck, p1, p2 = (str(tmp_path / n) for n in ("ck.dat", "a.dat", "b.dat"))
+    with make("fp32", gpu_lib) as a:
+        a.run(13)
+        a.save_checkpoint(ck)
+        a.save_flow_field(p1)
+    with make("fp32", gpu_lib, seed=8) as b:
+        b.load_checkpoint(ck)
+        b.save_flow_field(p2)
+    assert open(p1, "rb").read() == open(p2, "rb").read()
