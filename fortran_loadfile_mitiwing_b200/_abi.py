@@ -16,6 +16,8 @@ LBM_ERR_SOLVER = -5
 LBM_ERR_NONFINITE = -6
 LBM_ERR_RANGE = -7
 LBM_ERR_SIZE = -8
+LBM_TIMING_KERNELS = 1
+LBM_TIMING_SPAN = 2
 LBM_RESIDUAL_MAX_ROWS = 16384
 
 LBM_PREC_FP32 = 0

@@ -435,15 +435,18 @@ __global__ void __launch_bounds__(256) ib_assemble(const IBArgs base0, const IBA
         else a.bD[g] = v;
     }
     // half-bandwidth: boxes (<= 6 nodes wide) overlap only for markers closer
-    // than `reach` along the order's key
-    if (tid < BS) {
-        const int srt = blk * BS + tid;
+    // than `reach` along the order's key (ascending in the solve order, so
+    // the markers within reach are a run after srt). 16 threads per marker
+    // of the block scan that run, thread l the markers srt + 1 + l + 16 i.
+    {
+        static_assert(BS * 16 == 256, "16 threads per marker of a block");
+        const int m = tid >> 4, l = tid & 15, srt = blk * BS + m;
         if (srt < n) {
             const double reach = *a.reach;
-            const int4 p = bx[BS + tid];
+            const int4 p = bx[BS + m];
             const double ks = a.key[srt];
             int w = 0;
-            for (int t = srt + 1; t < n && a.key[t] - ks <= reach; ++t)
+            for (int t = srt + 1 + l; t < n && a.key[t] - ks <= reach; t += 16)
                 if (box_overlap(p, mbox(a.mk[a.perm[t]]))) w = t - srt;
             if (w) atomicMax(&wl, w);
         }
@@ -1030,35 +1033,44 @@ __global__ void __launch_bounds__(256) ib_tile_compact(const IBArgs base0, const
     if (t == 255) *a.nsup = before + x;
 }
 
+// One warp per correction tile (8 per CTA): most tiles list a few dozen
+// markers, which a warp sorts as fast as a CTA while holding an eighth of the
+// SM slots the lattice update runs in.
+constexpr int SORT_WARPS = 8;
 template <bool BATCH>
-__global__ void __launch_bounds__(TILE_CAP) ib_tile_sort(const IBArgs base0, const IBArgs *batch, int step0)
+__global__ void __launch_bounds__(32 * SORT_WARPS) ib_tile_sort(const IBArgs base0, const IBArgs *batch, int step0)
 {
     const IBArgs &base = BATCH ? batch[blockIdx.z] : base0;
     const int step_index = factor_step<BATCH>(base, step0);
     if (step_index < 0) return;
     const IBArgs a = member_args(base, step_index);
-    __shared__ int key[TILE_CAP];
-    const int ntile = *a.nsup, t = threadIdx.x;
-    for (int c = blockIdx.x; c < ntile; c += gridDim.x) {
+    __shared__ int keys[SORT_WARPS][TILE_CAP];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int *key = keys[warp];
+    const int ntile = *a.nsup;
+    for (int c = blockIdx.x * SORT_WARPS + warp; c < ntile; c += gridDim.x * SORT_WARPS) {
         int *list = a.tiles + (long long)a.ctile[c] * (TILE_CAP + 1);
         const int m = min(list[0], TILE_CAP);
-        key[t] = t < m ? list[1 + t] : 0x7fffffff;
         int np = 2;   // keys sorted: the power of two at or above the count
         while (np < m) np <<= 1;
-        __syncthreads();
-        // bitonic sort of np keys, ascending (the padding keys stay at the end)
+        for (int t = lane; t < np; t += 32) key[t] = t < m ? list[1 + t] : 0x7fffffff;
+        __syncwarp();
+        // bitonic sort of np keys, ascending (the padding keys stay at the
+        // end); the pairs (t, t ^ stride) of a stage are disjoint
         for (int size = 2; size <= np; size <<= 1)
             for (int stride = size >> 1; stride > 0; stride >>= 1) {
-                const int u = t ^ stride;
-                if (u > t) {
-                    const bool up = (t & size) == 0;
-                    const int x = key[t], y = key[u];
-                    if ((x > y) == up) { key[t] = y; key[u] = x; }
+                for (int t = lane; t < np; t += 32) {
+                    const int u = t ^ stride;
+                    if (u > t) {
+                        const bool up = (t & size) == 0;
+                        const int x = key[t], y = key[u];
+                        if ((x > y) == up) { key[t] = y; key[u] = x; }
+                    }
                 }
-                __syncthreads();
+                __syncwarp();
             }
-        if (t < m) list[1 + t] = key[t];
-        __syncthreads();
+        for (int t = lane; t < m; t += 32) list[1 + t] = key[t];
+        __syncwarp();
     }
 }
 
@@ -1497,8 +1509,8 @@ int launch_factor(lbm_handle *h, int step0, int count, cudaStream_t st)
     ib_factor<false><<<dim3(1, count), FACTOR_THREADS, kFactorSmem, st>>>(a, nullptr, step0);
     ib_tile_scatter<false><<<dim3((h->nseg + 255) / 256, count), 256, 0, st>>>(a, nullptr, step0);
     ib_tile_compact<false><<<dim3(1, count), 256, 0, st>>>(a, nullptr, step0);
-    ib_tile_sort<false><<<dim3(std::min(h->patch_gx() * h->patch_gy(), 148), count), TILE_CAP, 0, st>>>(a, nullptr,
-                                                                                                        step0);
+    const int sort_ctas = std::min((h->patch_gx() * h->patch_gy() + SORT_WARPS - 1) / SORT_WARPS, 148);
+    ib_tile_sort<false><<<dim3(sort_ctas, count), 32 * SORT_WARPS, 0, st>>>(a, nullptr, step0);
     h->launches += h->static_order ? 6 : 7;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
@@ -1589,7 +1601,8 @@ int launch_factor_batch(lbm_handle *const *hs, int ncase, const void *dargs, int
     ib_factor<true><<<dim3(1, count, ncase), FACTOR_THREADS, kFactorSmem, st>>>(IBArgs{}, d, step0);
     ib_tile_scatter<true><<<dim3((ns + 255) / 256, count, ncase), 256, 0, st>>>(IBArgs{}, d, step0);
     ib_tile_compact<true><<<dim3(1, count, ncase), 256, 0, st>>>(IBArgs{}, d, step0);
-    ib_tile_sort<true><<<dim3(std::min(tiles, 148), count, ncase), TILE_CAP, 0, st>>>(IBArgs{}, d, step0);
+    ib_tile_sort<true><<<dim3(std::min((tiles + SORT_WARPS - 1) / SORT_WARPS, 148), count, ncase), 32 * SORT_WARPS, 0,
+                         st>>>(IBArgs{}, d, step0);
     for (int c = 0; c < ncase; ++c) hs[c]->launches += any_order ? 7 : 6;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

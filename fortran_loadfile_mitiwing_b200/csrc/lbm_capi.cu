@@ -285,7 +285,7 @@ int check_status(lbm_handle *h)
 int collect_timing(lbm_handle *h, int count, bool split)
 {
     if (count < 1) return LBM_OK;
-    for (int s = 0; s < count; ++s) {
+    for (int s = 0; s < count && h->timing == LBM_TIMING_KERNELS; ++s) {
         float a = 0, b = 0, c = 0;
         CK(cudaEventElapsedTime(&a, h->ev[4 * s], h->ev[4 * s + 1]), "event time");
         CK(cudaEventElapsedTime(&b, h->ev[4 * s + 2], h->ev[4 * s + 3]), "event time");
@@ -297,8 +297,8 @@ int collect_timing(lbm_handle *h, int count, bool split)
             h->t_ib += a;
             h->t_kf += b;
         }
-        h->t_steps++;
     }
+    h->t_steps += count;
     float span = 0;
     CK(cudaEventElapsedTime(&span, h->ev[0], h->ev[4 * (count - 1) + 3]), "event time");
     h->t_step += span;
@@ -363,7 +363,10 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             h->fields_slot = fs;
             h->fields_step[fs] = h->n;
         }
-        cudaEvent_t *e = h->timing ? &h->ev[4 * slot] : nullptr;
+        // per-step events (LBM_TIMING_KERNELS); with LBM_TIMING_SPAN only the
+        // first step's start and the last step's end of each chunk of steps
+        cudaEvent_t *e = h->timing == LBM_TIMING_KERNELS ? &h->ev[4 * slot] : nullptr;
+        if (h->timing == LBM_TIMING_SPAN && slot == 0) CK(cudaEventRecord(h->ev[0], h->stream), "event");
         // the solve-residual check: on the last step of each factorization
         // batch and on the last step of the call
         const bool check_res = (h->n + 1) % K == 0 || s == nsteps - 1;
@@ -413,6 +416,7 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
                 CK(cudaEventRecord(h->ev_ib, h->side), "event");
                 CK(cudaStreamWaitEvent(h->stream, h->ev_ib, 0), "wait");
             }
+            if (h->timing == LBM_TIMING_SPAN) CK(cudaEventRecord(h->ev[4 * (pending - 1) + 3], h->stream), "event");
             if (rows_out)
                 CK(cudaMemcpyAsync(rows_out + (size_t)(done - pending) * h->row_len, h->d_ring,
                                    sizeof(double) * h->row_len * pending, cudaMemcpyDeviceToHost, h->stream),
@@ -428,6 +432,7 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             CK(cudaEventRecord(h->ev_ib, h->side), "event");
             CK(cudaStreamWaitEvent(h->stream, h->ev_ib, 0), "wait");
         }
+        if (h->timing == LBM_TIMING_SPAN) CK(cudaEventRecord(h->ev[4 * (pending - 1) + 3], h->stream), "event");
         if (rows_out)
             CK(cudaMemcpyAsync(rows_out + (size_t)(done - pending) * h->row_len, h->d_ring,
                                sizeof(double) * h->row_len * pending, cudaMemcpyDeviceToHost, h->stream),
@@ -941,7 +946,7 @@ int lbm_set_timing(lbm_t *h, int enable)
         for (auto &e : h->ev) CK(cudaEventCreate(&e), "event create");
         for (auto &e : h->ev_side) CK(cudaEventCreate(&e), "event create");
     }
-    h->timing = enable ? 1 : 0;
+    h->timing = enable == LBM_TIMING_SPAN ? LBM_TIMING_SPAN : (enable ? LBM_TIMING_KERNELS : 0);
     h->t_step = h->t_ib = h->t_kf = 0;
     h->t_steps = 0;
     return LBM_OK;

@@ -190,11 +190,17 @@ LBM_API int lbm_get_markers(lbm_t *h, double *xb2, double *yb2, double *solve_re
 
 /* Device timing of the step loop, the CUDA-event analogue of the driver's
  * per-phase cpu_time totals (main.f90:355-369, 420-433). With timing on,
- * lbm_step/lbm_run record CUDA events on the handle's stream around the
- * immersed-boundary kernels and around the lattice kernel of every step.
+ * enable = LBM_TIMING_KERNELS (or any other non-zero value but
+ * LBM_TIMING_SPAN): lbm_step/lbm_run record CUDA events on the handle's
+ * streams around the immersed-boundary kernels and around the lattice kernel
+ * of every step. enable = LBM_TIMING_SPAN: only at the start and the end of
+ * each run of up to 2048 steps, so that the steps are timed without the
+ * per-step events in their streams (the kernel totals stay 0). 0: off.
  * lbm_get_timing returns, since the last lbm_set_timing, the summed device
  * milliseconds of the whole steps, of the immersed-boundary kernels and of
  * the lattice kernel, and the number of steps timed (any pointer nullable). */
+#define LBM_TIMING_KERNELS 1
+#define LBM_TIMING_SPAN 2
 LBM_API int lbm_set_timing(lbm_t *h, int enable);
 LBM_API int lbm_get_timing(lbm_t *h, double *step_ms, double *ib_ms, double *lattice_ms, int *steps);
 

@@ -85,6 +85,29 @@ def test_step_and_run_agree_bitwise(gpu_lib):
     np.testing.assert_array_equal(ra, rb)
 
 
+def test_timing_modes(gpu_lib):
+    """LBM_TIMING_SPAN times the steps with events at the ends of the call
+    only (kernel totals stay 0); LBM_TIMING_KERNELS also times the lattice
+    kernel and the IB chain of every step. Neither changes the results."""
+    import ctypes as C
+    case = cases.small_case(precision="fp32", n_steps=100)
+    a, b = Lbm.from_case(case, gpu_lib), Lbm.from_case(case, gpu_lib)
+    ra = a.run(30)
+    out = []
+    for mode in (_abi.LBM_TIMING_SPAN, _abi.LBM_TIMING_KERNELS):
+        assert gpu_lib.lbm_set_timing(b.h, mode) == 0
+        rows = b.run(15)
+        t = [C.c_double() for _ in range(3)]
+        n = C.c_int()
+        gpu_lib.lbm_get_timing(b.h, *(C.byref(x) for x in t), C.byref(n))
+        out.append((rows, [x.value for x in t], n.value))
+    (r1, t1, n1), (r2, t2, n2) = out
+    assert n1 == 15 and n2 == 15
+    assert t1[0] > 0 and t1[1] == 0 and t1[2] == 0
+    assert t2[0] > 0 and t2[1] > 0 and t2[2] > 0
+    np.testing.assert_array_equal(np.concatenate([r1, r2]), ra)
+
+
 def test_launch_count_per_step(gpu_lib):
     """Per step of one rigid wing: the flow chain (interpolation, solve, update
     of the correction tiles, force row) and the lattice kernel; the residual
