@@ -1037,6 +1037,9 @@ __global__ void __launch_bounds__(256) ib_tile_compact(const IBArgs base0, const
 // markers, which a warp sorts as fast as a CTA while holding an eighth of the
 // SM slots the lattice update runs in.
 constexpr int SORT_WARPS = 8;
+// CTAs per step: 256 warps, about the correction tiles of a 1024-marker
+// contour; larger contours loop
+constexpr int SORT_CTAS = 32;
 template <bool BATCH>
 __global__ void __launch_bounds__(32 * SORT_WARPS) ib_tile_sort(const IBArgs base0, const IBArgs *batch, int step0)
 {
@@ -1509,7 +1512,7 @@ int launch_factor(lbm_handle *h, int step0, int count, cudaStream_t st)
     ib_factor<false><<<dim3(1, count), FACTOR_THREADS, kFactorSmem, st>>>(a, nullptr, step0);
     ib_tile_scatter<false><<<dim3((h->nseg + 255) / 256, count), 256, 0, st>>>(a, nullptr, step0);
     ib_tile_compact<false><<<dim3(1, count), 256, 0, st>>>(a, nullptr, step0);
-    const int sort_ctas = std::min((h->patch_gx() * h->patch_gy() + SORT_WARPS - 1) / SORT_WARPS, 148);
+    const int sort_ctas = std::min((h->patch_gx() * h->patch_gy() + SORT_WARPS - 1) / SORT_WARPS, SORT_CTAS);
     ib_tile_sort<false><<<dim3(sort_ctas, count), 32 * SORT_WARPS, 0, st>>>(a, nullptr, step0);
     h->launches += h->static_order ? 6 : 7;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
@@ -1601,8 +1604,8 @@ int launch_factor_batch(lbm_handle *const *hs, int ncase, const void *dargs, int
     ib_factor<true><<<dim3(1, count, ncase), FACTOR_THREADS, kFactorSmem, st>>>(IBArgs{}, d, step0);
     ib_tile_scatter<true><<<dim3((ns + 255) / 256, count, ncase), 256, 0, st>>>(IBArgs{}, d, step0);
     ib_tile_compact<true><<<dim3(1, count, ncase), 256, 0, st>>>(IBArgs{}, d, step0);
-    ib_tile_sort<true><<<dim3(std::min((tiles + SORT_WARPS - 1) / SORT_WARPS, 148), count, ncase), 32 * SORT_WARPS, 0,
-                         st>>>(IBArgs{}, d, step0);
+    ib_tile_sort<true><<<dim3(std::min((tiles + SORT_WARPS - 1) / SORT_WARPS, SORT_CTAS), count, ncase),
+                         32 * SORT_WARPS, 0, st>>>(IBArgs{}, d, step0);
     for (int c = 0; c < ncase; ++c) hs[c]->launches += any_order ? 7 : 6;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }
