@@ -115,3 +115,23 @@ def test_batch_refuses_mixed_precision(gpu_lib):
         with pytest.raises(LbmError):
             b.add(a)                     # already in the batch
         assert len(b) == 1 and b.lib.lbm_batch_count(b.b) == 1
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp16"])
+def test_odd_row_chunks_equal_alone(gpu_lib, precision):
+    """The lattice update pairs rows of a chunk for the paired FP32
+    instructions; with 5 or 7 rows per CTA every chunk ends with an unpaired
+    row, and a case with an odd number of interior rows ends the lattice with
+    one: each node's arithmetic is the same in either half of a pair, so the
+    results stay bit-for-bit those of the case alone (8 rows per CTA)."""
+    specs = SPECS[:2] + [dict(nx=100, ny=61, chord=20, pivot=(35, 31), markers=36, heave=0.2, pitch_deg=15.0,
+                              st=0.3, seed=17)]
+    for rows in (5, 7):
+        together = build(precision, 40, specs=specs, lib=gpu_lib)
+        alone = build(precision, 40, specs=specs, lib=gpu_lib)
+        with Batch(together) as b:
+            b.set_rows(rows)
+            rows_b = b.run(21)
+        for c, (t, a) in enumerate(zip(together, alone)):
+            np.testing.assert_array_equal(rows_b[c], a.run(21), err_msg=f"rows {rows} case {c}")
+            np.testing.assert_array_equal(t.populations(), a.populations(), err_msg=f"rows {rows} case {c}")
