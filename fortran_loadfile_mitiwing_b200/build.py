@@ -63,6 +63,25 @@ def build(force=False, verbose=False):
     return LIB
 
 
+DRIVER_SRC = os.path.join(CSRC, "lbm_main.cpp")
+DRIVER = os.path.join(LIBDIR, "lbm_main")
+
+
+def build_driver(force=False, verbose=False):
+    """Compiles the driver program (main.f90's loop over the C ABI) with the
+    host compiler, linked against the library in the same directory."""
+    lib = build(force=force, verbose=verbose)
+    if not force and os.path.exists(DRIVER) and os.path.getmtime(DRIVER) >= max(
+            os.path.getmtime(DRIVER_SRC), os.path.getmtime(lib)):
+        return DRIVER
+    cmd = [os.environ.get("CXX", "g++"), "-O2", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"),
+           DRIVER_SRC, "-o", DRIVER, "-L", LIBDIR, "-llbmb200", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return DRIVER
+
+
 def build_oracle(verbose=False):
     """Builds the CPU oracle (test infrastructure) with its Makefile."""
     cmd = ["make", "-s", "-C", os.path.join(ROOT, "oracle")]
@@ -73,3 +92,4 @@ def build_oracle(verbose=False):
 
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True)
+    build_driver(verbose=True)

@@ -66,11 +66,20 @@ double feq(double rh, double u1, double v1, int k)
 std::mutex g_alloc_mu;
 std::unordered_map<void *, std::pair<lbm_handle *, size_t>> g_allocs;
 
+// Every allocation is zero-filled on the handle's stream, ahead of all work
+// that uses it (the other streams are ordered after the main stream's
+// position by events), so that no kernel can see data a freed allocation of
+// an earlier handle left in the same memory.
 template <typename P> cudaError_t dmalloc(lbm_handle *h, P **p, size_t bytes)
 {
     void *q = nullptr;
-    const cudaError_t e = cudaMalloc(&q, bytes);
+    cudaError_t e = cudaMalloc(&q, bytes);
     if (e != cudaSuccess) return e;
+    e = h->stream ? cudaMemsetAsync(q, 0, bytes, h->stream) : cudaMemset(q, 0, bytes);
+    if (e != cudaSuccess) {
+        cudaFree(q);
+        return e;
+    }
     *p = (P *)q;
     std::lock_guard<std::mutex> lock(g_alloc_mu);
     g_allocs[q] = {h, bytes};
