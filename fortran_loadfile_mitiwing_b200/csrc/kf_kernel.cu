@@ -170,9 +170,11 @@ constexpr int TW = 256;        // strip width (threads per CTA)
 // pipeline stages: 2-byte storage halves the bytes of a stage, so it keeps
 // twice the stages to hold the same bytes in flight
 template <typename T> __host__ __device__ constexpr int tma_stages() { return sizeof(T) == 2 ? 2 * LBM_KF_STAGES : LBM_KF_STAGES; }
-// Resident CTAs per SM the register budget is sized for. Three leave room on
-// each SM for the immersed-boundary kernels that run beside the lattice
-// update; four make the lattice kernel alone ~2% faster but starve them.
+// Resident CTAs per SM the register budget is sized for (64 registers a
+// thread at four). Four keep more rows in flight than three, which leave
+// registers free for the immersed-boundary CTAs beside the lattice update
+// but measured slower beside them as well (FP32 0.1227 against 0.1183 ms a
+// step on 4096x2048).
 constexpr int KF_MINB = LBM_KF_MINB;
 // CTAs per SM the staged kernel is compiled for: FP64 storage keeps 3 (its
 // ring alone, ~75 KB a CTA, allows no more), the others LBM_KF_MINB
