@@ -76,7 +76,9 @@ def large_case(args, n_steps, precision=None):
 def workload(args):
     return {
         "workload": f"heave+pitch NACA 0012, {args.nx}x{args.ny} D2Q9 MRT lattice, chord {args.ny // 4} lu, "
-                    f"{args.ny // 2} markers, Re 1000, St 0.3, U0 0.05, 4-point delta",
+                    f"{args.ny // 2} markers in the reference's boundary.dat layout (x uniform; cosine spacing "
+                    f"makes the marker system singular), live boundary_condition1 outer boundary, Re 1000, "
+                    f"St 0.3, U0 0.05, 4-point delta",
         "nx": args.nx, "ny": args.ny, "markers": args.ny // 2, "storage": args.precision,
         "l2": "inputs larger than L2 (two population buffers of 9*nx*ny elements)",
         "parallelism": "replicas",
@@ -323,22 +325,33 @@ def run_e2e(args, lib):
     k = args.steps
     case = large_case(args, n_steps=k + 8)
     nn = args.nx * args.ny
+    marks = []
     t0 = time.perf_counter()
     s = Lbm(case.params, lib)
+    marks.append(("create", time.perf_counter()))
     for wi, (x, y) in enumerate(case.contours, start=1):
         s.set_boundary(wi, x, y)
     s.set_motion_table(case.table)
+    marks.append(("boundary_motion", time.perf_counter()))
     s.init(case.du, case.dv)
+    marks.append(("init", time.perf_counter()))
     rows = s.run(k)
+    marks.append(("run", time.perf_counter()))
     rho, u, v = s.fields()
+    marks.append(("fields", time.perf_counter()))
     el = time.perf_counter() - t0
     assert rows.shape[0] == k and np.all(np.isfinite(rows))
     s.close()
+    stages, prev = {}, t0
+    for name, t in marks:
+        stages[name] = (t - prev) * 1e3
+        prev = t
     # host -> device: motion table, contours and the perturbation du, dv (the
     # initial populations and fields are built on the device from them)
     h2d = (case.table.nbytes + 2 * nn * 8 + sum(x.nbytes + y.nbytes for x, y in case.contours)) / k
     d2h = s.row_len * 8 + 3 * nn * 8 / k
     return {"value": nn * k / el / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "stages_ms": stages,
             "note": "wall clock around the C-ABI calls (create, boundary, motion table, init, run, fields); "
                     "set-up upload and final fields amortised over the steps"}
 

@@ -16,6 +16,7 @@ LBM_ERR_SOLVER = -5
 LBM_ERR_NONFINITE = -6
 LBM_ERR_RANGE = -7
 LBM_ERR_SIZE = -8
+LBM_ERR_INDEX = -9
 LBM_TIMING_KERNELS = 1
 LBM_TIMING_SPAN = 2
 LBM_RESIDUAL_MAX_ROWS = 16384
@@ -32,7 +33,19 @@ LBM_DELTA_PESKIN4 = 0
 LBM_DELTA_SMOOTH = 1
 
 STATUS_NAMES = {0: "LBM_OK", 1: "LBM_DONE", -1: "LBM_ERR_ARG", -2: "LBM_ERR_CUDA", -3: "LBM_ERR_STATE",
-                -4: "LBM_ERR_IO", -5: "LBM_ERR_SOLVER", -6: "LBM_ERR_NONFINITE", -7: "LBM_ERR_RANGE"}
+                -4: "LBM_ERR_IO", -5: "LBM_ERR_SOLVER", -6: "LBM_ERR_NONFINITE", -7: "LBM_ERR_RANGE",
+                -8: "LBM_ERR_SIZE", -9: "LBM_ERR_INDEX"}
+
+# device status bits of the kernels (csrc/lbm_common.cuh), for
+# lbm_describe_status
+LBM_ST_RANGE = 0x1
+LBM_ST_SOLVER = 0x2
+LBM_ST_NONFINITE = 0x4
+LBM_ST_OVERFLOW = 0x8
+LBM_ST_TIMEOUT = 0x10
+LBM_ST_INDEX_KERNELS = {0x100: "ib_interp", 0x200: "ib_assemble", 0x400: "ib_factor", 0x800: "ib_solve",
+                        0x1000: "ib_tile_scatter", 0x2000: "ib_tile_sort", 0x4000: "ib_tile_update",
+                        0x8000: "ib_forces", 0x10000: "ib_residual", 0x20000: "kf_tma"}
 
 
 class LbmParams(C.Structure):
@@ -71,6 +84,7 @@ ABI = {
     "lbm_get_populations": (C.c_int, [_P, _D]),
     "lbm_set_populations": (C.c_int, [_P, _D]),
     "lbm_residual": (C.c_int, [_P, _D]),
+    "lbm_mass": (C.c_int, [_P, _D]),
     "lbm_get_markers": (C.c_int, [_P, _D, _D, _D, C.POINTER(C.c_int)]),
     "lbm_set_timing": (C.c_int, [_P, C.c_int]),
     "lbm_get_timing": (C.c_int, [_P, _D, _D, _D, C.POINTER(C.c_int)]),
@@ -79,6 +93,8 @@ ABI = {
     "lbm_step_index": (C.c_int, [_P]),
     "lbm_device_bytes": (C.c_int, [_P, C.POINTER(C.c_longlong)]),
     "lbm_last_error": (C.c_char_p, [_P]),
+    "lbm_describe_status": (C.c_int, [C.c_uint, C.c_char_p, C.c_int]),
+    "lbm_device_check": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "lbm_write_tecplot": (C.c_int, [_P, C.c_char_p, C.c_int, C.c_int, C.c_int]),
     "lbm_write_tecplot_fields": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                            C.c_double, C.c_double, C.c_int, C.c_int, _D, _D, _D, C.c_int, C.c_int,

@@ -257,7 +257,9 @@ __global__ void __launch_bounds__(256) ib_interp(const IBArgs a0, const IBArgs *
     const int k = blockIdx.x * 8 + warp;
     if (k >= a.nseg) return;
     const Marker m = a.mk[k];
-    const int nbx = m.i2 - m.i1 + 1, nby = m.j2 - m.j1 + 1;
+    const bool ok = box_in_bounds(m.i1, m.i2, m.j1, m.j2, a.nx, a.ny);
+    if (!ok && lane == 0) atomicOr(a.status, LBM_ST_INDEX_INTERP);
+    const int nbx = ok ? m.i2 - m.i1 + 1 : 0, nby = ok ? m.j2 - m.j1 + 1 : 0;
     const int nn = nbx > 0 && nby > 0 ? nbx * nby : 0;
     double su = 0.0, sv = 0.0;
     for (int t = lane; t < nn; t += 32) {
@@ -298,6 +300,41 @@ __device__ __forceinline__ bool box_overlap(int4 p, int4 q)
 }
 
 __device__ __forceinline__ int4 mbox(const Marker &m) { return make_int4(m.i1, m.i2, m.j1, m.j2); }
+
+// a marker as make_marker leaves it: support box within bounds (an empty
+// box included) and a wing index of the case
+__device__ __forceinline__ bool marker_ok(const IBArgs &a, const Marker &m)
+{
+    return box_in_bounds(m.i1, m.i2, m.j1, m.j2, a.nx, a.ny) && m.wing >= 0 && m.wing < a.nwing;
+}
+
+// the marker at position srt of the solve order, or null (and the kernel's
+// status bit set) when the order holds an index outside the markers or the
+// marker is not as make_marker leaves it
+__device__ __forceinline__ const Marker *sorted_marker(const IBArgs &a, int srt, unsigned bit)
+{
+    const int k = a.perm[srt];
+    if (k < 0 || k >= a.nseg || !marker_ok(a, a.mk[k])) {
+        atomicOr(a.status, bit);
+        return nullptr;
+    }
+    return a.mk + k;
+}
+
+// marker at position s of the solve order, or -1 (and the kernel's status
+// bit set) when the order holds an index outside the markers
+__device__ __forceinline__ int order_at(const IBArgs &a, int s, unsigned bit)
+{
+    const int k = a.perm[s];
+    if (k < 0 || k >= a.nseg) {
+        atomicOr(a.status, bit);
+        return -1;
+    }
+    return k;
+}
+
+// tiles of the patch grid (the tile lists of one slot)
+__device__ __forceinline__ int patch_tiles(const IBArgs &a) { return (int)(a.st_tiles / (TILE_CAP + 1)); }
 
 // time and motion columns of this step's force.dat row (solution.f90:350-375)
 __device__ void write_header(const IBArgs &a, const double *row, double time, int ring_slot)
@@ -403,14 +440,15 @@ __global__ void __launch_bounds__(256) ib_assemble(const IBArgs base0, const IBA
         const int m = q / 12, c = q % 12, srt = (blk - 1) * BS + m;
         double v = 0.0;
         if (srt >= 0 && srt < n) {
-            const Marker &mm = a.mk[a.perm[srt]];
-            v = c < 6 ? mm.phx[c] : mm.phy[c - 6];
+            const Marker *mm = sorted_marker(a, srt, LBM_ST_INDEX_ASSEMBLE);
+            if (mm) v = c < 6 ? mm->phx[c] : mm->phy[c - 6];
         }
         ph[m][c] = v;
     }
     for (int m = tid; m < 2 * BS; m += blockDim.x) {
         const int srt = (blk - 1) * BS + m;
-        bx[m] = (srt >= 0 && srt < n) ? mbox(a.mk[a.perm[srt]]) : make_int4(1, 0, 1, 0);
+        const Marker *mm = (srt >= 0 && srt < n) ? sorted_marker(a, srt, LBM_ST_INDEX_ASSEMBLE) : nullptr;
+        bx[m] = mm ? mbox(*mm) : make_int4(1, 0, 1, 0);
     }
     __syncthreads();
     for (int q = tid; q < 2 * BS * BS; q += blockDim.x) {
@@ -446,8 +484,10 @@ __global__ void __launch_bounds__(256) ib_assemble(const IBArgs base0, const IBA
             const int4 p = bx[BS + m];
             const double ks = a.key[srt];
             int w = 0;
-            for (int t = srt + 1 + l; t < n && a.key[t] - ks <= reach; t += 16)
-                if (box_overlap(p, mbox(a.mk[a.perm[t]]))) w = t - srt;
+            for (int t = srt + 1 + l; t < n && a.key[t] - ks <= reach; t += 16) {
+                const Marker *mt = sorted_marker(a, t, LBM_ST_INDEX_ASSEMBLE);
+                if (mt && box_overlap(p, mbox(*mt))) w = t - srt;
+            }
             if (w) atomicMax(&wl, w);
         }
     }
@@ -554,7 +594,8 @@ __device__ void dense_factor(const IBArgs &a, int *bad)
     double *L = a.B;
     for (long long q = tid; q < (long long)n * n; q += nt) {
         const int k = (int)(q / n), l = (int)(q % n);
-        L[q] = bval(a.mk[a.perm[k]], a.mk[a.perm[l]]);
+        const Marker *mk = sorted_marker(a, k, LBM_ST_INDEX_FACTOR), *ml = sorted_marker(a, l, LBM_ST_INDEX_FACTOR);
+        L[q] = mk && ml ? bval(*mk, *ml) : (k == l ? 1.0 : 0.0);
     }
     __syncthreads();
     for (int k = 0; k < n; ++k) {
@@ -634,6 +675,10 @@ __global__ void __launch_bounds__(FACTOR_THREADS) ib_factor(const IBArgs base0, 
         int b0 = 1 << 30, b1 = 1 << 30, b2 = -1, b3 = -1;
         for (int k = tid; k < n; k += blockDim.x) {
             const int4 q = mbox(a.mk[k]);
+            if (!box_in_bounds(q.x, q.y, q.z, q.w, a.nx, a.ny)) {
+                atomicOr(a.status, LBM_ST_INDEX_FACTOR);
+                continue;
+            }
             if (q.y >= q.x && q.w >= q.z) { b0 = min(b0, q.x); b1 = min(b1, q.z); b2 = max(b2, q.y); b3 = max(b3, q.w); }
         }
         for (int off = 16; off; off >>= 1) {
@@ -835,20 +880,24 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a0, const
     if (n == 0) return;
     if (a.fmode[0]) {   // dense factor
         for (int s = tid; s < n; s += nt) {
-            X[s] = a.rhs[a.perm[s]];
-            X[n + s] = a.rhs[n + a.perm[s]];
+            const int k = order_at(a, s, LBM_ST_INDEX_SOLVE);
+            X[s] = k >= 0 ? a.rhs[k] : 0.0;
+            X[n + s] = k >= 0 ? a.rhs[n + k] : 0.0;
         }
         __syncthreads();
         dense_tri(a, X);
         for (int s = tid; s < n; s += nt) {
-            a.y[a.perm[s]] = X[s];
-            a.y[n + a.perm[s]] = X[n + s];
+            const int k = order_at(a, s, LBM_ST_INDEX_SOLVE);
+            if (k < 0) continue;
+            a.y[k] = X[s];
+            a.y[n + k] = X[n + s];
         }
         return;
     }
     for (int s = tid; s < nb * BS; s += nt) {
-        X[2 * s] = s < n ? a.rhs[a.perm[s]] : 0.0;
-        X[2 * s + 1] = s < n ? a.rhs[n + a.perm[s]] : 0.0;
+        const int k = s < n ? order_at(a, s, LBM_ST_INDEX_SOLVE) : -1;
+        X[2 * s] = k >= 0 ? a.rhs[k] : 0.0;
+        X[2 * s + 1] = k >= 0 ? a.rhs[n + k] : 0.0;
     }
     const double *Gf = a.gf;
     uint32_t parity = 0;
@@ -965,8 +1014,10 @@ __global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a0, const
         return;
     }
     for (int s = tid; s < n; s += nt) {
-        a.y[a.perm[s]] = X[2 * s];
-        a.y[n + a.perm[s]] = X[2 * s + 1];
+        const int k = order_at(a, s, LBM_ST_INDEX_SOLVE);
+        if (k < 0) continue;
+        a.y[k] = X[2 * s];
+        a.y[n + k] = X[2 * s + 1];
     }
 }
 
@@ -988,7 +1039,18 @@ __global__ void __launch_bounds__(256) ib_tile_scatter(const IBArgs base0, const
     if (k >= a.nseg) return;
     const PatchInfo pi = *a.pinfo;
     const int4 q = mbox(a.mk[k]);
+    if (!box_in_bounds(q.x, q.y, q.z, q.w, a.nx, a.ny)) {
+        atomicOr(a.status, LBM_ST_INDEX_SCATTER);
+        return;
+    }
     if (q.y < q.x || q.w < q.z || pi.w <= 0) return;
+    // the box lies in the patch rectangle (its bounding box), which the tile
+    // grid covers; a box or rectangle that says otherwise is not indexed
+    if (q.x < pi.i0 || q.z < pi.j0 || q.y >= pi.i0 + a.tiles_x * TILE ||
+        (long long)((q.w - pi.j0) / TILE + 1) * a.tiles_x > patch_tiles(a)) {
+        atomicOr(a.status, LBM_ST_INDEX_SCATTER);
+        return;
+    }
     const int tx0 = (q.x - pi.i0) / TILE, tx1 = (q.y - pi.i0) / TILE;
     const int ty0 = (q.z - pi.j0) / TILE, ty1 = (q.w - pi.j0) / TILE;
     for (int ty = ty0; ty <= ty1; ++ty)
@@ -1050,9 +1112,19 @@ __global__ void __launch_bounds__(32 * SORT_WARPS) ib_tile_sort(const IBArgs bas
     __shared__ int keys[SORT_WARPS][TILE_CAP];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     int *key = keys[warp];
-    const int ntile = *a.nsup;
+    const int nt = patch_tiles(a);
+    int ntile = *a.nsup;
+    if (ntile < 0 || ntile > nt) {
+        if (lane == 0) atomicOr(a.status, LBM_ST_INDEX_SORT);
+        ntile = 0;
+    }
     for (int c = blockIdx.x * SORT_WARPS + warp; c < ntile; c += gridDim.x * SORT_WARPS) {
-        int *list = a.tiles + (long long)a.ctile[c] * (TILE_CAP + 1);
+        const int tile = a.ctile[c];
+        if (tile < 0 || tile >= nt) {
+            if (lane == 0) atomicOr(a.status, LBM_ST_INDEX_SORT);
+            continue;
+        }
+        int *list = a.tiles + (long long)tile * (TILE_CAP + 1);
         const int m = min(list[0], TILE_CAP);
         int np = 2;   // keys sorted: the power of two at or above the count
         while (np < m) np <<= 1;
@@ -1087,11 +1159,21 @@ __global__ void __launch_bounds__(256) ib_forces(const IBArgs a0, const IBArgs *
     const IBArgs &a = BATCH ? batch[blockIdx.z] : a0;
     __shared__ double red[8][NPART];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int ntile = a.nseg > 0 ? *a.nsup : 0;
+    const int nt = patch_tiles(a);
+    int ntile = a.nseg > 0 ? *a.nsup : 0;
+    if (ntile < 0 || ntile > nt) {
+        if (threadIdx.x == 0) atomicOr(a.status, LBM_ST_INDEX_FORCES);
+        ntile = 0;
+    }
     for (int w = 0; w < a.nwing; ++w) {
         double s0 = 0, s1 = 0, s2 = 0;
         for (int c = threadIdx.x; c < ntile; c += blockDim.x) {
-            const double *p = a.partial + (long long)a.ctile[c] * NPART + 3 * w;
+            const int tile = a.ctile[c];
+            if (tile < 0 || tile >= nt) {
+                atomicOr(a.status, LBM_ST_INDEX_FORCES);
+                continue;
+            }
+            const double *p = a.partial + (long long)tile * NPART + 3 * w;
             s0 += p[0]; s1 += p[1]; s2 += p[2];
         }
 #pragma unroll
@@ -1140,16 +1222,20 @@ __global__ void __launch_bounds__(256) ib_residual(const IBArgs a0, const IBArgs
     const int n = a.nseg, s = blockIdx.x * 8 + warp;
     const int nblk = (n + 7) / 8;
     if ((int)blockIdx.x >= nblk) return;    // batched launches size the grid for the largest case
-    const int hw = (int)a.solve_res[1];
+    const int hw = min(max((int)a.solve_res[1], 0), n);
     double rnum = 0.0, rden = 0.0;
-    if (s < n) {
-        const int ks = a.perm[s];
+    const int ks = s < n ? order_at(a, s, LBM_ST_INDEX_RESIDUAL) : -1;
+    if (ks >= 0) {
         const Marker &ms = a.mk[ks];
+        const bool ok_s = marker_ok(a, ms);
+        if (!ok_s && lane == 0) atomicOr(a.status, LBM_ST_INDEX_RESIDUAL);
         double b0 = 0.0, b1 = 0.0;
-        for (int t = s - hw + lane; t <= s + hw; t += 32) {
+        for (int t = s - hw + lane; t <= s + hw && ok_s; t += 32) {
             if (t < 0 || t >= n) continue;
-            const int l = a.perm[t];
-            const double b = bval(ms, a.mk[l]);
+            const Marker *ml = sorted_marker(a, t, LBM_ST_INDEX_RESIDUAL);
+            if (!ml) continue;
+            const int l = (int)(ml - a.mk);
+            const double b = bval(ms, *ml);
             b0 += b * a.y[l];
             b1 += b * a.y[n + l];
         }
@@ -1223,8 +1309,13 @@ __global__ void __launch_bounds__(256) ib_tile_update(const IBArgs a0, const IBA
     __shared__ double sph[256][12];
     __shared__ double sy[256][2];
     __shared__ int swing[256];
+    const int nt = patch_tiles(a);
     const int ntile = *a.nsup;
     if (ntile == 0) return;   // no correction tile
+    if (ntile < 0 || ntile > nt) {
+        if (threadIdx.x == 0) atomicOr(a.status, LBM_ST_INDEX_TILE);
+        return;
+    }
     const PatchInfo pi = *a.pinfo;
     const T *__restrict__ fin = (const T *)kf.fin;
     const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
@@ -1233,12 +1324,22 @@ __global__ void __launch_bounds__(256) ib_tile_update(const IBArgs a0, const IBA
     // particular order; each tile's result depends on the tile only)
     for (int c = blockIdx.x; c < ntile; c += gridDim.x) {
         const int tile = a.ctile[c];
+        if (tile < 0 || tile >= nt) {   // the same for every thread of the CTA
+            if (threadIdx.x == 0) atomicOr(a.status, LBM_ST_INDEX_TILE);
+            continue;
+        }
         const int ti0 = (tile % a.tiles_x) * TILE, tj0 = (tile / a.tiles_x) * TILE;
         const int *tlist = a.tiles + (long long)tile * (TILE_CAP + 1);
         const int listed = tlist[0];
         const int li = ti0 + tx, lj = tj0 + ty;                    // patch-relative
         const int gi = pi.i0 + li, gj = pi.j0 + lj;                // 0-based node
-        const bool active = li < pi.w && lj < pi.h;
+        bool active = li < pi.w && lj < pi.h;
+        // the patch rectangle is the bounding box of the support boxes, all
+        // interior nodes; a node outside the interior is not updated here
+        if (active && (gi < 1 || gi > kf.nx - 2 || gj < 1 || gj > kf.ny - 2)) {
+            atomicOr(a.status, LBM_ST_INDEX_TILE);
+            active = false;
+        }
         const int ta = pi.i0 + ti0, tb = ta + TILE - 1, sa_ = pi.j0 + tj0, sb_ = sa_ + TILE - 1;
         // the node's streamed populations first: their loads overlap the
         // staging of the markers
@@ -1251,13 +1352,20 @@ __global__ void __launch_bounds__(256) ib_tile_update(const IBArgs a0, const IBA
             if (threadIdx.x == 0) nlist = listed;
             if ((int)threadIdx.x < listed) {
                 const int k = tlist[1 + threadIdx.x];
-                const Marker &m = a.mk[k];
-                sbox[threadIdx.x] = mbox(m);
+                if (k >= 0 && k < a.nseg && marker_ok(a, a.mk[k])) {
+                    const Marker &m = a.mk[k];
+                    sbox[threadIdx.x] = mbox(m);
 #pragma unroll
-                for (int q = 0; q < 6; ++q) { sph[threadIdx.x][q] = m.phx[q]; sph[threadIdx.x][6 + q] = m.phy[q]; }
-                sy[threadIdx.x][0] = a.y[k];
-                sy[threadIdx.x][1] = a.y[a.nseg + k];
-                swing[threadIdx.x] = m.wing;
+                    for (int q = 0; q < 6; ++q) { sph[threadIdx.x][q] = m.phx[q]; sph[threadIdx.x][6 + q] = m.phy[q]; }
+                    sy[threadIdx.x][0] = a.y[k];
+                    sy[threadIdx.x][1] = a.y[a.nseg + k];
+                    swing[threadIdx.x] = m.wing;
+                } else {   // not staged: an empty box meets no node
+                    atomicOr(a.status, LBM_ST_INDEX_TILE);
+                    sbox[threadIdx.x] = make_int4(1, 0, 1, 0);
+                    sy[threadIdx.x][0] = sy[threadIdx.x][1] = 0.0;
+                    swing[threadIdx.x] = 0;
+                }
             }
             __syncthreads();
             if (active) {
@@ -1278,8 +1386,12 @@ __global__ void __launch_bounds__(256) ib_tile_update(const IBArgs a0, const IBA
                 bool hit = false;
                 int4 q = make_int4(1, 0, 1, 0);
                 if (k < a.nseg) {
-                    q = mbox(a.mk[k]);
-                    hit = q.x <= tb && q.y >= ta && q.z <= sb_ && q.w >= sa_ && q.y >= q.x;
+                    if (marker_ok(a, a.mk[k])) {
+                        q = mbox(a.mk[k]);
+                        hit = q.x <= tb && q.y >= ta && q.z <= sb_ && q.w >= sa_ && q.y >= q.x;
+                    } else {
+                        atomicOr(a.status, LBM_ST_INDEX_TILE);
+                    }
                 }
                 const unsigned bal = __ballot_sync(0xffffffffu, hit);
                 if (lane == 0) wsum[warp] = __popc(bal);

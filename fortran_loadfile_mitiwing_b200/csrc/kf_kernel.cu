@@ -32,7 +32,12 @@ __device__ __forceinline__ bool corr_tile(const KFArgs<C> &a, const PatchInfo &r
 {
     const unsigned li = (unsigned)(i - r.i0), lj = (unsigned)(j - r.j0);
     if (li >= (unsigned)r.w || lj >= (unsigned)r.h) return false;
-    return a.tiles[(long long)((lj >> 4) * a.tiles_x + (li >> 4)) * a.tile_stride] > 0;
+    const unsigned tx = li >> 4, t = (lj >> 4) * (unsigned)a.tiles_x + tx;
+    if (tx >= (unsigned)a.tiles_x || t >= (unsigned)a.tiles_n) {   // a rectangle larger than the tile grid
+        atomicOr(a.status, LBM_ST_INDEX_LATTICE);
+        return false;
+    }
+    return a.tiles[(long long)t * a.tile_stride] > 0;
 }
 
 // node-level device functions: lbm_node.cuh
@@ -594,7 +599,77 @@ __global__ void residual_kernel(const C *__restrict__ fa, const C *__restrict__ 
     }
 }
 
+// Global mass check (FP64): the sum over every node and direction of the
+// stored deviations g = f - w, whose total plus nx*ny (the weights sum to 1
+// per node) is the mass sum_ij sum_k f_k. Each CTA sums a fixed set of rows
+// in a fixed order; the last CTA to finish adds the CTA partials in CTA
+// order, so the result does not depend on scheduling. The reference's own
+// reduction over the lattice is erranalysis (solution.f90:102-109).
+constexpr int MASS_BLOCKS = 296, MASS_THREADS = 256;
+template <typename T>
+__global__ void __launch_bounds__(MASS_THREADS) mass_kernel(const T *__restrict__ f, int nx, int ny, int pitch,
+                                                            long long plane, double *__restrict__ part,
+                                                            unsigned *__restrict__ counter)
+{
+    __shared__ double red[MASS_THREADS / 32];
+    __shared__ bool amlast;
+    double s = 0.0;
+    for (int j = blockIdx.x; j < ny; j += gridDim.x)
+        for (int i = threadIdx.x; i < nx; i += blockDim.x) {
+            const T *p = f + (long long)j * pitch + i;
+            double t = 0.0;
+#pragma unroll
+            for (int k = 0; k < 9; ++k) t += (double)Store<T>::ld(p + k * plane);
+            s += t;
+        }
+    for (int off = 16; off; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) red[wid] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int w = 0; w < MASS_THREADS / 32; ++w) t += red[w];
+        part[blockIdx.x] = t;
+        __threadfence();
+        amlast = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!amlast) return;
+    __threadfence();
+    if (threadIdx.x == 0) {
+        double t = 0.0;
+        for (int b = 0; b < (int)gridDim.x; ++b) t += __ldcg(part + b);
+        part[MASS_BLOCKS] = t;
+        *counter = 0u;
+    }
+}
+
 }  // namespace
+
+// the deviation sum of the populations in `fsrc` into h->d_mass[MASS_BLOCKS],
+// on stream st (the caller copies it back)
+int launch_mass(lbm_handle *h, const void *fsrc, cudaStream_t st)
+{
+    switch (h->prec) {
+    case LBM_PREC_FP32:
+        mass_kernel<float><<<MASS_BLOCKS, MASS_THREADS, 0, st>>>((const float *)fsrc, h->nx, h->ny, h->pitch, h->plane, h->d_mass, h->d_mcount);
+        break;
+    case LBM_PREC_FP64:
+        mass_kernel<double><<<MASS_BLOCKS, MASS_THREADS, 0, st>>>((const double *)fsrc, h->nx, h->ny, h->pitch, h->plane, h->d_mass, h->d_mcount);
+        break;
+    case LBM_PREC_FP16:
+        mass_kernel<__half><<<MASS_BLOCKS, MASS_THREADS, 0, st>>>((const __half *)fsrc, h->nx, h->ny, h->pitch, h->plane, h->d_mass, h->d_mcount);
+        break;
+    case LBM_PREC_BF16:
+        mass_kernel<__nv_bfloat16><<<MASS_BLOCKS, MASS_THREADS, 0, st>>>((const __nv_bfloat16 *)fsrc, h->nx, h->ny, h->pitch, h->plane, h->d_mass, h->d_mcount);
+        break;
+    default: return -1;
+    }
+    h->launches += 1;
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
+
+int mass_slots() { return MASS_BLOCKS + 1; }
 
 template <typename T, typename C>
 int launch_kf_multi_t(const void *cases, const int4 *table, int nentries, bool fields, bool cons0, cudaStream_t st)

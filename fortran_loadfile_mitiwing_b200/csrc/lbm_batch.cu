@@ -539,6 +539,28 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
     }
     // the rows of the last steps (also when every case ended before nsteps)
     if (pending > 0 && rc == LBM_OK) rc = flush();
+    // the global mass of every case that ran, at the end of the run (FP64 on
+    // the device; a non-finite mass fails that case)
+    if (rc == LBM_OK) {
+        std::vector<double> dsum(nc, 0.0);
+        for (int c = 0; c < nc && rc == LBM_OK; ++c)
+            if (done[c] > 0) rc = handle_mass_launch(b->cases[c], b->main, &dsum[c]);
+        if (rc == LBM_OK) {
+            BCK(cudaStreamSynchronize(b->main), "sync mass");
+            for (int c = 0; c < nc; ++c) {
+                const int st = done[c] > 0 ? handle_mass_result(b->cases[c], dsum[c]) : LBM_OK;
+                if (st) {
+                    b->status[c] = st;
+                    if (rc == LBM_OK) {
+                        rc = st;
+                        b->err = std::string("batch: case ") + std::to_string(c) + ": " + b->cases[c]->err;
+                    }
+                }
+            }
+        } else {
+            b->err = std::string("batch: mass check: ") + b->cases[0]->err;
+        }
+    }
     // leave every stream idle: the cases' own calls follow on their streams
     sync_streams(b);
     restore();

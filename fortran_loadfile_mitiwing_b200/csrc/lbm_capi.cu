@@ -271,6 +271,55 @@ int ensure_ib(lbm_handle *h)
     return LBM_OK;
 }
 
+}  // namespace
+
+// The error code and message of a device status word (the LBM_ST_* bits the
+// kernels set); LBM_OK and "" for 0. An index error is reported first: the
+// kernel that saw it skipped the access, so the step's results are not valid.
+int status_error(unsigned st, std::string &msg)
+{
+    msg.clear();
+    if (!st) return LBM_OK;
+    if (st & LBM_ST_INDEX_MASK) {
+        static const struct {
+            unsigned bit;
+            const char *kernel;
+        } names[] = {{LBM_ST_INDEX_INTERP, "ib_interp"},     {LBM_ST_INDEX_ASSEMBLE, "ib_assemble"},
+                     {LBM_ST_INDEX_FACTOR, "ib_factor"},     {LBM_ST_INDEX_SOLVE, "ib_solve"},
+                     {LBM_ST_INDEX_SCATTER, "ib_tile_scatter"}, {LBM_ST_INDEX_SORT, "ib_tile_sort"},
+                     {LBM_ST_INDEX_TILE, "ib_tile_update"}, {LBM_ST_INDEX_FORCES, "ib_forces"},
+                     {LBM_ST_INDEX_RESIDUAL, "ib_residual"}, {LBM_ST_INDEX_LATTICE, "kf_tma"}};
+        msg = "device index out of range, access skipped in:";
+        for (const auto &n : names)
+            if (st & n.bit) msg += std::string(" ") + n.kernel;
+        return LBM_ERR_INDEX;
+    }
+    if (st & LBM_ST_TIMEOUT) {
+        msg = "a bounded wait for a shared-memory copy gave up";
+        return LBM_ERR_CUDA;
+    }
+    if (st & LBM_ST_RANGE) {
+        msg = "move_boundary: a marker support box reaches the three outermost node layers";
+        return LBM_ERR_RANGE;
+    }
+    if (st & LBM_ST_OVERFLOW) {
+        msg = "immersed boundary: correction patch overflow";
+        return LBM_ERR_RANGE;
+    }
+    if (st & LBM_ST_SOLVER) {
+        msg = "immersed boundary: D D^T not positive definite";
+        return LBM_ERR_SOLVER;
+    }
+    if (st & LBM_ST_NONFINITE) {
+        msg = "non-finite flow at the markers or force (the flow diverged)";
+        return LBM_ERR_NONFINITE;
+    }
+    msg = "unknown device status";
+    return LBM_ERR_CUDA;
+}
+
+namespace {
+
 int check_status(lbm_handle *h)
 {
     unsigned st = 0;
@@ -278,13 +327,28 @@ int check_status(lbm_handle *h)
     CK(cudaStreamSynchronize(h->stream), "step sync");
     if (!st) return LBM_OK;
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream), "clear status");
-    if (st & LBM_ST_RANGE)
-        return set_err(h, LBM_ERR_RANGE, "move_boundary: a marker support box reaches the three outermost node layers");
-    if (st & LBM_ST_OVERFLOW) return set_err(h, LBM_ERR_RANGE, "immersed boundary: correction patch overflow");
-    if (st & LBM_ST_SOLVER) return set_err(h, LBM_ERR_SOLVER, "immersed boundary: D D^T not positive definite");
-    if (st & LBM_ST_NONFINITE)
-        return set_err(h, LBM_ERR_NONFINITE, "non-finite flow at the markers or force (the flow diverged)");
-    return set_err(h, LBM_ERR_CUDA, "unknown device status");
+    std::string msg;
+    const int code = status_error(st, msg);
+    return set_err(h, code, msg.c_str());
+}
+
+// Global mass check: queues the FP64 deviation sum of the current populations
+// on stream st and its copy into *dsum (the caller synchronises st), then
+// mass_result turns it into the mass and checks that it is finite.
+int mass_launch(lbm_handle *h, cudaStream_t st, double *dsum)
+{
+    if (launch_mass(h, h->fbuf[h->cur], st)) return cuda_err(h, cudaGetLastError(), "launch mass");
+    CK(cudaMemcpyAsync(dsum, h->d_mass + (mass_slots() - 1), sizeof(double), cudaMemcpyDeviceToHost, st), "copy mass");
+    return LBM_OK;
+}
+
+int mass_result(lbm_handle *h, double dsum)
+{
+    const double m = (double)h->nx * (double)h->ny + dsum;   // sum_k w_k = 1 per node
+    h->last_mass = m;
+    h->last_mass_step = h->steps_done;
+    if (!std::isfinite(m)) return set_err(h, LBM_ERR_NONFINITE, "mass check: non-finite populations (the flow diverged)");
+    return LBM_OK;
 }
 
 // sums the event intervals of `count` step slots after the streams are idle:
@@ -321,6 +385,10 @@ int collect_timing(lbm_handle *h, int count, bool split)
 // the main stream then waits for the IB chain and updates the envelope.
 int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool fields_every)
 {
+    // the mass is checked at every copy of force rows of lbm_run (every
+    // kRing steps and at the end of the call), and by lbm_step on every
+    // kRing-th step
+    auto mass_due = [&]() { return !fields_every || (h->n - 1) % kRing == 0; };
     if (!h->inited) return set_err(h, LBM_ERR_STATE, "step: lbm_init not called");
     for (int w = 0; w < h->nwing; ++w)
         if (!h->have_wing[w]) return set_err(h, LBM_ERR_STATE, "step: boundary of a wing not set");
@@ -425,13 +493,19 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
                 CK(cudaEventRecord(h->ev_ib, h->side), "event");
                 CK(cudaStreamWaitEvent(h->stream, h->ev_ib, 0), "wait");
             }
-            if (h->timing == LBM_TIMING_SPAN) CK(cudaEventRecord(h->ev[4 * (pending - 1) + 3], h->stream), "event");
             if (rows_out)
                 CK(cudaMemcpyAsync(rows_out + (size_t)(done - pending) * h->row_len, h->d_ring,
                                    sizeof(double) * h->row_len * pending, cudaMemcpyDeviceToHost, h->stream),
                    "copy force rows");
-            int st = check_status(h);
+            double dsum = 0.0;
+            const bool mass = mass_due();
+            int st = mass ? mass_launch(h, h->stream, &dsum) : LBM_OK;
             if (st) return st;
+            // the span ends after the chunk's row copy and mass check
+            if (h->timing == LBM_TIMING_SPAN) CK(cudaEventRecord(h->ev[4 * (pending - 1) + 3], h->stream), "event");
+            st = check_status(h);
+            if (st) return st;
+            if (mass && (st = mass_result(h, dsum))) return st;
             if (h->timing && (st = collect_timing(h, pending, split))) return st;
             pending = 0;
         }
@@ -441,13 +515,18 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             CK(cudaEventRecord(h->ev_ib, h->side), "event");
             CK(cudaStreamWaitEvent(h->stream, h->ev_ib, 0), "wait");
         }
-        if (h->timing == LBM_TIMING_SPAN) CK(cudaEventRecord(h->ev[4 * (pending - 1) + 3], h->stream), "event");
         if (rows_out)
             CK(cudaMemcpyAsync(rows_out + (size_t)(done - pending) * h->row_len, h->d_ring,
                                sizeof(double) * h->row_len * pending, cudaMemcpyDeviceToHost, h->stream),
                "copy force rows");
-        int st = check_status(h);
+        double dsum = 0.0;
+        const bool mass = mass_due();
+        int st = mass ? mass_launch(h, h->stream, &dsum) : LBM_OK;
         if (st) return st;
+        if (h->timing == LBM_TIMING_SPAN) CK(cudaEventRecord(h->ev[4 * (pending - 1) + 3], h->stream), "event");
+        st = check_status(h);
+        if (st) return st;
+        if (mass && (st = mass_result(h, dsum))) return st;
         if (h->timing && (st = collect_timing(h, pending, split))) return st;
     }
     if (done_out) *done_out = done;
@@ -456,8 +535,14 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
 
 }  // namespace
 
+// an empty kernel, compiled like every other kernel of the library: its
+// attributes tell which architecture the library's device code is for
+__global__ void arch_probe() {}
+
 // for lbm_batch.cu
 int handle_prepare_ib(lbm_handle *h) { return ensure_ib(h); }
+int handle_mass_launch(lbm_handle *h, cudaStream_t st, double *dsum) { return mass_launch(h, st, dsum); }
+int handle_mass_result(lbm_handle *h, double dsum) { return mass_result(h, dsum); }
 int handle_error(lbm_handle *h, int code, const char *msg) { return set_err(h, code, msg); }
 int handle_status(lbm_handle *h) { return check_status(h); }
 
@@ -658,7 +743,6 @@ int lbm_create(const lbm_params *p, lbm_t **out)
     const size_t fbytes = h->elem * (9 * (size_t)h->plane + 2 * LBM_FPAD);
     for (int b = 0; b < 2; ++b) {
         if ((e = dmalloc(h, &h->falloc[b], fbytes)) != cudaSuccess) return fail(e, "alloc f");
-        if ((e = cudaMemset(h->falloc[b], 0, fbytes)) != cudaSuccess) return fail(e, "clear f");
         h->fbuf[b] = (char *)h->falloc[b] + h->elem * LBM_FPAD;
     }
     const size_t cs = compute_size(h->prec);
@@ -670,21 +754,21 @@ int lbm_create(const lbm_params *p, lbm_t **out)
     if ((e = dmalloc(h, &h->d_counter, sizeof(unsigned))) != cudaSuccess) return fail(e, "alloc counter");
     if ((e = dmalloc(h, &h->d_pinfo, LBM_NSLOT_MAX * sizeof(PatchInfo))) != cudaSuccess) return fail(e, "alloc pinfo");
     if ((e = dmalloc(h, &h->d_red, sizeof(double) * 2 * 296)) != cudaSuccess) return fail(e, "alloc red");
+    if ((e = dmalloc(h, &h->d_mass, sizeof(double) * mass_slots())) != cudaSuccess) return fail(e, "alloc mass");
+    if ((e = dmalloc(h, &h->d_mcount, sizeof(unsigned))) != cudaSuccess) return fail(e, "alloc mass counter");
     if ((e = dmalloc(h, &h->d_kftab, (size_t)KF_TABLE_ENTRIES * KF_ARGS_STRIDE)) != cudaSuccess)
         return fail(e, "alloc lattice arguments");
     if ((e = dmalloc(h, &h->d_solve_res, 2 * sizeof(double))) != cudaSuccess) return fail(e, "alloc res");
     if ((e = dmalloc(h, &h->d_ring, sizeof(double) * h->row_len * (size_t)h->ring_cap)) != cudaSuccess)
         return fail(e, "alloc ring");
-    cudaMemset(h->d_status, 0, sizeof(unsigned));
-    cudaMemset(h->d_counter, 0, sizeof(unsigned));
-    cudaMemset(h->d_pinfo, 0, LBM_NSLOT_MAX * sizeof(PatchInfo));
-    cudaMemset(h->d_solve_res, 0, 2 * sizeof(double));
     if (h->npts > 0) {
         if ((e = dmalloc(h, &h->d_xb0, sizeof(double) * h->npts)) != cudaSuccess) return fail(e, "alloc xb0");
         if ((e = dmalloc(h, &h->d_yb0, sizeof(double) * h->npts)) != cudaSuccess) return fail(e, "alloc yb0");
         if ((e = dmalloc(h, &h->d_arc, sizeof(double) * h->nseg)) != cudaSuccess) return fail(e, "alloc arc");
     }
-    if ((e = cudaDeviceSynchronize()) != cudaSuccess) return fail(e, "sync");
+    // the zero-fills queued on the handle's stream are done (later calls
+    // order their work after them on the same stream in any case)
+    if ((e = cudaStreamSynchronize(h->stream)) != cudaSuccess) return fail(e, "sync");
     *out = h;
     return LBM_OK;
 }
@@ -702,6 +786,7 @@ int lbm_destroy(lbm_t *h)
     free_ib(h);
     free_devp(h->d_pinfo); free_devp(h->d_counter);
     free_devp(h->d_ring); free_devp(h->d_status); free_devp(h->d_solve_res); free_devp(h->d_red);
+    free_devp(h->d_mass); free_devp(h->d_mcount);
     free_dev(h->d_kftab);
     free_devp(h->d_stage);
     if (h->side) cudaStreamSynchronize(h->side);
@@ -838,6 +923,10 @@ int lbm_init(lbm_t *h, const double *du, const double *dv)
     free_devp(h->d_stage);   // the FP64 staging planes are made for each transfer, not kept
     h->n = 1;
     h->steps_done = 0;
+    // the patch rectangles were cleared above: the factorization slots are
+    // filled again from the first step
+    h->batch_in_half[0] = h->batch_in_half[1] = -1;
+    h->fgroup[0] = h->fgroup[1] = -1;
     h->inited = 1;
     return LBM_OK;
 }
@@ -927,6 +1016,19 @@ int lbm_residual(lbm_t *h, double *err)
     return LBM_OK;
 }
 
+int lbm_mass(lbm_t *h, double *mass)
+{
+    if (!h || !mass) return LBM_ERR_ARG;
+    if (!h->inited) return set_err(h, LBM_ERR_STATE, "mass: not initialised");
+    double dsum = 0.0;
+    int rc = mass_launch(h, h->stream, &dsum);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(h->stream), "sync mass");
+    rc = mass_result(h, dsum);
+    *mass = h->last_mass;
+    return rc;
+}
+
 int lbm_get_markers(lbm_t *h, double *xb2, double *yb2, double *solve_residual, int *half_bandwidth)
 {
     if (!h) return LBM_ERR_ARG;
@@ -988,5 +1090,30 @@ int lbm_device_bytes(const lbm_t *h, long long *bytes)
 }
 
 const char *lbm_last_error(const lbm_t *h) { return h ? h->err.c_str() : "lbm_create failed (bad parameters or no CUDA device)"; }
+
+int lbm_device_check(int *binary_version, int *sm_count)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return LBM_ERR_CUDA;
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, arch_probe) != cudaSuccess) return LBM_ERR_CUDA;
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return LBM_ERR_CUDA;
+    if (binary_version) *binary_version = fa.binaryVersion;
+    if (sm_count) *sm_count = sms;
+    return LBM_OK;
+}
+
+int lbm_describe_status(unsigned int status, char *message, int capacity)
+{
+    std::string msg;
+    const int code = status_error(status, msg);
+    if (message && capacity > 0) {
+        const size_t n = std::min(msg.size(), (size_t)capacity - 1);
+        memcpy(message, msg.data(), n);
+        message[n] = 0;
+    }
+    return code;
+}
 
 }  // extern "C"

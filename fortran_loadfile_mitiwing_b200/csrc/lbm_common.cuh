@@ -34,6 +34,21 @@ __host__ __device__ constexpr int lbm_ey(int k)
 #define LBM_ST_NONFINITE 4u  // NaN/Inf in forces
 #define LBM_ST_OVERFLOW 8u   // patch larger than its allocation
 #define LBM_ST_TIMEOUT 16u   // a bounded wait on a shared-memory barrier gave up
+// An index read from device memory (a solve-order position, a tile-list
+// entry, a correction-tile number, a marker's support box or wing) fell
+// outside the buffer it indexes. The kernel that saw it sets its own bit and
+// skips that access; the host reports the error naming the kernel.
+#define LBM_ST_INDEX_INTERP 0x100u      // ib_interp: support box
+#define LBM_ST_INDEX_ASSEMBLE 0x200u    // ib_assemble: solve order, support box
+#define LBM_ST_INDEX_FACTOR 0x400u      // ib_factor (dense path): solve order, support box
+#define LBM_ST_INDEX_SOLVE 0x800u       // ib_solve: solve order
+#define LBM_ST_INDEX_SCATTER 0x1000u    // ib_tile_scatter: tile of a support box
+#define LBM_ST_INDEX_SORT 0x2000u       // ib_tile_sort: correction tile
+#define LBM_ST_INDEX_TILE 0x4000u       // ib_tile_update: correction tile, listed marker, box, wing
+#define LBM_ST_INDEX_FORCES 0x8000u     // ib_forces: correction tile
+#define LBM_ST_INDEX_RESIDUAL 0x10000u  // ib_residual: solve order, support box
+#define LBM_ST_INDEX_LATTICE 0x20000u   // kf_tma: tile of the patch rectangle
+#define LBM_ST_INDEX_MASK 0x3ff00u
 
 // current immersed-boundary correction patch (0-based node rectangle)
 struct PatchInfo {
@@ -50,6 +65,16 @@ struct Marker {
     int wing;                 // 0-based
     int pad;
 };
+
+// A support box (0-based, inclusive: x..y columns, z..w rows) as make_marker
+// leaves it: empty, or inside columns 1..nx-2 and rows 1..ny-2 and at most
+// LBM_BOX nodes per axis, so that every node of it has all eight neighbours
+// and its kernel values index phx/phy within bounds.
+__host__ __device__ __forceinline__ bool box_in_bounds(int x, int y, int z, int w, int nx, int ny)
+{
+    if (y < x || w < z) return true;   // empty: no node is visited
+    return x >= 1 && y <= nx - 2 && z >= 1 && w <= ny - 2 && y - x < LBM_BOX && w - z < LBM_BOX;
+}
 
 // compute precision of a storage type: FP64 storage computes in FP64,
 // everything else in FP32

@@ -31,6 +31,7 @@ struct KFArgs {
     const PatchInfo *pinfo;            // the step's patch rectangle (KF_OUTER)
     const int *tiles;                  // the step's tile lists: count per 16 x 16 tile (KF_OUTER)
     int tiles_x, tile_stride;          // tiles per rectangle row; ints per tile
+    int tiles_n;                       // tiles of the grid (bound of the tile index)
     C *rho_out, *u_out, *v_out;        // fields, when requested (else null)
     int mode;                          // KF_ALL, or KF_OUTER (all but the correction tiles)
     int rows_per_cta;                  // row sweep length of the staged kernel
@@ -185,6 +186,12 @@ struct lbm_handle {
     int fields_slot = 0;           // slot written by the last field step
     int fields_step[2] = {-1, -1}; // step index written into each slot
     double *d_red = nullptr;       // residual reduction scratch
+    // global mass check: CTA partials, then the deviation sum (mass_slots()
+    // doubles), its last-CTA counter, and the last mass found (host)
+    double *d_mass = nullptr;
+    unsigned *d_mcount = nullptr;
+    double last_mass = 0.0;
+    int last_mass_step = -1;
     double *d_stage = nullptr;     // FP64 (nx,ny,9) staging for get/set of populations
     // device timing (lbm_set_timing): per step slot of the ring, four events on
     // the main stream (start, lattice part 1 done, lattice part 2 start, end)
@@ -217,6 +224,10 @@ int launch_check(lbm_handle *h, int slot, int ring_slot, bool residual, cudaStre
 int handle_prepare_ib(lbm_handle *h);                    // immersed-boundary buffers (once per geometry)
 int handle_error(lbm_handle *h, int code, const char *msg);
 int handle_status(lbm_handle *h);                        // reads and clears the device status
+// global mass check of a case: queue the sum on st into *dsum, then (after st
+// is synchronised) check it
+int handle_mass_launch(lbm_handle *h, cudaStream_t st, double *dsum);
+int handle_mass_result(lbm_handle *h, double dsum);
 // boundary reference values from the edge f0 populations (layout of edge_f0)
 int handle_set_edges(lbm_handle *h, const double *edge_f0);
 // state of a restart file in the reference's layout: populations f(nx,ny,9),
@@ -244,3 +255,8 @@ int launch_pack(lbm_handle *h, const double *src, void *fdst);     // f (FP64) -
 // of the perturbation (nullable)
 int launch_init_lattice(lbm_handle *h, const double *du, const double *dv);
 int launch_fields_to_double(lbm_handle *h, const void *fields, double *rho, double *u, double *v);
+// global mass check (FP64, deterministic) of the populations in fsrc
+int launch_mass(lbm_handle *h, const void *fsrc, cudaStream_t st);
+int mass_slots();
+// error code and message of a device status word
+int status_error(unsigned st, std::string &msg);

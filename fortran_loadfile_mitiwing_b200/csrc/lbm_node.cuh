@@ -43,6 +43,7 @@ inline KFArgs<C> make_kf_args(lbm_handle *h, const void *fin, void *fout, void *
     a.tiles = h->d_tiles ? h->d_tiles + (size_t)h->pinfo_slot * h->tiles_slot : nullptr;
     a.tiles_x = h->patch_gx();
     a.tile_stride = ib_tile_ints();
+    a.tiles_n = h->patch_gx() * h->patch_gy();
     if (fields) {
         C *fc = (C *)fields;
         const long long nn = (long long)h->nx * h->ny;

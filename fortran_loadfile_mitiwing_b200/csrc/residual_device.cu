@@ -17,17 +17,23 @@
 // LBM_RESIDUAL_MAX_ROWS interior rows (ny - 2), i.e. 256 KiB. Larger ny is
 // rejected with LBM_ERR_SIZE before anything is launched.
 //
-// Set-up: the first call on each device, with that device current, looks up
-// the scratch's device address (cudaGetSymbolAddress) and caches it per
-// device. That first call should come before any stream capture on the
-// device. Every call then clears the completion counter on the caller's
-// stream, launches one kernel and copies the two totals back, synchronising
-// that stream.
+// Set-up: the first call in each CUDA context looks up the scratch's device
+// address (cudaGetSymbolAddress) and keeps it for that context. A context is
+// the device's primary context that the runtime makes current (one per
+// device), or a context the caller created and made current itself, as a
+// CUDA Fortran or OpenACC runtime may; each context holds its own copy of the
+// scratch at its own address, so the cache is keyed by the context's unique
+// ID (cuCtxGetId), which also tells a context re-created after
+// cudaDeviceReset from the one it replaces. The first call in a context
+// should come before any stream capture in it. Every call then clears the
+// completion counter on the caller's stream, launches one kernel and copies
+// the two totals back to host memory, so each call waits for its stream.
 //
 // There is one scratch array per device, shared by every caller: two calls
 // whose work overlaps on the GPU (different streams, or different host
 // threads on the same device) race on it and may return wrong values. Callers
 // must serialise them.
+#include <cuda.h>   // CUcontext and CUresult; the two driver calls are looked up at run time
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -38,7 +44,7 @@
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kMaxDevices = 64;
+constexpr int kMaxContexts = 64;   // contexts whose scratch address is kept
 constexpr int kRows = LBM_RESIDUAL_MAX_ROWS;
 // layout of the scratch (doubles): [0, 2*kRows) row partials,
 // [2*kRows] completion counter (as unsigned), [2*kRows + 2, +4) totals
@@ -49,7 +55,16 @@ constexpr int kScratchDoubles = 2 * kRows + 4;
 static __device__ __align__(256) double lbm_residual_scratch[kScratchDoubles];
 
 std::mutex g_setup_mutex;
-double *g_scratch[kMaxDevices] = {};
+struct ScratchAddress {
+    unsigned long long ctx_id;   // 0: unused
+    double *ptr;
+};
+ScratchAddress g_scratch[kMaxContexts] = {};
+int g_scratch_next = 0;   // entry replaced next when all are in use
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+CtxGetCurrentFn g_ctx_current = nullptr;
+CtxGetIdFn g_ctx_id = nullptr;
 
 // deterministic sum of one value per thread over the block (fixed tree)
 __device__ __forceinline__ void block_sum2(double &a, double &b, double *sh)
@@ -110,18 +125,47 @@ __global__ void __launch_bounds__(kThreads) residual_rows(const C *__restrict__ 
     }
 }
 
-// scratch address on the current device, looked up on the first call there
-int scratch_for_current_device(double **out)
+// unique ID of the CUDA context current on this thread; when none is current
+// yet, the current device's primary context is made current first (as the
+// runtime's own first call on a thread would). 0 on failure.
+unsigned long long current_context_id()
 {
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return LBM_ERR_CUDA;
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_scratch[dev]) {
-        void *p = nullptr;
-        if (cudaGetSymbolAddress(&p, lbm_residual_scratch) != cudaSuccess || !p) return LBM_ERR_CUDA;
-        g_scratch[dev] = static_cast<double *>(p);
+    if (!g_ctx_current || !g_ctx_id) {
+        void *f1 = nullptr, *f2 = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, nullptr) != cudaSuccess || !f1 ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, nullptr) != cudaSuccess || !f2)
+            return 0;
+        g_ctx_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+        g_ctx_id = reinterpret_cast<CtxGetIdFn>(f2);
     }
-    *out = g_scratch[dev];
+    CUcontext ctx = nullptr;
+    if (g_ctx_current(&ctx) != CUDA_SUCCESS) return 0;
+    if (!ctx) {
+        int dev = -1;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaSetDevice(dev) != cudaSuccess) return 0;
+        if (g_ctx_current(&ctx) != CUDA_SUCCESS || !ctx) return 0;
+    }
+    unsigned long long id = 0;
+    if (g_ctx_id(ctx, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
+// scratch address in the current context, looked up on the first call there
+int scratch_for_current_context(double **out)
+{
+    std::lock_guard<std::mutex> lock(g_setup_mutex);
+    const unsigned long long id = current_context_id();
+    if (!id) return LBM_ERR_CUDA;
+    for (const ScratchAddress &e : g_scratch)
+        if (e.ctx_id == id) {
+            *out = e.ptr;
+            return LBM_OK;
+        }
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, lbm_residual_scratch) != cudaSuccess || !p) return LBM_ERR_CUDA;
+    g_scratch[g_scratch_next] = ScratchAddress{id, static_cast<double *>(p)};
+    g_scratch_next = (g_scratch_next + 1) % kMaxContexts;
+    *out = static_cast<double *>(p);
     return LBM_OK;
 }
 
@@ -134,7 +178,7 @@ extern "C" LBM_API int lbm_residual_device(const void *u, const void *v, const v
     if (precision != LBM_PREC_FP32 && precision != LBM_PREC_FP64) return LBM_ERR_ARG;
     if (ny - 2 > LBM_RESIDUAL_MAX_ROWS) return LBM_ERR_SIZE;
     double *scratch = nullptr;
-    const int st = scratch_for_current_device(&scratch);
+    const int st = scratch_for_current_context(&scratch);
     if (st != LBM_OK) return st;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (cudaMemsetAsync(scratch + kCounter, 0, sizeof(unsigned), s) != cudaSuccess) return LBM_ERR_CUDA;

@@ -157,6 +157,13 @@ class Lbm:
         self._ck(self.lib.lbm_residual(self.h, C.byref(e)))
         return e.value
 
+    def mass(self):
+        """Global mass sum of f over the lattice after the last step (lbm_mass,
+        FP64 on the device)."""
+        m = C.c_double()
+        self._ck(self.lib.lbm_mass(self.h, C.byref(m)))
+        return m.value
+
     def markers(self):
         """(xb2, yb2, solve residual) of the last step."""
         x, y, r, _ = self.solver_info()

@@ -49,6 +49,9 @@ extern "C" {
 #define LBM_ERR_NONFINITE   -6   /* NaN/Inf seen in forces, in the flow at the markers or in the mass check */
 #define LBM_ERR_RANGE       -7   /* a marker's support box reaches the three outermost node layers */
 #define LBM_ERR_SIZE        -8   /* size beyond a fixed maximum (lbm_residual_device) */
+#define LBM_ERR_INDEX       -9   /* a kernel found an index read from device memory out of range and
+                                    skipped that access; the message names the kernel. Not expected:
+                                    it means device state was overwritten (report it) */
 
 /* storage precision of the populations (all collision arithmetic is FP32,
  * or FP64 for LBM_PREC_FP64; immersed-boundary solve and force sums are FP64) */
@@ -181,6 +184,17 @@ LBM_API int lbm_set_populations(lbm_t *h, const double *f);
  * LBM_ERR_STATE). */
 LBM_API int lbm_residual(lbm_t *h, double *err);
 
+/* Global mass sum_ij sum_k f_k of the populations after the last step,
+ * summed on the device in FP64 in a fixed order (the same value on every
+ * call for the same state). lbm_run also checks it at every copy of force
+ * rows (every 2048 steps and at the end of the call), lbm_step on every
+ * 2048th step and lbm_batch_run at the end of the call for each case; a
+ * non-finite mass ends the run with LBM_ERR_NONFINITE. The reference has no
+ * mass check; its lattice-wide reduction is erranalysis
+ * (solution.f90:102-109). Returns LBM_ERR_NONFINITE (with *mass set) if the
+ * mass is not finite. */
+LBM_API int lbm_mass(lbm_t *h, double *mass);
+
 /* immersed-boundary diagnostics of the last step: marker midpoints xb2,yb2
  * (airfoil.f90:267-270; n = wing_count*(points_per_wing-1) each), the
  * relative residual ||B y - rhs|| / ||rhs|| of the marker system solve, and
@@ -218,11 +232,13 @@ LBM_API int lbm_get_timing(lbm_t *h, double *step_ms, double *ib_ms, double *lat
  *     as `precision` says (LBM_PREC_FP64 / LBM_PREC_FP32), on the current
  *     device; interior nodes only enter the sums, as in the reference.
  *   stream: a cudaStream_t, or NULL for the legacy default stream; the call
- *     synchronises it and writes *err = ||u - u0|| / (||u|| + 1e-30).
- * The first call on each device (with that device current) looks up the
- * scratch's address; make that first call before any stream capture. Calls
- * whose work overlaps on the GPU (other streams, other host threads on the
- * same device) share the scratch and race: serialise them. */
+ *     copies the result to host memory, so it waits for that stream, and
+ *     writes *err = ||u - u0|| / (||u|| + 1e-30).
+ * The first call in each CUDA context (the device's primary context, or a
+ * context the caller created and made current) looks up the scratch's
+ * address in that context; make that first call before any stream capture.
+ * Calls whose work overlaps on the GPU (other streams, other host threads on
+ * the same device) share the scratch and race: serialise them. */
 #define LBM_RESIDUAL_MAX_ROWS 16384
 LBM_API int lbm_residual_device(const void *u, const void *v, const void *u0, const void *v0,
                                 int nx, int ny, int precision, void *stream, double *err);
@@ -245,6 +261,21 @@ LBM_API int lbm_device_bytes(const lbm_t *h, long long *bytes);
 /* message of the last failing call on h ("" if none); h may be NULL for
  * errors of lbm_create. The string stays valid until the next call on h. */
 LBM_API const char *lbm_last_error(const lbm_t *h);
+
+/* Whether this library's kernels run on the current device:
+ * *binary_version = the architecture they were compiled for (100 for
+ * sm_100a, as cudaFuncAttributes::binaryVersion gives it) and *sm_count =
+ * the device's multiprocessors (both nullable). LBM_ERR_CUDA when there is no
+ * device or the device cannot load them. The reference picks its GPU target
+ * at build time (nvfortran -gpu, Makefile:1-16) and has no such check. */
+LBM_API int lbm_device_check(int *binary_version, int *sm_count);
+
+/* The status code and message (into message[capacity], nullable) that a
+ * device status word of the kernels turns into: the translation lbm_step /
+ * lbm_run apply after each run of steps. Host only; needs no device. The
+ * reference has no device status: its cuSOLVER status is ignored and bad
+ * input stops the program (stop 1). */
+LBM_API int lbm_describe_status(unsigned int status, char *message, int capacity);
 
 /* ---- output and restart files -------------------------------------------
  * lbm_write_tecplot: the reference's output (solution.f90:129-238) for the

@@ -29,7 +29,9 @@ def fnum(tok):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_reference_constants.py <reference source directory>")
+    ref = sys.argv[1]
     sol = read(ref, "solution.f90")
     rows = {}
     for m in re.finditer(r"matm\((\d)\s*,\s*:\s*\)\s*=\s*\(/([^/]*)/\)", sol):

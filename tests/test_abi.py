@@ -29,10 +29,36 @@ def test_library_exports_every_declared_symbol(lib):
 
 
 def test_library_is_built_for_sm100a():
-    out = subprocess.run(["cuobjdump", "--list-elf", _abi.LIB_PATH], capture_output=True, text=True)
-    if out.returncode != 0:
-        pytest.skip("cuobjdump unavailable")
-    assert "sm_100a" in out.stdout
+    """Every source is compiled and linked for sm_100a only (the GPU tests
+    also ask the loaded kernels: lbm_device_check)."""
+    flags = build.NVCC_FLAGS
+    i = flags.index("-gencode")
+    assert flags[i + 1] == "arch=compute_100a,code=sm_100a"
+    assert flags.count("-gencode") == 1
+
+
+def test_status_words_decode_to_codes_and_kernel_names(lib):
+    """The device status word the kernels set becomes the call's status code
+    and message (host logic, no device): an index error names every kernel
+    that skipped an access and comes before the other errors."""
+    buf = C.create_string_buffer(256)
+    assert lib.lbm_describe_status(0, buf, 256) == _abi.LBM_OK and buf.value == b""
+    for bit, kernel in _abi.LBM_ST_INDEX_KERNELS.items():
+        assert lib.lbm_describe_status(bit | _abi.LBM_ST_SOLVER, buf, 256) == _abi.LBM_ERR_INDEX
+        assert buf.value.decode().split(":")[-1].split() == [kernel]
+    both = 0x4000 | 0x8000
+    assert lib.lbm_describe_status(both, buf, 256) == _abi.LBM_ERR_INDEX
+    assert buf.value.decode().split(":")[-1].split() == ["ib_tile_update", "ib_forces"]
+    assert lib.lbm_describe_status(_abi.LBM_ST_RANGE, buf, 256) == _abi.LBM_ERR_RANGE
+    assert lib.lbm_describe_status(_abi.LBM_ST_OVERFLOW, buf, 256) == _abi.LBM_ERR_RANGE
+    assert lib.lbm_describe_status(_abi.LBM_ST_SOLVER, buf, 256) == _abi.LBM_ERR_SOLVER
+    assert lib.lbm_describe_status(_abi.LBM_ST_NONFINITE, buf, 256) == _abi.LBM_ERR_NONFINITE
+    assert lib.lbm_describe_status(_abi.LBM_ST_TIMEOUT, buf, 256) == _abi.LBM_ERR_CUDA
+    # a short buffer gets a terminated prefix; a null buffer only the code
+    small = C.create_string_buffer(8)
+    assert lib.lbm_describe_status(0x100, small, 8) == _abi.LBM_ERR_INDEX
+    assert len(small.value) == 7
+    assert lib.lbm_describe_status(0x100, None, 0) == _abi.LBM_ERR_INDEX
 
 
 def test_default_params_are_the_reference_parameters(lib):

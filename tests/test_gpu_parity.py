@@ -7,7 +7,13 @@ Tolerances:
     window): populations, velocity field and per-step C_D/C_L within 1e-5
     relative; populations as max|df|/max|f|, velocity as ||du||/||u||, forces
     per step against max(|C|, rms C over the window) so that zero crossings of
-    C_L are not divided by ~0.
+    C_L are not divided by ~0. The same bars on the benchmarked 4096x2048
+    heave + pitch case over its first 24 steps.
+  FP32 storage, 400x200 plunge case, two whole periods after step 1000:
+    per-period mean C_D within 0.5% of |mean C_D|, mean C_L within 0.5% of
+    the RMS of C_L.
+  FP64 storage, 400x200 plunge case, 1000 steps: populations and fields
+    within 1e-10 absolute, force coefficients 1e-8 relative.
 """
 import numpy as np
 import pytest
@@ -121,10 +127,10 @@ def test_timing_modes(gpu_lib):
 def test_launch_count_per_step(gpu_lib):
     """Per step of one rigid wing: the flow chain (interpolation, solve, update
     of the correction tiles, force row) and the lattice kernel; the residual
-    check on the last step of each batch of 4 steps and of the call; per batch
-    of steps, the six kernels of the batched factorization of the marker
-    system (geometry, band assembly, factorization, patch-tile lists in three
-    passes)."""
+    check on the last step of each batch of 4 steps and of the call; the mass
+    check at the end of the call; per batch of steps, the six kernels of the
+    batched factorization of the marker system (geometry, band assembly,
+    factorization, patch-tile lists in three passes)."""
     import ctypes as C
     case = cases.small_case(precision="fp32", n_steps=100)
     g = Lbm.from_case(case, gpu_lib)
@@ -138,7 +144,7 @@ def test_launch_count_per_step(gpu_lib):
     per_step = 4 + 1
     # steps n = 2 .. 13: checked where (n + 1) % 4 == 0 (3, 7, 11) and the last (13)
     checks = sum(1 for n in range(2, 2 + steps) if (n + 1) % 4 == 0 or n == 1 + steps)
-    rest = total - steps * per_step - checks
+    rest = total - steps * per_step - checks - 1
     assert rest > 0 and rest % 6 == 0, total
     assert 1 <= rest // 6 <= steps, total
 
@@ -246,3 +252,77 @@ def test_large_case_short_run_properties(gpu_lib):
     assert w <= 16 and res < 1e-10
     rho, u, v = s.fields()
     assert np.all(np.isfinite(u)) and abs(rho.mean() - 1.0) < 1e-3
+
+
+def _period_means(rows, start, period):
+    """Per-period means of the force columns 1..2 (C_D, C_L of wing 1) over
+    whole periods from `start` on."""
+    n = (rows.shape[0] - start) // period
+    return np.array([rows[start + p * period:start + (p + 1) * period, 1:3].mean(axis=0) for p in range(n)])
+
+
+def test_fp32_parity_plunge_400x200_two_periods_after_step_1000(gpu_lib, oracle_mod):
+    """The second parity bar on the 400x200 plunge case: after the first 1000
+    steps, the per-period mean C_D within 0.5% of |mean C_D| of the oracle,
+    and the per-period mean C_L within 0.5% of the oracle's RMS C_L (its mean
+    is close to 0), over two whole periods (2 x 2667 steps)."""
+    period = 2667   # 1 / (f* dt) = 1 / (0.6 * 6.25e-4) = 2666.7 steps
+    nsteps = 1000 + 2 * period
+    case = cases.plunge_case(precision="fp32", n_steps=nsteps + 8)
+    g = Lbm.from_case(case, gpu_lib)
+    o = oracle_mod.Oracle.from_case(case)
+    rg = g.run(nsteps)
+    ro = o.run(nsteps)
+    assert rg.shape == ro.shape == (nsteps, g.row_len)
+    mg, mo = _period_means(rg, 1000, period), _period_means(ro, 1000, period)
+    assert mg.shape == (2, 2)
+    rms_cl = np.sqrt(np.mean(ro[1000:, 2] ** 2))
+    err_cd = np.abs(mg[:, 0] - mo[:, 0]) / np.abs(mo[:, 0])
+    err_cl = np.abs(mg[:, 1] - mo[:, 1]) / rms_cl
+    assert err_cd.max() < 5e-3, err_cd
+    assert err_cl.max() < 5e-3, err_cl
+
+
+def test_fp64_parity_plunge_400x200_first_1000_steps(gpu_lib, oracle_mod):
+    """FP64 storage (the GPU FP64 oracle of the precision study) against the
+    CPU oracle over the first 1000 steps of the 400x200 plunge case, the size
+    the study runs at: populations within 1e-10 absolute (rounding of two
+    different summation orders, accumulated over 1000 steps), fields likewise,
+    per-step force coefficients within 1e-8 relative."""
+    case = cases.plunge_case(precision="fp64", n_steps=1010)
+    g, o, rg, ro = run_both(case, 1000, gpu_lib, oracle_mod, use_run=True)
+    assert np.abs(g.populations() - o.populations()).max() < 1e-10
+    for a, b in zip(g.fields(), o.fields()):
+        assert np.abs(a - b).max() < 1e-10
+    assert rel_series(rg[:, 1:4], ro[:, 1:4]) < 1e-8
+
+
+def test_fp32_parity_heave_pitch_4096x2048_first_24_steps(gpu_lib, oracle_mod):
+    """The benchmarked case (4096x2048, 1024 markers, heave + pitch, FP32
+    storage) against the oracle over its first 24 steps: populations
+    (max|df|/max|f|), velocity field (||du||/||u||) and per-step C_D/C_L/C_M
+    within 1e-5 relative, the FP32 tolerance."""
+    case = cases.heave_pitch_case(n_steps=40, precision="fp32")
+    g, o, rg, ro = run_both(case, 24, gpu_lib, oracle_mod, use_run=True)
+    assert rel_series(rg[:, 1:4], ro[:, 1:4]) < 1e-5
+    np.testing.assert_array_equal(rg[:, 0], ro[:, 0])
+    fg = g.populations()
+    fo = o.populations()
+    assert np.abs(fg - fo).max() / np.abs(fo).max() < 1e-5
+    del fg, fo
+    _, ug, vg = g.fields()
+    _, uo, vo = o.fields()
+    vel = np.sqrt(np.sum((ug - uo) ** 2 + (vg - vo) ** 2) / np.sum(uo ** 2 + vo ** 2))
+    assert vel < 1e-5
+    g.close()
+    o.close()
+
+
+def test_library_kernels_are_sm100a(gpu_lib):
+    """The loaded kernels are sm_100a code (cudaFuncAttributes::binaryVersion)
+    and the device is a B200-class part."""
+    import ctypes as C
+    ver, sms = C.c_int(), C.c_int()
+    assert gpu_lib.lbm_device_check(C.byref(ver), C.byref(sms)) == 0
+    assert ver.value == 100
+    assert sms.value >= 132

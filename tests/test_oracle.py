@@ -214,11 +214,12 @@ def test_no_body_runs(oracle_mod):
 
 
 def test_geometry_generator_reproduces_reference_boundary_file():
-    """naca0012(204) is the layout of the reference's own boundary.dat."""
-    ref = "/root/reference/boundary.dat"
-    if not os.path.exists(ref):
-        pytest.skip("reference tree not present")
+    """naca0012(204) is the layout of the reference's own boundary.dat
+    (tests/golden/reference_boundary.dat is that file, byte for byte: the
+    205-point closed NACA 0012 contour in chords, (2f14.8))."""
+    ref = os.path.join(os.path.dirname(__file__), "golden", "reference_boundary.dat")
     d = np.loadtxt(ref)
+    assert d.shape == (205, 2)
     x, y = cases.naca0012(204)
     assert np.abs(x - d[:, 0]).max() < 1.5e-8
     assert np.abs(y - d[:, 1]).max() < 1.5e-8
