@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--ny", type=int, default=2048)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched and served measurements")
     return ap.parse_args()
 
 
@@ -304,6 +305,9 @@ def run_ours(args, world, rank, local):
         torch.distributed.barrier()
     if rank == 0 and world == 1 and not args.no_e2e:
         line["e2e"] = run_e2e(args, lib)
+    if rank == 0 and world == 1 and not args.no_batch:
+        line["batched"] = run_batched(lib)
+        line["served"] = run_served(lib)
     if rank == 0 and world == 1 and not args.no_cpu:
         mlups, steps, cores, el = cpu_oracle_rate(large_case(args, n_steps=200, precision="fp64"))
         line["cpu_baseline"] = {"value": mlups, "unit": UNIT, "cores": cores, "kind": "port",
@@ -354,6 +358,54 @@ def run_e2e(args, lib):
             "stages_ms": stages,
             "note": "wall clock around the C-ABI calls (create, boundary, motion table, init, run, fields); "
                     "set-up upload and final fields amortised over the steps"}
+
+
+def run_batched(lib, n_cases=64, steps=100, warmup=12):
+    """The metric's batched form: a seeded sweep of cases of different grids
+    and kinematics (Nx in [512, 2048], Ny = Nx/2, chord = Ny/4; Re, heave,
+    pitch, phase, St drawn per case), stepped one at a time in FP32
+    (lbm_run per case) and together as one batch in FP16 storage
+    (lbm_batch_run). Cases per hour extrapolate each form's measured lattice
+    update rate to 5 flapping periods of every case."""
+    from fortran_loadfile_mitiwing_b200 import sweep
+    specs = sweep.sweep_specs(n_cases, 2026)
+    t0 = time.perf_counter()
+    r_alone, _ = sweep.run_alone(specs, steps, warmup, "fp32", lib)
+    r16, _, _, rows = sweep.run_batch(specs, steps, warmup, "fp16", lib)
+    base, b16 = sweep.cases_per_hour(specs, r_alone), sweep.cases_per_hour(specs, r16)
+    return {"cases": n_cases, "steps_per_case": steps, "alone_fp32_mlups": r_alone / 1e6,
+            "batch_fp16_mlups": r16 / 1e6, "alone_fp32_cases_per_hour": base, "batch_fp16_cases_per_hour": b16,
+            "batch_fp16_vs_alone_fp32": b16 / base, "rows_per_cta": rows,
+            "wall_s": time.perf_counter() - t0}
+
+
+def run_served(lib, n_req=64, rate=32.0, periods=3.0, check=8):
+    """The metric's served form: the same case distribution arriving as a
+    Poisson stream at `rate` requests/s in real time, each solved for
+    `periods` flapping periods with continuous batching in FP16 storage under
+    a 150 GB budget; p50/p99 time from arrival to result and cases per hour,
+    against FP32 one-at-a-time service of the same arrivals (first come, first
+    served, each case's service time measured alone), and the first `check`
+    results' per-period mean C_D and C_L against the same cases in FP64."""
+    from fortran_loadfile_mitiwing_b200 import serve, sweep
+    specs = sweep.sweep_specs(n_req, 2026)
+    t0 = time.perf_counter()
+    service = serve.alone_service_times(specs, periods, lib=lib)
+    res, summ = serve.serve_stream(specs, rate, periods, 150e9, "fp16", 100, seed=2026, lib=lib,
+                                   keep_rows=set(range(check)))
+    ref = serve.fp64_reference_rows(specs[:check], periods, lib)
+    errs = [serve.period_errors(res[i].rows, ref[i], specs[i]["period_steps"], periods) for i in range(check)]
+    arr = serve.poisson_arrivals(rate, n_req, 2026)
+    fin = serve.fifo_one_at_a_time(arr, service)
+    lat = [f - a for f, a in zip(fin, arr)]
+    alone_cph = n_req * 3600.0 / float(max(fin))
+    return {"requests": n_req, "rate_per_s": rate, "periods": periods, "storage": "fp16",
+            "p50_s": summ["p50_s"], "p99_s": summ["p99_s"], "cases_per_hour": summ["cases_per_hour"],
+            "fp32_one_at_a_time_p50_s": serve.percentile(lat, 50), "fp32_one_at_a_time_p99_s": serve.percentile(lat, 99),
+            "fp32_one_at_a_time_cases_per_hour": alone_cph, "vs_fp32_one_at_a_time": summ["cases_per_hour"] / alone_cph,
+            "max_period_mean_err_cd_vs_fp64": max(e["cd"] for e in errs),
+            "max_period_mean_err_cl_vs_fp64": max(e["cl"] for e in errs),
+            "peak_cases": summ["peak_cases"], "wall_s": time.perf_counter() - t0}
 
 
 def main():

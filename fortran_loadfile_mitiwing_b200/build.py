@@ -12,7 +12,8 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "liblbmb200.so")
 ROOT = os.path.dirname(HERE)
 
-SOURCES = ["lbm_capi.cu", "kf_kernel.cu", "ib_kernels.cu", "host_io.cu", "residual_device.cu", "lbm_batch.cu", "output_io.cu"]
+SOURCES = ["lbm_capi.cu", "kf_kernel.cu", "ib_kernels.cu", "host_io.cu", "host_xfer.cu", "residual_device.cu",
+           "lbm_batch.cu", "output_io.cu"]
 HEADERS = ["lbm_common.cuh", "lbm_internal.h"]
 
 NVCC_FLAGS = [
@@ -39,28 +40,31 @@ def _stale():
     return any(os.path.getmtime(d) > t for d in deps)
 
 
-def build(force=False, verbose=False):
-    """Compiles every CUDA source into one shared library; returns its path."""
-    if not force and not _stale():
+def build(force=False, verbose=False, out=None, defines=()):
+    """Compiles every CUDA source into one shared library; returns its path.
+    `out` and `defines` (-D values) build a variant elsewhere, for tuning."""
+    lib = out or LIB
+    if not force and out is None and not _stale():
         return LIB
-    os.makedirs(LIBDIR, exist_ok=True)
+    libdir = os.path.dirname(lib)
+    os.makedirs(libdir, exist_ok=True)
     objs = []
     for src in SOURCES:
-        obj = os.path.join(LIBDIR, src.replace(".cu", ".o"))
-        cmd = [_nvcc(), *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-c",
+        obj = os.path.join(libdir, src.replace(".cu", ".o"))
+        cmd = [_nvcc(), *NVCC_FLAGS, *[f"-D{d}" for d in defines], "-I", os.path.join(ROOT, "include"), "-c",
                os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
         objs.append(obj)
-    cmd = [_nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", LIB,
+    cmd = [_nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", lib,
            "-Xlinker", "--exclude-libs,ALL"]
     if verbose:
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
     for o in objs:
         os.remove(o)
-    return LIB
+    return lib
 
 
 DRIVER_SRC = os.path.join(CSRC, "lbm_main.cpp")

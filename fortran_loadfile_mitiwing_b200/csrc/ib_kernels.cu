@@ -60,14 +60,23 @@ namespace {
 
 constexpr int BS = 16;                 // block size of the cyclic reduction
 constexpr int NMARK_MAX = 2048;        // largest marker count
-constexpr int FACTOR_THREADS = 512;
+#ifndef LBM_FACTOR_THREADS
+#define LBM_FACTOR_THREADS 512
+#endif
+#ifndef LBM_SOLVE_THREADS
+#define LBM_SOLVE_THREADS 1024
+#endif
+#ifndef LBM_SOLVE_SMEM
+#define LBM_SOLVE_SMEM 232192
+#endif
+constexpr int FACTOR_THREADS = LBM_FACTOR_THREADS;
 constexpr int BOPS_WARPS = FACTOR_THREADS / 32;   // warps running block operations
-constexpr int SOLVE_THREADS = 1024;
+constexpr int SOLVE_THREADS = LBM_SOLVE_THREADS;
 constexpr int STAGE_BLOCKS = 32;       // factor blocks of one level staged in shared memory by ib_solve
 constexpr int FL = 2 * BS;             // columns of a coupling panel [L_o | L_q^T]
 constexpr int GW = 3 * BS;             // row width of a stored factor block [D^-1 | F_L | F_U]
 constexpr int GP = BS + 1;             // padded row stride of square blocks in shared memory
-constexpr int SOLVE_SMEM_BUDGET = 232192;   // dynamic shared memory of ib_solve (bytes)
+constexpr int SOLVE_SMEM_BUDGET = LBM_SOLVE_SMEM;   // dynamic shared memory of ib_solve (bytes)
 
 // factor blocks ib_solve can stage next to the right-hand sides of nb blocks
 __host__ __device__ constexpr int stage_cap(int nb)
@@ -658,7 +667,7 @@ __device__ void dense_tri(const IBArgs &a, double *yv)
 // keeps D_0^-1. The even neighbours are updated as
 //   D_e -= L_q^T F_L(q) + L_e F_U(p),   L_e <- -L_e F_L(p)   (p = e - st, q = e + st).
 template <bool BATCH>
-__global__ void __launch_bounds__(FACTOR_THREADS) ib_factor(const IBArgs base0, const IBArgs *batch, int step0)
+__global__ void __launch_bounds__(FACTOR_THREADS, 65536 / (FACTOR_THREADS * 128)) ib_factor(const IBArgs base0, const IBArgs *batch, int step0)
 {
     const IBArgs &base = BATCH ? batch[blockIdx.z] : base0;
     const int step_index = factor_step<BATCH>(base, step0);
@@ -852,7 +861,7 @@ __global__ void __launch_bounds__(FACTOR_THREADS) ib_factor(const IBArgs base0, 
 // blocks, then the right-hand sides in the solve order (two per marker,
 // padded to whole blocks), then the mbarrier.
 template <bool BATCH>
-__global__ void __launch_bounds__(SOLVE_THREADS) ib_solve(const IBArgs a0, const IBArgs *batch, int step_index,
+__global__ void __launch_bounds__(SOLVE_THREADS, 1024 / SOLVE_THREADS) ib_solve(const IBArgs a0, const IBArgs *batch, int step_index,
                                                           int ring_slot)
 {
     const IBArgs &a = BATCH ? batch[blockIdx.z] : a0;

@@ -161,20 +161,26 @@ __global__ void __launch_bounds__(128) kf_vec(const KFArgs<C> a)
 // KS x 9 row segments in flight per CTA without holding them in registers.
 // Rows 0 and ny-1 are handled by one extra CTA row of the grid, and columns
 // 0 and nx-1 by the scalar edge path. With FP32 arithmetic (FP32, FP16 and
-// BF16 storage) a thread updates two rows of its column at once with the
-// paired FP32 instructions (collide_pair), which halves the arithmetic
-// instructions of the collision.
+// BF16 storage) a thread updates two nodes at once with the paired FP32
+// instructions (collide_pair), which halves the arithmetic instructions of
+// the collision: with FP32 storage rows j and j+1 of its column, with 2-byte
+// storage columns i and i+1 of one row. The 2-byte column pair is one 32-bit
+// word in shared and in global memory, so it is read with one load (two for
+// the x-shifted planes, joined by a byte permute), converted with one paired
+// conversion and written with one store; the CTA's strip is then 512
+// columns wide, and each staged row segment is 1 KB, as with FP32 storage.
 
-constexpr int TW = 256;        // strip width (threads per CTA)
+constexpr int TW = 256;        // threads per CTA (the strip width of 4- and 8-byte storage)
 #ifndef LBM_KF_STAGES
 #define LBM_KF_STAGES 4
 #endif
 #ifndef LBM_KF_MINB
 #define LBM_KF_MINB 4
 #endif
-// pipeline stages: 2-byte storage halves the bytes of a stage, so it keeps
-// twice the stages to hold the same bytes in flight
-template <typename T> __host__ __device__ constexpr int tma_stages() { return sizeof(T) == 2 ? 2 * LBM_KF_STAGES : LBM_KF_STAGES; }
+// pipeline stages (a stage holds the 9 plane rows of one output row)
+template <typename T> __host__ __device__ constexpr int tma_stages() { return LBM_KF_STAGES; }
+// columns of a CTA's strip: two per thread with 2-byte storage
+template <typename T> __host__ __device__ constexpr int tma_strip() { return sizeof(T) == 2 ? 2 * TW : TW; }
 // Resident CTAs per SM the register budget is sized for (64 registers a
 // thread at four). Four keep more rows in flight than three, which leave
 // registers free for the immersed-boundary CTAs beside the lattice update
@@ -188,8 +194,41 @@ template <typename T> constexpr int kf_minb() { return sizeof(T) == 8 ? 3 : KF_M
 // mbarrier and bulk-copy helpers: lbm_common.cuh
 
 template <typename T> __host__ __device__ constexpr int tma_halo() { return 16 / (int)sizeof(T); }
-template <typename T> __host__ __device__ constexpr int tma_seg() { return TW + 2 * tma_halo<T>(); }
+template <typename T> __host__ __device__ constexpr int tma_seg() { return tma_strip<T>() + 2 * tma_halo<T>(); }
 template <typename T> constexpr size_t tma_smem() { return sizeof(T) * tma_stages<T>() * 9 * tma_seg<T>() + 2 * 8 * tma_stages<T>(); }
+
+// the updated pair of columns i, i+1 of row j (2-byte storage): one 32-bit
+// store per plane when both nodes are written (v0, v1), else the one that is
+template <typename T, bool FIELDS>
+__device__ __forceinline__ void store_pair2(const KFArgs<float> &a, T *__restrict__ fout, int i, int j, bool v0,
+                                            bool v1, const float2 o[9], float2 frho, float2 fu, float2 fv)
+{
+    const long long base = (long long)j * a.pitch + i;
+    if (v0 && v1) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k)
+            *reinterpret_cast<uint32_t *>(fout + (long long)k * a.plane + base) = Pair2<T>::pack(o[k]);
+    } else if (v0) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) fout[(long long)k * a.plane + base] = Store<T>::pack(o[k].x);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) fout[(long long)k * a.plane + base + 1] = Store<T>::pack(o[k].y);
+    }
+    if (FIELDS) {
+        const long long q = (long long)j * a.nx + i;
+        if (v0) {
+            a.rho_out[q] = frho.x;
+            a.u_out[q] = fu.x;
+            a.v_out[q] = fv.x;
+        }
+        if (v1) {
+            a.rho_out[q + 1] = frho.y;
+            a.u_out[q + 1] = fu.y;
+            a.v_out[q + 1] = fv.y;
+        }
+    }
+}
 
 // One CTA of the staged kernel: strip bx (of gx) and row chunk by (of gy; the
 // last chunk is the edge CTA row) of the lattice described by `a`.
@@ -197,23 +236,25 @@ template <typename T, typename C, bool FIELDS, bool CONS0>
 __device__ __forceinline__ void kf_tma_cta(const KFArgs<C> &a, int bx, int by, int gx, int gy, unsigned char *smraw)
 {
     constexpr int H = tma_halo<T>(), SEG = tma_seg<T>(), NWARP = TW / 32, KS = tma_stages<T>();
+    constexpr int SW = tma_strip<T>();
+    constexpr bool XPAIR = sizeof(T) == 2;   // two columns per thread
     T *buf = reinterpret_cast<T *>(smraw);
     uint64_t *full = reinterpret_cast<uint64_t *>(smraw + sizeof(T) * KS * 9 * SEG);
     uint64_t *empty = full + KS;
     const int tid = threadIdx.x, lane = tid & 31;
-    const int x0 = bx * TW;
-    const int i = x0 + tid;
+    const int x0 = bx * SW;
+    const int i = x0 + (XPAIR ? 2 * tid : tid);
     const T *__restrict__ fin = (const T *)a.fin;
     T *__restrict__ fout = (T *)a.fout;
     const PatchInfo rr = a.mode == KF_OUTER ? *a.pinfo : PatchInfo{0, 0, 0, 0};   // step's patch rectangle
     if (by == gy - 1) {
         // the edge nodes: rows 0 and ny-1 of this strip, and a share of the
         // nodes of columns 0 and nx-1 (which the strips' row sweeps skip)
-        if (i < a.nx)
+        for (int ie = x0 + tid; ie < min(x0 + SW, a.nx); ie += TW)
             for (int j = 0; j < a.ny; j += a.ny - 1) {
                 C gout[9], frho, fu, fv;
-                edge_update<T, C>(a, fin, i, j, gout, frho, fu, fv);
-                store_node<T, C, FIELDS>(a, fout, i, j, gout, frho, fu, fv);
+                edge_update<T, C>(a, fin, ie, j, gout, frho, fu, fv);
+                store_node<T, C, FIELDS>(a, fout, ie, j, gout, frho, fu, fv);
             }
         for (int q = bx * TW + tid; q < 2 * (a.ny - 2); q += gx * TW) {
             const int j = 1 + q / 2, ie = (q & 1) ? a.nx - 1 : 0;
@@ -226,7 +267,7 @@ __device__ __forceinline__ void kf_tma_cta(const KFArgs<C> &a, int bx, int by, i
     const int j0 = 1 + by * a.rows_per_cta;
     const int nrows = min(a.rows_per_cta, a.ny - 1 - j0);
     if (nrows <= 0) return;
-    const int width = min(TW, a.nx - x0);
+    const int width = min(SW, a.nx - x0);
     const uint32_t bytes = (uint32_t)((((width + 2 * H) * (int)sizeof(T)) + 15) / 16 * 16);
     if (tid == 0) {
         for (int s = 0; s < KS; ++s) {
@@ -258,7 +299,39 @@ __device__ __forceinline__ void kf_tma_cta(const KFArgs<C> &a, int bx, int by, i
     // with row r + KS once all warps have arrived. Only warp 0 waits for the
     // other warps; they run up to KS - 1 rows ahead.
     bool ok = true;
-    if constexpr (std::is_same<C, float>::value) {
+    if constexpr (XPAIR) {
+        // 2-byte storage: columns i and i+1 of each row as one pair
+        for (int r = 0; r < nrows; ++r) {
+            const int s = r % KS, j = j0 + r;
+            const uint32_t parity = (uint32_t)((r / KS) & 1);
+            if (!wait(&full[s], parity)) { ok = false; break; }
+            const bool v0 = i >= 1 && i <= a.nx - 2 && !(a.mode == KF_OUTER && corr_tile(a, rr, i, j));
+            const bool v1 = i + 1 <= a.nx - 2 && !(a.mode == KF_OUTER && corr_tile(a, rr, i + 1, j));
+            if (v0 || v1) {
+                float2 g[9], o[9], frho, fu, fv;
+                // word t of a staged plane row holds the columns x0 + 2t, x0 + 2t + 1
+                const uint32_t *w = reinterpret_cast<const uint32_t *>(buf + s * 9 * SEG + H) + tid;
+#pragma unroll
+                for (int k = 0; k < 9; ++k) {
+                    const uint32_t *wk = w + k * (SEG / 2);
+                    uint32_t pr;
+                    if (lbm_ex(k) == 0) pr = wk[0];
+                    else if (lbm_ex(k) == 1) pr = __byte_perm(wk[-1], wk[0], 0x5432);   // columns i-1, i
+                    else pr = __byte_perm(wk[0], wk[1], 0x5432);                        // columns i+1, i+2
+                    g[k] = Pair2<T>::unpack(pr);
+                }
+                collide_pair<CONS0, FIELDS>(a, g, o, frho, fu, fv);
+                store_pair2<T, FIELDS>(a, fout, i, j, v0, v1, o, frho, fu, fv);
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[s]);
+            if (tid == 0 && r + KS < nrows) {
+                if (!wait(&empty[s], parity)) { ok = false; break; }
+                fence_proxy_async();
+                issue(r + KS);
+            }
+        }
+    } else if constexpr (std::is_same<C, float>::value) {
         // FP32 arithmetic: rows r and r + 1 of a thread's column as one pair
         // of the paired instructions (collide_pair); an odd last row is
         // computed in both halves and stored once
@@ -381,7 +454,7 @@ void launch_tma_f(const KFArgs<C> &a, const KFArgs<C> *da, dim3 grid, dim3 block
 template <typename T, typename C>
 void launch_tma(const KFArgs<C> &a, const KFArgs<C> *da, bool fields, int nx, int ny, cudaStream_t st)
 {
-    dim3 block(TW, 1), grid((nx + TW - 1) / TW, (ny - 2 + a.rows_per_cta - 1) / a.rows_per_cta + 1);
+    dim3 block(TW, 1), grid((nx + tma_strip<T>() - 1) / tma_strip<T>(), (ny - 2 + a.rows_per_cta - 1) / a.rows_per_cta + 1);
     const size_t smem = tma_smem<T>();
     if (fields)
         launch_tma_f<T, C, true>(a, da, grid, block, smem, st);
@@ -460,9 +533,10 @@ int configure_tma()
 
 // case table entry {case, strip, chunk, gx | gy << 16} of the staged kernel's
 // grid for one lattice
-void tma_grid(int nx, int ny, int rows_per_cta, int *gx, int *gy)
+void tma_grid(int nx, int ny, int rows_per_cta, size_t elem, int *gx, int *gy)
 {
-    *gx = (nx + TW - 1) / TW;
+    const int sw = elem == 2 ? tma_strip<__half>() : TW;
+    *gx = (nx + sw - 1) / sw;
     *gy = (ny - 2 + rows_per_cta - 1) / rows_per_cta + 1;
 }
 
@@ -703,7 +777,7 @@ void kf_args_write(lbm_handle *h, const void *fin, void *fout, void *fields, int
         *(KFArgs<float> *)dst = make_kf_args<float>(h, fin, fout, fields, mode);
 }
 
-void kf_tma_grid(const lbm_handle *h, int *gx, int *gy) { tma_grid(h->nx, h->ny, h->kf_rows, gx, gy); }
+void kf_tma_grid(const lbm_handle *h, int *gx, int *gy) { tma_grid(h->nx, h->ny, h->kf_rows, h->elem, gx, gy); }
 
 // the staged lattice kernel over a batch of cases (device arrays of their
 // arguments and of the case table)

@@ -905,12 +905,16 @@ int lbm_init(lbm_t *h, const double *du, const double *dv)
         const int rc = handle_set_edges(h, ef.data());
         if (rc) return rc;
     }
-    // populations and the initial fields (rho = 1, u, v) in slot 0: u0 of the first step
+    // populations and the initial fields (rho = 1, u, v) in slot 0: u0 of the
+    // first step. The perturbation goes up into the second population buffer,
+    // which the first step overwrites before anything reads it: 9 planes of
+    // at least nx*ny elements of at least 2 bytes hold the 2*nx*ny doubles,
+    // and no allocation is needed.
     double *ddu = nullptr, *ddv = nullptr;
     if (du || dv) {
-        if (!h->d_stage) CK(dmalloc(h, &h->d_stage, sizeof(double) * nn * 2), "alloc stage");
-        if (du) CK(cudaMemcpyAsync(ddu = h->d_stage, du, sizeof(double) * nn, cudaMemcpyHostToDevice, h->stream), "copy du");
-        if (dv) CK(cudaMemcpyAsync(ddv = h->d_stage + nn, dv, sizeof(double) * nn, cudaMemcpyHostToDevice, h->stream), "copy dv");
+        double *stage = (double *)h->fbuf[1];
+        if (du) CK(xfer_h2d(ddu = stage, du, sizeof(double) * nn, h->stream), "copy du");
+        if (dv) CK(xfer_h2d(ddv = stage + nn, dv, sizeof(double) * nn, h->stream), "copy dv");
     }
     if (launch_init_lattice(h, ddu, ddv)) return cuda_err(h, cudaGetLastError(), "init");
     h->cur = 0;
@@ -920,7 +924,6 @@ int lbm_init(lbm_t *h, const double *du, const double *dv)
     CK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->stream), "clear status");
     CK(cudaMemsetAsync(h->d_pinfo, 0, LBM_NSLOT_MAX * sizeof(PatchInfo), h->stream), "clear pinfo");
     CK(cudaStreamSynchronize(h->stream), "sync init");
-    free_devp(h->d_stage);   // the FP64 staging planes are made for each transfer, not kept
     h->n = 1;
     h->steps_done = 0;
     // the patch rectangles were cleared above: the factorization slots are
@@ -957,21 +960,13 @@ int lbm_get_fields(lbm_t *h, double *rho, double *u, double *v)
         return set_err(h, LBM_ERR_STATE, "get_fields: the last step did not keep its fields");
     const size_t nn = (size_t)h->nx * h->ny;
     double *dst[3] = {rho, u, v};
-    if (h->prec == LBM_PREC_FP64) {
-        for (int c = 0; c < 3; ++c)
-            if (dst[c])
-                CK(cudaMemcpyAsync(dst[c], (const double *)h->d_fields[slot] + c * nn, sizeof(double) * nn,
-                                   cudaMemcpyDeviceToHost, h->stream), "copy fields");
-        CK(cudaStreamSynchronize(h->stream), "sync fields");
-    } else {
-        std::vector<float> tmp(nn);
-        for (int c = 0; c < 3; ++c) {
-            if (!dst[c]) continue;
-            CK(cudaMemcpyAsync(tmp.data(), (const float *)h->d_fields[slot] + c * nn, sizeof(float) * nn,
-                               cudaMemcpyDeviceToHost, h->stream), "copy fields");
-            CK(cudaStreamSynchronize(h->stream), "sync fields");
-            for (size_t q = 0; q < nn; ++q) dst[c][q] = tmp[q];
-        }
+    for (int c = 0; c < 3; ++c) {
+        if (!dst[c]) continue;
+        if (h->prec == LBM_PREC_FP64)
+            CK(xfer_d2h(dst[c], (const double *)h->d_fields[slot] + c * nn, sizeof(double) * nn, h->stream),
+               "copy fields");
+        else
+            CK(xfer_d2h_widen(dst[c], (const float *)h->d_fields[slot] + c * nn, nn, h->stream), "copy fields");
     }
     return LBM_OK;
 }
@@ -983,8 +978,7 @@ int lbm_get_populations(lbm_t *h, double *f)
     const size_t nn = (size_t)h->nx * h->ny;
     if (!h->d_stage) CK(dmalloc(h, &h->d_stage, sizeof(double) * nn * 9), "alloc stage");
     if (launch_unpack(h, h->fbuf[h->cur], h->d_stage)) return cuda_err(h, cudaGetLastError(), "unpack");
-    CK(cudaMemcpyAsync(f, h->d_stage, sizeof(double) * nn * 9, cudaMemcpyDeviceToHost, h->stream), "copy f");
-    CK(cudaStreamSynchronize(h->stream), "sync f");
+    CK(xfer_d2h(f, h->d_stage, sizeof(double) * nn * 9, h->stream), "copy f");
     free_devp(h->d_stage);
     return LBM_OK;
 }
@@ -996,7 +990,7 @@ int lbm_set_populations(lbm_t *h, const double *f)
     if (!h->inited) return set_err(h, LBM_ERR_STATE, "set_populations: not initialised");
     const size_t nn = (size_t)h->nx * h->ny;
     if (!h->d_stage) CK(dmalloc(h, &h->d_stage, sizeof(double) * nn * 9), "alloc stage");
-    CK(cudaMemcpyAsync(h->d_stage, f, sizeof(double) * nn * 9, cudaMemcpyHostToDevice, h->stream), "copy f");
+    CK(xfer_h2d(h->d_stage, f, sizeof(double) * nn * 9, h->stream), "copy f");
     if (launch_pack(h, h->d_stage, h->fbuf[h->cur])) return cuda_err(h, cudaGetLastError(), "pack");
     CK(cudaStreamSynchronize(h->stream), "sync f");
     free_devp(h->d_stage);

@@ -13,6 +13,7 @@
 #include <cuda_fp16.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
+#include <string.h>
 
 #define LBM_Q 9
 #define LBM_MAXW 8
@@ -108,6 +109,41 @@ template <> struct Store<__nv_bfloat16> {
     static __device__ __forceinline__ void st(__nv_bfloat16 *p, float x) { *p = __float2bfloat16_rn(x); }
     static __device__ __forceinline__ float cvt(__nv_bfloat16 x) { return __bfloat162float(x); }
     static __device__ __forceinline__ __nv_bfloat16 pack(float x) { return __float2bfloat16_rn(x); }
+};
+
+// two adjacent 2-byte elements as one 32-bit word (low half: the lower
+// column) <-> a float2 (x: the lower column); the paired conversions round
+// each element to nearest, as the scalar ones above do
+template <typename T> struct Pair2;
+template <> struct Pair2<__half> {
+    static __device__ __forceinline__ float2 unpack(uint32_t w)
+    {
+        __half2 h;
+        memcpy(&h, &w, 4);
+        return __half22float2(h);
+    }
+    static __device__ __forceinline__ uint32_t pack(float2 f)
+    {
+        const __half2 h = __float22half2_rn(f);
+        uint32_t w;
+        memcpy(&w, &h, 4);
+        return w;
+    }
+};
+template <> struct Pair2<__nv_bfloat16> {
+    static __device__ __forceinline__ float2 unpack(uint32_t w)
+    {
+        __nv_bfloat162 h;
+        memcpy(&h, &w, 4);
+        return __bfloat1622float2(h);
+    }
+    static __device__ __forceinline__ uint32_t pack(float2 f)
+    {
+        const __nv_bfloat162 h = __float22bfloat162_rn(f);
+        uint32_t w;
+        memcpy(&w, &h, 4);
+        return w;
+    }
 };
 
 // m = M g for the MRT matrix of solution.f90:17-25 (rows: rho, e, eps, jx, qx,

@@ -260,3 +260,9 @@ int launch_mass(lbm_handle *h, const void *fsrc, cudaStream_t st);
 int mass_slots();
 // error code and message of a device status word
 int status_error(unsigned st, std::string &msg);
+// host <-> device copies of host arrays through the pinned staging ring
+// (host_xfer.cu); the d2h calls return with the data on the host, xfer_h2d
+// with the copies queued on st
+cudaError_t xfer_d2h_widen(double *dst, const float *src, size_t n, cudaStream_t st);
+cudaError_t xfer_d2h(void *dst, const void *src, size_t bytes, cudaStream_t st);
+cudaError_t xfer_h2d(void *dst, const void *src, size_t bytes, cudaStream_t st);

@@ -168,9 +168,12 @@ def test_period_errors():
     ref[:, 2] = np.cos(2 * np.pi * t / 100.0)
     got = ref.copy()
     got[100:200, 1] += 0.01          # period 2: C_D mean off by 0.01
+    got[200:300, 2] += 0.005         # period 3: C_L mean off by 0.005
     e = period_errors(got, ref, 100.0, 3)
-    rms = math.sqrt(float(np.mean(ref[100:200, 1] ** 2)))
-    assert abs(e["cd"] - 0.01 / rms) < 1e-12 and e["cl"] < 1e-12
+    mean_cd = abs(float(np.mean(ref[100:200, 1])))              # C_D: relative to |mean|
+    rms_cl = math.sqrt(float(np.mean(ref[200:300, 2] ** 2)))    # C_L: relative to its RMS
+    assert abs(e["cd"] - 0.01 / mean_cd) < 1e-12
+    assert abs(e["cl"] - 0.005 / rms_cl) < 1e-12
 
 
 def test_server_returns_a_failed_case_and_serves_the_rest(monkeypatch):
