@@ -13,6 +13,7 @@
 // Edge nodes recompute the moments of the one or two interior neighbours
 // their formula needs (O(perimeter) extra reads) so that no second launch and
 // no side buffer is needed for the boundary condition.
+#include <algorithm>
 #include <cstring>
 #include <type_traits>
 #include <vector>
@@ -285,12 +286,31 @@ __device__ __forceinline__ void kf_tma_cta(const KFArgs<C> &a, int bx, int by, i
             bulk_g2s(buf + (s * 9 + k) * SEG,
                      fin + (long long)k * a.plane + (long long)(j - lbm_ey(k)) * a.pitch + (x0 - H), bytes, &full[s]);
     };
-    // bounded wait: a barrier that never completes is reported, not waited on forever
+    // bounded wait: a barrier that never completes is reported, not waited on
+    // forever. The outcome is made the same for the whole warp (full_wait), or
+    // broadcast from thread 0 (refill), so that a warp leaves the row loop as
+    // a whole and no lane is left waiting in __syncwarp for one that left.
     auto wait = [&](uint64_t *bar, uint32_t parity) -> bool {
         int spins = 0;
         while (!mbar_try_wait(bar, parity))
             if (++spins > (1 << 22)) return false;
         return true;
+    };
+    auto full_wait = [&](int r) -> bool {
+        return __all_sync(0xffffffffu, wait(&full[r % KS], (uint32_t)((r / KS) & 1)));
+    };
+    // thread 0: refills the stage of row q with row q + KS once every warp is
+    // done with it; false (in every lane of warp 0) if that wait gave up
+    auto refill = [&](int q) -> bool {
+        bool good = true;
+        if (tid == 0 && q + KS < nrows) {
+            good = wait(&empty[q % KS], (uint32_t)((q / KS) & 1));
+            if (good) {
+                fence_proxy_async();
+                issue(q + KS);
+            }
+        }
+        return __shfl_sync(0xffffffffu, good, 0);
     };
     if (tid == 0)
         for (int r = 0; r < KS && r < nrows; ++r) issue(r);
@@ -303,8 +323,7 @@ __device__ __forceinline__ void kf_tma_cta(const KFArgs<C> &a, int bx, int by, i
         // 2-byte storage: columns i and i+1 of each row as one pair
         for (int r = 0; r < nrows; ++r) {
             const int s = r % KS, j = j0 + r;
-            const uint32_t parity = (uint32_t)((r / KS) & 1);
-            if (!wait(&full[s], parity)) { ok = false; break; }
+            if (!full_wait(r)) { ok = false; break; }
             const bool v0 = i >= 1 && i <= a.nx - 2 && !(a.mode == KF_OUTER && corr_tile(a, rr, i, j));
             const bool v1 = i + 1 <= a.nx - 2 && !(a.mode == KF_OUTER && corr_tile(a, rr, i + 1, j));
             if (v0 || v1) {
@@ -325,11 +344,7 @@ __device__ __forceinline__ void kf_tma_cta(const KFArgs<C> &a, int bx, int by, i
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[s]);
-            if (tid == 0 && r + KS < nrows) {
-                if (!wait(&empty[s], parity)) { ok = false; break; }
-                fence_proxy_async();
-                issue(r + KS);
-            }
+            if (!refill(r)) { ok = false; break; }
         }
     } else if constexpr (std::is_same<C, float>::value) {
         // FP32 arithmetic: rows r and r + 1 of a thread's column as one pair
@@ -339,7 +354,7 @@ __device__ __forceinline__ void kf_tma_cta(const KFArgs<C> &a, int bx, int by, i
         for (int r = 0; r < nrows; r += 2) {
             const int r1 = min(r + 1, nrows - 1);
             const int s0 = r % KS, s1 = r1 % KS, j = j0 + r;
-            if (!wait(&full[s0], (uint32_t)((r / KS) & 1)) || !wait(&full[s1], (uint32_t)((r1 / KS) & 1))) {
+            if (!full_wait(r) || !full_wait(r1)) {
                 ok = false;
                 break;
             }
@@ -370,24 +385,15 @@ __device__ __forceinline__ void kf_tma_cta(const KFArgs<C> &a, int bx, int by, i
                 mbar_arrive(&empty[s0]);
                 if (r1 != r) mbar_arrive(&empty[s1]);
             }
-            if (tid == 0) {
-                for (int q = r; q <= r1 && ok; ++q)
-                    if (q + KS < nrows) {
-                        if (!wait(&empty[q % KS], (uint32_t)((q / KS) & 1))) {
-                            ok = false;
-                            break;
-                        }
-                        fence_proxy_async();
-                        issue(q + KS);
-                    }
-                if (!ok) break;
+            if (!refill(r) || (r1 != r && !refill(r1))) {
+                ok = false;
+                break;
             }
         }
     } else
     for (int r = 0; r < nrows; ++r) {
         const int s = r % KS, j = j0 + r;
-        const uint32_t parity = (uint32_t)((r / KS) & 1);
-        if (!wait(&full[s], parity)) { ok = false; break; }
+        if (!full_wait(r)) { ok = false; break; }
         const bool skip = a.mode == KF_OUTER && corr_tile(a, rr, i, j);
         if (i > 0 && i < a.nx - 1 && !skip) {
             C gout[9], frho, fu, fv;
@@ -400,32 +406,76 @@ __device__ __forceinline__ void kf_tma_cta(const KFArgs<C> &a, int bx, int by, i
         }
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[s]);
-        if (tid == 0 && r + KS < nrows) {
-            if (!wait(&empty[s], parity)) { ok = false; break; }
-            fence_proxy_async();
-            issue(r + KS);
-        }
+        if (!refill(r)) { ok = false; break; }
     }
     if (!ok) {
         // report, then wait (bounded) for this CTA's copies still in flight
-        atomicOr(a.status, LBM_ST_TIMEOUT);
+        if (lane == 0) atomicOr(a.status, LBM_ST_TIMEOUT);
         for (int s = 0; s < KS; ++s) {
             int spins = 0;
             while (!mbar_try_wait(&full[s], 0) && !mbar_try_wait(&full[s], 1) && ++spins < (1 << 20)) {
             }
         }
     }
+    // every thread is done with the ring: its barriers are invalidated, so
+    // that the next item of a persistent CTA can initialise them again
+    __syncthreads();
+    if (tid == 0)
+        for (int s = 0; s < KS; ++s) {
+            mbar_inval(&full[s]);
+            mbar_inval(&empty[s]);
+        }
 }
 
-// The arguments are read from global memory (the handle's table of argument
-// variants, kf_table_entry): loaded where used rather than held in registers
-// as kernel parameters would be, which keeps the kernel within the 64
-// registers of 4 CTAs per SM.
+// SM identifier of the executing CTA, and the number of identifiers
+static __device__ __forceinline__ unsigned sm_id()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
+    return r;
+}
+static __device__ __forceinline__ unsigned sm_ids()
+{
+    unsigned r;
+    asm volatile("mov.u32 %0, %%nsmid;" : "=r"(r));
+    return r;
+}
+
+// The single-case lattice update as a persistent kernel: about one wave of
+// CTAs (kf_minb per SM) that take the work items (strip, row chunk) from a
+// queue in global memory, the edge row's items first, until none is left.
+// CTAs that land on the last `reserve` SM identifiers take no item, so that
+// those SMs stay free for the immersed-boundary kernels running beside the
+// update on the side stream (the solve and the factorization need a whole
+// SM each). The last CTA to finish resets the queue for the next launch on
+// the same stream. No CTA waits for another one.
+// The arguments are __grid_constant__ kernel parameters, read in place from
+// the parameter bank: no global loads of them in the row loop (measured as
+// 6.6 loads per node when they were read from a table in global memory,
+// which every store may alias) and no registers held for them.
 template <typename T, typename C, bool FIELDS, bool CONS0>
-__global__ void __launch_bounds__(TW, kf_minb<T>()) kf_tma(const KFArgs<C> *__restrict__ a)
+__global__ void __launch_bounds__(TW, kf_minb<T>())
+    kf_tma(const __grid_constant__ KFArgs<C> a, int gx, int gy, unsigned *queue, int reserve)
 {
     extern __shared__ __align__(128) unsigned char smraw[];
-    kf_tma_cta<T, C, FIELDS, CONS0>(*a, blockIdx.x, blockIdx.y, gridDim.x, gridDim.y, smraw);
+    __shared__ int item;
+    const int nitems = gx * gy;
+    if (sm_id() + (unsigned)reserve < sm_ids()) {
+        for (;;) {
+            if (threadIdx.x == 0) item = (int)atomicAdd(queue, 1u);
+            __syncthreads();
+            const int it = item;
+            if (it >= nitems) break;
+            // the edge row (chunk gy - 1) first: its nodes take longer
+            const int by = it < gx ? gy - 1 : (it - gx) / gx, bx = it % gx;
+            kf_tma_cta<T, C, FIELDS, CONS0>(a, bx, by, gx, gy, smraw);
+            __syncthreads();   // the ring and `item` are reused by the next item
+        }
+    }
+    if (threadIdx.x == 0 && atomicAdd(queue + 1, 1u) == gridDim.x - 1) {
+        queue[0] = 0u;   // every CTA has left the loop
+        queue[1] = 0u;
+    }
 }
 
 // Several lattices (a batch of cases) in one launch: CTA b runs entry b of
@@ -442,71 +492,27 @@ __global__ void __launch_bounds__(TW, kf_minb<T>()) kf_tma_multi(const KFArgs<C>
 template <typename C> bool cons0(const KFArgs<C> &a) { return a.s[0] == C(0) && a.s[3] == C(0) && a.s[5] == C(0); }
 
 template <typename T, typename C, bool FIELDS>
-void launch_tma_f(const KFArgs<C> &a, const KFArgs<C> *da, dim3 grid, dim3 block, size_t smem, cudaStream_t st)
+void launch_tma_f(const KFArgs<C> &a, int ctas, int gx, int gy, unsigned *queue, int reserve, cudaStream_t st)
 {
-    if (cons0(a))
-        kf_tma<T, C, FIELDS, true><<<grid, block, smem, st>>>(da);
-    else
-        kf_tma<T, C, FIELDS, false><<<grid, block, smem, st>>>(da);
-}
-
-// a: the launch's arguments on the host; da: the same in device memory
-template <typename T, typename C>
-void launch_tma(const KFArgs<C> &a, const KFArgs<C> *da, bool fields, int nx, int ny, cudaStream_t st)
-{
-    dim3 block(TW, 1), grid((nx + tma_strip<T>() - 1) / tma_strip<T>(), (ny - 2 + a.rows_per_cta - 1) / a.rows_per_cta + 1);
     const size_t smem = tma_smem<T>();
-    if (fields)
-        launch_tma_f<T, C, true>(a, da, grid, block, smem, st);
+    if (cons0(a))
+        kf_tma<T, C, FIELDS, true><<<ctas, TW, smem, st>>>(a, gx, gy, queue, reserve);
     else
-        launch_tma_f<T, C, false>(a, da, grid, block, smem, st);
+        kf_tma<T, C, FIELDS, false><<<ctas, TW, smem, st>>>(a, gx, gy, queue, reserve);
 }
 
-// The handle's table of lattice-argument variants in device memory: the
-// populations' current buffer (2) x the fields written (none, slot 0, slot 1)
-// x the step's slot (patch rectangle and tile lists, LBM_NSLOT_MAX) x the
-// mode (KF_ALL, KF_OUTER), KF_ARGS_STRIDE bytes each. Built when first
-// needed and again after the immersed-boundary scratch or the rows per CTA
-// change.
-template <typename C>
-int kf_table_build(lbm_handle *h)
+// one wave of persistent CTAs over the (strip, row chunk) items of the lattice
+template <typename T, typename C>
+void launch_tma(const lbm_handle *h, const KFArgs<C> &a, bool fields, cudaStream_t st)
 {
-    static_assert(sizeof(KFArgs<C>) <= KF_ARGS_STRIDE, "KFArgs larger than its table stride");
-    if (h->fstream) cudaStreamSynchronize(h->fstream);
-    if (h->side) cudaStreamSynchronize(h->side);
-    cudaStreamSynchronize(h->stream);   // no queued launch still reads the table
-    std::vector<unsigned char> host((size_t)KF_TABLE_ENTRIES * KF_ARGS_STRIDE, 0);
-    const int saved = h->pinfo_slot;
-    for (int cur = 0; cur < 2; ++cur)
-        for (int fsel = 0; fsel < 3; ++fsel)
-            for (int q = 0; q < LBM_NSLOT_MAX; ++q)
-                for (int mode = 0; mode < 2; ++mode) {
-                    h->pinfo_slot = q;
-                    const KFArgs<C> a = make_kf_args<C>(h, h->fbuf[cur], h->fbuf[cur ^ 1],
-                                                        fsel ? h->d_fields[fsel - 1] : nullptr, mode);
-                    const size_t e = ((size_t)((cur * 3 + fsel) * LBM_NSLOT_MAX + q) * 2 + mode);
-                    memcpy(host.data() + e * KF_ARGS_STRIDE, &a, sizeof a);
-                }
-    h->pinfo_slot = saved;
-    if (cudaMemcpy(h->d_kftab, host.data(), host.size(), cudaMemcpyHostToDevice) != cudaSuccess) return -1;
-    h->kftab_rows = h->kf_rows;
-    h->kftab_ok = 1;
-    return 0;
-}
-
-// the table entry of a launch; null if the launch is not one of the variants
-template <typename C>
-const KFArgs<C> *kf_table_entry(lbm_handle *h, const void *fin, void *fout, void *fields, int mode)
-{
-    if (!h->d_kftab) return nullptr;
-    if ((!h->kftab_ok || h->kftab_rows != h->kf_rows) && kf_table_build<C>(h)) return nullptr;
-    const int cur = fin == h->fbuf[0] ? 0 : (fin == h->fbuf[1] ? 1 : -1);
-    const int fsel = !fields ? 0 : (fields == h->d_fields[0] ? 1 : (fields == h->d_fields[1] ? 2 : -1));
-    if (cur < 0 || fsel < 0 || fout != h->fbuf[cur ^ 1] || h->pinfo_slot < 0 || h->pinfo_slot >= LBM_NSLOT_MAX ||
-        (mode != KF_ALL && mode != KF_OUTER))
-        return nullptr;
-    const size_t e = ((size_t)((cur * 3 + fsel) * LBM_NSLOT_MAX + h->pinfo_slot) * 2 + mode);
-    return (const KFArgs<C> *)((const unsigned char *)h->d_kftab + e * KF_ARGS_STRIDE);
+    const int gx = (h->nx + tma_strip<T>() - 1) / tma_strip<T>();
+    const int gy = (h->ny - 2 + a.rows_per_cta - 1) / a.rows_per_cta + 1;
+    const int ctas = std::min(gx * gy, std::max(1, h->sm_count) * kf_minb<T>());
+    const int reserve = std::min(h->kf_reserve, std::max(0, h->sm_count - 1));
+    if (fields)
+        launch_tma_f<T, C, true>(a, ctas, gx, gy, h->d_queue, reserve, st);
+    else
+        launch_tma_f<T, C, false>(a, ctas, gx, gy, h->d_queue, reserve, st);
 }
 
 template <typename T, typename C, bool FIELDS, bool CONS0>
@@ -564,9 +570,7 @@ int launch_kf_t(lbm_handle *h, const void *fin, void *fout, void *fields, int mo
             if (configure_tma<T, C>()) return -1;
             configured = true;
         }
-        const KFArgs<C> *da = kf_table_entry<C>(h, fin, fout, fields, mode);
-        if (!da) return -1;
-        launch_tma<T, C>(a, da, fields != nullptr, h->nx, h->ny, st);
+        launch_tma<T, C>(h, a, fields != nullptr, st);
     } else if (mode == KF_ALL && vec == 4 && h->pitch % 4 == 0) {
         launch_vec<T, C, 4>(a, fields != nullptr, h->nx, h->ny, st);
     } else if (mode == KF_ALL && vec == 2 && h->pitch % 2 == 0) {

@@ -20,6 +20,8 @@ const double kWref[9] = {4.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0,
 const int kEx[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
 const int kEy[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
 const int kRing = 2048;   // force rows kept on the device between host copies
+// SMs the single-case lattice kernel leaves to the immersed-boundary kernels
+const int kKfReserve = 2;
 
 int set_err(lbm_handle *h, int code, const char *msg)
 {
@@ -166,7 +168,6 @@ void free_ib(lbm_handle *h)
     if (h->side) cudaStreamSynchronize(h->side);
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->ib_ready = 0;
-    h->kftab_ok = 0;   // the lattice arguments point into the scratch
     h->batch_in_half[0] = h->batch_in_half[1] = -1;
     free_devp(h->d_mk); free_devp(h->d_rhs); free_devp(h->d_B); free_devp(h->d_y); free_devp(h->d_partial);
     free_devp(h->d_bD); free_devp(h->d_bL); free_devp(h->d_gf); free_devp(h->d_fmode); free_devp(h->d_fstatus); free_devp(h->d_tiles); free_devp(h->d_nsup); free_devp(h->d_ctile);
@@ -493,6 +494,9 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
                 CK(cudaEventRecord(h->ev_ib, h->side), "event");
                 CK(cudaStreamWaitEvent(h->stream, h->ev_ib, 0), "wait");
             }
+            // the span ends with the chunk's last step; the row copy and the
+            // mass check after it are per-call work, not per-step work
+            if (h->timing == LBM_TIMING_SPAN) CK(cudaEventRecord(h->ev[4 * (pending - 1) + 3], h->stream), "event");
             if (rows_out)
                 CK(cudaMemcpyAsync(rows_out + (size_t)(done - pending) * h->row_len, h->d_ring,
                                    sizeof(double) * h->row_len * pending, cudaMemcpyDeviceToHost, h->stream),
@@ -501,8 +505,6 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             const bool mass = mass_due();
             int st = mass ? mass_launch(h, h->stream, &dsum) : LBM_OK;
             if (st) return st;
-            // the span ends after the chunk's row copy and mass check
-            if (h->timing == LBM_TIMING_SPAN) CK(cudaEventRecord(h->ev[4 * (pending - 1) + 3], h->stream), "event");
             st = check_status(h);
             if (st) return st;
             if (mass && (st = mass_result(h, dsum))) return st;
@@ -515,6 +517,7 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             CK(cudaEventRecord(h->ev_ib, h->side), "event");
             CK(cudaStreamWaitEvent(h->stream, h->ev_ib, 0), "wait");
         }
+        if (h->timing == LBM_TIMING_SPAN) CK(cudaEventRecord(h->ev[4 * (pending - 1) + 3], h->stream), "event");
         if (rows_out)
             CK(cudaMemcpyAsync(rows_out + (size_t)(done - pending) * h->row_len, h->d_ring,
                                sizeof(double) * h->row_len * pending, cudaMemcpyDeviceToHost, h->stream),
@@ -523,7 +526,6 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
         const bool mass = mass_due();
         int st = mass ? mass_launch(h, h->stream, &dsum) : LBM_OK;
         if (st) return st;
-        if (h->timing == LBM_TIMING_SPAN) CK(cudaEventRecord(h->ev[4 * (pending - 1) + 3], h->stream), "event");
         st = check_status(h);
         if (st) return st;
         if (mass && (st = mass_result(h, dsum))) return st;
@@ -676,6 +678,7 @@ int lbm_create(const lbm_params *p, lbm_t **out)
     lbm_handle *h = new lbm_handle();
     h->p = *p;
     cudaGetDevice(&h->dev);
+    cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->dev);
     h->nx = p->nx;
     h->ny = p->ny;
     h->pitch = (p->nx + 63) / 64 * 64;
@@ -700,6 +703,13 @@ int lbm_create(const lbm_params *p, lbm_t **out)
         if (v == 1 || v == 2 || v == 4) h->kf_vec = v;
     }
     if (const char *ev = getenv("LBM_KF_TMA")) h->kf_tma = atoi(ev) != 0;
+    // SMs the persistent lattice kernel leaves free for the immersed-boundary
+    // kernels; LBM_KF_RESERVE overrides the default for tuning
+    h->kf_reserve = kKfReserve;
+    if (const char *ev = getenv("LBM_KF_RESERVE")) {
+        const int v = atoi(ev);
+        if (v >= 0 && v <= 64) h->kf_reserve = v;
+    }
     if (const char *ev = getenv("LBM_KF_ROWS")) {
         const int v = atoi(ev);
         if (v >= 1 && v <= 4096) h->kf_rows = v;
@@ -756,8 +766,7 @@ int lbm_create(const lbm_params *p, lbm_t **out)
     if ((e = dmalloc(h, &h->d_red, sizeof(double) * 2 * 296)) != cudaSuccess) return fail(e, "alloc red");
     if ((e = dmalloc(h, &h->d_mass, sizeof(double) * mass_slots())) != cudaSuccess) return fail(e, "alloc mass");
     if ((e = dmalloc(h, &h->d_mcount, sizeof(unsigned))) != cudaSuccess) return fail(e, "alloc mass counter");
-    if ((e = dmalloc(h, &h->d_kftab, (size_t)KF_TABLE_ENTRIES * KF_ARGS_STRIDE)) != cudaSuccess)
-        return fail(e, "alloc lattice arguments");
+    if ((e = dmalloc(h, &h->d_queue, 2 * sizeof(unsigned))) != cudaSuccess) return fail(e, "alloc queue");
     if ((e = dmalloc(h, &h->d_solve_res, 2 * sizeof(double))) != cudaSuccess) return fail(e, "alloc res");
     if ((e = dmalloc(h, &h->d_ring, sizeof(double) * h->row_len * (size_t)h->ring_cap)) != cudaSuccess)
         return fail(e, "alloc ring");
@@ -787,7 +796,7 @@ int lbm_destroy(lbm_t *h)
     free_devp(h->d_pinfo); free_devp(h->d_counter);
     free_devp(h->d_ring); free_devp(h->d_status); free_devp(h->d_solve_res); free_devp(h->d_red);
     free_devp(h->d_mass); free_devp(h->d_mcount);
-    free_dev(h->d_kftab);
+    free_devp(h->d_queue);
     free_devp(h->d_stage);
     if (h->side) cudaStreamSynchronize(h->side);
     if (h->fstream) cudaStreamSynchronize(h->fstream);

@@ -44,9 +44,6 @@ struct KFArgs {
 #define KF_ALL 0
 #define KF_OUTER 1
 
-// table of lattice-argument variants of a handle (kf_table_build)
-#define KF_ARGS_STRIDE 512
-#define KF_TABLE_ENTRIES (2 * 3 * LBM_NSLOT_MAX * 2)
 
 // arguments of the immersed-boundary kernels
 struct IBArgs {
@@ -109,8 +106,11 @@ struct lbm_handle {
     int kf_vec = 1;   // nodes per thread of the register-loading lattice kernel (1, 2 or 4)
     int kf_tma = 1;   // bulk-copy staged lattice kernel (the default)
     int kf_rows = 8;  // rows swept by one CTA of the staged kernel
-    void *d_kftab = nullptr;   // lattice-argument variants (KF_TABLE_ENTRIES x KF_ARGS_STRIDE bytes)
-    int kftab_ok = 0, kftab_rows = -1;
+    // the persistent lattice kernel's work queue (next item, CTAs done), the
+    // SMs it leaves to the immersed-boundary kernels, the device's SM count
+    unsigned *d_queue = nullptr;
+    int kf_reserve = 0;
+    int sm_count = 0;
     int dev = 0;
     cudaStream_t stream = nullptr;
     void *fbuf[2] = {nullptr, nullptr};     // first element of plane 0
