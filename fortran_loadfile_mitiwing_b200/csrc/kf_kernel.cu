@@ -417,65 +417,21 @@ __device__ __forceinline__ void kf_tma_cta(const KFArgs<C> &a, int bx, int by, i
             }
         }
     }
-    // every thread is done with the ring: its barriers are invalidated, so
-    // that the next item of a persistent CTA can initialise them again
-    __syncthreads();
-    if (tid == 0)
-        for (int s = 0; s < KS; ++s) {
-            mbar_inval(&full[s]);
-            mbar_inval(&empty[s]);
-        }
 }
 
-// SM identifier of the executing CTA, and the number of identifiers
-static __device__ __forceinline__ unsigned sm_id()
-{
-    unsigned r;
-    asm volatile("mov.u32 %0, %%smid;" : "=r"(r));
-    return r;
-}
-static __device__ __forceinline__ unsigned sm_ids()
-{
-    unsigned r;
-    asm volatile("mov.u32 %0, %%nsmid;" : "=r"(r));
-    return r;
-}
-
-// The single-case lattice update as a persistent kernel: about one wave of
-// CTAs (kf_minb per SM) that take the work items (strip, row chunk) from a
-// queue in global memory, the edge row's items first, until none is left.
-// CTAs that land on the last `reserve` SM identifiers take no item, so that
-// those SMs stay free for the immersed-boundary kernels running beside the
-// update on the side stream (the solve and the factorization need a whole
-// SM each). The last CTA to finish resets the queue for the next launch on
-// the same stream. No CTA waits for another one.
+// One CTA per (strip, row chunk) of the lattice; the edge row's CTAs
+// (chunk gy - 1, whose nodes take longer) are numbered first so that they
+// start in the first wave rather than in the tail.
 // The arguments are __grid_constant__ kernel parameters, read in place from
 // the parameter bank: no global loads of them in the row loop (measured as
 // 6.6 loads per node when they were read from a table in global memory,
 // which every store may alias) and no registers held for them.
 template <typename T, typename C, bool FIELDS, bool CONS0>
-__global__ void __launch_bounds__(TW, kf_minb<T>())
-    kf_tma(const __grid_constant__ KFArgs<C> a, int gx, int gy, unsigned *queue, int reserve)
+__global__ void __launch_bounds__(TW, kf_minb<T>()) kf_tma(const __grid_constant__ KFArgs<C> a)
 {
     extern __shared__ __align__(128) unsigned char smraw[];
-    __shared__ int item;
-    const int nitems = gx * gy;
-    if (sm_id() + (unsigned)reserve < sm_ids()) {
-        for (;;) {
-            if (threadIdx.x == 0) item = (int)atomicAdd(queue, 1u);
-            __syncthreads();
-            const int it = item;
-            if (it >= nitems) break;
-            // the edge row (chunk gy - 1) first: its nodes take longer
-            const int by = it < gx ? gy - 1 : (it - gx) / gx, bx = it % gx;
-            kf_tma_cta<T, C, FIELDS, CONS0>(a, bx, by, gx, gy, smraw);
-            __syncthreads();   // the ring and `item` are reused by the next item
-        }
-    }
-    if (threadIdx.x == 0 && atomicAdd(queue + 1, 1u) == gridDim.x - 1) {
-        queue[0] = 0u;   // every CTA has left the loop
-        queue[1] = 0u;
-    }
+    const int gy = gridDim.y, by = blockIdx.y == 0 ? gy - 1 : blockIdx.y - 1;
+    kf_tma_cta<T, C, FIELDS, CONS0>(a, blockIdx.x, by, gridDim.x, gy, smraw);
 }
 
 // Several lattices (a batch of cases) in one launch: CTA b runs entry b of
@@ -492,27 +448,24 @@ __global__ void __launch_bounds__(TW, kf_minb<T>()) kf_tma_multi(const KFArgs<C>
 template <typename C> bool cons0(const KFArgs<C> &a) { return a.s[0] == C(0) && a.s[3] == C(0) && a.s[5] == C(0); }
 
 template <typename T, typename C, bool FIELDS>
-void launch_tma_f(const KFArgs<C> &a, int ctas, int gx, int gy, unsigned *queue, int reserve, cudaStream_t st)
+void launch_tma_f(const KFArgs<C> &a, dim3 grid, cudaStream_t st)
 {
     const size_t smem = tma_smem<T>();
     if (cons0(a))
-        kf_tma<T, C, FIELDS, true><<<ctas, TW, smem, st>>>(a, gx, gy, queue, reserve);
+        kf_tma<T, C, FIELDS, true><<<grid, TW, smem, st>>>(a);
     else
-        kf_tma<T, C, FIELDS, false><<<ctas, TW, smem, st>>>(a, gx, gy, queue, reserve);
+        kf_tma<T, C, FIELDS, false><<<grid, TW, smem, st>>>(a);
 }
 
-// one wave of persistent CTAs over the (strip, row chunk) items of the lattice
+// one CTA per (strip, row chunk) of the lattice, and the edge CTA row
 template <typename T, typename C>
 void launch_tma(const lbm_handle *h, const KFArgs<C> &a, bool fields, cudaStream_t st)
 {
-    const int gx = (h->nx + tma_strip<T>() - 1) / tma_strip<T>();
-    const int gy = (h->ny - 2 + a.rows_per_cta - 1) / a.rows_per_cta + 1;
-    const int ctas = std::min(gx * gy, std::max(1, h->sm_count) * kf_minb<T>());
-    const int reserve = std::min(h->kf_reserve, std::max(0, h->sm_count - 1));
+    const dim3 grid((h->nx + tma_strip<T>() - 1) / tma_strip<T>(), (h->ny - 2 + a.rows_per_cta - 1) / a.rows_per_cta + 1);
     if (fields)
-        launch_tma_f<T, C, true>(a, ctas, gx, gy, h->d_queue, reserve, st);
+        launch_tma_f<T, C, true>(a, grid, st);
     else
-        launch_tma_f<T, C, false>(a, ctas, gx, gy, h->d_queue, reserve, st);
+        launch_tma_f<T, C, false>(a, grid, st);
 }
 
 template <typename T, typename C, bool FIELDS, bool CONS0>

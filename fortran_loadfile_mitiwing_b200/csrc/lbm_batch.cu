@@ -37,6 +37,10 @@ struct lbm_batch {
     int prec = -1, fbatch = 4, nslots = 8, dev = 0;
     cudaStream_t main = nullptr, side = nullptr, fstream = nullptr;
     cudaEvent_t ev_ib = nullptr, ev_done = nullptr, ev_fready = nullptr, ev_side = nullptr;
+    // device time of the last run's steps (lbm_batch_get_timing)
+    cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;
+    double last_ms = 0.0;
+    int last_steps = 0;
     // argument arrays: flow chain and lattice per step (a ring of kArgRing,
     // so a step's upload never overwrites arguments a queued launch still
     // reads), the case table (two buffers, uploaded again only when the set
@@ -118,7 +122,7 @@ void free_batch(lbm_batch *b)
         if (b->ev_fup[r]) cudaEventDestroy(b->ev_fup[r]);
     for (int r = 0; r < kGroupRing; ++r)
         if (b->ev_group[r]) cudaEventDestroy(b->ev_group[r]);
-    for (cudaEvent_t e : {b->ev_ib, b->ev_done, b->ev_fready, b->ev_side})
+    for (cudaEvent_t e : {b->ev_ib, b->ev_done, b->ev_fready, b->ev_side, b->ev_t0, b->ev_t1})
         if (e) cudaEventDestroy(e);
     if (b->main) cudaStreamDestroy(b->main);
     if (b->side) cudaStreamDestroy(b->side);
@@ -233,6 +237,8 @@ int lbm_batch_create(lbm_t *const *cases, int count, lbm_batch_t **out)
     if ((e = cudaStreamCreateWithPriority(&b->side, cudaStreamNonBlocking, prio_high)) != cudaSuccess)
         return fail(e, "stream");
     if ((e = cudaStreamCreateWithFlags(&b->fstream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
+    for (cudaEvent_t *ev : {&b->ev_t0, &b->ev_t1})
+        if ((e = cudaEventCreate(ev)) != cudaSuccess) return fail(e, "event");
     for (cudaEvent_t *ev : {&b->ev_ib, &b->ev_done, &b->ev_fready, &b->ev_side, &b->ev_tup[0], &b->ev_tup[1],
                             &b->ev_tuse[0], &b->ev_tuse[1]})
         if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
@@ -286,6 +292,14 @@ int lbm_batch_destroy(lbm_batch_t *b)
     if (!b) return LBM_ERR_ARG;
     free_batch(b);
     delete b;
+    return LBM_OK;
+}
+
+int lbm_batch_get_timing(const lbm_batch_t *b, double *ms, int *steps)
+{
+    if (!b) return LBM_ERR_ARG;
+    if (ms) *ms = b->last_ms;
+    if (steps) *steps = b->last_steps;
     return LBM_OK;
 }
 
@@ -408,6 +422,9 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
     };
     BCK(cudaEventRecord(b->ev_done, b->main), "event");
     BCK(cudaEventRecord(b->ev_side, b->side), "event");
+    BCK(cudaEventRecord(b->ev_t0, b->main), "event");
+    b->last_ms = 0.0;
+    b->last_steps = 0;
     std::vector<lbm_handle *> act;
     std::vector<int> act_idx;
     std::vector<long long> waited;
@@ -537,6 +554,12 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
             if ((rc = flush())) break;
         }
     }
+    // device time of the steps: from before the first step's launches to the
+    // end of the last step's side-stream work
+    if (step > 0 && rc == LBM_OK) {
+        BCK(cudaStreamWaitEvent(b->main, b->ev_side, 0), "wait");
+        BCK(cudaEventRecord(b->ev_t1, b->main), "event");
+    }
     // the rows of the last steps (also when every case ended before nsteps)
     if (pending > 0 && rc == LBM_OK) rc = flush();
     // the global mass of every case that ran, at the end of the run (FP64 on
@@ -563,6 +586,13 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
     }
     // leave every stream idle: the cases' own calls follow on their streams
     sync_streams(b);
+    if (step > 0 && rc == LBM_OK) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, b->ev_t0, b->ev_t1) == cudaSuccess) {
+            b->last_ms = ms;
+            b->last_steps = step;
+        }
+    }
     restore();
     if (done_steps)
         for (int c = 0; c < nc; ++c) done_steps[c] = done[c];

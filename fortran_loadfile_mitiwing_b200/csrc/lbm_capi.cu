@@ -20,8 +20,7 @@ const double kWref[9] = {4.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0,
 const int kEx[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
 const int kEy[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
 const int kRing = 2048;   // force rows kept on the device between host copies
-// SMs the single-case lattice kernel leaves to the immersed-boundary kernels
-const int kKfReserve = 2;
+
 
 int set_err(lbm_handle *h, int code, const char *msg)
 {
@@ -678,7 +677,6 @@ int lbm_create(const lbm_params *p, lbm_t **out)
     lbm_handle *h = new lbm_handle();
     h->p = *p;
     cudaGetDevice(&h->dev);
-    cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, h->dev);
     h->nx = p->nx;
     h->ny = p->ny;
     h->pitch = (p->nx + 63) / 64 * 64;
@@ -703,13 +701,7 @@ int lbm_create(const lbm_params *p, lbm_t **out)
         if (v == 1 || v == 2 || v == 4) h->kf_vec = v;
     }
     if (const char *ev = getenv("LBM_KF_TMA")) h->kf_tma = atoi(ev) != 0;
-    // SMs the persistent lattice kernel leaves free for the immersed-boundary
-    // kernels; LBM_KF_RESERVE overrides the default for tuning
-    h->kf_reserve = kKfReserve;
-    if (const char *ev = getenv("LBM_KF_RESERVE")) {
-        const int v = atoi(ev);
-        if (v >= 0 && v <= 64) h->kf_reserve = v;
-    }
+
     if (const char *ev = getenv("LBM_KF_ROWS")) {
         const int v = atoi(ev);
         if (v >= 1 && v <= 4096) h->kf_rows = v;
@@ -766,7 +758,7 @@ int lbm_create(const lbm_params *p, lbm_t **out)
     if ((e = dmalloc(h, &h->d_red, sizeof(double) * 2 * 296)) != cudaSuccess) return fail(e, "alloc red");
     if ((e = dmalloc(h, &h->d_mass, sizeof(double) * mass_slots())) != cudaSuccess) return fail(e, "alloc mass");
     if ((e = dmalloc(h, &h->d_mcount, sizeof(unsigned))) != cudaSuccess) return fail(e, "alloc mass counter");
-    if ((e = dmalloc(h, &h->d_queue, 2 * sizeof(unsigned))) != cudaSuccess) return fail(e, "alloc queue");
+
     if ((e = dmalloc(h, &h->d_solve_res, 2 * sizeof(double))) != cudaSuccess) return fail(e, "alloc res");
     if ((e = dmalloc(h, &h->d_ring, sizeof(double) * h->row_len * (size_t)h->ring_cap)) != cudaSuccess)
         return fail(e, "alloc ring");
@@ -796,7 +788,7 @@ int lbm_destroy(lbm_t *h)
     free_devp(h->d_pinfo); free_devp(h->d_counter);
     free_devp(h->d_ring); free_devp(h->d_status); free_devp(h->d_solve_res); free_devp(h->d_red);
     free_devp(h->d_mass); free_devp(h->d_mcount);
-    free_devp(h->d_queue);
+
     free_devp(h->d_stage);
     if (h->side) cudaStreamSynchronize(h->side);
     if (h->fstream) cudaStreamSynchronize(h->fstream);

@@ -235,13 +235,6 @@ static __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
 
 static __device__ __forceinline__ void mbar_init_fence() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 
-// a barrier no thread uses any more, before its shared memory is initialised
-// again (a CTA of a persistent kernel reuses its ring for the next item)
-static __device__ __forceinline__ void mbar_inval(uint64_t *bar)
-{
-    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
 static __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");

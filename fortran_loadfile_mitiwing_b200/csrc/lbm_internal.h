@@ -106,11 +106,6 @@ struct lbm_handle {
     int kf_vec = 1;   // nodes per thread of the register-loading lattice kernel (1, 2 or 4)
     int kf_tma = 1;   // bulk-copy staged lattice kernel (the default)
     int kf_rows = 8;  // rows swept by one CTA of the staged kernel
-    // the persistent lattice kernel's work queue (next item, CTAs done), the
-    // SMs it leaves to the immersed-boundary kernels, the device's SM count
-    unsigned *d_queue = nullptr;
-    int kf_reserve = 0;
-    int sm_count = 0;
     int dev = 0;
     cudaStream_t stream = nullptr;
     void *fbuf[2] = {nullptr, nullptr};     // first element of plane 0

@@ -94,7 +94,6 @@ def estimate_device_bytes(case):
     total += cs * (6 * ny + 36)                                # edge values
     total += 4 + 4 + _NSLOT_MAX * _PATCHINFO_BYTES + 8 * 2 * 296 + 16 + 8 * row_len * _RING
     total += 8 * (_MASS_BLOCKS + 1) + 4                        # mass check: partials and sum, counter
-    total += 2 * 4                                             # lattice kernel's work queue
     if nwing:
         dt = p.scale * p.uu
         msteps = int((case.table[-1, 0] + 1e-12) / dt) + 1

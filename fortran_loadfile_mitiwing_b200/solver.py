@@ -270,17 +270,31 @@ class Batch:
             raise LbmError(rc, self.lib.lbm_batch_last_error(self.b).decode())   # not a case's own failure
         return out, status
 
-    def autotune(self, steps_per_trial=20, candidates=(4, 8, 16)):
+    def device_time(self):
+        """(device milliseconds, steps) of the last run (lbm_batch_get_timing)."""
+        ms, n = C.c_double(), C.c_int()
+        rc = self.lib.lbm_batch_get_timing(self.b, C.byref(ms), C.byref(n))
+        if rc != 0:
+            raise LbmError(rc, self.lib.lbm_batch_last_error(self.b).decode())
+        return ms.value, n.value
+
+    def autotune(self, steps_per_trial=20, candidates=(4, 8, 16), rounds=2):
         """Picks the lattice kernel's rows per CTA for this batch by timing
-        `steps_per_trial` real steps with each candidate (the steps advance
-        the cases; the results do not depend on the choice). Returns
-        {rows: seconds per step} and keeps the fastest."""
-        import time
+        `steps_per_trial` real steps with each candidate on the device (CUDA
+        events around the steps of each trial, `rounds` trials per candidate
+        in alternating order, the best kept); the steps advance the cases and
+        the results do not depend on the choice. Returns {rows: seconds per
+        step} and keeps the fastest."""
         timing = {}
-        for r in candidates:
-            self.set_rows(r)
-            t0 = time.perf_counter()
-            self.run(steps_per_trial, keep_rows=False)
-            timing[r] = (time.perf_counter() - t0) / steps_per_trial
-        self.set_rows(min(timing, key=timing.get))
+        order = list(candidates)
+        for k in range(rounds):
+            for r in (order if k % 2 == 0 else order[::-1]):
+                self.set_rows(r)
+                self.run(steps_per_trial, keep_rows=False)
+                ms, n = self.device_time()
+                if n > 0:
+                    t = ms / 1e3 / n
+                    timing[r] = min(timing.get(r, t), t)
+        if timing:
+            self.set_rows(min(timing, key=timing.get))
         return timing

@@ -383,7 +383,11 @@ LBM_API int lbm_read_flow_field_file(const char *path, int nx, int ny, int wing_
  *     nullable pointers) receives case c's rows as lbm_run would. Fields are
  *     kept for the last two steps of the call and of each case that ends.
  *   lbm_batch_set_rows: rows per CTA of the lattice kernel for the batch
- *     (0: the cases' own); the batch autotuner of the Python layer sets it. */
+ *     (0: the cases' own); the batch autotuner of the Python layer sets it.
+ *   lbm_batch_get_timing: device milliseconds of the last lbm_batch_run's
+ *     steps (CUDA events on the batch's streams, from before the first
+ *     step's launches to the end of the last step) and the number of steps
+ *     it ran; 0 after a run that failed. */
 typedef struct lbm_batch lbm_batch_t;
 LBM_API int lbm_batch_create(lbm_t *const *cases, int count, lbm_batch_t **out);
 LBM_API int lbm_batch_destroy(lbm_batch_t *b);
@@ -392,6 +396,7 @@ LBM_API int lbm_batch_remove(lbm_batch_t *b, lbm_t *h);
 LBM_API int lbm_batch_count(const lbm_batch_t *b);
 LBM_API int lbm_batch_case_status(const lbm_batch_t *b, int c);
 LBM_API int lbm_batch_set_rows(lbm_batch_t *b, int rows_per_cta);
+LBM_API int lbm_batch_get_timing(const lbm_batch_t *b, double *ms, int *steps);
 LBM_API int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *done_steps);
 LBM_API const char *lbm_batch_last_error(const lbm_batch_t *b);
 
