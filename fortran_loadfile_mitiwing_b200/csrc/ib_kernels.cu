@@ -1549,13 +1549,14 @@ IBArgs make_args(lbm_handle *h, const void *fin, int slot)
 
 template <typename T, typename C>
 int launch_flow_t(lbm_handle *h, const void *fin, void *fout, void *fields, int step_index, int ring_slot, int slot,
-                  cudaStream_t st)
+                  cudaStream_t st, cudaEvent_t after_interp)
 {
     IBArgs a = make_args(h, fin, slot);
     if (h->nseg > 0) {
         ib_interp<T, false><<<(h->nseg + 7) / 8, 256, 0, st>>>(a, nullptr);
         h->launches += 1;
     }
+    if (after_interp && cudaEventRecord(after_interp, st) != cudaSuccess) return -1;
     ib_solve<false><<<1, SOLVE_THREADS, solve_smem(h->nseg), st>>>(a, nullptr, step_index, ring_slot);
     const int grid = std::min(h->patch_gx() * h->patch_gy(), 2 * 148);   // strided over the correction tiles
     const KFArgs<C> kf = make_kf_args<C>(h, fin, fout, fields, KF_OUTER);
@@ -1648,15 +1649,18 @@ int launch_check(lbm_handle *h, int slot, int ring_slot, bool residual, cudaStre
 // flow chain of step `step_index`: interpolation, solve with the factor of
 // `slot`, spread and forces
 int launch_flow(lbm_handle *h, const void *fin, void *fout, void *fields, int step_index, int ring_slot, int slot,
-                cudaStream_t st)
+                cudaStream_t st, cudaEvent_t after_interp)
 {
     if (!st) st = h->stream;
     switch (h->prec) {
-    case LBM_PREC_FP32: return launch_flow_t<float, float>(h, fin, fout, fields, step_index, ring_slot, slot, st);
-    case LBM_PREC_FP64: return launch_flow_t<double, double>(h, fin, fout, fields, step_index, ring_slot, slot, st);
-    case LBM_PREC_FP16: return launch_flow_t<__half, float>(h, fin, fout, fields, step_index, ring_slot, slot, st);
+    case LBM_PREC_FP32:
+        return launch_flow_t<float, float>(h, fin, fout, fields, step_index, ring_slot, slot, st, after_interp);
+    case LBM_PREC_FP64:
+        return launch_flow_t<double, double>(h, fin, fout, fields, step_index, ring_slot, slot, st, after_interp);
+    case LBM_PREC_FP16:
+        return launch_flow_t<__half, float>(h, fin, fout, fields, step_index, ring_slot, slot, st, after_interp);
     case LBM_PREC_BF16:
-        return launch_flow_t<__nv_bfloat16, float>(h, fin, fout, fields, step_index, ring_slot, slot, st);
+        return launch_flow_t<__nv_bfloat16, float>(h, fin, fout, fields, step_index, ring_slot, slot, st, after_interp);
     }
     return -1;
 }
@@ -1688,10 +1692,11 @@ int max_seg(lbm_handle *const *hs, int n)
 
 template <typename T, typename C>
 int launch_flow_batch_t(lbm_handle *const *hs, int ncase, const IBArgs *dargs, const void *dkf, int step_index,
-                        int ring_slot, bool fields, cudaStream_t st)
+                        int ring_slot, bool fields, cudaStream_t st, cudaEvent_t after_interp)
 {
     const int ns = max_seg(hs, ncase);
     ib_interp<T, true><<<dim3((ns + 7) / 8, 1, ncase), 256, 0, st>>>(IBArgs{}, dargs);
+    if (after_interp && cudaEventRecord(after_interp, st) != cudaSuccess) return -1;
     ib_solve<true><<<dim3(1, 1, ncase), SOLVE_THREADS, solve_smem(ns), st>>>(IBArgs{}, dargs, step_index, ring_slot);
     int tiles = 1;
     for (int c = 0; c < ncase; ++c) tiles = std::max(tiles, hs[c]->patch_gx() * hs[c]->patch_gy());
@@ -1734,16 +1739,20 @@ int launch_factor_batch(lbm_handle *const *hs, int ncase, const void *dargs, int
 // flow chains of one step of every case (dargs: the cases' arguments of the
 // step's slot; dkf: their lattice arguments)
 int launch_flow_batch(lbm_handle *const *hs, int ncase, const void *dargs, const void *dkf, int step_index,
-                      int ring_slot, bool fields, cudaStream_t st)
+                      int ring_slot, bool fields, cudaStream_t st, cudaEvent_t after_interp)
 {
     if (ncase <= 0) return 0;
     const IBArgs *d = (const IBArgs *)dargs;
     switch (hs[0]->prec) {
-    case LBM_PREC_FP32: return launch_flow_batch_t<float, float>(hs, ncase, d, dkf, step_index, ring_slot, fields, st);
-    case LBM_PREC_FP64: return launch_flow_batch_t<double, double>(hs, ncase, d, dkf, step_index, ring_slot, fields, st);
-    case LBM_PREC_FP16: return launch_flow_batch_t<__half, float>(hs, ncase, d, dkf, step_index, ring_slot, fields, st);
+    case LBM_PREC_FP32:
+        return launch_flow_batch_t<float, float>(hs, ncase, d, dkf, step_index, ring_slot, fields, st, after_interp);
+    case LBM_PREC_FP64:
+        return launch_flow_batch_t<double, double>(hs, ncase, d, dkf, step_index, ring_slot, fields, st, after_interp);
+    case LBM_PREC_FP16:
+        return launch_flow_batch_t<__half, float>(hs, ncase, d, dkf, step_index, ring_slot, fields, st, after_interp);
     case LBM_PREC_BF16:
-        return launch_flow_batch_t<__nv_bfloat16, float>(hs, ncase, d, dkf, step_index, ring_slot, fields, st);
+        return launch_flow_batch_t<__nv_bfloat16, float>(hs, ncase, d, dkf, step_index, ring_slot, fields, st,
+                                                         after_interp);
     }
     return -1;
 }

@@ -16,6 +16,7 @@
 // a case's results in a batch are bit-for-bit those of running it alone.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <string>
 #include <vector>
 
@@ -39,6 +40,10 @@ struct lbm_batch {
     cudaEvent_t ev_ib = nullptr, ev_done = nullptr, ev_fready = nullptr, ev_side = nullptr;
     // device time of the last run's steps (lbm_batch_get_timing)
     cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;
+    // the step's interpolations are done; with after_interp the lattice
+    // launch waits for it (the solve CTAs then find whole SMs free)
+    cudaEvent_t ev_interp = nullptr;
+    int after_interp = 1;
     double last_ms = 0.0;
     int last_steps = 0;
     // argument arrays: flow chain and lattice per step (a ring of kArgRing,
@@ -122,7 +127,7 @@ void free_batch(lbm_batch *b)
         if (b->ev_fup[r]) cudaEventDestroy(b->ev_fup[r]);
     for (int r = 0; r < kGroupRing; ++r)
         if (b->ev_group[r]) cudaEventDestroy(b->ev_group[r]);
-    for (cudaEvent_t e : {b->ev_ib, b->ev_done, b->ev_fready, b->ev_side, b->ev_t0, b->ev_t1})
+    for (cudaEvent_t e : {b->ev_ib, b->ev_done, b->ev_fready, b->ev_side, b->ev_t0, b->ev_t1, b->ev_interp})
         if (e) cudaEventDestroy(e);
     if (b->main) cudaStreamDestroy(b->main);
     if (b->side) cudaStreamDestroy(b->side);
@@ -239,7 +244,8 @@ int lbm_batch_create(lbm_t *const *cases, int count, lbm_batch_t **out)
     if ((e = cudaStreamCreateWithFlags(&b->fstream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
     for (cudaEvent_t *ev : {&b->ev_t0, &b->ev_t1})
         if ((e = cudaEventCreate(ev)) != cudaSuccess) return fail(e, "event");
-    for (cudaEvent_t *ev : {&b->ev_ib, &b->ev_done, &b->ev_fready, &b->ev_side, &b->ev_tup[0], &b->ev_tup[1],
+    if (const char *ev = getenv("LBM_AFTER_INTERP")) b->after_interp = atoi(ev) != 0;
+    for (cudaEvent_t *ev : {&b->ev_interp, &b->ev_ib, &b->ev_done, &b->ev_fready, &b->ev_side, &b->ev_tup[0], &b->ev_tup[1],
                             &b->ev_tuse[0], &b->ev_tuse[1]})
         if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
     for (int q = 0; q < kArgRing; ++q)
@@ -517,8 +523,9 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
             }
         }
         BCK(cudaEventRecord(b->ev_fready, b->side), "event");   // uploads done, factorizations ready
+        cudaEvent_t ei = b->after_interp ? b->ev_interp : nullptr;
         if (launch_flow_batch(act.data(), (int)act.size(), b->d_sargs[buf], b->d_kargs[buf], 0, pending, fields,
-                              b->side)) {
+                              b->side, ei)) {
             rc = berr(b, LBM_ERR_CUDA, "batch: launch flow");
             break;
         }
@@ -532,6 +539,7 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
         if ((rc = factor_needed(act, act_idx, true))) break;
         // main stream: every case's lattice nodes but its correction tiles
         BCK(cudaStreamWaitEvent(b->main, b->ev_fready, 0), "wait");
+        if (ei) BCK(cudaStreamWaitEvent(b->main, ei, 0), "wait");   // the solves start first
         if (launch_kf_multi(b->prec, b->d_kargs[buf], b->d_table[tcur], ntab, fields, cons0, b->main)) {
             rc = berr(b, LBM_ERR_CUDA, "batch: launch lattice");
             break;

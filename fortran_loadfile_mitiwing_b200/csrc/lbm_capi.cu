@@ -454,7 +454,8 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             CK(cudaStreamWaitEvent(h->side, h->ev_inner, 0), "wait");
             CK(cudaStreamWaitEvent(h->side, h->ev_batch[half], 0), "wait");
             if (e) CK(cudaEventRecord(h->ev_side[2 * slot], h->side), "event");
-            if (launch_flow(h, fin, fout, fields, h->n, slot, q, h->side)) return cuda_err(h, cudaGetLastError(), "launch ib");
+            cudaEvent_t ei = h->after_interp ? h->ev_interp : nullptr;
+            if (launch_flow(h, fin, fout, fields, h->n, slot, q, h->side, ei)) return cuda_err(h, cudaGetLastError(), "launch ib");
             if (e) CK(cudaEventRecord(h->ev_side[2 * slot + 1], h->side), "event");
             CK(cudaEventRecord(h->ev_ib, h->side), "event");
             if (launch_check(h, q, slot, check_res, h->side)) return cuda_err(h, cudaGetLastError(), "launch check");
@@ -462,6 +463,7 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             // the next batch's factorization, overlapping this batch's steps
             if ((b + 1) * K <= last_step && h->batch_in_half[half ^ 1] != b + 1 && (rc = factor_batch(b + 1))) return rc;
             CK(cudaStreamWaitEvent(h->stream, h->ev_batch[half], 0), "wait");   // the step's correction tiles
+            if (ei) CK(cudaStreamWaitEvent(h->stream, ei, 0), "wait");   // the solve starts first
             if (e) CK(cudaEventRecord(e[0], h->stream), "event");
             if (launch_kf(h, fin, fout, fields, KF_OUTER)) return cuda_err(h, cudaGetLastError(), "launch kf");
             if (e) CK(cudaEventRecord(e[1], h->stream), "event");
@@ -728,6 +730,8 @@ int lbm_create(const lbm_params *p, lbm_t **out)
         return fail(e, "side stream");
     if ((e = cudaEventCreateWithFlags(&h->ev_ib, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
     if ((e = cudaEventCreateWithFlags(&h->ev_inner, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+    if ((e = cudaEventCreateWithFlags(&h->ev_interp, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+    if (const char *ev = getenv("LBM_AFTER_INTERP")) h->after_interp = atoi(ev) != 0;
     if ((e = cudaStreamCreateWithFlags(&h->fstream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "factor stream");
     for (int q = 0; q < 2; ++q) {
         if ((e = cudaEventCreateWithFlags(&h->ev_batch[q], cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
@@ -796,6 +800,7 @@ int lbm_destroy(lbm_t *h)
     for (auto &e : h->ev_side) cudaEventDestroy(e);
     if (h->ev_ib) cudaEventDestroy(h->ev_ib);
     if (h->ev_inner) cudaEventDestroy(h->ev_inner);
+    if (h->ev_interp) cudaEventDestroy(h->ev_interp);
     for (int q = 0; q < 2; ++q) {
         if (h->ev_batch[q]) cudaEventDestroy(h->ev_batch[q]);
         if (h->ev_free[q]) cudaEventDestroy(h->ev_free[q]);

@@ -164,6 +164,11 @@ struct lbm_handle {
     int env_x0 = 0, env_y0 = 0, env_w = 0, env_h = 0;
     cudaStream_t side = nullptr;
     cudaEvent_t ev_ib = nullptr, ev_inner = nullptr;
+    // the step's interpolation is done (side stream); with after_interp the
+    // lattice kernel waits for it, so that the one-CTA solve that follows
+    // finds a whole SM free instead of waiting for lattice CTAs to drain out
+    cudaEvent_t ev_interp = nullptr;
+    int after_interp = 1;
     // factorization batches (with the split): their own stream; ev_batch[h]
     // marks the batch of slot half h factorized, ev_free[h] the last use of
     // that half by a step's flow chain
@@ -212,8 +217,9 @@ int ib_partials_per_block();
 void ib_factor_scratch(int nseg, size_t *work_blocks, size_t *factor_slot);
 int launch_kf(lbm_handle *h, const void *fin, void *fout, void *fields, int mode = KF_ALL, cudaStream_t st = nullptr);
 int launch_factor(lbm_handle *h, int step0, int count, cudaStream_t st);
+// after_interp (nullable): recorded on st once the interpolation is done
 int launch_flow(lbm_handle *h, const void *fin, void *fout, void *fields, int step_index, int ring_slot, int slot,
-                cudaStream_t st);
+                cudaStream_t st, cudaEvent_t after_interp = nullptr);
 int launch_check(lbm_handle *h, int slot, int ring_slot, bool residual, cudaStream_t st);
 // batches of cases stepped together (lbm_batch.cu)
 int handle_prepare_ib(lbm_handle *h);                    // immersed-boundary buffers (once per geometry)
@@ -240,7 +246,7 @@ void ib_args_write(lbm_handle *h, const void *fin, int slot, void *dst);
 void ib_factor_args_write(lbm_handle *h, int step0, int count, void *dst);
 int launch_factor_batch(lbm_handle *const *hs, int ncase, const void *dargs, int step0, int count, cudaStream_t st);
 int launch_flow_batch(lbm_handle *const *hs, int ncase, const void *dargs, const void *dkf, int step_index,
-                      int ring_slot, bool fields, cudaStream_t st);
+                      int ring_slot, bool fields, cudaStream_t st, cudaEvent_t after_interp = nullptr);
 int launch_check_batch(lbm_handle *const *hs, int ncase, const void *dargs, int ring_slot, cudaStream_t st);
 int ib_tile_ints();   // ints per patch tile of the tile lists
 int launch_residual(lbm_handle *h, const void *fa, const void *fb, double *out2);
