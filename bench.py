@@ -306,6 +306,7 @@ def run_ours(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_e2e:
         line["e2e"] = run_e2e(args, lib)
     if rank == 0 and world == 1 and not args.no_batch:
+        line["storage_variants"] = run_storage_variants(args, lib, exclude=args.precision)
         line["batched"] = run_batched(lib)
         line["served"] = run_served(lib)
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -358,6 +359,40 @@ def run_e2e(args, lib):
             "stages_ms": stages,
             "note": "wall clock around the C-ABI calls (create, boundary, motion table, init, run, fields); "
                     "set-up upload and final fields amortised over the steps"}
+
+
+def run_storage_variants(args, lib, exclude, steps=1000, kernel_steps=300):
+    """The same case in the other storage precisions: step time over `steps`
+    steps (events at the ends of the call only) and the lattice kernel's time
+    with per-step events over `kernel_steps` more, each after 5 warm-up
+    steps; bytes per update 18 x the storage size."""
+    import ctypes as C
+    from fortran_loadfile_mitiwing_b200 import Lbm
+    from fortran_loadfile_mitiwing_b200 import _abi
+    out = {}
+    nn = args.nx * args.ny
+    peak, peak_kind = measured_peak()
+    for prec, elem in (("fp32", 4), ("fp16", 2), ("bf16", 2), ("fp64", 8)):
+        if prec == exclude:
+            continue
+        s = Lbm.from_case(large_case(args, n_steps=steps + kernel_steps + 16, precision=prec), lib)
+        s.run(5, keep_rows=False)
+        lib.lbm_set_timing(s.h, _abi.LBM_TIMING_SPAN)
+        s.run(steps, keep_rows=False)
+        step_ms, n = C.c_double(), C.c_int()
+        lib.lbm_get_timing(s.h, C.byref(step_ms), None, None, C.byref(n))
+        lib.lbm_set_timing(s.h, _abi.LBM_TIMING_KERNELS)
+        s.run(kernel_steps, keep_rows=False)
+        kf_ms, n2 = C.c_double(), C.c_int()
+        lib.lbm_get_timing(s.h, None, None, C.byref(kf_ms), C.byref(n2))
+        s.close()
+        ms = step_ms.value / n.value
+        kms = kf_ms.value / n2.value
+        achieved = 18 * elem * nn / (kms / 1e3) / 1e9
+        out[prec] = {"ms_per_step": ms, "mlups": nn / (ms / 1e3) / 1e6, "kernel_ms": kms,
+                     "kernel_gbs": achieved, "kernel_frac": achieved / peak, "peak_source": peak_kind,
+                     "steps": n.value}
+    return out
 
 
 def run_batched(lib, n_cases=64, steps=100, warmup=12):
