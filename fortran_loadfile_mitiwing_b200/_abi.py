@@ -114,6 +114,9 @@ ABI = {
     "lbm_batch_count": (C.c_int, [_P]),
     "lbm_batch_case_status": (C.c_int, [_P, C.c_int]),
     "lbm_batch_set_rows": (C.c_int, [_P, C.c_int]),
+    "lbm_batch_set_graphs": (C.c_int, [_P, C.c_int]),
+    "lbm_batch_graph_stats": (C.c_int, [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                                        C.POINTER(C.c_longlong)]),
     "lbm_batch_get_timing": (C.c_int, [_P, _D, C.POINTER(C.c_int)]),
     "lbm_batch_run": (C.c_int, [_P, C.c_int, C.POINTER(_D), C.POINTER(C.c_int)]),
     "lbm_batch_last_error": (C.c_char_p, [_P]),

@@ -877,7 +877,13 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 1024 / SOLVE_THREADS) ib_solve(
     if (tid == 0) {
         double time;
         const double *row = motion_row(a, BATCH ? a.cur_step : step_index, &time);
-        write_header(a, row, time, ring_slot);
+        // batched launches take the row from the case's arguments (a CUDA
+        // graph replays one launch for many steps)
+        const int rr = BATCH ? a.ring_row : ring_slot;
+        if (rr >= 0 && rr < a.ring_rows)
+            write_header(a, row, time, rr);
+        else
+            atomicOr(a.status, LBM_ST_INDEX_SOLVE);
         const unsigned fs = *a.fstatus;
         if (fs) { atomicOr(a.status, fs); *a.fstatus = 0u; }
         a.solve_res[1] = (double)a.fmode[1];
@@ -1195,7 +1201,12 @@ __global__ void __launch_bounds__(256) ib_forces(const IBArgs a0, const IBArgs *
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double *fr = a.force_ring + (long long)ring_slot * a.row_len;
+        const int rr = BATCH ? a.ring_row : ring_slot;
+        if (rr < 0 || rr >= a.ring_rows) {
+            atomicOr(a.status, LBM_ST_INDEX_FORCES);
+            return;
+        }
+        double *fr = a.force_ring + (long long)rr * a.row_len;
         double tot[3] = {0, 0, 0};
         const double uu = a.uu, scale = a.scale;
         for (int w = 0; w < a.nwing; ++w) {
@@ -1540,6 +1551,7 @@ IBArgs make_args(lbm_handle *h, const void *fin, int slot)
     a.patch_wmax = h->patch_wmax; a.patch_hmax = h->patch_hmax;
     a.partial = h->d_partial; a.counter = h->d_counter;
     a.force_ring = h->d_ring; a.row_len = h->row_len;
+    a.ring_row = 0; a.ring_rows = h->ring_cap;
     a.status = h->d_status; a.solve_res = h->d_solve_res;
     a.cur_step = h->n;
     a.fstep0 = 0; a.fcount = 0;

@@ -14,6 +14,16 @@
 //
 // Every kernel computes each case exactly as the single-case launches do, so
 // a case's results in a batch are bit-for-bit those of running it alone.
+//
+// Steady steps run as CUDA graphs (lbm_batch_set_graphs): a segment of
+// kGraphSteps steps in which the active cases, the case table and the force
+// ring stay as they are and no fields are written is captured once, with
+// every dependency of the per-step stream code as a graph edge and all of its
+// arguments in one device buffer uploaded by the graph's first node; later
+// segments of the same structure (the cases, and where in the segment each
+// factorization launch and wait falls) only rewrite that buffer's host copy
+// and relaunch the instantiated graph. The steps around them (the first step
+// of a run, the last two, a case's last two) go through the stream code.
 #include <algorithm>
 #include <cmath>
 #include <cstdlib>
@@ -31,6 +41,12 @@ constexpr int kGroupRing = 64;
 // per-step argument buffers in flight: the host prepares a step's arguments
 // while up to kArgRing - 1 earlier steps are still queued
 constexpr int kArgRing = 8;
+// steps per CUDA graph segment (a multiple of the factorization batch, so
+// that segments of a run share their structure) and instantiated graphs kept
+constexpr int kGraphSteps = 16;
+constexpr int kGraphCache = 8;
+
+size_t round256(size_t x) { return (x + 255) & ~(size_t)255; }
 }
 
 struct lbm_batch {
@@ -65,6 +81,27 @@ struct lbm_batch {
     size_t ib_sz = 0, kf_sz = 0;
     int rows_per_cta = 0;   // 0: the cases' own setting
     std::vector<int> status;   // each case's status in the last run (lbm_batch_case_status)
+    // CUDA graph segments: two argument buffers (device and pinned host) used
+    // by alternate segments, each with the event of the last graph launch
+    // that read it; the instantiated graphs by segment structure, each with
+    // the kernels it launches per case (lbm_get_launch_count)
+    int graphs = 1;
+    int gset = 0;
+    size_t seg_bytes = 0;
+    void *d_seg[2] = {}, *h_seg[2] = {};
+    cudaEvent_t ev_gdone[2] = {};
+    // events of the captured stream code (never waited on outside a capture):
+    // fork, upload, joins, and per step the flow chain's points, then one per
+    // factorization launch of the segment
+    cudaEvent_t ev_cap[9 + 2 * kGraphSteps] = {};
+    cudaEvent_t ev_gpre = nullptr;   // the factor stream's work before a graph launch
+    struct GraphEntry {
+        std::vector<long long> sig;
+        cudaGraphExec_t exec = nullptr;
+        std::vector<long long> launches;
+    };
+    std::vector<GraphEntry> gcache;
+    long long graph_steps = 0, graph_launches = 0, graph_builds = 0;   // lbm_batch_graph_stats
     std::string err;
 };
 
@@ -108,7 +145,24 @@ void free_arrays(lbm_batch *b)
         if (b->h_fargs[r]) cudaFreeHost(b->h_fargs[r]);
         b->d_fargs[r] = b->h_fargs[r] = nullptr;
     }
+    // the graphs name these buffers
+    for (auto &g : b->gcache)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    b->gcache.clear();
+    for (int q = 0; q < 2; ++q) {
+        if (b->d_seg[q]) cudaFree(b->d_seg[q]);
+        if (b->h_seg[q]) cudaFreeHost(b->h_seg[q]);
+        b->d_seg[q] = b->h_seg[q] = nullptr;
+    }
+    b->seg_bytes = 0;
     b->cap = b->table_cap = 0;
+}
+
+void clear_graphs(lbm_batch *b)
+{
+    for (auto &g : b->gcache)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    b->gcache.clear();
 }
 
 void free_batch(lbm_batch *b)
@@ -127,7 +181,10 @@ void free_batch(lbm_batch *b)
         if (b->ev_fup[r]) cudaEventDestroy(b->ev_fup[r]);
     for (int r = 0; r < kGroupRing; ++r)
         if (b->ev_group[r]) cudaEventDestroy(b->ev_group[r]);
-    for (cudaEvent_t e : {b->ev_ib, b->ev_done, b->ev_fready, b->ev_side, b->ev_t0, b->ev_t1, b->ev_interp})
+    for (cudaEvent_t e : {b->ev_ib, b->ev_done, b->ev_fready, b->ev_side, b->ev_t0, b->ev_t1, b->ev_interp,
+                          b->ev_gdone[0], b->ev_gdone[1], b->ev_gpre})
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : b->ev_cap)
         if (e) cudaEventDestroy(e);
     if (b->main) cudaStreamDestroy(b->main);
     if (b->side) cudaStreamDestroy(b->side);
@@ -154,6 +211,14 @@ int reserve(lbm_batch *b, int ncase, int ntab)
     for (int r = 0; r < kFactorRing; ++r) {
         BCK(cudaMalloc(&b->d_fargs[r], nc * b->ib_sz), "alloc");
         BCK(cudaMallocHost(&b->h_fargs[r], nc * b->ib_sz), "alloc");
+    }
+    // a graph segment's arguments: per step the flow-chain and lattice
+    // arguments of every case, and up to two factorization launches per step
+    b->seg_bytes = round256((size_t)kGraphSteps * nc * b->ib_sz) + round256((size_t)kGraphSteps * nc * b->kf_sz) +
+                   round256((size_t)2 * kGraphSteps * nc * b->ib_sz);
+    for (int q = 0; q < 2; ++q) {
+        BCK(cudaMalloc(&b->d_seg[q], b->seg_bytes), "alloc");
+        BCK(cudaMallocHost(&b->h_seg[q], b->seg_bytes), "alloc");
     }
     b->cap = nc;
     b->table_cap = nt;
@@ -210,6 +275,8 @@ int add_case(lbm_batch *b, lbm_handle *h)
     for (lbm_handle *o : b->cases) need += table_need(o);
     if ((rc = reserve(b, (int)b->cases.size() + 1, need))) return rc;
     b->cases.push_back(h);
+    sync_streams(b);
+    clear_graphs(b);
     return LBM_OK;
 }
 
@@ -245,9 +312,12 @@ int lbm_batch_create(lbm_t *const *cases, int count, lbm_batch_t **out)
     for (cudaEvent_t *ev : {&b->ev_t0, &b->ev_t1})
         if ((e = cudaEventCreate(ev)) != cudaSuccess) return fail(e, "event");
     if (const char *ev = getenv("LBM_AFTER_INTERP")) b->after_interp = atoi(ev) != 0;
+    if (const char *ev = getenv("LBM_BATCH_GRAPHS")) b->graphs = atoi(ev) != 0;
     for (cudaEvent_t *ev : {&b->ev_interp, &b->ev_ib, &b->ev_done, &b->ev_fready, &b->ev_side, &b->ev_tup[0], &b->ev_tup[1],
-                            &b->ev_tuse[0], &b->ev_tuse[1]})
+                            &b->ev_tuse[0], &b->ev_tuse[1], &b->ev_gdone[0], &b->ev_gdone[1], &b->ev_gpre})
         if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
+    for (cudaEvent_t &ev : b->ev_cap)
+        if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
     for (int q = 0; q < kArgRing; ++q)
         for (cudaEvent_t *ev : {&b->ev_upload[q], &b->ev_kdone[q]})
             if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
@@ -282,6 +352,7 @@ int lbm_batch_remove(lbm_batch_t *b, lbm_t *h)
     if (it == b->cases.end()) return berr(b, LBM_ERR_ARG, "batch: the case is not in the batch");
     sync_streams(b);
     b->cases.erase(it);
+    clear_graphs(b);
     return LBM_OK;
 }
 
@@ -306,6 +377,23 @@ int lbm_batch_get_timing(const lbm_batch_t *b, double *ms, int *steps)
     if (!b) return LBM_ERR_ARG;
     if (ms) *ms = b->last_ms;
     if (steps) *steps = b->last_steps;
+    return LBM_OK;
+}
+
+int lbm_batch_set_graphs(lbm_batch_t *b, int enable)
+{
+    if (!b) return LBM_ERR_ARG;
+    b->graphs = enable != 0;
+    return LBM_OK;
+}
+
+int lbm_batch_graph_stats(const lbm_batch_t *b, long long *graph_steps, long long *graph_launches,
+                          long long *graph_builds)
+{
+    if (!b) return LBM_ERR_ARG;
+    if (graph_steps) *graph_steps = b->graph_steps;
+    if (graph_launches) *graph_launches = b->graph_launches;
+    if (graph_builds) *graph_builds = b->graph_builds;
     return LBM_OK;
 }
 
@@ -426,19 +514,222 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
         }
         return st0;
     };
+    std::vector<lbm_handle *> act, prev_act;
+    std::vector<int> act_idx;
+    int tcur = -1, ntab = 0;           // table buffer in use, its entries
+    bool cons0 = true;                 // every case's conserved-moment relaxation rates are zero
+    for (lbm_handle *h : b->cases) cons0 = cons0 && h->s[0] == 0.0 && h->s[3] == 0.0 && h->s[5] == 0.0;
+    // One CUDA graph segment of kGraphSteps steps from `step` (the caller has
+    // checked that it may run one: the same active cases and case table as
+    // the step before, no fields, room in the force ring). The host plans the
+    // segment as the stream code would issue it (factorization groups, the
+    // waits on them, every step's arguments), writes the arguments into the
+    // host copy of one of the two segment buffers, and launches the graph of
+    // that structure, which it captures and instantiates first when new.
+    struct GroupPlan {
+        std::vector<int> members;   // active-case indices
+        long long seq = 0;
+        size_t off = 0;             // arguments in the segment buffer
+    };
+    struct StepPlan {
+        int cur = -1, next = -1;    // factorization groups before / after the flow chain
+        std::vector<int> waits;     // groups of this segment the flow chain waits for
+    };
+    auto graph_segment = [&]() -> int {
+        const int G = kGraphSteps, na = (int)act.size();
+        const int sb = b->gset;
+        b->gset ^= 1;
+        BCK(cudaEventSynchronize(b->ev_gdone[sb]), "sync segment");   // the last graph that read this buffer
+        char *hs = (char *)b->h_seg[sb], *ds = (char *)b->d_seg[sb];
+        const size_t off_k = round256((size_t)G * na * b->ib_sz);
+        const size_t off_f = off_k + round256((size_t)G * na * b->kf_sz);
+        std::vector<GroupPlan> groups;
+        std::vector<StepPlan> plan(G);
+        const long long seq_seg = b->gseq;   // groups numbered above it are the segment's own
+        // a factorization group, chosen as factor_needed chooses it
+        auto plan_factor = [&](bool next) -> int {
+            GroupPlan g;
+            for (int c = 0; c < na; ++c) {
+                lbm_handle *h = act[c];
+                const int bi = h->n / K + (next ? 1 : 0);
+                if (h->batch_in_half[bi & 1] == bi) continue;
+                if (next && bi * K > last_step[act_idx[c]]) continue;
+                g.members.push_back(c);
+            }
+            if (g.members.empty()) return -1;
+            g.off = off_f + groups.size() * (size_t)na * b->ib_sz;   // at most two groups a step
+            g.seq = ++b->gseq;
+            for (size_t m = 0; m < g.members.size(); ++m) {
+                lbm_handle *h = act[g.members[m]];
+                const int bi = h->n / K + (next ? 1 : 0);
+                const int s0 = std::max(1, bi * K);   // steps start at 1
+                ib_factor_args_write(h, s0, bi * K + K - s0, hs + g.off + m * b->ib_sz);
+                h->batch_in_half[bi & 1] = bi;
+                h->fgroup[bi & 1] = g.seq;
+            }
+            groups.push_back(std::move(g));
+            return (int)groups.size() - 1;
+        };
+        for (int t = 0; t < G; ++t) {
+            StepPlan &p = plan[t];
+            p.cur = plan_factor(false);
+            // groups from before the segment are complete when the graph starts
+            for (int c = 0; c < na; ++c) {
+                const long long g = act[c]->fgroup[(act[c]->n / K) & 1];
+                const int gi = (int)(g - seq_seg - 1);
+                if (g > seq_seg && std::find(p.waits.begin(), p.waits.end(), gi) == p.waits.end()) p.waits.push_back(gi);
+            }
+            for (int c = 0; c < na; ++c) {
+                lbm_handle *h = act[c];
+                const int q = h->n % b->nslots;
+                h->pinfo_slot = q;
+                IBArgs *ia = (IBArgs *)(hs + ((size_t)t * na + c) * b->ib_sz);
+                ib_args_write(h, h->fbuf[h->cur], q, ia);
+                // a segment holds neither the call's nor a case's last step
+                ia->check_res = (h->n + 1) % K == 0;
+                ia->ring_row = pending + t;
+                kf_args_write(h, h->fbuf[h->cur], h->fbuf[h->cur ^ 1], nullptr, KF_OUTER,
+                              hs + off_k + ((size_t)t * na + c) * b->kf_sz);
+            }
+            p.next = plan_factor(true);
+            for (int c = 0; c < na; ++c) {
+                lbm_handle *h = act[c];
+                h->cur ^= 1;
+                h->n++;
+                h->steps_done++;
+                done[act_idx[c]]++;
+            }
+        }
+        const size_t used = off_f + groups.size() * (size_t)na * b->ib_sz;
+        // the structure: what sets grid sizes, kernel variants, buffer
+        // addresses and the graph's edges
+        std::vector<long long> sig = {sb, G, na, b->prec, cons0, b->after_interp, tcur, ntab, K, (long long)used};
+        for (lbm_handle *h : act)
+            sig.insert(sig.end(), {(long long)(uintptr_t)h, h->nseg, h->patch_gx(), h->patch_gy(), h->static_order});
+        for (const StepPlan &p : plan) {
+            sig.insert(sig.end(), {p.cur, p.next, (long long)p.waits.size()});
+            sig.insert(sig.end(), p.waits.begin(), p.waits.end());
+        }
+        for (const GroupPlan &g : groups) {
+            sig.push_back((long long)g.members.size());
+            sig.insert(sig.end(), g.members.begin(), g.members.end());
+        }
+        // the segment's stream code: the per-step sequence of the stream path
+        // below, with every dependency inside the segment
+        auto emit = [&]() -> int {
+            cudaEvent_t *E = b->ev_cap;
+            BCK(cudaEventRecord(E[0], b->side), "event");
+            BCK(cudaMemcpyAsync(ds, hs, used, cudaMemcpyHostToDevice, b->side), "upload");
+            BCK(cudaEventRecord(E[1], b->side), "event");
+            BCK(cudaStreamWaitEvent(b->main, E[1], 0), "wait");
+            BCK(cudaStreamWaitEvent(b->fstream, E[1], 0), "wait");
+            cudaEvent_t ei = b->after_interp ? E[8] : nullptr;
+            std::vector<lbm_handle *> grp;
+            auto factor = [&](int gi, bool after_side) -> int {
+                grp.clear();
+                for (int m : groups[gi].members) grp.push_back(act[m]);
+                if (after_side) BCK(cudaStreamWaitEvent(b->fstream, E[6], 0), "wait");
+                if (launch_factor_batch(grp.data(), (int)grp.size(), ds + groups[gi].off, 0, K, b->fstream))
+                    return berr(b, LBM_ERR_CUDA, "batch: launch factor");
+                BCK(cudaEventRecord(E[9 + gi], b->fstream), "event");
+                return LBM_OK;
+            };
+            int erc = LBM_OK;
+            for (int t = 0; t < G; ++t) {
+                const StepPlan &p = plan[t];
+                if (p.cur >= 0 && (erc = factor(p.cur, t > 0))) return erc;
+                if (t > 0) BCK(cudaStreamWaitEvent(b->side, E[7], 0), "wait");
+                for (int gi : p.waits) BCK(cudaStreamWaitEvent(b->side, E[9 + gi], 0), "wait");
+                BCK(cudaEventRecord(E[4], b->side), "event");
+                const char *sa = ds + (size_t)t * na * b->ib_sz;
+                const char *ka = ds + off_k + (size_t)t * na * b->kf_sz;
+                if (launch_flow_batch(act.data(), na, sa, ka, 0, 0, false, b->side, ei))
+                    return berr(b, LBM_ERR_CUDA, "batch: launch flow");
+                BCK(cudaEventRecord(E[5], b->side), "event");
+                if (launch_check_batch(act.data(), na, sa, 0, b->side)) return berr(b, LBM_ERR_CUDA, "batch: launch check");
+                BCK(cudaEventRecord(E[6], b->side), "event");
+                if (p.next >= 0 && (erc = factor(p.next, true))) return erc;
+                BCK(cudaStreamWaitEvent(b->main, E[4], 0), "wait");
+                if (ei) BCK(cudaStreamWaitEvent(b->main, ei, 0), "wait");   // the solves start first
+                if (launch_kf_multi(b->prec, ka, b->d_table[tcur], ntab, false, cons0, b->main))
+                    return berr(b, LBM_ERR_CUDA, "batch: launch lattice");
+                for (lbm_handle *h : act) h->launches += 1;
+                BCK(cudaStreamWaitEvent(b->main, E[5], 0), "wait");
+                BCK(cudaEventRecord(E[7], b->main), "event");   // the step is complete
+            }
+            BCK(cudaEventRecord(E[2], b->main), "event");
+            BCK(cudaEventRecord(E[3], b->fstream), "event");
+            BCK(cudaStreamWaitEvent(b->side, E[2], 0), "wait");
+            BCK(cudaStreamWaitEvent(b->side, E[3], 0), "wait");
+            return LBM_OK;
+        };
+        // the graph starts after every stream's earlier work
+        BCK(cudaEventRecord(b->ev_gpre, b->fstream), "event");
+        BCK(cudaStreamWaitEvent(b->side, b->ev_done, 0), "wait");
+        BCK(cudaStreamWaitEvent(b->side, b->ev_gpre, 0), "wait");
+        lbm_batch::GraphEntry *ge = nullptr;
+        for (auto &e : b->gcache)
+            if (e.sig == sig) {
+                ge = &e;
+                break;
+            }
+        if (!ge) {
+            lbm_batch::GraphEntry e;
+            e.sig = std::move(sig);
+            std::vector<long long> l0(na);
+            for (int c = 0; c < na; ++c) l0[c] = act[c]->launches;
+            cudaGraph_t graph = nullptr;
+            BCK(cudaStreamBeginCapture(b->side, cudaStreamCaptureModeThreadLocal), "graph capture");
+            // the capture ends whatever emit returns, so that the streams
+            // are usable again
+            const int erc = emit();
+            const cudaError_t ce = cudaStreamEndCapture(b->side, &graph);
+            if (erc == LBM_OK && ce == cudaSuccess) {
+                const cudaError_t ie = cudaGraphInstantiate(&e.exec, graph, 0);
+                cudaGraphDestroy(graph);
+                if (ie != cudaSuccess) return berr(b, LBM_ERR_CUDA, std::string("batch: graph instantiate: ") + cudaGetErrorString(ie));
+            } else {
+                if (graph) cudaGraphDestroy(graph);
+                cudaGetLastError();
+                return erc ? erc : berr(b, LBM_ERR_CUDA, std::string("batch: graph capture: ") + cudaGetErrorString(ce));
+            }
+            e.launches.resize(na);
+            for (int c = 0; c < na; ++c) {
+                e.launches[c] = act[c]->launches - l0[c];
+                act[c]->launches = l0[c];
+            }
+            if ((int)b->gcache.size() >= kGraphCache) {
+                cudaGraphExecDestroy(b->gcache.front().exec);
+                b->gcache.erase(b->gcache.begin());
+            }
+            b->gcache.push_back(std::move(e));
+            ge = &b->gcache.back();
+            b->graph_builds++;
+        }
+        BCK(cudaGraphLaunch(ge->exec, b->side), "graph launch");
+        for (int c = 0; c < na; ++c) act[c]->launches += ge->launches[c];
+        b->graph_launches++;
+        b->graph_steps += G;
+        // the stream code after the graph sees it as its previous step
+        BCK(cudaEventRecord(b->ev_gdone[sb], b->side), "event");
+        BCK(cudaEventRecord(b->ev_done, b->side), "event");
+        BCK(cudaEventRecord(b->ev_side, b->side), "event");
+        BCK(cudaEventRecord(b->ev_tuse[tcur], b->side), "event");
+        for (const GroupPlan &g : groups) BCK(cudaEventRecord(b->ev_group[g.seq % kGroupRing], b->side), "event");
+        BCK(cudaStreamWaitEvent(b->main, b->ev_done, 0), "wait");
+        BCK(cudaStreamWaitEvent(b->fstream, b->ev_side, 0), "wait");
+        return LBM_OK;
+    };
     BCK(cudaEventRecord(b->ev_done, b->main), "event");
     BCK(cudaEventRecord(b->ev_side, b->side), "event");
     BCK(cudaEventRecord(b->ev_t0, b->main), "event");
     b->last_ms = 0.0;
     b->last_steps = 0;
-    std::vector<lbm_handle *> act;
-    std::vector<int> act_idx;
     std::vector<long long> waited;
     std::vector<int> tkey, tkey_now;   // grids of the active cases the current table was built for
-    bool cons0 = true;                 // every case's conserved-moment relaxation rates are zero
-    for (lbm_handle *h : b->cases) cons0 = cons0 && h->s[0] == 0.0 && h->s[3] == 0.0 && h->s[5] == 0.0;
-    int tcur = -1, ntab = 0;           // table buffer in use, its entries
+    const int ring_cap = b->cases[0]->ring_cap;
     for (; step < nsteps; ++step) {
+        prev_act.swap(act);
         act.clear();
         act_idx.clear();
         for (int c = 0; c < nc; ++c)
@@ -447,6 +738,19 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
                 act_idx.push_back(c);
             }
         if (act.empty()) break;
+        // a graph segment where the next kGraphSteps steps allow one
+        if (b->graphs && tcur >= 0 && act == prev_act && step + kGraphSteps <= nsteps - 2 &&
+            pending + kGraphSteps <= ring_cap) {
+            bool ok = true;
+            for (size_t c = 0; c < act.size() && ok; ++c) ok = act[c]->n + kGraphSteps < last_step[act_idx[c]];
+            if (ok) {
+                if ((rc = graph_segment())) break;
+                step += kGraphSteps - 1;
+                pending += kGraphSteps;
+                if (pending == ring_cap && (rc = flush())) break;
+                continue;
+            }
+        }
         const int buf = step % kArgRing;
         // fields (rho, u, v) for the last two steps of the call and of every
         // case that ends within them (all active cases keep them then)
@@ -475,6 +779,7 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
             // the solve-residual check: last step of the case's factorization
             // batch, of the call, or of the case's motion
             ia->check_res = (h->n + 1) % K == 0 || step == nsteps - 1 || h->n >= last_step[act_idx[c]];
+            ia->ring_row = pending;
             kf_args_write(h, fin, fout, fd, KF_OUTER, (char *)b->h_kargs[buf] + c * b->kf_sz);
             int gx, gy;
             kf_tma_grid(h, &gx, &gy);
@@ -558,7 +863,7 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
         }
         pending++;
         // force rows to the host every ring's worth of steps
-        if (pending == b->cases[0]->ring_cap) {
+        if (pending == ring_cap) {
             if ((rc = flush())) break;
         }
     }

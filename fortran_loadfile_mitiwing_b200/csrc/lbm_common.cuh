@@ -42,11 +42,11 @@ __host__ __device__ constexpr int lbm_ey(int k)
 #define LBM_ST_INDEX_INTERP 0x100u      // ib_interp: support box
 #define LBM_ST_INDEX_ASSEMBLE 0x200u    // ib_assemble: solve order, support box
 #define LBM_ST_INDEX_FACTOR 0x400u      // ib_factor (dense path): solve order, support box
-#define LBM_ST_INDEX_SOLVE 0x800u       // ib_solve: solve order
+#define LBM_ST_INDEX_SOLVE 0x800u       // ib_solve: solve order, force-ring row
 #define LBM_ST_INDEX_SCATTER 0x1000u    // ib_tile_scatter: tile of a support box
 #define LBM_ST_INDEX_SORT 0x2000u       // ib_tile_sort: correction tile
 #define LBM_ST_INDEX_TILE 0x4000u       // ib_tile_update: correction tile, listed marker, box, wing
-#define LBM_ST_INDEX_FORCES 0x8000u     // ib_forces: correction tile
+#define LBM_ST_INDEX_FORCES 0x8000u     // ib_forces: correction tile, force-ring row
 #define LBM_ST_INDEX_RESIDUAL 0x10000u  // ib_residual: solve order, support box
 #define LBM_ST_INDEX_LATTICE 0x20000u   // kf_tma: tile of the patch rectangle
 #define LBM_ST_INDEX_MASK 0x3ff00u

@@ -91,6 +91,9 @@ struct IBArgs {
     unsigned *counter;  // last-block counter
     double *force_ring; // [ring_cap][row_len]
     int row_len;
+    // batched launches: the force-ring row of this case's step (the rows
+    // held: ring_rows); single-case launches take the row as a parameter
+    int ring_row, ring_rows;
     unsigned *status;
     double *solve_res;  // relative residual of the last solve
 };

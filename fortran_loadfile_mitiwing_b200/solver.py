@@ -246,6 +246,23 @@ class Batch:
             raise LbmError(rc, self.lib.lbm_batch_last_error(self.b).decode())
         self.rows = int(rows_per_cta)
 
+    def set_graphs(self, enable):
+        """Steady steps as replayed CUDA graphs of 16 steps (True, the
+        default) or every launch issued from the host (False); the results
+        are the same bit for bit."""
+        rc = self.lib.lbm_batch_set_graphs(self.b, 1 if enable else 0)
+        if rc != 0:
+            raise LbmError(rc, self.lib.lbm_batch_last_error(self.b).decode())
+
+    def graph_stats(self):
+        """(steps run as graph segments, graph launches, graphs
+        instantiated) over the batch's life."""
+        v = [C.c_longlong() for _ in range(3)]
+        rc = self.lib.lbm_batch_graph_stats(self.b, *[C.byref(x) for x in v])
+        if rc != 0:
+            raise LbmError(rc, self.lib.lbm_batch_last_error(self.b).decode())
+        return tuple(x.value for x in v)
+
     def run(self, nsteps, keep_rows=True, errors="raise"):
         """Steps every case up to `nsteps` times; returns each case's force
         rows (trimmed to the steps it ran) or the step counts. A failed case

@@ -109,13 +109,53 @@ def run_batch(specs, steps, warmup, precision, lib=None, tune=True):
     return lups / el, el, timing, b.rows
 
 
+def launch_floor(counts=(1, 8, 64), steps=192, warmup=24, lib=None):
+    """Time per step of batches of tiny cases (128x64 lattices, 40 markers,
+    where the GPU has almost nothing to do): the floor that issuing the
+    launches sets, with the steady steps replayed as CUDA graphs and with
+    every launch issued from the host, and one case stepped alone (lbm_run)
+    for comparison. Wall clock around one run of `steps` steps after a
+    warm-up run, in microseconds per step; the device time of the same run
+    (lbm_batch_get_timing) beside it."""
+    out = {}
+    n_steps = 2 * (steps + warmup) + 64
+    one = Lbm.from_case(cs.small_case(nx=128, ny=64, n_steps=n_steps), lib)
+    one.run(warmup, keep_rows=False)
+    t0 = time.perf_counter()
+    one.run(steps, keep_rows=False)
+    out["alone_us"] = (time.perf_counter() - t0) / steps * 1e6
+    one.close()
+    for n in counts:
+        hs = [Lbm.from_case(cs.small_case(nx=128, ny=64, n_steps=n_steps, seed=7 + c), lib) for c in range(n)]
+        row = {}
+        with Batch(hs) as b:
+            for graphs in (True, False):
+                b.set_graphs(graphs)
+                b.run(warmup, keep_rows=False)
+                t0 = time.perf_counter()
+                b.run(steps, keep_rows=False)
+                el = time.perf_counter() - t0
+                ms, k = b.device_time()
+                key = "graphs" if graphs else "stream"
+                row[key + "_us"] = el / steps * 1e6
+                row[key + "_device_us"] = ms * 1e3 / max(k, 1)
+        for h in hs:
+            h.close()
+        out[str(n)] = row
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--cases", type=int, default=64)
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=12)
     ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--floor", action="store_true", help="only the per-step floor of batches of tiny cases")
     args = ap.parse_args()
+    if args.floor:
+        print(json.dumps(launch_floor()))
+        return
     specs = sweep_specs(args.cases, args.seed)
     res = {"cases": args.cases, "steps_per_case": args.steps, "seed": args.seed,
            "grid_nodes_total": sum(s["nx"] * s["ny"] for s in specs)}

@@ -387,7 +387,19 @@ LBM_API int lbm_read_flow_field_file(const char *path, int nx, int ny, int wing_
  *   lbm_batch_get_timing: device milliseconds of the last lbm_batch_run's
  *     steps (CUDA events on the batch's streams, from before the first
  *     step's launches to the end of the last step) and the number of steps
- *     it ran; 0 after a run that failed. */
+ *     it ran; 0 after a run that failed.
+ *   lbm_batch_set_graphs: 1 (the default; environment LBM_BATCH_GRAPHS=0
+ *     turns it off at creation) runs steady steps as CUDA graphs of 16
+ *     steps: wherever the next 16 steps keep the same active cases and
+ *     write no fields (not the first step of a run, nor the last two of the
+ *     call or of a case), the batch replays an instantiated graph of those
+ *     steps' launches, captured the first time a segment of that structure
+ *     occurs and kept (up to 8 per batch; adding or removing a case drops
+ *     them), after rewriting the host copy of the argument buffer the
+ *     graph's first node uploads. 0 issues every step's launches from the
+ *     host. The results are the same bit for bit.
+ *   lbm_batch_graph_stats: steps run as graph segments, graph launches and
+ *     graphs instantiated over the batch's life (each nullable). */
 typedef struct lbm_batch lbm_batch_t;
 LBM_API int lbm_batch_create(lbm_t *const *cases, int count, lbm_batch_t **out);
 LBM_API int lbm_batch_destroy(lbm_batch_t *b);
@@ -396,6 +408,9 @@ LBM_API int lbm_batch_remove(lbm_batch_t *b, lbm_t *h);
 LBM_API int lbm_batch_count(const lbm_batch_t *b);
 LBM_API int lbm_batch_case_status(const lbm_batch_t *b, int c);
 LBM_API int lbm_batch_set_rows(lbm_batch_t *b, int rows_per_cta);
+LBM_API int lbm_batch_set_graphs(lbm_batch_t *b, int enable);
+LBM_API int lbm_batch_graph_stats(const lbm_batch_t *b, long long *graph_steps, long long *graph_launches,
+                                  long long *graph_builds);
 LBM_API int lbm_batch_get_timing(const lbm_batch_t *b, double *ms, int *steps);
 LBM_API int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *done_steps);
 LBM_API const char *lbm_batch_last_error(const lbm_batch_t *b);

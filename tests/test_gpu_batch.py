@@ -138,3 +138,45 @@ def test_odd_row_chunks_equal_alone(gpu_lib, precision):
         for c, (t, a) in enumerate(zip(together, alone)):
             np.testing.assert_array_equal(rows_b[c], a.run(21), err_msg=f"rows {rows} case {c}")
             np.testing.assert_array_equal(t.populations(), a.populations(), err_msg=f"rows {rows} case {c}")
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp16"])
+def test_graph_segments_equal_stream_code(gpu_lib, precision):
+    """Steady steps replayed as CUDA graphs give the steps the host issues one
+    by one, bit for bit: two runs (the second starting mid-way through a
+    factorization batch and through the force ring's rows), with a case
+    joining in between at another phase of its factorization batches; the
+    graphs of repeated segments are reused, not captured again."""
+    graphed = build(precision, 160, lib=gpu_lib)
+    plain = build(precision, 160, lib=gpu_lib)
+    late_g = Lbm.from_case(cases.small_case(precision=precision, n_steps=160, **SPECS[0]), gpu_lib)
+    late_p = Lbm.from_case(cases.small_case(precision=precision, n_steps=160, **SPECS[0]), gpu_lib)
+    late_g.run(3)
+    late_p.run(3)
+    rows = {}
+    for key, cs, late, graphs in (("g", graphed, late_g, True), ("p", plain, late_p, False)):
+        with Batch(cs) as b:
+            b.set_graphs(graphs)
+            r1 = b.run(54)
+            b.add(late)
+            r2 = b.run(61)
+            rows[key] = (r1, r2)
+            stats = b.graph_stats()
+        if graphs:
+            # 3 segments in the first run, 3 in the second; both argument
+            # buffers alternate, so at most 2 structures per run
+            assert stats[0] == 16 * 6 and stats[1] == 6 and 1 <= stats[2] <= 5, stats
+        else:
+            assert stats == (0, 0, 0), stats
+    for c in range(len(SPECS)):
+        np.testing.assert_array_equal(rows["g"][0][c], rows["p"][0][c], err_msg=f"run 1 case {c}")
+        np.testing.assert_array_equal(rows["g"][1][c], rows["p"][1][c], err_msg=f"run 2 case {c}")
+        np.testing.assert_array_equal(graphed[c].populations(), plain[c].populations(), err_msg=f"case {c}")
+    np.testing.assert_array_equal(rows["g"][1][3], rows["p"][1][3], err_msg="joined case")
+    np.testing.assert_array_equal(late_g.populations(), late_p.populations())
+    # and the graphed batch equals each case alone
+    alone = build(precision, 160, lib=gpu_lib)
+    for c, a in enumerate(alone):
+        np.testing.assert_array_equal(np.concatenate(rows["g"][0][c:c + 1] + rows["g"][1][c:c + 1]), a.run(115),
+                                      err_msg=f"alone case {c}")
+        np.testing.assert_array_equal(graphed[c].populations(), a.populations())
