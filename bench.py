@@ -406,11 +406,12 @@ def run_batched(lib, n_cases=64, steps=100, warmup=12):
     specs = sweep.sweep_specs(n_cases, 2026)
     t0 = time.perf_counter()
     r_alone, _ = sweep.run_alone(specs, steps, warmup, "fp32", lib)
-    r16, _, _, rows = sweep.run_batch(specs, steps, warmup, "fp16", lib)
+    r16, _, _, choice = sweep.run_batch(specs, steps, warmup, "fp16", lib)
     base, b16 = sweep.cases_per_hour(specs, r_alone), sweep.cases_per_hour(specs, r16)
     return {"cases": n_cases, "steps_per_case": steps, "alone_fp32_mlups": r_alone / 1e6,
             "batch_fp16_mlups": r16 / 1e6, "alone_fp32_cases_per_hour": base, "batch_fp16_cases_per_hour": b16,
-            "batch_fp16_vs_alone_fp32": b16 / base, "rows_per_cta": rows,
+            "batch_fp16_vs_alone_fp32": b16 / base, "autotuned": choice,
+            "floor_us_per_step": sweep.launch_floor(lib=lib),
             "wall_s": time.perf_counter() - t0}
 
 

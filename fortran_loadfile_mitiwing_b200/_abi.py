@@ -114,6 +114,7 @@ ABI = {
     "lbm_batch_count": (C.c_int, [_P]),
     "lbm_batch_case_status": (C.c_int, [_P, C.c_int]),
     "lbm_batch_set_rows": (C.c_int, [_P, C.c_int]),
+    "lbm_batch_set_occupancy": (C.c_int, [_P, C.c_int]),
     "lbm_batch_set_graphs": (C.c_int, [_P, C.c_int]),
     "lbm_batch_graph_stats": (C.c_int, [_P, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                         C.POINTER(C.c_longlong)]),

@@ -468,14 +468,29 @@ void launch_tma(const lbm_handle *h, const KFArgs<C> &a, bool fields, cudaStream
         launch_tma_f<T, C, false>(a, grid, st);
 }
 
+// the largest dynamic shared memory a CTA may opt in to on the current device
+int smem_optin()
+{
+    static int v = 0;
+    if (!v) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+            v = 0;
+    }
+    return v;
+}
+
 template <typename T, typename C, bool FIELDS, bool CONS0>
 int configure_one(int smem)
 {
     if (cudaFuncSetAttribute(kf_tma<T, C, FIELDS, CONS0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
         cudaSuccess)
         return -1;
-    if (cudaFuncSetAttribute(kf_tma_multi<T, C, FIELDS, CONS0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
-        cudaSuccess)
+    // the batched launch may ask for more than it uses, to hold fewer CTAs
+    // per SM (multi_smem)
+    if (cudaFuncSetAttribute(kf_tma_multi<T, C, FIELDS, CONS0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             std::max(smem, smem_optin())) != cudaSuccess)
         return -1;
     return 0;
 }
@@ -702,15 +717,39 @@ int launch_mass(lbm_handle *h, const void *fsrc, cudaStream_t st)
 
 int mass_slots() { return MASS_BLOCKS + 1; }
 
+// Dynamic shared memory of a batched lattice launch that holds at most
+// `ctas_per_sm` CTAs on an SM (0: the kernel's own ring, as many CTAs as the
+// registers allow, 4 for 2- and 4-byte storage). The kernel uses only its
+// ring; the rest of the request is an occupancy limit for the autotuner.
+template <typename T>
+size_t multi_smem(int ctas_per_sm)
+{
+    const size_t base = tma_smem<T>();
+    if (ctas_per_sm <= 0) return base;
+    static int per_sm = 0, reserved = 0;
+    if (!per_sm) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+            cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess)
+            per_sm = reserved = 0;
+    }
+    if (per_sm <= 0) return base;
+    // ctas_per_sm CTAs of this size fit, one more does not
+    size_t s = ((size_t)per_sm / ctas_per_sm - (size_t)reserved) & ~(size_t)127;
+    return std::min(std::max(s, base), (size_t)std::max(smem_optin(), (int)base));
+}
+
 template <typename T, typename C>
-int launch_kf_multi_t(const void *cases, const int4 *table, int nentries, bool fields, bool cons0, cudaStream_t st)
+int launch_kf_multi_t(const void *cases, const int4 *table, int nentries, bool fields, bool cons0, int ctas_per_sm,
+                      cudaStream_t st)
 {
     static bool configured = false;   // per process; the attribute is per function
     if (!configured) {
         if (configure_tma<T, C>()) return -1;
         configured = true;
     }
-    const size_t smem = tma_smem<T>();
+    const size_t smem = multi_smem<T>(ctas_per_sm);
     const KFArgs<C> *c = (const KFArgs<C> *)cases;
     if (fields && cons0)
         kf_tma_multi<T, C, true, true><<<nentries, TW, smem, st>>>(c, table);
@@ -739,13 +778,16 @@ void kf_tma_grid(const lbm_handle *h, int *gx, int *gy) { tma_grid(h->nx, h->ny,
 // the staged lattice kernel over a batch of cases (device arrays of their
 // arguments and of the case table)
 int launch_kf_multi(int prec, const void *cases, const int4 *table, int nentries, bool fields, bool cons0,
-                    cudaStream_t st)
+                    int ctas_per_sm, cudaStream_t st)
 {
     switch (prec) {
-    case LBM_PREC_FP32: return launch_kf_multi_t<float, float>(cases, table, nentries, fields, cons0, st);
-    case LBM_PREC_FP64: return launch_kf_multi_t<double, double>(cases, table, nentries, fields, cons0, st);
-    case LBM_PREC_FP16: return launch_kf_multi_t<__half, float>(cases, table, nentries, fields, cons0, st);
-    case LBM_PREC_BF16: return launch_kf_multi_t<__nv_bfloat16, float>(cases, table, nentries, fields, cons0, st);
+    case LBM_PREC_FP32: return launch_kf_multi_t<float, float>(cases, table, nentries, fields, cons0, ctas_per_sm, st);
+    case LBM_PREC_FP64:
+        return launch_kf_multi_t<double, double>(cases, table, nentries, fields, cons0, ctas_per_sm, st);
+    case LBM_PREC_FP16:
+        return launch_kf_multi_t<__half, float>(cases, table, nentries, fields, cons0, ctas_per_sm, st);
+    case LBM_PREC_BF16:
+        return launch_kf_multi_t<__nv_bfloat16, float>(cases, table, nentries, fields, cons0, ctas_per_sm, st);
     }
     return -1;
 }

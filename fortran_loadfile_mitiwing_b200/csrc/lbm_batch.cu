@@ -80,6 +80,7 @@ struct lbm_batch {
     long long gseq = 0;   // factorization launches so far
     size_t ib_sz = 0, kf_sz = 0;
     int rows_per_cta = 0;   // 0: the cases' own setting
+    int ctas_per_sm = 0;    // lattice CTAs per SM at most (0: as many as fit)
     std::vector<int> status;   // each case's status in the last run (lbm_batch_case_status)
     // CUDA graph segments: two argument buffers (device and pinned host) used
     // by alternate segments, each with the event of the last graph launch
@@ -380,6 +381,13 @@ int lbm_batch_get_timing(const lbm_batch_t *b, double *ms, int *steps)
     return LBM_OK;
 }
 
+int lbm_batch_set_occupancy(lbm_batch_t *b, int ctas_per_sm)
+{
+    if (!b || ctas_per_sm < 0 || ctas_per_sm > 8) return LBM_ERR_ARG;
+    b->ctas_per_sm = ctas_per_sm;
+    return LBM_OK;
+}
+
 int lbm_batch_set_graphs(lbm_batch_t *b, int enable)
 {
     if (!b) return LBM_ERR_ARG;
@@ -603,7 +611,8 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
         const size_t used = off_f + groups.size() * (size_t)na * b->ib_sz;
         // the structure: what sets grid sizes, kernel variants, buffer
         // addresses and the graph's edges
-        std::vector<long long> sig = {sb, G, na, b->prec, cons0, b->after_interp, tcur, ntab, K, (long long)used};
+        std::vector<long long> sig = {sb, G, na, b->prec, cons0, b->after_interp, tcur, ntab, K, (long long)used,
+                                      b->ctas_per_sm};
         for (lbm_handle *h : act)
             sig.insert(sig.end(), {(long long)(uintptr_t)h, h->nseg, h->patch_gx(), h->patch_gy(), h->static_order});
         for (const StepPlan &p : plan) {
@@ -651,7 +660,7 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
                 if (p.next >= 0 && (erc = factor(p.next, true))) return erc;
                 BCK(cudaStreamWaitEvent(b->main, E[4], 0), "wait");
                 if (ei) BCK(cudaStreamWaitEvent(b->main, ei, 0), "wait");   // the solves start first
-                if (launch_kf_multi(b->prec, ka, b->d_table[tcur], ntab, false, cons0, b->main))
+                if (launch_kf_multi(b->prec, ka, b->d_table[tcur], ntab, false, cons0, b->ctas_per_sm, b->main))
                     return berr(b, LBM_ERR_CUDA, "batch: launch lattice");
                 for (lbm_handle *h : act) h->launches += 1;
                 BCK(cudaStreamWaitEvent(b->main, E[5], 0), "wait");
@@ -845,7 +854,8 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
         // main stream: every case's lattice nodes but its correction tiles
         BCK(cudaStreamWaitEvent(b->main, b->ev_fready, 0), "wait");
         if (ei) BCK(cudaStreamWaitEvent(b->main, ei, 0), "wait");   // the solves start first
-        if (launch_kf_multi(b->prec, b->d_kargs[buf], b->d_table[tcur], ntab, fields, cons0, b->main)) {
+        if (launch_kf_multi(b->prec, b->d_kargs[buf], b->d_table[tcur], ntab, fields, cons0, b->ctas_per_sm,
+                            b->main)) {
             rc = berr(b, LBM_ERR_CUDA, "batch: launch lattice");
             break;
         }

@@ -241,9 +241,10 @@ int handle_restore(lbm_handle *h, const double *f, const double *u, const double
 size_t kf_args_size(int prec);
 void kf_args_write(lbm_handle *h, const void *fin, void *fout, void *fields, int mode, void *dst);
 void kf_tma_grid(const lbm_handle *h, int *gx, int *gy);
-// cons0: every case's conserved-moment relaxation rates are zero
+// cons0: every case's conserved-moment relaxation rates are zero;
+// ctas_per_sm: at most that many CTAs on an SM (0: as many as fit)
 int launch_kf_multi(int prec, const void *cases, const int4 *table, int nentries, bool fields, bool cons0,
-                    cudaStream_t st);
+                    int ctas_per_sm, cudaStream_t st);
 size_t ib_args_size();
 void ib_args_write(lbm_handle *h, const void *fin, int slot, void *dst);
 void ib_factor_args_write(lbm_handle *h, int step0, int count, void *dst);

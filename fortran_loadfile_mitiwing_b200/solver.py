@@ -205,6 +205,7 @@ class Batch:
             raise LbmError(rc, msgs)
         self.b = b
         self.rows = 0
+        self.occupancy = 0
 
     def __len__(self):
         return len(self.cases)
@@ -245,6 +246,13 @@ class Batch:
         if rc != 0:
             raise LbmError(rc, self.lib.lbm_batch_last_error(self.b).decode())
         self.rows = int(rows_per_cta)
+
+    def set_occupancy(self, ctas_per_sm):
+        """At most `ctas_per_sm` lattice CTAs per SM (0: as many as fit)."""
+        rc = self.lib.lbm_batch_set_occupancy(self.b, int(ctas_per_sm))
+        if rc != 0:
+            raise LbmError(rc, self.lib.lbm_batch_last_error(self.b).decode())
+        self.occupancy = int(ctas_per_sm)
 
     def set_graphs(self, enable):
         """Steady steps as replayed CUDA graphs of 16 steps (True, the
@@ -295,23 +303,30 @@ class Batch:
             raise LbmError(rc, self.lib.lbm_batch_last_error(self.b).decode())
         return ms.value, n.value
 
-    def autotune(self, steps_per_trial=20, candidates=(4, 8, 16), rounds=2):
-        """Picks the lattice kernel's rows per CTA for this batch by timing
-        `steps_per_trial` real steps with each candidate on the device (CUDA
-        events around the steps of each trial, `rounds` trials per candidate
-        in alternating order, the best kept); the steps advance the cases and
-        the results do not depend on the choice. Returns {rows: seconds per
-        step} and keeps the fastest."""
+    def autotune(self, steps_per_trial=20, candidates=(4, 8, 16), rounds=2, occupancy=(0, 3)):
+        """Picks the lattice kernel's tile shape (rows per CTA: `candidates`)
+        and occupancy (lattice CTAs per SM: `occupancy`, 0 for as many as
+        fit) for this batch by timing `steps_per_trial` real steps with each
+        pair on the device (CUDA events around the steps of each trial,
+        `rounds` trials per pair in alternating order, the best kept); the
+        steps advance the cases and the results do not depend on the choice.
+        Returns {(rows, ctas_per_sm): seconds per step} and keeps the
+        fastest. The strip width, the ring depth and the registers per
+        thread are compile-time choices of the kernel, measured on the
+        single case."""
         timing = {}
-        order = list(candidates)
+        order = [(r, o) for r in candidates for o in occupancy]
         for k in range(rounds):
-            for r in (order if k % 2 == 0 else order[::-1]):
+            for r, o in (order if k % 2 == 0 else order[::-1]):
                 self.set_rows(r)
+                self.set_occupancy(o)
                 self.run(steps_per_trial, keep_rows=False)
                 ms, n = self.device_time()
                 if n > 0:
                     t = ms / 1e3 / n
-                    timing[r] = min(timing.get(r, t), t)
+                    timing[(r, o)] = min(timing.get((r, o), t), t)
         if timing:
-            self.set_rows(min(timing, key=timing.get))
+            r, o = min(timing, key=timing.get)
+            self.set_rows(r)
+            self.set_occupancy(o)
         return timing

@@ -97,6 +97,8 @@ def run_batch(specs, steps, warmup, precision, lib=None, tune=True):
     hs = [make(sp, steps + warmup + 64, precision, lib) for sp in specs]
     b = Batch(hs)
     timing = b.autotune(steps_per_trial=max(2, warmup // 3), candidates=(4, 8, 16)) if tune else {}
+    timing = {f"rows {r}, ctas/SM {o or 'max'}": t for (r, o), t in timing.items()}
+    choice = {"rows_per_cta": b.rows, "ctas_per_sm": b.occupancy}
     b.run(warmup, keep_rows=False)
     t0 = time.perf_counter()
     done = b.run(steps, keep_rows=False)
@@ -106,7 +108,7 @@ def run_batch(specs, steps, warmup, precision, lib=None, tune=True):
     b.close()
     for h in hs:
         h.close()
-    return lups / el, el, timing, b.rows
+    return lups / el, el, timing, choice
 
 
 def launch_floor(counts=(1, 8, 64), steps=192, warmup=24, lib=None):
@@ -162,9 +164,9 @@ def main():
     r, t = run_alone(specs, args.steps, args.warmup, "fp32")
     res["alone_fp32"] = {"mlups": r / 1e6, "seconds": t, "cases_per_hour_5_periods": cases_per_hour(specs, r)}
     for prec in ("fp32", "fp16"):
-        r, t, timing, rows = run_batch(specs, args.steps, args.warmup, prec)
+        r, t, timing, choice = run_batch(specs, args.steps, args.warmup, prec)
         res["batch_" + prec] = {"mlups": r / 1e6, "seconds": t, "cases_per_hour_5_periods": cases_per_hour(specs, r),
-                                "rows_per_cta": rows, "autotune_s_per_step": timing}
+                                "autotuned": choice, "autotune_s_per_step": timing}
     base = res["alone_fp32"]["cases_per_hour_5_periods"]
     for k in ("batch_fp32", "batch_fp16"):
         res[k]["vs_alone_fp32"] = res[k]["cases_per_hour_5_periods"] / base

@@ -384,6 +384,10 @@ LBM_API int lbm_read_flow_field_file(const char *path, int nx, int ny, int wing_
  *     kept for the last two steps of the call and of each case that ends.
  *   lbm_batch_set_rows: rows per CTA of the lattice kernel for the batch
  *     (0: the cases' own); the batch autotuner of the Python layer sets it.
+ *   lbm_batch_set_occupancy: at most ctas_per_sm (1..8) CTAs of the batch's
+ *     lattice kernel on an SM, by asking each CTA for that share of the
+ *     SM's shared memory (0, the default: as many as the registers allow,
+ *     4 for 2- and 4-byte storage); the autotuner sets it beside the rows.
  *   lbm_batch_get_timing: device milliseconds of the last lbm_batch_run's
  *     steps (CUDA events on the batch's streams, from before the first
  *     step's launches to the end of the last step) and the number of steps
@@ -408,6 +412,7 @@ LBM_API int lbm_batch_remove(lbm_batch_t *b, lbm_t *h);
 LBM_API int lbm_batch_count(const lbm_batch_t *b);
 LBM_API int lbm_batch_case_status(const lbm_batch_t *b, int c);
 LBM_API int lbm_batch_set_rows(lbm_batch_t *b, int rows_per_cta);
+LBM_API int lbm_batch_set_occupancy(lbm_batch_t *b, int ctas_per_sm);
 LBM_API int lbm_batch_set_graphs(lbm_batch_t *b, int enable);
 LBM_API int lbm_batch_graph_stats(const lbm_batch_t *b, long long *graph_steps, long long *graph_launches,
                                   long long *graph_builds);

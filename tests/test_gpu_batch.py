@@ -50,14 +50,16 @@ def test_autotuned_batch_still_equals_alone(gpu_lib):
     together = build("fp32", 120, lib=gpu_lib)
     alone = build("fp32", 120, lib=gpu_lib)
     with Batch(together) as b:
-        timing = b.autotune(steps_per_trial=5, candidates=(4, 8, 16), rounds=2)   # 30 steps
-        assert set(timing) == {4, 8, 16} and b.rows in timing
+        # rows per CTA x lattice CTAs per SM, 2 rounds of 5 steps: 60 steps
+        timing = b.autotune(steps_per_trial=5, candidates=(4, 8, 16), rounds=2, occupancy=(0, 2))
+        assert set(timing) == {(r, o) for r in (4, 8, 16) for o in (0, 2)}
+        assert (b.rows, b.occupancy) in timing
         assert all(0 < t < 1.0 for t in timing.values())
         b.run(10, keep_rows=False)
         ms, n = b.device_time()      # device time of the last run's steps
         assert n == 10 and ms > 0
     for t, a in zip(together, alone):
-        a.run(40)
+        a.run(70)
         np.testing.assert_array_equal(t.populations(), a.populations())
 
 
