@@ -853,7 +853,10 @@ __global__ void __launch_bounds__(FACTOR_THREADS, 65536 / (FACTOR_THREADS * 128)
 // fit (at most stage_cap), the lanes of warp 0 bring them into shared memory
 // with bulk copies (one 6-KB block each, completion on an mbarrier) before
 // the level's arithmetic, so that the level costs one memory round trip
-// instead of one per dependent load. Rows of a block are GW = 96 words apart,
+// instead of one per dependent load. The levels above the first usually fit
+// together (31 blocks for 1024 markers): they then come in one round trip and
+// serve both sweeps, so that the whole solve stages three times (level 1,
+// the levels above it, level 1 again) instead of twice per level. Rows of a block are GW = 96 words apart,
 // all on one bank: the backward sweep, which reads one row per lane pair,
 // walks the columns in a rotated order (lane row i starts at column i) so
 // that the 16 rows read in one step fall on distinct banks. Also writes the force row's header and reports the
@@ -916,34 +919,79 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 1024 / SOLVE_THREADS) ib_solve(
     }
     const double *Gf = a.gf;
     uint32_t parity = 0;
-    // factor blocks of the odd blocks of level st: staged (returns the base
-    // of block o at index (o/st - 1)/2), or read from global memory
-    auto stage_level = [&](int st) -> bool {
-        const int nodd = (nb - st + 2 * st - 1) / (2 * st);
-        if (nodd > scap) return false;
-        __syncthreads();   // previous readers of the stage buffer are done
-        if (warp == 0) {
-            constexpr uint32_t kBlockBytes = sizeof(double) * BS * GW;
-            if (lane == 0) mbar_expect_tx(bar, kBlockBytes * (uint32_t)nodd);
-            __syncwarp();
-            fence_proxy_async();
-            for (int m = lane; m < nodd; m += 32)
-                bulk_g2s(stage_buf + m * BS * GW, Gf + (long long)st * (2 * m + 1) * BS * GW, kBlockBytes, bar);
-        }
-        // bounded wait: copies that never land are reported, not waited on forever
+    constexpr uint32_t kBlockBytes = sizeof(double) * BS * GW;
+    auto nodd_of = [&](int st) { return (nb - st + 2 * st - 1) / (2 * st); };
+    // bounded wait for the staged copies: copies that never land are
+    // reported, not waited on forever
+    auto stage_wait = [&]() {
         int spins = 0;
         while (!mbar_try_wait(bar, parity)) {
             if (++spins > (1 << 22)) { timed_out = 1; break; }
         }
         parity ^= 1u;
         __syncthreads();   // every thread sees the same timed_out
+    };
+    // factor blocks of the odd blocks of level st: staged (returns the base
+    // of block o at index (o/st - 1)/2), or read from global memory
+    auto stage_level = [&](int st) -> bool {
+        const int nodd = nodd_of(st);
+        if (nodd > scap) return false;
+        __syncthreads();   // previous readers of the stage buffer are done
+        if (warp == 0) {
+            if (lane == 0) mbar_expect_tx(bar, kBlockBytes * (uint32_t)nodd);
+            __syncwarp();
+            fence_proxy_async();
+            for (int m = lane; m < nodd; m += 32)
+                bulk_g2s(stage_buf + m * BS * GW, Gf + (long long)st * (2 * m + 1) * BS * GW, kBlockBytes, bar);
+        }
+        stage_wait();
         return true;
+    };
+    // When the odd blocks of every level above the first fit in the stage
+    // buffer together, they are staged once, in one round trip, when the
+    // forward sweep reaches level 2, each level at its own base (upper_base),
+    // and stay there for the rest of the forward sweep and for the backward
+    // sweep down to level 2; only level 1 is staged twice (first and last).
+    int upper = 0;
+    for (int st = 2; st < nb; st <<= 1) upper += nodd_of(st);
+    const bool resident = nodd_of(1) <= scap && upper <= scap;
+    auto upper_base = [&](int st) {
+        int b = 0;
+        for (int s2 = 2; s2 < st; s2 <<= 1) b += nodd_of(s2);
+        return b;
+    };
+    auto stage_upper = [&]() {
+        __syncthreads();   // the first level's readers are done
+        if (warp == 0) {
+            if (lane == 0) mbar_expect_tx(bar, kBlockBytes * (uint32_t)upper);
+            __syncwarp();
+            fence_proxy_async();
+            int b = 0;
+            for (int st = 2; st < nb; st <<= 1) {
+                const int nodd = nodd_of(st);
+                for (int m = lane; m < nodd; m += 32)
+                    bulk_g2s(stage_buf + (b + m) * BS * GW, Gf + (long long)st * (2 * m + 1) * BS * GW, kBlockBytes,
+                             bar);
+                b += nodd;
+            }
+        }
+        stage_wait();
+    };
+    // the stage-buffer base (in blocks) of level st's odd blocks, staging
+    // them first where needed; -1: read them from global memory
+    auto level_base = [&](int st, bool forward) -> int {
+        if (resident && st >= 2) {
+            if (forward && st == 2) stage_upper();
+            return upper_base(st);
+        }
+        return stage_level(st) ? 0 : -1;
     };
     __syncthreads();
     const int i = lane >> 1, c = lane & 1;   // row of the block, right-hand side
     int levels = 0;
     for (int st = 1; st < nb; st <<= 1, ++levels) {
-        const bool staged = stage_level(st);
+        const int sbase = level_base(st, true);
+        const bool staged = sbase >= 0;
         if (timed_out) break;
         const int neven = (nb + 2 * st - 1) / (2 * st);
         // one even block e per warp: F_L(q) and F_U(p) from block bases that
@@ -968,8 +1016,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 1024 / SOLVE_THREADS) ib_solve(
         for (int m = warp; m < neven; m += nw) {
             const int e = 2 * st * m, o1 = e - st, o2 = e + st;
             const bool has_q = o2 < nb, has_p = m > 0;
-            if (staged)   // odd block st(2k+1) is staged at index k
-                fwd(stage_buf + m * BS * GW, stage_buf + (m - 1) * BS * GW, GW, e, has_q, has_p);
+            if (staged)   // odd block st(2k+1) is staged at index sbase + k
+                fwd(stage_buf + (sbase + m) * BS * GW, stage_buf + (sbase + m - 1) * BS * GW, GW, e, has_q, has_p);
             else
                 fwd(Gf + (long long)o2 * BS * GW, Gf + (long long)o1 * BS * GW, GW, e, has_q, has_p);
         }
@@ -987,7 +1035,8 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 1024 / SOLVE_THREADS) ib_solve(
         __syncthreads();
         for (int lv = levels - 1; lv >= 0; --lv) {
             const int st = 1 << lv;
-            const bool staged = stage_level(st);
+            const int sbase = level_base(st, false);
+            const bool staged = sbase >= 0;
             if (timed_out) break;
             const int nodd = (nb - st + 2 * st - 1) / (2 * st);
             auto bwd = [&](const double *G, int o) {
@@ -1012,7 +1061,7 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 1024 / SOLVE_THREADS) ib_solve(
             for (int m = warp; m < nodd; m += nw) {
                 const int o = st * (2 * m + 1);
                 if (staged)
-                    bwd(stage_buf + (m * BS + i) * GW, o);
+                    bwd(stage_buf + ((sbase + m) * BS + i) * GW, o);
                 else
                     bwd(Gf + ((long long)o * BS + i) * GW, o);
             }
