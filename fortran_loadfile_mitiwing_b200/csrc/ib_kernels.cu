@@ -1592,16 +1592,21 @@ IBArgs make_args(lbm_handle *h, const void *fin, int slot)
     a.st_tiles = (long long)h->patch_gx() * h->patch_gy() * (TILE_CAP + 1);
     a.tiles = h->d_tiles + slot * a.st_tiles;
     a.gf = h->d_gf + slot * h->gf_slot;
-    a.rhs = h->d_rhs; a.y = h->d_y;
+    // the step's own right-hand sides, solution, tile partials and residual
+    // slots: one set per step parity, so that the check of a step may run
+    // while the next step's flow chain fills the other set
+    const int par = h->n & 1;
+    const long long ns2 = 2ll * (h->nseg > 0 ? h->nseg : 1);
+    a.rhs = h->d_rhs + par * ns2; a.y = h->d_y + par * ns2;
     a.bD = h->d_bD; a.bL = h->d_bL;
     a.reach = h->d_reach; a.wmax = h->d_wmax;
     a.nsup = h->d_nsup + slot;
     a.ctile = h->d_ctile + slot * (a.st_tiles / (TILE_CAP + 1));
     a.patch_wmax = h->patch_wmax; a.patch_hmax = h->patch_hmax;
-    a.partial = h->d_partial; a.counter = h->d_counter;
+    a.partial = h->d_partial + par * (long long)h->part_stride; a.counter = h->d_counter;
     a.force_ring = h->d_ring; a.row_len = h->row_len;
     a.ring_row = 0; a.ring_rows = h->ring_cap;
-    a.status = h->d_status; a.solve_res = h->d_solve_res;
+    a.status = h->d_status; a.solve_res = h->d_solve_res + 2 * par;
     a.cur_step = h->n;
     a.fstep0 = 0; a.fcount = 0;
     a.check_res = 1;

@@ -253,6 +253,7 @@ int check_case(lbm_batch *b, lbm_handle *h)
     // the case's own queued work is done before the batch's streams use its buffers
     if (h->fstream) cudaStreamSynchronize(h->fstream);
     if (h->side) cudaStreamSynchronize(h->side);
+    if (h->cstream) cudaStreamSynchronize(h->cstream);
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) return handle_error(h, LBM_ERR_CUDA, "batch: sync");
     return LBM_OK;
 }
@@ -445,6 +446,7 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
         }
         if (h->fstream) cudaStreamSynchronize(h->fstream);
         if (h->side) cudaStreamSynchronize(h->side);
+        if (h->cstream) cudaStreamSynchronize(h->cstream);
         cudaStreamSynchronize(h->stream);
         int gx, gy;
         kf_tma_grid(h, &gx, &gy);

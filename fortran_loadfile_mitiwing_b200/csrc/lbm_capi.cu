@@ -116,6 +116,7 @@ void quiesce(lbm_handle *h)
 {
     if (h->fstream) cudaStreamSynchronize(h->fstream);
     if (h->side) cudaStreamSynchronize(h->side);
+    if (h->cstream) cudaStreamSynchronize(h->cstream);
     if (h->stream) cudaStreamSynchronize(h->stream);
 }
 
@@ -165,6 +166,7 @@ void free_ib(lbm_handle *h)
 {
     if (h->fstream) cudaStreamSynchronize(h->fstream);
     if (h->side) cudaStreamSynchronize(h->side);
+    if (h->cstream) cudaStreamSynchronize(h->cstream);
     if (h->stream) cudaStreamSynchronize(h->stream);
     h->ib_ready = 0;
     h->batch_in_half[0] = h->batch_in_half[1] = -1;
@@ -220,8 +222,9 @@ int ensure_ib(lbm_handle *h)
     const int ns = std::max(1, h->nseg);
     const size_t S = (size_t)h->nslots, K = (size_t)h->fbatch;
     CK(dmalloc(h, &h->d_mk, S * sizeof(Marker) * ns), "alloc markers");
-    CK(dmalloc(h, &h->d_rhs, sizeof(double) * 2 * ns), "alloc rhs");
-    CK(dmalloc(h, &h->d_y, sizeof(double) * 2 * ns), "alloc y");
+    // right-hand sides and solution: one pair per step parity
+    CK(dmalloc(h, &h->d_rhs, sizeof(double) * 2 * 2 * ns), "alloc rhs");
+    CK(dmalloc(h, &h->d_y, sizeof(double) * 2 * 2 * ns), "alloc y");
     CK(dmalloc(h, &h->d_B, S * sizeof(double) * (size_t)ns * ns), "alloc B");
     ib_factor_scratch(ns, &h->work_blocks, &h->gf_slot);
     CK(dmalloc(h, &h->d_bD, K * sizeof(double) * h->work_blocks), "alloc block D");
@@ -233,8 +236,10 @@ int ensure_ib(lbm_handle *h)
     CK(cudaMemsetAsync(h->d_fstatus, 0, S * sizeof(unsigned), h->stream), "clear factor status");
     const int nblk = h->patch_gx() * h->patch_gy();
     // partials of the spread (per patch tile) and of the residual check (per 8 markers)
+    // (one set per step parity)
     const size_t npart = std::max((size_t)ib_partials_per_block() * nblk, 2 * (size_t)((ns + 7) / 8));
-    CK(dmalloc(h, &h->d_partial, sizeof(double) * npart), "alloc partials");
+    h->part_stride = npart;
+    CK(dmalloc(h, &h->d_partial, sizeof(double) * 2 * npart), "alloc partials");
     h->tiles_slot = (size_t)ib_tile_ints() * nblk;
     CK(dmalloc(h, &h->d_tiles, S * sizeof(int) * h->tiles_slot), "alloc tile lists");
     CK(cudaMemsetAsync(h->d_tiles, 0, S * sizeof(int) * h->tiles_slot, h->stream), "clear tile lists");
@@ -453,13 +458,20 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
             if (h->batch_in_half[half] != b && (rc = factor_batch(b))) return rc;
             CK(cudaStreamWaitEvent(h->side, h->ev_inner, 0), "wait");
             CK(cudaStreamWaitEvent(h->side, h->ev_batch[half], 0), "wait");
+            // this step's buffers of its parity were last read by the check
+            // two steps back
+            CK(cudaStreamWaitEvent(h->side, h->ev_check[h->n & 1], 0), "wait");
             if (e) CK(cudaEventRecord(h->ev_side[2 * slot], h->side), "event");
             cudaEvent_t ei = h->after_interp ? h->ev_interp : nullptr;
             if (launch_flow(h, fin, fout, fields, h->n, slot, q, h->side, ei)) return cuda_err(h, cudaGetLastError(), "launch ib");
             if (e) CK(cudaEventRecord(h->ev_side[2 * slot + 1], h->side), "event");
             CK(cudaEventRecord(h->ev_ib, h->side), "event");
-            if (launch_check(h, q, slot, check_res, h->side)) return cuda_err(h, cudaGetLastError(), "launch check");
-            CK(cudaEventRecord(h->ev_free[half], h->side), "event");
+            // the force row and the residual check on their own stream; the
+            // slot half is free for the next factorization after them
+            CK(cudaStreamWaitEvent(h->cstream, h->ev_ib, 0), "wait");
+            if (launch_check(h, q, slot, check_res, h->cstream)) return cuda_err(h, cudaGetLastError(), "launch check");
+            CK(cudaEventRecord(h->ev_check[h->n & 1], h->cstream), "event");
+            CK(cudaEventRecord(h->ev_free[half], h->cstream), "event");
             // the next batch's factorization, overlapping this batch's steps
             if ((b + 1) * K <= last_step && h->batch_in_half[half ^ 1] != b + 1 && (rc = factor_batch(b + 1))) return rc;
             CK(cudaStreamWaitEvent(h->stream, h->ev_batch[half], 0), "wait");   // the step's correction tiles
@@ -491,9 +503,11 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
         done++;
         pending++;
         if (pending == h->ring_cap || s == nsteps - 1) {
-            if (split) {   // force rows and residual checks run on the side stream after the update
+            if (split) {   // force rows and residual checks run on the check stream after the update
                 CK(cudaEventRecord(h->ev_ib, h->side), "event");
                 CK(cudaStreamWaitEvent(h->stream, h->ev_ib, 0), "wait");
+                CK(cudaEventRecord(h->ev_cjoin, h->cstream), "event");
+                CK(cudaStreamWaitEvent(h->stream, h->ev_cjoin, 0), "wait");
             }
             // the span ends with the chunk's last step; the row copy and the
             // mass check after it are per-call work, not per-step work
@@ -517,6 +531,8 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
         if (split) {
             CK(cudaEventRecord(h->ev_ib, h->side), "event");
             CK(cudaStreamWaitEvent(h->stream, h->ev_ib, 0), "wait");
+            CK(cudaEventRecord(h->ev_cjoin, h->cstream), "event");
+            CK(cudaStreamWaitEvent(h->stream, h->ev_cjoin, 0), "wait");
         }
         if (h->timing == LBM_TIMING_SPAN) CK(cudaEventRecord(h->ev[4 * (pending - 1) + 3], h->stream), "event");
         if (rows_out)
@@ -733,6 +749,10 @@ int lbm_create(const lbm_params *p, lbm_t **out)
     if ((e = cudaEventCreateWithFlags(&h->ev_interp, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
     if (const char *ev = getenv("LBM_AFTER_INTERP")) h->after_interp = atoi(ev) != 0;
     if ((e = cudaStreamCreateWithFlags(&h->fstream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "factor stream");
+    if ((e = cudaStreamCreateWithPriority(&h->cstream, cudaStreamNonBlocking, prio_high)) != cudaSuccess)
+        return fail(e, "check stream");
+    for (cudaEvent_t *ev : {&h->ev_check[0], &h->ev_check[1], &h->ev_cjoin})
+        if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
     for (int q = 0; q < 2; ++q) {
         if ((e = cudaEventCreateWithFlags(&h->ev_batch[q], cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
         if ((e = cudaEventCreateWithFlags(&h->ev_free[q], cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
@@ -763,7 +783,8 @@ int lbm_create(const lbm_params *p, lbm_t **out)
     if ((e = dmalloc(h, &h->d_mass, sizeof(double) * mass_slots())) != cudaSuccess) return fail(e, "alloc mass");
     if ((e = dmalloc(h, &h->d_mcount, sizeof(unsigned))) != cudaSuccess) return fail(e, "alloc mass counter");
 
-    if ((e = dmalloc(h, &h->d_solve_res, 2 * sizeof(double))) != cudaSuccess) return fail(e, "alloc res");
+    // solve residual and half-bandwidth, per step parity
+    if ((e = dmalloc(h, &h->d_solve_res, 2 * 2 * sizeof(double))) != cudaSuccess) return fail(e, "alloc res");
     if ((e = dmalloc(h, &h->d_ring, sizeof(double) * h->row_len * (size_t)h->ring_cap)) != cudaSuccess)
         return fail(e, "alloc ring");
     if (h->npts > 0) {
@@ -784,6 +805,7 @@ int lbm_destroy(lbm_t *h)
     // no queued work of the handle may still use what is freed below
     if (h->fstream) cudaStreamSynchronize(h->fstream);
     if (h->side) cudaStreamSynchronize(h->side);
+    if (h->cstream) cudaStreamSynchronize(h->cstream);
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (int b = 0; b < 2; ++b) { free_dev(h->falloc[b]); h->fbuf[b] = nullptr; free_dev(h->d_fields[b]); }
     free_dev(h->edge_c);
@@ -795,6 +817,7 @@ int lbm_destroy(lbm_t *h)
 
     free_devp(h->d_stage);
     if (h->side) cudaStreamSynchronize(h->side);
+    if (h->cstream) cudaStreamSynchronize(h->cstream);
     if (h->fstream) cudaStreamSynchronize(h->fstream);
     for (auto &e : h->ev) cudaEventDestroy(e);
     for (auto &e : h->ev_side) cudaEventDestroy(e);
@@ -805,6 +828,9 @@ int lbm_destroy(lbm_t *h)
         if (h->ev_batch[q]) cudaEventDestroy(h->ev_batch[q]);
         if (h->ev_free[q]) cudaEventDestroy(h->ev_free[q]);
     }
+    for (cudaEvent_t ev : {h->ev_check[0], h->ev_check[1], h->ev_cjoin})
+        if (ev) cudaEventDestroy(ev);
+    if (h->cstream) cudaStreamDestroy(h->cstream);
     if (h->fstream) cudaStreamDestroy(h->fstream);
     if (h->side) cudaStreamDestroy(h->side);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -1037,7 +1063,8 @@ int lbm_get_markers(lbm_t *h, double *xb2, double *yb2, double *solve_residual, 
     const Marker *last = h->d_mk + (size_t)((h->n - 1) % h->nslots) * h->nseg;   // slot of the last step
     CK(cudaMemcpyAsync(mk.data(), last, sizeof(Marker) * h->nseg, cudaMemcpyDeviceToHost, h->stream), "copy markers");
     double res[2] = {0, 0};
-    CK(cudaMemcpyAsync(res, h->d_solve_res, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "copy res");
+    const double *last_res = h->d_solve_res + 2 * ((h->n - 1) & 1);   // parity of the last step
+    CK(cudaMemcpyAsync(res, last_res, 2 * sizeof(double), cudaMemcpyDeviceToHost, h->stream), "copy res");
     CK(cudaStreamSynchronize(h->stream), "sync markers");
     for (int k = 0; k < h->nseg; ++k) {
         if (xb2) xb2[k] = mk[k].xm;

@@ -177,6 +177,14 @@ struct lbm_handle {
     // that half by a step's flow chain
     cudaStream_t fstream = nullptr;
     cudaEvent_t ev_batch[2] = {nullptr, nullptr}, ev_free[2] = {nullptr, nullptr};
+    // the step's force row and solve-residual check (with the split): their
+    // own stream, after the step's correction tiles, so that the next step's
+    // flow chain need not wait for them. What they read is kept per step
+    // parity (right-hand sides, solution, tile partials, residual slots), and
+    // ev_check[p] marks the check of the last step of parity p done.
+    cudaStream_t cstream = nullptr;
+    cudaEvent_t ev_check[2] = {nullptr, nullptr}, ev_cjoin = nullptr;
+    size_t part_stride = 0;   // doubles of one parity's tile partials
     double *d_partial = nullptr;
     unsigned *d_counter = nullptr;
     double *d_ring = nullptr;

@@ -578,6 +578,7 @@ int lbm_save_checkpoint(lbm_t *h, const char *path)
     if (!h->inited) return io_err(h, LBM_ERR_STATE, "save_checkpoint: not initialised");
     if (h->fstream) cudaStreamSynchronize(h->fstream);
     if (h->side) cudaStreamSynchronize(h->side);
+    if (h->cstream) cudaStreamSynchronize(h->cstream);
     CkptHeader hd;
     std::vector<unsigned char> blob;
     int rc = gather_state(h, hd, blob);
@@ -602,6 +603,7 @@ int lbm_load_checkpoint(lbm_t *h, const char *path)
     }
     if (h->fstream) cudaStreamSynchronize(h->fstream);
     if (h->side) cudaStreamSynchronize(h->side);
+    if (h->cstream) cudaStreamSynchronize(h->cstream);
     cudaStreamSynchronize(h->stream);
     const unsigned char *q = blob.data();
     h->cur = 0;

@@ -92,7 +92,7 @@ def estimate_device_bytes(case):
     total = 2 * elem * (9 * pitch * ny + 2 * _FPAD)          # populations, two buffers
     total += 2 * 3 * cs * nx * ny                              # fields, two slots
     total += cs * (6 * ny + 36)                                # edge values
-    total += 4 + 4 + _NSLOT_MAX * _PATCHINFO_BYTES + 8 * 2 * 296 + 16 + 8 * row_len * _RING
+    total += 4 + 4 + _NSLOT_MAX * _PATCHINFO_BYTES + 8 * 2 * 296 + 2 * 16 + 8 * row_len * _RING
     total += 8 * (_MASS_BLOCKS + 1) + 4                        # mass check: partials and sum, counter
     if nwing:
         dt = p.scale * p.uu
@@ -103,9 +103,10 @@ def estimate_device_bytes(case):
         nb = (ns + _BS - 1) // _BS
         pw, ph = patch_extent(case)
         nblk = max(1, (pw + 15) // 16) * max(1, (ph + 15) // 16)
-        total += S * _MARKER_BYTES * ns + 2 * 8 * 2 * ns + S * 8 * ns * ns
+        # right-hand sides, solution and tile partials: one set per step parity
+        total += S * _MARKER_BYTES * ns + 2 * 2 * 8 * 2 * ns + S * 8 * ns * ns
         total += 2 * K * 8 * nb * _BS * _BS + S * 8 * nb * _BS * _GW + S * 2 * 4 + S * 4
-        total += 8 * max(_NPART * nblk, 2 * ((ns + 7) // 8))
+        total += 2 * 8 * max(_NPART * nblk, 2 * ((ns + 7) // 8))
         total += S * 4 * _TILE_INTS * nblk + S * 4 + S * 4 * nblk
         total += S * 4 * ns + S * 8 * ns + 8 + K * 4
     return int(total)
