@@ -53,6 +53,13 @@ struct lbm_batch {
     std::vector<lbm_handle *> cases;
     int prec = -1, fbatch = 4, nslots = 8, dev = 0;
     cudaStream_t main = nullptr, side = nullptr, fstream = nullptr;
+    // the steps' force rows and residual checks run on their own stream,
+    // after the step's correction tiles, so that the next step's flow chains
+    // need not wait for them (the cases keep what they read per step parity;
+    // ev_bcheck[p] marks the checks of the last step of parity p done). ev_side
+    // marks a step's flow chains and checks done.
+    cudaStream_t cstream = nullptr;
+    cudaEvent_t ev_bcheck[2] = {nullptr, nullptr}, ev_cpre = nullptr;
     cudaEvent_t ev_ib = nullptr, ev_done = nullptr, ev_fready = nullptr, ev_side = nullptr;
     // device time of the last run's steps (lbm_batch_get_timing)
     cudaEvent_t ev_t0 = nullptr, ev_t1 = nullptr;
@@ -94,7 +101,7 @@ struct lbm_batch {
     // events of the captured stream code (never waited on outside a capture):
     // fork, upload, joins, and per step the flow chain's points, then one per
     // factorization launch of the segment
-    cudaEvent_t ev_cap[9 + 2 * kGraphSteps] = {};
+    cudaEvent_t ev_cap[9 + 2 * kGraphSteps + 3] = {};
     cudaEvent_t ev_gpre = nullptr;   // the factor stream's work before a graph launch
     struct GraphEntry {
         std::vector<long long> sig;
@@ -125,6 +132,7 @@ void sync_streams(lbm_batch *b)
     if (b->main) cudaStreamSynchronize(b->main);
     if (b->side) cudaStreamSynchronize(b->side);
     if (b->fstream) cudaStreamSynchronize(b->fstream);
+    if (b->cstream) cudaStreamSynchronize(b->cstream);
 }
 
 void free_arrays(lbm_batch *b)
@@ -183,13 +191,14 @@ void free_batch(lbm_batch *b)
     for (int r = 0; r < kGroupRing; ++r)
         if (b->ev_group[r]) cudaEventDestroy(b->ev_group[r]);
     for (cudaEvent_t e : {b->ev_ib, b->ev_done, b->ev_fready, b->ev_side, b->ev_t0, b->ev_t1, b->ev_interp,
-                          b->ev_gdone[0], b->ev_gdone[1], b->ev_gpre})
+                          b->ev_gdone[0], b->ev_gdone[1], b->ev_gpre, b->ev_bcheck[0], b->ev_bcheck[1], b->ev_cpre})
         if (e) cudaEventDestroy(e);
     for (cudaEvent_t e : b->ev_cap)
         if (e) cudaEventDestroy(e);
     if (b->main) cudaStreamDestroy(b->main);
     if (b->side) cudaStreamDestroy(b->side);
     if (b->fstream) cudaStreamDestroy(b->fstream);
+    if (b->cstream) cudaStreamDestroy(b->cstream);
 }
 
 // argument arrays for `ncase` cases and `ntab` case-table entries (grown, never shrunk)
@@ -311,12 +320,15 @@ int lbm_batch_create(lbm_t *const *cases, int count, lbm_batch_t **out)
     if ((e = cudaStreamCreateWithPriority(&b->side, cudaStreamNonBlocking, prio_high)) != cudaSuccess)
         return fail(e, "stream");
     if ((e = cudaStreamCreateWithFlags(&b->fstream, cudaStreamNonBlocking)) != cudaSuccess) return fail(e, "stream");
+    if ((e = cudaStreamCreateWithPriority(&b->cstream, cudaStreamNonBlocking, prio_high)) != cudaSuccess)
+        return fail(e, "stream");
     for (cudaEvent_t *ev : {&b->ev_t0, &b->ev_t1})
         if ((e = cudaEventCreate(ev)) != cudaSuccess) return fail(e, "event");
     if (const char *ev = getenv("LBM_AFTER_INTERP")) b->after_interp = atoi(ev) != 0;
     if (const char *ev = getenv("LBM_BATCH_GRAPHS")) b->graphs = atoi(ev) != 0;
     for (cudaEvent_t *ev : {&b->ev_interp, &b->ev_ib, &b->ev_done, &b->ev_fready, &b->ev_side, &b->ev_tup[0], &b->ev_tup[1],
-                            &b->ev_tuse[0], &b->ev_tuse[1], &b->ev_gdone[0], &b->ev_gdone[1], &b->ev_gpre})
+                            &b->ev_tuse[0], &b->ev_tuse[1], &b->ev_gdone[0], &b->ev_gdone[1], &b->ev_gpre,
+                            &b->ev_bcheck[0], &b->ev_bcheck[1], &b->ev_cpre})
         if ((e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
     for (cudaEvent_t &ev : b->ev_cap)
         if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return fail(e, "event");
@@ -629,11 +641,14 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
         // below, with every dependency inside the segment
         auto emit = [&]() -> int {
             cudaEvent_t *E = b->ev_cap;
+            // the checks of steps t (parity t & 1) and the check stream's join
+            cudaEvent_t *EC = b->ev_cap + 9 + 2 * kGraphSteps;
             BCK(cudaEventRecord(E[0], b->side), "event");
             BCK(cudaMemcpyAsync(ds, hs, used, cudaMemcpyHostToDevice, b->side), "upload");
             BCK(cudaEventRecord(E[1], b->side), "event");
             BCK(cudaStreamWaitEvent(b->main, E[1], 0), "wait");
             BCK(cudaStreamWaitEvent(b->fstream, E[1], 0), "wait");
+            BCK(cudaStreamWaitEvent(b->cstream, E[1], 0), "wait");
             cudaEvent_t ei = b->after_interp ? E[8] : nullptr;
             std::vector<lbm_handle *> grp;
             auto factor = [&](int gi, bool after_side) -> int {
@@ -652,13 +667,19 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
                 if (t > 0) BCK(cudaStreamWaitEvent(b->side, E[7], 0), "wait");
                 for (int gi : p.waits) BCK(cudaStreamWaitEvent(b->side, E[9 + gi], 0), "wait");
                 BCK(cudaEventRecord(E[4], b->side), "event");
+                // the checks two steps back (those before the segment are done
+                // when it starts)
+                if (t >= 2) BCK(cudaStreamWaitEvent(b->side, EC[t & 1], 0), "wait");
                 const char *sa = ds + (size_t)t * na * b->ib_sz;
                 const char *ka = ds + off_k + (size_t)t * na * b->kf_sz;
                 if (launch_flow_batch(act.data(), na, sa, ka, 0, 0, false, b->side, ei))
                     return berr(b, LBM_ERR_CUDA, "batch: launch flow");
                 BCK(cudaEventRecord(E[5], b->side), "event");
-                if (launch_check_batch(act.data(), na, sa, 0, b->side)) return berr(b, LBM_ERR_CUDA, "batch: launch check");
-                BCK(cudaEventRecord(E[6], b->side), "event");
+                BCK(cudaStreamWaitEvent(b->cstream, E[5], 0), "wait");
+                if (launch_check_batch(act.data(), na, sa, 0, b->cstream))
+                    return berr(b, LBM_ERR_CUDA, "batch: launch check");
+                BCK(cudaEventRecord(EC[t & 1], b->cstream), "event");
+                BCK(cudaEventRecord(E[6], b->cstream), "event");   // flow chains and checks of step t
                 if (p.next >= 0 && (erc = factor(p.next, true))) return erc;
                 BCK(cudaStreamWaitEvent(b->main, E[4], 0), "wait");
                 if (ei) BCK(cudaStreamWaitEvent(b->main, ei, 0), "wait");   // the solves start first
@@ -670,14 +691,18 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
             }
             BCK(cudaEventRecord(E[2], b->main), "event");
             BCK(cudaEventRecord(E[3], b->fstream), "event");
+            BCK(cudaEventRecord(EC[2], b->cstream), "event");
             BCK(cudaStreamWaitEvent(b->side, E[2], 0), "wait");
             BCK(cudaStreamWaitEvent(b->side, E[3], 0), "wait");
+            BCK(cudaStreamWaitEvent(b->side, EC[2], 0), "wait");
             return LBM_OK;
         };
         // the graph starts after every stream's earlier work
         BCK(cudaEventRecord(b->ev_gpre, b->fstream), "event");
+        BCK(cudaEventRecord(b->ev_cpre, b->cstream), "event");
         BCK(cudaStreamWaitEvent(b->side, b->ev_done, 0), "wait");
         BCK(cudaStreamWaitEvent(b->side, b->ev_gpre, 0), "wait");
+        BCK(cudaStreamWaitEvent(b->side, b->ev_cpre, 0), "wait");
         lbm_batch::GraphEntry *ge = nullptr;
         for (auto &e : b->gcache)
             if (e.sig == sig) {
@@ -726,9 +751,12 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
         BCK(cudaEventRecord(b->ev_done, b->side), "event");
         BCK(cudaEventRecord(b->ev_side, b->side), "event");
         BCK(cudaEventRecord(b->ev_tuse[tcur], b->side), "event");
+        BCK(cudaEventRecord(b->ev_bcheck[0], b->side), "event");
+        BCK(cudaEventRecord(b->ev_bcheck[1], b->side), "event");
         for (const GroupPlan &g : groups) BCK(cudaEventRecord(b->ev_group[g.seq % kGroupRing], b->side), "event");
         BCK(cudaStreamWaitEvent(b->main, b->ev_done, 0), "wait");
         BCK(cudaStreamWaitEvent(b->fstream, b->ev_side, 0), "wait");
+        BCK(cudaStreamWaitEvent(b->cstream, b->ev_side, 0), "wait");
         return LBM_OK;
     };
     BCK(cudaEventRecord(b->ev_done, b->main), "event");
@@ -839,6 +867,9 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
             }
         }
         BCK(cudaEventRecord(b->ev_fready, b->side), "event");   // uploads done, factorizations ready
+        // the cases' buffers of this step's parity were last read by the
+        // checks two steps back
+        BCK(cudaStreamWaitEvent(b->side, b->ev_bcheck[step & 1], 0), "wait");
         cudaEvent_t ei = b->after_interp ? b->ev_interp : nullptr;
         if (launch_flow_batch(act.data(), (int)act.size(), b->d_sargs[buf], b->d_kargs[buf], 0, pending, fields,
                               b->side, ei)) {
@@ -846,11 +877,13 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
             break;
         }
         BCK(cudaEventRecord(b->ev_ib, b->side), "event");
-        if (launch_check_batch(act.data(), (int)act.size(), b->d_sargs[buf], pending, b->side)) {
+        BCK(cudaStreamWaitEvent(b->cstream, b->ev_ib, 0), "wait");
+        if (launch_check_batch(act.data(), (int)act.size(), b->d_sargs[buf], pending, b->cstream)) {
             rc = berr(b, LBM_ERR_CUDA, "batch: launch check");
             break;
         }
-        BCK(cudaEventRecord(b->ev_side, b->side), "event");
+        BCK(cudaEventRecord(b->ev_bcheck[step & 1], b->cstream), "event");
+        BCK(cudaEventRecord(b->ev_side, b->cstream), "event");
         // the next factorization batches, overlapping these steps
         if ((rc = factor_needed(act, act_idx, true))) break;
         // main stream: every case's lattice nodes but its correction tiles
