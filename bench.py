@@ -358,7 +358,8 @@ def run_e2e(args, lib):
     return {"value": nn * k / el / 1e6, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
             "stages_ms": stages,
             "note": "wall clock around the C-ABI calls (create, boundary, motion table, init, run, fields); "
-                    "set-up upload and final fields amortised over the steps"}
+                    "set-up upload and final fields amortised over the steps; device memory from the library's "
+                    "stream-ordered pool, which the bench's earlier handles in this process have filled"}
 
 
 def run_storage_variants(args, lib, exclude, steps=1000, kernel_steps=300):

@@ -67,19 +67,68 @@ double feq(double rh, double u1, double v1, int k)
 std::mutex g_alloc_mu;
 std::unordered_map<void *, std::pair<lbm_handle *, size_t>> g_allocs;
 
+// The handles' device memory comes from one stream-ordered memory pool per
+// device, owned by the library, that keeps what freed handles return
+// (release threshold: never) for the next allocations: a handle created
+// after another was destroyed, as a sweep or a serving loop does many times,
+// reuses memory that is already mapped instead of mapping it again, and a
+// free does not synchronise the device as cudaFree does. The pool holds the
+// process's peak of live handle memory until the process exits.
+cudaMemPool_t handle_pool(int dev)
+{
+    static std::mutex mu;
+    static std::unordered_map<int, cudaMemPool_t> pools;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = pools.find(dev);
+    if (it != pools.end()) return it->second;
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool = nullptr;
+    if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+        cudaGetLastError();
+        pool = nullptr;   // plain cudaMalloc / cudaFree then
+    } else {
+        unsigned long long keep = ~0ull;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    pools[dev] = pool;
+    return pool;
+}
+
+// allocations from the pool, by address (freed back to it)
+std::unordered_map<void *, bool> g_pooled;
+
 // Every allocation is zero-filled on the handle's stream, ahead of all work
 // that uses it (the other streams are ordered after the main stream's
-// position by events), so that no kernel can see data a freed allocation of
-// an earlier handle left in the same memory.
+// position by events or a synchronisation), so that no kernel can see data a
+// freed allocation of an earlier handle left in the same memory.
 template <typename P> cudaError_t dmalloc(lbm_handle *h, P **p, size_t bytes)
 {
     void *q = nullptr;
-    cudaError_t e = cudaMalloc(&q, bytes);
+    cudaMemPool_t pool = h->stream ? handle_pool(h->dev) : nullptr;
+    cudaError_t e = cudaErrorMemoryAllocation;
+    if (pool && (e = cudaMallocFromPoolAsync(&q, bytes, pool, h->stream)) != cudaSuccess) {
+        // a pool unusable here (a context other than the one it was made in,
+        // or one reset since): a plain allocation
+        cudaGetLastError();
+        pool = nullptr;
+    }
+    if (!pool) e = cudaMalloc(&q, bytes);
     if (e != cudaSuccess) return e;
     e = h->stream ? cudaMemsetAsync(q, 0, bytes, h->stream) : cudaMemset(q, 0, bytes);
     if (e != cudaSuccess) {
-        cudaFree(q);
+        if (pool)
+            cudaFreeAsync(q, h->stream);
+        else
+            cudaFree(q);
         return e;
+    }
+    if (pool) {
+        std::lock_guard<std::mutex> lock(g_alloc_mu);
+        g_pooled[q] = true;
     }
     *p = (P *)q;
     std::lock_guard<std::mutex> lock(g_alloc_mu);
@@ -88,18 +137,32 @@ template <typename P> cudaError_t dmalloc(lbm_handle *h, P **p, size_t bytes)
     return e;
 }
 
+// Callers first synchronise the streams of the handle that owns p (no queued
+// work may still use it); a pooled allocation goes back to the pool on the
+// owner's main stream, idle by then.
 void free_dev(void *&p)
 {
     if (p) {
+        bool pooled = false;
+        cudaStream_t st = nullptr;
         {
             std::lock_guard<std::mutex> lock(g_alloc_mu);
             auto it = g_allocs.find(p);
             if (it != g_allocs.end()) {
                 it->second.first->dev_bytes -= (long long)it->second.second;
+                st = it->second.first->stream;
                 g_allocs.erase(it);
             }
+            auto jt = g_pooled.find(p);
+            if (jt != g_pooled.end()) {
+                pooled = true;
+                g_pooled.erase(jt);
+            }
         }
-        cudaFree(p);
+        if (pooled)
+            cudaFreeAsync(p, st);
+        else
+            cudaFree(p);
     }
     p = nullptr;
 }
