@@ -14,6 +14,7 @@
 // it in turn under a mutex.
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <condition_variable>
 #include <cstring>
 #include <functional>
@@ -53,6 +54,7 @@ class WorkPool {
             std::lock_guard<std::mutex> lk(mu_);
             cur_ = &job;
             ++gen_;
+            posted_.store(gen_, std::memory_order_release);
         }
         cv_.notify_all();
         work(job);
@@ -91,6 +93,19 @@ class WorkPool {
         long long seen = 0;
         for (;;) {
             Job *j;
+            // A transfer posts one job per staging chunk, a fraction of a
+            // millisecond apart: a worker that sleeps on the condition
+            // variable between them wakes too late to take a part, and the
+            // calling thread copies most of the chunk alone (measured: a
+            // 67 MB upload 3-4x slower than with workers that stay awake).
+            // So a worker first watches for the next job for up to
+            // kSpinMicros, then sleeps.
+            const auto t0 = std::chrono::steady_clock::now();
+            for (int i = 0; posted_.load(std::memory_order_acquire) == seen; ++i) {
+                if ((i & 255) == 255 &&
+                    std::chrono::steady_clock::now() - t0 > std::chrono::microseconds(kSpinMicros))
+                    break;
+            }
             {
                 std::unique_lock<std::mutex> lk(mu_);
                 cv_.wait(lk, [&] { return gen_ != seen && cur_ != nullptr; });
@@ -103,7 +118,9 @@ class WorkPool {
             if (--j->users == 0 && j->pending == 0) done_cv_.notify_all();
         }
     }
+    static constexpr int kSpinMicros = 300;
     int workers_ = 0;
+    std::atomic<long long> posted_{0};   // gen_ as last posted, read without the lock
     std::mutex call_mu_, mu_;
     std::condition_variable cv_, done_cv_;
     Job *cur_ = nullptr;
