@@ -101,10 +101,15 @@ typedef struct lbm_handle lbm_t;
 LBM_API int lbm_default_params(lbm_params *p);
 
 /* ini_mesh (ini_mesh.f90:1-81): validates the parameters and allocates the
- * device state (two population buffers, IB scratch, step table). */
+ * device state (two population buffers, IB scratch, step table). The device
+ * memory comes from a stream-ordered pool that the library keeps per device
+ * for the life of the process: memory a destroyed handle returned is reused
+ * by the next handles without mapping it again. */
 LBM_API int lbm_create(const lbm_params *p, lbm_t **out);
 
-/* frees everything the handle owns (the reference frees nothing) */
+/* frees everything the handle owns (the reference frees nothing); its
+ * device memory goes back to the library's pool (no device-wide
+ * synchronisation) */
 LBM_API int lbm_destroy(lbm_t *h);
 
 /* read_boundary (airfoil.f90:207-242) for one wing from memory: npts
