@@ -265,19 +265,37 @@ __global__ void __launch_bounds__(256) ib_interp(const IBArgs a0, const IBArgs *
     }
     const int k = blockIdx.x * 8 + warp;
     if (k >= a.nseg) return;
-    const Marker m = a.mk[k];
-    const bool ok = box_in_bounds(m.i1, m.i2, m.j1, m.j2, a.nx, a.ny);
+    // the marker's box and kernel values are read where they lie (a local
+    // copy of the struct, indexed by node, would live on the stack)
+    const Marker *mp = a.mk + k;
+    const int i1 = mp->i1, i2 = mp->i2, j1 = mp->j1, j2 = mp->j2;
+    const bool ok = box_in_bounds(i1, i2, j1, j2, a.nx, a.ny);
     if (!ok && lane == 0) atomicOr(a.status, LBM_ST_INDEX_INTERP);
-    const int nbx = ok ? m.i2 - m.i1 + 1 : 0, nby = ok ? m.j2 - m.j1 + 1 : 0;
+    const int nbx = ok ? i2 - i1 + 1 : 0, nby = ok ? j2 - j1 + 1 : 0;
     const int nn = nbx > 0 && nby > 0 ? nbx * nby : 0;
     double su = 0.0, sv = 0.0;
-    for (int t = lane; t < nn; t += 32) {
-        const int ii = t % nbx, jj = t / nbx;
-        double rho, u, v;
-        node_moments<T>(a, m.i1 + ii, m.j1 + jj, rho, u, v);
-        const double wgt = m.phx[ii] * m.phy[jj];   // X1(k,i) = kernel1*kernel2 (:1602)
-        su += wgt * u;
-        sv += wgt * v;
+    if (nn > 0) {
+        // at most LBM_BOX^2 = 36 nodes: lane t takes nodes t and t + 32, and
+        // both nodes' populations are loaded before either is summed (a lane
+        // without a second node loads its first again and weighs it 0); the
+        // sums are the loop's, node t then node t + 32, each a fused
+        // multiply-add onto the running sum
+        const bool h0 = lane < nn, h1 = lane + 32 < nn;
+        const int t0 = h0 ? lane : 0, t1 = h1 ? lane + 32 : t0;
+        const int ii0 = t0 % nbx, jj0 = t0 / nbx, ii1 = t1 % nbx, jj1 = t1 / nbx;
+        double rho0, u0, v0, rho1, u1, v1;
+        node_moments<T>(a, i1 + ii0, j1 + jj0, rho0, u0, v0);
+        node_moments<T>(a, i1 + ii1, j1 + jj1, rho1, u1, v1);
+        const double w0 = mp->phx[ii0] * mp->phy[jj0];   // X1(k,i) = kernel1*kernel2 (:1602)
+        const double w1 = mp->phx[ii1] * mp->phy[jj1];
+        if (h0) {
+            su = fma(w0, u0, su);
+            sv = fma(w0, v0, sv);
+        }
+        if (h1) {
+            su = fma(w1, u1, su);
+            sv = fma(w1, v1, sv);
+        }
     }
 #pragma unroll
     for (int off = 16; off; off >>= 1) {
@@ -285,8 +303,8 @@ __global__ void __launch_bounds__(256) ib_interp(const IBArgs a0, const IBArgs *
         sv += __shfl_down_sync(0xffffffffu, sv, off);
     }
     if (lane == 0) {
-        a.rhs[k] = m.ub - su;                 // comj (:1624-1629)
-        a.rhs[a.nseg + k] = m.vb - sv;
+        a.rhs[k] = mp->ub - su;                 // comj (:1624-1629)
+        a.rhs[a.nseg + k] = mp->vb - sv;
     }
 }
 
