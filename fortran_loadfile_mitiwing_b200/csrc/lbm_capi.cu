@@ -173,8 +173,9 @@ template <typename P> void free_devp(P *&p)
     p = nullptr;
 }
 
-// waits for all of the handle's queued work (lattice, immersed-boundary and
-// factorization streams): before its device buffers are rewritten or freed
+// waits for all of the handle's queued work (lattice, immersed-boundary,
+// check and factorization streams): before its device buffers are rewritten
+// or freed
 void quiesce(lbm_handle *h)
 {
     if (h->fstream) cudaStreamSynchronize(h->fstream);
@@ -448,9 +449,10 @@ int collect_timing(lbm_handle *h, int count, bool split)
 
 // The per-step sequence. Without a body, or with the split off: IB chain,
 // then the fused lattice update, on the main stream. With the split: the IB
-// chain runs on the side stream (after the previous step's inner update)
-// while the main stream updates the lattice outside the motion envelope;
-// the main stream then waits for the IB chain and updates the envelope.
+// flow chain runs on the side stream (after the previous step) and its force
+// row and residual check on the check stream, while the main stream updates
+// every node outside the step's correction tiles; the main stream's step
+// ends once the side stream has updated the correction tiles.
 int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool fields_every)
 {
     // the mass is checked at every copy of force rows of lbm_run (every
@@ -479,7 +481,7 @@ int run_steps(lbm_handle *h, int nsteps, double *rows_out, int *done_out, bool f
         h->batch_in_half[half] = b;
         if (h->nseg == 0 || s1 < s0) return LBM_OK;
         cudaStream_t st = split ? h->fstream : h->stream;
-        // the half's previous users: the side-stream chains of its steps
+        // the half's previous users: the flow chains and checks of its steps
         // (ev_free) and the lattice kernels of those steps on the main stream,
         // which read the slots' patch rectangles and tile counts (ev_inner:
         // the main stream's last completed step)
