@@ -85,6 +85,16 @@ __host__ __device__ constexpr int stage_cap(int nb)
                ? (SOLVE_SMEM_BUDGET - 16 - 2 * nb * BS * (int)sizeof(double)) / (BS * GW * (int)sizeof(double))
                : STAGE_BLOCKS;
 }
+// factor blocks a solve of nb blocks stages at once: level 1's odd blocks or
+// those of all the levels above it together, whichever is more (the first
+// and the second staging of the resident form), within stage_cap
+__host__ __device__ constexpr int stage_blocks(int nb)
+{
+    int upper = 0;
+    for (int st = 2; st < nb; st <<= 1) upper += (nb + st - 1) / (2 * st);
+    const int need = nb / 2 > upper ? nb / 2 : upper;
+    return need < stage_cap(nb) ? need : stage_cap(nb);
+}
 constexpr int WS = BS * GP + BS * FL + BS * GP;   // workspace per warp (doubles)
 constexpr int NPART = 3 * LBM_MAXW + 3;           // per-CTA partials of ib_tile_update
 constexpr int TILE = 16;                          // correction-patch tile (nodes per side)
@@ -861,7 +871,8 @@ __global__ void __launch_bounds__(FACTOR_THREADS, 65536 / (FACTOR_THREADS * 128)
     if (tid == 0 && bad) atomicOr(a.status, LBM_ST_SOLVER);
 }
 
-// The flow-dependent solve of one step, one CTA of SOLVE_THREADS threads,
+// The flow-dependent solve of one step, one CTA (solve_threads: up to
+// SOLVE_THREADS threads),
 // with the cyclic-reduction factors of the step's slot:
 //   forward, st = 1, 2, 4, ...:  r_e -= F_L(q)^T r_q + F_U(p)^T r_p  (even e)
 //   block 0:                     x_0 = D_0^-1 r_0
@@ -891,7 +902,11 @@ __global__ void __launch_bounds__(SOLVE_THREADS, 1024 / SOLVE_THREADS) ib_solve(
     const int warp = tid >> 5, lane = tid & 31, nw = nt >> 5;
     const int nb = (n + BS - 1) / BS;
     double *stage_buf = smem;
-    const int scap = stage_cap(nb);
+    // the staged blocks the launch made room for (solve_smem: stage_blocks(nb)),
+    // read back from the dynamic shared-memory size rather than recomputed
+    uint32_t dsm;
+    asm("mov.u32 %0, %%dynamic_smem_size;" : "=r"(dsm));
+    const int scap = ((int)dsm - 16 - 2 * nb * BS * (int)sizeof(double)) / (BS * GW * (int)sizeof(double));
     double *X = smem + scap * BS * GW;
     uint64_t *bar = reinterpret_cast<uint64_t *>(X + 2 * nb * BS);
     __shared__ int timed_out;
@@ -1572,7 +1587,18 @@ constexpr size_t kSolveSmemMax = SOLVE_SMEM_BUDGET;
 size_t solve_smem(int nseg)
 {
     const int nb = (nseg + BS - 1) / BS;
-    return sizeof(double) * ((size_t)stage_cap(nb) * BS * GW + 2 * (size_t)nb * BS) + 16;
+    return sizeof(double) * ((size_t)stage_blocks(nb) * BS * GW + 2 * (size_t)nb * BS) + 16;
+}
+
+// threads of the solve's CTA: one warp per even block of the first level
+// (the widest), from 4 to SOLVE_THREADS / 32 warps. A solve of a few hundred
+// markers then holds a fraction of an SM beside the lattice kernel instead
+// of a whole one; each block's arithmetic is one warp's whatever the count,
+// so the results do not depend on it.
+int solve_threads(int nseg)
+{
+    const int nb = (nseg + BS - 1) / BS;
+    return 32 * std::min(SOLVE_THREADS / 32, std::max(4, (nb + 1) / 2));
 }
 
 // arguments of the flow chain of the step held in buffer slot `slot`; for
@@ -1641,7 +1667,7 @@ int launch_flow_t(lbm_handle *h, const void *fin, void *fout, void *fields, int 
         h->launches += 1;
     }
     if (after_interp && cudaEventRecord(after_interp, st) != cudaSuccess) return -1;
-    ib_solve<false><<<1, SOLVE_THREADS, solve_smem(h->nseg), st>>>(a, nullptr, step_index, ring_slot);
+    ib_solve<false><<<1, solve_threads(h->nseg), solve_smem(h->nseg), st>>>(a, nullptr, step_index, ring_slot);
     const int grid = std::min(h->patch_gx() * h->patch_gy(), 2 * 148);   // strided over the correction tiles
     const KFArgs<C> kf = make_kf_args<C>(h, fin, fout, fields, KF_OUTER);
     if (fields)
@@ -1781,7 +1807,8 @@ int launch_flow_batch_t(lbm_handle *const *hs, int ncase, const IBArgs *dargs, c
     const int ns = max_seg(hs, ncase);
     ib_interp<T, true><<<dim3((ns + 7) / 8, 1, ncase), 256, 0, st>>>(IBArgs{}, dargs);
     if (after_interp && cudaEventRecord(after_interp, st) != cudaSuccess) return -1;
-    ib_solve<true><<<dim3(1, 1, ncase), SOLVE_THREADS, solve_smem(ns), st>>>(IBArgs{}, dargs, step_index, ring_slot);
+    ib_solve<true><<<dim3(1, 1, ncase), solve_threads(ns), solve_smem(ns), st>>>(IBArgs{}, dargs, step_index,
+                                                                                ring_slot);
     int tiles = 1;
     for (int c = 0; c < ncase; ++c) tiles = std::max(tiles, hs[c]->patch_gx() * hs[c]->patch_gy());
     const dim3 grid(std::min(tiles, 2 * 148), 1, ncase);
