@@ -99,8 +99,11 @@ struct lbm_batch {
     void *d_seg[2] = {}, *h_seg[2] = {};
     cudaEvent_t ev_gdone[2] = {};
     // events of the captured stream code (never waited on outside a capture):
-    // fork, upload, joins, and per step the flow chain's points, then one per
-    // factorization launch of the segment
+    // [1] upload done, [2] [3] the main and factor streams' joins, [4] to [8]
+    // the step's points (flow ready, correction tiles done, checks done, step
+    // done, interpolation done), then one per factorization launch of the
+    // segment, then the checks of the two step parities and the check
+    // stream's join ([0] is not used)
     cudaEvent_t ev_cap[9 + 2 * kGraphSteps + 3] = {};
     cudaEvent_t ev_gpre = nullptr;   // the factor stream's work before a graph launch
     struct GraphEntry {
@@ -643,7 +646,6 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
             cudaEvent_t *E = b->ev_cap;
             // the checks of steps t (parity t & 1) and the check stream's join
             cudaEvent_t *EC = b->ev_cap + 9 + 2 * kGraphSteps;
-            BCK(cudaEventRecord(E[0], b->side), "event");
             BCK(cudaMemcpyAsync(ds, hs, used, cudaMemcpyHostToDevice, b->side), "upload");
             BCK(cudaEventRecord(E[1], b->side), "event");
             BCK(cudaStreamWaitEvent(b->main, E[1], 0), "wait");

@@ -884,6 +884,10 @@ int lbm_destroy(lbm_t *h)
     if (h->side) cudaStreamSynchronize(h->side);
     if (h->cstream) cudaStreamSynchronize(h->cstream);
     if (h->fstream) cudaStreamSynchronize(h->fstream);
+    // the frees above went to the pool on the main stream: once they have
+    // completed, an allocation on any other stream may reuse the memory (one
+    // made before the driver has seen them complete maps new memory instead)
+    if (h->stream) cudaStreamSynchronize(h->stream);
     for (auto &e : h->ev) cudaEventDestroy(e);
     for (auto &e : h->ev_side) cudaEventDestroy(e);
     if (h->ev_ib) cudaEventDestroy(h->ev_ib);
