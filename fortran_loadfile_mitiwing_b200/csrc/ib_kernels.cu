@@ -1800,6 +1800,8 @@ int max_seg(lbm_handle *const *hs, int n)
     return m;
 }
 
+constexpr int kBatchTileCtas = 64;
+
 template <typename T, typename C>
 int launch_flow_batch_t(lbm_handle *const *hs, int ncase, const IBArgs *dargs, const void *dkf, int step_index,
                         int ring_slot, bool fields, cudaStream_t st, cudaEvent_t after_interp)
@@ -1809,9 +1811,14 @@ int launch_flow_batch_t(lbm_handle *const *hs, int ncase, const IBArgs *dargs, c
     if (after_interp && cudaEventRecord(after_interp, st) != cudaSuccess) return -1;
     ib_solve<true><<<dim3(1, 1, ncase), solve_threads(ns), solve_smem(ns), st>>>(IBArgs{}, dargs, step_index,
                                                                                 ring_slot);
+    // CTAs per case, strided over the case's correction tiles: the patch
+    // grids bound the tiles several times over (a sweep case of chord 256
+    // has some 60 correction tiles in a grid of hundreds), and CTAs past a
+    // case's tiles still take lattice slots at the flow chain's priority, so
+    // a batch launches at most kBatchTileCtas per case
     int tiles = 1;
     for (int c = 0; c < ncase; ++c) tiles = std::max(tiles, hs[c]->patch_gx() * hs[c]->patch_gy());
-    const dim3 grid(std::min(tiles, 2 * 148), 1, ncase);
+    const dim3 grid(std::min(tiles, kBatchTileCtas), 1, ncase);
     const KFArgs<C> *kf = (const KFArgs<C> *)dkf;
     if (fields)
         ib_tile_update<T, C, true, true><<<grid, 256, 0, st>>>(IBArgs{}, dargs, KFArgs<C>{}, kf, step_index, ring_slot);
