@@ -96,6 +96,8 @@ ABI = {
     "lbm_describe_status": (C.c_int, [C.c_uint, C.c_char_p, C.c_int]),
     "lbm_device_check": (C.c_int, [C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "lbm_write_tecplot": (C.c_int, [_P, C.c_char_p, C.c_int, C.c_int, C.c_int]),
+    "lbm_write_gforce": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, _D,
+                                   _D]),
     "lbm_write_tecplot_fields": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                            C.c_double, C.c_double, C.c_int, C.c_int, _D, _D, _D, C.c_int, C.c_int,
                                            _D, _D]),

@@ -162,6 +162,63 @@ bool write_field_zone(FILE *f, const FieldGrid &g)
     return true;
 }
 
+// g<n>.dat of the reference's output_gforce (solution.f90:240-267): one line
+// of (25e25.17) per position of its loop, which runs i over 1..Ny (outer)
+// and j over 1..Nx and writes ox + (i-1) scale, oy + (j-1) scale,
+// gforce(i,j,1), gforce(i,j,2), as written. gforce is an (Nx,Ny) array;
+// positions the loop reaches outside it (j > Ny when Nx > Ny) and null
+// arrays write 0, the value gforce holds on the live path (move_boundary
+// zeroes it at the support nodes, airfoil.f90:280-281, and no live routine
+// writes it).
+struct GforceGrid {
+    int nx, ny;
+    double ox, oy, scale;
+    const double *gx, *gy;   // (nx, ny), x fastest; nullable
+};
+
+int gforce_line(const GforceGrid &g, int i, int j, char *out)   // loop position, 0-based
+{
+    double fx = 0.0, fy = 0.0;
+    if (i < g.nx && j < g.ny) {
+        const size_t q = (size_t)j * g.nx + i;
+        if (g.gx) fx = g.gx[q];
+        if (g.gy) fy = g.gy[q];
+    }
+    const double vals[4] = {g.ox + (double)i * g.scale, g.oy + (double)j * g.scale, fx, fy};
+    int k = 0;
+    for (int c = 0; c < 4; ++c) k += fmt_e(out + k, vals[c], 25, 17);
+    out[k++] = '\n';
+    return k;
+}
+
+// the rows of the loop (i) written by threads into per-chunk buffers, in order
+bool write_gforce_zone(FILE *f, const GforceGrid &g)
+{
+    const int line = 4 * 25 + 1;
+    unsigned nt = std::thread::hardware_concurrency();
+    nt = nt ? std::min(nt, 32u) : 4u;
+    const int rows_per_chunk = std::max(1, (int)(4u << 20) / (line * g.nx));   // ~4 MB of text per chunk
+    for (int r0 = 0; r0 < g.ny; r0 += rows_per_chunk * (int)nt) {
+        std::vector<std::string> buf(nt);
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < nt; ++t) {
+            const int a = r0 + (int)t * rows_per_chunk, b = std::min(g.ny, a + rows_per_chunk);
+            if (a >= b) break;
+            th.emplace_back([&, t, a, b]() {
+                std::string &s = buf[t];
+                s.resize((size_t)(b - a) * g.nx * line);
+                char *p = &s[0];
+                for (int i = a; i < b; ++i)
+                    for (int j = 0; j < g.nx; ++j) p += gforce_line(g, i, j, p);
+            });
+        }
+        for (auto &x : th) x.join();
+        for (unsigned t = 0; t < th.size(); ++t)
+            if (!write_all(f, buf[t].data(), buf[t].size())) return false;
+    }
+    return true;
+}
+
 // contour points xb1, yb1 (airfoil.f90:255-266) of step `s` (1-based step
 // index of the motion table row the step used)
 void contour_points(const lbm_handle *h, int s, std::vector<double> &x, std::vector<double> &y)
@@ -552,6 +609,21 @@ int lbm_write_tecplot_fields(const char *path, int nx, int ny, double ox, double
     FieldGrid g{nx, ny, stride_x, stride_y, ox, oy, scale, uu, rho, u, v};
     std::string msg;
     return write_tecplot(path, 0, g, solution_time, wing_count, points_per_wing, xb1, yb1, msg);
+}
+
+int lbm_write_gforce(const char *path, int cycle, int nx, int ny, double ox, double oy, double scale,
+                     const double *gforce_x, const double *gforce_y)
+{
+    if (!path || nx < 1 || ny < 1 || !(scale > 0)) return LBM_ERR_ARG;
+    FILE *f = fopen(path, "wb");
+    if (!f) return LBM_ERR_IO;
+    // the two header lines: (a), then list-directed items
+    std::string head = "VARIABLES = \"X\" \"Y\" \"gforcex\" \"gforcey\" \n";
+    head += " zone,t=\"" + ld_int(cycle) + "\",i=" + ld_int(nx) + ",j=" + ld_int(ny) + "\n";
+    GforceGrid g{nx, ny, ox, oy, scale, gforce_x, gforce_y};
+    bool ok = write_all(f, head.data(), head.size()) && write_gforce_zone(f, g);
+    ok = (fclose(f) == 0) && ok;
+    return ok ? LBM_OK : LBM_ERR_IO;
 }
 
 int lbm_write_tecplot(lbm_t *h, const char *path, int cycle, int stride_x, int stride_y)

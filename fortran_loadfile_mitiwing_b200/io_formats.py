@@ -7,6 +7,7 @@
   F<n>.dat            Tecplot ASCII                solution.f90:129-238 (written by
                       the library: lbm_write_tecplot, Lbm.write_tecplot; from host
                       arrays: write_tecplot_fields)
+  g<n>.dat            (25e25.17) per loop position solution.f90:240-267 (write_gforce)
 """
 import ctypes as C
 import os
@@ -100,6 +101,21 @@ def write_tecplot_fields(path, rho, u, v, ox, oy, scale, uu, solution_time, stri
                                       _abi.dptr(yb1) if wing_count else None)
     if rc != 0:
         raise IOError(f"lbm_write_tecplot_fields({path}) = {rc}")
+
+
+def write_gforce(path, cycle, nx, ny, ox, oy, scale, gforce_x=None, gforce_y=None, lib=None):
+    """g<n>.dat of output_gforce through lbm_write_gforce: gforce_x, gforce_y
+    host arrays (ny, nx) or None for zeros, the live path's value."""
+    lib = lib or _abi.load_library()
+    a = [None if g is None else np.ascontiguousarray(g, dtype=np.float64).reshape(-1) for g in (gforce_x, gforce_y)]
+    for g in a:
+        if g is not None and g.size != nx * ny:
+            raise ValueError("gforce arrays must hold nx*ny values")
+    rc = lib.lbm_write_gforce(os.fsencode(path), int(cycle), int(nx), int(ny), float(ox), float(oy), float(scale),
+                              _abi.dptr(a[0]) if a[0] is not None else None,
+                              _abi.dptr(a[1]) if a[1] is not None else None)
+    if rc != 0:
+        raise IOError(f"lbm_write_gforce({path}) = {rc}")
 
 
 def edge_count(nx, ny):

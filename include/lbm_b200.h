@@ -310,6 +310,19 @@ LBM_API int lbm_describe_status(unsigned int status, char *message, int capacity
  *   of the reference's form='binary' file. Load after lbm_init of a handle
  *   with the same parameters, boundary and motion table. */
 LBM_API int lbm_write_tecplot(lbm_t *h, const char *path, int cycle, int stride_x, int stride_y);
+
+/* output_gforce (solution.f90:240-267): the file g<n>.dat (n = cycle) with
+ * the Eulerian force density gforce(Nx,Ny,2), host arrays in Fortran order
+ * (x fastest; each nullable: zeros). The header line is written as (a), the
+ * zone line list-directed in spirit; then one line of (25e25.17) per
+ * position of the reference's loop as written, i = 1..Ny outer, j = 1..Nx
+ * inner: ox+(i-1)scale, oy+(j-1)scale, gforce(i,j,1), gforce(i,j,2), with 0
+ * for positions outside the array (j > Ny, reached when Nx > Ny). On the
+ * live path gforce is 0 everywhere: move_boundary zeroes it at the support
+ * nodes (airfoil.f90:280-281) and no routine of the live step writes it;
+ * the live driver never calls output_gforce. */
+LBM_API int lbm_write_gforce(const char *path, int cycle, int nx, int ny, double ox, double oy, double scale,
+                             const double *gforce_x, const double *gforce_y);
 LBM_API int lbm_write_tecplot_fields(const char *path, int nx, int ny, double ox, double oy, double scale, double uu,
                                      double solution_time, int stride_x, int stride_y, const double *rho,
                                      const double *u, const double *v, int wing_count, int points_per_wing,

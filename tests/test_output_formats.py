@@ -92,3 +92,37 @@ def test_airfoil_motion_rows(tmp_path):
     io_formats.write_airfoil_motion(str(p), [0.0, 0.000625], 2)
     lines = p.read_text().splitlines()
     assert lines[1] == "     0.00062500" + "     0.00000000" * 6
+
+
+@pytest.mark.parametrize("nx,ny", [(5, 3), (3, 4)])
+def test_gforce_file_follows_the_write_statements(tmp_path, nx, ny):
+    """g<n>.dat (output_gforce, solution.f90:240-267) against its WRITE
+    statements restated: the (a) header, the zone line, then (25e25.17) of
+    ox+(i-1)scale, oy+(j-1)scale, gforce(i,j,1:2) for i = 1..Ny outer and
+    j = 1..Nx inner as the loop is written; positions outside the (Nx,Ny)
+    array (j > Ny when Nx > Ny) hold 0, as does every node without arrays."""
+    rng = np.random.default_rng(11)
+    gx, gy = rng.standard_normal((ny, nx)), rng.standard_normal((ny, nx)) * 1e-7
+    ox, oy, scale = -1.25, -0.5, 0.01
+    path = tmp_path / "g7.dat"
+    io_formats.write_gforce(path, 7, nx, ny, ox, oy, scale, gx, gy)
+    lines = open(path).read().split("\n")
+    assert lines[0] == 'VARIABLES = "X" "Y" "gforcex" "gforcey" '
+    # list-directed items: integers in 12 columns (the spacing is the
+    # compiler's; the values and their order are the reference's)
+    assert lines[1] == f' zone,t="{7:12d}",i={nx:12d},j={ny:12d}'
+    assert lines[1].replace(" ", "") == f'zone,t="7",i={nx},j={ny}'
+    want = []
+    fx_all, fy_all = gx.reshape(-1), gy.reshape(-1)   # gforce(i,j) at (i-1) + (j-1) nx
+    for i in range(ny):
+        for j in range(nx):
+            inside = i < nx and j < ny
+            fx = fx_all[j * nx + i] if inside else 0.0
+            fy = fy_all[j * nx + i] if inside else 0.0
+            want.append("".join(fortran_e(v, 25, 17) for v in (ox + i * scale, oy + j * scale, fx, fy)))
+    assert lines[2:2 + nx * ny] == want
+    assert lines[2 + nx * ny:] == [""]
+    zero = tmp_path / "g8.dat"
+    io_formats.write_gforce(zero, 8, nx, ny, ox, oy, scale)
+    body = open(zero).read().split("\n")[2:2 + nx * ny]
+    assert all(ln[50:] == fortran_e(0.0, 25, 17) * 2 for ln in body)
