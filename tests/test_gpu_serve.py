@@ -32,17 +32,21 @@ def test_estimate_covers_device_bytes(gpu_lib, precision):
         assert got <= est <= got * 1.02, (precision, i, est, got)
 
 
-@pytest.mark.parametrize("workers", [0, 1])
-def test_served_results_equal_alone(gpu_lib, workers):
-    lens = [30, 52, 41, 23, 35]
+@pytest.mark.parametrize("workers,tick", [(0, 7), (1, 7), (1, 40)])
+def test_served_results_equal_alone(gpu_lib, workers, tick):
+    """Ticks of 7 steps run every step from the host; ticks of 40 replay
+    graph segments of 16 steps between their first and last steps."""
+    lens = [30, 52, 41, 23, 35] if tick < 20 else [60, 90, 75, 44, 66]
     reqs = [Request(i, make(i, n)) for i, n in enumerate(lens)]
     ests = [estimate_device_bytes(r.make()) for r in reqs]
     budget = sorted(ests)[-1] + sorted(ests)[-2]          # room for two cases at most
-    with Server(budget, tick_steps=7, lib=gpu_lib, keep_handles=True, workers=workers) as srv:
+    with Server(budget, tick_steps=tick, lib=gpu_lib, keep_handles=True, workers=workers) as srv:
         for r in reqs:
             srv.submit(r)
         while not srv.idle():
             srv.tick(wait_for_ready=True)
+        if tick >= 20:
+            assert srv.batch.graph_stats()[0] > 0         # steps run as graph segments
         res = sorted(srv.done, key=lambda r: r.rid)
         assert [r.rid for r in res] == list(range(len(lens)))
         assert 1 <= srv.peak_cases <= 2 and srv.peak_used <= budget
