@@ -1,7 +1,8 @@
 """Host logic of the serving loop: first-come first-served admission against
 a byte budget, the one-at-a-time queue model, arrivals, the device-memory
 estimate's arithmetic (its agreement with what a case holds is a GPU test),
-and the server's join/finish bookkeeping over a stand-in for the device."""
+and the server's join/finish bookkeeping over a stand-in for the device, and
+the batch autotuner's choice over a stand-in for the library."""
 import math
 
 import numpy as np
@@ -240,3 +241,39 @@ def test_cancel_waiting_preparing_and_running(monkeypatch):
     assert res[0].error is None and res[0].steps == 30
     assert res[2].error is None and res[2].steps == 30
     assert sorted(_FakeCase.closed) == [0, 1, 2]
+
+
+def test_batch_autotune_keeps_the_fastest_pair():
+    """Batch.autotune times every (rows per CTA, CTAs per SM) pair on the
+    device in alternating order over its rounds, keeps each pair's best
+    trial and leaves the batch on the fastest pair; a stand-in replaces the
+    library calls (the GPU test checks the results do not depend on it)."""
+    from fortran_loadfile_mitiwing_b200.solver import Batch
+    b = Batch.__new__(Batch)
+    b.rows, b.occupancy, b.b = 0, 0, None
+    cost = {(4, 0): 1.3, (4, 3): 1.4, (8, 0): 1.0, (8, 3): 0.9, (16, 0): 1.1, (16, 3): 1.2}
+    trials = []
+
+    def set_rows(r):
+        b.rows = r
+
+    def set_occupancy(o):
+        b.occupancy = o
+
+    def run(n, keep_rows=True):
+        trials.append((b.rows, b.occupancy))
+        b._n = n
+
+    def device_time():
+        # a slower first trial of each pair: the best of the rounds is kept
+        first = trials.count((b.rows, b.occupancy)) == 1
+        return cost[(b.rows, b.occupancy)] * b._n * (1.5 if first else 1.0), b._n
+
+    b.set_rows, b.set_occupancy, b.run, b.device_time = set_rows, set_occupancy, run, device_time
+    timing = b.autotune(steps_per_trial=5, candidates=(4, 8, 16), rounds=2, occupancy=(0, 3))
+    assert set(timing) == set(cost)
+    assert trials[:6] == [(r, o) for r in (4, 8, 16) for o in (0, 3)]
+    assert trials[6:] == trials[:6][::-1]                     # the second round in reverse order
+    for pair, t in timing.items():
+        assert t == pytest.approx(cost[pair] / 1e3)            # seconds per step, best trial
+    assert (b.rows, b.occupancy) == (8, 3)
