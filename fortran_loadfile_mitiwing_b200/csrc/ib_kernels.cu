@@ -1876,13 +1876,16 @@ int launch_flow_batch(lbm_handle *const *hs, int ncase, const void *dargs, const
 }
 
 // force rows and residual checks of one step of every case
-int launch_check_batch(lbm_handle *const *hs, int ncase, const void *dargs, int ring_slot, cudaStream_t st)
+int launch_check_batch(lbm_handle *const *hs, int ncase, const void *dargs, int ring_slot, bool residual,
+                       cudaStream_t st)
 {
     if (ncase <= 0) return 0;
     const IBArgs *d = (const IBArgs *)dargs;
     const int ns = max_seg(hs, ncase);
     ib_forces<true><<<dim3(1, 1, ncase), 256, 0, st>>>(IBArgs{}, d, ring_slot);
+    for (int c = 0; c < ncase; ++c) hs[c]->launches += 1;
+    if (!residual) return cudaGetLastError() == cudaSuccess ? 0 : -1;   // no case checks this step
     ib_residual<true><<<dim3((ns + 7) / 8, 1, ncase), 256, 0, st>>>(IBArgs{}, d);
-    for (int c = 0; c < ncase; ++c) hs[c]->launches += 2;
+    for (int c = 0; c < ncase; ++c) hs[c]->launches += 1;
     return cudaGetLastError() == cudaSuccess ? 0 : -1;
 }

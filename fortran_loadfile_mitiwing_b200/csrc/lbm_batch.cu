@@ -559,6 +559,7 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
     struct StepPlan {
         int cur = -1, next = -1;    // factorization groups before / after the flow chain
         std::vector<int> waits;     // groups of this segment the flow chain waits for
+        bool residual = false;      // some case checks its solve residual
     };
     auto graph_segment = [&]() -> int {
         const int G = kGraphSteps, na = (int)act.size();
@@ -612,6 +613,7 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
                 ib_args_write(h, h->fbuf[h->cur], q, ia);
                 // a segment holds neither the call's nor a case's last step
                 ia->check_res = (h->n + 1) % K == 0;
+                p.residual = p.residual || ia->check_res;
                 ia->ring_row = pending + t;
                 kf_args_write(h, h->fbuf[h->cur], h->fbuf[h->cur ^ 1], nullptr, KF_OUTER,
                               hs + off_k + ((size_t)t * na + c) * b->kf_sz);
@@ -633,7 +635,7 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
         for (lbm_handle *h : act)
             sig.insert(sig.end(), {(long long)(uintptr_t)h, h->nseg, h->patch_gx(), h->patch_gy(), h->static_order});
         for (const StepPlan &p : plan) {
-            sig.insert(sig.end(), {p.cur, p.next, (long long)p.waits.size()});
+            sig.insert(sig.end(), {p.cur, p.next, (long long)p.residual, (long long)p.waits.size()});
             sig.insert(sig.end(), p.waits.begin(), p.waits.end());
         }
         for (const GroupPlan &g : groups) {
@@ -678,7 +680,7 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
                     return berr(b, LBM_ERR_CUDA, "batch: launch flow");
                 BCK(cudaEventRecord(E[5], b->side), "event");
                 BCK(cudaStreamWaitEvent(b->cstream, E[5], 0), "wait");
-                if (launch_check_batch(act.data(), na, sa, 0, b->cstream))
+                if (launch_check_batch(act.data(), na, sa, 0, p.residual, b->cstream))
                     return berr(b, LBM_ERR_CUDA, "batch: launch check");
                 BCK(cudaEventRecord(EC[t & 1], b->cstream), "event");
                 BCK(cudaEventRecord(E[6], b->cstream), "event");   // flow chains and checks of step t
@@ -802,6 +804,7 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
         // steps back, is done)
         BCK(cudaEventSynchronize(b->ev_upload[buf]), "sync upload");
         tkey_now.clear();
+        bool any_check = false;   // some case checks its solve residual this step
         for (size_t c = 0; c < act.size(); ++c) {
             lbm_handle *h = act[c];
             const int q = h->n % b->nslots;
@@ -820,6 +823,7 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
             // the solve-residual check: last step of the case's factorization
             // batch, of the call, or of the case's motion
             ia->check_res = (h->n + 1) % K == 0 || step == nsteps - 1 || h->n >= last_step[act_idx[c]];
+            any_check = any_check || ia->check_res;
             ia->ring_row = pending;
             kf_args_write(h, fin, fout, fd, KF_OUTER, (char *)b->h_kargs[buf] + c * b->kf_sz);
             int gx, gy;
@@ -880,7 +884,7 @@ int lbm_batch_run(lbm_batch_t *b, int nsteps, double *const *force_rows, int *do
         }
         BCK(cudaEventRecord(b->ev_ib, b->side), "event");
         BCK(cudaStreamWaitEvent(b->cstream, b->ev_ib, 0), "wait");
-        if (launch_check_batch(act.data(), (int)act.size(), b->d_sargs[buf], pending, b->cstream)) {
+        if (launch_check_batch(act.data(), (int)act.size(), b->d_sargs[buf], pending, any_check, b->cstream)) {
             rc = berr(b, LBM_ERR_CUDA, "batch: launch check");
             break;
         }

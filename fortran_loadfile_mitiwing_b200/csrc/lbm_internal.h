@@ -259,7 +259,9 @@ void ib_factor_args_write(lbm_handle *h, int step0, int count, void *dst);
 int launch_factor_batch(lbm_handle *const *hs, int ncase, const void *dargs, int step0, int count, cudaStream_t st);
 int launch_flow_batch(lbm_handle *const *hs, int ncase, const void *dargs, const void *dkf, int step_index,
                       int ring_slot, bool fields, cudaStream_t st, cudaEvent_t after_interp = nullptr);
-int launch_check_batch(lbm_handle *const *hs, int ncase, const void *dargs, int ring_slot, cudaStream_t st);
+// residual: some case runs its solve-residual check this step (IBArgs::check_res)
+int launch_check_batch(lbm_handle *const *hs, int ncase, const void *dargs, int ring_slot, bool residual,
+                       cudaStream_t st);
 int ib_tile_ints();   // ints per patch tile of the tile lists
 int launch_residual(lbm_handle *h, const void *fa, const void *fb, double *out2);
 int launch_unpack(lbm_handle *h, const void *fsrc, double *dst);   // deviation -> f (FP64)

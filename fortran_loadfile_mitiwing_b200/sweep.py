@@ -18,8 +18,10 @@ Each form runs a fixed sample of steps per case after a warm-up; the report
 gives the aggregate lattice updates per second and the cases per hour that
 rate gives for 5 flapping periods of every case (a case's period is
 c / (f U0) steps, f = St / (2 heave)). Run as
-`python -m fortran_loadfile_mitiwing_b200.sweep [--cases N] [--steps S]`;
-prints one JSON object. Needs a GPU.
+`python -m fortran_loadfile_mitiwing_b200.sweep [--cases N] [--steps S]
+[--forms alone_fp32,batch_fp32,batch_fp16] [--no-tune]`, or with `--floor`
+for the per-step floor of batches of tiny cases; prints one JSON object.
+Needs a GPU.
 """
 import argparse
 import json
@@ -154,22 +156,31 @@ def main():
     ap.add_argument("--warmup", type=int, default=12)
     ap.add_argument("--seed", type=int, default=2026)
     ap.add_argument("--floor", action="store_true", help="only the per-step floor of batches of tiny cases")
+    ap.add_argument("--forms", default="alone_fp32,batch_fp32,batch_fp16",
+                    help="comma-separated subset of alone_fp32, batch_fp32, batch_fp16")
+    ap.add_argument("--no-tune", action="store_true", help="batches keep the cases' own rows per CTA")
     args = ap.parse_args()
     if args.floor:
         print(json.dumps(launch_floor()))
         return
+    forms = [f.strip() for f in args.forms.split(",") if f.strip()]
     specs = sweep_specs(args.cases, args.seed)
     res = {"cases": args.cases, "steps_per_case": args.steps, "seed": args.seed,
            "grid_nodes_total": sum(s["nx"] * s["ny"] for s in specs)}
-    r, t = run_alone(specs, args.steps, args.warmup, "fp32")
-    res["alone_fp32"] = {"mlups": r / 1e6, "seconds": t, "cases_per_hour_5_periods": cases_per_hour(specs, r)}
+    if "alone_fp32" in forms:
+        r, t = run_alone(specs, args.steps, args.warmup, "fp32")
+        res["alone_fp32"] = {"mlups": r / 1e6, "seconds": t, "cases_per_hour_5_periods": cases_per_hour(specs, r)}
     for prec in ("fp32", "fp16"):
-        r, t, timing, choice = run_batch(specs, args.steps, args.warmup, prec)
+        if "batch_" + prec not in forms:
+            continue
+        r, t, timing, choice = run_batch(specs, args.steps, args.warmup, prec, tune=not args.no_tune)
         res["batch_" + prec] = {"mlups": r / 1e6, "seconds": t, "cases_per_hour_5_periods": cases_per_hour(specs, r),
                                 "autotuned": choice, "autotune_s_per_step": timing}
-    base = res["alone_fp32"]["cases_per_hour_5_periods"]
-    for k in ("batch_fp32", "batch_fp16"):
-        res[k]["vs_alone_fp32"] = res[k]["cases_per_hour_5_periods"] / base
+    if "alone_fp32" in res:
+        base = res["alone_fp32"]["cases_per_hour_5_periods"]
+        for k in ("batch_fp32", "batch_fp16"):
+            if k in res:
+                res[k]["vs_alone_fp32"] = res[k]["cases_per_hour_5_periods"] / base
     print(json.dumps(res))
 
 
