@@ -142,3 +142,18 @@ def test_motion_parser_errors(lib, tmp_path):
 def test_force_row_format():
     s = io_formats.format_force_row([0.0125, -1.23456789, 12.5])
     assert s == "     0.01250000    -1.23456789    12.50000000"
+
+
+def test_fortran_interfaces_name_declared_entry_points():
+    """Every bind(C, name=...) of the Fortran interfaces in INTEGRATION.md
+    names an entry point the header declares (a maintainer who pastes them
+    binds symbols that exist)."""
+    import os
+    import re
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    header = open(os.path.join(root, "include", "lbm_b200.h")).read()
+    declared = set(re.findall(r"LBM_API\s+[\w\s\*]+?\b(lbm_\w+)\s*\(", header))
+    doc = open(os.path.join(root, "INTEGRATION.md")).read()
+    bound = set(re.findall(r"bind\(C,\s*name='(lbm_\w+)'\)", doc))
+    assert bound, "no Fortran interfaces found"
+    assert bound <= declared, sorted(bound - declared)
